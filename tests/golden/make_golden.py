@@ -1,0 +1,253 @@
+"""Generate the golden fixtures in this folder by running the reference itself.
+
+The reference (kiliancmd/pycfd, pure Python) is imported from a source tree given
+on the command line (default ``/root/reference``) and driven through its own
+public API.  Nothing here runs on the GPU host: the fixtures it writes are the
+committed ``*.npz`` files beside this script, which the tests read.
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+Cases (all seeded, all synthetic):
+  rhs.npz        momentum RHS (Numba kernel) on random ghosted fields, blend 0 / 0.6
+  poisson.npz    assembled Poisson operators for six boundary/obstacle layouts
+  multigrid.npz  hierarchies (A_l, P_l, weights) and one V-cycle for four layouts
+  solvers.npz    solve() of every iterative solver on seeded right-hand sides
+  steps.npz      initialise + N steps for nine boundary/solver/scheme mixes
+  cavity64.npz   64x64 lid cavity, Re 100, CG 1e-10, adaptive dt: steps 100/500/2000
+  cylinder.npz   256x128 cylinder channel, MG-PCG, 30 steps with Cd/Cl history
+  masks.npz      circle_mask at 2048x1024 (packed bits) and at 256x128
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, REF)
+
+from pycfd.config import BCKind, BCSpec, SimulationConfig  # noqa: E402
+from pycfd.core import kernels  # noqa: E402
+from pycfd.core.mesh import StructuredMesh  # noqa: E402
+from pycfd.core.multigrid import MultigridHierarchy  # noqa: E402
+from pycfd.core.pressure import assemble_poisson_matrix, make_pressure_solver  # noqa: E402
+from pycfd.core.solver import ProjectionSolver  # noqa: E402
+from pycfd.core.timestepper import TimeStepper  # noqa: E402
+from pycfd.geometry.obstacles import circle_mask  # noqa: E402
+from pycfd.physics.incompressible import Simulation  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, OUT)
+import cases  # noqa: E402
+
+
+def save(name, **arrays):
+    path = os.path.join(OUT, name)
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {name}: {os.path.getsize(path) / 1024:.0f} KiB", flush=True)
+
+
+def csr_parts(prefix, A, out):
+    A = A.tocsr()
+    A.sort_indices()
+    out[prefix + "_data"] = A.data
+    out[prefix + "_indices"] = A.indices.astype(np.int32)
+    out[prefix + "_indptr"] = A.indptr.astype(np.int64)
+    out[prefix + "_shape"] = np.array(A.shape)
+
+
+def gen_rhs():
+    out = {}
+    for k, (nx, ny, blend) in enumerate(((24, 24, 0.0), (24, 24, 0.6), (20, 13, 0.6), (9, 31, 0.0))):
+        u = np.random.default_rng(10 + k).standard_normal((nx + 3, ny + 2))
+        v = np.random.default_rng(20 + k).standard_normal((nx + 2, ny + 3))
+        ru, rv = np.empty((nx + 1, ny)), np.empty((nx, ny + 1))
+        args = (0.01 * (1 + k), 0.02, 0.001 * (k + 1), blend, 0.1, -0.2)
+        kernels._kernel_serial(u, v, *args, ru, rv)
+        out.update({f"c{k}_u": u, f"c{k}_v": v, f"c{k}_args": np.array(args),
+                    f"c{k}_rhs_u": ru, f"c{k}_rhs_v": rv})
+    save("rhs.npz", **out)
+
+
+def poisson_cases():
+    m1 = StructuredMesh(12, 10, 1.2, 1.0)
+    m2 = StructuredMesh(8, 12, 1.0, 1.5)
+    m3 = StructuredMesh(10, 8)
+    m4 = StructuredMesh(16, 16)
+    m5 = StructuredMesh(12, 8, 1.5, 1.0)
+    m6 = StructuredMesh(8, 8)
+    ring = np.zeros((8, 8), bool)
+    ring[2:5, 2:5] = True
+    ring[3, 3] = False                       # a fluid cell enclosed by solid
+    return [
+        ("walls", m1, dict()),
+        ("periodic", m2, dict(periodic_x=True, periodic_y=True)),
+        ("periodic_x", m3, dict(periodic_x=True)),
+        ("obstacle", m4, dict(solid_mask=circle_mask(m4, (0.5, 0.5), 0.2).mask)),
+        ("dirichlet", m5, dict(dirichlet={"right": 0.3})),
+        ("isolated", m6, dict(solid_mask=ring)),
+    ]
+
+
+def gen_poisson():
+    out = {}
+    for name, mesh, kw in poisson_cases():
+        s = assemble_poisson_matrix(mesh, **kw)
+        csr_parts(name + "_A", s.A, out)
+        out[name + "_fluid"] = s.fluid
+        out[name + "_singular"] = np.array(s.singular)
+        out[name + "_pin"] = np.array(s.pin)
+        out[name + "_bc"] = s.bc_rhs
+        out[name + "_solid"] = kw.get("solid_mask", np.zeros(mesh.shape, bool))
+        out[name + "_geom"] = np.array([mesh.nx, mesh.ny, mesh.lx, mesh.ly,
+                                        kw.get("periodic_x", False), kw.get("periodic_y", False)],
+                                       dtype=float)
+    save("poisson.npz", **out)
+
+
+def gen_multigrid():
+    out = {}
+    m1 = StructuredMesh(32, 32)
+    m2 = StructuredMesh(24, 20, 1.2, 1.0)
+    m3 = StructuredMesh(40, 24, 5.0 / 3.0, 1.0)
+    m4 = StructuredMesh(33, 17, 33 / 17, 1.0)
+    mg_cases = [
+        ("walls", m1, dict()),
+        ("periodic", m2, dict(periodic_x=True, periodic_y=True)),
+        ("obstacle", m3, dict(solid_mask=circle_mask(m3, (0.6, 0.5), 0.2).mask)),
+        ("odd_dirichlet", m4, dict(dirichlet={"right": 0.0})),
+    ]
+    for name, mesh, kw in mg_cases:
+        s = assemble_poisson_matrix(mesh, **kw)
+        h = MultigridHierarchy(s.A, mesh.shape, s.fluid, s.singular)
+        out[name + "_nlev"] = np.array(h.n_levels)
+        for l, lv in enumerate(h.levels):
+            csr_parts(f"{name}_A{l}", lv.A, out)
+            if lv.P is not None:
+                csr_parts(f"{name}_P{l}", lv.P, out)
+            out[f"{name}_w{l}"] = np.array(lv.weight)
+            out[f"{name}_shape{l}"] = np.array(lv.shape)
+            out[f"{name}_active{l}"] = lv.active
+        r = np.random.default_rng(5).standard_normal(s.n)
+        out[name + "_r"] = r
+        out[name + "_z"] = h.apply(r)
+    save("multigrid.npz", **out)
+
+
+def gen_solvers():
+    out = {}
+    for case, mesh, kw in (("walls", StructuredMesh(24, 24), {}),
+                           ("periodic", StructuredMesh(16, 20, 1.0, 1.25),
+                            dict(periodic_x=True, periodic_y=True))):
+        s = assemble_poisson_matrix(mesh, **kw)
+        rhs = np.random.default_rng(7).standard_normal(mesh.shape)
+        p0 = 0.1 * np.random.default_rng(8).standard_normal(mesh.shape)
+        out[case + "_rhs"] = rhs
+        out[case + "_p0"] = p0
+        for kind, tol in (("cg", 1e-12), ("jacobi", 1e-7), ("sor", 1e-11),
+                          ("multigrid", 1e-12), ("mgcg", 1e-12), ("direct", 1e-12)):
+            solver = make_pressure_solver(kind, s, tol=tol, maxiter=200_000)
+            p = solver.solve(rhs, p0 if kind != "direct" else None)
+            out[f"{case}_{kind}_p"] = p
+            out[f"{case}_{kind}_it"] = np.array(solver.last_iterations)
+            out[f"{case}_{kind}_res"] = np.array(solver.last_residual)
+    save("solvers.npz", **out)
+
+
+def ref_config(d):
+    return cases.to_config(d, SimulationConfig, BCSpec, BCKind)
+
+
+def run_step_case(spec):
+    cfg = cases.step_config(spec, SimulationConfig, BCSpec, BCKind)
+    mesh = StructuredMesh.from_config(cfg)
+    solid = None
+    if "circle" in spec:
+        solid = circle_mask(mesh, *spec["circle"]).mask
+    solver = ProjectionSolver(cfg, mesh, solid)
+    u_init, v_init = cases.step_init(spec, cfg.nx, cfg.ny, cfg.lx, cfg.ly)
+    if spec.get("tg"):                       # the reference's own mesh coordinates
+        Xu, Yu = mesh.u_grid()
+        Xv, Yv = mesh.v_grid()
+        u_init, v_init = np.sin(Xu) * np.cos(Yu), -np.cos(Xv) * np.sin(Yv)
+    fields = solver.initialize(u_init, v_init)
+    init = (fields.u.copy(), fields.v.copy(), fields.p.copy())
+    fx, fy = [], []
+    if cfg.advection_scheme.value == "upwind":
+        solver.set_upwind_blend(solver.upwind_blend_for(fields, spec["dt"]))
+    for _ in range(spec["steps"]):
+        fields = solver.step(fields, spec["dt"])
+        fx.append(solver.body_force_reaction[0])
+        fy.append(solver.body_force_reaction[1])
+    return init, fields, np.array(fx), np.array(fy), solid
+
+
+def gen_steps():
+    out = {}
+    for name, spec in cases.STEP_CASES.items():
+        t0 = time.perf_counter()
+        init, f, fx, fy, solid = run_step_case(spec)
+        out.update({f"{name}_u0": init[0], f"{name}_v0": init[1], f"{name}_p0": init[2],
+                    f"{name}_u": f.u, f"{name}_v": f.v, f"{name}_p": f.p,
+                    f"{name}_fx": fx, f"{name}_fy": fy,
+                    f"{name}_solid": solid if solid is not None else np.zeros((1, 1), bool)})
+        print(f"  {name}: {time.perf_counter() - t0:.1f}s", flush=True)
+    save("steps.npz", **out)
+
+
+def cavity64_config():
+    return ref_config(cases.CAVITY64)
+
+
+def gen_cavity64():
+    sim = Simulation(cavity64_config())
+    out = {}
+    done = 0
+    for target in (100, 500, 2000):
+        sim.run(max_steps=target - done)
+        done = target
+        f = sim.fields
+        out.update({f"s{target}_u": f.u, f"s{target}_v": f.v, f"s{target}_p": f.p,
+                    f"s{target}_t": np.array(f.t), f"s{target}_step": np.array(f.step)})
+        print(f"  cavity64 step {target}: t={f.t:.6f}", flush=True)
+    save("cavity64.npz", **out)
+
+
+def gen_cylinder():
+    nx, ny = 256, 128
+    cfg = ref_config(cases.cylinder_cfg(nx, ny))
+    ob = circle_mask(StructuredMesh.from_config(cfg), (0.5, 0.5), 0.05)
+    u0, v0 = cases.cylinder_init(nx, ny)
+    sim = Simulation(cfg, obstacle=ob, u_init=u0, v_init=v0)
+    cd, cl = [], []
+    for _ in range(30):
+        sim.run(max_steps=1)
+        c = sim.force_coefficients()
+        cd.append(c[0])
+        cl.append(c[1])
+    f = sim.fields
+    save("cylinder.npz", u=f.u, v=f.v, p=f.p, t=np.array(f.t), cd=np.array(cd),
+         cl=np.array(cl), mask=ob.mask)
+
+
+def gen_masks():
+    big = StructuredMesh(2048, 1024, 2.0, 1.0)
+    m = circle_mask(big, (0.5, 0.5), 0.05).mask
+    small = StructuredMesh(256, 128, 2.0, 1.0)
+    m2 = circle_mask(small, (0.5, 0.5), 0.05).mask
+    save("masks.npz", big_bits=np.packbits(m.ravel()), big_count=np.array(int(m.sum())),
+         small=m2)
+
+
+if __name__ == "__main__":
+    which = set(sys.argv[2:]) or {"rhs", "poisson", "multigrid", "solvers", "steps",
+                                  "cavity64", "cylinder", "masks"}
+    for name in ("rhs", "poisson", "multigrid", "solvers", "steps", "cavity64",
+                 "cylinder", "masks"):
+        if name in which:
+            t0 = time.perf_counter()
+            globals()["gen_" + name]()
+            print(f"{name}: {time.perf_counter() - t0:.1f}s", flush=True)
