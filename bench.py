@@ -1,0 +1,243 @@
+"""Throughput of the projection step: cell-updates/s on the 512x512 Taylor-Green vortex.
+
+One step = one SSP-RK3 time step of the whole 512x512 doubly periodic vortex
+(Re 1000, fixed dt = 0.4*2pi/512, MG-PCG to 1e-10, three projections).
+value = cells x steps / device time of the timed steps (CUDA events on the
+launching stream, barrier + synchronise on both sides, max over ranks).  The
+working set (~60 MB) fits in the 126 MB L2, so L2 is flushed between timed
+steps by writing a 256 MB buffer outside the timed events.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed]
+
+--impl reference times the reference algorithm's CPU implementation (the NumPy/
+SciPy restatement in oracle/, which only this arm and the cpu_baseline leg run)
+on the host cores, on the same workload and metric.  Under torchrun every rank
+advances its own replica of the vortex (the path does not shard: replicas only)
+and rank 0 prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 512
+RE = 1000.0
+TOL = 1e-10
+METRIC = "cell-updates/s per projection step, mixed vs FP64 at 1e-8 div; HBM % peak"
+UNIT = "cell-updates/s"
+
+
+def tgv_config():
+    from pycfd_b200.config import BCKind, BCSpec, SimulationConfig
+    per = {w: BCSpec(BCKind.PERIODIC) for w in ("left", "right", "bottom", "top")}
+    return SimulationConfig(nx=N, ny=N, lx=2 * np.pi, ly=2 * np.pi, re=RE, dt=0.4 * 2 * np.pi / N,
+                            t_end=1e9, adaptive_dt=False, pressure_solver="mgcg", poisson_tol=TOL,
+                            boundary_config=per, name="tgv512")
+
+
+def tgv_init(mesh):
+    Xu, Yu = mesh.u_grid()
+    Xv, Yv = mesh.v_grid()
+    return np.sin(Xu) * np.cos(Yu), -np.cos(Xv) * np.sin(Yv)
+
+
+def workload_config(extra=None):
+    d = {"workload": f"taylor_green_{N}x{N}", "re": RE, "scheme": "ssp-rk3",
+         "pressure_solver": "mgcg", "poisson_tol": TOL, "dt": 0.4 * 2 * np.pi / N,
+         "cells": N * N, "cell_update": "one cell advanced by one full RK3 step (3 projections)",
+         "l2": "flushed between timed steps (256 MB write)"}
+    d.update(extra or {})
+    return d
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed steps run."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        rows = [r.split(", ") for r in out.strip().splitlines() if r.count(",") >= 6]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(steps=3):
+    """The oracle (NumPy/SciPy restatement of the reference) on a bounded sample."""
+    from oracle import OracleSolver
+    from pycfd_b200.mesh import StructuredMesh
+    cfg = tgv_config()
+    t0 = time.perf_counter()
+    s = OracleSolver(cfg)
+    u, v, p = s.initialize(*tgv_init(StructuredMesh.from_config(cfg)))
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u, v, p = s.step(u, v, cfg.dt)
+    el = time.perf_counter() - t0
+    return {"value": N * N * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} RK3 steps of the 512x512 vortex after initialisation "
+                      f"({el:.1f} s; setup {setup:.1f} s excluded); NumPy/SciPy, one thread"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import torch  # noqa: F401  (same process layout as the GPU arm)
+    steps = max(1, min(args.steps, 4))
+    cb = cpu_baseline(steps)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": 0, "ms_per_step": 1e3 * N * N / cb["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference", "config": workload_config(),
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    from pycfd_b200.mesh import StructuredMesh
+    cfg = tgv_config()
+    opts = GpuOptions(precision=args.precision)
+    solver = ProjectionSolver(cfg, options=opts)
+    f = solver.initialize(*tgv_init(solver.mesh))
+    dt = cfg.dt
+    for _ in range(args.warmup):
+        f = solver.step(f, dt)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    iters = []
+    clocks = Clocks(local) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        evs[k][0].record(stream)
+        f = solver.step(f, dt)
+        evs[k][1].record(stream)
+        iters.append(solver.last_stats.total_iterations)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop() if clocks else None
+    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms = float(t.item())
+    value = world * N * N * args.steps / (dev_ms / 1e3)
+    st = solver.field_stats(f)
+
+    # end to end through the public host-buffer call: copies inside the timed region
+    u_h = torch.empty(solver.mesh.u_shape, dtype=torch.float64).pin_memory()
+    v_h = torch.empty(solver.mesh.v_shape, dtype=torch.float64).pin_memory()
+    u_h.copy_(f.u)
+    v_h.copy_(f.v)
+    un, vn = u_h.numpy(), v_h.numpy()
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        un2, vn2, pn2 = solver.step_host(un, vn, dt)
+        un, vn = un2, vn2
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * N * N * e2e_steps / float(te.item())
+    h2d = (un.size + vn.size) * 8
+    d2h = (un.size + vn.size + pn2.size) * 8
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = peaks.get("hbm_gbs", 6650.0)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64/f32",
+                "data": "synthetic",
+                "config": workload_config({"precision": args.precision,
+                                           "parallelism": f"replicas x{world}",
+                                           "mgpcg_iterations_per_step": float(np.mean(iters)),
+                                           "max_div": st.max_div}),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "clocks": ck, "hbm_peak_gbs": hbm}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(2)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

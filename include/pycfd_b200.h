@@ -1,0 +1,213 @@
+/*
+ * pycfd_b200 -- C ABI of the B200-native projection hot path.
+ *
+ * The reference solver (kiliancmd/pycfd) is pure Python and exposes no foreign
+ * function interface; the entry points below are the calls its Python layer
+ * would bind if the per-timestep path were moved behind one.  Each one names
+ * the reference function or method it replaces (file:line in the reference
+ * project).  All device pointers are CUDA global memory on the current device;
+ * every launch goes to the `stream` argument (a cudaStream_t, NULL = legacy
+ * default stream).  Nothing here takes a framework tensor type.
+ *
+ * Array layout (pycfd/core/mesh.py:13-38): row-major doubles with y fastest,
+ *   u: (nx+3) x (ny+2)   v: (nx+2) x (ny+3)   p: (nx+2) x (ny+2)
+ * Poisson vectors are flat (nx*ny), index i*ny + j (pycfd/core/pressure.py:178).
+ *
+ * Every function returns 0 on success or a negative PCFD_E_* code;
+ * pycfd_last_error() gives the message of the last failure on this thread.
+ */
+#ifndef PYCFD_B200_H
+#define PYCFD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PCFD_OK 0
+#define PCFD_E_ARG (-1)        /* bad argument: maps to ValueError          */
+#define PCFD_E_CUDA (-2)       /* CUDA runtime error                         */
+#define PCFD_E_NOCONV (-3)     /* iterative solve failed: RuntimeError       */
+#define PCFD_E_STALL (-4)      /* SOR/Jacobi/MG stalled: RuntimeError        */
+#define PCFD_E_UNSUPPORTED (-5) /* configuration the GPU path rejects        */
+
+/* ---- boundary kinds (pycfd/config.py:85-94) ----------------------------- */
+#define PCFD_BC_NO_SLIP 0
+#define PCFD_BC_MOVING_WALL 1
+#define PCFD_BC_INLET 2
+#define PCFD_BC_OUTLET 3
+#define PCFD_BC_PRESSURE_OUTLET 4
+#define PCFD_BC_PERIODIC 5
+#define PCFD_BC_SYMMETRY 6
+
+/* ---- pressure solvers (pycfd/config.py:74-82; "direct" is not provided) -- */
+#define PCFD_SOLVER_CG 1
+#define PCFD_SOLVER_JACOBI 2
+#define PCFD_SOLVER_SOR 3
+#define PCFD_SOLVER_MULTIGRID 4
+#define PCFD_SOLVER_MGCG 5
+
+/* ---- time schemes (pycfd/config.py:46-59) ------------------------------- */
+#define PCFD_EULER 0
+#define PCFD_RK2 1
+#define PCFD_RK3 2
+
+/* ---- precision forms ---------------------------------------------------- */
+#define PCFD_FP64 0
+#define PCFD_MIXED 1   /* FP32 MG-PCG inner solve inside FP64 iterative refinement */
+
+#define PCFD_MAX_BODIES 8
+
+typedef struct pycfd_solver pycfd_solver;
+
+/* One multigrid level as built on the host (pycfd/core/multigrid.py:293-321).
+ * Level 0 is the fine Poisson operator, which the device applies matrix-free
+ * from the cell flags; its a_* fields are ignored.  For l >= 1, A_l is given
+ * in CSR and P_l (the prolongation from level l to level l-1, n_{l-1} x n_l)
+ * in CSR; restriction is its transpose, formed on the device side.         */
+typedef struct {
+    int n;                       /* unknowns on this level                   */
+    int shape_x, shape_y;        /* grid this level's unknowns lie on        */
+    double weight;               /* damped-Jacobi weight (4/3)/rho           */
+    const double* weighted_dinv; /* n: weight / diag (ignored on level 0)    */
+    const uint8_t* active;       /* n: 1 where the row is an active unknown  */
+    const int64_t* a_indptr;     /* CSR of A_l (l >= 1)                      */
+    const int32_t* a_indices;
+    const double* a_data;
+    const int64_t* p_indptr;     /* CSR of P_l (l >= 1)                      */
+    const int32_t* p_indices;
+    const double* p_data;
+} pycfd_mg_level;
+
+typedef struct {
+    int nx, ny;
+    double dx, dy, nu;
+    double body_fx, body_fy;                  /* config.body_force          */
+    int bc_kind[4];                           /* left, right, bottom, top   */
+    double bc_velocity[4];
+    double bc_p_ref[4];
+    const double* bc_profile[4];              /* parabolic inlet normal-face line
+                                                 (full ghosted line), or NULL */
+    const uint8_t* solid;                     /* nx*ny cell mask, or NULL    */
+    const uint8_t* body_id;                   /* nx*ny: body index+1 of a solid
+                                                 cell when several bodies report
+                                                 separate forces, else NULL  */
+    int n_bodies;                             /* 0 or 2..PCFD_MAX_BODIES     */
+    int solver_kind;                          /* PCFD_SOLVER_*               */
+    double tol;
+    int maxiter;
+    double sor_omega;
+    int mg_sweeps;
+    int time_scheme;                          /* PCFD_EULER/RK2/RK3          */
+    int precision;                            /* PCFD_FP64 / PCFD_MIXED      */
+    double inner_tol;                         /* mixed: inner FP32 relative tol */
+    int n_levels;                             /* multigrid solvers only      */
+    const pycfd_mg_level* levels;
+    const double* coarsest_inverse;           /* n_L x n_L row-major pseudo-inverse
+                                                 of the coarsest operator    */
+} pycfd_solver_desc;
+
+/* Per-call results the Python layer reads back (one small D2H copy). */
+typedef struct {
+    int iterations;          /* last solve: CG/MG-PCG iterations, sweeps or cycles */
+    int converged;           /* last solve met its tolerance                  */
+    int status;              /* 0 ok, PCFD_E_NOCONV / PCFD_E_STALL otherwise   */
+    int total_iterations;    /* summed over the solves of the last call        */
+    double last_residual;    /* ||b - A p|| / ||b|| of the last solve         */
+    double fx, fy;           /* immersed-boundary reaction force (solver.py:553-599) */
+    double body_fx[PCFD_MAX_BODIES], body_fy[PCFD_MAX_BODIES];
+    int ir_iterations;       /* mixed form: outer refinement passes, last solve */
+    int pad_;
+} pycfd_stats;
+
+/* Reductions over a state, for dt control, health and diagnostics
+ * (pycfd/core/timestepper.py:94-142, :208-212, :251-266;
+ *  pycfd/analysis/postprocess.py:73-79; pycfd/core/solver.py:545-550). */
+typedef struct {
+    double max_u, max_v;     /* max |u|, |v| over the physical faces          */
+    double max_du, max_dv;   /* max |u - u_prev|, |v - v_prev| (whole arrays) */
+    double max_div;          /* max |div u| over fluid cells                  */
+    double kinetic_energy;   /* 0.5 sum(uc^2+vc^2) dA, solid cells zeroed     */
+    double max_vorticity;    /* max |omega| averaged to cell centres          */
+    int finite;              /* 1 if u, v, p hold no NaN/Inf                  */
+    int pad_;
+} pycfd_field_stats;
+
+const char* pycfd_last_error(void);
+int pycfd_version(void);
+
+/* Build a solver: uploads masks, boundary tables and the multigrid hierarchy,
+ * allocates the device workspace.  Replaces ProjectionSolver.__init__
+ * (pycfd/core/solver.py:101-195) minus host assembly, and
+ * make_pressure_solver (pycfd/core/pressure.py:645-660). */
+int pycfd_solver_create(const pycfd_solver_desc* desc, pycfd_solver** out);
+int pycfd_solver_destroy(pycfd_solver* s);
+
+/* Fused momentum RHS, stateless: rhs_u (nx+1)*ny, rhs_v nx*(ny+1).
+ * Replaces kernels._momentum_rhs_body (pycfd/core/kernels.py:39-110). */
+int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double dx, double dy,
+                       double nu, double blend, double fx, double fy, double* rhs_u,
+                       double* rhs_v, void* stream);
+
+/* Cell divergence, stateless: out nx*ny.  ProjectionSolver.divergence
+ * (pycfd/core/solver.py:532-543). */
+int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy,
+                     double* out, void* stream);
+
+/* Boundary pass on (u, v) in place.  BoundaryManager.apply_velocity
+ * (pycfd/core/boundary.py:375-379), plus enforce_global_mass_balance (:423-487)
+ * when mass_balance != 0. */
+int pycfd_apply_velocity_bc(pycfd_solver* s, double* u, double* v, int predictor,
+                            int mass_balance, void* stream);
+
+/* Poisson solve: rhs (nx*ny, the divergence over dt) -> p (nx*ny).  p0 is the
+ * warm start or NULL.  PoissonSolverBase.solve (pycfd/core/pressure.py:325-327)
+ * with CGSolver :366-398, JacobiSolver :410-454, SORSolver :457-526,
+ * MultigridSolver :545-574, MultigridCGSolver :577-632. */
+int pycfd_poisson_solve(pycfd_solver* s, const double* rhs, const double* p0, double* p,
+                        void* stream);
+
+/* One V-cycle from zero applied to r: the preconditioner.
+ * MultigridHierarchy.apply (pycfd/core/multigrid.py:460-474). */
+int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream);
+
+/* Project (u, v) in place and write the ghosted pressure p.  Uses and updates
+ * the solver's warm start.  ProjectionSolver.project (pycfd/core/solver.py:643-683). */
+int pycfd_project(pycfd_solver* s, double* u, double* v, double* p, double dt, void* stream);
+
+/* Initial state: BCs, mass balance, mask, projection with dt = 1.
+ * ProjectionSolver.initialize (pycfd/core/solver.py:301-329); u, v hold the
+ * initial physical faces on entry (ghosts zero) and p receives the pressure. */
+int pycfd_initialize(pycfd_solver* s, double* u, double* v, double* p, void* stream);
+
+/* One projected Euler substep: (u, v) -> (us, vs, p); inputs untouched.
+ * ProjectionSolver.substep (pycfd/core/solver.py:612-640). */
+int pycfd_substep(pycfd_solver* s, const double* u, const double* v, double* us, double* vs,
+                  double* p, double dt, double blend, void* stream);
+
+/* One time step with the configured scheme: (u0, v0) -> (u, v, p).
+ * ProjectionSolver.step (pycfd/core/solver.py:686-731). */
+int pycfd_step(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
+               double* p, double dt, double blend, void* stream);
+
+/* The same step on HOST buffers: copies the inputs in, steps, copies u, v, p
+ * back, all on `stream`, and returns after the stream has finished. */
+int pycfd_step_host(pycfd_solver* s, const double* u0_host, const double* v0_host,
+                    double* u_host, double* v_host, double* p_host, double dt, double blend,
+                    void* stream);
+
+/* Results of the last solve/step (synchronises `stream`). */
+int pycfd_get_stats(pycfd_solver* s, pycfd_stats* out, void* stream);
+
+/* Field reductions (synchronises `stream`).  u_prev/v_prev may be NULL. */
+int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const double* p,
+                      const double* u_prev, const double* v_prev, pycfd_field_stats* out,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

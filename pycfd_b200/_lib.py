@@ -1,0 +1,143 @@
+"""ctypes binding of ``libpycfd_b200.so`` (the C ABI in ``include/pycfd_b200.h``).
+
+The library is built in-tree by :mod:`pycfd_b200.build`.  Loading fails loudly
+when it is missing: the package has no CPU fallback for the hot path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpycfd_b200.so")
+
+PCFD_E_ARG, PCFD_E_CUDA, PCFD_E_NOCONV, PCFD_E_STALL, PCFD_E_UNSUPPORTED = -1, -2, -3, -4, -5
+
+BC_CODES = {"no_slip": 0, "moving_wall": 1, "inlet": 2, "outlet": 3, "pressure_outlet": 4,
+            "periodic": 5, "symmetry": 6}
+SOLVER_CODES = {"cg": 1, "jacobi": 2, "sor": 3, "multigrid": 4, "mgcg": 5}
+SCHEME_CODES = {"euler": 0, "rk2": 1, "rk3": 2}
+MAX_BODIES = 8
+
+# Every exported symbol of the C ABI (checked against the header by the tests).
+EXPORTS = (
+    "pycfd_last_error", "pycfd_version", "pycfd_solver_create", "pycfd_solver_destroy",
+    "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
+    "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
+    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
+)
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class MgLevel(C.Structure):
+    _fields_ = [("n", C.c_int), ("shape_x", C.c_int), ("shape_y", C.c_int),
+                ("weight", C.c_double), ("weighted_dinv", _dp), ("active", _u8p),
+                ("a_indptr", C.POINTER(C.c_int64)), ("a_indices", C.POINTER(C.c_int32)),
+                ("a_data", _dp), ("p_indptr", C.POINTER(C.c_int64)),
+                ("p_indices", C.POINTER(C.c_int32)), ("p_data", _dp)]
+
+
+class SolverDesc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("nu", C.c_double), ("body_fx", C.c_double), ("body_fy", C.c_double),
+                ("bc_kind", C.c_int * 4), ("bc_velocity", C.c_double * 4),
+                ("bc_p_ref", C.c_double * 4), ("bc_profile", _dp * 4), ("solid", _u8p),
+                ("body_id", _u8p), ("n_bodies", C.c_int), ("solver_kind", C.c_int),
+                ("tol", C.c_double), ("maxiter", C.c_int), ("sor_omega", C.c_double),
+                ("mg_sweeps", C.c_int), ("time_scheme", C.c_int), ("precision", C.c_int),
+                ("inner_tol", C.c_double), ("n_levels", C.c_int),
+                ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("status", C.c_int),
+                ("total_iterations", C.c_int), ("last_residual", C.c_double),
+                ("fx", C.c_double), ("fy", C.c_double),
+                ("body_fx", C.c_double * MAX_BODIES), ("body_fy", C.c_double * MAX_BODIES),
+                ("ir_iterations", C.c_int), ("pad_", C.c_int)]
+
+
+class FieldStats(C.Structure):
+    _fields_ = [("max_u", C.c_double), ("max_v", C.c_double), ("max_du", C.c_double),
+                ("max_dv", C.c_double), ("max_div", C.c_double),
+                ("kinetic_energy", C.c_double), ("max_vorticity", C.c_double),
+                ("finite", C.c_int), ("pad_", C.c_int)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the library (once) and declare the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"pycfd_b200 native library not found at {path}; build it with "
+            "`python -m pycfd_b200.build` (there is no CPU fallback)")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    sig = {
+        "pycfd_last_error": (C.c_char_p, []),
+        "pycfd_version": (C.c_int, []),
+        "pycfd_solver_create": (C.c_int, [C.POINTER(SolverDesc), C.POINTER(vp)]),
+        "pycfd_solver_destroy": (C.c_int, [vp]),
+        "pycfd_momentum_rhs": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         C.c_double, C.c_double, C.c_double, C.c_double,
+                                         vp, vp, vp]),
+        "pycfd_divergence": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp, vp]),
+        "pycfd_apply_velocity_bc": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp]),
+        "pycfd_poisson_solve": (C.c_int, [vp, vp, vp, vp, vp]),
+        "pycfd_mg_apply": (C.c_int, [vp, vp, vp, vp]),
+        "pycfd_project": (C.c_int, [vp, vp, vp, vp, C.c_double, vp]),
+        "pycfd_initialize": (C.c_int, [vp, vp, vp, vp, vp]),
+        "pycfd_substep": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+        "pycfd_step": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+        "pycfd_step_host": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+        "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
+        "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class NativeError(RuntimeError):
+    """A CUDA runtime failure inside the native library."""
+
+
+def check(rc: int) -> None:
+    """Map a status code onto the reference's exception types."""
+    if rc == 0:
+        return
+    msg = _lib.pycfd_last_error().decode() if _lib is not None else ""
+    if rc == PCFD_E_ARG:
+        raise ValueError(msg)
+    if rc == PCFD_E_UNSUPPORTED:
+        raise NotImplementedError(msg)
+    if rc in (PCFD_E_NOCONV, PCFD_E_STALL):
+        raise RuntimeError(msg)
+    raise NativeError(msg or f"native call failed with status {rc}")
+
+
+def ptr(t) -> C.c_void_p:
+    """Device (or host) address of a torch tensor / numpy array / None."""
+    if t is None:
+        return C.c_void_p(0)
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return C.c_void_p(t.ctypes.data)
+
+
+def cast(a, ctype):
+    """numpy array -> typed ctypes pointer (None -> NULL)."""
+    if a is None:
+        return C.cast(C.c_void_p(0), C.POINTER(ctype))
+    return a.ctypes.data_as(C.POINTER(ctype))

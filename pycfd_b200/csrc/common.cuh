@@ -1,0 +1,185 @@
+// Shared device helpers: geometry, scalar slots and deterministic grid reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pcfd {
+
+#define PCFD_MAX_BODIES_DEV 8
+
+// Wall order of every boundary pass (pycfd/core/boundary.py:375-379).
+enum { W_LEFT = 0, W_RIGHT = 1, W_BOTTOM = 2, W_TOP = 3 };
+enum { BC_NO_SLIP = 0, BC_MOVING_WALL = 1, BC_INLET = 2, BC_OUTLET = 3,
+       BC_PRESSURE_OUTLET = 4, BC_PERIODIC = 5, BC_SYMMETRY = 6 };
+
+// Cell flags of the fine Poisson operator: which of the four faces carry a
+// 1/h^2 coupling (both cells fluid and joined inside the domain or across a
+// periodic wrap) and whether the row is a solvable unknown
+// (pycfd/core/pressure.py:209-247).
+enum : uint8_t { F_W = 1, F_E = 2, F_S = 4, F_N = 8, F_SOLV = 16 };
+
+// Device scalar slots (doubles) shared by the kernels of one solver.
+enum Slot {
+  S_DT = 0, S_BLEND,
+  S_BNORM2, S_ATOL, S_RNORM2, S_RHO, S_RHO_PREV, S_ALPHA, S_BETA, S_PQ,
+  S_MEAN_B, S_MEAN_R, S_MEAN_X, S_RESID, S_RES_PREV, S_SUM_R, S_TOL,
+  S_BNORM2_0, S_IR_RNORM2, S_MEAN_Z, S_IR_BNORM,
+  S_FX, S_FY,
+  S_BODY_FX,                      // PCFD_MAX_BODIES slots
+  S_BODY_FY = S_BODY_FX + 8,
+  S_MASS_IN = S_BODY_FY + 8, S_MASS_OUT,
+  S_STAT0,                        // field stats block (8 slots)
+  S_COUNT = S_STAT0 + 8 + 8
+};
+
+// Device int slots.
+enum ISlot {
+  I_IT = 0, I_DONE, I_CONVERGED, I_STATUS, I_STALLED, I_TOTAL_IT, I_ZERO_RHS, I_MAXITER,
+  I_IR_IT, I_IR_DONE, I_FINITE,
+  I_COUNT = 16
+};
+
+struct Geo {
+  int nx, ny;
+  double dx, dy, nu, fx, fy;
+  int u_lo, u_hi, v_lo, v_hi;   // solvable face ranges (pycfd/core/solver.py:235-263)
+  int periodic_x, periodic_y;
+  int dir_w, dir_e, dir_s, dir_n;  // Dirichlet (pressure outlet) walls
+  double pref_w, pref_e, pref_s, pref_n;
+  double cx, cy;                // 1/dx^2, 1/dy^2
+  int n_fluid;                  // number of solvable cells
+};
+
+// Reduction workspace: one row of NV partials per block plus a ticket counter.
+struct RedBuf {
+  double* partials;
+  unsigned int* counter;
+};
+
+constexpr int kMaxRedBlocks = 1184;   // 148 SMs x 8 resident blocks
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide reduction of NV values (sum, or max where bit k of MAXMASK is set).
+// Result valid in thread 0.  Fixed tree: deterministic for a fixed block size.
+template <int NV, unsigned MAXMASK = 0u>
+__device__ __forceinline__ void block_reduce(double (&v)[NV]) {
+  __shared__ double sm[NV][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    v[k] = ((MAXMASK >> k) & 1u) ? warp_max(v[k]) : warp_sum(v[k]);
+    if (lane == 0) sm[k][wid] = v[k];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = (lane < nw) ? sm[k][lane] : (((MAXMASK >> k) & 1u) ? -INFINITY : 0.0);
+      v[k] = ((MAXMASK >> k) & 1u) ? warp_max(t) : warp_sum(t);
+    }
+  }
+  __syncthreads();
+}
+
+// Grid-wide reduction.  Every block contributes NV values; the last block to
+// arrive (ticket counter) combines the partials in block order and calls
+// fin(totals) on its thread 0.  Returns true in that thread.
+template <int NV, unsigned MAXMASK = 0u, class Fin>
+__device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin) {
+  block_reduce<NV, MAXMASK>(v);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) rb.partials[blockIdx.x * NV + k] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(rb.counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double acc[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double p = ((volatile double*)rb.partials)[b * NV + k];
+      acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], p) : acc[k] + p;
+    }
+  }
+  block_reduce<NV, MAXMASK>(acc);
+  if (threadIdx.x == 0) {
+    fin(acc);
+    *rb.counter = 0u;
+  }
+}
+
+// Fine-level diagonal, accumulated face by face in the reference's order
+// (left, [left Dirichlet], right, [right Dirichlet], bottom, ..., top), so it is
+// bit-identical to the assembled matrix (pycfd/core/pressure.py:229-247).
+__device__ __forceinline__ double fine_diag(uint8_t f, int i, int j, const Geo& g) {
+  if (!(f & F_SOLV)) return 1.0;
+  double d = 0.0;
+  if (f & F_W) d -= g.cx;
+  if (g.dir_w && i == 0) d -= 2.0 * g.cx;
+  if (f & F_E) d -= g.cx;
+  if (g.dir_e && i == g.nx - 1) d -= 2.0 * g.cx;
+  if (f & F_S) d -= g.cy;
+  if (g.dir_s && j == 0) d -= 2.0 * g.cy;
+  if (f & F_N) d -= g.cy;
+  if (g.dir_n && j == g.ny - 1) d -= 2.0 * g.cy;
+  return d;
+}
+
+// Dirichlet right-hand-side contribution -2 c p_ref per Dirichlet wall the
+// cell touches, in wall order (pycfd/core/pressure.py:240-247).
+__device__ __forceinline__ double fine_bc(uint8_t f, int i, int j, const Geo& g) {
+  if (!(f & F_SOLV)) return 0.0;
+  double b = 0.0;
+  if (g.dir_w && i == 0) b -= 2.0 * g.cx * g.pref_w;
+  if (g.dir_e && i == g.nx - 1) b -= 2.0 * g.cx * g.pref_e;
+  if (g.dir_s && j == 0) b -= 2.0 * g.cy * g.pref_s;
+  if (g.dir_n && j == g.ny - 1) b -= 2.0 * g.cy * g.pref_n;
+  return b;
+}
+
+// Neighbour indices across the four faces (periodic wrap applied; only read
+// where the face flag is set).
+__device__ __forceinline__ int nb_w(int i, int j, const Geo& g) { return (i > 0 ? i - 1 : g.nx - 1) * g.ny + j; }
+__device__ __forceinline__ int nb_e(int i, int j, const Geo& g) { return (i < g.nx - 1 ? i + 1 : 0) * g.ny + j; }
+__device__ __forceinline__ int nb_s(int i, int j, const Geo& g) { return i * g.ny + (j > 0 ? j - 1 : g.ny - 1); }
+__device__ __forceinline__ int nb_n(int i, int j, const Geo& g) { return i * g.ny + (j < g.ny - 1 ? j + 1 : 0); }
+
+// (A x)_c for the fine operator with x supplied by a functor (so neighbour
+// values can be formed on the fly).
+template <class T, class X>
+__device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Geo& g, X x) {
+  T acc = (T)fine_diag(f, i, j, g) * x(c);
+  if (f & F_W) acc += (T)g.cx * x(nb_w(i, j, g));
+  if (f & F_E) acc += (T)g.cx * x(nb_e(i, j, g));
+  if (f & F_S) acc += (T)g.cy * x(nb_s(i, j, g));
+  if (f & F_N) acc += (T)g.cy * x(nb_n(i, j, g));
+  return acc;
+}
+
+inline int grid_for(long n, int threads, int max_blocks = kMaxRedBlocks) {
+  long b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (int)b;
+}
+
+}  // namespace pcfd

@@ -1,0 +1,246 @@
+// V-cycle kernels of the smoothed-aggregation multigrid
+// (pycfd/core/multigrid.py:424-474, :524-543).
+//
+// Level 0 is applied matrix-free from the cell flags.  Coarse operators, the
+// prolongators P_l and the restrictions R_l = P_l^T are ELLPACK blocks; a row
+// is handled by L lanes (L = 1 for the narrow fine-side stencils, up to 32 for
+// the wide Galerkin stencils of the coarse levels, whose rows reach 500
+// entries).  With L = 1 the entries are column-major so neighbouring rows
+// coalesce; with L > 1 a row's entries are contiguous so its lanes coalesce.
+// Damped-Jacobi smoothing is x += wdinv*(b - A x); from a zero start the first
+// sweep is the pointwise x = wdinv*b, fused with the residual that follows.
+#pragma once
+#include "common.cuh"
+
+namespace pcfd {
+
+template <class T>
+struct Ell {
+  const int* col;
+  const T* val;
+  int n;          // rows
+  int K;          // stored entries per row
+  int rowmajor;   // 1: [row*K + k], 0: [k*n + row]
+};
+
+// Row dot product by L lanes.  Every lane of the warp must call this (the
+// lane shuffle uses the full mask); rows past the end contribute nothing.
+template <int L, class T, class X>
+__device__ __forceinline__ double ell_row(const Ell<T>& E, int row, int lane, X x) {
+  double acc = 0.0;
+  if (row >= E.n) {
+  } else if (E.rowmajor) {
+    const long base = (long)row * E.K;
+    for (int k = lane; k < E.K; k += L) {
+      const T a = E.val[base + k];
+      acc += (double)a * x(E.col[base + k]);
+    }
+  } else {
+    for (int k = lane; k < E.K; k += L) {
+      const long e = (long)k * E.n + row;
+      acc += (double)E.val[e] * x(E.col[e]);
+    }
+  }
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
+  return acc;
+}
+
+// x = wd*b; res = b - A(wd*b)          (first sweep from zero + residual)
+template <int L, class T>
+__global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
+                          T* __restrict__ x, T* __restrict__ res) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(t / L), lane = (int)(t % L);
+  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
+  if (lane == 0 && row < A.n) {
+    const double bx = (double)b[row];
+    x[row] = (T)((double)wd[row] * bx);
+    res[row] = (T)(bx - s);
+  }
+}
+
+// xo = x + wd*(b - A x)
+template <int L, class T>
+__global__ void k_ell_smooth(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
+                             const T* __restrict__ x, T* __restrict__ xo) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(t / L), lane = (int)(t % L);
+  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
+  if (lane == 0 && row < A.n) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+}
+
+// res = b - A x
+template <int L, class T>
+__global__ void k_ell_resid(Ell<T> A, const T* __restrict__ b, const T* __restrict__ x,
+                            T* __restrict__ res) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(t / L), lane = (int)(t % L);
+  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
+  if (lane == 0 && row < A.n) res[row] = (T)((double)b[row] - s);
+}
+
+// y = M x (restriction with M = R), or y += M x (prolongation with M = P).
+template <int L, bool ADD, class T>
+__global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(t / L), lane = (int)(t % L);
+  const double s = ell_row<L>(M, row, lane, [&](int c) { return (double)x[c]; });
+  if (lane == 0 && row < M.n) y[row] = ADD ? (T)((double)y[row] + s) : (T)s;
+}
+
+// Coarsest level: x = C b with C the precomputed pseudo-inverse (pinned LU
+// followed by mean removal, pycfd/core/multigrid.py:524-543), column-major.
+template <class T>
+__global__ void k_dense(const T* __restrict__ C, int n, const T* __restrict__ b, T* __restrict__ x) {
+  for (int row = threadIdx.x; row < n; row += blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < n; ++k) acc += (double)C[(long)k * n + row] * (double)b[k];
+    x[row] = (T)acc;
+  }
+}
+
+// ---- level 0 (matrix-free) --------------------------------------------------
+// Right-hand side of the fine level: the CG residual projected onto the
+// active set (multigrid.py:453-458), or a stored vector.
+template <class T>
+struct BFromR {
+  const T* r;
+  const uint8_t* f;
+  double mean;
+  __device__ __forceinline__ double operator()(long k) const {
+    return (f[k] & F_SOLV) ? (double)r[k] - mean : 0.0;
+  }
+};
+template <class T>
+struct BStored {
+  const T* b;
+  __device__ __forceinline__ double operator()(long k) const { return (double)b[k]; }
+};
+
+__device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo& g, double w) {
+  return w * (1.0 / fine_diag(f, i, j, g));
+}
+
+// x = wd*b and res = b - A(wd*b) on level 0.
+template <class T, class B>
+__global__ void k_fine_pre(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
+                           T* __restrict__ x, T* __restrict__ res) {
+  const long n = (long)g.nx * g.ny;
+  auto xv = [&](long k) -> double {
+    const int ii = (int)(k / g.ny), jj = (int)(k % g.ny);
+    return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
+  };
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    const double xc = xv(c);
+    x[c] = (T)xc;
+    res[c] = (T)(bf(c) - fine_apply<double>(f, i, j, (int)c, g, xv));
+  }
+}
+
+// xo = x + wd*(b - A x) on level 0.  MODE 0: plain; MODE 1: last sweep of the
+// preconditioner, with sum_solvable(xo) and r.xo for the projected z and
+// rho = r.z (r = CG residual, rsum = its solvable sum); MODE 2: last sweep of
+// a standalone cycle, with sum_solvable(xo) for the projection.
+template <class T, class B, int MODE>
+__global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
+                              const T* __restrict__ x, T* __restrict__ xo,
+                              const T* __restrict__ rcg, int singular, double* __restrict__ S,
+                              RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  auto xv = [&](long k) -> double { return (double)x[k]; };
+  double acc[2] = {0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
+                                  (bf(c) - fine_apply<double>(f, i, j, (int)c, g, xv)));
+    xo[c] = (T)xn;
+    if (MODE != 0 && (f & F_SOLV)) {
+      acc[0] += xn;
+      if (MODE == 1) acc[1] += (double)rcg[c] * xn;
+    }
+  }
+  if (MODE == 0) return;
+  grid_reduce<2>(acc, rb, [&](double* t) {
+    const double m = (singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
+    if (MODE == 1) {
+      S[S_MEAN_Z] = m;
+      S[S_RHO_PREV] = S[S_RHO];
+      S[S_RHO] = t[1] - m * S[S_SUM_R];
+    } else {
+      S[S_MEAN_X] = m;
+    }
+  });
+}
+
+// res = b - A x on level 0.
+template <class T, class B>
+__global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
+                             const T* __restrict__ x, T* __restrict__ res) {
+  const long n = (long)g.nx * g.ny;
+  auto xv = [&](long k) -> double { return (double)x[k]; };
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    res[c] = (T)(bf(c) - fine_apply<double>(flags[c], i, j, (int)c, g, xv));
+  }
+}
+
+// x = wd*b on level 0 (first sweep from zero when more sweeps follow).
+template <class T, class B>
+__global__ void k_fine_wdb(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
+                           T* __restrict__ x) {
+  const long n = (long)g.nx * g.ny;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    x[c] = (T)(fine_wdinv(flags[c], i, j, g, w) * bf(c));
+  }
+}
+
+// Materialise a fine right-hand side (single-level hierarchies only).
+template <class T, class B>
+__global__ void k_fine_store(B bf, long n, T* __restrict__ out) {
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+    out[c] = (T)bf(c);
+}
+
+// Fine-level sums after a single-level "cycle" (dense solve): same finisher as
+// k_fine_smooth MODE 1/2 without the smoothing.
+template <class T, int MODE>
+__global__ void k_fine_sums(const T* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
+                            const T* __restrict__ rcg, int singular, double* __restrict__ S,
+                            RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  double acc[2] = {0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    if (flags[c] & F_SOLV) {
+      acc[0] += (double)x[c];
+      if (MODE == 1) acc[1] += (double)rcg[c] * (double)x[c];
+    }
+  }
+  grid_reduce<2>(acc, rb, [&](double* t) {
+    const double m = (singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
+    if (MODE == 1) {
+      S[S_MEAN_Z] = m;
+      S[S_RHO_PREV] = S[S_RHO];
+      S[S_RHO] = t[1] - m * S[S_SUM_R];
+    } else {
+      S[S_MEAN_X] = m;
+    }
+  });
+}
+
+// Materialise the projected fine right-hand side of the preconditioner from
+// the CG residual r (pycfd/core/multigrid.py:453-458, 468-469).
+template <class T>
+__global__ void k_fine_store_from_r(const T* __restrict__ r, const uint8_t* __restrict__ flags, Geo g,
+                                    const double* __restrict__ S, int singular, T* __restrict__ out) {
+  const long n = (long)g.nx * g.ny;
+  const double m = singular ? S[S_MEAN_R] : 0.0;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+    out[c] = (flags[c] & F_SOLV) ? (T)((double)r[c] - m) : (T)0;
+}
+
+}  // namespace pcfd

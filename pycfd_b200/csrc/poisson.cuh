@@ -1,0 +1,342 @@
+// Fine-level Poisson kernels: right-hand-side conditioning, the conjugate-
+// gradient recurrence (Jacobi- or multigrid-preconditioned), damped Jacobi,
+// red/black SOR, residual norms and result normalisation.
+//
+// The fine operator is applied matrix-free from one flag byte per cell.  CG
+// follows SciPy's recurrence (scipy/sparse/linalg/_isolve/iterative.py:311 in
+// SciPy 1.18.1, as called by pycfd/core/pressure.py:388-391 and :619-623):
+// each pass tests the recurrence residual first, then z = M r, rho = r.z,
+// p = z + (rho/rho_prev) p, q = A p, alpha = rho/(p.q), x += alpha p,
+// r -= alpha q.  Two kernels per pass: p/q/(p.q) and x/r/(r.r, r.z).
+// Vector kernels are templated on the storage type T (double, or float for the
+// inner solve of the mixed form); scalars and dot products are always double.
+#pragma once
+#include "common.cuh"
+
+namespace pcfd {
+
+enum Precond { PC_JACOBI = 0, PC_MG = 1 };
+
+// Solve-level constants the finishers need.
+struct SolveCfg {
+  double tol;
+  int maxiter;
+  int singular;
+  int check_every;   // stationary solvers: residual cadence
+};
+
+template <class T> struct VecRef { T* p; };
+
+// ---- right-hand side and initial residual --------------------------------
+// b <- b_raw - mean (solvable rows, singular systems), r = b - A x0 (x0 = 0
+// when has_x0 == 0), with ||b||^2, ||r||^2, r.(r/d) and sum_solvable(r).
+// (pycfd/core/pressure.py:300-308; scipy cg: r = b - A x0)
+template <class T>
+__global__ void k_rhs_init(double* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
+                           const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
+                           int has_x0, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
+  double acc[4] = {0, 0, 0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    double bc = b[c];
+    if (f & F_SOLV) bc = bc - mean;
+    else bc = 0.0;
+    b[c] = bc;
+    double ax = 0.0;
+    if (has_x0) ax = fine_apply<double>(f, i, j, (int)c, g, [&](long k) { return (double)x[k]; });
+    else x[c] = (T)0;
+    const double rc = bc - ax;
+    r[c] = (T)rc;
+    const double d = fine_diag(f, i, j, g);
+    acc[0] += bc * bc;
+    acc[1] += rc * rc;
+    acc[2] += rc * (rc / d);
+    if (f & F_SOLV) acc[3] += rc;
+  }
+  grid_reduce<4>(acc, rb, [&](double* t) {
+    S[S_BNORM2] = t[0];
+    S[S_ATOL] = cfg.tol * sqrt(t[0]);
+    S[S_RNORM2] = t[1];
+    S[S_RHO] = t[2];
+    S[S_RHO_PREV] = 1.0;
+    S[S_SUM_R] = t[3];
+    S[S_MEAN_R] = g.n_fluid ? t[3] / g.n_fluid : 0.0;
+    I[I_IT] = 0;
+    I[I_ZERO_RHS] = (t[0] == 0.0);
+    const bool conv = (t[0] == 0.0) || (sqrt(t[1]) < S[S_ATOL]);
+    I[I_CONVERGED] = conv;
+    I[I_DONE] = conv || cfg.maxiter <= 0;
+    I[I_STATUS] = 0;
+  });
+}
+
+// p = z + beta p_old with z = r/d (Jacobi) or z = z_raw - mean_z on solvable
+// rows (multigrid; z_raw from the V-cycle), q = A p, and p.q -> alpha.
+template <class T, int PC>
+__global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
+                        const T* __restrict__ p_old, T* __restrict__ p_new, T* __restrict__ q,
+                        const uint8_t* __restrict__ flags, Geo g, double* __restrict__ S,
+                        const int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const bool first = I[I_IT] == 0;
+  const double beta = first ? 0.0 : S[S_RHO] / S[S_RHO_PREV];
+  const double mz = S[S_MEAN_Z];
+  auto pval = [&](long k) -> double {
+    const int ii = (int)(k / g.ny), jj = (int)(k % g.ny);
+    const uint8_t fk = flags[k];
+    double z;
+    if (PC == PC_JACOBI) z = (double)r[k] / fine_diag(fk, ii, jj, g);
+    else z = (fk & F_SOLV) ? (double)zraw[k] - mz : 0.0;
+    if (first) return (double)(T)z;
+    return (double)(T)((double)p_old[k] * beta + z);
+  };
+  double acc[1] = {0.0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    const double pc = pval(c);
+    const double qc = fine_apply<double>(f, i, j, (int)c, g, pval);
+    p_new[c] = (T)pc;
+    q[c] = (T)qc;
+    acc[0] += pc * qc;
+  }
+  grid_reduce<1>(acc, rb, [&](double* t) {
+    S[S_PQ] = t[0];
+    S[S_ALPHA] = S[S_RHO] / t[0];
+  });
+}
+
+// x += alpha p, r -= alpha q; ||r||^2, r.(r/d), sum_solvable(r); convergence
+// test of the next pass (scipy's top-of-loop ||r|| < atol), iteration count.
+template <class T, int PC>
+__global__ void k_cg_xr(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                        const T* __restrict__ q, const uint8_t* __restrict__ flags, Geo g,
+                        SolveCfg cfg, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double alpha = S[S_ALPHA];
+  double acc[3] = {0, 0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    const double xc = (double)x[c] + alpha * (double)p[c];
+    const double rc = (double)(T)((double)r[c] - alpha * (double)q[c]);
+    x[c] = (T)xc;
+    r[c] = (T)rc;
+    acc[0] += rc * rc;
+    if (PC == PC_JACOBI) acc[1] += rc * (rc / fine_diag(f, i, j, g));
+    if (f & F_SOLV) acc[2] += rc;
+  }
+  grid_reduce<3>(acc, rb, [&](double* t) {
+    const int it = I[I_IT] + 1;
+    I[I_IT] = it;
+    I[I_TOTAL_IT] += 1;
+    S[S_RNORM2] = t[0];
+    if (PC == PC_JACOBI) { S[S_RHO_PREV] = S[S_RHO]; S[S_RHO] = t[1]; }
+    S[S_SUM_R] = t[2];
+    S[S_MEAN_R] = g.n_fluid ? t[2] / g.n_fluid : 0.0;
+    const bool conv = sqrt(t[0]) < S[S_ATOL];
+    I[I_CONVERGED] = conv;
+    I[I_DONE] = conv || it >= cfg.maxiter;
+  });
+}
+
+// ---- result normalisation -------------------------------------------------
+// ||b - A x||^2 and sum_solvable(x) -> last_residual and the mean
+// (pycfd/core/pressure.py:310-322).  keep_resid: the stationary solvers
+// report the residual of their last check instead.
+template <class T>
+__global__ void k_finish_stats(const T* __restrict__ x, const double* __restrict__ b,
+                               const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
+                               int pcg, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const bool zero = I[I_ZERO_RHS] != 0;
+  auto xv = [&](long k) -> double { return zero ? 0.0 : (double)x[k]; };
+  double acc[2] = {0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    if (pcg) {
+      const double rc = b[c] - fine_apply<double>(f, i, j, (int)c, g, xv);
+      acc[0] += rc * rc;
+    }
+    if (f & F_SOLV) acc[1] += xv(c);
+  }
+  grid_reduce<2>(acc, rb, [&](double* t) {
+    const double nb = sqrt(S[S_BNORM2]);
+    if (pcg) {
+      S[S_RESID] = sqrt(t[0]) / (nb > 1e-300 ? nb : 1.0);
+      if (!I[I_CONVERGED] && S[S_RESID] > fmax(cfg.tol * 10.0, 1e-8)) I[I_STATUS] = -3;
+    }
+    S[S_MEAN_X] = (cfg.singular && g.n_fluid) ? t[1] / g.n_fluid : 0.0;
+  });
+}
+
+// x <- x - mean on solvable rows, 0 elsewhere; also the double copy for the
+// projection (xo may alias x when T is double).
+template <class T>
+__global__ void k_finish_apply(T* x, double* xo,
+                               const uint8_t* __restrict__ flags, Geo g,
+                               const double* __restrict__ S, const int* __restrict__ I) {
+  const long n = (long)g.nx * g.ny;
+  const bool zero = I[I_ZERO_RHS] != 0;
+  const double m = S[S_MEAN_X];
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const double v = (!zero && (flags[c] & F_SOLV)) ? (double)x[c] - m : 0.0;
+    x[c] = (T)v;
+    xo[c] = v;
+  }
+}
+
+// ---- stationary solvers -----------------------------------------------------
+// Initial iterate and right-hand side of Jacobi/SOR/standalone multigrid:
+// b final (mean removed), x = x0 with non-solvable rows zeroed (or 0),
+// ||b||^2 and sum_solvable(x) (pycfd/core/pressure.py:420-430, :506-513).
+__global__ void k_stationary_init(double* __restrict__ b, double* __restrict__ x,
+                                  const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
+                                  int has_x0, int project_x0, double* __restrict__ S,
+                                  int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
+  double acc[3] = {0, 0, 0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const uint8_t f = flags[c];
+    const double bc = (f & F_SOLV) ? b[c] - mean : 0.0;
+    b[c] = bc;
+    const double xc = (has_x0 && (f & F_SOLV)) ? x[c] : 0.0;
+    x[c] = xc;
+    acc[0] += bc * bc;
+    if (f & F_SOLV) { acc[1] += bc; acc[2] += xc; }
+  }
+  grid_reduce<3>(acc, rb, [&](double* t) {
+    S[S_BNORM2] = t[0];
+    // standalone multigrid projects b and x0 once more (multigrid.py:490-493)
+    S[S_MEAN_B] = (project_x0 && cfg.singular && g.n_fluid) ? t[1] / g.n_fluid : 0.0;
+    S[S_MEAN_X] = (project_x0 && cfg.singular && g.n_fluid) ? t[2] / g.n_fluid : 0.0;
+    S[S_RES_PREV] = 0.0;
+    I[I_IT] = 0;
+    I[I_DONE] = 0;
+    I[I_CONVERGED] = 0;
+    I[I_STATUS] = 0;
+    I[I_STALLED] = 0;
+    I[I_ZERO_RHS] = 0;
+  });
+}
+
+// One damped-Jacobi sweep p <- p + omega*dinv*(b - A p) on the iterate with its
+// pending mean removed, plus the new fluid sum (pycfd/core/pressure.py:432-436).
+__global__ void k_jacobi_sweep(const double* __restrict__ xin, double* __restrict__ xout,
+                               const double* __restrict__ b, const uint8_t* __restrict__ flags,
+                               Geo g, double omega, int singular, double* __restrict__ S,
+                               int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double m = S[S_MEAN_X];
+  auto xe = [&](long k) -> double { return (flags[k] & F_SOLV) ? xin[k] - m : xin[k]; };
+  double acc[1] = {0.0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    const double d = fine_diag(f, i, j, g);
+    const double dinv = 1.0 / d;
+    const double xn = xe(c) + omega * dinv * (b[c] - fine_apply<double>(f, i, j, (int)c, g, xe));
+    xout[c] = xn;
+    if (f & F_SOLV) acc[0] += xn;
+  }
+  grid_reduce<1>(acc, rb, [&](double* t) {
+    S[S_MEAN_X] = (singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
+    I[I_IT] += 1;
+    I[I_TOTAL_IT] += 1;
+  });
+}
+
+// One red (colour 0) or black (colour 1) SOR half-sweep in place
+// (pycfd/core/pressure.py:514-517).  Values of the colour being updated and, on
+// the red pass, its neighbours still carry the previous sweep's mean; the
+// black pass finishes the new fluid mean.
+__global__ void k_sor_half(double* __restrict__ x, const double* __restrict__ b,
+                           const uint8_t* __restrict__ flags, Geo g, double omega, int colour,
+                           int singular, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double m = S[S_MEAN_X];
+  // red pass: every value is in the old frame; black pass: red neighbours are new.
+  auto xe = [&](long k) -> double {
+    const bool adj = (flags[k] & F_SOLV) && (colour == 0 || ((k / g.ny + k % g.ny) & 1) == 1);
+    return adj ? x[k] - m : x[k];
+  };
+  double acc[1] = {0.0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    if (((i + j) & 1) != colour) continue;
+    const uint8_t f = flags[c];
+    const double d = fine_diag(f, i, j, g);
+    double off = 0.0;
+    if (f & F_W) off += g.cx * xe(nb_w(i, j, g));
+    if (f & F_E) off += g.cx * xe(nb_e(i, j, g));
+    if (f & F_S) off += g.cy * xe(nb_s(i, j, g));
+    if (f & F_N) off += g.cy * xe(nb_n(i, j, g));
+    const double xn = (1.0 - omega) * xe(c) + omega * (b[c] - off) / d;
+    x[c] = xn;
+    if (f & F_SOLV) acc[0] += xn;
+  }
+  grid_reduce<1>(acc, rb, [&](double* t) {
+    if (colour == 0) {
+      S[S_SUM_R] = t[0];
+    } else {
+      S[S_MEAN_X] = (singular && g.n_fluid) ? (S[S_SUM_R] + t[0]) / g.n_fluid : 0.0;
+      I[I_IT] += 1;
+      I[I_TOTAL_IT] += 1;
+    }
+  });
+}
+
+// ||b - A(x - m)|| / ||b|| on the iterate with its pending mean m, then the
+// stopping rule of the calling solver:
+//   mode 0 (Jacobi/SOR): done when res < tol or the sweep budget is spent;
+//   mode 1 (standalone multigrid, pycfd/core/multigrid.py:498-511): also stop
+//   after three cycles that fail to shrink the residual by 0.995.
+// write_back: store the projected iterate x - m (multigrid projects every cycle).
+__global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
+                          const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg, int mode,
+                          int count_cycle, int pending, double* __restrict__ S, int* __restrict__ I,
+                          RedBuf rb) {
+  const long n = (long)g.nx * g.ny;
+  const double m = pending ? S[S_MEAN_X] : 0.0;
+  auto xe = [&](long k) -> double { return (flags[k] & F_SOLV) ? x[k] - m : 0.0; };
+  double acc[1] = {0.0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const double rc = b[c] - fine_apply<double>(flags[c], i, j, (int)c, g, xe);
+    acc[0] += rc * rc;
+  }
+  grid_reduce<1>(acc, rb, [&](double* t) {
+    const double nb = sqrt(S[S_BNORM2]);
+    const double res = sqrt(t[0]) / (nb > 1e-300 ? nb : 1.0);
+    const int it = I[I_IT] + (count_cycle ? 1 : 0);
+    if (count_cycle) { I[I_IT] = it; I[I_TOTAL_IT] += 1; }
+    const double prev = S[S_RES_PREV];
+    S[S_RESID] = res;
+    const bool conv = res < cfg.tol;
+    I[I_CONVERGED] = conv;
+    if (mode == 1) {
+      if (count_cycle) I[I_STALLED] = (res > 0.995 * prev) ? I[I_STALLED] + 1 : 0;
+      S[S_RES_PREV] = res;
+      I[I_DONE] = !(it < cfg.maxiter && res >= cfg.tol && I[I_STALLED] < 3);
+    } else {
+      I[I_DONE] = conv || it >= cfg.maxiter;
+    }
+    if (I[I_DONE] && res > cfg.tol) I[I_STATUS] = -4;
+  });
+}
+
+// Apply a pending mean: x <- x - S[slot] on solvable rows.
+__global__ void k_apply_mean(double* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
+                             const double* __restrict__ S, int slot) {
+  const long n = (long)g.nx * g.ny;
+  const double m = S[slot];
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+    if (flags[c] & F_SOLV) x[c] = x[c] - m;
+}
+
+}  // namespace pcfd

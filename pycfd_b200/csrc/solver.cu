@@ -1,0 +1,1053 @@
+// Host runtime of the projection hot path: solver construction (flags, face
+// lists, multigrid upload), launch orchestration of the substep / projection /
+// Poisson solves, and the C ABI declared in include/pycfd_b200.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pycfd_b200.h"
+#include "boundary.cuh"
+#include "common.cuh"
+#include "multigrid.cuh"
+#include "poisson.cuh"
+#include "stencil.cuh"
+
+using namespace pcfd;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CU(x)                                                                        \
+  do {                                                                               \
+    cudaError_t e_ = (x);                                                            \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(PCFD_E_CUDA, "%s failed: %s (%s:%d)", #x, cudaGetErrorString(e_),  \
+                  __FILE__, __LINE__);                                               \
+  } while (0)
+
+#define CHECK_LAUNCH() CU(cudaGetLastError())
+#define TRY(x)             \
+  do {                     \
+    int rc_ = (x);         \
+    if (rc_ != 0) return rc_; \
+  } while (0)
+
+namespace {
+
+template <class T>
+struct DevEll {
+  int* col = nullptr;
+  T* val = nullptr;
+  int n = 0, K = 0, rowmajor = 0, lanes = 1;
+  Ell<T> view() const { return Ell<T>{col, val, n, K, rowmajor}; }
+};
+
+template <class T>
+struct LevelBuf {
+  T *b = nullptr, *xa = nullptr, *xb = nullptr, *res = nullptr;
+};
+
+struct Level {
+  int n = 0, sx = 0, sy = 0;
+  double weight = 1.0;
+  DevEll<double> A, P, R;   // P: rows of the finer level; R = P^T: rows of this level
+  DevEll<float> Af, Pf, Rf;
+  double* wd = nullptr;
+  float* wdf = nullptr;
+  LevelBuf<double> d;
+  LevelBuf<float> f;
+};
+
+int choose_lanes(int K) {
+  if (K <= 8) return 1;
+  if (K <= 32) return 4;
+  if (K <= 96) return 8;
+  if (K <= 200) return 16;
+  return 32;
+}
+
+}  // namespace
+
+struct pycfd_solver {
+  Geo g{};
+  BcTable bc{};
+  int solver_kind = 0, maxiter = 0, mg_sweeps = 1, scheme = 2, precision = 0;
+  double tol = 1e-10, omega = 1.8, inner_tol = 1e-4;
+  int singular = 1;
+  std::vector<void*> allocs;
+
+  uint8_t* flags = nullptr;
+  uint8_t* solid = nullptr;
+  int* mask_u = nullptr;
+  int* mask_v = nullptr;
+  int* bc_kind_dev = nullptr;
+  double* profile[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  double* S = nullptr;
+  int* I = nullptr;
+  double* partials = nullptr;
+  unsigned int* counter = nullptr;
+  double* hS = nullptr;   // pinned mirrors
+  int* hI = nullptr;
+
+  // state work buffers
+  double *us1 = nullptr, *vs1 = nullptr, *us2 = nullptr, *vs2 = nullptr;
+  double *hu0 = nullptr, *hv0 = nullptr, *hu = nullptr, *hv = nullptr, *hp = nullptr;
+  // Poisson
+  double *b = nullptr, *x = nullptr, *x_api = nullptr, *r = nullptr, *pa = nullptr,
+         *pb = nullptr, *q = nullptr, *z = nullptr, *xtmp = nullptr;
+  bool has_guess = false;
+  // mixed-form inner vectors
+  float *r32 = nullptr, *x32 = nullptr, *pa32 = nullptr, *pb32 = nullptr, *q32 = nullptr,
+        *z32 = nullptr;
+  std::vector<Level> lv;
+  double* C = nullptr;
+  float* Cf = nullptr;
+  int nc = 0;
+  int last_ir = 0;
+
+  RedBuf rb() const { return RedBuf{partials, counter}; }
+  SolveCfg cfg() const { return SolveCfg{tol, maxiter, singular, 0}; }
+  long ncell() const { return (long)g.nx * g.ny; }
+};
+
+namespace {
+
+template <class T>
+int dalloc(pycfd_solver* s, T** p, size_t count) {
+  void* ptr = nullptr;
+  CU(cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T)));
+  CU(cudaMemset(ptr, 0, std::max<size_t>(count, 1) * sizeof(T)));
+  s->allocs.push_back(ptr);
+  *p = (T*)ptr;
+  return 0;
+}
+
+template <class T>
+int upload(pycfd_solver* s, T** p, const T* host, size_t count) {
+  TRY(dalloc(s, p, count));
+  if (count) CU(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// CSR -> ELL (entries of a row sorted by column) in the layout its lane count wants.
+template <class T>
+int make_ell(pycfd_solver* s, DevEll<T>* E, int n, const int64_t* indptr, const int32_t* idx,
+             const double* data) {
+  int K = 0;
+  for (int r = 0; r < n; ++r) K = std::max<int>(K, (int)(indptr[r + 1] - indptr[r]));
+  K = std::max(K, 1);
+  const int L = choose_lanes(K);
+  const int rowmajor = L > 1;
+  const int Kp = rowmajor ? ((K + L - 1) / L) * L : K;
+  std::vector<int> col((size_t)n * Kp);
+  std::vector<T> val((size_t)n * Kp, (T)0);
+  std::vector<std::pair<int, double>> row;
+  for (int r = 0; r < n; ++r) {
+    row.clear();
+    for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) row.push_back({idx[e], data[e]});
+    std::sort(row.begin(), row.end(),
+              [](const std::pair<int, double>& a, const std::pair<int, double>& b) { return a.first < b.first; });
+    const int pad_col = row.empty() ? 0 : row[0].first;
+    for (int k = 0; k < Kp; ++k) {
+      const size_t at = rowmajor ? (size_t)r * Kp + k : (size_t)k * n + r;
+      if (k < (int)row.size()) {
+        col[at] = row[k].first;
+        val[at] = (T)row[k].second;
+      } else {
+        col[at] = pad_col;
+        val[at] = (T)0;
+      }
+    }
+  }
+  TRY(upload(s, &E->col, col.data(), col.size()));
+  TRY(upload(s, &E->val, val.data(), val.size()));
+  E->n = n;
+  E->K = Kp;
+  E->rowmajor = rowmajor;
+  E->lanes = L;
+  return 0;
+}
+
+// CSR transpose (rows = columns of the input).
+void csr_transpose(int nrows, int ncols, const int64_t* indptr, const int32_t* idx,
+                   const double* data, std::vector<int64_t>& tp, std::vector<int32_t>& ti,
+                   std::vector<double>& td) {
+  tp.assign(ncols + 1, 0);
+  const int64_t nnz = indptr[nrows];
+  for (int64_t e = 0; e < nnz; ++e) tp[idx[e] + 1]++;
+  for (int c = 0; c < ncols; ++c) tp[c + 1] += tp[c];
+  ti.resize(nnz);
+  td.resize(nnz);
+  std::vector<int64_t> pos(tp.begin(), tp.end() - 1);
+  for (int r = 0; r < nrows; ++r)
+    for (int64_t e = indptr[r]; e < indptr[r + 1]; ++e) {
+      const int64_t at = pos[idx[e]]++;
+      ti[at] = r;
+      td[at] = data[e];
+    }
+}
+
+cudaStream_t st(void* stream) { return (cudaStream_t)stream; }
+
+// ---- launch helpers ---------------------------------------------------------
+int launch_boundary(pycfd_solver* s, double* u, double* v, std::initializer_list<int> ops,
+                    cudaStream_t stream) {
+  BcProgram prog{};
+  int k = 0;
+  for (int op : ops) prog.op[k++] = op;
+  prog.op[k] = OP_END;
+  k_boundary<<<1, 1024, 0, stream>>>(u, v, s->g, s->bc, prog, s->S);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int grid1(pycfd_solver* s) { return grid_for(s->ncell(), kRedThreads, kMaxRedBlocks); }
+
+// Generic dispatcher over the lane count of an ELL block.
+#define ELL_DISPATCH(LANES, CALL)                 \
+  switch (LANES) {                                \
+    case 1: { constexpr int L = 1; CALL; } break;  \
+    case 4: { constexpr int L = 4; CALL; } break;  \
+    case 8: { constexpr int L = 8; CALL; } break;  \
+    case 16: { constexpr int L = 16; CALL; } break; \
+    default: { constexpr int L = 32; CALL; } break; \
+  }
+
+inline int ell_grid(int n, int L) { return (int)(((long)n * L + 255) / 256); }
+
+template <class T>
+const DevEll<T>& lvA(const Level& l);
+template <>
+const DevEll<double>& lvA<double>(const Level& l) { return l.A; }
+template <>
+const DevEll<float>& lvA<float>(const Level& l) { return l.Af; }
+template <class T>
+const DevEll<T>& lvP(const Level& l);
+template <>
+const DevEll<double>& lvP<double>(const Level& l) { return l.P; }
+template <>
+const DevEll<float>& lvP<float>(const Level& l) { return l.Pf; }
+template <class T>
+const DevEll<T>& lvR(const Level& l);
+template <>
+const DevEll<double>& lvR<double>(const Level& l) { return l.R; }
+template <>
+const DevEll<float>& lvR<float>(const Level& l) { return l.Rf; }
+template <class T>
+LevelBuf<T>& lvB(Level& l);
+template <>
+LevelBuf<double>& lvB<double>(Level& l) { return l.d; }
+template <>
+LevelBuf<float>& lvB<float>(Level& l) { return l.f; }
+template <class T>
+T* lvWd(Level& l);
+template <>
+double* lvWd<double>(Level& l) { return l.wd; }
+template <>
+float* lvWd<float>(Level& l) { return l.wdf; }
+template <class T>
+const T* coarseC(pycfd_solver* s);
+template <>
+const double* coarseC<double>(pycfd_solver* s) { return s->C; }
+template <>
+const float* coarseC<float>(pycfd_solver* s) { return s->Cf; }
+
+// One V-cycle from zero applied to the CG residual r: z_out gets the
+// unprojected result; the last fine sweep's finisher leaves mean(z) and r.z
+// in the scalar slots (pycfd/core/multigrid.py:430-474).
+template <class T>
+int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
+  const int Lv = (int)s->lv.size();
+  const Geo& g = s->g;
+  const int sw = s->mg_sweeps;
+  const int G = grid1(s);
+  // Materialise the projected fine right-hand side b0 = r - mean(r) (solvable
+  // rows; the mean was left in S_MEAN_R by the kernel that produced r) into
+  // level 0's b buffer; the fine kernels read it as a stored vector.
+  LevelBuf<T>& B0 = lvB<T>(s->lv[0]);
+  k_fine_store_from_r<T><<<G, kRedThreads, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
+  CHECK_LAUNCH();
+  BStored<T> bf0{B0.b};
+  if (Lv == 1) {
+    k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, B0.b, z_out);
+    CHECK_LAUNCH();
+    k_fine_sums<T, 1><<<G, kRedThreads, 0, stream>>>(z_out, s->flags, g, r, s->singular, s->S, s->rb());
+    CHECK_LAUNCH();
+    return 0;
+  }
+  const double w0 = s->lv[0].weight;
+  // ---- down ----
+  T* cur[32];
+  if (sw == 1) {
+    k_fine_pre<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
+    CHECK_LAUNCH();
+    cur[0] = B0.xa;
+  } else {
+    k_fine_wdb<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
+    CHECK_LAUNCH();
+    T* a = B0.xa;
+    T* bb = B0.xb;
+    for (int k = 1; k < sw; ++k) {
+      k_fine_smooth<T, BStored<T>, 0><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
+                                                                     s->singular, s->S, s->rb());
+      CHECK_LAUNCH();
+      std::swap(a, bb);
+    }
+    k_fine_resid<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, a, B0.res);
+    CHECK_LAUNCH();
+    cur[0] = a;
+  }
+  for (int l = 1; l < Lv; ++l) {
+    Level& Lc = s->lv[l];
+    LevelBuf<T>& Bc = lvB<T>(Lc);
+    const T* res_f = lvB<T>(s->lv[l - 1]).res;
+    const DevEll<T>& R = lvR<T>(Lc);
+    ELL_DISPATCH(R.lanes, (k_ell_spmv<L, false, T><<<ell_grid(R.n, L), 256, 0, stream>>>(R.view(), res_f, Bc.b)));
+    CHECK_LAUNCH();
+    if (l == Lv - 1) {
+      k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, Bc.b, Bc.xa);
+      CHECK_LAUNCH();
+      cur[l] = Bc.xa;
+      break;
+    }
+    const DevEll<T>& A = lvA<T>(Lc);
+    T* wd = lvWd<T>(Lc);
+    ELL_DISPATCH(A.lanes, (k_ell_pre<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bc.b, Bc.xa, Bc.res)));
+    CHECK_LAUNCH();
+    T* a = Bc.xa;
+    T* bb = Bc.xb;
+    if (sw > 1) {
+      for (int k = 1; k < sw; ++k) {
+        ELL_DISPATCH(A.lanes, (k_ell_smooth<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bc.b, a, bb)));
+        CHECK_LAUNCH();
+        std::swap(a, bb);
+      }
+      ELL_DISPATCH(A.lanes, (k_ell_resid<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), Bc.b, a, Bc.res)));
+      CHECK_LAUNCH();
+    }
+    cur[l] = a;
+  }
+  // ---- up ----
+  for (int l = Lv - 2; l >= 0; --l) {
+    Level& Lf = s->lv[l];
+    LevelBuf<T>& Bf = lvB<T>(Lf);
+    const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
+    T* xf = cur[l];
+    ELL_DISPATCH(P.lanes, (k_ell_spmv<L, true, T><<<ell_grid(P.n, L), 256, 0, stream>>>(P.view(), cur[l + 1], xf)));
+    CHECK_LAUNCH();
+    T* other = (xf == Bf.xa) ? Bf.xb : Bf.xa;
+    for (int k = 1; k <= sw; ++k) {
+      if (l == 0) {
+        T* dst = (k == sw) ? z_out : other;
+        if (k == sw)
+          k_fine_smooth<T, BStored<T>, 1><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+                                                                         s->singular, s->S, s->rb());
+        else
+          k_fine_smooth<T, BStored<T>, 0><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+                                                                         s->singular, s->S, s->rb());
+        CHECK_LAUNCH();
+        other = xf;
+        xf = dst;
+      } else {
+        const DevEll<T>& A = lvA<T>(Lf);
+        T* wd = lvWd<T>(Lf);
+        ELL_DISPATCH(A.lanes, (k_ell_smooth<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bf.b, xf, other)));
+        CHECK_LAUNCH();
+        std::swap(xf, other);
+      }
+    }
+    cur[l] = xf;
+  }
+  return 0;
+}
+
+// One standalone V-cycle from the current fine iterate x with right-hand side
+// b (both double).  Leaves the fine mean of the result in S_MEAN_X.
+int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream) {
+  const int Lv = (int)s->lv.size();
+  const Geo& g = s->g;
+  const int sw = s->mg_sweeps;
+  const int G = grid1(s);
+  BStored<double> bf{b};
+  LevelBuf<double>& B0 = s->lv[0].d;
+  if (Lv == 1) {
+    k_dense<double><<<1, 256, 0, stream>>>(s->C, s->nc, b, x);
+    CHECK_LAUNCH();
+    k_fine_sums<double, 2><<<G, kRedThreads, 0, stream>>>(x, s->flags, g, nullptr, s->singular, s->S, s->rb());
+    CHECK_LAUNCH();
+    return 0;
+  }
+  const double w0 = s->lv[0].weight;
+  double* a = x;
+  double* t = s->xtmp;
+  for (int k = 0; k < sw; ++k) {
+    k_fine_smooth<double, BStored<double>, 0><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, a, t, nullptr,
+                                                                             s->singular, s->S, s->rb());
+    CHECK_LAUNCH();
+    std::swap(a, t);
+  }
+  k_fine_resid<double, BStored<double>><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, a, B0.res);
+  CHECK_LAUNCH();
+  double* cur[32];
+  cur[0] = a;
+  for (int l = 1; l < Lv; ++l) {
+    Level& Lc = s->lv[l];
+    const double* res_f = s->lv[l - 1].d.res;
+    ELL_DISPATCH(Lc.R.lanes, (k_ell_spmv<L, false, double><<<ell_grid(Lc.R.n, L), 256, 0, stream>>>(Lc.R.view(), res_f, Lc.d.b)));
+    CHECK_LAUNCH();
+    if (l == Lv - 1) {
+      k_dense<double><<<1, 256, 0, stream>>>(s->C, s->nc, Lc.d.b, Lc.d.xa);
+      CHECK_LAUNCH();
+      cur[l] = Lc.d.xa;
+      break;
+    }
+    ELL_DISPATCH(Lc.A.lanes, (k_ell_pre<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.wd, Lc.d.b, Lc.d.xa, Lc.d.res)));
+    CHECK_LAUNCH();
+    double* p = Lc.d.xa;
+    double* o = Lc.d.xb;
+    if (sw > 1) {
+      for (int k = 1; k < sw; ++k) {
+        ELL_DISPATCH(Lc.A.lanes, (k_ell_smooth<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.wd, Lc.d.b, p, o)));
+        CHECK_LAUNCH();
+        std::swap(p, o);
+      }
+      ELL_DISPATCH(Lc.A.lanes, (k_ell_resid<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.d.b, p, Lc.d.res)));
+      CHECK_LAUNCH();
+    }
+    cur[l] = p;
+  }
+  for (int l = Lv - 2; l >= 0; --l) {
+    Level& Lf = s->lv[l];
+    const DevEll<double>& P = s->lv[l + 1].P;
+    double* xf = cur[l];
+    ELL_DISPATCH(P.lanes, (k_ell_spmv<L, true, double><<<ell_grid(P.n, L), 256, 0, stream>>>(P.view(), cur[l + 1], xf)));
+    CHECK_LAUNCH();
+    if (l == 0) {
+      double* o = (xf == x) ? s->xtmp : x;
+      for (int k = 1; k <= sw; ++k) {
+        if (k == sw)
+          k_fine_smooth<double, BStored<double>, 2><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+                                                                                   s->singular, s->S, s->rb());
+        else
+          k_fine_smooth<double, BStored<double>, 0><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+                                                                                   s->singular, s->S, s->rb());
+        CHECK_LAUNCH();
+        std::swap(xf, o);
+      }
+      if (xf != x) CU(cudaMemcpyAsync(x, xf, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    } else {
+      double* o = (xf == Lf.d.xa) ? Lf.d.xb : Lf.d.xa;
+      for (int k = 1; k <= sw; ++k) {
+        ELL_DISPATCH(Lf.A.lanes, (k_ell_smooth<L, double><<<ell_grid(Lf.A.n, L), 256, 0, stream>>>(Lf.A.view(), Lf.wd, Lf.d.b, xf, o)));
+        CHECK_LAUNCH();
+        std::swap(xf, o);
+      }
+      cur[l] = xf;
+    }
+  }
+  return 0;
+}
+
+int read_flags(pycfd_solver* s, cudaStream_t stream) {
+  CU(cudaMemcpyAsync(s->hI, s->I, sizeof(int) * I_COUNT, cudaMemcpyDeviceToHost, stream));
+  CU(cudaStreamSynchronize(stream));
+  return 0;
+}
+
+// ---- Poisson solve on the prepared raw right-hand side s->b --------------
+// Result (normalised) in x.  has_x0: x holds the warm start on entry.
+int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
+  const Geo& g = s->g;
+  const int G = grid1(s);
+  const SolveCfg cfg = s->cfg();
+  const int kind = s->solver_kind;
+  if (kind == PCFD_SOLVER_CG || kind == PCFD_SOLVER_MGCG) {
+    k_rhs_init<double><<<G, kRedThreads, 0, stream>>>(s->b, x, s->r, s->flags, g, cfg, has_x0, s->S,
+                                                      s->I, s->rb());
+    CHECK_LAUNCH();
+    double* pc = s->pa;
+    double* po = s->pb;
+    for (;;) {
+      TRY(read_flags(s, stream));
+      if (s->hI[I_DONE]) break;
+      if (kind == PCFD_SOLVER_CG) {
+        k_cg_pq<double, PC_JACOBI><<<G, kRedThreads, 0, stream>>>(s->r, nullptr, pc, po, s->q, s->flags, g,
+                                                                  s->S, s->I, s->rb());
+        CHECK_LAUNCH();
+        k_cg_xr<double, PC_JACOBI><<<G, kRedThreads, 0, stream>>>(x, s->r, po, s->q, s->flags, g, cfg, s->S,
+                                                                  s->I, s->rb());
+      } else {
+        TRY(vcycle_pcg<double>(s, s->r, s->z, stream));
+        k_cg_pq<double, PC_MG><<<G, kRedThreads, 0, stream>>>(s->r, s->z, pc, po, s->q, s->flags, g, s->S,
+                                                              s->I, s->rb());
+        CHECK_LAUNCH();
+        k_cg_xr<double, PC_MG><<<G, kRedThreads, 0, stream>>>(x, s->r, po, s->q, s->flags, g, cfg, s->S,
+                                                              s->I, s->rb());
+      }
+      CHECK_LAUNCH();
+      std::swap(pc, po);
+    }
+    k_finish_stats<double><<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
+    CHECK_LAUNCH();
+  } else {
+    const int project_x0 = kind == PCFD_SOLVER_MULTIGRID;
+    k_stationary_init<<<G, kRedThreads, 0, stream>>>(s->b, x, s->flags, g, cfg, has_x0, project_x0, s->S,
+                                                     s->I, s->rb());
+    CHECK_LAUNCH();
+    if (kind == PCFD_SOLVER_MULTIGRID) {
+      k_apply_mean<<<G, kRedThreads, 0, stream>>>(s->b, s->flags, g, s->S, S_MEAN_B);
+      k_apply_mean<<<G, kRedThreads, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
+      CHECK_LAUNCH();
+      k_resnorm<<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb());
+      CHECK_LAUNCH();
+      for (;;) {
+        TRY(read_flags(s, stream));
+        if (s->hI[I_DONE]) break;
+        TRY(vcycle_standalone(s, s->b, x, stream));
+        k_resnorm<<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 1, 1, s->S, s->I, s->rb());
+        CHECK_LAUNCH();
+        k_apply_mean<<<G, kRedThreads, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
+        CHECK_LAUNCH();
+      }
+    } else {
+      double* cur = x;
+      double* oth = s->xtmp;
+      const int every = kind == PCFD_SOLVER_JACOBI ? 20 : 5;
+      for (int it = 1; it <= s->maxiter; ++it) {
+        if (kind == PCFD_SOLVER_JACOBI) {
+          k_jacobi_sweep<<<G, kRedThreads, 0, stream>>>(cur, oth, s->b, s->flags, g, 2.0 / 3.0, s->singular,
+                                                        s->S, s->I, s->rb());
+          CHECK_LAUNCH();
+          std::swap(cur, oth);
+        } else {
+          k_sor_half<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
+                                                    s->I, s->rb());
+          k_sor_half<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
+                                                    s->I, s->rb());
+          CHECK_LAUNCH();
+        }
+        if (it % every == 0 || it == s->maxiter) {
+          k_resnorm<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, cfg, 0, 0, 1, s->S, s->I, s->rb());
+          CHECK_LAUNCH();
+          TRY(read_flags(s, stream));
+          if (s->hI[I_DONE]) break;
+        }
+      }
+      if (cur != x) CU(cudaMemcpyAsync(x, cur, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    }
+    k_finish_stats<double><<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 0, s->S, s->I, s->rb());
+    CHECK_LAUNCH();
+  }
+  k_finish_apply<double><<<G, kRedThreads, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int set_dt(pycfd_solver* s, double dt, double blend, cudaStream_t stream) {
+  // The step parameters live in device memory so a recorded step can replay
+  // with new values.  Written from pinned host memory, ordered on the stream.
+  CU(cudaStreamSynchronize(stream));
+  s->hS[S_DT] = dt;
+  s->hS[S_BLEND] = blend;
+  CU(cudaMemcpyAsync(s->S + S_DT, s->hS + S_DT, 2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+  return 0;
+}
+
+// ProjectionSolver.project: solve lap p = div(u)/dt with the warm start, then
+// correct the solvable faces and write the ghosted p.
+int project_impl(pycfd_solver* s, double* u, double* v, double* p, double dt_override,
+                 cudaStream_t stream) {
+  const int G = grid1(s);
+  k_div_rhs<<<G, kRedThreads, 0, stream>>>(u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  CHECK_LAUNCH();
+  TRY(solve_prepared(s, s->x, s->has_guess, stream));
+  s->has_guess = true;
+  const long nfaces = std::max<long>((long)(s->g.u_hi - s->g.u_lo) * s->g.ny, (long)s->g.nx * (s->g.v_hi - s->g.v_lo));
+  const int gc = grid_for(std::max(nfaces, s->ncell()), 256, kMaxRedBlocks) + 1;
+  k_correct<<<gc, 256, 0, stream>>>(u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int substep_impl(pycfd_solver* s, StageIn uin, StageIn vin, double* us, double* vs, double* p,
+                 cudaStream_t stream) {
+  const Geo& g = s->g;
+  dim3 blk(TJ, TI);
+  dim3 grd((g.ny + 3 + TJ - 1) / TJ, (g.nx + 3 + TI - 1) / TI);
+  k_predictor<<<grd, blk, 0, stream>>>(uin, vin, us, vs, g, s->S);
+  CHECK_LAUNCH();
+  TRY(launch_boundary(s, us, vs, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, stream));
+  TRY(project_impl(s, us, vs, p, -1.0, stream));
+  TRY(launch_boundary(s, us, vs, {OP_MASK_ACC, OP_WRAP_FACES, OP_VEL_CORR}, stream));
+  return 0;
+}
+
+int step_impl(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v, double* p,
+              cudaStream_t stream) {
+  const long nu = (long)(s->g.nx + 3) * (s->g.ny + 2), nv = (long)(s->g.nx + 2) * (s->g.ny + 3);
+  StageIn U0{u0, nullptr, 1.0, 0.0}, V0{v0, nullptr, 1.0, 0.0};
+  if (s->scheme == PCFD_EULER) {
+    TRY(substep_impl(s, U0, V0, u, v, p, stream));
+    return 0;
+  }
+  if (s->scheme == PCFD_RK2) {
+    TRY(substep_impl(s, U0, V0, s->us1, s->vs1, p, stream));
+    TRY(substep_impl(s, StageIn{s->us1, nullptr, 1.0, 0.0}, StageIn{s->vs1, nullptr, 1.0, 0.0}, s->us2,
+                     s->vs2, p, stream));
+    k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us2, 0.5, 0.5, u, nu);
+    k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs2, 0.5, 0.5, v, nv);
+    CHECK_LAUNCH();
+  } else {
+    TRY(substep_impl(s, U0, V0, s->us1, s->vs1, p, stream));
+    TRY(substep_impl(s, StageIn{s->us1, nullptr, 1.0, 0.0}, StageIn{s->vs1, nullptr, 1.0, 0.0}, s->us2,
+                     s->vs2, p, stream));
+    TRY(substep_impl(s, StageIn{u0, s->us2, 0.75, 0.25}, StageIn{v0, s->vs2, 0.75, 0.25}, s->us1, s->vs1,
+                     p, stream));
+    k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us1, 1.0 / 3.0, 2.0 / 3.0, u, nu);
+    k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs1, 1.0 / 3.0, 2.0 / 3.0, v, nv);
+    CHECK_LAUNCH();
+  }
+  TRY(launch_boundary(s, u, v, {OP_VEL_CORR, OP_WRAP_FACES}, stream));
+  return 0;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* pycfd_last_error(void) { return g_err.c_str(); }
+int pycfd_version(void) { return 1; }
+
+int pycfd_solver_destroy(pycfd_solver* s) {
+  if (!s) return 0;
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->hS) cudaFreeHost(s->hS);
+  if (s->hI) cudaFreeHost(s->hI);
+  delete s;
+  return 0;
+}
+
+int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
+  if (!d || !out) return fail(PCFD_E_ARG, "null descriptor");
+  if (d->nx < 4 || d->ny < 4) return fail(PCFD_E_ARG, "mesh must be at least 4x4 cells");
+  if (d->solver_kind < PCFD_SOLVER_CG || d->solver_kind > PCFD_SOLVER_MGCG)
+    return fail(PCFD_E_UNSUPPORTED, "pressure solver %d is not provided on the GPU path", d->solver_kind);
+  if (d->n_bodies < 0 || d->n_bodies > PCFD_MAX_BODIES) return fail(PCFD_E_ARG, "too many bodies");
+  pycfd_solver* s = new pycfd_solver();
+  auto bail = [&](int rc) { pycfd_solver_destroy(s); return rc; };
+  const int nx = d->nx, ny = d->ny;
+  Geo& g = s->g;
+  g.nx = nx;
+  g.ny = ny;
+  g.dx = d->dx;
+  g.dy = d->dy;
+  g.nu = d->nu;
+  g.fx = d->body_fx;
+  g.fy = d->body_fy;
+  g.cx = 1.0 / (d->dx * d->dx);
+  g.cy = 1.0 / (d->dy * d->dy);
+  const int* K = d->bc_kind;
+  g.periodic_x = K[W_LEFT] == BC_PERIODIC;
+  g.periodic_y = K[W_BOTTOM] == BC_PERIODIC;
+  if ((K[W_LEFT] == BC_PERIODIC) != (K[W_RIGHT] == BC_PERIODIC) ||
+      (K[W_BOTTOM] == BC_PERIODIC) != (K[W_TOP] == BC_PERIODIC))
+    return bail(fail(PCFD_E_ARG, "periodicity must be set on both walls of an axis"));
+  const int PO = BC_PRESSURE_OUTLET;
+  // solvable face ranges (pycfd/core/solver.py:235-263)
+  g.u_lo = (g.periodic_x || K[W_LEFT] == PO) ? 1 : 2;
+  g.u_hi = (K[W_RIGHT] == PO && !g.periodic_x) ? nx + 2 : nx + 1;
+  g.v_lo = (g.periodic_y || K[W_BOTTOM] == PO) ? 1 : 2;
+  g.v_hi = (K[W_TOP] == PO && !g.periodic_y) ? ny + 2 : ny + 1;
+  g.dir_w = K[W_LEFT] == PO;
+  g.dir_e = K[W_RIGHT] == PO;
+  g.dir_s = K[W_BOTTOM] == PO;
+  g.dir_n = K[W_TOP] == PO;
+  g.pref_w = d->bc_p_ref[W_LEFT];
+  g.pref_e = d->bc_p_ref[W_RIGHT];
+  g.pref_s = d->bc_p_ref[W_BOTTOM];
+  g.pref_n = d->bc_p_ref[W_TOP];
+  s->singular = !(g.dir_w || g.dir_e || g.dir_s || g.dir_n);
+  s->solver_kind = d->solver_kind;
+  s->tol = d->tol;
+  s->maxiter = d->maxiter;
+  s->omega = d->sor_omega;
+  s->mg_sweeps = std::max(1, d->mg_sweeps);
+  s->scheme = d->time_scheme;
+  s->precision = d->precision;
+  s->inner_tol = d->inner_tol > 0 ? d->inner_tol : 1e-4;
+
+  // ---- cell flags of the fine operator (pycfd/core/pressure.py:209-247) ----
+  const long n = (long)nx * ny;
+  std::vector<uint8_t> solid(n, 0), flags(n, 0);
+  if (d->solid)
+    for (long c = 0; c < n; ++c) solid[c] = d->solid[c] ? 1 : 0;
+  auto fluid = [&](int i, int j) { return !solid[(long)i * ny + j]; };
+  int n_fluid = 0;
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      if (!fluid(i, j)) continue;
+      uint8_t f = 0;
+      const bool in_w = i > 0 || g.periodic_x, in_e = i < nx - 1 || g.periodic_x;
+      const bool in_s = j > 0 || g.periodic_y, in_n = j < ny - 1 || g.periodic_y;
+      if (in_w && fluid((i + nx - 1) % nx, j)) f |= F_W;
+      if (in_e && fluid((i + 1) % nx, j)) f |= F_E;
+      if (in_s && fluid(i, (j + ny - 1) % ny)) f |= F_S;
+      if (in_n && fluid(i, (j + 1) % ny)) f |= F_N;
+      // isolated = no active face and no Dirichlet wall contribution
+      const bool dirw = g.dir_w && i == 0, dire = g.dir_e && i == nx - 1;
+      const bool dirs = g.dir_s && j == 0, dirn = g.dir_n && j == ny - 1;
+      if (f || dirw || dire || dirs || dirn) {
+        f |= F_SOLV;
+        ++n_fluid;
+      }
+      flags[(long)i * ny + j] = f;
+    }
+  g.n_fluid = n_fluid;
+  if (s->solver_kind == PCFD_SOLVER_SOR) {
+    // red/black colouring must not couple a colour to itself (pycfd/core/pressure.py:486-496)
+    bool bad = false;
+    if (g.periodic_x && (nx % 2 == 1))
+      for (int j = 0; j < ny && !bad; ++j) bad = (flags[(long)(nx - 1) * ny + j] & F_E) != 0;
+    if (g.periodic_y && (ny % 2 == 1))
+      for (int i = 0; i < nx && !bad; ++i) bad = (flags[(long)i * ny + ny - 1] & F_N) != 0;
+    if (bad)
+      return bail(fail(PCFD_E_ARG,
+                       "red/black ordering is invalid for this grid (cells of one colour are coupled "
+                       "to each other). This happens with an odd number of cells on a periodic axis; "
+                       "use an even nx/ny"));
+  }
+  int rc;
+  if ((rc = upload(s, &s->flags, flags.data(), n))) return bail(rc);
+  if ((rc = upload(s, &s->solid, solid.data(), n))) return bail(rc);
+
+  // ---- mask face lists (pycfd/core/solver.py:62-79, :285-296) ----
+  auto solid_at = [&](int ci, int cj, int axis) -> int {
+    // zero-based cell (ci, cj); off-domain = fluid unless periodic
+    if (axis == 0) {
+      if (ci < 0 || ci >= nx) {
+        if (!g.periodic_x) return 0;
+        ci = (ci % nx + nx) % nx;
+      }
+    } else {
+      if (cj < 0 || cj >= ny) {
+        if (!g.periodic_y) return 0;
+        cj = (cj % ny + ny) % ny;
+      }
+    }
+    const long c = (long)ci * ny + cj;
+    if (!solid[c]) return 0;
+    return d->body_id ? d->body_id[c] : 1;
+  };
+  const int nb = d->n_bodies;
+  std::vector<std::vector<int>> mu(std::max(nb, 1)), mv(std::max(nb, 1));
+  if (d->solid) {
+    for (int m = g.u_lo; m < g.u_hi; ++m)
+      for (int j = 1; j <= ny; ++j) {
+        const int a = solid_at(m - 2, j - 1, 0), b = solid_at(m - 1, j - 1, 0);
+        if (a || b) {
+          const int body = nb ? std::max(a, b) - 1 : 0;
+          mu[std::max(0, std::min(body, std::max(nb, 1) - 1))].push_back(m * (ny + 2) + j);
+        }
+      }
+    for (int i = 1; i <= nx; ++i)
+      for (int k = g.v_lo; k < g.v_hi; ++k) {
+        const int a = solid_at(i - 1, k - 2, 1), b = solid_at(i - 1, k - 1, 1);
+        if (a || b) {
+          const int body = nb ? std::max(a, b) - 1 : 0;
+          mv[std::max(0, std::min(body, std::max(nb, 1) - 1))].push_back(i * (ny + 3) + k);
+        }
+      }
+  }
+  std::vector<int> lu, lvv;
+  s->bc.n_bodies = nb;
+  for (int b = 0; b < std::max(nb, 1); ++b) {
+    s->bc.body_u_start[b] = (int)lu.size();
+    s->bc.body_v_start[b] = (int)lvv.size();
+    lu.insert(lu.end(), mu[b].begin(), mu[b].end());
+    lvv.insert(lvv.end(), mv[b].begin(), mv[b].end());
+  }
+  s->bc.body_u_start[std::max(nb, 1)] = (int)lu.size();
+  s->bc.body_v_start[std::max(nb, 1)] = (int)lvv.size();
+  if ((rc = upload(s, &s->mask_u, lu.data(), lu.size()))) return bail(rc);
+  if ((rc = upload(s, &s->mask_v, lvv.data(), lvv.size()))) return bail(rc);
+  s->bc.mask_u = s->mask_u;
+  s->bc.mask_v = s->mask_v;
+  s->bc.n_mask_u = (int)lu.size();
+  s->bc.n_mask_v = (int)lvv.size();
+  s->bc.area = d->dx * d->dy;
+  s->bc.has_outlet = 0;
+  for (int w = 0; w < 4; ++w) {
+    s->bc.kind[w] = K[w];
+    s->bc.vel[w] = d->bc_velocity[w];
+    s->bc.pref[w] = d->bc_p_ref[w];
+    s->bc.profile[w] = nullptr;
+    if (K[w] == BC_OUTLET) s->bc.has_outlet = 1;
+    if (K[w] == BC_INLET && d->bc_profile[w]) {
+      const int len = w < 2 ? ny + 2 : nx + 2;
+      if ((rc = upload(s, &s->profile[w], d->bc_profile[w], len))) return bail(rc);
+      s->bc.profile[w] = s->profile[w];
+    }
+  }
+  if ((rc = upload(s, &s->bc_kind_dev, K, 4))) return bail(rc);
+
+  // ---- workspace ----
+  const long nu_all = (long)(nx + 3) * (ny + 2), nv_all = (long)(nx + 2) * (ny + 3);
+  if ((rc = dalloc(s, &s->S, S_COUNT)) || (rc = dalloc(s, &s->I, I_COUNT)) ||
+      (rc = dalloc(s, &s->partials, (size_t)kMaxRedBlocks * 8)) || (rc = dalloc(s, &s->counter, 1)) ||
+      (rc = dalloc(s, &s->us1, nu_all)) || (rc = dalloc(s, &s->vs1, nv_all)) ||
+      (rc = dalloc(s, &s->us2, nu_all)) || (rc = dalloc(s, &s->vs2, nv_all)) ||
+      (rc = dalloc(s, &s->b, n)) || (rc = dalloc(s, &s->x, n)) || (rc = dalloc(s, &s->x_api, n)) ||
+      (rc = dalloc(s, &s->r, n)) || (rc = dalloc(s, &s->pa, n)) || (rc = dalloc(s, &s->pb, n)) ||
+      (rc = dalloc(s, &s->q, n)) || (rc = dalloc(s, &s->z, n)) || (rc = dalloc(s, &s->xtmp, n)))
+    return bail(rc);
+  if (cudaHostAlloc((void**)&s->hS, S_COUNT * sizeof(double), cudaHostAllocDefault) != cudaSuccess ||
+      cudaHostAlloc((void**)&s->hI, I_COUNT * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+    return bail(fail(PCFD_E_CUDA, "pinned allocation failed"));
+  memset(s->hS, 0, S_COUNT * sizeof(double));
+  memset(s->hI, 0, I_COUNT * sizeof(int));
+
+  // ---- multigrid hierarchy ----
+  const bool mg = s->solver_kind == PCFD_SOLVER_MULTIGRID || s->solver_kind == PCFD_SOLVER_MGCG;
+  if (mg) {
+    if (d->n_levels < 1 || !d->levels || !d->coarsest_inverse)
+      return bail(fail(PCFD_E_ARG, "multigrid solver needs a hierarchy"));
+    if (d->levels[0].n != n) return bail(fail(PCFD_E_ARG, "level 0 must have nx*ny unknowns"));
+    s->lv.resize(d->n_levels);
+    for (int l = 0; l < d->n_levels; ++l) {
+      const pycfd_mg_level& in = d->levels[l];
+      Level& L = s->lv[l];
+      L.n = in.n;
+      L.sx = in.shape_x;
+      L.sy = in.shape_y;
+      L.weight = in.weight;
+      const bool coarsest = l == d->n_levels - 1;
+      if ((rc = dalloc(s, &L.d.b, L.n)) || (rc = dalloc(s, &L.d.xa, L.n)) || (rc = dalloc(s, &L.d.xb, L.n)) ||
+          (rc = dalloc(s, &L.d.res, L.n)) || (rc = dalloc(s, &L.f.b, L.n)) || (rc = dalloc(s, &L.f.xa, L.n)) ||
+          (rc = dalloc(s, &L.f.xb, L.n)) || (rc = dalloc(s, &L.f.res, L.n)))
+        return bail(rc);
+      if (l >= 1) {
+        const pycfd_mg_level& up = d->levels[l - 1];
+        if (!coarsest) {
+          if (!in.a_indptr || !in.weighted_dinv) return bail(fail(PCFD_E_ARG, "level %d lacks A", l));
+          if ((rc = make_ell(s, &L.A, L.n, in.a_indptr, in.a_indices, in.a_data)) ||
+              (rc = make_ell(s, &L.Af, L.n, in.a_indptr, in.a_indices, in.a_data)))
+            return bail(rc);
+          std::vector<float> wf(in.weighted_dinv, in.weighted_dinv + L.n);
+          if ((rc = upload(s, &L.wd, in.weighted_dinv, L.n)) || (rc = upload(s, &L.wdf, wf.data(), L.n)))
+            return bail(rc);
+        }
+        if (!in.p_indptr) return bail(fail(PCFD_E_ARG, "level %d lacks P", l));
+        if ((rc = make_ell(s, &L.P, up.n, in.p_indptr, in.p_indices, in.p_data)) ||
+            (rc = make_ell(s, &L.Pf, up.n, in.p_indptr, in.p_indices, in.p_data)))
+          return bail(rc);
+        std::vector<int64_t> tp;
+        std::vector<int32_t> ti;
+        std::vector<double> td;
+        csr_transpose(up.n, L.n, in.p_indptr, in.p_indices, in.p_data, tp, ti, td);
+        if ((rc = make_ell(s, &L.R, L.n, tp.data(), ti.data(), td.data())) ||
+            (rc = make_ell(s, &L.Rf, L.n, tp.data(), ti.data(), td.data())))
+          return bail(rc);
+      }
+    }
+    const int ncs = d->levels[d->n_levels - 1].n;
+    s->nc = ncs;
+    std::vector<double> cm((size_t)ncs * ncs);
+    std::vector<float> cf((size_t)ncs * ncs);
+    for (int r0 = 0; r0 < ncs; ++r0)
+      for (int k = 0; k < ncs; ++k) {
+        cm[(size_t)k * ncs + r0] = d->coarsest_inverse[(size_t)r0 * ncs + k];
+        cf[(size_t)k * ncs + r0] = (float)d->coarsest_inverse[(size_t)r0 * ncs + k];
+      }
+    if ((rc = upload(s, &s->C, cm.data(), cm.size())) || (rc = upload(s, &s->Cf, cf.data(), cf.size())))
+      return bail(rc);
+  }
+  if (s->precision == PCFD_MIXED) {
+    if ((rc = dalloc(s, &s->r32, n)) || (rc = dalloc(s, &s->x32, n)) || (rc = dalloc(s, &s->pa32, n)) ||
+        (rc = dalloc(s, &s->pb32, n)) || (rc = dalloc(s, &s->q32, n)) || (rc = dalloc(s, &s->z32, n)))
+      return bail(rc);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(PCFD_E_CUDA, "setup failed"));
+  *out = s;
+  return 0;
+}
+
+int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double dx, double dy, double nu,
+                       double blend, double fx, double fy, double* rhs_u, double* rhs_v, void* stream) {
+  if (!u || !v || !rhs_u || !rhs_v || nx < 1 || ny < 1) return fail(PCFD_E_ARG, "bad arguments");
+  dim3 blk(TJ, TI), grd((ny + 1 + TJ - 1) / TJ, (nx + 1 + TI - 1) / TI);
+  k_rhs<<<grd, blk, 0, st(stream)>>>(u, v, nx, ny, dx, dy, nu, blend, fx, fy, rhs_u, rhs_v);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy, double* out,
+                     void* stream) {
+  if (!u || !v || !out || nx < 1 || ny < 1) return fail(PCFD_E_ARG, "bad arguments");
+  k_divergence<<<grid_for((long)nx * ny, 256), 256, 0, st(stream)>>>(u, v, nx, ny, dx, dy, out);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_apply_velocity_bc(pycfd_solver* s, double* u, double* v, int predictor, int mass_balance,
+                            void* stream) {
+  if (!s || !u || !v) return fail(PCFD_E_ARG, "bad arguments");
+  if (mass_balance)
+    return launch_boundary(s, u, v, {predictor ? OP_VEL_PRED : OP_VEL_CORR, OP_MASS}, st(stream));
+  return launch_boundary(s, u, v, {predictor ? OP_VEL_PRED : OP_VEL_CORR}, st(stream));
+}
+
+int pycfd_poisson_solve(pycfd_solver* s, const double* rhs, const double* p0, double* p, void* stream) {
+  if (!s || !rhs || !p) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  const int G = grid1(s);
+  TRY(set_dt(s, 1.0, 0.0, sm));
+  k_div_rhs<<<G, kRedThreads, 0, sm>>>(nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  CHECK_LAUNCH();
+  if (p0) CU(cudaMemcpyAsync(s->x_api, p0, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
+  TRY(solve_prepared(s, s->x_api, p0 != nullptr, sm));
+  CU(cudaMemcpyAsync(p, s->x_api, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
+  return 0;
+}
+
+int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream) {
+  if (!s || !r || !z) return fail(PCFD_E_ARG, "bad arguments");
+  if (s->lv.empty()) return fail(PCFD_E_ARG, "solver has no multigrid hierarchy");
+  cudaStream_t sm = st(stream);
+  const int G = grid1(s);
+  // mean of r over the active set, then one cycle and the projection of z
+  k_div_rhs<<<G, kRedThreads, 0, sm>>>(nullptr, nullptr, r, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  CHECK_LAUNCH();
+  // k_div_rhs left the solvable sum in S_MEAN_B; the cycle reads S_MEAN_R.
+  CU(cudaMemcpyAsync(s->S + S_MEAN_R, s->S + S_MEAN_B, sizeof(double), cudaMemcpyDeviceToDevice, sm));
+  CU(cudaMemsetAsync(s->S + S_SUM_R, 0, sizeof(double), sm));
+  CU(cudaMemsetAsync(s->I + I_ZERO_RHS, 0, sizeof(int), sm));
+  TRY(vcycle_pcg<double>(s, r, s->z, sm));
+  // z = z_raw - mean_z on solvable rows, 0 elsewhere
+  CU(cudaMemcpyAsync(s->S + S_MEAN_X, s->S + S_MEAN_Z, sizeof(double), cudaMemcpyDeviceToDevice, sm));
+  k_finish_apply<double><<<G, kRedThreads, 0, sm>>>(s->z, z, s->flags, s->g, s->S, s->I);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_project(pycfd_solver* s, double* u, double* v, double* p, double dt, void* stream) {
+  if (!s || !u || !v || !p || !(dt > 0)) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  TRY(set_dt(s, dt, 0.0, sm));
+  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
+  return project_impl(s, u, v, p, -1.0, sm);
+}
+
+int pycfd_initialize(pycfd_solver* s, double* u, double* v, double* p, void* stream) {
+  if (!s || !u || !v || !p) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  TRY(set_dt(s, 1.0, 0.0, sm));
+  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
+  TRY(launch_boundary(s, u, v, {OP_VEL_PRED, OP_MASS, OP_MASK_NONE, OP_WRAP_FACES}, sm));
+  TRY(project_impl(s, u, v, p, -1.0, sm));
+  TRY(launch_boundary(s, u, v, {OP_MASK_NONE, OP_WRAP_FACES, OP_VEL_CORR}, sm));
+  return 0;
+}
+
+int pycfd_substep(pycfd_solver* s, const double* u, const double* v, double* us, double* vs, double* p,
+                  double dt, double blend, void* stream) {
+  if (!s || !u || !v || !us || !vs || !p) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  TRY(set_dt(s, dt, blend, sm));
+  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
+  return substep_impl(s, StageIn{u, nullptr, 1.0, 0.0}, StageIn{v, nullptr, 1.0, 0.0}, us, vs, p, sm);
+}
+
+int pycfd_step(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v, double* p,
+               double dt, double blend, void* stream) {
+  if (!s || !u0 || !v0 || !u || !v || !p) return fail(PCFD_E_ARG, "bad arguments");
+  if (u0 == u || v0 == v) return fail(PCFD_E_ARG, "step outputs must not alias its inputs");
+  cudaStream_t sm = st(stream);
+  TRY(set_dt(s, dt, blend, sm));
+  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
+  return step_impl(s, u0, v0, u, v, p, sm);
+}
+
+int pycfd_step_host(pycfd_solver* s, const double* u0h, const double* v0h, double* uh, double* vh,
+                    double* ph, double dt, double blend, void* stream) {
+  if (!s || !u0h || !v0h || !uh || !vh || !ph) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  const long nu = (long)(s->g.nx + 3) * (s->g.ny + 2), nv = (long)(s->g.nx + 2) * (s->g.ny + 3),
+             np = (long)(s->g.nx + 2) * (s->g.ny + 2);
+  if (!s->hu0) {
+    int rc;
+    if ((rc = dalloc(s, &s->hu0, nu)) || (rc = dalloc(s, &s->hv0, nv)) || (rc = dalloc(s, &s->hu, nu)) ||
+        (rc = dalloc(s, &s->hv, nv)) || (rc = dalloc(s, &s->hp, np)))
+      return rc;
+  }
+  CU(cudaMemcpyAsync(s->hu0, u0h, nu * sizeof(double), cudaMemcpyHostToDevice, sm));
+  CU(cudaMemcpyAsync(s->hv0, v0h, nv * sizeof(double), cudaMemcpyHostToDevice, sm));
+  TRY(pycfd_step(s, s->hu0, s->hv0, s->hu, s->hv, s->hp, dt, blend, stream));
+  CU(cudaMemcpyAsync(uh, s->hu, nu * sizeof(double), cudaMemcpyDeviceToHost, sm));
+  CU(cudaMemcpyAsync(vh, s->hv, nv * sizeof(double), cudaMemcpyDeviceToHost, sm));
+  CU(cudaMemcpyAsync(ph, s->hp, np * sizeof(double), cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  return 0;
+}
+
+int pycfd_get_stats(pycfd_solver* s, pycfd_stats* o, void* stream) {
+  if (!s || !o) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  CU(cudaMemcpyAsync(s->hS, s->S, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, sm));
+  CU(cudaMemcpyAsync(s->hI, s->I, sizeof(int) * I_COUNT, cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  memset(o, 0, sizeof *o);
+  o->iterations = s->hI[I_IT];
+  o->converged = s->hI[I_CONVERGED];
+  o->status = s->hI[I_STATUS];
+  o->total_iterations = s->hI[I_TOTAL_IT];
+  o->last_residual = s->hS[S_RESID];
+  o->fx = s->hS[S_FX];
+  o->fy = s->hS[S_FY];
+  for (int b = 0; b < PCFD_MAX_BODIES; ++b) {
+    o->body_fx[b] = s->hS[S_BODY_FX + b];
+    o->body_fy[b] = s->hS[S_BODY_FY + b];
+  }
+  o->ir_iterations = s->last_ir;
+  return 0;
+}
+
+int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const double* p, const double* up,
+                      const double* vp, pycfd_field_stats* o, void* stream) {
+  if (!s || !u || !v || !o) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  const long nmax = (long)(s->g.nx + 3) * (s->g.ny + 3);
+  k_field_stats<<<grid_for(nmax, kRedThreads), kRedThreads, 0, sm>>>(u, v, p, up, vp, s->solid, s->g, s->rb(),
+                                                                     s->S);
+  CHECK_LAUNCH();
+  CU(cudaMemcpyAsync(s->hS + S_STAT0, s->S + S_STAT0, 8 * sizeof(double), cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  const double* t = s->hS + S_STAT0;
+  o->max_u = t[0];
+  o->max_v = t[1];
+  o->max_du = t[2];
+  o->max_dv = t[3];
+  o->max_div = t[4];
+  o->kinetic_energy = t[5] * (s->g.dx * s->g.dy);
+  o->max_vorticity = t[6];
+  o->finite = t[7] == 0.0;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,336 @@
+// MAC-grid stencils: momentum predictor, divergence, projection correction,
+// Runge-Kutta stage combination, field statistics.
+//
+// Arithmetic follows the reference expression by expression (no FMA
+// contraction: the library is built with -fmad=false), so the predictor, the
+// divergence and the correction are bit-identical to the reference's
+// NumPy/Numba path on the same inputs.
+#pragma once
+#include "common.cuh"
+
+namespace pcfd {
+
+constexpr int TJ = 32;   // threads along y (contiguous)
+constexpr int TI = 8;    // threads along x
+
+// A stage field read either directly or as the Runge-Kutta combination
+// ca*a + cb*b formed on the fly (pycfd/core/solver.py:716-717).
+struct StageIn {
+  const double* a;
+  const double* b;   // nullptr: plain read of a
+  double ca, cb;
+  __device__ __forceinline__ double operator[](long k) const {
+    return b ? ca * a[k] + cb * b[k] : a[k];
+  }
+};
+
+// u-momentum RHS at u-face (m, j), 1<=m<=nx+1, 1<=j<=ny
+// (pycfd/core/kernels.py:54-80).
+template <class U, class V>
+__device__ __forceinline__ double rhs_u_at(const U& u, const V& v, int m, int j, int ny,
+                                           double dx, double dy, double nu, double blend,
+                                           double fx) {
+  const long W = ny + 2, WV = ny + 3;
+  const double u0 = u[m * W + j];
+  const double ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
+  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+  const double u_right = 0.5 * (u0 + ue);
+  const double u_left = 0.5 * (uw + u0);
+  double duudx = (u_right * u_right - u_left * u_left) / dx;
+  const double u_top = 0.5 * (u0 + un);
+  const double v_top = 0.5 * (v[(m - 1) * WV + j + 1] + v[m * WV + j + 1]);
+  const double u_bot = 0.5 * (us + u0);
+  const double v_bot = 0.5 * (v[(m - 1) * WV + j] + v[m * WV + j]);
+  double duvdy = (u_top * v_top - u_bot * v_bot) / dy;
+  if (blend > 0.0) {
+    duudx += blend / dx * (fabs(u_right) * (u0 - ue) * 0.5 - fabs(u_left) * (uw - u0) * 0.5);
+    duvdy += blend / dy * (fabs(v_top) * (u0 - un) * 0.5 - fabs(v_bot) * (us - u0) * 0.5);
+  }
+  const double lap = ((uw - 2.0 * u0 + ue) / (dx * dx) + (us - 2.0 * u0 + un) / (dy * dy));
+  return -(duudx + duvdy) + nu * lap + fx;
+}
+
+// v-momentum RHS at v-face (i, n), 1<=i<=nx, 1<=n<=ny+1
+// (pycfd/core/kernels.py:83-110).
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n, int ny,
+                                           double dx, double dy, double nu, double blend,
+                                           double fy) {
+  const long W = ny + 2, WV = ny + 3;
+  const double v0 = v[i * WV + n];
+  const double vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
+  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+  const double v_top = 0.5 * (v0 + vn);
+  const double v_bot = 0.5 * (vs + v0);
+  double dvvdy = (v_top * v_top - v_bot * v_bot) / dy;
+  const double u_right = 0.5 * (u[(i + 1) * W + n - 1] + u[(i + 1) * W + n]);
+  const double v_right = 0.5 * (v0 + ve);
+  const double u_left = 0.5 * (u[i * W + n - 1] + u[i * W + n]);
+  const double v_left = 0.5 * (vw + v0);
+  double duvdx = (u_right * v_right - u_left * v_left) / dx;
+  if (blend > 0.0) {
+    dvvdy += blend / dy * (fabs(v_top) * (v0 - vn) * 0.5 - fabs(v_bot) * (vs - v0) * 0.5);
+    duvdx += blend / dx * (fabs(u_right) * (v0 - ve) * 0.5 - fabs(u_left) * (vw - v0) * 0.5);
+  }
+  const double lap = ((vw - 2.0 * v0 + ve) / (dx * dx) + (vs - 2.0 * v0 + vn) / (dy * dy));
+  return -(duvdx + dvvdy) + nu * lap + fy;
+}
+
+// Stateless RHS into (nx+1, ny) and (nx, ny+1) blocks.
+__global__ void k_rhs(const double* __restrict__ u, const double* __restrict__ v, int nx, int ny,
+                      double dx, double dy, double nu, double blend, double fx, double fy,
+                      double* __restrict__ rhs_u, double* __restrict__ rhs_v) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;   // 0..ny
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;   // 0..nx
+  if (i <= nx && j < ny) rhs_u[(long)i * ny + j] = rhs_u_at(u, v, i + 1, j + 1, ny, dx, dy, nu, blend, fx);
+  if (i < nx && j <= ny) rhs_v[(long)i * (ny + 1) + j] = rhs_v_at(u, v, i + 1, j + 1, ny, dx, dy, nu, blend, fy);
+}
+
+// Predictor: us = U + dt*rhs_u on the solvable u-faces, U elsewhere (same for
+// v), where U is the stage input (pycfd/core/solver.py:619-622).  dt and the
+// upwind blend are read from device scalars so a captured step can be replayed.
+__global__ void k_predictor(StageIn u, StageIn v, double* __restrict__ us, double* __restrict__ vs,
+                            Geo g, const double* __restrict__ S) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny;
+  const double dt = S[S_DT], blend = S[S_BLEND];
+  if (i < nx + 3 && j < ny + 2) {
+    const long k = (long)i * (ny + 2) + j;
+    double val = u[k];
+    if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
+      val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
+    us[k] = val;
+  }
+  if (i < nx + 2 && j < ny + 3) {
+    const long k = (long)i * (ny + 3) + j;
+    double val = v[k];
+    if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
+      val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
+    vs[k] = val;
+  }
+}
+
+__device__ __forceinline__ double cell_div(const double* u, const double* v, int ci, int cj,
+                                           int ny, double dx, double dy) {
+  const long W = ny + 2, WV = ny + 3;
+  return (u[(long)(ci + 2) * W + cj + 1] - u[(long)(ci + 1) * W + cj + 1]) / dx +
+         (v[(long)(ci + 1) * WV + cj + 2] - v[(long)(ci + 1) * WV + cj + 1]) / dy;
+}
+
+__global__ void k_divergence(const double* __restrict__ u, const double* __restrict__ v, int nx,
+                             int ny, double dx, double dy, double* __restrict__ out) {
+  const long n = (long)nx * ny;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / ny), j = (int)(c % ny);
+    out[c] = cell_div(u, v, i, j, ny, dx, dy);
+  }
+}
+
+// Poisson right-hand side b = div/dt (+ Dirichlet term), zero on non-solvable
+// rows, with the fluid sum for the compatibility mean
+// (pycfd/core/solver.py:659-661, pycfd/core/pressure.py:300-308).
+// rhs_in != nullptr: take a given right-hand side instead of the divergence.
+__global__ void k_div_rhs(const double* __restrict__ u, const double* __restrict__ v,
+                          const double* __restrict__ rhs_in, const uint8_t* __restrict__ flags,
+                          Geo g, const double* __restrict__ S, double* __restrict__ b,
+                          RedBuf rb, double* __restrict__ Sout) {
+  const long n = (long)g.nx * g.ny;
+  const double dt = S[S_DT];
+  double acc[1] = {0.0};
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+    const uint8_t f = flags[c];
+    double val = 0.0;
+    if (f & F_SOLV) {
+      const double r = rhs_in ? rhs_in[c] : cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt;
+      val = r * 1.0 + fine_bc(f, i, j, g);
+      acc[0] += val;
+    }
+    b[c] = val;
+  }
+  grid_reduce<1>(acc, rb, [&](double* t) { Sout[S_MEAN_B] = g.n_fluid ? t[0] / g.n_fluid : 0.0; });
+}
+
+// Ghosted pressure at a face-adjacent ghost or interior position from the
+// normalised interior solution x (pycfd/core/boundary.py:166-169, :293-303,
+// :412-420).  Only non-corner ghosts are formed here.
+__device__ __forceinline__ double p_at(const double* x, int i, int j, const Geo& g) {
+  const int nx = g.nx, ny = g.ny;
+  if (i == 0) {
+    if (g.periodic_x) return x[(long)(nx - 1) * ny + (j - 1)];
+    const double in = x[(long)(j - 1)];
+    return g.dir_w ? 2.0 * g.pref_w - in : in;
+  }
+  if (i == nx + 1) {
+    if (g.periodic_x) return x[(long)(j - 1)];
+    const double in = x[(long)(nx - 1) * ny + (j - 1)];
+    return g.dir_e ? 2.0 * g.pref_e - in : in;
+  }
+  if (j == 0) {
+    if (g.periodic_y) return x[(long)(i - 1) * ny + ny - 1];
+    const double in = x[(long)(i - 1) * ny];
+    return g.dir_s ? 2.0 * g.pref_s - in : in;
+  }
+  if (j == ny + 1) {
+    if (g.periodic_y) return x[(long)(i - 1) * ny];
+    const double in = x[(long)(i - 1) * ny + ny - 1];
+    return g.dir_n ? 2.0 * g.pref_n - in : in;
+  }
+  return x[(long)(i - 1) * ny + (j - 1)];
+}
+
+// Velocity correction u -= dt*(p[m]-p[m-1])/dx on exactly the solvable faces
+// (pycfd/core/solver.py:665-682), plus the ghosted pressure output.  The last
+// block fills the pressure ghost layer wall by wall in the reference's order
+// (so the corner values agree too); all other blocks update faces and copy
+// the interior.  dt_override < 0 reads dt from the device scalars.
+__global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
+                          double* __restrict__ p, const double* __restrict__ x, Geo g,
+                          const double* __restrict__ S, double dt_override,
+                          const int* __restrict__ bc_kind) {
+  const int nx = g.nx, ny = g.ny;
+  const double dt = dt_override > 0.0 ? dt_override : S[S_DT];
+  if (blockIdx.x == gridDim.x - 1) {
+    // The other blocks copy the interior.  This block rebuilds the ghost ring
+    // from zero (the reference fills a fresh zero array) wall by wall.
+    const long WP = ny + 2;
+    for (int k = threadIdx.x; k < 2 * (nx + 2) + 2 * ny; k += blockDim.x) {
+      long idx;
+      if (k < ny + 2) idx = k;                                         // row 0
+      else if (k < 2 * (ny + 2)) idx = (long)(nx + 1) * WP + (k - (ny + 2));  // row nx+1
+      else if (k < 2 * (ny + 2) + nx) idx = (long)(k - 2 * (ny + 2) + 1) * WP;  // col 0
+      else idx = (long)(k - 2 * (ny + 2) - nx + 1) * WP + ny + 1;            // col ny+1
+      p[idx] = 0.0;
+    }
+    __syncthreads();
+    for (int w = 0; w < 4; ++w) {
+      const int kind = bc_kind[w];
+      if (kind == BC_PERIODIC) continue;
+      const int axis = w < 2 ? 0 : 1;
+      const int ghost = (w == W_LEFT || w == W_BOTTOM) ? 0 : (axis == 0 ? nx + 1 : ny + 1);
+      const int inner = (w == W_LEFT || w == W_BOTTOM) ? 1 : (axis == 0 ? nx : ny);
+      const double pref = w == W_LEFT ? g.pref_w : w == W_RIGHT ? g.pref_e : w == W_BOTTOM ? g.pref_s : g.pref_n;
+      const int len = axis == 0 ? ny + 2 : nx + 2;
+      for (int k = threadIdx.x; k < len; k += blockDim.x) {
+        // interior value of the line (may itself be a ghost set earlier: read p)
+        const int ii = axis == 0 ? inner : k, jj = axis == 0 ? k : inner;
+        double in;
+        if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) in = x[(long)(ii - 1) * ny + (jj - 1)];
+        else in = p[(long)ii * WP + jj];
+        const double val = (kind == BC_PRESSURE_OUTLET) ? 2.0 * pref - in : in;
+        const int gi = axis == 0 ? ghost : k, gj = axis == 0 ? k : ghost;
+        p[(long)gi * WP + gj] = val;
+      }
+      __syncthreads();
+    }
+    if (g.periodic_x) {
+      for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
+        const double a = (k >= 1 && k <= ny) ? x[(long)(nx - 1) * ny + k - 1] : p[(long)nx * WP + k];
+        p[k] = a;
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
+        const double a = (k >= 1 && k <= ny) ? x[(long)(k - 1)] : p[WP + k];
+        p[(long)(nx + 1) * WP + k] = a;
+      }
+      __syncthreads();
+    }
+    if (g.periodic_y) {
+      for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
+        const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny + ny - 1] : p[(long)k * WP + ny];
+        p[(long)k * WP] = a;
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
+        const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny] : p[(long)k * WP + 1];
+        p[(long)k * WP + ny + 1] = a;
+      }
+    }
+    return;
+  }
+  const long nthreads = (long)(gridDim.x - 1) * blockDim.x;
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  // interior copy of p
+  const long ncell = (long)nx * ny;
+  for (long c = tid; c < ncell; c += nthreads) {
+    const int i = (int)(c / ny), j = (int)(c % ny);
+    p[(long)(i + 1) * (ny + 2) + j + 1] = x[c];
+  }
+  // u faces [u_lo, u_hi) x [1, ny]
+  const long nu_f = (long)(g.u_hi - g.u_lo) * ny;
+  for (long c = tid; c < nu_f; c += nthreads) {
+    const int m = g.u_lo + (int)(c / ny), j = 1 + (int)(c % ny);
+    const long k = (long)m * (ny + 2) + j;
+    u[k] = u[k] - dt * (p_at(x, m, j, g) - p_at(x, m - 1, j, g)) / g.dx;
+  }
+  const long nv_f = (long)nx * (g.v_hi - g.v_lo);
+  const int vw = g.v_hi - g.v_lo;
+  for (long c = tid; c < nv_f; c += nthreads) {
+    const int i = 1 + (int)(c / vw), n = g.v_lo + (int)(c % vw);
+    const long k = (long)i * (ny + 3) + n;
+    v[k] = v[k] - dt * (p_at(x, i, n, g) - p_at(x, i, n - 1, g)) / g.dy;
+  }
+}
+
+// out = ca*a + cb*b over whole arrays (pycfd/core/solver.py:705-721).
+__global__ void k_combine(const double* __restrict__ a, const double* __restrict__ b, double ca,
+                          double cb, double* __restrict__ out, long n) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+    out[k] = ca * a[k] + cb * b[k];
+}
+
+// Field statistics: max|u|, max|v| (physical faces), max|du|, max|dv|,
+// max|div| (fluid), kinetic energy sum, max|vorticity|, non-finite count.
+__global__ void k_field_stats(const double* __restrict__ u, const double* __restrict__ v,
+                              const double* __restrict__ p, const double* __restrict__ up,
+                              const double* __restrict__ vp, const uint8_t* __restrict__ solid,
+                              Geo g, RedBuf rb, double* __restrict__ Sout) {
+  const int nx = g.nx, ny = g.ny;
+  const long W = ny + 2, WV = ny + 3;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // max,max,max,max,max,sum,max,sum
+  const long nt = (long)gridDim.x * blockDim.x;
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nu_all = (long)(nx + 3) * W, nv_all = (long)(nx + 2) * WV, np_all = (long)(nx + 2) * (ny + 2);
+  for (long k = tid; k < nu_all; k += nt) {
+    const int i = (int)(k / W), j = (int)(k % W);
+    const double a = u[k];
+    if (!isfinite(a)) acc[7] += 1.0;
+    if (i >= 1 && i <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
+    if (up) acc[2] = fmax(acc[2], fabs(a - up[k]));
+  }
+  for (long k = tid; k < nv_all; k += nt) {
+    const int i = (int)(k / WV), j = (int)(k % WV);
+    const double a = v[k];
+    if (!isfinite(a)) acc[7] += 1.0;
+    if (i >= 1 && i <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
+    if (vp) acc[3] = fmax(acc[3], fabs(a - vp[k]));
+  }
+  if (p)
+    for (long k = tid; k < np_all; k += nt)
+      if (!isfinite(p[k])) acc[7] += 1.0;
+  const long ncell = (long)nx * ny;
+  for (long c = tid; c < ncell; c += nt) {
+    const int i = (int)(c / ny), j = (int)(c % ny);
+    const bool sol = solid && solid[c];
+    if (!sol) acc[4] = fmax(acc[4], fabs(cell_div(u, v, i, j, ny, g.dx, g.dy)));
+    const double uc = 0.5 * (u[(long)(i + 1) * W + j + 1] + u[(long)(i + 2) * W + j + 1]);
+    const double vc = 0.5 * (v[(long)(i + 1) * WV + j + 1] + v[(long)(i + 1) * WV + j + 2]);
+    if (!sol) acc[5] += 0.5 * (uc * uc + vc * vc);
+    // vorticity at the four corners of the cell (pycfd/analysis/postprocess.py:21-40)
+    double w4 = 0.0;
+    for (int di = 0; di < 2; ++di)
+      for (int dj = 0; dj < 2; ++dj) {
+        const int a = i + di, bb = j + dj;  // corner index (0..nx, 0..ny)
+        const double dvdx = (v[(long)(a + 1) * WV + bb + 1] - v[(long)a * WV + bb + 1]) / g.dx;
+        const double dudy = (u[(long)(a + 1) * W + bb + 1] - u[(long)(a + 1) * W + bb]) / g.dy;
+        w4 += dvdx - dudy;
+      }
+    acc[6] = fmax(acc[6], fabs(0.25 * w4));
+  }
+  grid_reduce<8, 0x5Fu>(acc, rb, [&](double* t) {
+    for (int k = 0; k < 8; ++k) Sout[S_STAT0 + k] = t[k];
+  });
+}
+
+}  // namespace pcfd

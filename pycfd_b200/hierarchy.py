@@ -1,0 +1,194 @@
+"""Host set-up of the Poisson operator and its multigrid hierarchy.
+
+Runs once per solver, before anything is uploaded.  The fine operator is
+assembled in CSR (the device applies it matrix-free; the CSR form seeds the
+Galerkin products), then the smoothed-aggregation hierarchy of
+``pycfd/core/multigrid.py`` is built level by level with the same rules --
+seeded power-iteration weight, anisotropy-driven coarsening, 2x2 blocks with
+singleton leftovers, one damped-Jacobi pass over the 0/1 prolongator,
+``A_c = P^T A P`` with identity on dropped aggregates, stop at <= 96 unknowns
+or when a level shrinks by less than 1.3x -- and handed to the library as CSR
+blocks plus the dense pseudo-inverse of the coarsest operator.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.sparse as sp
+
+COARSEST_UNKNOWNS = 96
+MAX_LEVELS = 20
+MIN_COARSENING_RATIO = 1.3
+JACOBI_WEIGHT_FACTOR = 4.0 / 3.0
+POWER_ITERATIONS = 12
+ANISOTROPY_THRESHOLD = 2.0
+
+
+@dataclass
+class FineOperator:
+    """The assembled fine Poisson operator (``pycfd/core/pressure.py:69-94``)."""
+
+    A: sp.csr_matrix
+    shape: tuple
+    fluid: np.ndarray        # solvable rows, flat
+    singular: bool
+    pin: int
+    bc_rhs: np.ndarray
+
+
+def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None) -> FineOperator:
+    """5-point operator over the projected face set (``pycfd/core/pressure.py:110-270``).
+
+    Couplings are gathered per face direction with index arithmetic; the
+    diagonal accumulates the directions in the order left, right, bottom, top,
+    Dirichlet walls adding ``-2/h^2`` in place, which reproduces the reference's
+    matrix exactly.
+    """
+    n = nx * ny
+    fluid = np.ones((nx, ny), bool) if solid is None else ~np.asarray(solid, bool)
+    dirichlet = dict(dirichlet or {})
+    ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    cid = ii * ny + jj
+    diag = np.zeros((nx, ny))
+    bc = np.zeros((nx, ny))
+    rows, cols, vals = [], [], []
+    cx, cy = 1.0 / (dx * dx), 1.0 / (dy * dy)
+    for wall, di, dj, c, per in (("left", -1, 0, cx, periodic_x), ("right", 1, 0, cx, periodic_x),
+                                 ("bottom", 0, -1, cy, periodic_y), ("top", 0, 1, cy, periodic_y)):
+        ni, nj = ii + di, jj + dj
+        inside = (ni >= 0) & (ni < nx) & (nj >= 0) & (nj < ny)
+        if per:
+            inside[:] = True
+        ni, nj = ni % nx, nj % ny
+        coupled = fluid & inside & fluid[ni, nj]
+        rows.append(cid[coupled])
+        cols.append((ni * ny + nj)[coupled])
+        vals.append(np.full(int(coupled.sum()), c))
+        diag -= c * coupled
+        if wall in dirichlet:
+            on_wall = fluid & ~inside
+            diag -= 2.0 * c * on_wall
+            bc -= 2.0 * c * dirichlet[wall] * on_wall
+    solvable = fluid & (diag != 0.0)
+    diag = np.where(solvable, diag, 1.0)
+    bc = np.where(solvable, bc, 0.0)
+    rows.append(cid.ravel())
+    cols.append(cid.ravel())
+    vals.append(diag.ravel())
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n, n))
+    A.sum_duplicates()
+    flat = solvable.ravel()
+    pin = int(np.argmax(flat)) if flat.any() else 0
+    return FineOperator(A, (nx, ny), flat.copy(), not dirichlet, pin, bc.ravel())
+
+
+@dataclass
+class MgLevelHost:
+    n: int
+    shape: tuple
+    weight: float
+    weighted_dinv: np.ndarray
+    active: np.ndarray
+    A: sp.csr_matrix
+    P: sp.csr_matrix | None = None
+    arrays: list = field(default_factory=list)   # keeps ctypes-backed buffers alive
+
+
+def _rho(A, dinv):
+    """Power-iteration estimate of rho(D^-1 A), x1.05 (``pycfd/core/multigrid.py:129-157``)."""
+    n = A.shape[0]
+    if n == 0:
+        return 1.0
+    v = np.random.default_rng(0).standard_normal(n)
+    nv = float(np.linalg.norm(v))
+    if nv == 0.0:
+        return 1.0
+    v = v / nv
+    est = 1.0
+    for _ in range(POWER_ITERATIONS):
+        w = dinv * (A @ v)
+        nw = float(np.linalg.norm(w))
+        if nw == 0.0:
+            return est
+        est = nw
+        v = w / nw
+    return est * 1.05
+
+
+def _factors(A, shape):
+    """Axis coarsening factors from the mean band strengths (``multigrid.py:167-204``)."""
+    nx, ny = shape
+    if nx < 2 and ny < 2:
+        return 1, 1
+    band = lambda k: float(np.abs(A.diagonal(k)).mean()) if k < A.shape[0] and A.diagonal(k).size else 0.0
+    sx, sy = band(ny), band(1)
+    if nx >= 2 and sx > ANISOTROPY_THRESHOLD * sy:
+        return 2, 1
+    if ny >= 2 and sy > ANISOTROPY_THRESHOLD * sx:
+        return 1, 2
+    return (2 if nx >= 2 else 1), (2 if ny >= 2 else 1)
+
+
+def _level(A, shape, active, P):
+    d = A.diagonal()
+    dinv = 1.0 / np.where(d == 0.0, 1.0, d)
+    rho = _rho(A, dinv)
+    w = JACOBI_WEIGHT_FACTOR / rho if rho > 0.0 else 1.0
+    return MgLevelHost(A.shape[0], tuple(shape), w, w * dinv, active, A, P), dinv
+
+
+def build_hierarchy(op: FineOperator):
+    """Levels (finest first) and the coarsest pseudo-inverse (row-major)."""
+    lv, dinv = _level(op.A, op.shape, op.fluid.copy(), None)
+    levels = [lv]
+    while len(levels) < MAX_LEVELS and lv.n > COARSEST_UNKNOWNS:
+        fx, fy = _factors(lv.A, lv.shape)
+        nx, ny = lv.shape
+        ncx, ncy = max(-(-nx // fx), 1), max(-(-ny // fy), 1)
+        nc = ncx * ncy
+        if nc == 0 or lv.n < MIN_COARSENING_RATIO * nc:
+            break
+        ii, jj = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+        agg = ((ii // fx) * ncy + (jj // fy)).ravel()
+        rows = np.flatnonzero(lv.active)
+        T = sp.csr_matrix((np.ones(rows.size), (rows, agg[rows])), shape=(lv.n, nc))
+        cact = np.zeros(nc, bool)
+        cact[agg[rows]] = True
+        P = (T - sp.diags(lv.weight * dinv) @ (lv.A @ T)).tocsr()
+        Ac = sp.csr_matrix(P.T @ lv.A @ P)
+        if not cact.all():
+            Ac = (Ac + sp.diags((~cact).astype(float))).tocsr()
+        Ac.sum_duplicates()
+        lv, dinv = _level(Ac, (ncx, ncy), cact, P)
+        levels.append(lv)
+    return levels, coarsest_pseudo_inverse(levels[-1], op.singular)
+
+
+def coarsest_pseudo_inverse(level: MgLevelHost, singular: bool) -> np.ndarray:
+    """Dense matrix of the coarsest solve (``pycfd/core/multigrid.py:514-543``).
+
+    The reference pins one unknown, factorises, and removes the mean before and
+    after; that map is linear in the right-hand side, so it is materialised
+    column by column here and applied on the device as one small mat-vec.
+    """
+    n = level.n
+    act = level.active
+    M = level.A.toarray()
+    pin = int(np.argmax(act)) if act.any() else 0
+    if singular and n:
+        M[pin, :] = 0.0
+        M[pin, pin] = 1.0
+    Minv = np.linalg.inv(M)
+    E = np.eye(n)
+    if singular:
+        E[~act, :] = 0.0
+        E[act, :] -= E[act, :].mean(axis=0)
+        E[pin, :] = 0.0
+    X = Minv @ E
+    X[~act, :] = 0.0
+    if singular and act.any():
+        X[act, :] -= X[act, :].mean(axis=0)
+    return np.ascontiguousarray(X)

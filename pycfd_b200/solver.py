@@ -1,0 +1,435 @@
+"""GPU projection solver with the reference's ``ProjectionSolver`` surface.
+
+Construction does the host set-up the reference does (face ranges, face
+solid flags, Poisson assembly, multigrid hierarchy) and hands it to the native
+library; every per-step operation -- momentum RHS, predictor, boundary passes,
+mask, divergence, Poisson solve, correction, stage combination -- runs as
+sm_100a kernels on the current CUDA stream.  Public methods and attributes
+follow ``pycfd/core/solver.py:82-756``; arrays are float64 CUDA tensors in the
+reference's ghosted layout.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .config import (AdvectionScheme, BCKind, PressureSolver, SimulationConfig, SolverType,
+                     TimeScheme, WALLS)
+from .fields import FlowField
+from .hierarchy import assemble, build_hierarchy
+from .mesh import StructuredMesh
+
+
+@dataclass
+class GpuOptions:
+    """Knobs of the GPU path that the reference configuration has no field for.
+
+    precision: ``"fp64"`` (drop-in) or ``"mixed"`` (FP32 multigrid-preconditioned
+    CG inside FP64 iterative refinement; MG-PCG only).
+    inner_tol: relative tolerance of each FP32 inner solve of the mixed form.
+    """
+
+    precision: str = "fp64"
+    inner_tol: float = 1e-4
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("pycfd_b200 needs a CUDA device; there is no CPU fallback")
+    return torch
+
+
+def _stream():
+    torch = _torch()
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def face_solid_mask(solid, lo, hi, axis, periodic):
+    """Faces in ``[lo, hi)`` touching a solid cell (``pycfd/core/solver.py:62-79``)."""
+    m = np.arange(lo, hi)
+    if periodic:
+        n = solid.shape[axis]
+        return np.take(solid, (m - 2) % n, axis=axis) | np.take(solid, (m - 1) % n, axis=axis)
+    pad = [(0, 0), (0, 0)]
+    pad[axis] = (1, 1)
+    padded = np.pad(solid, pad, constant_values=False)
+    return np.take(padded, m - 1, axis=axis) | np.take(padded, m, axis=axis)
+
+
+class BoundaryInfo:
+    """Host view of the wall conditions (``pycfd/core/boundary.py:359-504``)."""
+
+    def __init__(self, boundary_config, mesh):
+        self.mesh = mesh
+        self.specs = {w: boundary_config[w] for w in WALLS}
+        self.kinds = {w: BCKind(self.specs[w].kind) for w in WALLS}
+        self.periodic_x = self.kinds["left"] is BCKind.PERIODIC
+        self.periodic_y = self.kinds["bottom"] is BCKind.PERIODIC
+
+    def pressure_boundary_kinds(self):
+        return {w: ("periodic" if k is BCKind.PERIODIC else
+                    "dirichlet" if k is BCKind.PRESSURE_OUTLET else "neumann")
+                for w, k in self.kinds.items()}
+
+    def dirichlet_pressure(self):
+        return {w: self.specs[w].p_ref for w in WALLS
+                if self.kinds[w] is BCKind.PRESSURE_OUTLET}
+
+    def profile(self, wall):
+        """Normal-face line of a parabolic inlet (``pycfd/core/boundary.py:203-215``)."""
+        spec = self.specs[wall]
+        outward = -1.0 if wall in ("left", "bottom") else 1.0
+        speed = -outward * spec.velocity
+        m = self.mesh
+        if wall in ("left", "right"):
+            coord, extent, length = m.yc, m.ly, m.ny + 2
+        else:
+            coord, extent, length = m.xc, m.lx, m.nx + 2
+        prof = 4.0 * coord * (extent - coord) / extent ** 2
+        full = np.zeros(length)
+        full[1:1 + coord.size] = speed * prof
+        return full
+
+
+class GpuPoissonSolver:
+    """``PoissonSolverBase`` surface over the native solve (``pycfd/core/pressure.py:273-327``)."""
+
+    warm_startable = True
+
+    def __init__(self, owner: "ProjectionSolver", kind: PressureSolver):
+        self._owner = owner
+        self.name = kind.value
+        self.system = owner.poisson
+        self.tol = owner.config.poisson_tol
+        self.maxiter = owner.config.poisson_maxiter
+        self.last_iterations = 0
+        self.last_residual = 0.0
+        self.hierarchy_levels = owner._levels
+
+    def solve(self, rhs, p0=None):
+        """Solve ``lap(p) = rhs`` and return ``p`` with shape ``(nx, ny)`` (device tensor)."""
+        torch = _torch()
+        o = self._owner
+        nx, ny = o.mesh.shape
+        rhs_t = o._dev(rhs).reshape(nx, ny).contiguous()
+        p0_t = None if p0 is None else o._dev(p0).reshape(nx, ny).contiguous()
+        out = torch.empty((nx, ny), dtype=torch.float64, device=rhs_t.device)
+        _lib.check(o._L.pycfd_poisson_solve(o._h, _lib.ptr(rhs_t), _lib.ptr(p0_t),
+                                            _lib.ptr(out), _stream()))
+        o._read_stats(raise_on_error=True)
+        return out
+
+
+class ProjectionSolver:
+    """Fractional-step solver whose hot path runs on one B200 (see module doc)."""
+
+    def __init__(self, config: SimulationConfig, mesh: StructuredMesh | None = None,
+                 obstacle=None, bodies=None, options: GpuOptions | None = None) -> None:
+        if SolverType(config.solver_type) is SolverType.SIMPLE:
+            raise NotImplementedError(
+                "solver_type='simple' is reserved for a future SIMPLE implementation; only "
+                "'projection' is available. Set solver_type='projection'.")
+        if config.use_les:
+            raise NotImplementedError("the GPU projection path is laminar; use_les=True is not provided")
+        kind = PressureSolver(config.pressure_solver)
+        if kind is PressureSolver.DIRECT:
+            raise NotImplementedError(
+                "pressure_solver='direct' (sparse LU) is not provided on the GPU path; use "
+                "'mgcg', 'cg', 'multigrid', 'sor' or 'jacobi'")
+        self.options = options or GpuOptions()
+        if self.options.precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {self.options.precision!r}")
+        if self.options.precision == "mixed" and kind is not PressureSolver.MGCG:
+            raise NotImplementedError("the mixed-precision form is provided for pressure_solver='mgcg'")
+        self._L = _lib.load()
+        _torch()
+        self.config = config
+        self.mesh = mesh if mesh is not None else StructuredMesh.from_config(config)
+        self.metrics = self.mesh.metrics
+        self.nu = config.nu
+        self.boundaries = BoundaryInfo(config.boundary_config, self.mesh)
+        self.periodic_x, self.periodic_y = self.boundaries.periodic_x, self.boundaries.periodic_y
+        nx, ny = self.mesh.shape
+        if obstacle is None:
+            self.solid = np.zeros((nx, ny), dtype=bool)
+        else:
+            self.solid = np.asarray(getattr(obstacle, "mask", obstacle), dtype=bool)
+            if self.solid.shape != (nx, ny):
+                raise ValueError(f"obstacle mask must have shape {(nx, ny)}, got {self.solid.shape}")
+        self.has_obstacle = bool(self.solid.any())
+        self.body_masks = ()
+        if bodies is not None and len(bodies) > 1:
+            if len(bodies) > _lib.MAX_BODIES:
+                raise ValueError(f"at most {_lib.MAX_BODIES} bodies report separate forces")
+            self.body_masks = tuple(np.asarray(b, dtype=bool) for b in bodies)
+            for k, b in enumerate(self.body_masks):
+                if b.shape != (nx, ny):
+                    raise ValueError(f"body {k} mask must have shape {(nx, ny)}, got {b.shape}")
+        self._build_slices()
+        self.dirichlet_pressure = self.boundaries.dirichlet_pressure()
+        self.poisson = assemble(nx, ny, self.mesh.dx, self.mesh.dy, self.periodic_x,
+                                self.periodic_y, self.solid if self.has_obstacle else None,
+                                self.dirichlet_pressure or None)
+        self._levels, self._cinv = (None, None)
+        if kind in (PressureSolver.MULTIGRID, PressureSolver.MGCG):
+            self._levels, self._cinv = build_hierarchy(self.poisson)
+        self._create_native(kind)
+        self.pressure_solver = GpuPoissonSolver(self, kind)
+        self.turbulence = None
+        self.body_force_reaction = (0.0, 0.0)
+        self.body_force_reactions = tuple((0.0, 0.0) for _ in self.body_masks)
+        self._blend = 0.0
+        self.last_stats = None
+
+    # ------------------------------------------------------------------ #
+    def _build_slices(self) -> None:
+        """Solvable face ranges and face solid flags (``pycfd/core/solver.py:235-296``)."""
+        nx, ny = self.mesh.shape
+        k = self.boundaries.kinds
+        out = BCKind.PRESSURE_OUTLET
+        u_lo = 1 if (self.periodic_x or k["left"] is out) else 2
+        u_hi = nx + 2 if (k["right"] is out and not self.periodic_x) else nx + 1
+        v_lo = 1 if (self.periodic_y or k["bottom"] is out) else 2
+        v_hi = ny + 2 if (k["top"] is out and not self.periodic_y) else ny + 1
+        self.u_upd = (slice(u_lo, u_hi), slice(1, ny + 1))
+        self.v_upd = (slice(1, nx + 1), slice(v_lo, v_hi))
+        self.u_rhs_sel = slice(u_lo - 1, u_hi - 1)
+        self.v_rhs_sel = slice(v_lo - 1, v_hi - 1)
+        if self.has_obstacle:
+            self.u_face_solid = face_solid_mask(self.solid, u_lo, u_hi, 0, self.periodic_x)
+            self.v_face_solid = face_solid_mask(self.solid, v_lo, v_hi, 1, self.periodic_y)
+        else:
+            self.u_face_solid = self.v_face_solid = None
+
+    def _create_native(self, kind: PressureSolver) -> None:
+        cfg, mesh = self.config, self.mesh
+        nx, ny = mesh.shape
+        d = _lib.SolverDesc()
+        d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, mesh.dx, mesh.dy, self.nu
+        d.body_fx, d.body_fy = cfg.body_force
+        keep = []
+        for w, wall in enumerate(WALLS):
+            spec = self.boundaries.specs[wall]
+            d.bc_kind[w] = _lib.BC_CODES[self.boundaries.kinds[wall].value]
+            d.bc_velocity[w] = spec.velocity
+            d.bc_p_ref[w] = spec.p_ref
+            if self.boundaries.kinds[wall] is BCKind.INLET and spec.profile == "parabolic":
+                prof = self.boundaries.profile(wall)
+                keep.append(prof)
+                d.bc_profile[w] = _lib.cast(prof, C.c_double)
+            else:
+                d.bc_profile[w] = _lib.cast(None, C.c_double)
+        solid_u8 = np.ascontiguousarray(self.solid.astype(np.uint8))
+        keep.append(solid_u8)
+        d.solid = _lib.cast(solid_u8 if self.has_obstacle else None, C.c_uint8)
+        if self.body_masks:
+            bid = np.zeros((nx, ny), np.uint8)
+            for kb, b in enumerate(self.body_masks):
+                bid[b] = kb + 1
+            keep.append(bid)
+            d.body_id = _lib.cast(bid, C.c_uint8)
+            d.n_bodies = len(self.body_masks)
+        else:
+            d.body_id = _lib.cast(None, C.c_uint8)
+            d.n_bodies = 0
+        d.solver_kind = _lib.SOLVER_CODES[kind.value]
+        d.tol = cfg.poisson_tol
+        d.maxiter = cfg.poisson_maxiter
+        d.sor_omega = cfg.sor_omega
+        d.mg_sweeps = cfg.mg_sweeps
+        d.time_scheme = _lib.SCHEME_CODES[TimeScheme(cfg.time_scheme).value]
+        d.precision = 1 if self.options.precision == "mixed" else 0
+        d.inner_tol = self.options.inner_tol
+        if self._levels is not None:
+            arr = (_lib.MgLevel * len(self._levels))()
+            for l, lv in enumerate(self._levels):
+                e = arr[l]
+                e.n, e.shape_x, e.shape_y, e.weight = lv.n, lv.shape[0], lv.shape[1], lv.weight
+                wd = np.ascontiguousarray(lv.weighted_dinv, dtype=np.float64)
+                act = np.ascontiguousarray(lv.active.astype(np.uint8))
+                keep += [wd, act]
+                e.weighted_dinv = _lib.cast(wd, C.c_double)
+                e.active = _lib.cast(act, C.c_uint8)
+                A = lv.A.tocsr()
+                ap = np.ascontiguousarray(A.indptr, np.int64)
+                ai = np.ascontiguousarray(A.indices, np.int32)
+                ad = np.ascontiguousarray(A.data, np.float64)
+                keep += [ap, ai, ad]
+                e.a_indptr, e.a_indices, e.a_data = (_lib.cast(ap, C.c_int64), _lib.cast(ai, C.c_int32),
+                                                     _lib.cast(ad, C.c_double))
+                if lv.P is not None:
+                    P = lv.P.tocsr()
+                    pp = np.ascontiguousarray(P.indptr, np.int64)
+                    pi = np.ascontiguousarray(P.indices, np.int32)
+                    pd = np.ascontiguousarray(P.data, np.float64)
+                    keep += [pp, pi, pd]
+                    e.p_indptr, e.p_indices, e.p_data = (_lib.cast(pp, C.c_int64),
+                                                         _lib.cast(pi, C.c_int32),
+                                                         _lib.cast(pd, C.c_double))
+                else:
+                    e.p_indptr = _lib.cast(None, C.c_int64)
+                    e.p_indices = _lib.cast(None, C.c_int32)
+                    e.p_data = _lib.cast(None, C.c_double)
+            cinv = np.ascontiguousarray(self._cinv, np.float64)
+            keep.append(cinv)
+            d.n_levels = len(self._levels)
+            d.levels = arr
+            d.coarsest_inverse = _lib.cast(cinv, C.c_double)
+        else:
+            d.n_levels = 0
+            d.levels = C.cast(C.c_void_p(0), C.POINTER(_lib.MgLevel))
+            d.coarsest_inverse = _lib.cast(None, C.c_double)
+        h = C.c_void_p()
+        _lib.check(self._L.pycfd_solver_create(C.byref(d), C.byref(h)))
+        self._h = h
+        del keep
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._L.pycfd_solver_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------------ #
+    def _dev(self, a):
+        torch = _torch()
+        if isinstance(a, torch.Tensor):
+            return a.to(device="cuda", dtype=torch.float64)
+        return torch.as_tensor(np.asarray(a, dtype=np.float64), device="cuda")
+
+    def _read_stats(self, raise_on_error: bool = True):
+        st = _lib.Stats()
+        _lib.check(self._L.pycfd_get_stats(self._h, C.byref(st), _stream()))
+        self.last_stats = st
+        ps = self.pressure_solver if hasattr(self, "pressure_solver") else None
+        if ps is not None:
+            ps.last_iterations = st.iterations
+            ps.last_residual = st.last_residual
+        if self.has_obstacle:
+            self.body_force_reaction = (st.fx, st.fy)
+            if self.body_masks:
+                self.body_force_reactions = tuple((st.body_fx[k], st.body_fy[k])
+                                                  for k in range(len(self.body_masks)))
+        if raise_on_error and st.status != 0:
+            kind = self.config.pressure_solver
+            raise RuntimeError(
+                f"{PressureSolver(kind).value} pressure solve failed to converge: relative "
+                f"residual {st.last_residual:.3e} after {st.iterations} iterations "
+                f"(tol {self.config.poisson_tol:.1e})")
+        return st
+
+    def _empty_state(self):
+        torch = _torch()
+        m = self.mesh
+        e = lambda s: torch.empty(s, dtype=torch.float64, device="cuda")
+        return e(m.u_shape), e(m.v_shape), e(m.p_shape)
+
+    # ------------------------------------------------------------------ #
+    def initialize(self, u_init=None, v_init=None) -> FlowField:
+        """Initial field with BCs applied and projected (``pycfd/core/solver.py:301-329``)."""
+        fields = FlowField.zeros(self.mesh)
+        if u_init is not None:
+            fields.u_phys[...] = self._dev(u_init) if not np.isscalar(u_init) else float(u_init)
+        if v_init is not None:
+            fields.v_phys[...] = self._dev(v_init) if not np.isscalar(v_init) else float(v_init)
+        _lib.check(self._L.pycfd_initialize(self._h, _lib.ptr(fields.u), _lib.ptr(fields.v),
+                                            _lib.ptr(fields.p), _stream()))
+        self._read_stats()
+        return fields
+
+    def momentum_rhs(self, u, v, blend: float = 0.0):
+        """``-A(u) + nu lap(u) + f`` as ``(nx+1, ny)`` and ``(nx, ny+1)`` tensors."""
+        torch = _torch()
+        u, v = self._dev(u).contiguous(), self._dev(v).contiguous()
+        nx, ny = self.mesh.shape
+        ru = torch.empty((nx + 1, ny), dtype=torch.float64, device="cuda")
+        rv = torch.empty((nx, ny + 1), dtype=torch.float64, device="cuda")
+        fx, fy = self.config.body_force
+        _lib.check(self._L.pycfd_momentum_rhs(_lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx,
+                                              self.mesh.dy, self.nu, float(blend), fx, fy,
+                                              _lib.ptr(ru), _lib.ptr(rv), _stream()))
+        return ru, rv
+
+    def divergence(self, u, v):
+        """Cell divergence ``(nx, ny)`` (``pycfd/core/solver.py:532-543``)."""
+        torch = _torch()
+        u, v = self._dev(u).contiguous(), self._dev(v).contiguous()
+        nx, ny = self.mesh.shape
+        out = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+        _lib.check(self._L.pycfd_divergence(_lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx,
+                                            self.mesh.dy, _lib.ptr(out), _stream()))
+        return out
+
+    def field_stats(self, fields: FlowField, previous: FlowField | None = None):
+        """One fused reduction over a state (max |u|, |v|, |du|, |div|, KE, finiteness)."""
+        st = _lib.FieldStats()
+        _lib.check(self._L.pycfd_reduce_fields(
+            self._h, _lib.ptr(fields.u), _lib.ptr(fields.v), _lib.ptr(fields.p),
+            _lib.ptr(previous.u if previous is not None else None),
+            _lib.ptr(previous.v if previous is not None else None), C.byref(st), _stream()))
+        return st
+
+    def max_divergence(self, fields: FlowField) -> float:
+        """Largest |div u| over fluid cells (``pycfd/core/solver.py:545-550``)."""
+        return float(self.field_stats(fields).max_div)
+
+    def project(self, u, v, dt: float):
+        """Project ``(u, v)`` in place; return the ghosted pressure (``solver.py:643-683``)."""
+        torch = _torch()
+        p = torch.empty(self.mesh.p_shape, dtype=torch.float64, device="cuda")
+        _lib.check(self._L.pycfd_project(self._h, _lib.ptr(u), _lib.ptr(v), _lib.ptr(p),
+                                         float(dt), _stream()))
+        self._read_stats()
+        return p
+
+    def substep(self, fields: FlowField, dt: float, blend: float = 0.0):
+        """One projected Euler substep; returns fresh ``(u, v, p)`` (``solver.py:612-640``)."""
+        us, vs, p = self._empty_state()
+        _lib.check(self._L.pycfd_substep(self._h, _lib.ptr(fields.u.contiguous()),
+                                         _lib.ptr(fields.v.contiguous()), _lib.ptr(us),
+                                         _lib.ptr(vs), _lib.ptr(p), float(dt), float(blend),
+                                         _stream()))
+        self._read_stats()
+        return us, vs, p
+
+    def step(self, fields: FlowField, dt: float) -> FlowField:
+        """Advance by ``dt`` with the configured scheme (``pycfd/core/solver.py:686-731``)."""
+        u, v, p = self._empty_state()
+        _lib.check(self._L.pycfd_step(self._h, _lib.ptr(fields.u.contiguous()),
+                                      _lib.ptr(fields.v.contiguous()), _lib.ptr(u), _lib.ptr(v),
+                                      _lib.ptr(p), float(dt), float(self._blend), _stream()))
+        self._read_stats()
+        return FlowField(self.mesh, u, v, p, fields.t + dt, fields.step + 1)
+
+    def step_host(self, u0: np.ndarray, v0: np.ndarray, dt: float):
+        """The same step on host arrays: copies in, steps, copies ``(u, v, p)`` out."""
+        u0 = np.ascontiguousarray(u0, np.float64)
+        v0 = np.ascontiguousarray(v0, np.float64)
+        u, v, p = (np.empty(self.mesh.u_shape), np.empty(self.mesh.v_shape),
+                   np.empty(self.mesh.p_shape))
+        _lib.check(self._L.pycfd_step_host(self._h, _lib.ptr(u0), _lib.ptr(v0), _lib.ptr(u),
+                                           _lib.ptr(v), _lib.ptr(p), float(dt), float(self._blend),
+                                           _stream()))
+        return u, v, p
+
+    # ------------------------------------------------------------------ #
+    def set_upwind_blend(self, blend: float) -> None:
+        self._blend = float(np.clip(blend, 0.0, 1.0))
+
+    def upwind_blend_for(self, fields: FlowField, dt: float) -> float:
+        """Donor-cell blend for the state (``pycfd/core/solver.py:740-756``)."""
+        if AdvectionScheme(self.config.advection_scheme) is AdvectionScheme.CENTRAL:
+            return 0.0
+        if self.config.upwind_blend is not None:
+            return self.config.upwind_blend
+        st = fields._stats if fields._stats is not None else self.field_stats(fields)
+        courant = max(st.max_u * dt / self.mesh.dx, st.max_v * dt / self.mesh.dy)
+        return float(min(1.0, 1.2 * courant))
