@@ -144,12 +144,12 @@ def run_ours(args, world, rank, local):
     from pycfd_b200.solver import GpuOptions, ProjectionSolver
     from pycfd_b200.mesh import StructuredMesh
     cfg = tgv_config()
-    opts = GpuOptions(precision=args.precision)
+    opts = GpuOptions(precision=args.precision, graphs=not args.eager)
     solver = ProjectionSolver(cfg, options=opts)
     f = solver.initialize(*tgv_init(solver.mesh))
     dt = cfg.dt
     for _ in range(args.warmup):
-        f = solver.step(f, dt)
+        f = solver.advance(f, dt)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -162,7 +162,7 @@ def run_ours(args, world, rank, local):
     for k in range(args.steps):
         flush.fill_(float(k))
         evs[k][0].record(stream)
-        f = solver.step(f, dt)
+        f = solver.advance(f, dt)
         evs[k][1].record(stream)
         iters.append(solver.last_stats.total_iterations)
     torch.cuda.synchronize()
@@ -232,6 +232,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--eager", action="store_true", help="launch kernels one by one (no CUDA graph)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -193,6 +193,13 @@ int pycfd_substep(pycfd_solver* s, const double* u, const double* v, double* us,
 int pycfd_step(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
                double* p, double dt, double blend, void* stream);
 
+/* The same step, recorded once per (u0, v0, u, v, p) address tuple into a
+ * CUDA graph whose Poisson iteration loops are device-side conditional WHILE
+ * nodes, then replayed: no host round trip inside a step.  Jacobi and SOR
+ * solves (host-checked residual cadence) run eagerly instead. */
+int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
+                     double* p, double dt, double blend, void* stream);
+
 /* The same step on HOST buffers: copies the inputs in, steps, copies u, v, p
  * back, all on `stream`, and returns after the stream has finished. */
 int pycfd_step_host(pycfd_solver* s, const double* u0_host, const double* v0_host,

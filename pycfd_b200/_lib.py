@@ -25,7 +25,7 @@ EXPORTS = (
     "pycfd_last_error", "pycfd_version", "pycfd_solver_create", "pycfd_solver_destroy",
     "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
-    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
+    "pycfd_step_graph", "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -97,6 +97,7 @@ def load(path: str = LIB_PATH):
         "pycfd_initialize": (C.c_int, [vp, vp, vp, vp, vp]),
         "pycfd_substep": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_step": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+        "pycfd_step_graph": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_step_host": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),

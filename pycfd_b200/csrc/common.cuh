@@ -75,8 +75,9 @@ __device__ __forceinline__ double warp_max(double v) {
 template <int NV, unsigned MAXMASK = 0u>
 __device__ __forceinline__ void block_reduce(double (&v)[NV]) {
   __shared__ double sm[NV][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int nw = (blockDim.x + 31) >> 5;
+  const int t = threadIdx.x + threadIdx.y * blockDim.x;
+  const int lane = t & 31, wid = t >> 5;
+  const int nw = (blockDim.x * blockDim.y + 31) >> 5;
 #pragma unroll
   for (int k = 0; k < NV; ++k) {
     v[k] = ((MAXMASK >> k) & 1u) ? warp_max(v[k]) : warp_sum(v[k]);
@@ -100,12 +101,16 @@ template <int NV, unsigned MAXMASK = 0u, class Fin>
 __device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin) {
   block_reduce<NV, MAXMASK>(v);
   __shared__ bool last;
-  if (threadIdx.x == 0) {
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+  const int bid = blockIdx.x + blockIdx.y * gridDim.x;
+  const int nblk = gridDim.x * gridDim.y;
+  if (tid == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) rb.partials[blockIdx.x * NV + k] = v[k];
+    for (int k = 0; k < NV; ++k) rb.partials[bid * NV + k] = v[k];
     __threadfence();
     unsigned t = atomicAdd(rb.counter, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == (unsigned)nblk - 1);
   }
   __syncthreads();
   if (!last) return;
@@ -113,7 +118,7 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin)
   double acc[NV];
 #pragma unroll
   for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+  for (int b = tid; b < nblk; b += nthr) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
       double p = ((volatile double*)rb.partials)[b * NV + k];
@@ -121,7 +126,7 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin)
     }
   }
   block_reduce<NV, MAXMASK>(acc);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     fin(acc);
     *rb.counter = 0u;
   }
@@ -156,23 +161,46 @@ __device__ __forceinline__ double fine_bc(uint8_t f, int i, int j, const Geo& g)
   return b;
 }
 
-// Neighbour indices across the four faces (periodic wrap applied; only read
-// where the face flag is set).
-__device__ __forceinline__ int nb_w(int i, int j, const Geo& g) { return (i > 0 ? i - 1 : g.nx - 1) * g.ny + j; }
-__device__ __forceinline__ int nb_e(int i, int j, const Geo& g) { return (i < g.nx - 1 ? i + 1 : 0) * g.ny + j; }
-__device__ __forceinline__ int nb_s(int i, int j, const Geo& g) { return i * g.ny + (j > 0 ? j - 1 : g.ny - 1); }
-__device__ __forceinline__ int nb_n(int i, int j, const Geo& g) { return i * g.ny + (j < g.ny - 1 ? j + 1 : 0); }
+// Neighbour coordinates across the four faces (periodic wrap applied; only
+// used where the face flag is set).
+__device__ __forceinline__ int wrap_w(int i, const Geo& g) { return i > 0 ? i - 1 : g.nx - 1; }
+__device__ __forceinline__ int wrap_e(int i, const Geo& g) { return i < g.nx - 1 ? i + 1 : 0; }
+__device__ __forceinline__ int wrap_s(int j, const Geo& g) { return j > 0 ? j - 1 : g.ny - 1; }
+__device__ __forceinline__ int wrap_n(int j, const Geo& g) { return j < g.ny - 1 ? j + 1 : 0; }
+__device__ __forceinline__ int nb_w(int i, int j, const Geo& g) { return wrap_w(i, g) * g.ny + j; }
+__device__ __forceinline__ int nb_e(int i, int j, const Geo& g) { return wrap_e(i, g) * g.ny + j; }
+__device__ __forceinline__ int nb_s(int i, int j, const Geo& g) { return i * g.ny + wrap_s(j, g); }
+__device__ __forceinline__ int nb_n(int i, int j, const Geo& g) { return i * g.ny + wrap_n(j, g); }
 
-// (A x)_c for the fine operator with x supplied by a functor (so neighbour
-// values can be formed on the fly).
+// (A x)_c for the fine operator; the functor x(k, i, j) supplies the value at
+// flat index k = i*ny + j (so neighbour values can be formed on the fly).
 template <class T, class X>
 __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Geo& g, X x) {
-  T acc = (T)fine_diag(f, i, j, g) * x(c);
-  if (f & F_W) acc += (T)g.cx * x(nb_w(i, j, g));
-  if (f & F_E) acc += (T)g.cx * x(nb_e(i, j, g));
-  if (f & F_S) acc += (T)g.cy * x(nb_s(i, j, g));
-  if (f & F_N) acc += (T)g.cy * x(nb_n(i, j, g));
+  T acc = (T)fine_diag(f, i, j, g) * x(c, i, j);
+  if (f & F_W) { const int a = wrap_w(i, g); acc += (T)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_E) { const int a = wrap_e(i, g); acc += (T)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_S) { const int b = wrap_s(j, g); acc += (T)g.cy * x(i * g.ny + b, i, b); }
+  if (f & F_N) { const int b = wrap_n(j, g); acc += (T)g.cy * x(i * g.ny + b, i, b); }
   return acc;
+}
+
+// Cells of the fine grid for a 2D launch (threads along y, blocks striding x):
+// no integer division anywhere in the fine-level kernels.
+#define FOR_CELLS(g)                                                                    \
+  for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < (g).nx; i += gridDim.y * blockDim.y) \
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < (g).ny; j += gridDim.x * blockDim.x)
+
+constexpr int kCellTJ = 32, kCellTI = 8;
+
+// 2D launch shape over nx x ny cells with at most kMaxRedBlocks blocks.
+inline void cell_launch(int nx, int ny, dim3* grid, dim3* block) {
+  *block = dim3(kCellTJ, kCellTI);
+  int gx = (ny + kCellTJ - 1) / kCellTJ;
+  if (gx > kMaxRedBlocks) gx = kMaxRedBlocks;
+  int gy = (nx + kCellTI - 1) / kCellTI;
+  const int cap = kMaxRedBlocks / gx > 0 ? kMaxRedBlocks / gx : 1;
+  if (gy > cap) gy = cap;
+  *grid = dim3(gx, gy);
 }
 
 inline int grid_for(long n, int threads, int max_blocks = kMaxRedBlocks) {

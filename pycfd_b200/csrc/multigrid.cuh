@@ -91,12 +91,15 @@ __global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y)
 
 // Coarsest level: x = C b with C the precomputed pseudo-inverse (pinned LU
 // followed by mean removal, pycfd/core/multigrid.py:524-543), column-major.
+// One warp per row of C (row-major), lanes over its columns.
 template <class T>
 __global__ void k_dense(const T* __restrict__ C, int n, const T* __restrict__ b, T* __restrict__ x) {
-  for (int row = threadIdx.x; row < n; row += blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (int row = threadIdx.x >> 5; row < n; row += blockDim.x >> 5) {
     double acc = 0.0;
-    for (int k = 0; k < n; ++k) acc += (double)C[(long)k * n + row] * (double)b[k];
-    x[row] = (T)acc;
+    for (int k = lane; k < n; k += 32) acc += (double)C[(long)row * n + k] * (double)b[k];
+    acc = warp_sum(acc);
+    if (lane == 0) x[row] = (T)acc;
   }
 }
 
@@ -108,14 +111,14 @@ struct BFromR {
   const T* r;
   const uint8_t* f;
   double mean;
-  __device__ __forceinline__ double operator()(long k) const {
+  __device__ __forceinline__ double operator()(int k) const {
     return (f[k] & F_SOLV) ? (double)r[k] - mean : 0.0;
   }
 };
 template <class T>
 struct BStored {
   const T* b;
-  __device__ __forceinline__ double operator()(long k) const { return (double)b[k]; }
+  __device__ __forceinline__ double operator()(int k) const { return (double)b[k]; }
 };
 
 __device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo& g, double w) {
@@ -126,17 +129,15 @@ __device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo&
 template <class T, class B>
 __global__ void k_fine_pre(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x, T* __restrict__ res) {
-  const long n = (long)g.nx * g.ny;
-  auto xv = [&](long k) -> double {
-    const int ii = (int)(k / g.ny), jj = (int)(k % g.ny);
+  auto xv = [&](int k, int ii, int jj) -> double {
     return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
   };
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
-    const double xc = xv(c);
+    const double xc = xv(c, i, j);
     x[c] = (T)xc;
-    res[c] = (T)(bf(c) - fine_apply<double>(f, i, j, (int)c, g, xv));
+    res[c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
   }
 }
 
@@ -149,14 +150,13 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
                               const T* __restrict__ x, T* __restrict__ xo,
                               const T* __restrict__ rcg, int singular, double* __restrict__ S,
                               RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
-  auto xv = [&](long k) -> double { return (double)x[k]; };
+  auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   double acc[2] = {0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
-                                  (bf(c) - fine_apply<double>(f, i, j, (int)c, g, xv)));
+                                  (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
     xo[c] = (T)xn;
     if (MODE != 0 && (f & F_SOLV)) {
       acc[0] += xn;
@@ -180,11 +180,10 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
 template <class T, class B>
 __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
                              const T* __restrict__ x, T* __restrict__ res) {
-  const long n = (long)g.nx * g.ny;
-  auto xv = [&](long k) -> double { return (double)x[k]; };
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
-    res[c] = (T)(bf(c) - fine_apply<double>(flags[c], i, j, (int)c, g, xv));
+  auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
+    res[c] = (T)(bf(c) - fine_apply<double>(flags[c], i, j, c, g, xv));
   }
 }
 
@@ -192,18 +191,19 @@ __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
 template <class T, class B>
 __global__ void k_fine_wdb(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x) {
-  const long n = (long)g.nx * g.ny;
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     x[c] = (T)(fine_wdinv(flags[c], i, j, g, w) * bf(c));
   }
 }
 
 // Materialise a fine right-hand side (single-level hierarchies only).
 template <class T, class B>
-__global__ void k_fine_store(B bf, long n, T* __restrict__ out) {
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+__global__ void k_fine_store(B bf, Geo g, T* __restrict__ out) {
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     out[c] = (T)bf(c);
+  }
 }
 
 // Fine-level sums after a single-level "cycle" (dense solve): same finisher as
@@ -212,9 +212,9 @@ template <class T, int MODE>
 __global__ void k_fine_sums(const T* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
                             const T* __restrict__ rcg, int singular, double* __restrict__ S,
                             RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   double acc[2] = {0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     if (flags[c] & F_SOLV) {
       acc[0] += (double)x[c];
       if (MODE == 1) acc[1] += (double)rcg[c] * (double)x[c];
@@ -237,10 +237,11 @@ __global__ void k_fine_sums(const T* __restrict__ x, const uint8_t* __restrict__
 template <class T>
 __global__ void k_fine_store_from_r(const T* __restrict__ r, const uint8_t* __restrict__ flags, Geo g,
                                     const double* __restrict__ S, int singular, T* __restrict__ out) {
-  const long n = (long)g.nx * g.ny;
   const double m = singular ? S[S_MEAN_R] : 0.0;
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     out[c] = (flags[c] & F_SOLV) ? (T)((double)r[c] - m) : (T)0;
+  }
 }
 
 }  // namespace pcfd

@@ -25,6 +25,16 @@ struct SolveCfg {
   int check_every;   // stationary solvers: residual cadence
 };
 
+// Loop control of a solve recorded in a CUDA graph: the finisher of the kernel
+// that decides convergence sets the WHILE node's condition (0 ends the loop).
+struct LoopCtl {
+  cudaGraphConditionalHandle handle;
+  int active;
+  __device__ __forceinline__ void set(bool keep_going) const {
+    if (active) cudaGraphSetConditional(handle, keep_going ? 1u : 0u);
+  }
+};
+
 template <class T> struct VecRef { T* p; };
 
 // ---- right-hand side and initial residual --------------------------------
@@ -34,19 +44,19 @@ template <class T> struct VecRef { T* p; };
 template <class T>
 __global__ void k_rhs_init(double* __restrict__ b, T* __restrict__ x, T* __restrict__ r,
                            const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
-                           int has_x0, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
+                           int has_x0, double* __restrict__ S, int* __restrict__ I, RedBuf rb,
+                           LoopCtl loop) {
   const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
   double acc[4] = {0, 0, 0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     double bc = b[c];
     if (f & F_SOLV) bc = bc - mean;
     else bc = 0.0;
     b[c] = bc;
     double ax = 0.0;
-    if (has_x0) ax = fine_apply<double>(f, i, j, (int)c, g, [&](long k) { return (double)x[k]; });
+    if (has_x0) ax = fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return (double)x[k]; });
     else x[c] = (T)0;
     const double rc = bc - ax;
     r[c] = (T)rc;
@@ -70,6 +80,7 @@ __global__ void k_rhs_init(double* __restrict__ b, T* __restrict__ x, T* __restr
     I[I_CONVERGED] = conv;
     I[I_DONE] = conv || cfg.maxiter <= 0;
     I[I_STATUS] = 0;
+    loop.set(!I[I_DONE]);
   });
 }
 
@@ -80,12 +91,10 @@ __global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
                         const T* __restrict__ p_old, T* __restrict__ p_new, T* __restrict__ q,
                         const uint8_t* __restrict__ flags, Geo g, double* __restrict__ S,
                         const int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   const bool first = I[I_IT] == 0;
   const double beta = first ? 0.0 : S[S_RHO] / S[S_RHO_PREV];
   const double mz = S[S_MEAN_Z];
-  auto pval = [&](long k) -> double {
-    const int ii = (int)(k / g.ny), jj = (int)(k % g.ny);
+  auto pval = [&](int k, int ii, int jj) -> double {
     const uint8_t fk = flags[k];
     double z;
     if (PC == PC_JACOBI) z = (double)r[k] / fine_diag(fk, ii, jj, g);
@@ -94,11 +103,11 @@ __global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
     return (double)(T)((double)p_old[k] * beta + z);
   };
   double acc[1] = {0.0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
-    const double pc = pval(c);
-    const double qc = fine_apply<double>(f, i, j, (int)c, g, pval);
+    const double pc = pval(c, i, j);
+    const double qc = fine_apply<double>(f, i, j, c, g, pval);
     p_new[c] = (T)pc;
     q[c] = (T)qc;
     acc[0] += pc * qc;
@@ -111,18 +120,22 @@ __global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
 
 // x += alpha p, r -= alpha q; ||r||^2, r.(r/d), sum_solvable(r); convergence
 // test of the next pass (scipy's top-of-loop ||r|| < atol), iteration count.
+// p_keep != nullptr: also store p there, so a recorded loop body always reads
+// the previous direction from the same buffer.
 template <class T, int PC>
 __global__ void k_cg_xr(T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                        const T* __restrict__ q, const uint8_t* __restrict__ flags, Geo g,
-                        SolveCfg cfg, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
+                        const T* __restrict__ q, T* __restrict__ p_keep,
+                        const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
+                        double* __restrict__ S, int* __restrict__ I, RedBuf rb, LoopCtl loop) {
   const double alpha = S[S_ALPHA];
   double acc[3] = {0, 0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
-    const double xc = (double)x[c] + alpha * (double)p[c];
+    const T pc = p[c];
+    const double xc = (double)x[c] + alpha * (double)pc;
     const double rc = (double)(T)((double)r[c] - alpha * (double)q[c]);
+    if (p_keep) p_keep[c] = pc;
     x[c] = (T)xc;
     r[c] = (T)rc;
     acc[0] += rc * rc;
@@ -140,6 +153,7 @@ __global__ void k_cg_xr(T* __restrict__ x, T* __restrict__ r, const T* __restric
     const bool conv = sqrt(t[0]) < S[S_ATOL];
     I[I_CONVERGED] = conv;
     I[I_DONE] = conv || it >= cfg.maxiter;
+    loop.set(!I[I_DONE]);
   });
 }
 
@@ -151,18 +165,17 @@ template <class T>
 __global__ void k_finish_stats(const T* __restrict__ x, const double* __restrict__ b,
                                const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                                int pcg, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   const bool zero = I[I_ZERO_RHS] != 0;
-  auto xv = [&](long k) -> double { return zero ? 0.0 : (double)x[k]; };
+  auto xv = [&](int k, int, int) -> double { return zero ? 0.0 : (double)x[k]; };
   double acc[2] = {0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     if (pcg) {
-      const double rc = b[c] - fine_apply<double>(f, i, j, (int)c, g, xv);
+      const double rc = b[c] - fine_apply<double>(f, i, j, c, g, xv);
       acc[0] += rc * rc;
     }
-    if (f & F_SOLV) acc[1] += xv(c);
+    if (f & F_SOLV) acc[1] += xv(c, i, j);
   }
   grid_reduce<2>(acc, rb, [&](double* t) {
     const double nb = sqrt(S[S_BNORM2]);
@@ -180,10 +193,10 @@ template <class T>
 __global__ void k_finish_apply(T* x, double* xo,
                                const uint8_t* __restrict__ flags, Geo g,
                                const double* __restrict__ S, const int* __restrict__ I) {
-  const long n = (long)g.nx * g.ny;
   const bool zero = I[I_ZERO_RHS] != 0;
   const double m = S[S_MEAN_X];
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const double v = (!zero && (flags[c] & F_SOLV)) ? (double)x[c] - m : 0.0;
     x[c] = (T)v;
     xo[c] = v;
@@ -198,10 +211,10 @@ __global__ void k_stationary_init(double* __restrict__ b, double* __restrict__ x
                                   const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                                   int has_x0, int project_x0, double* __restrict__ S,
                                   int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
   double acc[3] = {0, 0, 0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     const double bc = (f & F_SOLV) ? b[c] - mean : 0.0;
     b[c] = bc;
@@ -231,16 +244,15 @@ __global__ void k_jacobi_sweep(const double* __restrict__ xin, double* __restric
                                const double* __restrict__ b, const uint8_t* __restrict__ flags,
                                Geo g, double omega, int singular, double* __restrict__ S,
                                int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   const double m = S[S_MEAN_X];
-  auto xe = [&](long k) -> double { return (flags[k] & F_SOLV) ? xin[k] - m : xin[k]; };
+  auto xe = [&](int k, int, int) -> double { return (flags[k] & F_SOLV) ? xin[k] - m : xin[k]; };
   double acc[1] = {0.0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     const double d = fine_diag(f, i, j, g);
     const double dinv = 1.0 / d;
-    const double xn = xe(c) + omega * dinv * (b[c] - fine_apply<double>(f, i, j, (int)c, g, xe));
+    const double xn = xe(c, i, j) + omega * dinv * (b[c] - fine_apply<double>(f, i, j, c, g, xe));
     xout[c] = xn;
     if (f & F_SOLV) acc[0] += xn;
   }
@@ -258,25 +270,24 @@ __global__ void k_jacobi_sweep(const double* __restrict__ xin, double* __restric
 __global__ void k_sor_half(double* __restrict__ x, const double* __restrict__ b,
                            const uint8_t* __restrict__ flags, Geo g, double omega, int colour,
                            int singular, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
   const double m = S[S_MEAN_X];
   // red pass: every value is in the old frame; black pass: red neighbours are new.
-  auto xe = [&](long k) -> double {
-    const bool adj = (flags[k] & F_SOLV) && (colour == 0 || ((k / g.ny + k % g.ny) & 1) == 1);
+  auto xe = [&](int k, int ii, int jj) -> double {
+    const bool adj = (flags[k] & F_SOLV) && (colour == 0 || ((ii + jj) & 1) == 1);
     return adj ? x[k] - m : x[k];
   };
   double acc[1] = {0.0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     if (((i + j) & 1) != colour) continue;
     const uint8_t f = flags[c];
     const double d = fine_diag(f, i, j, g);
     double off = 0.0;
-    if (f & F_W) off += g.cx * xe(nb_w(i, j, g));
-    if (f & F_E) off += g.cx * xe(nb_e(i, j, g));
-    if (f & F_S) off += g.cy * xe(nb_s(i, j, g));
-    if (f & F_N) off += g.cy * xe(nb_n(i, j, g));
-    const double xn = (1.0 - omega) * xe(c) + omega * (b[c] - off) / d;
+    if (f & F_W) { const int a = wrap_w(i, g); off += g.cx * xe(a * g.ny + j, a, j); }
+    if (f & F_E) { const int a = wrap_e(i, g); off += g.cx * xe(a * g.ny + j, a, j); }
+    if (f & F_S) { const int bb = wrap_s(j, g); off += g.cy * xe(i * g.ny + bb, i, bb); }
+    if (f & F_N) { const int bb = wrap_n(j, g); off += g.cy * xe(i * g.ny + bb, i, bb); }
+    const double xn = (1.0 - omega) * xe(c, i, j) + omega * (b[c] - off) / d;
     x[c] = xn;
     if (f & F_SOLV) acc[0] += xn;
   }
@@ -300,14 +311,13 @@ __global__ void k_sor_half(double* __restrict__ x, const double* __restrict__ b,
 __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
                           const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg, int mode,
                           int count_cycle, int pending, double* __restrict__ S, int* __restrict__ I,
-                          RedBuf rb) {
-  const long n = (long)g.nx * g.ny;
+                          RedBuf rb, LoopCtl loop) {
   const double m = pending ? S[S_MEAN_X] : 0.0;
-  auto xe = [&](long k) -> double { return (flags[k] & F_SOLV) ? x[k] - m : 0.0; };
+  auto xe = [&](int k, int, int) -> double { return (flags[k] & F_SOLV) ? x[k] - m : 0.0; };
   double acc[1] = {0.0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
-    const double rc = b[c] - fine_apply<double>(flags[c], i, j, (int)c, g, xe);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
+    const double rc = b[c] - fine_apply<double>(flags[c], i, j, c, g, xe);
     acc[0] += rc * rc;
   }
   grid_reduce<1>(acc, rb, [&](double* t) {
@@ -327,16 +337,28 @@ __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
       I[I_DONE] = conv || it >= cfg.maxiter;
     }
     if (I[I_DONE] && res > cfg.tol) I[I_STATUS] = -4;
+    loop.set(!I[I_DONE]);
   });
+}
+
+// Start of a call: step parameters into the device scalar block (kernel
+// arguments, so no host synchronisation is needed) and the per-call counters.
+__global__ void k_begin(double* __restrict__ S, int* __restrict__ I, double dt, double blend) {
+  if (threadIdx.x == 0) {
+    S[S_DT] = dt;
+    S[S_BLEND] = blend;
+    I[I_TOTAL_IT] = 0;
+  }
 }
 
 // Apply a pending mean: x <- x - S[slot] on solvable rows.
 __global__ void k_apply_mean(double* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
                              const double* __restrict__ S, int slot) {
-  const long n = (long)g.nx * g.ny;
   const double m = S[slot];
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     if (flags[c] & F_SOLV) x[c] = x[c] - m;
+  }
 }
 
 }  // namespace pcfd

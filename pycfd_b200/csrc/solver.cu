@@ -118,7 +118,17 @@ struct pycfd_solver {
   float* Cf = nullptr;
   int nc = 0;
   int last_ir = 0;
+  // CUDA-graph recording of whole steps
+  bool capturing = false;
+  cudaStream_t aux = nullptr;
+  struct GraphEntry {
+    const void* key[5];
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs;
 
+  dim3 cgrid, cblock;   // 2D launch over the fine cells
   RedBuf rb() const { return RedBuf{partials, counter}; }
   SolveCfg cfg() const { return SolveCfg{tol, maxiter, singular, 0}; }
   long ncell() const { return (long)g.nx * g.ny; }
@@ -279,13 +289,13 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   // rows; the mean was left in S_MEAN_R by the kernel that produced r) into
   // level 0's b buffer; the fine kernels read it as a stored vector.
   LevelBuf<T>& B0 = lvB<T>(s->lv[0]);
-  k_fine_store_from_r<T><<<G, kRedThreads, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
+  k_fine_store_from_r<T><<<s->cgrid, s->cblock, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
   CHECK_LAUNCH();
   BStored<T> bf0{B0.b};
   if (Lv == 1) {
     k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, B0.b, z_out);
     CHECK_LAUNCH();
-    k_fine_sums<T, 1><<<G, kRedThreads, 0, stream>>>(z_out, s->flags, g, r, s->singular, s->S, s->rb());
+    k_fine_sums<T, 1><<<s->cgrid, s->cblock, 0, stream>>>(z_out, s->flags, g, r, s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     return 0;
   }
@@ -293,21 +303,21 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   // ---- down ----
   T* cur[32];
   if (sw == 1) {
-    k_fine_pre<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
+    k_fine_pre<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
     CHECK_LAUNCH();
     cur[0] = B0.xa;
   } else {
-    k_fine_wdb<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
+    k_fine_wdb<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
     CHECK_LAUNCH();
     T* a = B0.xa;
     T* bb = B0.xb;
     for (int k = 1; k < sw; ++k) {
-      k_fine_smooth<T, BStored<T>, 0><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
+      k_fine_smooth<T, BStored<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
                                                                      s->singular, s->S, s->rb());
       CHECK_LAUNCH();
       std::swap(a, bb);
     }
-    k_fine_resid<T, BStored<T>><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, a, B0.res);
+    k_fine_resid<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, a, B0.res);
     CHECK_LAUNCH();
     cur[0] = a;
   }
@@ -354,10 +364,10 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
       if (l == 0) {
         T* dst = (k == sw) ? z_out : other;
         if (k == sw)
-          k_fine_smooth<T, BStored<T>, 1><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+          k_fine_smooth<T, BStored<T>, 1><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
                                                                          s->singular, s->S, s->rb());
         else
-          k_fine_smooth<T, BStored<T>, 0><<<G, kRedThreads, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+          k_fine_smooth<T, BStored<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
                                                                          s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         other = xf;
@@ -387,7 +397,7 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   if (Lv == 1) {
     k_dense<double><<<1, 256, 0, stream>>>(s->C, s->nc, b, x);
     CHECK_LAUNCH();
-    k_fine_sums<double, 2><<<G, kRedThreads, 0, stream>>>(x, s->flags, g, nullptr, s->singular, s->S, s->rb());
+    k_fine_sums<double, 2><<<s->cgrid, s->cblock, 0, stream>>>(x, s->flags, g, nullptr, s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     return 0;
   }
@@ -395,12 +405,12 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   double* a = x;
   double* t = s->xtmp;
   for (int k = 0; k < sw; ++k) {
-    k_fine_smooth<double, BStored<double>, 0><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, a, t, nullptr,
+    k_fine_smooth<double, BStored<double>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, a, t, nullptr,
                                                                              s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     std::swap(a, t);
   }
-  k_fine_resid<double, BStored<double>><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, a, B0.res);
+  k_fine_resid<double, BStored<double>><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, a, B0.res);
   CHECK_LAUNCH();
   double* cur[32];
   cur[0] = a;
@@ -440,10 +450,10 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
       double* o = (xf == x) ? s->xtmp : x;
       for (int k = 1; k <= sw; ++k) {
         if (k == sw)
-          k_fine_smooth<double, BStored<double>, 2><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+          k_fine_smooth<double, BStored<double>, 2><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         else
-          k_fine_smooth<double, BStored<double>, 0><<<G, kRedThreads, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+          k_fine_smooth<double, BStored<double>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         std::swap(xf, o);
@@ -468,6 +478,53 @@ int read_flags(pycfd_solver* s, cudaStream_t stream) {
   return 0;
 }
 
+// ---- iteration loops -------------------------------------------------------
+// A solve's iteration loop runs either on the host (read the done flag after
+// every pass) or, while a step is being recorded into a CUDA graph, as a
+// conditional WHILE node whose body is recorded on the auxiliary stream and
+// whose condition the converging kernel sets on the device.
+struct Loop {
+  LoopCtl ctl{0, 0};
+  cudaGraph_t body = nullptr;
+};
+
+int loop_handle(pycfd_solver* s, cudaStream_t stream, Loop* L) {
+  if (!s->capturing) return 0;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, nullptr, nullptr));
+  cudaGraphConditionalHandle h;
+  CU(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  L->ctl = LoopCtl{h, 1};
+  return 0;
+}
+
+// Append the WHILE node after everything captured so far; begin recording its body on aux.
+int loop_open(pycfd_solver* s, cudaStream_t stream, Loop* L) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CU(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = L->ctl.handle;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CU(cudaGraphAddNode(&node, g, deps, nd, &np));
+  L->body = np.conditional.phGraph_out[0];
+  CU(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+  CU(cudaStreamBeginCaptureToGraph(s->aux, L->body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  return 0;
+}
+
+int loop_close(pycfd_solver* s) {
+  cudaGraph_t out = nullptr;
+  CU(cudaStreamEndCapture(s->aux, &out));
+  return 0;
+}
+
 // ---- Poisson solve on the prepared raw right-hand side s->b --------------
 // Result (normalised) in x.  has_x0: x holds the warm start on entry.
 int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
@@ -475,73 +532,101 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
   const int G = grid1(s);
   const SolveCfg cfg = s->cfg();
   const int kind = s->solver_kind;
+  const bool cap = s->capturing;
   if (kind == PCFD_SOLVER_CG || kind == PCFD_SOLVER_MGCG) {
-    k_rhs_init<double><<<G, kRedThreads, 0, stream>>>(s->b, x, s->r, s->flags, g, cfg, has_x0, s->S,
-                                                      s->I, s->rb());
+    Loop L;
+    TRY(loop_handle(s, stream, &L));
+    k_rhs_init<double><<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->r, s->flags, g, cfg, has_x0, s->S,
+                                                      s->I, s->rb(), L.ctl);
     CHECK_LAUNCH();
-    double* pc = s->pa;
-    double* po = s->pb;
-    for (;;) {
-      TRY(read_flags(s, stream));
-      if (s->hI[I_DONE]) break;
+    // one pass of the recurrence on stream `st`; p_old -> p_new
+    auto pass = [&](cudaStream_t st, double* p_old, double* p_new, double* keep) -> int {
       if (kind == PCFD_SOLVER_CG) {
-        k_cg_pq<double, PC_JACOBI><<<G, kRedThreads, 0, stream>>>(s->r, nullptr, pc, po, s->q, s->flags, g,
-                                                                  s->S, s->I, s->rb());
+        k_cg_pq<double, PC_JACOBI><<<s->cgrid, s->cblock, 0, st>>>(s->r, nullptr, p_old, p_new, s->q, s->flags,
+                                                              g, s->S, s->I, s->rb());
         CHECK_LAUNCH();
-        k_cg_xr<double, PC_JACOBI><<<G, kRedThreads, 0, stream>>>(x, s->r, po, s->q, s->flags, g, cfg, s->S,
-                                                                  s->I, s->rb());
+        k_cg_xr<double, PC_JACOBI><<<s->cgrid, s->cblock, 0, st>>>(x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+                                                              s->S, s->I, s->rb(), L.ctl);
       } else {
-        TRY(vcycle_pcg<double>(s, s->r, s->z, stream));
-        k_cg_pq<double, PC_MG><<<G, kRedThreads, 0, stream>>>(s->r, s->z, pc, po, s->q, s->flags, g, s->S,
-                                                              s->I, s->rb());
+        TRY(vcycle_pcg<double>(s, s->r, s->z, st));
+        k_cg_pq<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->r, s->z, p_old, p_new, s->q, s->flags, g,
+                                                          s->S, s->I, s->rb());
         CHECK_LAUNCH();
-        k_cg_xr<double, PC_MG><<<G, kRedThreads, 0, stream>>>(x, s->r, po, s->q, s->flags, g, cfg, s->S,
-                                                              s->I, s->rb());
+        k_cg_xr<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+                                                          s->S, s->I, s->rb(), L.ctl);
       }
       CHECK_LAUNCH();
-      std::swap(pc, po);
-    }
-    k_finish_stats<double><<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
-    CHECK_LAUNCH();
-  } else {
-    const int project_x0 = kind == PCFD_SOLVER_MULTIGRID;
-    k_stationary_init<<<G, kRedThreads, 0, stream>>>(s->b, x, s->flags, g, cfg, has_x0, project_x0, s->S,
-                                                     s->I, s->rb());
-    CHECK_LAUNCH();
-    if (kind == PCFD_SOLVER_MULTIGRID) {
-      k_apply_mean<<<G, kRedThreads, 0, stream>>>(s->b, s->flags, g, s->S, S_MEAN_B);
-      k_apply_mean<<<G, kRedThreads, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
-      CHECK_LAUNCH();
-      k_resnorm<<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb());
-      CHECK_LAUNCH();
+      return 0;
+    };
+    if (cap) {
+      TRY(loop_open(s, stream, &L));
+      TRY(pass(s->aux, s->pa, s->pb, s->pa));
+      TRY(loop_close(s));
+    } else {
+      double* pc = s->pa;
+      double* po = s->pb;
       for (;;) {
         TRY(read_flags(s, stream));
         if (s->hI[I_DONE]) break;
-        TRY(vcycle_standalone(s, s->b, x, stream));
-        k_resnorm<<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 1, 1, s->S, s->I, s->rb());
+        TRY(pass(stream, pc, po, nullptr));
+        std::swap(pc, po);
+      }
+    }
+    k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
+    CHECK_LAUNCH();
+  } else {
+    const int project_x0 = kind == PCFD_SOLVER_MULTIGRID;
+    k_stationary_init<<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->flags, g, cfg, has_x0, project_x0, s->S,
+                                                     s->I, s->rb());
+    CHECK_LAUNCH();
+    if (kind == PCFD_SOLVER_MULTIGRID) {
+      Loop L;
+      TRY(loop_handle(s, stream, &L));
+      k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(s->b, s->flags, g, s->S, S_MEAN_B);
+      k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
+      CHECK_LAUNCH();
+      k_resnorm<<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb(), L.ctl);
+      CHECK_LAUNCH();
+      auto cycle = [&](cudaStream_t st) -> int {
+        TRY(vcycle_standalone(s, s->b, x, st));
+        k_resnorm<<<s->cgrid, s->cblock, 0, st>>>(x, s->b, s->flags, g, cfg, 1, 1, 1, s->S, s->I, s->rb(), L.ctl);
         CHECK_LAUNCH();
-        k_apply_mean<<<G, kRedThreads, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
+        k_apply_mean<<<s->cgrid, s->cblock, 0, st>>>(x, s->flags, g, s->S, S_MEAN_X);
         CHECK_LAUNCH();
+        return 0;
+      };
+      if (cap) {
+        TRY(loop_open(s, stream, &L));
+        TRY(cycle(s->aux));
+        TRY(loop_close(s));
+      } else {
+        for (;;) {
+          TRY(read_flags(s, stream));
+          if (s->hI[I_DONE]) break;
+          TRY(cycle(stream));
+        }
       }
     } else {
+      if (cap) return fail(PCFD_E_UNSUPPORTED, "Jacobi/SOR solves are not recorded into graphs");
       double* cur = x;
       double* oth = s->xtmp;
       const int every = kind == PCFD_SOLVER_JACOBI ? 20 : 5;
       for (int it = 1; it <= s->maxiter; ++it) {
         if (kind == PCFD_SOLVER_JACOBI) {
-          k_jacobi_sweep<<<G, kRedThreads, 0, stream>>>(cur, oth, s->b, s->flags, g, 2.0 / 3.0, s->singular,
+          k_jacobi_sweep<<<s->cgrid, s->cblock, 0, stream>>>(cur, oth, s->b, s->flags, g, 2.0 / 3.0, s->singular,
                                                         s->S, s->I, s->rb());
           CHECK_LAUNCH();
           std::swap(cur, oth);
         } else {
-          k_sor_half<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
+          k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
                                                     s->I, s->rb());
-          k_sor_half<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
+          k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
                                                     s->I, s->rb());
           CHECK_LAUNCH();
         }
         if (it % every == 0 || it == s->maxiter) {
-          k_resnorm<<<G, kRedThreads, 0, stream>>>(cur, s->b, s->flags, g, cfg, 0, 0, 1, s->S, s->I, s->rb());
+          k_resnorm<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, cfg, 0, 0, 1, s->S, s->I, s->rb(),
+                                                   LoopCtl{0, 0});
           CHECK_LAUNCH();
           TRY(read_flags(s, stream));
           if (s->hI[I_DONE]) break;
@@ -549,21 +634,19 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
       }
       if (cur != x) CU(cudaMemcpyAsync(x, cur, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     }
-    k_finish_stats<double><<<G, kRedThreads, 0, stream>>>(x, s->b, s->flags, g, cfg, 0, s->S, s->I, s->rb());
+    k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 0, s->S, s->I, s->rb());
     CHECK_LAUNCH();
   }
-  k_finish_apply<double><<<G, kRedThreads, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
+  k_finish_apply<double><<<s->cgrid, s->cblock, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
   CHECK_LAUNCH();
   return 0;
 }
 
 int set_dt(pycfd_solver* s, double dt, double blend, cudaStream_t stream) {
-  // The step parameters live in device memory so a recorded step can replay
-  // with new values.  Written from pinned host memory, ordered on the stream.
-  CU(cudaStreamSynchronize(stream));
-  s->hS[S_DT] = dt;
-  s->hS[S_BLEND] = blend;
-  CU(cudaMemcpyAsync(s->S + S_DT, s->hS + S_DT, 2 * sizeof(double), cudaMemcpyHostToDevice, stream));
+  // Step parameters live in device memory so a recorded step replays with new
+  // values; they travel as kernel arguments, so no host synchronisation.
+  k_begin<<<1, 32, 0, stream>>>(s->S, s->I, dt, blend);
+  CHECK_LAUNCH();
   return 0;
 }
 
@@ -572,12 +655,11 @@ int set_dt(pycfd_solver* s, double dt, double blend, cudaStream_t stream) {
 int project_impl(pycfd_solver* s, double* u, double* v, double* p, double dt_override,
                  cudaStream_t stream) {
   const int G = grid1(s);
-  k_div_rhs<<<G, kRedThreads, 0, stream>>>(u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  k_div_rhs<<<s->cgrid, s->cblock, 0, stream>>>(u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   TRY(solve_prepared(s, s->x, s->has_guess, stream));
   s->has_guess = true;
-  const long nfaces = std::max<long>((long)(s->g.u_hi - s->g.u_lo) * s->g.ny, (long)s->g.nx * (s->g.v_hi - s->g.v_lo));
-  const int gc = grid_for(std::max(nfaces, s->ncell()), 256, kMaxRedBlocks) + 1;
+  const int gc = std::min(s->g.nx + 2, kMaxRedBlocks) + 1;   // rows + the ghost-ring block
   k_correct<<<gc, 256, 0, stream>>>(u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
   CHECK_LAUNCH();
   return 0;
@@ -637,6 +719,11 @@ int pycfd_version(void) { return 1; }
 
 int pycfd_solver_destroy(pycfd_solver* s) {
   if (!s) return 0;
+  for (auto& e : s->graphs) {
+    cudaGraphExecDestroy(e.exec);
+    cudaGraphDestroy(e.graph);
+  }
+  if (s->aux) cudaStreamDestroy(s->aux);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   if (s->hI) cudaFreeHost(s->hI);
@@ -720,6 +807,7 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
       flags[(long)i * ny + j] = f;
     }
   g.n_fluid = n_fluid;
+  cell_launch(nx, ny, &s->cgrid, &s->cblock);
   if (s->solver_kind == PCFD_SOLVER_SOR) {
     // red/black colouring must not couple a colour to itself (pycfd/core/pressure.py:486-496)
     bool bad = false;
@@ -870,11 +958,10 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
     s->nc = ncs;
     std::vector<double> cm((size_t)ncs * ncs);
     std::vector<float> cf((size_t)ncs * ncs);
-    for (int r0 = 0; r0 < ncs; ++r0)
-      for (int k = 0; k < ncs; ++k) {
-        cm[(size_t)k * ncs + r0] = d->coarsest_inverse[(size_t)r0 * ncs + k];
-        cf[(size_t)k * ncs + r0] = (float)d->coarsest_inverse[(size_t)r0 * ncs + k];
-      }
+    for (size_t e = 0; e < (size_t)ncs * ncs; ++e) {   // row-major, as given
+      cm[e] = d->coarsest_inverse[e];
+      cf[e] = (float)d->coarsest_inverse[e];
+    }
     if ((rc = upload(s, &s->C, cm.data(), cm.size())) || (rc = upload(s, &s->Cf, cf.data(), cf.size())))
       return bail(rc);
   }
@@ -900,7 +987,9 @@ int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double 
 int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy, double* out,
                      void* stream) {
   if (!u || !v || !out || nx < 1 || ny < 1) return fail(PCFD_E_ARG, "bad arguments");
-  k_divergence<<<grid_for((long)nx * ny, 256), 256, 0, st(stream)>>>(u, v, nx, ny, dx, dy, out);
+  dim3 cg, cb;
+  cell_launch(nx, ny, &cg, &cb);
+  k_divergence<<<cg, cb, 0, st(stream)>>>(u, v, nx, ny, dx, dy, out);
   CHECK_LAUNCH();
   return 0;
 }
@@ -918,7 +1007,7 @@ int pycfd_poisson_solve(pycfd_solver* s, const double* rhs, const double* p0, do
   cudaStream_t sm = st(stream);
   const int G = grid1(s);
   TRY(set_dt(s, 1.0, 0.0, sm));
-  k_div_rhs<<<G, kRedThreads, 0, sm>>>(nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  k_div_rhs<<<s->cgrid, s->cblock, 0, sm>>>(nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   if (p0) CU(cudaMemcpyAsync(s->x_api, p0, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
   TRY(solve_prepared(s, s->x_api, p0 != nullptr, sm));
@@ -932,7 +1021,7 @@ int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream) {
   cudaStream_t sm = st(stream);
   const int G = grid1(s);
   // mean of r over the active set, then one cycle and the projection of z
-  k_div_rhs<<<G, kRedThreads, 0, sm>>>(nullptr, nullptr, r, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  k_div_rhs<<<s->cgrid, s->cblock, 0, sm>>>(nullptr, nullptr, r, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   // k_div_rhs left the solvable sum in S_MEAN_B; the cycle reads S_MEAN_R.
   CU(cudaMemcpyAsync(s->S + S_MEAN_R, s->S + S_MEAN_B, sizeof(double), cudaMemcpyDeviceToDevice, sm));
@@ -941,7 +1030,7 @@ int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream) {
   TRY(vcycle_pcg<double>(s, r, s->z, sm));
   // z = z_raw - mean_z on solvable rows, 0 elsewhere
   CU(cudaMemcpyAsync(s->S + S_MEAN_X, s->S + S_MEAN_Z, sizeof(double), cudaMemcpyDeviceToDevice, sm));
-  k_finish_apply<double><<<G, kRedThreads, 0, sm>>>(s->z, z, s->flags, s->g, s->S, s->I);
+  k_finish_apply<double><<<s->cgrid, s->cblock, 0, sm>>>(s->z, z, s->flags, s->g, s->S, s->I);
   CHECK_LAUNCH();
   return 0;
 }
@@ -950,7 +1039,6 @@ int pycfd_project(pycfd_solver* s, double* u, double* v, double* p, double dt, v
   if (!s || !u || !v || !p || !(dt > 0)) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
   TRY(set_dt(s, dt, 0.0, sm));
-  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
   return project_impl(s, u, v, p, -1.0, sm);
 }
 
@@ -958,7 +1046,6 @@ int pycfd_initialize(pycfd_solver* s, double* u, double* v, double* p, void* str
   if (!s || !u || !v || !p) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
   TRY(set_dt(s, 1.0, 0.0, sm));
-  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
   TRY(launch_boundary(s, u, v, {OP_VEL_PRED, OP_MASS, OP_MASK_NONE, OP_WRAP_FACES}, sm));
   TRY(project_impl(s, u, v, p, -1.0, sm));
   TRY(launch_boundary(s, u, v, {OP_MASK_NONE, OP_WRAP_FACES, OP_VEL_CORR}, sm));
@@ -970,7 +1057,6 @@ int pycfd_substep(pycfd_solver* s, const double* u, const double* v, double* us,
   if (!s || !u || !v || !us || !vs || !p) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
   TRY(set_dt(s, dt, blend, sm));
-  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
   return substep_impl(s, StageIn{u, nullptr, 1.0, 0.0}, StageIn{v, nullptr, 1.0, 0.0}, us, vs, p, sm);
 }
 
@@ -980,8 +1066,50 @@ int pycfd_step(pycfd_solver* s, const double* u0, const double* v0, double* u, d
   if (u0 == u || v0 == v) return fail(PCFD_E_ARG, "step outputs must not alias its inputs");
   cudaStream_t sm = st(stream);
   TRY(set_dt(s, dt, blend, sm));
-  CU(cudaMemsetAsync(s->I + I_TOTAL_IT, 0, sizeof(int), sm));
   return step_impl(s, u0, v0, u, v, p, sm);
+}
+
+int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
+                     double* p, double dt, double blend, void* stream) {
+  if (!s || !u0 || !v0 || !u || !v || !p) return fail(PCFD_E_ARG, "bad arguments");
+  if (u0 == u || v0 == v) return fail(PCFD_E_ARG, "step outputs must not alias its inputs");
+  cudaStream_t sm = st(stream);
+  if (s->solver_kind == PCFD_SOLVER_JACOBI || s->solver_kind == PCFD_SOLVER_SOR)
+    return pycfd_step(s, u0, v0, u, v, p, dt, blend, stream);   // host-checked cadence
+  TRY(set_dt(s, dt, blend, sm));
+  const void* key[5] = {u0, v0, u, v, p};
+  pycfd_solver::GraphEntry* hit = nullptr;
+  for (auto& e : s->graphs)
+    if (!memcmp(e.key, key, sizeof key)) hit = &e;
+  if (!hit) {
+    if (!s->aux) CU(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal));
+    s->capturing = true;
+    const int rc = step_impl(s, u0, v0, u, v, p, sm);
+    s->capturing = false;
+    const cudaError_t ec = cudaStreamEndCapture(sm, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(PCFD_E_CUDA, "step capture failed: %s", cudaGetErrorString(ec));
+    cudaGraphExec_t exec = nullptr;
+    CU(cudaGraphInstantiate(&exec, graph, 0));
+    if (s->graphs.size() >= 4) {   // small cache: drop the oldest recording
+      cudaGraphExecDestroy(s->graphs.front().exec);
+      cudaGraphDestroy(s->graphs.front().graph);
+      s->graphs.erase(s->graphs.begin());
+    }
+    pycfd_solver::GraphEntry e;
+    memcpy(e.key, key, sizeof key);
+    e.graph = graph;
+    e.exec = exec;
+    s->graphs.push_back(e);
+    hit = &s->graphs.back();
+  }
+  CU(cudaGraphLaunch(hit->exec, sm));
+  return 0;
 }
 
 int pycfd_step_host(pycfd_solver* s, const double* u0h, const double* v0h, double* uh, double* vh,
@@ -1032,8 +1160,7 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
                       const double* vp, pycfd_field_stats* o, void* stream) {
   if (!s || !u || !v || !o) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
-  const long nmax = (long)(s->g.nx + 3) * (s->g.ny + 3);
-  k_field_stats<<<grid_for(nmax, kRedThreads), kRedThreads, 0, sm>>>(u, v, p, up, vp, s->solid, s->g, s->rb(),
+  k_field_stats<<<std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, sm>>>(u, v, p, up, vp, s->solid, s->g, s->rb(),
                                                                      s->S);
   CHECK_LAUNCH();
   CU(cudaMemcpyAsync(s->hS + S_STAT0, s->S + S_STAT0, 8 * sizeof(double), cudaMemcpyDeviceToHost, sm));

@@ -120,11 +120,9 @@ __device__ __forceinline__ double cell_div(const double* u, const double* v, int
 
 __global__ void k_divergence(const double* __restrict__ u, const double* __restrict__ v, int nx,
                              int ny, double dx, double dy, double* __restrict__ out) {
-  const long n = (long)nx * ny;
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / ny), j = (int)(c % ny);
-    out[c] = cell_div(u, v, i, j, ny, dx, dy);
-  }
+  for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < nx; i += gridDim.y * blockDim.y)
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ny; j += gridDim.x * blockDim.x)
+      out[(long)i * ny + j] = cell_div(u, v, i, j, ny, dx, dy);
 }
 
 // Poisson right-hand side b = div/dt (+ Dirichlet term), zero on non-solvable
@@ -135,11 +133,10 @@ __global__ void k_div_rhs(const double* __restrict__ u, const double* __restrict
                           const double* __restrict__ rhs_in, const uint8_t* __restrict__ flags,
                           Geo g, const double* __restrict__ S, double* __restrict__ b,
                           RedBuf rb, double* __restrict__ Sout) {
-  const long n = (long)g.nx * g.ny;
   const double dt = S[S_DT];
   double acc[1] = {0.0};
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c / g.ny), j = (int)(c % g.ny);
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
     const uint8_t f = flags[c];
     double val = 0.0;
     if (f & F_SOLV) {
@@ -249,27 +246,23 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
     }
     return;
   }
-  const long nthreads = (long)(gridDim.x - 1) * blockDim.x;
-  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  // interior copy of p
-  const long ncell = (long)nx * ny;
-  for (long c = tid; c < ncell; c += nthreads) {
-    const int i = (int)(c / ny), j = (int)(c % ny);
-    p[(long)(i + 1) * (ny + 2) + j + 1] = x[c];
-  }
-  // u faces [u_lo, u_hi) x [1, ny]
-  const long nu_f = (long)(g.u_hi - g.u_lo) * ny;
-  for (long c = tid; c < nu_f; c += nthreads) {
-    const int m = g.u_lo + (int)(c / ny), j = 1 + (int)(c % ny);
-    const long k = (long)m * (ny + 2) + j;
-    u[k] = u[k] - dt * (p_at(x, m, j, g) - p_at(x, m - 1, j, g)) / g.dx;
-  }
-  const long nv_f = (long)nx * (g.v_hi - g.v_lo);
-  const int vw = g.v_hi - g.v_lo;
-  for (long c = tid; c < nv_f; c += nthreads) {
-    const int i = 1 + (int)(c / vw), n = g.v_lo + (int)(c % vw);
-    const long k = (long)i * (ny + 3) + n;
-    v[k] = v[k] - dt * (p_at(x, i, n, g) - p_at(x, i, n - 1, g)) / g.dy;
+  // 2D sweep over rows i = 0..nx+1 (blocks in y), columns j = 0..ny+1 (threads)
+  const int rows = nx + 2;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x - 1) {
+    for (int j = threadIdx.x; j < ny + 3; j += blockDim.x) {
+      // interior copy of p: ghosted row r = i+1 for i in [0, nx)
+      if (r >= 1 && r <= nx && j >= 1 && j <= ny) p[(long)r * (ny + 2) + j] = x[(long)(r - 1) * ny + (j - 1)];
+      // u faces [u_lo, u_hi) x [1, ny]: row m = r
+      if (r >= g.u_lo && r < g.u_hi && j >= 1 && j <= ny) {
+        const long k = (long)r * (ny + 2) + j;
+        u[k] = u[k] - dt * (p_at(x, r, j, g) - p_at(x, r - 1, j, g)) / g.dx;
+      }
+      // v faces [1, nx] x [v_lo, v_hi): row i = r
+      if (r >= 1 && r <= nx && j >= g.v_lo && j < g.v_hi) {
+        const long k = (long)r * (ny + 3) + j;
+        v[k] = v[k] - dt * (p_at(x, r, j, g) - p_at(x, r, j - 1, g)) / g.dy;
+      }
+    }
   }
 }
 
@@ -282,6 +275,7 @@ __global__ void k_combine(const double* __restrict__ a, const double* __restrict
 
 // Field statistics: max|u|, max|v| (physical faces), max|du|, max|dv|,
 // max|div| (fluid), kinetic energy sum, max|vorticity|, non-finite count.
+// Blocks stride over array rows, threads over the contiguous y index.
 __global__ void k_field_stats(const double* __restrict__ u, const double* __restrict__ v,
                               const double* __restrict__ p, const double* __restrict__ up,
                               const double* __restrict__ vp, const uint8_t* __restrict__ solid,
@@ -289,44 +283,42 @@ __global__ void k_field_stats(const double* __restrict__ u, const double* __rest
   const int nx = g.nx, ny = g.ny;
   const long W = ny + 2, WV = ny + 3;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // max,max,max,max,max,sum,max,sum
-  const long nt = (long)gridDim.x * blockDim.x;
-  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long nu_all = (long)(nx + 3) * W, nv_all = (long)(nx + 2) * WV, np_all = (long)(nx + 2) * (ny + 2);
-  for (long k = tid; k < nu_all; k += nt) {
-    const int i = (int)(k / W), j = (int)(k % W);
-    const double a = u[k];
-    if (!isfinite(a)) acc[7] += 1.0;
-    if (i >= 1 && i <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
-    if (up) acc[2] = fmax(acc[2], fabs(a - up[k]));
-  }
-  for (long k = tid; k < nv_all; k += nt) {
-    const int i = (int)(k / WV), j = (int)(k % WV);
-    const double a = v[k];
-    if (!isfinite(a)) acc[7] += 1.0;
-    if (i >= 1 && i <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
-    if (vp) acc[3] = fmax(acc[3], fabs(a - vp[k]));
-  }
-  if (p)
-    for (long k = tid; k < np_all; k += nt)
-      if (!isfinite(p[k])) acc[7] += 1.0;
-  const long ncell = (long)nx * ny;
-  for (long c = tid; c < ncell; c += nt) {
-    const int i = (int)(c / ny), j = (int)(c % ny);
-    const bool sol = solid && solid[c];
-    if (!sol) acc[4] = fmax(acc[4], fabs(cell_div(u, v, i, j, ny, g.dx, g.dy)));
-    const double uc = 0.5 * (u[(long)(i + 1) * W + j + 1] + u[(long)(i + 2) * W + j + 1]);
-    const double vc = 0.5 * (v[(long)(i + 1) * WV + j + 1] + v[(long)(i + 1) * WV + j + 2]);
-    if (!sol) acc[5] += 0.5 * (uc * uc + vc * vc);
-    // vorticity at the four corners of the cell (pycfd/analysis/postprocess.py:21-40)
-    double w4 = 0.0;
-    for (int di = 0; di < 2; ++di)
-      for (int dj = 0; dj < 2; ++dj) {
-        const int a = i + di, bb = j + dj;  // corner index (0..nx, 0..ny)
-        const double dvdx = (v[(long)(a + 1) * WV + bb + 1] - v[(long)a * WV + bb + 1]) / g.dx;
-        const double dudy = (u[(long)(a + 1) * W + bb + 1] - u[(long)(a + 1) * W + bb]) / g.dy;
-        w4 += dvdx - dudy;
+  for (int r = blockIdx.x; r < nx + 3; r += gridDim.x) {
+    for (int j = threadIdx.x; j < ny + 3; j += blockDim.x) {
+      if (j < ny + 2) {
+        const long k = (long)r * W + j;
+        const double a = u[k];
+        if (!isfinite(a)) acc[7] += 1.0;
+        if (r >= 1 && r <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
+        if (up) acc[2] = fmax(acc[2], fabs(a - up[k]));
       }
-    acc[6] = fmax(acc[6], fabs(0.25 * w4));
+      if (r < nx + 2) {
+        const long k = (long)r * WV + j;
+        const double a = v[k];
+        if (!isfinite(a)) acc[7] += 1.0;
+        if (r >= 1 && r <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
+        if (vp) acc[3] = fmax(acc[3], fabs(a - vp[k]));
+        if (p && j < ny + 2 && !isfinite(p[(long)r * W + j])) acc[7] += 1.0;
+      }
+      if (r < nx && j < ny) {
+        const int i = r;
+        const bool sol = solid && solid[(long)i * ny + j];
+        if (!sol) acc[4] = fmax(acc[4], fabs(cell_div(u, v, i, j, ny, g.dx, g.dy)));
+        const double uc = 0.5 * (u[(long)(i + 1) * W + j + 1] + u[(long)(i + 2) * W + j + 1]);
+        const double vc = 0.5 * (v[(long)(i + 1) * WV + j + 1] + v[(long)(i + 1) * WV + j + 2]);
+        if (!sol) acc[5] += 0.5 * (uc * uc + vc * vc);
+        // vorticity at the four corners of the cell (pycfd/analysis/postprocess.py:21-40)
+        double w4 = 0.0;
+        for (int di = 0; di < 2; ++di)
+          for (int dj = 0; dj < 2; ++dj) {
+            const int a = i + di, bb = j + dj;
+            const double dvdx = (v[(long)(a + 1) * WV + bb + 1] - v[(long)a * WV + bb + 1]) / g.dx;
+            const double dudy = (u[(long)(a + 1) * W + bb + 1] - u[(long)(a + 1) * W + bb]) / g.dy;
+            w4 += dvdx - dudy;
+          }
+        acc[6] = fmax(acc[6], fabs(0.25 * w4));
+      }
+    }
   }
   grid_reduce<8, 0x5Fu>(acc, rb, [&](double* t) {
     for (int k = 0; k < 8; ++k) Sout[S_STAT0 + k] = t[k];

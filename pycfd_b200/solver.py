@@ -35,6 +35,9 @@ class GpuOptions:
 
     precision: str = "fp64"
     inner_tol: float = 1e-4
+    #: record each step once into a CUDA graph (device-side Poisson loops) and
+    #: replay it; ``advance()`` and the time stepper use it.
+    graphs: bool = True
 
 
 def _torch():
@@ -185,6 +188,7 @@ class ProjectionSolver:
         self.body_force_reactions = tuple((0.0, 0.0) for _ in self.body_masks)
         self._blend = 0.0
         self.last_stats = None
+        self._ring = None
 
     # ------------------------------------------------------------------ #
     def _build_slices(self) -> None:
@@ -406,6 +410,25 @@ class ProjectionSolver:
         _lib.check(self._L.pycfd_step(self._h, _lib.ptr(fields.u.contiguous()),
                                       _lib.ptr(fields.v.contiguous()), _lib.ptr(u), _lib.ptr(v),
                                       _lib.ptr(p), float(dt), float(self._blend), _stream()))
+        self._read_stats()
+        return FlowField(self.mesh, u, v, p, fields.t + dt, fields.step + 1)
+
+    def advance(self, fields: FlowField, dt: float) -> FlowField:
+        """``step`` into solver-owned ping-pong buffers, replaying a recorded CUDA graph.
+
+        The returned state lives in one of two buffers the solver reuses: it stays
+        valid until the step after next (copy it to keep it longer).
+        """
+        if not self.options.graphs:
+            return self.step(fields, dt)
+        if self._ring is None:
+            self._ring = [self._empty_state(), self._empty_state()]
+        out = self._ring[0] if fields.u.data_ptr() != self._ring[0][0].data_ptr() else self._ring[1]
+        u, v, p = out
+        _lib.check(self._L.pycfd_step_graph(self._h, _lib.ptr(fields.u.contiguous()),
+                                            _lib.ptr(fields.v.contiguous()), _lib.ptr(u),
+                                            _lib.ptr(v), _lib.ptr(p), float(dt),
+                                            float(self._blend), _stream()))
         self._read_stats()
         return FlowField(self.mesh, u, v, p, fields.t + dt, fields.step + 1)
 

@@ -110,7 +110,7 @@ class TimeStepper:
             dt = min(dt, t_end - fields.t)
             self.solver.set_upwind_blend(self.solver.upwind_blend_for(fields, dt))
             previous = fields
-            fields = self.solver.step(previous, dt)
+            fields = self.solver.advance(previous, dt)
             steps_taken += 1
             st = self.solver.field_stats(fields, previous)
             fields._stats = st

@@ -167,3 +167,29 @@ def test_rejected_configurations():
                               pressure_solver="sor"))
     with pytest.raises(ValueError, match="shape"):
         ProjectionSolver(_cfg(base, pressure_solver="cg"), obstacle=np.zeros((4, 4), bool))
+
+
+@pytest.mark.parametrize("solver", ["cg", "mgcg", "multigrid"])
+def test_graph_replay_matches_eager_bitwise(solver):
+    """A step recorded into a CUDA graph (device-side solve loops) replays the eager launches."""
+    from pycfd_b200.obstacles import circle_mask
+    from pycfd_b200.mesh import StructuredMesh
+    from pycfd_b200.solver import GpuOptions
+    d = dict(nx=48, ny=32, lx=3.0, ly=2.0, re=50.0, pressure_solver=solver, poisson_tol=1e-12,
+             boundary_config=cases.bcs(left=("inlet", 1.0), right=("outlet",), top=("symmetry",),
+                                       bottom=("symmetry",)))
+    out = []
+    for graphs in (False, True):
+        cfg = _cfg(d)
+        ob = circle_mask(StructuredMesh.from_config(cfg), (1.0, 1.0), 0.25)
+        s = _solver(cfg, ob.mask, options=GpuOptions(graphs=graphs))
+        f = s.initialize(1.0)
+        its = []
+        for _ in range(6):
+            f = s.advance(f, 2e-3)
+            its.append(s.last_stats.total_iterations)
+        out.append((f.numpy(), s.body_force_reaction, its))
+    (a, fa, ia), (b, fb, ib) = out
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert fa == fb and ia == ib
