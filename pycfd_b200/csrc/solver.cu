@@ -120,7 +120,8 @@ struct pycfd_solver {
   int last_ir = 0;
   // CUDA-graph recording of whole steps
   bool capturing = false;
-  cudaStream_t aux = nullptr;
+  cudaStream_t aux = nullptr;   // records the bodies of the solve loops
+  cudaStream_t rec = nullptr;   // records whole steps
   struct GraphEntry {
     const void* key[5];
     cudaGraph_t graph;
@@ -724,6 +725,7 @@ int pycfd_solver_destroy(pycfd_solver* s) {
     cudaGraphDestroy(e.graph);
   }
   if (s->aux) cudaStreamDestroy(s->aux);
+  if (s->rec) cudaStreamDestroy(s->rec);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   if (s->hI) cudaFreeHost(s->hI);
@@ -1082,13 +1084,16 @@ int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double
   for (auto& e : s->graphs)
     if (!memcmp(e.key, key, sizeof key)) hit = &e;
   if (!hit) {
+    // Record on the solver's own stream (the caller's may be the legacy default
+    // stream, which cannot be captured); recording executes nothing.
     if (!s->aux) CU(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    if (!s->rec) CU(cudaStreamCreateWithFlags(&s->rec, cudaStreamNonBlocking));
     cudaGraph_t graph = nullptr;
-    CU(cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal));
+    CU(cudaStreamBeginCapture(s->rec, cudaStreamCaptureModeThreadLocal));
     s->capturing = true;
-    const int rc = step_impl(s, u0, v0, u, v, p, sm);
+    const int rc = step_impl(s, u0, v0, u, v, p, s->rec);
     s->capturing = false;
-    const cudaError_t ec = cudaStreamEndCapture(sm, &graph);
+    const cudaError_t ec = cudaStreamEndCapture(s->rec, &graph);
     if (rc) {
       if (graph) cudaGraphDestroy(graph);
       return rc;
