@@ -214,6 +214,28 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
                       const double* u_prev, const double* v_prev, pycfd_field_stats* out,
                       void* stream);
 
+/* No counterpart in the reference.  The reductions of pycfd_reduce_fields for
+ * callers that cannot allocate device memory at the moment they need them: a
+ * host whose own allocator owns all device memory, a real-time loop that cannot
+ * afford the implicit device synchronisation of cudaMalloc, code that issues its
+ * work while a stream is being captured.  It needs no solver handle and calls
+ * no allocator.  Its scratch is a static device array of
+ * PCFD_NOALLOC_MAX_ROWS*8 + 66 doubles (about 258 KiB) that every GPU which
+ * loads the library holds until the process exits; one thread block runs per
+ * row of u, so nx may be at most PCFD_NOALLOC_MAX_ROWS - 3 (larger grids are
+ * refused with PCFD_E_ARG).  Every call on a device shares that scratch and it
+ * keeps the last call's contents: calls whose work overlaps on the GPU (for
+ * instance on two streams) race, so serialise them.  The first call on a
+ * device looks up the scratch's device address with that device current; make
+ * that first call before any stream capture.  u, v, p, u_prev, v_prev and solid
+ * (nx*ny bytes, or NULL) are device pointers; *out is written once the stream
+ * has finished the reduction. */
+#define PCFD_NOALLOC_MAX_ROWS 4096
+int pycfd_reduce_fields_noalloc(const double* u, const double* v, const double* p,
+                                const double* u_prev, const double* v_prev, const uint8_t* solid,
+                                int nx, int ny, double dx, double dy, pycfd_field_stats* out,
+                                void* stream);
+
 #ifdef __cplusplus
 }
 #endif

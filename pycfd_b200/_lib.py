@@ -26,6 +26,7 @@ EXPORTS = (
     "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
+    "pycfd_reduce_fields_noalloc",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -101,6 +102,9 @@ def load(path: str = LIB_PATH):
         "pycfd_step_host": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),
+        "pycfd_reduce_fields_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int, C.c_int,
+                                                  C.c_double, C.c_double, C.POINTER(FieldStats),
+                                                  vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

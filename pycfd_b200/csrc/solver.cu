@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1183,3 +1184,79 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Field reduction without device allocation
+// ============================================================================
+// Some hosts cannot call cudaMalloc at the moment they want a reduction: an
+// application that hands every byte of device memory to its own allocator, a
+// real-time loop that must not take the implicit device synchronisation of an
+// allocation, or code that builds its work while a stream is being captured.
+// This entry point serves them.  Its scratch -- one block of scalar slots laid
+// out like a solver's (the results land in the statistics slots), one row of 8
+// partial sums per thread block and the ticket counter of the grid reduction --
+// is the file-scope array below: PCFD_NOALLOC_MAX_ROWS*8 + S_COUNT + 2 doubles
+// (about 258 KiB), held by every GPU that loads this library until the process
+// exits.  The kernel runs one block per row of the u array, so nx + 3 rows must
+// fit: nx <= PCFD_NOALLOC_MAX_ROWS - 3.
+static __device__ __align__(256) double g_noalloc_scratch[S_COUNT + PCFD_NOALLOC_MAX_ROWS * 8 + 2];
+
+namespace {
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[128] = {};   // device address of the scratch, per device ordinal
+
+// Host code must not use the array's name as a device address (it names a
+// host-side stand-in); the address is looked up once per device, with that
+// device current, and cached.
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(PCFD_E_ARG, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+}  // namespace
+
+extern "C" int pycfd_reduce_fields_noalloc(const double* u, const double* v, const double* p,
+                                           const double* u_prev, const double* v_prev,
+                                           const uint8_t* solid, int nx, int ny, double dx, double dy,
+                                           pycfd_field_stats* o, void* stream) {
+  if (!u || !v || !o || nx < 1 || ny < 1 || !(dx > 0) || !(dy > 0))
+    return fail(PCFD_E_ARG, "bad arguments");
+  if (nx + 3 > PCFD_NOALLOC_MAX_ROWS)
+    return fail(PCFD_E_ARG,
+                "pycfd_reduce_fields_noalloc handles nx <= %d (its static scratch holds %d block rows); "
+                "got nx = %d -- use pycfd_reduce_fields for larger grids",
+                PCFD_NOALLOC_MAX_ROWS - 3, PCFD_NOALLOC_MAX_ROWS, nx);
+  cudaStream_t sm = st(stream);
+  double* scr = nullptr;
+  TRY(noalloc_scratch(&scr));
+  double* partials = scr + S_COUNT;
+  unsigned int* counter = reinterpret_cast<unsigned int*>(partials + PCFD_NOALLOC_MAX_ROWS * 8);
+  CU(cudaMemsetAsync(counter, 0, sizeof(unsigned int), sm));   // the ticket must start at zero
+  Geo g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.dx = dx;
+  g.dy = dy;
+  k_field_stats<<<nx + 3, kRedThreads, 0, sm>>>(u, v, p, u_prev, v_prev, solid, g, RedBuf{partials, counter}, scr);
+  CHECK_LAUNCH();
+  double t[8];
+  CU(cudaMemcpyAsync(t, scr + S_STAT0, sizeof t, cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  o->max_u = t[0];
+  o->max_v = t[1];
+  o->max_du = t[2];
+  o->max_dv = t[3];
+  o->max_div = t[4];
+  o->kinetic_energy = t[5] * (dx * dy);
+  o->max_vorticity = t[6];
+  o->finite = t[7] == 0.0;
+  return 0;
+}
