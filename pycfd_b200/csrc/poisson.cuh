@@ -341,6 +341,78 @@ __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
   });
 }
 
+// ---- mixed form: FP64 iterative refinement around an FP32 MG-PCG ----------
+// One refinement pass: r = b - A x in FP64 (first pass: finalise b from the raw
+// right-hand side and take x from the warm start or zero), the outer stopping
+// rule ||r|| < tol ||b|| on this true residual, and the set-up of the inner
+// FP32 solve A e = r from e = 0 (r32 = r, inner atol = inner_tol ||r||).
+__global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
+                              float* __restrict__ r32, float* __restrict__ e32,
+                              const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
+                              double inner_tol, int max_passes, int first, int has_x0,
+                              double* __restrict__ S, int* __restrict__ I, RedBuf rb,
+                              LoopCtl outer) {
+  const double mean = (first && cfg.singular) ? S[S_MEAN_B] : 0.0;
+  double acc[3] = {0, 0, 0};
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
+    const uint8_t f = flags[c];
+    double bc = b[c];
+    if (first) {
+      bc = (f & F_SOLV) ? bc - mean : 0.0;
+      b[c] = bc;
+      if (!has_x0) x[c] = 0.0;
+    }
+    const double ax = (first && !has_x0) ? 0.0
+                      : fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return x[k]; });
+    const double rc = bc - ax;
+    r32[c] = (float)rc;
+    e32[c] = 0.0f;
+    acc[0] += rc * rc;
+    if (f & F_SOLV) acc[1] += (double)(float)rc;
+    if (first) acc[2] += bc * bc;
+  }
+  grid_reduce<3>(acc, rb, [&](double* t) {
+    if (first) {
+      S[S_IR_BNORM] = sqrt(t[2]);
+      S[S_BNORM2_0] = t[2];
+      I[I_IR_IT] = 0;
+      I[I_ZERO_RHS] = (t[2] == 0.0);
+      I[I_STATUS] = 0;
+    }
+    const double nb = S[S_IR_BNORM];
+    S[S_IR_RNORM2] = t[0];
+    const bool conv = (nb == 0.0) || (sqrt(t[0]) < cfg.tol * nb);
+    const bool done = conv || I[I_IR_IT] >= max_passes;
+    I[I_CONVERGED] = conv;
+    I[I_IR_DONE] = done;
+    // inner solve from e = 0: its residual is r itself
+    S[S_BNORM2] = t[0];
+    S[S_ATOL] = inner_tol * sqrt(t[0]);
+    S[S_RNORM2] = t[0];
+    S[S_SUM_R] = t[1];
+    S[S_MEAN_R] = g.n_fluid ? t[1] / g.n_fluid : 0.0;
+    I[I_IT] = 0;
+    I[I_DONE] = done;
+    outer.set(!done);
+  });
+}
+
+// Arm the inner solve's loop from the flags of the last refinement pass.
+__global__ void k_ir_arm(const int* __restrict__ I, LoopCtl inner) {
+  if (threadIdx.x == 0) inner.set(!I[I_DONE]);
+}
+
+// x += e (FP32 correction promoted to FP64) on solvable rows; count the pass.
+__global__ void k_ir_update(double* __restrict__ x, const float* __restrict__ e32,
+                            const uint8_t* __restrict__ flags, Geo g, int* __restrict__ I) {
+  FOR_CELLS(g) {
+    const int c = i * g.ny + j;
+    if (flags[c] & F_SOLV) x[c] = x[c] + (double)e32[c];
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) I[I_IR_IT] += 1;
+}
+
 // Start of a call: step parameters into the device scalar block (kernel
 // arguments, so no host synchronisation is needed) and the per-call counters.
 __global__ void k_begin(double* __restrict__ S, int* __restrict__ I, double dt, double blend) {

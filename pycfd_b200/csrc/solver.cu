@@ -122,6 +122,7 @@ struct pycfd_solver {
   // CUDA-graph recording of whole steps
   bool capturing = false;
   cudaStream_t aux = nullptr;   // records the bodies of the solve loops
+  cudaStream_t aux2 = nullptr;  // records loop bodies nested one level deeper
   cudaStream_t rec = nullptr;   // records whole steps
   struct GraphEntry {
     const void* key[5];
@@ -527,6 +528,93 @@ int loop_close(pycfd_solver* s) {
   return 0;
 }
 
+// ---- mixed form: FP64 iterative refinement around an FP32 MG-PCG ----------
+// Outer passes r = b - A x (FP64) until ||r|| < tol ||b||; each pass solves
+// A e = r in FP32 storage with the FP32 copy of the hierarchy to a relative
+// inner_tol and adds e to x.  Recorded, the outer loop and the inner CG loop
+// are nested WHILE nodes.
+constexpr int kIrMaxPasses = 40;
+constexpr int kInnerMaxIter = 200;
+
+int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
+  const Geo& g = s->g;
+  const SolveCfg cfg = s->cfg();
+  const SolveCfg icfg{s->inner_tol, kInnerMaxIter, s->singular, 0};
+  const bool cap = s->capturing;
+  Loop outer, inner;
+  TRY(loop_handle(s, stream, &outer));
+  k_ir_residual<<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->r32, s->x32, s->flags, g, cfg,
+                                                    s->inner_tol, kIrMaxPasses, 1, has_x0, s->S, s->I,
+                                                    s->rb(), outer.ctl);
+  CHECK_LAUNCH();
+  auto inner_pass = [&](cudaStream_t st) -> int {
+    TRY(vcycle_pcg<float>(s, s->r32, s->z32, st));
+    k_cg_pq<float, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->r32, s->z32, s->pa32, s->pb32, s->q32, s->flags,
+                                                          g, s->S, s->I, s->rb());
+    CHECK_LAUNCH();
+    k_cg_xr<float, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->x32, s->r32, s->pb32, s->q32, s->pa32, s->flags,
+                                                          g, icfg, s->S, s->I, s->rb(), inner.ctl);
+    CHECK_LAUNCH();
+    return 0;
+  };
+  auto refine = [&](cudaStream_t st) -> int {
+    k_ir_update<<<s->cgrid, s->cblock, 0, st>>>(x, s->x32, s->flags, g, s->I);
+    CHECK_LAUNCH();
+    k_ir_residual<<<s->cgrid, s->cblock, 0, st>>>(s->b, x, s->r32, s->x32, s->flags, g, cfg, s->inner_tol,
+                                                  kIrMaxPasses, 0, 1, s->S, s->I, s->rb(), outer.ctl);
+    CHECK_LAUNCH();
+    return 0;
+  };
+  if (cap) {
+    TRY(loop_open(s, stream, &outer));          // outer body recorded on aux
+    // inner loop inside the outer body: handle on the body graph, body on aux2
+    {
+      cudaGraphConditionalHandle h;
+      CU(cudaGraphConditionalHandleCreate(&h, outer.body, 0, 0));
+      inner.ctl = LoopCtl{h, 1};
+      k_ir_arm<<<1, 32, 0, s->aux>>>(s->I, inner.ctl);
+      CHECK_LAUNCH();
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t gb = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      CU(cudaStreamGetCaptureInfo(s->aux, &cs, nullptr, &gb, &deps, &nd));
+      cudaGraphNodeParams np{};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      CU(cudaGraphAddNode(&node, gb, deps, nd, &np));
+      CU(cudaStreamUpdateCaptureDependencies(s->aux, &node, 1, cudaStreamSetCaptureDependencies));
+      if (!s->aux2) CU(cudaStreamCreateWithFlags(&s->aux2, cudaStreamNonBlocking));
+      CU(cudaStreamBeginCaptureToGraph(s->aux2, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed));
+      TRY(inner_pass(s->aux2));
+      cudaGraph_t dummy = nullptr;
+      CU(cudaStreamEndCapture(s->aux2, &dummy));
+    }
+    TRY(refine(s->aux));
+    TRY(loop_close(s));
+  } else {
+    for (;;) {
+      TRY(read_flags(s, stream));
+      if (s->hI[I_IR_DONE]) break;
+      for (;;) {
+        TRY(read_flags(s, stream));
+        if (s->hI[I_DONE]) break;
+        TRY(inner_pass(stream));
+      }
+      TRY(refine(stream));
+    }
+  }
+  k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
+  CHECK_LAUNCH();
+  k_finish_apply<double><<<s->cgrid, s->cblock, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
+  CHECK_LAUNCH();
+  return 0;
+}
+
 // ---- Poisson solve on the prepared raw right-hand side s->b --------------
 // Result (normalised) in x.  has_x0: x holds the warm start on entry.
 int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
@@ -659,7 +747,8 @@ int project_impl(pycfd_solver* s, double* u, double* v, double* p, double dt_ove
   const int G = grid1(s);
   k_div_rhs<<<s->cgrid, s->cblock, 0, stream>>>(u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
-  TRY(solve_prepared(s, s->x, s->has_guess, stream));
+  if (s->precision == PCFD_MIXED) TRY(solve_mixed(s, s->x, s->has_guess, stream));
+  else TRY(solve_prepared(s, s->x, s->has_guess, stream));
   s->has_guess = true;
   const int gc = std::min(s->g.nx + 2, kMaxRedBlocks) + 1;   // rows + the ghost-ring block
   k_correct<<<gc, 256, 0, stream>>>(u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
@@ -727,6 +816,7 @@ int pycfd_solver_destroy(pycfd_solver* s) {
   }
   if (s->aux) cudaStreamDestroy(s->aux);
   if (s->rec) cudaStreamDestroy(s->rec);
+  if (s->aux2) cudaStreamDestroy(s->aux2);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   if (s->hI) cudaFreeHost(s->hI);
@@ -1013,7 +1103,8 @@ int pycfd_poisson_solve(pycfd_solver* s, const double* rhs, const double* p0, do
   k_div_rhs<<<s->cgrid, s->cblock, 0, sm>>>(nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   if (p0) CU(cudaMemcpyAsync(s->x_api, p0, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
-  TRY(solve_prepared(s, s->x_api, p0 != nullptr, sm));
+  if (s->precision == PCFD_MIXED) TRY(solve_mixed(s, s->x_api, p0 != nullptr, sm));
+  else TRY(solve_prepared(s, s->x_api, p0 != nullptr, sm));
   CU(cudaMemcpyAsync(p, s->x_api, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
   return 0;
 }
@@ -1158,7 +1249,7 @@ int pycfd_get_stats(pycfd_solver* s, pycfd_stats* o, void* stream) {
     o->body_fx[b] = s->hS[S_BODY_FX + b];
     o->body_fy[b] = s->hS[S_BODY_FY + b];
   }
-  o->ir_iterations = s->last_ir;
+  o->ir_iterations = s->hI[I_IR_IT];
   return 0;
 }
 
