@@ -108,6 +108,9 @@ typedef struct {
     const pycfd_mg_level* levels;
     const double* coarsest_inverse;           /* n_L x n_L row-major pseudo-inverse
                                                  of the coarsest operator    */
+    int coarse_cluster_rows;                  /* levels with at most this many rows run
+                                                 as one thread-block cluster per V-cycle;
+                                                 0 = one kernel per phase    */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */
@@ -200,11 +203,44 @@ int pycfd_step(pycfd_solver* s, const double* u0, const double* v0, double* u, d
 int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
                      double* p, double dt, double blend, void* stream);
 
+/* Device-side time-step control for stepping without host round trips. */
+typedef struct {
+    int adaptive;          /* config.adaptive_dt                                  */
+    double cfl;            /* config.cfl_max                                      */
+    double visc_limit;     /* 0.8 / (2 nu (1/dx^2 + 1/dy^2))                      */
+    double dt_cap;         /* config.dt                                           */
+    double t_end;          /* dt is clamped so the clock lands on t_end            */
+    int blend_mode;        /* 0: fixed blend below; 1: 1.2 x Courant number (upwind) */
+    double blend;
+} pycfd_dt_control;
+
+/* One step whose dt is computed on the device from the current state, with
+ * the reference's formula and order (TimeStepper.compute_dt and _check_health,
+ * pycfd/core/timestepper.py:94-142), recorded once per address tuple into a
+ * CUDA graph together with that reduction.  Health problems set sticky flags
+ * read by pycfd_get_clock (1 non-finite, 2 |u| > 1e6, 4 dt < 1e-8). */
+int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
+                        double* p, const pycfd_dt_control* ctl, void* stream);
+int pycfd_set_clock(pycfd_solver* s, double t, void* stream);
+int pycfd_get_clock(pycfd_solver* s, double* t, double* dt, int* steps, int* health, void* stream);
+
 /* The same step on HOST buffers: copies the inputs in, steps, copies u, v, p
  * back, all on `stream`, and returns after the stream has finished. */
 int pycfd_step_host(pycfd_solver* s, const double* u0_host, const double* v0_host,
                     double* u_host, double* v_host, double* p_host, double dt, double blend,
                     void* stream);
+
+/* Measurement support (no counterpart in the reference): bracket every eager
+ * launch of one kernel with CUDA events on its stream, then read the summed
+ * device time.  Ids: 1 CG direction/A-product (k_cg_pq), 2 last fine smoothing
+ * sweep of the V-cycle, 3 first fine sweep + residual, 4 coarse-level cluster
+ * cycle, 6 momentum predictor, 7 projection correction; 0 switches it off.
+ * Steps replayed from a recorded graph are not bracketed. */
+int pycfd_profile_kernel(pycfd_solver* s, int kernel_id);
+/* Kernel launches issued by this library so far (eager launches; a recorded
+ * step counts its launches once, when it is recorded). */
+long long pycfd_launch_count(void);
+int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* stream);
 
 /* Results of the last solve/step (synchronises `stream`). */
 int pycfd_get_stats(pycfd_solver* s, pycfd_stats* out, void* stream);

@@ -25,8 +25,10 @@ EXPORTS = (
     "pycfd_last_error", "pycfd_version", "pycfd_solver_create", "pycfd_solver_destroy",
     "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
-    "pycfd_step_graph", "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
-    "pycfd_reduce_fields_noalloc",
+    "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
+    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
+    "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_launch_count",
+    "pycfd_profile_read",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -50,7 +52,14 @@ class SolverDesc(C.Structure):
                 ("tol", C.c_double), ("maxiter", C.c_int), ("sor_omega", C.c_double),
                 ("mg_sweeps", C.c_int), ("time_scheme", C.c_int), ("precision", C.c_int),
                 ("inner_tol", C.c_double), ("n_levels", C.c_int),
-                ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp)]
+                ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp),
+                ("coarse_cluster_rows", C.c_int)]
+
+
+class DtControl(C.Structure):
+    _fields_ = [("adaptive", C.c_int), ("cfl", C.c_double), ("visc_limit", C.c_double),
+                ("dt_cap", C.c_double), ("t_end", C.c_double), ("blend_mode", C.c_int),
+                ("blend", C.c_double)]
 
 
 class Stats(C.Structure):
@@ -100,7 +109,14 @@ def load(path: str = LIB_PATH):
         "pycfd_step": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_step_graph": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_step_host": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
+        "pycfd_step_adaptive": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(DtControl), vp]),
+        "pycfd_set_clock": (C.c_int, [vp, C.c_double, vp]),
+        "pycfd_get_clock": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_int), vp]),
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
+        "pycfd_profile_kernel": (C.c_int, [vp, C.c_int]),
+        "pycfd_launch_count": (C.c_longlong, []),
+        "pycfd_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),
         "pycfd_reduce_fields_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int, C.c_int,
                                                   C.c_double, C.c_double, C.POINTER(FieldStats),

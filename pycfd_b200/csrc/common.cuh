@@ -23,7 +23,7 @@ enum Slot {
   S_DT = 0, S_BLEND,
   S_BNORM2, S_ATOL, S_RNORM2, S_RHO, S_RHO_PREV, S_ALPHA, S_BETA, S_PQ,
   S_MEAN_B, S_MEAN_R, S_MEAN_X, S_RESID, S_RES_PREV, S_SUM_R, S_TOL,
-  S_BNORM2_0, S_IR_RNORM2, S_MEAN_Z, S_IR_BNORM,
+  S_BNORM2_0, S_IR_RNORM2, S_MEAN_Z, S_IR_BNORM, S_T,
   S_FX, S_FY,
   S_BODY_FX,                      // PCFD_MAX_BODIES slots
   S_BODY_FY = S_BODY_FX + 8,
@@ -35,7 +35,7 @@ enum Slot {
 // Device int slots.
 enum ISlot {
   I_IT = 0, I_DONE, I_CONVERGED, I_STATUS, I_STALLED, I_TOTAL_IT, I_ZERO_RHS, I_MAXITER,
-  I_IR_IT, I_IR_DONE, I_FINITE,
+  I_IR_IT, I_IR_DONE, I_FINITE, I_HEALTH, I_STEPS,
   I_COUNT = 16
 };
 
@@ -56,7 +56,11 @@ struct RedBuf {
   unsigned int* counter;
 };
 
-constexpr int kMaxRedBlocks = 1184;   // 148 SMs x 8 resident blocks
+constexpr int kMaxRedBlocks = 1184;   // 148 SMs x 8 resident blocks (partials buffer size)
+// Streaming grids are sized to one wave: 148 SMs x 4 resident 256-thread
+// blocks (every streaming kernel here stays at <= 64 registers per thread),
+// with grid-stride loops, so no kernel pays a partial second wave.
+constexpr int kWaveBlocks = 592;
 constexpr int kRedThreads = 256;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -196,9 +200,9 @@ constexpr int kCellTJ = 32, kCellTI = 8;
 inline void cell_launch(int nx, int ny, dim3* grid, dim3* block) {
   *block = dim3(kCellTJ, kCellTI);
   int gx = (ny + kCellTJ - 1) / kCellTJ;
-  if (gx > kMaxRedBlocks) gx = kMaxRedBlocks;
+  if (gx > kWaveBlocks) gx = kWaveBlocks;
   int gy = (nx + kCellTI - 1) / kCellTI;
-  const int cap = kMaxRedBlocks / gx > 0 ? kMaxRedBlocks / gx : 1;
+  const int cap = kWaveBlocks / gx > 0 ? kWaveBlocks / gx : 1;
   if (gy > cap) gy = cap;
   *grid = dim3(gx, gy);
 }

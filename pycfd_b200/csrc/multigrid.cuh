@@ -10,6 +10,8 @@
 // Damped-Jacobi smoothing is x += wdinv*(b - A x); from a zero start the first
 // sweep is the pointwise x = wdinv*b, fused with the residual that follows.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace pcfd {
@@ -46,17 +48,26 @@ __device__ __forceinline__ double ell_row(const Ell<T>& E, int row, int lane, X 
   return acc;
 }
 
+// Rows of an ELL pass, L lanes each, grid-stride over one wave of blocks.
+// A warp's row groups share `base`, so every lane of a warp runs the same
+// number of rounds (the lane shuffle needs them all).
+#define FOR_ELL_ROWS(E, L)                                                                   \
+  const int lane = (int)(threadIdx.x % (L));                                                 \
+  const int per = (int)(gridDim.x * blockDim.x / (L));                                       \
+  for (int base = (int)(blockIdx.x * blockDim.x / (L)); base < (E).n; base += per)            \
+    for (int row = base + (int)(threadIdx.x / (L)), once_ = 1; once_; once_ = 0)
+
 // x = wd*b; res = b - A(wd*b)          (first sweep from zero + residual)
 template <int L, class T>
 __global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                           T* __restrict__ x, T* __restrict__ res) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int row = (int)(t / L), lane = (int)(t % L);
-  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
-  if (lane == 0 && row < A.n) {
-    const double bx = (double)b[row];
-    x[row] = (T)((double)wd[row] * bx);
-    res[row] = (T)(bx - s);
+  FOR_ELL_ROWS(A, L) {
+    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
+    if (lane == 0 && row < A.n) {
+      const double bx = (double)b[row];
+      x[row] = (T)((double)wd[row] * bx);
+      res[row] = (T)(bx - s);
+    }
   }
 }
 
@@ -64,29 +75,29 @@ __global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restric
 template <int L, class T>
 __global__ void k_ell_smooth(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                              const T* __restrict__ x, T* __restrict__ xo) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int row = (int)(t / L), lane = (int)(t % L);
-  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
-  if (lane == 0 && row < A.n) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+  FOR_ELL_ROWS(A, L) {
+    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
+    if (lane == 0 && row < A.n) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+  }
 }
 
 // res = b - A x
 template <int L, class T>
 __global__ void k_ell_resid(Ell<T> A, const T* __restrict__ b, const T* __restrict__ x,
                             T* __restrict__ res) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int row = (int)(t / L), lane = (int)(t % L);
-  const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
-  if (lane == 0 && row < A.n) res[row] = (T)((double)b[row] - s);
+  FOR_ELL_ROWS(A, L) {
+    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
+    if (lane == 0 && row < A.n) res[row] = (T)((double)b[row] - s);
+  }
 }
 
 // y = M x (restriction with M = R), or y += M x (prolongation with M = P).
 template <int L, bool ADD, class T>
 __global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y) {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const int row = (int)(t / L), lane = (int)(t % L);
-  const double s = ell_row<L>(M, row, lane, [&](int c) { return (double)x[c]; });
-  if (lane == 0 && row < M.n) y[row] = ADD ? (T)((double)y[row] + s) : (T)s;
+  FOR_ELL_ROWS(M, L) {
+    const double s = ell_row<L>(M, row, lane, [&](int c) { return (double)x[c]; });
+    if (lane == 0 && row < M.n) y[row] = ADD ? (T)((double)y[row] + s) : (T)s;
+  }
 }
 
 // Coarsest level: x = C b with C the precomputed pseudo-inverse (pinned LU
@@ -103,6 +114,46 @@ __global__ void k_dense(const T* __restrict__ C, int n, const T* __restrict__ b,
   }
 }
 
+// Restriction into the coarsest level and its dense solve in one block:
+// b = R res (rows n <= a few hundred, one warp per row), then x = C b.
+template <class T>
+__global__ void k_restrict_dense(Ell<T> R, int L, const T* __restrict__ res, const T* __restrict__ C,
+                                 T* __restrict__ b, T* __restrict__ x) {
+  extern __shared__ double sb[];
+  // restriction: L lanes per row, the same partial-sum order as the ELL kernels
+  const int lane = threadIdx.x % L, per = blockDim.x / L;
+  for (int base = 0; base < R.n; base += per) {
+    const int row = base + threadIdx.x / L;
+    double acc = 0.0;
+    if (row < R.n) {
+      if (R.rowmajor) {
+        const long o = (long)row * R.K;
+        for (int k = lane; k < R.K; k += L) acc += (double)R.val[o + k] * (double)res[R.col[o + k]];
+      } else {
+        for (int k = lane; k < R.K; k += L) {
+          const long e = (long)k * R.n + row;
+          acc += (double)R.val[e] * (double)res[R.col[e]];
+        }
+      }
+    }
+    for (int s = L >> 1; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s, L);
+    if (lane == 0 && row < R.n) {
+      sb[row] = (double)(T)acc;
+      b[row] = (T)acc;
+    }
+  }
+  __syncthreads();
+  // dense solve: one warp per row
+  const int wl = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int n = R.n;
+  for (int row = warp; row < n; row += nw) {
+    double acc = 0.0;
+    for (int k = wl; k < n; k += 32) acc += (double)C[(long)row * n + k] * sb[k];
+    acc = warp_sum(acc);
+    if (wl == 0) x[row] = (T)acc;
+  }
+}
+
 // ---- level 0 (matrix-free) --------------------------------------------------
 // Right-hand side of the fine level: the CG residual projected onto the
 // active set (multigrid.py:453-458), or a stored vector.
@@ -111,12 +162,28 @@ struct BFromR {
   const T* r;
   const uint8_t* f;
   double mean;
+  __device__ __forceinline__ void load() {}
   __device__ __forceinline__ double operator()(int k) const {
     return (f[k] & F_SOLV) ? (double)r[k] - mean : 0.0;
   }
 };
+// Same projection with the mean read from the device scalars at kernel start.
+template <class T>
+struct BFromRS {
+  const T* r;
+  const uint8_t* f;
+  const double* S;
+  int singular;
+  double mean;
+  __device__ __forceinline__ void load() { mean = singular ? S[S_MEAN_R] : 0.0; }
+  __device__ __forceinline__ double operator()(int k) const {
+    return (f[k] & F_SOLV) ? (double)r[k] - mean : 0.0;
+  }
+};
+
 template <class T>
 struct BStored {
+  __device__ __forceinline__ void load() {}
   const T* b;
   __device__ __forceinline__ double operator()(int k) const { return (double)b[k]; }
 };
@@ -129,6 +196,7 @@ __device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo&
 template <class T, class B>
 __global__ void k_fine_pre(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x, T* __restrict__ res) {
+  bf.load();
   auto xv = [&](int k, int ii, int jj) -> double {
     return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
   };
@@ -150,6 +218,7 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
                               const T* __restrict__ x, T* __restrict__ xo,
                               const T* __restrict__ rcg, int singular, double* __restrict__ S,
                               RedBuf rb) {
+  bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   double acc[2] = {0, 0};
   FOR_CELLS(g) {
@@ -180,6 +249,7 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
 template <class T, class B>
 __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
                              const T* __restrict__ x, T* __restrict__ res) {
+  bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
@@ -191,6 +261,7 @@ __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
 template <class T, class B>
 __global__ void k_fine_wdb(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x) {
+  bf.load();
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
     x[c] = (T)(fine_wdinv(flags[c], i, j, g, w) * bf(c));
@@ -241,6 +312,134 @@ __global__ void k_fine_store_from_r(const T* __restrict__ r, const uint8_t* __re
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
     out[c] = (flags[c] & F_SOLV) ? (T)((double)r[c] - m) : (T)0;
+  }
+}
+
+// ---- coarse levels in one thread-block cluster ------------------------------
+// The coarse levels of a V-cycle hold few rows (<= ~16K) but wide Galerkin
+// stencils; as separate kernels each phase is launch- and latency-bound.  Here
+// one cluster of up to 16 CTAs runs every coarse phase -- restriction, first
+// smoothing sweep + residual, coarsest dense solve, prolongation, smoothing --
+// separated by hardware cluster barriers (no spin loops: every thread reaches
+// the same barriers, and the CTAs of a cluster are co-scheduled).  Vectors
+// written inside the kernel are read through L2 (ld.global.cg), never a stale L1.
+constexpr int kMaxCLevels = 12;
+
+template <class T>
+struct CLevel {
+  Ell<T> A, R, P;      // A, R: rows of this level; P: prolongation into the finer level
+  int la, lr, lp;      // lanes per row of each block
+  const T* wd;
+  T *b, *xa, *xb, *res;
+};
+
+template <class T>
+struct CTable {
+  CLevel<T> lv[kMaxCLevels];
+  int nlev;            // lv[0] is the first cluster level, lv[nlev-1] the coarsest
+  const T* res_in;     // residual of the level above lv[0]
+  const T* C;          // coarsest pseudo-inverse, row-major nc x nc
+  int nc;
+  int sweeps;
+};
+
+template <class T>
+__device__ __forceinline__ double ldcg(const T* p) { return (double)__ldcg(p); }
+
+// One ELL pass over all rows, distributed over the cluster's threads, L lanes
+// per row (runtime).  Every thread runs the same number of rounds.
+template <class T, class X, class W>
+__device__ __forceinline__ void cl_ell(const Ell<T>& E, int L, int gtid, int nthr, X x, W write) {
+  const int per = nthr / L;
+  const int lane = gtid % L, r0 = gtid / L;
+  for (int base = 0; base < E.n; base += per) {
+    const int row = base + r0;
+    double acc = 0.0;
+    if (row < E.n) {
+      if (E.rowmajor) {
+        const long o = (long)row * E.K;
+        for (int k = lane; k < E.K; k += L) acc += (double)E.val[o + k] * x(E.col[o + k]);
+      } else {
+        for (int k = lane; k < E.K; k += L) {
+          const long e = (long)k * E.n + row;
+          acc += (double)E.val[e] * x(E.col[e]);
+        }
+      }
+    }
+    for (int s = L >> 1; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s, L);
+    if (lane == 0 && row < E.n) write(row, acc);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_coarse_cycle(CTable<T> t) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int nthr = (int)(blockDim.x * cl.num_blocks());
+  const int gtid = (int)(cl.block_rank() * blockDim.x + threadIdx.x);
+  T* cur[kMaxCLevels];
+  // ---- down: restrict, first sweep from zero + residual (more sweeps if asked)
+  for (int l = 0; l < t.nlev; ++l) {
+    const CLevel<T>& L = t.lv[l];
+    const T* src = (l == 0) ? t.res_in : t.lv[l - 1].res;
+    cl_ell(L.R, L.lr, gtid, nthr, [&](int c) { return ldcg(src + c); },
+           [&](int row, double s) { L.b[row] = (T)s; });
+    cl.sync();
+    if (l == t.nlev - 1) {   // coarsest: x = C b, one warp per row
+      const int lane = gtid & 31;
+      for (int row = gtid >> 5; row < t.nc; row += nthr >> 5) {   // uniform within a warp
+        double acc = 0.0;
+        for (int k = lane; k < t.nc; k += 32) acc += (double)t.C[(long)row * t.nc + k] * ldcg(L.b + k);
+        acc = warp_sum(acc);
+        if (lane == 0) L.xa[row] = (T)acc;
+      }
+      cur[l] = L.xa;
+      cl.sync();
+      break;
+    }
+    cl_ell(L.A, L.la, gtid, nthr, [&](int c) { return (double)L.wd[c] * ldcg(L.b + c); },
+           [&](int row, double s) {
+             const double bx = ldcg(L.b + row);
+             L.xa[row] = (T)((double)L.wd[row] * bx);
+             L.res[row] = (T)(bx - s);
+           });
+    cl.sync();
+    T* a = L.xa;
+    T* o = L.xb;
+    if (t.sweeps > 1) {
+      for (int k = 1; k < t.sweeps; ++k) {
+        cl_ell(L.A, L.la, gtid, nthr, [&](int c) { return ldcg(a + c); },
+               [&](int row, double s) {
+                 o[row] = (T)(ldcg(a + row) + (double)L.wd[row] * (ldcg(L.b + row) - s));
+               });
+        cl.sync();
+        T* tmp = a; a = o; o = tmp;
+      }
+      cl_ell(L.A, L.la, gtid, nthr, [&](int c) { return ldcg(a + c); },
+             [&](int row, double s) { L.res[row] = (T)(ldcg(L.b + row) - s); });
+      cl.sync();
+    }
+    cur[l] = a;
+  }
+  // ---- up: prolong, smooth
+  for (int l = t.nlev - 2; l >= 0; --l) {
+    const CLevel<T>& L = t.lv[l];
+    const CLevel<T>& Lc = t.lv[l + 1];
+    T* xf = cur[l];
+    const T* xc = cur[l + 1];
+    cl_ell(Lc.P, Lc.lp, gtid, nthr, [&](int c) { return ldcg(xc + c); },
+           [&](int row, double s) { xf[row] = (T)(ldcg(xf + row) + s); });
+    cl.sync();
+    T* o = (xf == L.xa) ? L.xb : L.xa;
+    for (int k = 0; k < t.sweeps; ++k) {
+      cl_ell(L.A, L.la, gtid, nthr, [&](int c) { return ldcg(xf + c); },
+             [&](int row, double s) {
+               o[row] = (T)(ldcg(xf + row) + (double)L.wd[row] * (ldcg(L.b + row) - s));
+             });
+      cl.sync();
+      T* tmp = xf; xf = o; o = tmp;
+    }
+    cur[l] = xf;
   }
 }
 

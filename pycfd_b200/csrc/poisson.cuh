@@ -413,6 +413,50 @@ __global__ void k_ir_update(double* __restrict__ x, const float* __restrict__ e3
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) I[I_IR_IT] += 1;
 }
 
+// Device-side time-step control (pycfd/core/timestepper.py:94-142) from the
+// field statistics of the current state left in the scalar block:
+// dt = min(cfl/(umax/dx + vmax/dy), viscous limit, dt_cap) (the same double
+// operations, so the same dt), health flags on the unclamped dt (sticky bits:
+// 1 non-finite, 2 velocity above the divergence limit, 4 collapsed dt), the
+// clamp onto t_end, the donor-cell blend, and the clock.
+struct DtControl {
+  int adaptive;
+  double cfl, visc_limit, dt_cap, t_end, dx, dy;
+  int blend_mode;     // 0 fixed blend (below), 1 follow the Courant number
+  double blend;
+};
+
+__global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtControl c) {
+  if (threadIdx.x != 0) return;
+  const double umax = S[S_STAT0], vmax = S[S_STAT0 + 1];
+  double dt = c.dt_cap;
+  if (c.adaptive) {
+    const double scale = umax / c.dx + vmax / c.dy;
+    const double dt_conv = scale > 1.0e-12 ? c.cfl / scale : INFINITY;
+    dt = fmin(fmin(dt_conv, c.visc_limit), c.dt_cap);
+  }
+  int h = I[I_HEALTH];
+  if (S[S_STAT0 + 7] != 0.0) h |= 1;
+  if (fmax(umax, vmax) > 1.0e6) h |= 2;
+  if (dt < 1.0e-8) h |= 4;
+  I[I_HEALTH] = h;
+  const double t = S[S_T];
+  dt = fmin(dt, c.t_end - t);
+  S[S_DT] = dt;
+  S[S_BLEND] = c.blend_mode ? fmin(1.0, 1.2 * fmax(umax * dt / c.dx, vmax * dt / c.dy)) : c.blend;
+  S[S_T] = t + dt;
+  I[I_STEPS] += 1;
+  I[I_TOTAL_IT] = 0;
+}
+
+__global__ void k_set_clock(double* __restrict__ S, int* __restrict__ I, double t) {
+  if (threadIdx.x == 0) {
+    S[S_T] = t;
+    I[I_STEPS] = 0;
+    I[I_HEALTH] = 0;
+  }
+}
+
 // Start of a call: step parameters into the device scalar block (kernel
 // arguments, so no host synchronisation is needed) and the per-call counters.
 __global__ void k_begin(double* __restrict__ S, int* __restrict__ I, double dt, double blend) {

@@ -2,6 +2,7 @@
 // lists, multigrid upload), launch orchestration of the substep / projection /
 // Poisson solves, and the C ABI declared in include/pycfd_b200.h.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -39,7 +40,14 @@ static int fail(int code, const char* fmt, ...) {
                   __FILE__, __LINE__);                                               \
   } while (0)
 
-#define CHECK_LAUNCH() CU(cudaGetLastError())
+// Every kernel launch is followed by exactly one CHECK_LAUNCH, which also
+// counts it (pycfd_launch_count) -- recorded launches count once, when recorded.
+static std::atomic<long long> g_launches{0};
+#define CHECK_LAUNCH()          \
+  do {                          \
+    g_launches.fetch_add(1);    \
+    CU(cudaGetLastError());     \
+  } while (0)
 #define TRY(x)             \
   do {                     \
     int rc_ = (x);         \
@@ -119,6 +127,12 @@ struct pycfd_solver {
   float* Cf = nullptr;
   int nc = 0;
   int last_ir = 0;
+  // per-kernel timing of eager launches (measurement support)
+  int prof_id = 0;
+  std::vector<cudaEvent_t> prof_ev;
+  int prof_n = 0;
+  int cluster_from = 1 << 30;   // first level run inside the coarse cluster kernel
+  int cluster_size = 0;         // CTAs per cluster (0: not used)
   // CUDA-graph recording of whole steps
   bool capturing = false;
   cudaStream_t aux = nullptr;   // records the bodies of the solve loops
@@ -128,6 +142,8 @@ struct pycfd_solver {
     const void* key[5];
     cudaGraph_t graph;
     cudaGraphExec_t exec;
+    int adaptive;
+    DtControl ctl;
   };
   std::vector<GraphEntry> graphs;
 
@@ -216,6 +232,18 @@ void csr_transpose(int nrows, int ncols, const int64_t* indptr, const int32_t* i
 
 cudaStream_t st(void* stream) { return (cudaStream_t)stream; }
 
+// Bracket one launch of the profiled kernel with a pair of events on its
+// stream (eager launches only: recorded graphs carry no events).
+constexpr int kProfPairs = 4096;
+inline void prof_mark(pycfd_solver* s, int id, cudaStream_t stream) {
+  if (s->prof_id != id || s->capturing || s->prof_n >= 2 * kProfPairs) return;
+  if (s->prof_ev.empty()) {
+    s->prof_ev.resize(2 * kProfPairs);
+    for (auto& e : s->prof_ev) cudaEventCreate(&e);
+  }
+  cudaEventRecord(s->prof_ev[s->prof_n++], stream);
+}
+
 // ---- launch helpers ---------------------------------------------------------
 int launch_boundary(pycfd_solver* s, double* u, double* v, std::initializer_list<int> ops,
                     cudaStream_t stream) {
@@ -240,7 +268,7 @@ int grid1(pycfd_solver* s) { return grid_for(s->ncell(), kRedThreads, kMaxRedBlo
     default: { constexpr int L = 32; CALL; } break; \
   }
 
-inline int ell_grid(int n, int L) { return (int)(((long)n * L + 255) / 256); }
+inline int ell_grid(int n, int L) { return (int)std::min<long>(((long)n * L + 255) / 256, kWaveBlocks); }
 
 template <class T>
 const DevEll<T>& lvA(const Level& l);
@@ -279,6 +307,61 @@ const double* coarseC<double>(pycfd_solver* s) { return s->C; }
 template <>
 const float* coarseC<float>(pycfd_solver* s) { return s->Cf; }
 
+// Launch the cluster kernel over levels [lc, Lv) of the hierarchy; returns in
+// *out the buffer that holds x_lc afterwards (the kernel's ping-pong, replayed).
+template <class T>
+int launch_coarse_cluster(pycfd_solver* s, int lc, const T* res_in, T** out, cudaStream_t stream) {
+  const int Lv = (int)s->lv.size();
+  CTable<T> t{};
+  t.nlev = Lv - lc;
+  t.res_in = res_in;
+  t.C = coarseC<T>(s);
+  t.nc = s->nc;
+  t.sweeps = s->mg_sweeps;
+  for (int k = 0; k < t.nlev; ++k) {
+    Level& L = s->lv[lc + k];
+    CLevel<T>& c = t.lv[k];
+    if (lc + k < Lv - 1) {
+      c.A = lvA<T>(L).view();
+      c.la = lvA<T>(L).lanes;
+    }
+    c.R = lvR<T>(L).view();
+    c.lr = lvR<T>(L).lanes;
+    c.P = lvP<T>(L).view();
+    c.lp = lvP<T>(L).lanes;
+    c.wd = lvWd<T>(L);
+    LevelBuf<T>& B = lvB<T>(L);
+    c.b = B.b;
+    c.xa = B.xa;
+    c.xb = B.xb;
+    c.res = B.res;
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(s->cluster_size);
+  cfg.blockDim = dim3(1024);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = s->cluster_size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  prof_mark(s, 4, stream);
+  CU(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T>, t));
+  g_launches.fetch_add(1);
+  prof_mark(s, 4, stream);
+  // where x_lc ends: the first sweep writes xa; each further sweep swaps
+  LevelBuf<T>& B = lvB<T>(s->lv[lc]);
+  T* xf = B.xa;
+  if (lc < Lv - 1) {
+    if (s->mg_sweeps > 1 && ((s->mg_sweeps - 1) & 1)) xf = B.xb;
+    if (s->mg_sweeps & 1) xf = (xf == B.xa) ? B.xb : B.xa;
+  }
+  *out = xf;
+  return 0;
+}
+
 // One V-cycle from zero applied to the CG residual r: z_out gets the
 // unprojected result; the last fine sweep's finisher leaves mean(z) and r.z
 // in the scalar slots (pycfd/core/multigrid.py:430-474).
@@ -292,10 +375,10 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   // rows; the mean was left in S_MEAN_R by the kernel that produced r) into
   // level 0's b buffer; the fine kernels read it as a stored vector.
   LevelBuf<T>& B0 = lvB<T>(s->lv[0]);
-  k_fine_store_from_r<T><<<s->cgrid, s->cblock, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
-  CHECK_LAUNCH();
-  BStored<T> bf0{B0.b};
+  BFromRS<T> bf0{r, s->flags, s->S, s->singular, 0.0};
   if (Lv == 1) {
+    k_fine_store_from_r<T><<<s->cgrid, s->cblock, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
+    CHECK_LAUNCH();
     k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, B0.b, z_out);
     CHECK_LAUNCH();
     k_fine_sums<T, 1><<<s->cgrid, s->cblock, 0, stream>>>(z_out, s->flags, g, r, s->singular, s->S, s->rb());
@@ -306,37 +389,45 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   // ---- down ----
   T* cur[32];
   if (sw == 1) {
-    k_fine_pre<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
+    prof_mark(s, 3, stream);
+    k_fine_pre<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
+    prof_mark(s, 3, stream);
     CHECK_LAUNCH();
     cur[0] = B0.xa;
   } else {
-    k_fine_wdb<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
+    k_fine_wdb<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
     CHECK_LAUNCH();
     T* a = B0.xa;
     T* bb = B0.xb;
     for (int k = 1; k < sw; ++k) {
-      k_fine_smooth<T, BStored<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
-                                                                     s->singular, s->S, s->rb());
+      k_fine_smooth<T, BFromRS<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
+                                                                      s->singular, s->S, s->rb());
       CHECK_LAUNCH();
       std::swap(a, bb);
     }
-    k_fine_resid<T, BStored<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, a, B0.res);
+    k_fine_resid<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, a, B0.res);
     CHECK_LAUNCH();
     cur[0] = a;
   }
+  const int lc = std::max(1, std::min(s->cluster_from, Lv));
   for (int l = 1; l < Lv; ++l) {
+    if (l >= lc) {   // the rest of the cycle below l runs in one cluster
+      TRY(launch_coarse_cluster<T>(s, l, lvB<T>(s->lv[l - 1]).res, &cur[l], stream));
+      break;
+    }
     Level& Lc = s->lv[l];
     LevelBuf<T>& Bc = lvB<T>(Lc);
     const T* res_f = lvB<T>(s->lv[l - 1]).res;
     const DevEll<T>& R = lvR<T>(Lc);
-    ELL_DISPATCH(R.lanes, (k_ell_spmv<L, false, T><<<ell_grid(R.n, L), 256, 0, stream>>>(R.view(), res_f, Bc.b)));
-    CHECK_LAUNCH();
-    if (l == Lv - 1) {
-      k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, Bc.b, Bc.xa);
+    if (l == Lv - 1) {   // coarsest: restriction and dense solve in one block
+      k_restrict_dense<T><<<1, 1024, R.n * sizeof(double), stream>>>(R.view(), R.lanes, res_f, coarseC<T>(s),
+                                                                    Bc.b, Bc.xa);
       CHECK_LAUNCH();
       cur[l] = Bc.xa;
       break;
     }
+    ELL_DISPATCH(R.lanes, (k_ell_spmv<L, false, T><<<ell_grid(R.n, L), 256, 0, stream>>>(R.view(), res_f, Bc.b)));
+    CHECK_LAUNCH();
     const DevEll<T>& A = lvA<T>(Lc);
     T* wd = lvWd<T>(Lc);
     ELL_DISPATCH(A.lanes, (k_ell_pre<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bc.b, Bc.xa, Bc.res)));
@@ -355,7 +446,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     cur[l] = a;
   }
   // ---- up ----
-  for (int l = Lv - 2; l >= 0; --l) {
+  for (int l = std::min(Lv - 2, lc - 1); l >= 0; --l) {
     Level& Lf = s->lv[l];
     LevelBuf<T>& Bf = lvB<T>(Lf);
     const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
@@ -367,11 +458,15 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
       if (l == 0) {
         T* dst = (k == sw) ? z_out : other;
         if (k == sw)
-          k_fine_smooth<T, BStored<T>, 1><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
-                                                                         s->singular, s->S, s->rb());
+          {
+            prof_mark(s, 2, stream);
+            k_fine_smooth<T, BFromRS<T>, 1><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+                                                                          s->singular, s->S, s->rb());
+            prof_mark(s, 2, stream);
+          }
         else
-          k_fine_smooth<T, BStored<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
-                                                                         s->singular, s->S, s->rb());
+          k_fine_smooth<T, BFromRS<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+                                                                          s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         other = xf;
         xf = dst;
@@ -639,8 +734,10 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
                                                               s->S, s->I, s->rb(), L.ctl);
       } else {
         TRY(vcycle_pcg<double>(s, s->r, s->z, st));
+        prof_mark(s, 1, st);
         k_cg_pq<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->r, s->z, p_old, p_new, s->q, s->flags, g,
                                                           s->S, s->I, s->rb());
+        prof_mark(s, 1, st);
         CHECK_LAUNCH();
         k_cg_xr<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(x, s->r, p_new, s->q, keep, s->flags, g, cfg,
                                                           s->S, s->I, s->rb(), L.ctl);
@@ -673,6 +770,7 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
       Loop L;
       TRY(loop_handle(s, stream, &L));
       k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(s->b, s->flags, g, s->S, S_MEAN_B);
+      CHECK_LAUNCH();
       k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
       CHECK_LAUNCH();
       k_resnorm<<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb(), L.ctl);
@@ -710,6 +808,7 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
         } else {
           k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
                                                     s->I, s->rb());
+          CHECK_LAUNCH();
           k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
                                                     s->I, s->rb());
           CHECK_LAUNCH();
@@ -751,7 +850,9 @@ int project_impl(pycfd_solver* s, double* u, double* v, double* p, double dt_ove
   else TRY(solve_prepared(s, s->x, s->has_guess, stream));
   s->has_guess = true;
   const int gc = std::min(s->g.nx + 2, kMaxRedBlocks) + 1;   // rows + the ghost-ring block
+  prof_mark(s, 7, stream);
   k_correct<<<gc, 256, 0, stream>>>(u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
+  prof_mark(s, 7, stream);
   CHECK_LAUNCH();
   return 0;
 }
@@ -761,7 +862,9 @@ int substep_impl(pycfd_solver* s, StageIn uin, StageIn vin, double* us, double* 
   const Geo& g = s->g;
   dim3 blk(TJ, TI);
   dim3 grd((g.ny + 3 + TJ - 1) / TJ, (g.nx + 3 + TI - 1) / TI);
+  prof_mark(s, 6, stream);
   k_predictor<<<grd, blk, 0, stream>>>(uin, vin, us, vs, g, s->S);
+  prof_mark(s, 6, stream);
   CHECK_LAUNCH();
   TRY(launch_boundary(s, us, vs, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, stream));
   TRY(project_impl(s, us, vs, p, -1.0, stream));
@@ -782,6 +885,7 @@ int step_impl(pycfd_solver* s, const double* u0, const double* v0, double* u, do
     TRY(substep_impl(s, StageIn{s->us1, nullptr, 1.0, 0.0}, StageIn{s->vs1, nullptr, 1.0, 0.0}, s->us2,
                      s->vs2, p, stream));
     k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us2, 0.5, 0.5, u, nu);
+    CHECK_LAUNCH();
     k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs2, 0.5, 0.5, v, nv);
     CHECK_LAUNCH();
   } else {
@@ -791,6 +895,7 @@ int step_impl(pycfd_solver* s, const double* u0, const double* v0, double* u, do
     TRY(substep_impl(s, StageIn{u0, s->us2, 0.75, 0.25}, StageIn{v0, s->vs2, 0.75, 0.25}, s->us1, s->vs1,
                      p, stream));
     k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us1, 1.0 / 3.0, 2.0 / 3.0, u, nu);
+    CHECK_LAUNCH();
     k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs1, 1.0 / 3.0, 2.0 / 3.0, v, nv);
     CHECK_LAUNCH();
   }
@@ -810,6 +915,7 @@ int pycfd_version(void) { return 1; }
 
 int pycfd_solver_destroy(pycfd_solver* s) {
   if (!s) return 0;
+  for (auto& e : s->prof_ev) cudaEventDestroy(e);
   for (auto& e : s->graphs) {
     cudaGraphExecDestroy(e.exec);
     cudaGraphDestroy(e.graph);
@@ -1058,6 +1164,45 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
     if ((rc = upload(s, &s->C, cm.data(), cm.size())) || (rc = upload(s, &s->Cf, cf.data(), cf.size())))
       return bail(rc);
   }
+  if (mg && d->coarse_cluster_rows > 0 && s->lv.size() > 1) {
+    // coarse levels: first level (>= 1) with at most coarse_cluster_rows rows
+    for (int l = 1; l < (int)s->lv.size(); ++l)
+      if (s->lv[l].n <= d->coarse_cluster_rows) {
+        s->cluster_from = l;
+        break;
+      }
+    int best = 0;
+    for (int cs : {16, 8}) {
+      if (cs == 16) {
+        if (cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+      }
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(1024);
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, k_coarse_cycle<double>, &cfg) == cudaSuccess &&
+          nclusters > 0) {
+        best = cs;
+        break;
+      }
+      cudaGetLastError();
+    }
+    s->cluster_size = best;
+    if (!best) s->cluster_from = 1 << 30;
+  }
   if (s->precision == PCFD_MIXED) {
     if ((rc = dalloc(s, &s->r32, n)) || (rc = dalloc(s, &s->x32, n)) || (rc = dalloc(s, &s->pa32, n)) ||
         (rc = dalloc(s, &s->pb32, n)) || (rc = dalloc(s, &s->q32, n)) || (rc = dalloc(s, &s->z32, n)))
@@ -1174,7 +1319,7 @@ int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double
   const void* key[5] = {u0, v0, u, v, p};
   pycfd_solver::GraphEntry* hit = nullptr;
   for (auto& e : s->graphs)
-    if (!memcmp(e.key, key, sizeof key)) hit = &e;
+    if (!e.adaptive && !memcmp(e.key, key, sizeof key)) hit = &e;
   if (!hit) {
     // Record on the solver's own stream (the caller's may be the legacy default
     // stream, which cannot be captured); recording executes nothing.
@@ -1198,7 +1343,7 @@ int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double
       cudaGraphDestroy(s->graphs.front().graph);
       s->graphs.erase(s->graphs.begin());
     }
-    pycfd_solver::GraphEntry e;
+    pycfd_solver::GraphEntry e{};
     memcpy(e.key, key, sizeof key);
     e.graph = graph;
     e.exec = exec;
@@ -1206,6 +1351,82 @@ int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double
     hit = &s->graphs.back();
   }
   CU(cudaGraphLaunch(hit->exec, sm));
+  return 0;
+}
+
+int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
+                        double* p, const pycfd_dt_control* ctl, void* stream) {
+  if (!s || !u0 || !v0 || !u || !v || !p || !ctl) return fail(PCFD_E_ARG, "bad arguments");
+  if (u0 == u || v0 == v) return fail(PCFD_E_ARG, "step outputs must not alias its inputs");
+  if (s->solver_kind == PCFD_SOLVER_JACOBI || s->solver_kind == PCFD_SOLVER_SOR)
+    return fail(PCFD_E_UNSUPPORTED, "device-side stepping needs a cg, multigrid or mgcg solver");
+  cudaStream_t sm = st(stream);
+  DtControl c{ctl->adaptive, ctl->cfl, ctl->visc_limit, ctl->dt_cap, ctl->t_end, s->g.dx, s->g.dy,
+              ctl->blend_mode, ctl->blend};
+  // key: the five addresses plus the control values (recorded into the graph)
+  const void* key[5] = {u0, v0, u, v, p};
+  pycfd_solver::GraphEntry* hit = nullptr;
+  for (auto& e : s->graphs)
+    if (e.adaptive && !memcmp(e.key, key, sizeof key) && !memcmp(&e.ctl, &c, sizeof c)) hit = &e;
+  if (!hit) {
+    if (!s->aux) CU(cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking));
+    if (!s->rec) CU(cudaStreamCreateWithFlags(&s->rec, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(s->rec, cudaStreamCaptureModeThreadLocal));
+    s->capturing = true;
+    int rc = 0;
+    k_field_stats<<<std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, s->rec>>>(
+        u0, v0, nullptr, nullptr, nullptr, s->solid, s->g, s->rb(), s->S);
+    if (cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "stats launch failed");
+    g_launches.fetch_add(1);
+    k_adaptive_dt<<<1, 32, 0, s->rec>>>(s->S, s->I, c);
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "dt launch failed");
+    g_launches.fetch_add(1);
+    if (!rc) rc = step_impl(s, u0, v0, u, v, p, s->rec);
+    s->capturing = false;
+    const cudaError_t ec = cudaStreamEndCapture(s->rec, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(PCFD_E_CUDA, "step capture failed: %s", cudaGetErrorString(ec));
+    cudaGraphExec_t exec = nullptr;
+    CU(cudaGraphInstantiate(&exec, graph, 0));
+    if (s->graphs.size() >= 6) {
+      cudaGraphExecDestroy(s->graphs.front().exec);
+      cudaGraphDestroy(s->graphs.front().graph);
+      s->graphs.erase(s->graphs.begin());
+    }
+    pycfd_solver::GraphEntry e{};
+    memcpy(e.key, key, sizeof key);
+    e.graph = graph;
+    e.exec = exec;
+    e.adaptive = 1;
+    e.ctl = c;
+    s->graphs.push_back(e);
+    hit = &s->graphs.back();
+  }
+  CU(cudaGraphLaunch(hit->exec, sm));
+  return 0;
+}
+
+int pycfd_set_clock(pycfd_solver* s, double t, void* stream) {
+  if (!s) return fail(PCFD_E_ARG, "bad arguments");
+  k_set_clock<<<1, 32, 0, st(stream)>>>(s->S, s->I, t);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_get_clock(pycfd_solver* s, double* t, double* dt, int* steps, int* health, void* stream) {
+  if (!s || !t || !dt || !steps || !health) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  CU(cudaMemcpyAsync(s->hS, s->S, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, sm));
+  CU(cudaMemcpyAsync(s->hI, s->I, sizeof(int) * I_COUNT, cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  *t = s->hS[S_T];
+  *dt = s->hS[S_DT];
+  *steps = s->hI[I_STEPS];
+  *health = s->hI[I_HEALTH];
   return 0;
 }
 
@@ -1228,6 +1449,30 @@ int pycfd_step_host(pycfd_solver* s, const double* u0h, const double* v0h, doubl
   CU(cudaMemcpyAsync(vh, s->hv, nv * sizeof(double), cudaMemcpyDeviceToHost, sm));
   CU(cudaMemcpyAsync(ph, s->hp, np * sizeof(double), cudaMemcpyDeviceToHost, sm));
   CU(cudaStreamSynchronize(sm));
+  return 0;
+}
+
+long long pycfd_launch_count(void) { return g_launches.load(); }
+
+int pycfd_profile_kernel(pycfd_solver* s, int kernel_id) {
+  if (!s || kernel_id < 0 || kernel_id > 7) return fail(PCFD_E_ARG, "bad arguments");
+  s->prof_id = kernel_id;
+  s->prof_n = 0;
+  return 0;
+}
+
+int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* stream) {
+  if (!s || !total_ms || !launches) return fail(PCFD_E_ARG, "bad arguments");
+  CU(cudaStreamSynchronize(st(stream)));
+  double t = 0.0;
+  for (int k = 0; k + 1 < s->prof_n; k += 2) {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, s->prof_ev[k], s->prof_ev[k + 1]));
+    t += ms;
+  }
+  *total_ms = t;
+  *launches = s->prof_n / 2;
+  s->prof_n = 0;
   return 0;
 }
 

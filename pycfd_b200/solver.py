@@ -38,6 +38,10 @@ class GpuOptions:
     #: record each step once into a CUDA graph (device-side Poisson loops) and
     #: replay it; ``advance()`` and the time stepper use it.
     graphs: bool = True
+    #: multigrid levels with at most this many rows run inside one thread-block
+    #: cluster per V-cycle (0, the default: one kernel per phase on every level;
+    #: the cluster form is bit-identical but slower while coarse stencils are wide).
+    coarse_cluster_rows: int = 0
 
 
 def _torch():
@@ -249,6 +253,7 @@ class ProjectionSolver:
         d.time_scheme = _lib.SCHEME_CODES[TimeScheme(cfg.time_scheme).value]
         d.precision = 1 if self.options.precision == "mixed" else 0
         d.inner_tol = self.options.inner_tol
+        d.coarse_cluster_rows = int(self.options.coarse_cluster_rows)
         if self._levels is not None:
             arr = (_lib.MgLevel * len(self._levels))()
             for l, lv in enumerate(self._levels):
@@ -431,6 +436,62 @@ class ProjectionSolver:
                                             float(self._blend), _stream()))
         self._read_stats()
         return FlowField(self.mesh, u, v, p, fields.t + dt, fields.step + 1)
+
+    def dt_control(self):
+        """Device-side time-step control matching :class:`TimeStepper` for this configuration."""
+        cfg = self.config
+        nu = self.nu
+        dx, dy = self.mesh.dx, self.mesh.dy
+        visc = float("inf") if nu <= 0 else 0.8 / (2.0 * nu * (1.0 / dx ** 2 + 1.0 / dy ** 2))
+        c = _lib.DtControl()
+        c.adaptive = int(bool(cfg.adaptive_dt))
+        c.cfl = cfg.cfl_max
+        c.visc_limit = visc
+        c.dt_cap = cfg.dt
+        c.t_end = float("inf")
+        central = AdvectionScheme(cfg.advection_scheme) is AdvectionScheme.CENTRAL
+        c.blend_mode = 0 if (central or cfg.upwind_blend is not None) else 1
+        c.blend = 0.0 if central else float(cfg.upwind_blend or 0.0)
+        return c
+
+    def set_clock(self, t: float = 0.0) -> None:
+        """Reset the device clock, step counter and health flags of device-side stepping."""
+        _lib.check(self._L.pycfd_set_clock(self._h, float(t), _stream()))
+
+    def clock(self):
+        """``(t, last dt, steps, health bits)`` of device-side stepping (synchronises)."""
+        t, dt, n, h = C.c_double(), C.c_double(), C.c_int(), C.c_int()
+        _lib.check(self._L.pycfd_get_clock(self._h, C.byref(t), C.byref(dt), C.byref(n),
+                                           C.byref(h), _stream()))
+        return t.value, dt.value, n.value, h.value
+
+    def advance_adaptive(self, fields: FlowField, ctl=None) -> FlowField:
+        """One step with dt chosen on the device (no host round trip), into the ring buffers.
+
+        The dt, health checks and clock follow :class:`TimeStepper` exactly but live
+        on the device; read them with :meth:`clock`.  The returned field's ``t`` is
+        not known on the host (``nan``) until the clock is read.
+        """
+        if self._ring is None:
+            self._ring = [self._empty_state(), self._empty_state()]
+        if ctl is None:
+            ctl = self._ctl = getattr(self, "_ctl", None) or self.dt_control()
+        out = self._ring[0] if fields.u.data_ptr() != self._ring[0][0].data_ptr() else self._ring[1]
+        u, v, p = out
+        _lib.check(self._L.pycfd_step_adaptive(self._h, _lib.ptr(fields.u), _lib.ptr(fields.v),
+                                               _lib.ptr(u), _lib.ptr(v), _lib.ptr(p), C.byref(ctl),
+                                               _stream()))
+        return FlowField(self.mesh, u, v, p, float("nan"), fields.step + 1)
+
+    def launches_per_step(self, fields: FlowField, dt: float) -> int:
+        """Kernels one step of ``fields`` launches, counted on an eager step (inputs untouched).
+
+        A recorded step replays the same kernels; the eager step updates the
+        warm start of the next solve like any step does.
+        """
+        before = self._L.pycfd_launch_count()
+        self.step(fields, dt)
+        return int(self._L.pycfd_launch_count() - before)
 
     def step_host(self, u0: np.ndarray, v0: np.ndarray, dt: float):
         """The same step on host arrays: copies in, steps, copies ``(u, v, p)`` out."""

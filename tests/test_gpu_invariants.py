@@ -193,3 +193,23 @@ def test_graph_replay_matches_eager_bitwise(solver):
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
     assert fa == fb and ia == ib
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_coarse_cluster_matches_per_level_kernels(precision):
+    """Coarse levels run in one thread-block cluster give the per-kernel V-cycle bit for bit."""
+    from pycfd_b200.solver import GpuOptions
+    d = dict(nx=96, ny=64, lx=1.5, ly=1.0, re=200.0, pressure_solver="mgcg", poisson_tol=1e-12,
+             boundary_config=cases.bcs(top=("moving_wall", 1.0)))
+    out = []
+    for rows in (0, 20000):   # per-level kernels vs the coarse cluster
+        s = _solver(_cfg(d), options=GpuOptions(precision=precision, coarse_cluster_rows=rows))
+        f = s.initialize()
+        its = []
+        for _ in range(4):
+            f = s.advance(f, 2e-3)
+            its.append(s.last_stats.total_iterations)
+        out.append((f.numpy(), its))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert out[0][1] == out[1][1]
