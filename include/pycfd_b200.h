@@ -111,6 +111,8 @@ typedef struct {
     int coarse_cluster_rows;                  /* levels with at most this many rows run
                                                  as one thread-block cluster per V-cycle;
                                                  0 = one kernel per phase    */
+    int sequential_launch;                    /* 1: plain stream order between kernels;
+                                                 0: programmatic dependent launch */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */

@@ -53,7 +53,7 @@ class SolverDesc(C.Structure):
                 ("mg_sweeps", C.c_int), ("time_scheme", C.c_int), ("precision", C.c_int),
                 ("inner_tol", C.c_double), ("n_levels", C.c_int),
                 ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp),
-                ("coarse_cluster_rows", C.c_int)]
+                ("coarse_cluster_rows", C.c_int), ("sequential_launch", C.c_int)]
 
 
 class DtControl(C.Structure):

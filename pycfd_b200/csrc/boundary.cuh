@@ -217,6 +217,7 @@ __device__ void bc_wrap_faces(double* u, double* v, const Geo& g) {
 
 __global__ void __launch_bounds__(1024) k_boundary(double* u, double* v, Geo g, BcTable T,
                                                    BcProgram prog, double* S) {
+  pdl_begin();
   for (int s = 0; s < 8 && prog.op[s] != OP_END; ++s) {
     switch (prog.op[s]) {
       case OP_VEL_PRED: bc_velocity(u, v, g, T, true); break;

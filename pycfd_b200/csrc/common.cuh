@@ -63,6 +63,17 @@ constexpr int kMaxRedBlocks = 1184;   // 148 SMs x 8 resident blocks (partials b
 constexpr int kWaveBlocks = 592;
 constexpr int kRedThreads = 256;
 
+// Programmatic dependent launch (sm_90+): a kernel launched with the
+// programmatic-serialization attribute may be scheduled while its predecessor
+// is still running.  Every kernel therefore first waits for the predecessor's
+// completion and memory (a no-op without the attribute), then allows its own
+// successor to be scheduled, so the launch latency between dependent kernels
+// overlaps execution.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

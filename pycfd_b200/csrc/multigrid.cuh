@@ -61,6 +61,7 @@ __device__ __forceinline__ double ell_row(const Ell<T>& E, int row, int lane, X 
 template <int L, class T>
 __global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                           T* __restrict__ x, T* __restrict__ res) {
+  pdl_begin();
   FOR_ELL_ROWS(A, L) {
     const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
     if (lane == 0 && row < A.n) {
@@ -75,6 +76,7 @@ __global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restric
 template <int L, class T>
 __global__ void k_ell_smooth(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                              const T* __restrict__ x, T* __restrict__ xo) {
+  pdl_begin();
   FOR_ELL_ROWS(A, L) {
     const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
     if (lane == 0 && row < A.n) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
@@ -85,6 +87,7 @@ __global__ void k_ell_smooth(Ell<T> A, const T* __restrict__ wd, const T* __rest
 template <int L, class T>
 __global__ void k_ell_resid(Ell<T> A, const T* __restrict__ b, const T* __restrict__ x,
                             T* __restrict__ res) {
+  pdl_begin();
   FOR_ELL_ROWS(A, L) {
     const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
     if (lane == 0 && row < A.n) res[row] = (T)((double)b[row] - s);
@@ -94,6 +97,7 @@ __global__ void k_ell_resid(Ell<T> A, const T* __restrict__ b, const T* __restri
 // y = M x (restriction with M = R), or y += M x (prolongation with M = P).
 template <int L, bool ADD, class T>
 __global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y) {
+  pdl_begin();
   FOR_ELL_ROWS(M, L) {
     const double s = ell_row<L>(M, row, lane, [&](int c) { return (double)x[c]; });
     if (lane == 0 && row < M.n) y[row] = ADD ? (T)((double)y[row] + s) : (T)s;
@@ -105,6 +109,7 @@ __global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y)
 // One warp per row of C (row-major), lanes over its columns.
 template <class T>
 __global__ void k_dense(const T* __restrict__ C, int n, const T* __restrict__ b, T* __restrict__ x) {
+  pdl_begin();
   const int lane = threadIdx.x & 31;
   for (int row = threadIdx.x >> 5; row < n; row += blockDim.x >> 5) {
     double acc = 0.0;
@@ -119,6 +124,7 @@ __global__ void k_dense(const T* __restrict__ C, int n, const T* __restrict__ b,
 template <class T>
 __global__ void k_restrict_dense(Ell<T> R, int L, const T* __restrict__ res, const T* __restrict__ C,
                                  T* __restrict__ b, T* __restrict__ x) {
+  pdl_begin();
   extern __shared__ double sb[];
   // restriction: L lanes per row, the same partial-sum order as the ELL kernels
   const int lane = threadIdx.x % L, per = blockDim.x / L;
@@ -196,6 +202,7 @@ __device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo&
 template <class T, class B>
 __global__ void k_fine_pre(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x, T* __restrict__ res) {
+  pdl_begin();
   bf.load();
   auto xv = [&](int k, int ii, int jj) -> double {
     return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
@@ -218,6 +225,7 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
                               const T* __restrict__ x, T* __restrict__ xo,
                               const T* __restrict__ rcg, int singular, double* __restrict__ S,
                               RedBuf rb) {
+  pdl_begin();
   bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   double acc[2] = {0, 0};
@@ -249,6 +257,7 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
 template <class T, class B>
 __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
                              const T* __restrict__ x, T* __restrict__ res) {
+  pdl_begin();
   bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   FOR_CELLS(g) {
@@ -261,6 +270,7 @@ __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
 template <class T, class B>
 __global__ void k_fine_wdb(B bf, const uint8_t* __restrict__ flags, Geo g, double w,
                            T* __restrict__ x) {
+  pdl_begin();
   bf.load();
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
@@ -271,6 +281,7 @@ __global__ void k_fine_wdb(B bf, const uint8_t* __restrict__ flags, Geo g, doubl
 // Materialise a fine right-hand side (single-level hierarchies only).
 template <class T, class B>
 __global__ void k_fine_store(B bf, Geo g, T* __restrict__ out) {
+  pdl_begin();
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
     out[c] = (T)bf(c);
@@ -283,6 +294,7 @@ template <class T, int MODE>
 __global__ void k_fine_sums(const T* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
                             const T* __restrict__ rcg, int singular, double* __restrict__ S,
                             RedBuf rb) {
+  pdl_begin();
   double acc[2] = {0, 0};
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
@@ -308,6 +320,7 @@ __global__ void k_fine_sums(const T* __restrict__ x, const uint8_t* __restrict__
 template <class T>
 __global__ void k_fine_store_from_r(const T* __restrict__ r, const uint8_t* __restrict__ flags, Geo g,
                                     const double* __restrict__ S, int singular, T* __restrict__ out) {
+  pdl_begin();
   const double m = singular ? S[S_MEAN_R] : 0.0;
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
@@ -373,6 +386,7 @@ __device__ __forceinline__ void cl_ell(const Ell<T>& E, int L, int gtid, int nth
 
 template <class T>
 __global__ void __launch_bounds__(1024) k_coarse_cycle(CTable<T> t) {
+  pdl_begin();
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const int nthr = (int)(blockDim.x * cl.num_blocks());

@@ -46,6 +46,7 @@ __global__ void k_rhs_init(double* __restrict__ b, T* __restrict__ x, T* __restr
                            const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                            int has_x0, double* __restrict__ S, int* __restrict__ I, RedBuf rb,
                            LoopCtl loop) {
+  pdl_begin();
   const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
   double acc[4] = {0, 0, 0, 0};
   FOR_CELLS(g) {
@@ -91,6 +92,7 @@ __global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
                         const T* __restrict__ p_old, T* __restrict__ p_new, T* __restrict__ q,
                         const uint8_t* __restrict__ flags, Geo g, double* __restrict__ S,
                         const int* __restrict__ I, RedBuf rb) {
+  pdl_begin();
   const bool first = I[I_IT] == 0;
   const double beta = first ? 0.0 : S[S_RHO] / S[S_RHO_PREV];
   const double mz = S[S_MEAN_Z];
@@ -127,6 +129,7 @@ __global__ void k_cg_xr(T* __restrict__ x, T* __restrict__ r, const T* __restric
                         const T* __restrict__ q, T* __restrict__ p_keep,
                         const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                         double* __restrict__ S, int* __restrict__ I, RedBuf rb, LoopCtl loop) {
+  pdl_begin();
   const double alpha = S[S_ALPHA];
   double acc[3] = {0, 0, 0};
   FOR_CELLS(g) {
@@ -165,6 +168,7 @@ template <class T>
 __global__ void k_finish_stats(const T* __restrict__ x, const double* __restrict__ b,
                                const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                                int pcg, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  pdl_begin();
   const bool zero = I[I_ZERO_RHS] != 0;
   auto xv = [&](int k, int, int) -> double { return zero ? 0.0 : (double)x[k]; };
   double acc[2] = {0, 0};
@@ -193,6 +197,7 @@ template <class T>
 __global__ void k_finish_apply(T* x, double* xo,
                                const uint8_t* __restrict__ flags, Geo g,
                                const double* __restrict__ S, const int* __restrict__ I) {
+  pdl_begin();
   const bool zero = I[I_ZERO_RHS] != 0;
   const double m = S[S_MEAN_X];
   FOR_CELLS(g) {
@@ -211,6 +216,7 @@ __global__ void k_stationary_init(double* __restrict__ b, double* __restrict__ x
                                   const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
                                   int has_x0, int project_x0, double* __restrict__ S,
                                   int* __restrict__ I, RedBuf rb) {
+  pdl_begin();
   const double mean = cfg.singular ? S[S_MEAN_B] : 0.0;
   double acc[3] = {0, 0, 0};
   FOR_CELLS(g) {
@@ -244,6 +250,7 @@ __global__ void k_jacobi_sweep(const double* __restrict__ xin, double* __restric
                                const double* __restrict__ b, const uint8_t* __restrict__ flags,
                                Geo g, double omega, int singular, double* __restrict__ S,
                                int* __restrict__ I, RedBuf rb) {
+  pdl_begin();
   const double m = S[S_MEAN_X];
   auto xe = [&](int k, int, int) -> double { return (flags[k] & F_SOLV) ? xin[k] - m : xin[k]; };
   double acc[1] = {0.0};
@@ -270,6 +277,7 @@ __global__ void k_jacobi_sweep(const double* __restrict__ xin, double* __restric
 __global__ void k_sor_half(double* __restrict__ x, const double* __restrict__ b,
                            const uint8_t* __restrict__ flags, Geo g, double omega, int colour,
                            int singular, double* __restrict__ S, int* __restrict__ I, RedBuf rb) {
+  pdl_begin();
   const double m = S[S_MEAN_X];
   // red pass: every value is in the old frame; black pass: red neighbours are new.
   auto xe = [&](int k, int ii, int jj) -> double {
@@ -312,6 +320,7 @@ __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
                           const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg, int mode,
                           int count_cycle, int pending, double* __restrict__ S, int* __restrict__ I,
                           RedBuf rb, LoopCtl loop) {
+  pdl_begin();
   const double m = pending ? S[S_MEAN_X] : 0.0;
   auto xe = [&](int k, int, int) -> double { return (flags[k] & F_SOLV) ? x[k] - m : 0.0; };
   double acc[1] = {0.0};
@@ -352,6 +361,7 @@ __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
                               double inner_tol, int max_passes, int first, int has_x0,
                               double* __restrict__ S, int* __restrict__ I, RedBuf rb,
                               LoopCtl outer) {
+  pdl_begin();
   const double mean = (first && cfg.singular) ? S[S_MEAN_B] : 0.0;
   double acc[3] = {0, 0, 0};
   FOR_CELLS(g) {
@@ -400,12 +410,14 @@ __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
 
 // Arm the inner solve's loop from the flags of the last refinement pass.
 __global__ void k_ir_arm(const int* __restrict__ I, LoopCtl inner) {
+  pdl_begin();
   if (threadIdx.x == 0) inner.set(!I[I_DONE]);
 }
 
 // x += e (FP32 correction promoted to FP64) on solvable rows; count the pass.
 __global__ void k_ir_update(double* __restrict__ x, const float* __restrict__ e32,
                             const uint8_t* __restrict__ flags, Geo g, int* __restrict__ I) {
+  pdl_begin();
   FOR_CELLS(g) {
     const int c = i * g.ny + j;
     if (flags[c] & F_SOLV) x[c] = x[c] + (double)e32[c];
@@ -427,6 +439,7 @@ struct DtControl {
 };
 
 __global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtControl c) {
+  pdl_begin();
   if (threadIdx.x != 0) return;
   const double umax = S[S_STAT0], vmax = S[S_STAT0 + 1];
   double dt = c.dt_cap;
@@ -450,6 +463,7 @@ __global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtCon
 }
 
 __global__ void k_set_clock(double* __restrict__ S, int* __restrict__ I, double t) {
+  pdl_begin();
   if (threadIdx.x == 0) {
     S[S_T] = t;
     I[I_STEPS] = 0;
@@ -460,6 +474,7 @@ __global__ void k_set_clock(double* __restrict__ S, int* __restrict__ I, double 
 // Start of a call: step parameters into the device scalar block (kernel
 // arguments, so no host synchronisation is needed) and the per-call counters.
 __global__ void k_begin(double* __restrict__ S, int* __restrict__ I, double dt, double blend) {
+  pdl_begin();
   if (threadIdx.x == 0) {
     S[S_DT] = dt;
     S[S_BLEND] = blend;
@@ -470,6 +485,7 @@ __global__ void k_begin(double* __restrict__ S, int* __restrict__ I, double dt, 
 // Apply a pending mean: x <- x - S[slot] on solvable rows.
 __global__ void k_apply_mean(double* __restrict__ x, const uint8_t* __restrict__ flags, Geo g,
                              const double* __restrict__ S, int slot) {
+  pdl_begin();
   const double m = S[slot];
   FOR_CELLS(g) {
     const int c = i * g.ny + j;

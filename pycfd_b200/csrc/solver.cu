@@ -131,6 +131,7 @@ struct pycfd_solver {
   int prof_id = 0;
   std::vector<cudaEvent_t> prof_ev;
   int prof_n = 0;
+  int pdl = 1;                  // programmatic dependent launch between step kernels
   int cluster_from = 1 << 30;   // first level run inside the coarse cluster kernel
   int cluster_size = 0;         // CTAs per cluster (0: not used)
   // CUDA-graph recording of whole steps
@@ -245,13 +246,31 @@ inline void prof_mark(pycfd_solver* s, int id, cudaStream_t stream) {
 }
 
 // ---- launch helpers ---------------------------------------------------------
+// Launch a kernel of the step with the programmatic-serialization attribute
+// (see pdl_begin): the launch of a dependent kernel overlaps its predecessor.
+// Launch errors surface through the CHECK_LAUNCH that follows every launch.
+template <class... P, class... A>
+inline void pdl_launch(pycfd_solver* s, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t stream, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = s->pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 int launch_boundary(pycfd_solver* s, double* u, double* v, std::initializer_list<int> ops,
                     cudaStream_t stream) {
   BcProgram prog{};
   int k = 0;
   for (int op : ops) prog.op[k++] = op;
   prog.op[k] = OP_END;
-  k_boundary<<<1, 1024, 0, stream>>>(u, v, s->g, s->bc, prog, s->S);
+  pdl_launch(s, k_boundary, 1, 1024, 0, stream, u, v, s->g, s->bc, prog, s->S);
   CHECK_LAUNCH();
   return 0;
 }
@@ -377,11 +396,11 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   LevelBuf<T>& B0 = lvB<T>(s->lv[0]);
   BFromRS<T> bf0{r, s->flags, s->S, s->singular, 0.0};
   if (Lv == 1) {
-    k_fine_store_from_r<T><<<s->cgrid, s->cblock, 0, stream>>>(r, s->flags, g, s->S, s->singular, B0.b);
+    pdl_launch(s, k_fine_store_from_r<T>, s->cgrid, s->cblock, 0, stream, r, s->flags, g, s->S, s->singular, B0.b);
     CHECK_LAUNCH();
-    k_dense<T><<<1, 256, 0, stream>>>(coarseC<T>(s), s->nc, B0.b, z_out);
+    pdl_launch(s, k_dense<T>, 1, 256, 0, stream, coarseC<T>(s), s->nc, B0.b, z_out);
     CHECK_LAUNCH();
-    k_fine_sums<T, 1><<<s->cgrid, s->cblock, 0, stream>>>(z_out, s->flags, g, r, s->singular, s->S, s->rb());
+    pdl_launch(s, k_fine_sums<T, 1>, s->cgrid, s->cblock, 0, stream, z_out, s->flags, g, r, s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     return 0;
   }
@@ -390,22 +409,22 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   T* cur[32];
   if (sw == 1) {
     prof_mark(s, 3, stream);
-    k_fine_pre<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa, B0.res);
+    pdl_launch(s, k_fine_pre<T, BFromRS<T>>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, B0.xa, B0.res);
     prof_mark(s, 3, stream);
     CHECK_LAUNCH();
     cur[0] = B0.xa;
   } else {
-    k_fine_wdb<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, B0.xa);
+    pdl_launch(s, k_fine_wdb<T, BFromRS<T>>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, B0.xa);
     CHECK_LAUNCH();
     T* a = B0.xa;
     T* bb = B0.xb;
     for (int k = 1; k < sw; ++k) {
-      k_fine_smooth<T, BFromRS<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, a, bb, r,
+      pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, a, bb, r,
                                                                       s->singular, s->S, s->rb());
       CHECK_LAUNCH();
       std::swap(a, bb);
     }
-    k_fine_resid<T, BFromRS<T>><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, a, B0.res);
+    pdl_launch(s, k_fine_resid<T, BFromRS<T>>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, a, B0.res);
     CHECK_LAUNCH();
     cur[0] = a;
   }
@@ -420,27 +439,27 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     const T* res_f = lvB<T>(s->lv[l - 1]).res;
     const DevEll<T>& R = lvR<T>(Lc);
     if (l == Lv - 1) {   // coarsest: restriction and dense solve in one block
-      k_restrict_dense<T><<<1, 1024, R.n * sizeof(double), stream>>>(R.view(), R.lanes, res_f, coarseC<T>(s),
+      pdl_launch(s, k_restrict_dense<T>, 1, 1024, R.n * sizeof(double), stream, R.view(), R.lanes, res_f, coarseC<T>(s),
                                                                     Bc.b, Bc.xa);
       CHECK_LAUNCH();
       cur[l] = Bc.xa;
       break;
     }
-    ELL_DISPATCH(R.lanes, (k_ell_spmv<L, false, T><<<ell_grid(R.n, L), 256, 0, stream>>>(R.view(), res_f, Bc.b)));
+    ELL_DISPATCH(R.lanes, (pdl_launch(s, k_ell_spmv<L, false, T>, ell_grid(R.n, L), 256, 0, stream, R.view(), res_f, Bc.b)));
     CHECK_LAUNCH();
     const DevEll<T>& A = lvA<T>(Lc);
     T* wd = lvWd<T>(Lc);
-    ELL_DISPATCH(A.lanes, (k_ell_pre<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bc.b, Bc.xa, Bc.res)));
+    ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_pre<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bc.b, Bc.xa, Bc.res)));
     CHECK_LAUNCH();
     T* a = Bc.xa;
     T* bb = Bc.xb;
     if (sw > 1) {
       for (int k = 1; k < sw; ++k) {
-        ELL_DISPATCH(A.lanes, (k_ell_smooth<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bc.b, a, bb)));
+        ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bc.b, a, bb)));
         CHECK_LAUNCH();
         std::swap(a, bb);
       }
-      ELL_DISPATCH(A.lanes, (k_ell_resid<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), Bc.b, a, Bc.res)));
+      ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_resid<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), Bc.b, a, Bc.res)));
       CHECK_LAUNCH();
     }
     cur[l] = a;
@@ -451,7 +470,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     LevelBuf<T>& Bf = lvB<T>(Lf);
     const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
     T* xf = cur[l];
-    ELL_DISPATCH(P.lanes, (k_ell_spmv<L, true, T><<<ell_grid(P.n, L), 256, 0, stream>>>(P.view(), cur[l + 1], xf)));
+    ELL_DISPATCH(P.lanes, (pdl_launch(s, k_ell_spmv<L, true, T>, ell_grid(P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
     CHECK_LAUNCH();
     T* other = (xf == Bf.xa) ? Bf.xb : Bf.xa;
     for (int k = 1; k <= sw; ++k) {
@@ -460,12 +479,12 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
         if (k == sw)
           {
             prof_mark(s, 2, stream);
-            k_fine_smooth<T, BFromRS<T>, 1><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+            pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, xf, dst, r,
                                                                           s->singular, s->S, s->rb());
             prof_mark(s, 2, stream);
           }
         else
-          k_fine_smooth<T, BFromRS<T>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf0, s->flags, g, w0, xf, dst, r,
+          pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, xf, dst, r,
                                                                           s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         other = xf;
@@ -473,7 +492,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
       } else {
         const DevEll<T>& A = lvA<T>(Lf);
         T* wd = lvWd<T>(Lf);
-        ELL_DISPATCH(A.lanes, (k_ell_smooth<L, T><<<ell_grid(A.n, L), 256, 0, stream>>>(A.view(), wd, Bf.b, xf, other)));
+        ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bf.b, xf, other)));
         CHECK_LAUNCH();
         std::swap(xf, other);
       }
@@ -493,9 +512,9 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   BStored<double> bf{b};
   LevelBuf<double>& B0 = s->lv[0].d;
   if (Lv == 1) {
-    k_dense<double><<<1, 256, 0, stream>>>(s->C, s->nc, b, x);
+    pdl_launch(s, k_dense<double>, 1, 256, 0, stream, s->C, s->nc, b, x);
     CHECK_LAUNCH();
-    k_fine_sums<double, 2><<<s->cgrid, s->cblock, 0, stream>>>(x, s->flags, g, nullptr, s->singular, s->S, s->rb());
+    pdl_launch(s, k_fine_sums<double, 2>, s->cgrid, s->cblock, 0, stream, x, s->flags, g, nullptr, s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     return 0;
   }
@@ -503,37 +522,37 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   double* a = x;
   double* t = s->xtmp;
   for (int k = 0; k < sw; ++k) {
-    k_fine_smooth<double, BStored<double>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, a, t, nullptr,
+    pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, a, t, nullptr,
                                                                              s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     std::swap(a, t);
   }
-  k_fine_resid<double, BStored<double>><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, a, B0.res);
+  pdl_launch(s, k_fine_resid<double, BStored<double>>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, a, B0.res);
   CHECK_LAUNCH();
   double* cur[32];
   cur[0] = a;
   for (int l = 1; l < Lv; ++l) {
     Level& Lc = s->lv[l];
     const double* res_f = s->lv[l - 1].d.res;
-    ELL_DISPATCH(Lc.R.lanes, (k_ell_spmv<L, false, double><<<ell_grid(Lc.R.n, L), 256, 0, stream>>>(Lc.R.view(), res_f, Lc.d.b)));
+    ELL_DISPATCH(Lc.R.lanes, (pdl_launch(s, k_ell_spmv<L, false, double>, ell_grid(Lc.R.n, L), 256, 0, stream, Lc.R.view(), res_f, Lc.d.b)));
     CHECK_LAUNCH();
     if (l == Lv - 1) {
-      k_dense<double><<<1, 256, 0, stream>>>(s->C, s->nc, Lc.d.b, Lc.d.xa);
+      pdl_launch(s, k_dense<double>, 1, 256, 0, stream, s->C, s->nc, Lc.d.b, Lc.d.xa);
       CHECK_LAUNCH();
       cur[l] = Lc.d.xa;
       break;
     }
-    ELL_DISPATCH(Lc.A.lanes, (k_ell_pre<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.wd, Lc.d.b, Lc.d.xa, Lc.d.res)));
+    ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_pre<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, Lc.d.xa, Lc.d.res)));
     CHECK_LAUNCH();
     double* p = Lc.d.xa;
     double* o = Lc.d.xb;
     if (sw > 1) {
       for (int k = 1; k < sw; ++k) {
-        ELL_DISPATCH(Lc.A.lanes, (k_ell_smooth<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.wd, Lc.d.b, p, o)));
+        ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, p, o)));
         CHECK_LAUNCH();
         std::swap(p, o);
       }
-      ELL_DISPATCH(Lc.A.lanes, (k_ell_resid<L, double><<<ell_grid(Lc.A.n, L), 256, 0, stream>>>(Lc.A.view(), Lc.d.b, p, Lc.d.res)));
+      ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_resid<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.d.b, p, Lc.d.res)));
       CHECK_LAUNCH();
     }
     cur[l] = p;
@@ -542,16 +561,16 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
     Level& Lf = s->lv[l];
     const DevEll<double>& P = s->lv[l + 1].P;
     double* xf = cur[l];
-    ELL_DISPATCH(P.lanes, (k_ell_spmv<L, true, double><<<ell_grid(P.n, L), 256, 0, stream>>>(P.view(), cur[l + 1], xf)));
+    ELL_DISPATCH(P.lanes, (pdl_launch(s, k_ell_spmv<L, true, double>, ell_grid(P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
     CHECK_LAUNCH();
     if (l == 0) {
       double* o = (xf == x) ? s->xtmp : x;
       for (int k = 1; k <= sw; ++k) {
         if (k == sw)
-          k_fine_smooth<double, BStored<double>, 2><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+          pdl_launch(s, k_fine_smooth<double, BStored<double>, 2>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         else
-          k_fine_smooth<double, BStored<double>, 0><<<s->cgrid, s->cblock, 0, stream>>>(bf, s->flags, g, w0, xf, o, nullptr,
+          pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         std::swap(xf, o);
@@ -560,7 +579,7 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
     } else {
       double* o = (xf == Lf.d.xa) ? Lf.d.xb : Lf.d.xa;
       for (int k = 1; k <= sw; ++k) {
-        ELL_DISPATCH(Lf.A.lanes, (k_ell_smooth<L, double><<<ell_grid(Lf.A.n, L), 256, 0, stream>>>(Lf.A.view(), Lf.wd, Lf.d.b, xf, o)));
+        ELL_DISPATCH(Lf.A.lanes, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(Lf.A.n, L), 256, 0, stream, Lf.A.view(), Lf.wd, Lf.d.b, xf, o)));
         CHECK_LAUNCH();
         std::swap(xf, o);
       }
@@ -638,24 +657,24 @@ int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
   const bool cap = s->capturing;
   Loop outer, inner;
   TRY(loop_handle(s, stream, &outer));
-  k_ir_residual<<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->r32, s->x32, s->flags, g, cfg,
+  pdl_launch(s, k_ir_residual, s->cgrid, s->cblock, 0, stream, s->b, x, s->r32, s->x32, s->flags, g, cfg,
                                                     s->inner_tol, kIrMaxPasses, 1, has_x0, s->S, s->I,
                                                     s->rb(), outer.ctl);
   CHECK_LAUNCH();
   auto inner_pass = [&](cudaStream_t st) -> int {
     TRY(vcycle_pcg<float>(s, s->r32, s->z32, st));
-    k_cg_pq<float, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->r32, s->z32, s->pa32, s->pb32, s->q32, s->flags,
+    pdl_launch(s, k_cg_pq<float, PC_MG>, s->cgrid, s->cblock, 0, st, s->r32, s->z32, s->pa32, s->pb32, s->q32, s->flags,
                                                           g, s->S, s->I, s->rb());
     CHECK_LAUNCH();
-    k_cg_xr<float, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->x32, s->r32, s->pb32, s->q32, s->pa32, s->flags,
+    pdl_launch(s, k_cg_xr<float, PC_MG>, s->cgrid, s->cblock, 0, st, s->x32, s->r32, s->pb32, s->q32, s->pa32, s->flags,
                                                           g, icfg, s->S, s->I, s->rb(), inner.ctl);
     CHECK_LAUNCH();
     return 0;
   };
   auto refine = [&](cudaStream_t st) -> int {
-    k_ir_update<<<s->cgrid, s->cblock, 0, st>>>(x, s->x32, s->flags, g, s->I);
+    pdl_launch(s, k_ir_update, s->cgrid, s->cblock, 0, st, x, s->x32, s->flags, g, s->I);
     CHECK_LAUNCH();
-    k_ir_residual<<<s->cgrid, s->cblock, 0, st>>>(s->b, x, s->r32, s->x32, s->flags, g, cfg, s->inner_tol,
+    pdl_launch(s, k_ir_residual, s->cgrid, s->cblock, 0, st, s->b, x, s->r32, s->x32, s->flags, g, cfg, s->inner_tol,
                                                   kIrMaxPasses, 0, 1, s->S, s->I, s->rb(), outer.ctl);
     CHECK_LAUNCH();
     return 0;
@@ -667,7 +686,7 @@ int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
       cudaGraphConditionalHandle h;
       CU(cudaGraphConditionalHandleCreate(&h, outer.body, 0, 0));
       inner.ctl = LoopCtl{h, 1};
-      k_ir_arm<<<1, 32, 0, s->aux>>>(s->I, inner.ctl);
+      pdl_launch(s, k_ir_arm, 1, 32, 0, s->aux, s->I, inner.ctl);
       CHECK_LAUNCH();
       cudaStreamCaptureStatus cs;
       cudaGraph_t gb = nullptr;
@@ -703,9 +722,9 @@ int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
       TRY(refine(stream));
     }
   }
-  k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
+  pdl_launch(s, k_finish_stats<double>, s->cgrid, s->cblock, 0, stream, x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
   CHECK_LAUNCH();
-  k_finish_apply<double><<<s->cgrid, s->cblock, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
+  pdl_launch(s, k_finish_apply<double>, s->cgrid, s->cblock, 0, stream, x, x, s->flags, g, s->S, s->I);
   CHECK_LAUNCH();
   return 0;
 }
@@ -721,25 +740,25 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
   if (kind == PCFD_SOLVER_CG || kind == PCFD_SOLVER_MGCG) {
     Loop L;
     TRY(loop_handle(s, stream, &L));
-    k_rhs_init<double><<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->r, s->flags, g, cfg, has_x0, s->S,
+    pdl_launch(s, k_rhs_init<double>, s->cgrid, s->cblock, 0, stream, s->b, x, s->r, s->flags, g, cfg, has_x0, s->S,
                                                       s->I, s->rb(), L.ctl);
     CHECK_LAUNCH();
     // one pass of the recurrence on stream `st`; p_old -> p_new
     auto pass = [&](cudaStream_t st, double* p_old, double* p_new, double* keep) -> int {
       if (kind == PCFD_SOLVER_CG) {
-        k_cg_pq<double, PC_JACOBI><<<s->cgrid, s->cblock, 0, st>>>(s->r, nullptr, p_old, p_new, s->q, s->flags,
+        pdl_launch(s, k_cg_pq<double, PC_JACOBI>, s->cgrid, s->cblock, 0, st, s->r, nullptr, p_old, p_new, s->q, s->flags,
                                                               g, s->S, s->I, s->rb());
         CHECK_LAUNCH();
-        k_cg_xr<double, PC_JACOBI><<<s->cgrid, s->cblock, 0, st>>>(x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+        pdl_launch(s, k_cg_xr<double, PC_JACOBI>, s->cgrid, s->cblock, 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
                                                               s->S, s->I, s->rb(), L.ctl);
       } else {
         TRY(vcycle_pcg<double>(s, s->r, s->z, st));
         prof_mark(s, 1, st);
-        k_cg_pq<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(s->r, s->z, p_old, p_new, s->q, s->flags, g,
+        pdl_launch(s, k_cg_pq<double, PC_MG>, s->cgrid, s->cblock, 0, st, s->r, s->z, p_old, p_new, s->q, s->flags, g,
                                                           s->S, s->I, s->rb());
         prof_mark(s, 1, st);
         CHECK_LAUNCH();
-        k_cg_xr<double, PC_MG><<<s->cgrid, s->cblock, 0, st>>>(x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+        pdl_launch(s, k_cg_xr<double, PC_MG>, s->cgrid, s->cblock, 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
                                                           s->S, s->I, s->rb(), L.ctl);
       }
       CHECK_LAUNCH();
@@ -759,27 +778,27 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
         std::swap(pc, po);
       }
     }
-    k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
+    pdl_launch(s, k_finish_stats<double>, s->cgrid, s->cblock, 0, stream, x, s->b, s->flags, g, cfg, 1, s->S, s->I, s->rb());
     CHECK_LAUNCH();
   } else {
     const int project_x0 = kind == PCFD_SOLVER_MULTIGRID;
-    k_stationary_init<<<s->cgrid, s->cblock, 0, stream>>>(s->b, x, s->flags, g, cfg, has_x0, project_x0, s->S,
+    pdl_launch(s, k_stationary_init, s->cgrid, s->cblock, 0, stream, s->b, x, s->flags, g, cfg, has_x0, project_x0, s->S,
                                                      s->I, s->rb());
     CHECK_LAUNCH();
     if (kind == PCFD_SOLVER_MULTIGRID) {
       Loop L;
       TRY(loop_handle(s, stream, &L));
-      k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(s->b, s->flags, g, s->S, S_MEAN_B);
+      pdl_launch(s, k_apply_mean, s->cgrid, s->cblock, 0, stream, s->b, s->flags, g, s->S, S_MEAN_B);
       CHECK_LAUNCH();
-      k_apply_mean<<<s->cgrid, s->cblock, 0, stream>>>(x, s->flags, g, s->S, S_MEAN_X);
+      pdl_launch(s, k_apply_mean, s->cgrid, s->cblock, 0, stream, x, s->flags, g, s->S, S_MEAN_X);
       CHECK_LAUNCH();
-      k_resnorm<<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb(), L.ctl);
+      pdl_launch(s, k_resnorm, s->cgrid, s->cblock, 0, stream, x, s->b, s->flags, g, cfg, 1, 0, 0, s->S, s->I, s->rb(), L.ctl);
       CHECK_LAUNCH();
       auto cycle = [&](cudaStream_t st) -> int {
         TRY(vcycle_standalone(s, s->b, x, st));
-        k_resnorm<<<s->cgrid, s->cblock, 0, st>>>(x, s->b, s->flags, g, cfg, 1, 1, 1, s->S, s->I, s->rb(), L.ctl);
+        pdl_launch(s, k_resnorm, s->cgrid, s->cblock, 0, st, x, s->b, s->flags, g, cfg, 1, 1, 1, s->S, s->I, s->rb(), L.ctl);
         CHECK_LAUNCH();
-        k_apply_mean<<<s->cgrid, s->cblock, 0, st>>>(x, s->flags, g, s->S, S_MEAN_X);
+        pdl_launch(s, k_apply_mean, s->cgrid, s->cblock, 0, st, x, s->flags, g, s->S, S_MEAN_X);
         CHECK_LAUNCH();
         return 0;
       };
@@ -801,20 +820,20 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
       const int every = kind == PCFD_SOLVER_JACOBI ? 20 : 5;
       for (int it = 1; it <= s->maxiter; ++it) {
         if (kind == PCFD_SOLVER_JACOBI) {
-          k_jacobi_sweep<<<s->cgrid, s->cblock, 0, stream>>>(cur, oth, s->b, s->flags, g, 2.0 / 3.0, s->singular,
+          pdl_launch(s, k_jacobi_sweep, s->cgrid, s->cblock, 0, stream, cur, oth, s->b, s->flags, g, 2.0 / 3.0, s->singular,
                                                         s->S, s->I, s->rb());
           CHECK_LAUNCH();
           std::swap(cur, oth);
         } else {
-          k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
+          pdl_launch(s, k_sor_half, s->cgrid, s->cblock, 0, stream, cur, s->b, s->flags, g, s->omega, 0, s->singular, s->S,
                                                     s->I, s->rb());
           CHECK_LAUNCH();
-          k_sor_half<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
+          pdl_launch(s, k_sor_half, s->cgrid, s->cblock, 0, stream, cur, s->b, s->flags, g, s->omega, 1, s->singular, s->S,
                                                     s->I, s->rb());
           CHECK_LAUNCH();
         }
         if (it % every == 0 || it == s->maxiter) {
-          k_resnorm<<<s->cgrid, s->cblock, 0, stream>>>(cur, s->b, s->flags, g, cfg, 0, 0, 1, s->S, s->I, s->rb(),
+          pdl_launch(s, k_resnorm, s->cgrid, s->cblock, 0, stream, cur, s->b, s->flags, g, cfg, 0, 0, 1, s->S, s->I, s->rb(),
                                                    LoopCtl{0, 0});
           CHECK_LAUNCH();
           TRY(read_flags(s, stream));
@@ -823,10 +842,10 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
       }
       if (cur != x) CU(cudaMemcpyAsync(x, cur, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     }
-    k_finish_stats<double><<<s->cgrid, s->cblock, 0, stream>>>(x, s->b, s->flags, g, cfg, 0, s->S, s->I, s->rb());
+    pdl_launch(s, k_finish_stats<double>, s->cgrid, s->cblock, 0, stream, x, s->b, s->flags, g, cfg, 0, s->S, s->I, s->rb());
     CHECK_LAUNCH();
   }
-  k_finish_apply<double><<<s->cgrid, s->cblock, 0, stream>>>(x, x, s->flags, g, s->S, s->I);
+  pdl_launch(s, k_finish_apply<double>, s->cgrid, s->cblock, 0, stream, x, x, s->flags, g, s->S, s->I);
   CHECK_LAUNCH();
   return 0;
 }
@@ -834,7 +853,7 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
 int set_dt(pycfd_solver* s, double dt, double blend, cudaStream_t stream) {
   // Step parameters live in device memory so a recorded step replays with new
   // values; they travel as kernel arguments, so no host synchronisation.
-  k_begin<<<1, 32, 0, stream>>>(s->S, s->I, dt, blend);
+  pdl_launch(s, k_begin, 1, 32, 0, stream, s->S, s->I, dt, blend);
   CHECK_LAUNCH();
   return 0;
 }
@@ -844,14 +863,14 @@ int set_dt(pycfd_solver* s, double dt, double blend, cudaStream_t stream) {
 int project_impl(pycfd_solver* s, double* u, double* v, double* p, double dt_override,
                  cudaStream_t stream) {
   const int G = grid1(s);
-  k_div_rhs<<<s->cgrid, s->cblock, 0, stream>>>(u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  pdl_launch(s, k_div_rhs, s->cgrid, s->cblock, 0, stream, u, v, nullptr, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   if (s->precision == PCFD_MIXED) TRY(solve_mixed(s, s->x, s->has_guess, stream));
   else TRY(solve_prepared(s, s->x, s->has_guess, stream));
   s->has_guess = true;
   const int gc = std::min(s->g.nx + 2, kMaxRedBlocks) + 1;   // rows + the ghost-ring block
   prof_mark(s, 7, stream);
-  k_correct<<<gc, 256, 0, stream>>>(u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
+  pdl_launch(s, k_correct, gc, 256, 0, stream, u, v, p, s->x, s->g, s->S, dt_override, s->bc_kind_dev);
   prof_mark(s, 7, stream);
   CHECK_LAUNCH();
   return 0;
@@ -863,7 +882,7 @@ int substep_impl(pycfd_solver* s, StageIn uin, StageIn vin, double* us, double* 
   dim3 blk(TJ, TI);
   dim3 grd((g.ny + 3 + TJ - 1) / TJ, (g.nx + 3 + TI - 1) / TI);
   prof_mark(s, 6, stream);
-  k_predictor<<<grd, blk, 0, stream>>>(uin, vin, us, vs, g, s->S);
+  pdl_launch(s, k_predictor, grd, blk, 0, stream, uin, vin, us, vs, g, s->S);
   prof_mark(s, 6, stream);
   CHECK_LAUNCH();
   TRY(launch_boundary(s, us, vs, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, stream));
@@ -884,9 +903,9 @@ int step_impl(pycfd_solver* s, const double* u0, const double* v0, double* u, do
     TRY(substep_impl(s, U0, V0, s->us1, s->vs1, p, stream));
     TRY(substep_impl(s, StageIn{s->us1, nullptr, 1.0, 0.0}, StageIn{s->vs1, nullptr, 1.0, 0.0}, s->us2,
                      s->vs2, p, stream));
-    k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us2, 0.5, 0.5, u, nu);
+    pdl_launch(s, k_combine, grid_for(nu, 256), 256, 0, stream, u0, s->us2, 0.5, 0.5, u, nu);
     CHECK_LAUNCH();
-    k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs2, 0.5, 0.5, v, nv);
+    pdl_launch(s, k_combine, grid_for(nv, 256), 256, 0, stream, v0, s->vs2, 0.5, 0.5, v, nv);
     CHECK_LAUNCH();
   } else {
     TRY(substep_impl(s, U0, V0, s->us1, s->vs1, p, stream));
@@ -894,9 +913,9 @@ int step_impl(pycfd_solver* s, const double* u0, const double* v0, double* u, do
                      s->vs2, p, stream));
     TRY(substep_impl(s, StageIn{u0, s->us2, 0.75, 0.25}, StageIn{v0, s->vs2, 0.75, 0.25}, s->us1, s->vs1,
                      p, stream));
-    k_combine<<<grid_for(nu, 256), 256, 0, stream>>>(u0, s->us1, 1.0 / 3.0, 2.0 / 3.0, u, nu);
+    pdl_launch(s, k_combine, grid_for(nu, 256), 256, 0, stream, u0, s->us1, 1.0 / 3.0, 2.0 / 3.0, u, nu);
     CHECK_LAUNCH();
-    k_combine<<<grid_for(nv, 256), 256, 0, stream>>>(v0, s->vs1, 1.0 / 3.0, 2.0 / 3.0, v, nv);
+    pdl_launch(s, k_combine, grid_for(nv, 256), 256, 0, stream, v0, s->vs1, 1.0 / 3.0, 2.0 / 3.0, v, nv);
     CHECK_LAUNCH();
   }
   TRY(launch_boundary(s, u, v, {OP_VEL_CORR, OP_WRAP_FACES}, stream));
@@ -978,6 +997,7 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->scheme = d->time_scheme;
   s->precision = d->precision;
   s->inner_tol = d->inner_tol > 0 ? d->inner_tol : 1e-4;
+  s->pdl = d->sequential_launch ? 0 : 1;
 
   // ---- cell flags of the fine operator (pycfd/core/pressure.py:209-247) ----
   const long n = (long)nx * ny;
@@ -1245,7 +1265,7 @@ int pycfd_poisson_solve(pycfd_solver* s, const double* rhs, const double* p0, do
   cudaStream_t sm = st(stream);
   const int G = grid1(s);
   TRY(set_dt(s, 1.0, 0.0, sm));
-  k_div_rhs<<<s->cgrid, s->cblock, 0, sm>>>(nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  pdl_launch(s, k_div_rhs, s->cgrid, s->cblock, 0, sm, nullptr, nullptr, rhs, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   if (p0) CU(cudaMemcpyAsync(s->x_api, p0, s->ncell() * sizeof(double), cudaMemcpyDeviceToDevice, sm));
   if (s->precision == PCFD_MIXED) TRY(solve_mixed(s, s->x_api, p0 != nullptr, sm));
@@ -1260,7 +1280,7 @@ int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream) {
   cudaStream_t sm = st(stream);
   const int G = grid1(s);
   // mean of r over the active set, then one cycle and the projection of z
-  k_div_rhs<<<s->cgrid, s->cblock, 0, sm>>>(nullptr, nullptr, r, s->flags, s->g, s->S, s->b, s->rb(), s->S);
+  pdl_launch(s, k_div_rhs, s->cgrid, s->cblock, 0, sm, nullptr, nullptr, r, s->flags, s->g, s->S, s->b, s->rb(), s->S);
   CHECK_LAUNCH();
   // k_div_rhs left the solvable sum in S_MEAN_B; the cycle reads S_MEAN_R.
   CU(cudaMemcpyAsync(s->S + S_MEAN_R, s->S + S_MEAN_B, sizeof(double), cudaMemcpyDeviceToDevice, sm));
@@ -1269,7 +1289,7 @@ int pycfd_mg_apply(pycfd_solver* s, const double* r, double* z, void* stream) {
   TRY(vcycle_pcg<double>(s, r, s->z, sm));
   // z = z_raw - mean_z on solvable rows, 0 elsewhere
   CU(cudaMemcpyAsync(s->S + S_MEAN_X, s->S + S_MEAN_Z, sizeof(double), cudaMemcpyDeviceToDevice, sm));
-  k_finish_apply<double><<<s->cgrid, s->cblock, 0, sm>>>(s->z, z, s->flags, s->g, s->S, s->I);
+  pdl_launch(s, k_finish_apply<double>, s->cgrid, s->cblock, 0, sm, s->z, z, s->flags, s->g, s->S, s->I);
   CHECK_LAUNCH();
   return 0;
 }
@@ -1375,11 +1395,11 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
     CU(cudaStreamBeginCapture(s->rec, cudaStreamCaptureModeThreadLocal));
     s->capturing = true;
     int rc = 0;
-    k_field_stats<<<std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, s->rec>>>(
+    pdl_launch(s, k_field_stats, std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, s->rec, 
         u0, v0, nullptr, nullptr, nullptr, s->solid, s->g, s->rb(), s->S);
     if (cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "stats launch failed");
     g_launches.fetch_add(1);
-    k_adaptive_dt<<<1, 32, 0, s->rec>>>(s->S, s->I, c);
+    pdl_launch(s, k_adaptive_dt, 1, 32, 0, s->rec, s->S, s->I, c);
     if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "dt launch failed");
     g_launches.fetch_add(1);
     if (!rc) rc = step_impl(s, u0, v0, u, v, p, s->rec);
@@ -1502,7 +1522,7 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
                       const double* vp, pycfd_field_stats* o, void* stream) {
   if (!s || !u || !v || !o) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
-  k_field_stats<<<std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, sm>>>(u, v, p, up, vp, s->solid, s->g, s->rb(),
+  pdl_launch(s, k_field_stats, std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, sm, u, v, p, up, vp, s->solid, s->g, s->rb(),
                                                                      s->S);
   CHECK_LAUNCH();
   CU(cudaMemcpyAsync(s->hS + S_STAT0, s->S + S_STAT0, 8 * sizeof(double), cudaMemcpyDeviceToHost, sm));

@@ -80,6 +80,7 @@ __device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n,
 __global__ void k_rhs(const double* __restrict__ u, const double* __restrict__ v, int nx, int ny,
                       double dx, double dy, double nu, double blend, double fx, double fy,
                       double* __restrict__ rhs_u, double* __restrict__ rhs_v) {
+  pdl_begin();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;   // 0..ny
   const int i = blockIdx.y * blockDim.y + threadIdx.y;   // 0..nx
   if (i <= nx && j < ny) rhs_u[(long)i * ny + j] = rhs_u_at(u, v, i + 1, j + 1, ny, dx, dy, nu, blend, fx);
@@ -91,6 +92,7 @@ __global__ void k_rhs(const double* __restrict__ u, const double* __restrict__ v
 // upwind blend are read from device scalars so a captured step can be replayed.
 __global__ void k_predictor(StageIn u, StageIn v, double* __restrict__ us, double* __restrict__ vs,
                             Geo g, const double* __restrict__ S) {
+  pdl_begin();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y * blockDim.y + threadIdx.y;
   const int nx = g.nx, ny = g.ny;
@@ -120,6 +122,7 @@ __device__ __forceinline__ double cell_div(const double* u, const double* v, int
 
 __global__ void k_divergence(const double* __restrict__ u, const double* __restrict__ v, int nx,
                              int ny, double dx, double dy, double* __restrict__ out) {
+  pdl_begin();
   for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < nx; i += gridDim.y * blockDim.y)
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ny; j += gridDim.x * blockDim.x)
       out[(long)i * ny + j] = cell_div(u, v, i, j, ny, dx, dy);
@@ -133,6 +136,7 @@ __global__ void k_div_rhs(const double* __restrict__ u, const double* __restrict
                           const double* __restrict__ rhs_in, const uint8_t* __restrict__ flags,
                           Geo g, const double* __restrict__ S, double* __restrict__ b,
                           RedBuf rb, double* __restrict__ Sout) {
+  pdl_begin();
   const double dt = S[S_DT];
   double acc[1] = {0.0};
   FOR_CELLS(g) {
@@ -186,6 +190,7 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
                           double* __restrict__ p, const double* __restrict__ x, Geo g,
                           const double* __restrict__ S, double dt_override,
                           const int* __restrict__ bc_kind) {
+  pdl_begin();
   const int nx = g.nx, ny = g.ny;
   const double dt = dt_override > 0.0 ? dt_override : S[S_DT];
   if (blockIdx.x == gridDim.x - 1) {
@@ -269,6 +274,7 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
 // out = ca*a + cb*b over whole arrays (pycfd/core/solver.py:705-721).
 __global__ void k_combine(const double* __restrict__ a, const double* __restrict__ b, double ca,
                           double cb, double* __restrict__ out, long n) {
+  pdl_begin();
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
     out[k] = ca * a[k] + cb * b[k];
 }
@@ -280,6 +286,7 @@ __global__ void k_field_stats(const double* __restrict__ u, const double* __rest
                               const double* __restrict__ p, const double* __restrict__ up,
                               const double* __restrict__ vp, const uint8_t* __restrict__ solid,
                               Geo g, RedBuf rb, double* __restrict__ Sout) {
+  pdl_begin();
   const int nx = g.nx, ny = g.ny;
   const long W = ny + 2, WV = ny + 3;
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // max,max,max,max,max,sum,max,sum

@@ -42,6 +42,9 @@ class GpuOptions:
     #: cluster per V-cycle (0, the default: one kernel per phase on every level;
     #: the cluster form is bit-identical but slower while coarse stencils are wide).
     coarse_cluster_rows: int = 0
+    #: let each step kernel be scheduled while its predecessor runs
+    #: (programmatic dependent launch); False keeps plain stream order.
+    programmatic_launch: bool = True
 
 
 def _torch():
@@ -254,6 +257,7 @@ class ProjectionSolver:
         d.precision = 1 if self.options.precision == "mixed" else 0
         d.inner_tol = self.options.inner_tol
         d.coarse_cluster_rows = int(self.options.coarse_cluster_rows)
+        d.sequential_launch = 0 if self.options.programmatic_launch else 1
         if self._levels is not None:
             arr = (_lib.MgLevel * len(self._levels))()
             for l, lv in enumerate(self._levels):

@@ -213,3 +213,20 @@ def test_coarse_cluster_matches_per_level_kernels(precision):
     for a, b in zip(out[0][0], out[1][0]):
         assert np.array_equal(a, b)
     assert out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_programmatic_launch_matches_stream_order(precision):
+    """Kernels scheduled early (each waits on its predecessor) give the same bits."""
+    from pycfd_b200.solver import GpuOptions
+    d = dict(nx=64, ny=48, lx=4.0 / 3.0, ly=1.0, re=150.0, pressure_solver="mgcg",
+             poisson_tol=1e-12, boundary_config=cases.bcs(left=("inlet", 1.0), right=("outlet",)))
+    out = []
+    for pdl in (False, True):
+        s = _solver(_cfg(d), options=GpuOptions(precision=precision, programmatic_launch=pdl))
+        f = s.initialize(1.0)
+        for _ in range(5):
+            f = s.advance(f, 2e-3)
+        out.append(f.numpy())
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
