@@ -61,6 +61,15 @@ def workload_config(extra=None):
     return d
 
 
+def max_over_ranks(value, dist, device):
+    """Largest value over all ranks (the slowest rank sets the job's time)."""
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -281,11 +290,7 @@ def run_ours(args, world, rank, local):
     if dist:
         dist.barrier()
     ck = clocks.stop() if clocks else None
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([dev_ms], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    dev_ms = float(t.item())
+    dev_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, "cuda")
     value = world * N * N * args.steps / (dev_ms / 1e3)
     st = solver.field_stats(f)
     launches_per_step = solver.launches_per_step(f, dt)
@@ -302,11 +307,8 @@ def run_ours(args, world, rank, local):
     for _ in range(e2e_steps):
         un2, vn2, pn2 = solver.step_host(un, vn, dt)
         un, vn = un2, vn2
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * N * N * e2e_steps / float(te.item()) if e2e_steps else None
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+    e2e_value = world * N * N * e2e_steps / e2e_s if e2e_steps else None
     h2d = (un.size + vn.size) * 8
     d2h = (un.size + vn.size + int(np.prod(solver.mesh.p_shape))) * 8
 
