@@ -252,6 +252,57 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
                       const double* u_prev, const double* v_prev, pycfd_field_stats* out,
                       void* stream);
 
+/* ---- Batched stepping (no counterpart in the reference, whose Simulation
+ * advances one problem).  Many independent problems -- grids of uneven size,
+ * their own viscosity, boundary conditions, time step and end time -- advance
+ * together, every stage of the SSP-RK3 step ONE launch over all of them
+ * (block maps of (problem, tile)), the Poisson solves as MG-PCG (FP64) or as
+ * FP32 MG-PCG inside FP64 iterative refinement (mixed), with device-side loops
+ * that run while any problem still iterates.  Each problem keeps the
+ * single-problem arithmetic: ProjectionSolver.step (pycfd/core/solver.py:686-731)
+ * with TimeStepper.compute_dt (pycfd/core/timestepper.py:94-142). */
+typedef struct pycfd_batch pycfd_batch;
+
+typedef struct {
+    int precision;      /* PCFD_FP64 or PCFD_MIXED                                */
+    double tol;         /* relative Poisson tolerance (outer one, mixed form)     */
+    int maxiter;        /* CG iterations per solve (FP64 form)                    */
+    double inner_tol;   /* mixed: relative tolerance of each FP32 inner solve     */
+    int mg_sweeps;      /* damped-Jacobi sweeps before and after each coarse step */
+    int tile_rows;      /* rows of x per fine-level block: 8, 16, 32 or 64        */
+} pycfd_batch_opts;
+
+/* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver
+ * fields other than the hierarchy are taken from opts).  structure[i] names
+ * the problem whose multigrid hierarchy problem i shares (i itself, or an
+ * earlier problem with the same grid, boundary kinds and mask); only those
+ * leading problems need levels/coarsest_inverse, of at least 2 levels.  The
+ * state u[i], v[i], p[i] (device, the ghosted layout of pycfd_step) is advanced
+ * in place; dt_ctl[i] is problem i's time-step control; its clock starts at 0;
+ * it stops after max_steps[i] steps (max_steps may be NULL: no limit). */
+int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure,
+                       const pycfd_dt_control* dt_ctl, const int* max_steps, double* const* u,
+                       double* const* v, double* const* p, int n, const pycfd_batch_opts* opts,
+                       pycfd_batch** out);
+int pycfd_batch_destroy(pycfd_batch* b);
+/* Initial projection of every problem (pycfd_initialize, batched). */
+int pycfd_batch_initialize(pycfd_batch* b, void* stream);
+/* `steps` adaptive steps of every problem; record != 0 replays one recorded
+ * CUDA graph per step (recorded on first use).  A problem whose health flags
+ * trip (pycfd_get_clock), whose clock reaches t_end or that has taken its
+ * max_steps stops; the others go on. */
+int pycfd_batch_step(pycfd_batch* b, int steps, int record, void* stream);
+/* Problem i's single-problem handle (clock, stats, reductions; not for stepping). */
+pycfd_solver* pycfd_batch_problem(pycfd_batch* b, int i);
+/* Per-problem arrays of n: frozen (0 running, 1 stopped by a health flag,
+ * 2 reached t_end or max_steps), steps taken, solver iterations of the last step, solver
+ * status, clock and last dt.  Any pointer may be NULL. */
+int pycfd_batch_status(pycfd_batch* b, int* frozen, int* steps, int* iterations, int* status,
+                       double* t, double* dt, void* stream);
+/* Kernel launches the device executed for `steps` recorded steps since the
+ * last call (fixed part per step plus the loop bodies times the passes run). */
+int pycfd_batch_launches(pycfd_batch* b, int steps, long long* launches, void* stream);
+
 /* No counterpart in the reference.  The reductions of pycfd_reduce_fields for
  * callers that cannot allocate device memory at the moment they need them: a
  * host whose own allocator owns all device memory, a real-time loop that cannot

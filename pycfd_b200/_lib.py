@@ -28,7 +28,8 @@ EXPORTS = (
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
     "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
     "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_launch_count",
-    "pycfd_profile_read",
+    "pycfd_profile_read", "pycfd_batch_create", "pycfd_batch_destroy", "pycfd_batch_initialize",
+    "pycfd_batch_step", "pycfd_batch_problem", "pycfd_batch_status", "pycfd_batch_launches",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -60,6 +61,11 @@ class DtControl(C.Structure):
     _fields_ = [("adaptive", C.c_int), ("cfl", C.c_double), ("visc_limit", C.c_double),
                 ("dt_cap", C.c_double), ("t_end", C.c_double), ("blend_mode", C.c_int),
                 ("blend", C.c_double)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("maxiter", C.c_int),
+                ("inner_tol", C.c_double), ("mg_sweeps", C.c_int), ("tile_rows", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -121,6 +127,18 @@ def load(path: str = LIB_PATH):
         "pycfd_reduce_fields_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int, C.c_int,
                                                   C.c_double, C.c_double, C.POINTER(FieldStats),
                                                   vp]),
+        "pycfd_batch_create": (C.c_int, [C.POINTER(SolverDesc), C.POINTER(C.c_int),
+                                         C.POINTER(DtControl), C.POINTER(C.c_int), C.POINTER(vp),
+                                         C.POINTER(vp), C.POINTER(vp), C.c_int,
+                                         C.POINTER(BatchOpts), C.POINTER(vp)]),
+        "pycfd_batch_destroy": (C.c_int, [vp]),
+        "pycfd_batch_initialize": (C.c_int, [vp, vp]),
+        "pycfd_batch_step": (C.c_int, [vp, C.c_int, C.c_int, vp]),
+        "pycfd_batch_problem": (vp, [vp, C.c_int]),
+        "pycfd_batch_status": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
+        "pycfd_batch_launches": (C.c_int, [vp, C.c_int, C.POINTER(C.c_longlong), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

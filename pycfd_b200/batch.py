@@ -1,18 +1,22 @@
 """Batched form: many independent problems advanced together on one GPU.
 
-Each problem keeps its own solver, hierarchy and workspace; its whole time
-step -- the field reduction, the device-side dt (the reference's formula), the
-three projected substeps with their device-side Poisson loops -- is recorded
-once into a CUDA graph and replayed.  A step of the batch replays every
-problem's graph on a pool of streams, so the small problems' kernels overlap
-and fill the GPU that any one of them would leave mostly idle; nothing returns
-to the host until the batch is read.  An autotuner picks, per grid size, the
-solver knobs (precision form, inner tolerance, smoothing sweeps) by timing
-them on a sample problem, and caches the choice on disk.
+:class:`BatchedSolver` is the batched engine: every stage of the step -- field
+reduction, device-side dt, predictor, boundary programs, divergence, each
+phase of the MG-PCG (or FP32-in-FP64 mixed) Poisson solve, correction, stage
+combination -- is ONE launch over all problems, whatever their grid sizes,
+viscosities, boundary conditions and time steps; the step is recorded once as
+a CUDA graph whose solve loops run on the device while any problem still
+iterates.  :class:`BatchAutotuner` picks its tile shape, smoothing sweeps and
+inner tolerance by timing the batch itself, and caches the choice on disk.
+
+:class:`BatchRunner` is the plain alternative it is measured against: one
+single-problem solver per problem, each step a recorded per-problem graph,
+replayed on a pool of streams (with its own per-grid-size :class:`Autotuner`).
 """
 
 from __future__ import annotations
 
+import ctypes as C
 import json
 import os
 import time
@@ -20,8 +24,13 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .config import BCKind, BCSpec, SimulationConfig
-from .solver import GpuOptions, ProjectionSolver
+from . import _lib
+from .config import BCKind, BCSpec, PressureSolver, SimulationConfig, SolverType, TimeScheme
+from .fields import FlowField
+from .hierarchy import assemble, build_hierarchy
+from .mesh import StructuredMesh
+from .solver import (BoundaryInfo, GpuOptions, ProjectionSolver, _stream, _torch, dt_control_for,
+                     native_desc)
 
 
 def cavity_batch_configs(count: int = 256, seed: int = 0, sizes=(64, 96, 128, 192, 256),
@@ -170,3 +179,268 @@ class BatchRunner:
             out.append({"t": t, "dt": dt, "steps": n, "health": h,
                         "diverged": bool(h & 3), "dt_collapsed": bool(h & 4)})
         return out
+
+
+# ---------------------------------------------------------------------------
+# Batched engine
+# ---------------------------------------------------------------------------
+_HIERARCHIES: dict = {}
+
+
+class _Problem:
+    """Host set-up of one problem of a batch (the host half of ``ProjectionSolver.__init__``)."""
+
+    def __init__(self, cfg: SimulationConfig, obstacle=None):
+        if SolverType(cfg.solver_type) is SolverType.SIMPLE:
+            raise NotImplementedError("solver_type='simple' is not provided; use 'projection'")
+        if cfg.use_les:
+            raise NotImplementedError("the batched path is laminar; use_les=True is not provided")
+        if PressureSolver(cfg.pressure_solver) is not PressureSolver.MGCG:
+            raise NotImplementedError("the batched path solves the pressure with pressure_solver='mgcg'")
+        if TimeScheme(cfg.time_scheme) is not TimeScheme.RK3:
+            raise NotImplementedError("the batched path steps with time_scheme='rk3'")
+        self.config = cfg
+        self.mesh = StructuredMesh.from_config(cfg)
+        self.boundaries = BoundaryInfo(cfg.boundary_config, self.mesh)
+        nx, ny = self.mesh.shape
+        if obstacle is None:
+            self.solid = np.zeros((nx, ny), dtype=bool)
+        else:
+            self.solid = np.asarray(getattr(obstacle, "mask", obstacle), dtype=bool)
+            if self.solid.shape != (nx, ny):
+                raise ValueError(f"obstacle mask must have shape {(nx, ny)}, got {self.solid.shape}")
+        self.has_obstacle = bool(self.solid.any())
+        b = self.boundaries
+        self.dirichlet = b.dirichlet_pressure()
+        self.key = (nx, ny, self.mesh.dx, self.mesh.dy, b.periodic_x, b.periodic_y,
+                    tuple(sorted(self.dirichlet.items())),
+                    self.solid.tobytes() if self.has_obstacle else None)
+
+    def hierarchy(self):
+        """Multigrid hierarchy of this problem's structure (built once per process)."""
+        h = _HIERARCHIES.get(self.key)
+        if h is None:
+            nx, ny = self.mesh.shape
+            b = self.boundaries
+            A = assemble(nx, ny, self.mesh.dx, self.mesh.dy, b.periodic_x, b.periodic_y,
+                         self.solid if self.has_obstacle else None, self.dirichlet or None)
+            h = _HIERARCHIES[self.key] = build_hierarchy(A)
+        return h
+
+
+@dataclass
+class BatchOptions:
+    """Knobs of the batched engine (all results stay within the Poisson tolerance)."""
+
+    precision: str = "mixed"     #: "mixed" (FP32 MG-PCG in FP64 refinement) or "fp64"
+    inner_tol: float = 1e-4      #: mixed: relative tolerance of each inner FP32 solve
+    mg_sweeps: int = 1           #: damped-Jacobi sweeps before/after each coarse correction
+    tile_rows: int = 32          #: rows of x per fine-level block (8, 16, 32, 64)
+
+
+class BatchedSolver:
+    """Advance many independent problems with one launch per stage (module docstring).
+
+    ``configs``: one :class:`SimulationConfig` per problem (``pressure_solver='mgcg'``,
+    ``time_scheme='rk3'``; ``poisson_tol`` and ``poisson_maxiter`` shared).  Each
+    problem's state is projected once at construction, like
+    ``ProjectionSolver.initialize``; :meth:`step` then advances every problem by
+    adaptive steps (``TimeStepper.compute_dt`` per problem, on the device).  A
+    problem whose health check fails, whose clock reaches ``t_end`` or that has
+    taken ``max_steps`` steps stops; the others go on (:meth:`status`).  ``t_end``
+    and ``max_steps`` may be given per problem.
+    """
+
+    def __init__(self, configs, options: BatchOptions | None = None, obstacles=None,
+                 u_init=None, v_init=None, t_end=float("inf"), max_steps=None):
+        torch = _torch()
+        self._L = _lib.load()
+        self.options = opts = options or BatchOptions()
+        if opts.precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {opts.precision!r}")
+        self.configs = list(configs)
+        n = len(self.configs)
+        if n == 0:
+            raise ValueError("a batch needs at least one problem")
+        tol, maxiter = self.configs[0].poisson_tol, self.configs[0].poisson_maxiter
+        for cfg in self.configs:
+            if cfg.poisson_tol != tol or cfg.poisson_maxiter != maxiter:
+                raise ValueError("every problem of a batch shares poisson_tol and poisson_maxiter")
+        self.problems = [_Problem(cfg, None if obstacles is None else obstacles[k])
+                         for k, cfg in enumerate(self.configs)]
+        leader: dict = {}
+        structure = (C.c_int * n)()
+        descs = (_lib.SolverDesc * n)()
+        ctl = (_lib.DtControl * n)()
+        keep = []
+        gopts = GpuOptions(precision=opts.precision, inner_tol=opts.inner_tol)
+        for k, pb in enumerate(self.problems):
+            first = pb.key not in leader
+            if first:
+                leader[pb.key] = k
+            levels, cinv = pb.hierarchy() if first else (None, None)
+            d, kp = native_desc(pb.config, pb.mesh, pb.boundaries, pb.solid, pb.has_obstacle, (),
+                                PressureSolver.MGCG, gopts, levels, cinv)
+            keep.append((d, kp))
+            descs[k] = d
+            structure[k] = leader[pb.key]
+            te = t_end[k] if isinstance(t_end, (list, tuple, np.ndarray)) else t_end
+            ctl[k] = dt_control_for(pb.config, pb.mesh, float(te))
+        self.structures = len(leader)
+        self.fields = []
+        for k, pb in enumerate(self.problems):
+            f = FlowField.zeros(pb.mesh)
+            for init, view in ((u_init, "u_phys"), (v_init, "v_phys")):
+                if init is None:
+                    continue
+                val = init[k] if isinstance(init, (list, tuple)) else init
+                if val is None:
+                    continue
+                tgt = getattr(f, view)
+                tgt[...] = float(val) if np.isscalar(val) else torch.as_tensor(
+                    np.asarray(val, np.float64) if not isinstance(val, torch.Tensor) else val,
+                    dtype=torch.float64, device="cuda")
+            self.fields.append(f)
+        U = (C.c_void_p * n)(*[f.u.data_ptr() for f in self.fields])
+        V = (C.c_void_p * n)(*[f.v.data_ptr() for f in self.fields])
+        P = (C.c_void_p * n)(*[f.p.data_ptr() for f in self.fields])
+        bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
+                            float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows))
+        if max_steps is None:
+            ms = None
+        else:
+            ms = (C.c_int * n)(*[int(m) for m in (max_steps if isinstance(
+                max_steps, (list, tuple, np.ndarray)) else [max_steps] * n)])
+        h = C.c_void_p()
+        _lib.check(self._L.pycfd_batch_create(descs, structure, ctl, ms, U, V, P, n, C.byref(bo),
+                                              C.byref(h)))
+        self._h = h
+        del keep
+        self.cells = int(sum(pb.mesh.shape[0] * pb.mesh.shape[1] for pb in self.problems))
+        _lib.check(self._L.pycfd_batch_initialize(self._h, _stream()))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._L.pycfd_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def __len__(self) -> int:
+        return len(self.problems)
+
+    def step(self, count: int = 1, record: bool = True) -> None:
+        """``count`` adaptive steps of every running problem, queued on the current stream."""
+        _lib.check(self._L.pycfd_batch_step(self._h, int(count), int(bool(record)), _stream()))
+
+    def status(self) -> dict:
+        """Per-problem ``frozen`` (0 running, 1 health stop, 2 end time), ``steps``,
+        ``iterations`` (solver iterations of the last step), ``status``, ``t``, ``dt``."""
+        n = len(self)
+        fr, st, it, ss = ((C.c_int * n)() for _ in range(4))
+        t, dt = (C.c_double * n)(), (C.c_double * n)()
+        _lib.check(self._L.pycfd_batch_status(self._h, fr, st, it, ss, t, dt, _stream()))
+        return {"frozen": np.array(fr[:]), "steps": np.array(st[:]), "iterations": np.array(it[:]),
+                "status": np.array(ss[:]), "t": np.array(t[:]), "dt": np.array(dt[:])}
+
+    def field(self, k: int) -> FlowField:
+        """Problem ``k``'s state (the batch's own tensors; copy to keep a snapshot)."""
+        st = self.status()
+        f = self.fields[k]
+        return FlowField(f.mesh, f.u, f.v, f.p, float(st["t"][k]), int(st["steps"][k]))
+
+    def field_stats(self, k: int):
+        """max|u|, max|v|, max|div|, kinetic energy, vorticity, finiteness of problem ``k``."""
+        out = _lib.FieldStats()
+        f = self.fields[k]
+        hk = self._L.pycfd_batch_problem(self._h, int(k))
+        _lib.check(self._L.pycfd_reduce_fields(C.c_void_p(hk), _lib.ptr(f.u), _lib.ptr(f.v),
+                                               _lib.ptr(f.p), _lib.ptr(None), _lib.ptr(None),
+                                               C.byref(out), _stream()))
+        return out
+
+    def force(self, k: int):
+        """Immersed-boundary reaction ``(fx, fy)`` of problem ``k``'s last substep."""
+        st = _lib.Stats()
+        hk = self._L.pycfd_batch_problem(self._h, int(k))
+        _lib.check(self._L.pycfd_get_stats(C.c_void_p(hk), C.byref(st), _stream()))
+        return st.fx, st.fy
+
+    def launches(self, steps: int) -> int:
+        """Kernel launches the device ran for the last ``steps`` recorded steps."""
+        n = C.c_longlong()
+        _lib.check(self._L.pycfd_batch_launches(self._h, int(steps), C.byref(n), _stream()))
+        return int(n.value)
+
+
+BATCH_CANDIDATES = (
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=16),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32),
+    BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
+)
+
+
+@dataclass
+class BatchAutotuner:
+    """Choose the batched engine's knobs by timing candidate batches, cached on disk.
+
+    Every candidate reaches the same Poisson tolerance, so the choice changes
+    speed only.  The key is the device, the multiset of grid sizes, the tolerance
+    and the precisions allowed.
+    """
+
+    candidates: tuple = BATCH_CANDIDATES
+    steps: int = 4
+    warmup: int = 3
+    allowed_precisions: tuple = ("mixed", "fp64")
+    cache: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        try:
+            with open(_cache_path()) as fh:
+                self.cache = json.load(fh)
+        except Exception:
+            self.cache = {}
+
+    def key(self, configs) -> str:
+        import torch
+        sizes = {}
+        for c in configs:
+            sizes[f"{c.nx}x{c.ny}"] = sizes.get(f"{c.nx}x{c.ny}", 0) + 1
+        sig = ",".join(f"{k}:{v}" for k, v in sorted(sizes.items()))
+        prec = "+".join(self.allowed_precisions)
+        return f"batch|{torch.cuda.get_device_name()}|{sig}|{configs[0].poisson_tol:g}|{prec}"
+
+    def choose(self, configs, **kw) -> BatchOptions:
+        key = self.key(configs)
+        if key in self.cache:
+            return BatchOptions(**self.cache[key]["choice"])
+        import torch
+        tried = []
+        for cand in self.candidates:
+            if cand.precision not in self.allowed_precisions:
+                continue
+            b = BatchedSolver(configs, options=cand, **kw)
+            b.step(self.warmup)
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            b.step(self.steps)
+            e.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(e) / self.steps
+            tried.append((ms, cand))
+            del b
+        best = min(tried, key=lambda x: x[0])
+        self.cache[key] = {"choice": best[1].__dict__, "ms_per_step": best[0],
+                           "tried": [{"ms_per_step": t, **c.__dict__} for t, c in tried]}
+        try:
+            os.makedirs(os.path.dirname(_cache_path()), exist_ok=True)
+            with open(_cache_path(), "w") as fh:
+                json.dump(self.cache, fh, indent=1)
+        except OSError:
+            pass
+        return best[1]

@@ -1,0 +1,882 @@
+// Batched projection step: many independent problems -- grids of uneven size,
+// their own viscosity, boundary conditions, time step and stopping state --
+// advance together, and every stage of the step is ONE launch over all of
+// them.  A launch's blocks are listed in a block map of (problem, tile)
+// entries built on the host, so one grid covers every problem's cells (or
+// multigrid rows) without a per-problem launch.  Reductions are per problem
+// (partials per tile, the problem's last tile finishes), and the kernels that
+// end an iteration also take a launch-wide ticket whose last block decides
+// whether ANY problem still iterates -- the condition of the device-side WHILE
+// loop of a recorded step.  A problem that has converged, or is frozen (health
+// flag, end time reached), skips its blocks.
+//
+// The per-problem arithmetic is the single-problem path's, expression by
+// expression (pycfd/core/solver.py:612-731, pycfd/core/pressure.py:300-327,
+// pycfd/core/multigrid.py:424-474); only the reduction trees differ (tile
+// partials instead of grid-stride partials), so results agree with a solve of
+// the same problem alone to rounding, and with the reference within the
+// solver tolerance.
+#pragma once
+#include "boundary.cuh"
+#include "common.cuh"
+#include "multigrid.cuh"
+#include "poisson.cuh"
+#include "stencil.cuh"
+
+namespace pcfd {
+
+constexpr int kBMaxLevels = 12;
+constexpr int kBTileJ = 32;      // fine tile width along y (contiguous) = threads along y
+constexpr int kBThreadsI = 8;    // threads along x in a fine tile block
+constexpr int kBThreads = 256;   // every batched kernel runs 256-thread blocks
+constexpr int kBRows = 256;      // multigrid rows per block of an ELL launch
+
+// One coarse level (l >= 1) of a hierarchy shared by the problems of one
+// structure (same grid, boundary kinds and solid mask).
+template <class T>
+struct BLevel {
+  Ell<T> A, R, P;   // A, R: rows of this level; P: rows of the finer level
+  int la, lr, lp;   // lanes per row of each block
+  const T* wd;      // weighted inverse diagonal
+  int n;
+};
+
+template <class T>
+struct BHier {
+  BLevel<T> lv[kBMaxLevels];
+  double w0;        // smoother weight of level 0 (matrix-free)
+  const T* C;       // coarsest pseudo-inverse, row-major nc x nc
+  int nc;
+  int nlev;
+};
+
+// Device record of one problem.  T is the storage type of the (inner) CG and
+// multigrid vectors: double for the FP64 form, float for the mixed form.
+template <class T>
+struct BProb {
+  Geo g;
+  BcTable bc;
+  DtControl dtc;
+  int hier, nlev, singular;
+  int max_steps;                         // the problem stops after this many steps
+  int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
+  int red_base;                          // first partial row of this problem
+  const uint8_t* flags;
+  const uint8_t* solid;
+  const int* bc_kind;
+  double *u, *v, *p;                     // state (in place)
+  double *us1, *vs1, *us2, *vs2;         // stage buffers
+  double* S;
+  int* I;
+  unsigned* counter;                     // per-problem reduction ticket
+  double *b, *x;                         // FP64 right-hand side and solution (warm start)
+  T *xs, *r, *z, *pa, *pb, *q;           // (inner) CG iterate and vectors
+  T *lb[kBMaxLevels], *lxa[kBMaxLevels], *lxb[kBMaxLevels], *lres[kBMaxLevels];
+};
+
+// Launch-wide state of a batch (device pointers).
+struct BShared {
+  double* partials;      // per problem: tiles x 8 doubles, from red_base
+  unsigned* tickets;     // launch-wide tickets, one per deciding launch site
+  int* any;              // last "some problem still iterates" per site (host-driven loops)
+  long long* passes;     // per site: how often it let its loop body run (launch accounting)
+  unsigned* iters;       // per site: passes of the loop now running (the cap below)
+  int* capped;           // per site: set when a loop was ended by its pass cap
+};
+
+enum BTicket { TK_CG = 0, TK_IR = 1, TK_ARM = 2, TK_COUNT = 4 };
+
+template <class T>
+__device__ __forceinline__ bool b_frozen(const BProb<T>& P) { return P.I[I_FROZEN] != 0; }
+template <class T>
+__device__ __forceinline__ bool b_solving(const BProb<T>& P) {
+  return P.I[I_FROZEN] == 0 && P.I[I_DONE] == 0;
+}
+
+// Per-problem reduction over the tiles of one launch.  Every block of the
+// problem contributes NV values at row `tile`; the last to arrive combines them
+// in tile order and calls fin(totals) on its thread 0.  No early return, so a
+// launch-wide ticket may follow.
+template <int NV, unsigned MAXMASK = 0u, class Fin>
+__device__ __forceinline__ void b_reduce(double (&v)[NV], double* partials, unsigned* counter,
+                                         int tile, int ntiles, Fin fin) {
+  block_reduce<NV, MAXMASK>(v);
+  __shared__ bool last;
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[(long)tile * NV + k] = v[k];
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == (unsigned)ntiles - 1);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
+    for (int b = tid; b < ntiles; b += nthr) {
+#pragma unroll
+      for (int k = 0; k < NV; ++k) {
+        const double p = ((volatile double*)partials)[(long)b * NV + k];
+        acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], p) : acc[k] + p;
+      }
+    }
+    block_reduce<NV, MAXMASK>(acc);
+    if (tid == 0) {
+      fin(acc);
+      *counter = 0u;
+    }
+  }
+}
+
+// Launch-wide ticket: every block of the launch calls this last; the final
+// block sets the loop condition to "some unfrozen problem has flag `slot`
+// still 0", mirrors it into the site's `any` and rearms the ticket.  The
+// launch that opens a loop passes reset = 1; every later one counts a pass,
+// and at `cap` passes the loop ends whatever the flags say (each problem's
+// own iteration limit ends it first; the cap only bounds the device loop).
+template <class T>
+__device__ void b_loop_ticket(const BProb<T>* __restrict__ probs, int nprob, const BShared& sh,
+                              int site, int slot, int reset, int cap, LoopCtl loop) {
+  unsigned* ticket = sh.tickets + site;
+  __shared__ bool lastg;
+  __syncthreads();
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+  const unsigned nblk = gridDim.x * gridDim.y;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(ticket, 1u);
+    lastg = (t == nblk - 1);
+  }
+  __syncthreads();
+  if (!lastg) return;
+  __threadfence();
+  int any = 0;
+  for (int p = tid; p < nprob; p += nthr) {
+    const volatile int* I = probs[p].I;
+    if (I[I_FROZEN] == 0 && I[slot] == 0) any = 1;
+  }
+  any = __syncthreads_or(any);
+  if (tid == 0) {
+    const unsigned it = reset ? 0u : sh.iters[site] + 1u;
+    sh.iters[site] = it;
+    if (any && it >= (unsigned)cap) {
+      any = 0;
+      sh.capped[site] = 1;
+    }
+    sh.any[site] = any;
+    loop.set(any != 0);
+    *ticket = 0u;
+    if (any) sh.passes[site] += 1;
+  }
+}
+
+// ---- iteration over a fine tile -------------------------------------------
+// Block (32 x 8 threads) over the cells of one tile: rows [i0, i0+tile_i) of x,
+// 32 columns of y.  B_TILE_CELLS visits interior cells (i < nx, j < ny);
+// B_TILE_EXT visits a ghosted array of extent EI x EJ, the last tile row and
+// column stretching to the array's edge.
+#define B_TILE_CELLS(P, tile)                                                               \
+  const int ti_ = (tile) / (P).tiles_j, tj_ = (tile) - ti_ * (P).tiles_j;                   \
+  const int i1_ = min((ti_ + 1) * (P).tile_i, (P).g.nx);                                    \
+  const int j = tj_ * kBTileJ + (int)threadIdx.x;                                           \
+  if (j < (P).g.ny)                                                                         \
+    for (int i = ti_ * (P).tile_i + (int)threadIdx.y; i < i1_; i += kBThreadsI)
+
+#define B_TILE_EXT(P, tile, EI, EJ)                                                         \
+  const int ti_ = (tile) / (P).tiles_j, tj_ = (tile) - ti_ * (P).tiles_j;                   \
+  const int i1_ = (ti_ == (P).tiles_i - 1) ? (EI) : (ti_ + 1) * (P).tile_i;                  \
+  const int j1_ = (tj_ == (P).tiles_j - 1) ? (EJ) : (tj_ + 1) * kBTileJ;                     \
+  for (int i = ti_ * (P).tile_i + (int)threadIdx.y; i < i1_; i += kBThreadsI)                \
+    for (int j = tj_ * kBTileJ + (int)threadIdx.x; j < j1_; j += kBTileJ)
+
+// Stage arrays: 0 the state, 1 the first stage buffer, 2 the second.
+template <class T>
+__device__ __forceinline__ double* b_arr_u(const BProb<T>& P, int code) {
+  return code == 0 ? P.u : code == 1 ? P.us1 : P.us2;
+}
+template <class T>
+__device__ __forceinline__ double* b_arr_v(const BProb<T>& P, int code) {
+  return code == 0 ? P.v : code == 1 ? P.vs1 : P.vs2;
+}
+
+// ---- step bookkeeping -------------------------------------------------------
+// max|u|, max|v| over the physical faces and the non-finite count of u, v, p:
+// the inputs of the time-step control (pycfd/core/timestepper.py:94-142).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_stats(const BProb<T>* __restrict__ probs,
+                                                        const int2* __restrict__ map, BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const int nx = P.g.nx, ny = P.g.ny;
+  const long W = ny + 2, WV = ny + 3;
+  const double *u = P.u, *v = P.v, *p = P.p;
+  double acc[3] = {0, 0, 0};
+  {
+    B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
+      if (j < ny + 2) {
+        const double a = u[(long)i * W + j];
+        if (!isfinite(a)) acc[2] += 1.0;
+        if (i >= 1 && i <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
+      }
+      if (i < nx + 2) {
+        const double a = v[(long)i * WV + j];
+        if (!isfinite(a)) acc[2] += 1.0;
+        if (i >= 1 && i <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
+        if (j < ny + 2 && !isfinite(p[(long)i * W + j])) acc[2] += 1.0;
+      }
+    }
+  }
+  b_reduce<3, 0x3u>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    P.S[S_STAT0] = t[0];
+    P.S[S_STAT0 + 1] = t[1];
+    P.S[S_STAT0 + 7] = t[2];
+  });
+}
+
+// Per-problem time step (one thread per problem): the single-problem control;
+// a problem whose health flags trip, or whose end time or step count is
+// reached, freezes.
+template <class T>
+__global__ void k_b_dt(const BProb<T>* __restrict__ probs, int nprob) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nprob) return;
+  const BProb<T>& P = probs[k];
+  if (P.I[I_FROZEN]) return;
+  if (P.dtc.t_end - P.S[S_T] <= 0.0 || P.I[I_STEPS] >= P.max_steps) {
+    P.I[I_FROZEN] = 2;
+    return;
+  }
+  adaptive_dt_update(P.S, P.I, P.dtc);
+  if (P.I[I_HEALTH] != 0) {   // the step is not taken: state stays at the last good step
+    P.I[I_FROZEN] = 1;
+    P.S[S_T] -= P.S[S_DT];
+    P.I[I_STEPS] -= 1;
+  }
+}
+
+// Fixed step parameters (initial projection: dt = 1; fixed-dt runs).
+template <class T>
+__global__ void k_b_set_dt(const BProb<T>* __restrict__ probs, int nprob, double dt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nprob) return;
+  const BProb<T>& P = probs[k];
+  if (P.I[I_FROZEN]) return;
+  P.S[S_DT] = dt;
+  P.S[S_BLEND] = 0.0;
+  P.I[I_TOTAL_IT] = 0;
+}
+
+// ---- stencils ----------------------------------------------------------------
+// Predictor of one Runge-Kutta stage: out = U + dt*rhs on the solvable faces,
+// U elsewhere, U = ca*a + cb*b (b absent: U = a) (pycfd/core/solver.py:619-622).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __restrict__ probs,
+                                                            const int2* __restrict__ map, int src_a,
+                                                            int src_b, double ca, double cb, int dst) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const Geo& g = P.g;
+  const int nx = g.nx, ny = g.ny;
+  const StageIn u{b_arr_u(P, src_a), src_b >= 0 ? b_arr_u(P, src_b) : nullptr, ca, cb};
+  const StageIn v{b_arr_v(P, src_a), src_b >= 0 ? b_arr_v(P, src_b) : nullptr, ca, cb};
+  double* us = b_arr_u(P, dst);
+  double* vs = b_arr_v(P, dst);
+  const double dt = P.S[S_DT], blend = P.S[S_BLEND];
+  B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
+    if (j < ny + 2) {
+      const long k = (long)i * (ny + 2) + j;
+      double val = u[k];
+      if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
+        val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
+      us[k] = val;
+    }
+    if (i < nx + 2) {
+      const long k = (long)i * (ny + 3) + j;
+      double val = v[k];
+      if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
+        val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
+      vs[k] = val;
+    }
+  }
+}
+
+// Boundary program of every problem, one block each; p_ghosts first rebuilds
+// the ghost ring of p from the solution x (the single-problem path does this
+// in the correction's last block).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_boundary(const BProb<T>* __restrict__ probs, int arr,
+                                                           BcProgram prog, int p_ghosts) {
+  const BProb<T>& P = probs[blockIdx.x];
+  if (b_frozen(P)) return;
+  double* u = b_arr_u(P, arr);
+  double* v = b_arr_v(P, arr);
+  if (p_ghosts) {
+    p_ghost_ring(P.p, P.x, P.g, P.bc_kind);
+    __syncthreads();
+  }
+  for (int s = 0; s < 8 && prog.op[s] != OP_END; ++s) {
+    switch (prog.op[s]) {
+      case OP_VEL_PRED: bc_velocity(u, v, P.g, P.bc, true); break;
+      case OP_VEL_CORR: bc_velocity(u, v, P.g, P.bc, false); break;
+      case OP_MASS: if (P.bc.has_outlet) bc_mass_balance(u, v, P.g, P.bc); break;
+      case OP_MASK_NONE:
+      case OP_MASK_RESET:
+      case OP_MASK_ACC: if (P.bc.n_mask_u + P.bc.n_mask_v > 0) bc_mask(u, v, P.bc, P.S, prog.op[s]); break;
+      case OP_WRAP_FACES: bc_wrap_faces(u, v, P.g); break;
+      default: break;
+    }
+  }
+}
+
+// Poisson right-hand side b = div(u*)/dt + Dirichlet terms on solvable rows and
+// its fluid mean (pycfd/core/solver.py:659-661, pycfd/core/pressure.py:300-308).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restrict__ probs,
+                                                          const int2* __restrict__ map, int arr,
+                                                          BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const Geo& g = P.g;
+  const double* u = b_arr_u(P, arr);
+  const double* v = b_arr_v(P, arr);
+  const double dt = P.S[S_DT];
+  double acc[1] = {0.0};
+  {
+    B_TILE_CELLS(P, e.y) {
+      const int c = i * g.ny + j;
+      const uint8_t f = P.flags[c];
+      double val = 0.0;
+      if (f & F_SOLV) {
+        val = (cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt) * 1.0 + fine_bc(f, i, j, g);
+        acc[0] += val;
+      }
+      P.b[c] = val;
+    }
+  }
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles,
+              [&](double* t) { P.S[S_MEAN_B] = g.n_fluid ? t[0] / g.n_fluid : 0.0; });
+}
+
+// Velocity correction on the solvable faces and the interior of p
+// (pycfd/core/solver.py:665-682); the ghost ring follows in k_b_boundary.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_correct(const BProb<T>* __restrict__ probs,
+                                                          const int2* __restrict__ map, int arr) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const Geo& g = P.g;
+  const int nx = g.nx, ny = g.ny;
+  double* u = b_arr_u(P, arr);
+  double* v = b_arr_v(P, arr);
+  const double* x = P.x;
+  double* p = P.p;
+  const double dt = P.S[S_DT];
+  B_TILE_EXT(P, e.y, nx + 2, ny + 3) {
+    if (i >= 1 && i <= nx && j >= 1 && j <= ny) p[(long)i * (ny + 2) + j] = x[(long)(i - 1) * ny + (j - 1)];
+    if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny) {
+      const long k = (long)i * (ny + 2) + j;
+      u[k] = u[k] - dt * (p_at(x, i, j, g) - p_at(x, i - 1, j, g)) / g.dx;
+    }
+    if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi) {
+      const long k = (long)i * (ny + 3) + j;
+      v[k] = v[k] - dt * (p_at(x, i, j, g) - p_at(x, i, j - 1, g)) / g.dy;
+    }
+  }
+}
+
+// u = ca*a + cb*b over whole ghosted arrays, in place into the state
+// (pycfd/core/solver.py:705-721).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_combine(const BProb<T>* __restrict__ probs,
+                                                          const int2* __restrict__ map, int src_b,
+                                                          double ca, double cb) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const int nx = P.g.nx, ny = P.g.ny;
+  const double* bu = b_arr_u(P, src_b);
+  const double* bv = b_arr_v(P, src_b);
+  B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
+    if (j < ny + 2) {
+      const long k = (long)i * (ny + 2) + j;
+      P.u[k] = ca * P.u[k] + cb * bu[k];
+    }
+    if (i < nx + 2) {
+      const long k = (long)i * (ny + 3) + j;
+      P.v[k] = ca * P.v[k] + cb * bv[k];
+    }
+  }
+}
+
+// ---- FP64 MG-PCG ---------------------------------------------------------------
+// b <- b - mean (solvable rows), r = b - A x from the warm start x, norms and
+// the convergence test before the first pass (scipy cg, pressure.py:300-308).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __restrict__ probs,
+                                                           int nprob, const int2* __restrict__ map,
+                                                           double tol, int maxiter, BShared sh,
+                                                           LoopCtl loop) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_frozen(P)) {
+    const Geo& g = P.g;
+    const double mean = P.singular ? P.S[S_MEAN_B] : 0.0;
+    double acc[3] = {0, 0, 0};
+    {
+      B_TILE_CELLS(P, e.y) {
+        const int c = i * g.ny + j;
+        const uint8_t f = P.flags[c];
+        const double bc = (f & F_SOLV) ? P.b[c] - mean : 0.0;
+        P.b[c] = bc;
+        const double ax = fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return (double)P.xs[k]; });
+        const double rc = bc - ax;
+        P.r[c] = (T)rc;
+        acc[0] += bc * bc;
+        acc[1] += rc * rc;
+        if (f & F_SOLV) acc[2] += rc;
+      }
+    }
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+      double* S = P.S;
+      int* I = P.I;
+      S[S_BNORM2] = t[0];
+      S[S_ATOL] = tol * sqrt(t[0]);
+      S[S_RNORM2] = t[1];
+      S[S_RHO_PREV] = 1.0;
+      S[S_SUM_R] = t[2];
+      S[S_MEAN_R] = g.n_fluid ? t[2] / g.n_fluid : 0.0;
+      I[I_IT] = 0;
+      I[I_ZERO_RHS] = (t[0] == 0.0);
+      const bool conv = (t[0] == 0.0) || (sqrt(t[1]) < S[S_ATOL]);
+      I[I_CONVERGED] = conv;
+      I[I_DONE] = conv || maxiter <= 0;
+      I[I_STATUS] = 0;
+    });
+  }
+  b_loop_ticket(probs, nprob, sh, TK_CG, I_DONE, 1, maxiter + 1, loop);
+}
+
+// p = (z - mean z) + beta p_old on solvable rows, q = A p, p.q -> alpha.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restrict__ probs,
+                                                        const int2* __restrict__ map, BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_solving(P)) return;
+  const Geo& g = P.g;
+  const bool first = P.I[I_IT] == 0;
+  const double beta = first ? 0.0 : P.S[S_RHO] / P.S[S_RHO_PREV];
+  const double mz = P.S[S_MEAN_Z];
+  const uint8_t* flags = P.flags;
+  const T* zraw = P.z;
+  const T* p_old = P.pa;
+  auto pval = [&](int k, int, int) -> double {
+    const double z = (flags[k] & F_SOLV) ? (double)zraw[k] - mz : 0.0;
+    if (first) return (double)(T)z;
+    return (double)(T)((double)p_old[k] * beta + z);
+  };
+  double acc[1] = {0.0};
+  {
+    B_TILE_CELLS(P, e.y) {
+      const int c = i * g.ny + j;
+      const double pc = pval(c, i, j);
+      const double qc = fine_apply<double>(flags[c], i, j, c, g, pval);
+      P.pb[c] = (T)pc;
+      P.q[c] = (T)qc;
+      acc[0] += pc * qc;
+    }
+  }
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    P.S[S_PQ] = t[0];
+    P.S[S_ALPHA] = P.S[S_RHO] / t[0];
+  });
+}
+
+// x += alpha p, r -= alpha q, p kept for the next pass; ||r||^2 and sum(r);
+// the next pass's convergence test; launch-wide loop decision.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
+                                                        const int2* __restrict__ map, int maxiter,
+                                                        BShared sh, LoopCtl loop) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_solving(P)) {
+    const Geo& g = P.g;
+    const double alpha = P.S[S_ALPHA];
+    double acc[2] = {0, 0};
+    {
+      B_TILE_CELLS(P, e.y) {
+        const int c = i * g.ny + j;
+        const T pc = P.pb[c];
+        const double xc = (double)P.xs[c] + alpha * (double)pc;
+        const double rc = (double)(T)((double)P.r[c] - alpha * (double)P.q[c]);
+        P.pa[c] = pc;
+        P.xs[c] = (T)xc;
+        P.r[c] = (T)rc;
+        acc[0] += rc * rc;
+        if (P.flags[c] & F_SOLV) acc[1] += rc;
+      }
+    }
+    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+      double* S = P.S;
+      int* I = P.I;
+      const int it = I[I_IT] + 1;
+      I[I_IT] = it;
+      I[I_TOTAL_IT] += 1;
+      S[S_RNORM2] = t[0];
+      S[S_SUM_R] = t[1];
+      S[S_MEAN_R] = g.n_fluid ? t[1] / g.n_fluid : 0.0;
+      const bool conv = sqrt(t[0]) < S[S_ATOL];
+      I[I_CONVERGED] = conv;
+      I[I_DONE] = conv || it >= maxiter;
+    });
+  }
+  b_loop_ticket(probs, nprob, sh, TK_CG, I_DONE, 0, maxiter + 1, loop);
+}
+
+// ||b - A x||/||b|| and the fluid mean of x (pycfd/core/pressure.py:310-322).
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __restrict__ probs,
+                                                               const int2* __restrict__ map, double tol,
+                                                               BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const Geo& g = P.g;
+  const bool zero = P.I[I_ZERO_RHS] != 0;
+  const double* x = P.x;
+  auto xv = [&](int k, int, int) -> double { return zero ? 0.0 : x[k]; };
+  double acc[2] = {0, 0};
+  {
+    B_TILE_CELLS(P, e.y) {
+      const int c = i * g.ny + j;
+      const uint8_t f = P.flags[c];
+      const double rc = P.b[c] - fine_apply<double>(f, i, j, c, g, xv);
+      acc[0] += rc * rc;
+      if (f & F_SOLV) acc[1] += xv(c, i, j);
+    }
+  }
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    double* S = P.S;
+    const double nb = sqrt(S[S_BNORM2]);
+    S[S_RESID] = sqrt(t[0]) / (nb > 1e-300 ? nb : 1.0);
+    if (!P.I[I_CONVERGED] && S[S_RESID] > fmax(tol * 10.0, 1e-8)) P.I[I_STATUS] = -3;
+    S[S_MEAN_X] = (P.singular && g.n_fluid) ? t[1] / g.n_fluid : 0.0;
+  });
+}
+
+// x <- x - mean on solvable rows, 0 elsewhere.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_finish_apply(const BProb<T>* __restrict__ probs,
+                                                               const int2* __restrict__ map) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P)) return;
+  const bool zero = P.I[I_ZERO_RHS] != 0;
+  const double m = P.S[S_MEAN_X];
+  B_TILE_CELLS(P, e.y) {
+    const int c = i * P.g.ny + j;
+    P.x[c] = (!zero && (P.flags[c] & F_SOLV)) ? P.x[c] - m : 0.0;
+  }
+}
+
+// ---- mixed form: FP64 iterative refinement around the FP32 MG-PCG -----------
+// One refinement pass per problem (see k_ir_residual): r = b - A x in FP64, the
+// outer test ||r|| < tol ||b||, and the inner solve A e = r set up from e = 0.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __restrict__ probs,
+                                                              int nprob, const int2* __restrict__ map,
+                                                              double tol, double inner_tol,
+                                                              int max_passes, int first, BShared sh,
+                                                              LoopCtl outer) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_frozen(P) && (first || !P.I[I_IR_DONE])) {
+    const Geo& g = P.g;
+    const double mean = (first && P.singular) ? P.S[S_MEAN_B] : 0.0;
+    double acc[3] = {0, 0, 0};
+    {
+      B_TILE_CELLS(P, e.y) {
+        const int c = i * g.ny + j;
+        const uint8_t f = P.flags[c];
+        double bc = P.b[c];
+        if (first) {
+          bc = (f & F_SOLV) ? bc - mean : 0.0;
+          P.b[c] = bc;
+        }
+        const double rc = bc - fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return P.x[k]; });
+        P.r[c] = (T)rc;
+        P.xs[c] = (T)0;
+        acc[0] += rc * rc;
+        if (f & F_SOLV) acc[1] += (double)(T)rc;
+        if (first) acc[2] += bc * bc;
+      }
+    }
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+      double* S = P.S;
+      int* I = P.I;
+      if (first) {
+        S[S_IR_BNORM] = sqrt(t[2]);
+        S[S_BNORM2] = t[2];
+        I[I_IR_IT] = 0;
+        I[I_ZERO_RHS] = (t[2] == 0.0);
+        I[I_STATUS] = 0;
+      }
+      const double nb = S[S_IR_BNORM];
+      S[S_IR_RNORM2] = t[0];
+      const bool conv = (nb == 0.0) || (sqrt(t[0]) < tol * nb);
+      const bool done = conv || I[I_IR_IT] >= max_passes;
+      I[I_CONVERGED] = conv;
+      I[I_IR_DONE] = done;
+      S[S_ATOL] = inner_tol * sqrt(t[0]);
+      S[S_RNORM2] = t[0];
+      S[S_RHO_PREV] = 1.0;
+      S[S_SUM_R] = t[1];
+      S[S_MEAN_R] = g.n_fluid ? t[1] / g.n_fluid : 0.0;
+      I[I_IT] = 0;
+      I[I_DONE] = done;
+    });
+  }
+  b_loop_ticket(probs, nprob, sh, TK_IR, I_IR_DONE, first, max_passes + 1, outer);
+}
+
+// Arm the inner loop: does any problem run an inner solve in this pass?
+template <class T>
+__global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShared sh, LoopCtl inner) {
+  int any = 0;
+  for (int p = threadIdx.x; p < nprob; p += blockDim.x)
+    if (b_solving(probs[p])) any = 1;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    sh.any[TK_ARM] = any;
+    sh.iters[TK_CG] = 0u;   // the inner loop's passes count from here
+    inner.set(any != 0);
+    if (any) sh.passes[TK_ARM] += 1;
+  }
+}
+
+// x += e on solvable rows for the problems that ran this pass; count the pass.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_ir_update(const BProb<T>* __restrict__ probs,
+                                                            const int2* __restrict__ map) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (b_frozen(P) || P.I[I_IR_DONE]) return;
+  {
+    B_TILE_CELLS(P, e.y) {
+      const int c = i * P.g.ny + j;
+      if (P.flags[c] & F_SOLV) P.x[c] = P.x[c] + (double)P.xs[c];
+    }
+  }
+  if (e.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) P.I[I_IR_IT] += 1;
+}
+
+// ---- V-cycle ---------------------------------------------------------------------
+// Level-0 (matrix-free) phases.  The right-hand side is the CG residual r
+// projected onto the active set (r - mean r on solvable rows,
+// pycfd/core/multigrid.py:453-458).  Buffers: 0 level-0 xa, 1 level-0 xb, 2 z.
+enum BFineMode { FM_PRE = 0, FM_WDB, FM_SMOOTH, FM_RESID, FM_LAST };
+
+template <class T>
+__device__ __forceinline__ T* b_fine_buf(const BProb<T>& P, int sel) {
+  return sel == 0 ? P.lxa[0] : sel == 1 ? P.lxb[0] : P.z;
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict__ probs,
+                                                       const BHier<T>* __restrict__ hiers,
+                                                       const int2* __restrict__ map, int src, int dst,
+                                                       BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_solving(P)) return;
+  const Geo& g = P.g;
+  const double w = hiers[P.hier].w0;
+  const uint8_t* flags = P.flags;
+  const T* r = P.r;
+  const double mr = P.singular ? P.S[S_MEAN_R] : 0.0;
+  auto bf = [&](int k) -> double { return (flags[k] & F_SOLV) ? (double)r[k] - mr : 0.0; };
+  const T* x = b_fine_buf(P, src);
+  T* xo = b_fine_buf(P, dst);
+  double acc[2] = {0, 0};
+  {
+    B_TILE_CELLS(P, e.y) {
+      const int c = i * g.ny + j;
+      const uint8_t f = flags[c];
+      if (MODE == FM_PRE) {
+        auto xv = [&](int k, int ii, int jj) -> double {
+          return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
+        };
+        xo[c] = (T)xv(c, i, j);
+        P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+      } else if (MODE == FM_WDB) {
+        xo[c] = (T)(fine_wdinv(f, i, j, g, w) * bf(c));
+      } else if (MODE == FM_RESID) {
+        auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
+        P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+      } else {
+        auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
+        const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
+                                      (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
+        xo[c] = (T)xn;
+        if (MODE == FM_LAST && (f & F_SOLV)) {
+          acc[0] += xn;
+          acc[1] += (double)r[c] * xn;
+        }
+      }
+    }
+  }
+  if (MODE != FM_LAST) return;
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    double* S = P.S;
+    const double m = (P.singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
+    S[S_MEAN_Z] = m;
+    S[S_RHO_PREV] = S[S_RHO];
+    S[S_RHO] = t[1] - m * S[S_SUM_R];
+  });
+}
+
+// ELL phases of coarse level d (and prolongation into level 0).  Row blocks of
+// kBRows rows; lanes per row from the hierarchy (runtime), so problems of
+// different structures share one launch.
+enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG };
+
+template <class T>
+__device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
+  if (d == P.nlev - 1) return P.lxa[d];   // the coarsest result is always in xa
+  return sel == 0 ? P.lxa[d] : P.lxb[d];
+}
+
+// Row dot product of E by L lanes (L a power of two, runtime), rows past the
+// end contribute nothing; every lane of the warp calls it.
+template <class T, class X>
+__device__ __forceinline__ double b_ell_row(const Ell<T>& E, int L, int row, int lane, X x) {
+  double acc = 0.0;
+  if (row < E.n) {
+    if (E.rowmajor) {
+      const long base = (long)row * E.K;
+      for (int k = lane; k < E.K; k += L) acc += (double)E.val[base + k] * x(E.col[base + k]);
+    } else {
+      for (int k = lane; k < E.K; k += L) {
+        const long at = (long)k * E.n + row;
+        acc += (double)E.val[at] * x(E.col[at]);
+      }
+    }
+  }
+  for (int o = L >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
+  return acc;
+}
+
+template <class T, int OP>
+__global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict__ probs,
+                                                      const BHier<T>* __restrict__ hiers,
+                                                      const int2* __restrict__ map, int d, int src,
+                                                      int dst) {
+  extern __shared__ double sb[];
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_solving(P)) return;
+  const BHier<T>& H = hiers[P.hier];
+  if (OP == EO_RESTRICT && e.y < 0) {
+    // coarsest level d: restriction and dense solve in this block
+    const BLevel<T>& Lc = H.lv[d];
+    const T* res = P.lres[d - 1];
+    const int L = Lc.lr, lane = threadIdx.x & (L - 1);
+    const int per = kBThreads / L;
+    for (int base = 0; base < Lc.R.n; base += per) {
+      const int row = base + (int)threadIdx.x / L;
+      const double s = b_ell_row(Lc.R, L, row, lane, [&](int c) { return (double)res[c]; });
+      if (lane == 0 && row < Lc.R.n) {
+        sb[row] = (double)(T)s;
+        P.lb[d][row] = (T)s;
+      }
+    }
+    __syncthreads();
+    const int wl = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kBThreads >> 5;
+    const int n = Lc.R.n;
+    for (int row = warp; row < n; row += nw) {
+      double acc = 0.0;
+      for (int k = wl; k < n; k += 32) acc += (double)H.C[(long)row * n + k] * sb[k];
+      acc = warp_sum(acc);
+      if (wl == 0) P.lxa[d][row] = (T)acc;
+    }
+    return;
+  }
+  // rows [r0, r1) of level d
+  const int n = (d == 0) ? P.g.nx * P.g.ny : H.lv[d].n;
+  const int r0 = e.y * kBRows, r1 = min(n, r0 + kBRows);
+  if (OP == EO_PROLONG) {
+    // x_d += P_{d+1} x_{d+1}
+    const BLevel<T>& Lc = H.lv[d + 1];
+    const int L = Lc.lp, lane = threadIdx.x & (L - 1), per = kBThreads / L;
+    const T* xc = b_lvl_x(P, d + 1, src);
+    T* xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
+    for (int base = r0; base < r1; base += per) {
+      const int row = base + (int)threadIdx.x / L;
+      const double s = b_ell_row(Lc.P, L, row < r1 ? row : Lc.P.n, lane, [&](int c) { return (double)xc[c]; });
+      if (lane == 0 && row < r1) xf[row] = (T)((double)xf[row] + s);
+    }
+    return;
+  }
+  const BLevel<T>& Lv = H.lv[d];
+  if (OP == EO_RESTRICT) {
+    const T* res = (d == 1) ? P.lres[0] : P.lres[d - 1];
+    const int L = Lv.lr, lane = threadIdx.x & (L - 1), per = kBThreads / L;
+    for (int base = r0; base < r1; base += per) {
+      const int row = base + (int)threadIdx.x / L;
+      const double s = b_ell_row(Lv.R, L, row < r1 ? row : Lv.R.n, lane, [&](int c) { return (double)res[c]; });
+      if (lane == 0 && row < r1) P.lb[d][row] = (T)s;
+    }
+    return;
+  }
+  const int L = Lv.la, lane = threadIdx.x & (L - 1), per = kBThreads / L;
+  const T* b = P.lb[d];
+  const T* wd = Lv.wd;
+  const T* x = b_lvl_x(P, d, src);
+  T* xo = b_lvl_x(P, d, dst);
+  for (int base = r0; base < r1; base += per) {
+    const int row = base + (int)threadIdx.x / L;
+    const int rr = row < r1 ? row : Lv.A.n;
+    if (OP == EO_PRE) {
+      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
+      if (lane == 0 && row < r1) {
+        const double bx = (double)b[row];
+        P.lxa[d][row] = (T)((double)wd[row] * bx);
+        P.lres[d][row] = (T)(bx - s);
+      }
+    } else if (OP == EO_SMOOTH) {
+      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)x[c]; });
+      if (lane == 0 && row < r1) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+    } else {   // EO_RESID
+      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)x[c]; });
+      if (lane == 0 && row < r1) P.lres[d][row] = (T)((double)b[row] - s);
+    }
+  }
+}
+
+// Per-problem status for the host: frozen flag, steps, solver iterations of
+// the last step, status, clock and dt.
+template <class T>
+__global__ void k_b_gather(const BProb<T>* __restrict__ probs, int nprob, int* __restrict__ iout,
+                           double* __restrict__ dout) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nprob) return;
+  const BProb<T>& P = probs[k];
+  iout[4 * k + 0] = P.I[I_FROZEN];
+  iout[4 * k + 1] = P.I[I_STEPS];
+  iout[4 * k + 2] = P.I[I_TOTAL_IT];
+  iout[4 * k + 3] = P.I[I_STATUS];
+  dout[2 * k + 0] = P.S[S_T];
+  dout[2 * k + 1] = P.S[S_DT];
+}
+
+}  // namespace pcfd

@@ -386,6 +386,7 @@ __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
     if (first) {
       S[S_IR_BNORM] = sqrt(t[2]);
       S[S_BNORM2_0] = t[2];
+      S[S_BNORM2] = t[2];   // ||b||^2 of the outer system: the reported residual's scale
       I[I_IR_IT] = 0;
       I[I_ZERO_RHS] = (t[2] == 0.0);
       I[I_STATUS] = 0;
@@ -397,7 +398,6 @@ __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
     I[I_CONVERGED] = conv;
     I[I_IR_DONE] = done;
     // inner solve from e = 0: its residual is r itself
-    S[S_BNORM2] = t[0];
     S[S_ATOL] = inner_tol * sqrt(t[0]);
     S[S_RNORM2] = t[0];
     S[S_SUM_R] = t[1];
@@ -438,9 +438,7 @@ struct DtControl {
   double blend;
 };
 
-__global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtControl c) {
-  pdl_begin();
-  if (threadIdx.x != 0) return;
+__device__ __forceinline__ void adaptive_dt_update(double* S, int* I, const DtControl& c) {
   const double umax = S[S_STAT0], vmax = S[S_STAT0 + 1];
   double dt = c.dt_cap;
   if (c.adaptive) {
@@ -460,6 +458,12 @@ __global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtCon
   S[S_T] = t + dt;
   I[I_STEPS] += 1;
   I[I_TOTAL_IT] = 0;
+}
+
+__global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtControl c) {
+  pdl_begin();
+  if (threadIdx.x != 0) return;
+  adaptive_dt_update(S, I, c);
 }
 
 __global__ void k_set_clock(double* __restrict__ S, int* __restrict__ I, double t) {

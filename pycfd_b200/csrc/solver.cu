@@ -1616,3 +1616,7 @@ extern "C" int pycfd_reduce_fields_noalloc(const double* u, const double* v, con
   o->finite = t[7] == 0.0;
   return 0;
 }
+
+// Batched stepping: compiled in this translation unit (it builds on the
+// single-problem solver's records and upload helpers).
+#include "batch_runtime.cuh"

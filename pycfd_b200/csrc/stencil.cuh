@@ -181,6 +181,68 @@ __device__ __forceinline__ double p_at(const double* x, int i, int j, const Geo&
   return x[(long)(i - 1) * ny + (j - 1)];
 }
 
+// Pressure ghost ring of the ghosted p from the interior solution x, run by
+// one thread block: rebuilt from zero (the reference fills a fresh zero
+// array) wall by wall in the reference's order, so the corners agree too
+// (pycfd/core/boundary.py:166-169, :293-303, :412-420).
+__device__ void p_ghost_ring(double* __restrict__ p, const double* __restrict__ x, const Geo& g,
+                             const int* __restrict__ bc_kind) {
+  const int nx = g.nx, ny = g.ny;
+  const long WP = ny + 2;
+  for (int k = threadIdx.x; k < 2 * (nx + 2) + 2 * ny; k += blockDim.x) {
+    long idx;
+    if (k < ny + 2) idx = k;                                         // row 0
+    else if (k < 2 * (ny + 2)) idx = (long)(nx + 1) * WP + (k - (ny + 2));  // row nx+1
+    else if (k < 2 * (ny + 2) + nx) idx = (long)(k - 2 * (ny + 2) + 1) * WP;  // col 0
+    else idx = (long)(k - 2 * (ny + 2) - nx + 1) * WP + ny + 1;            // col ny+1
+    p[idx] = 0.0;
+  }
+  __syncthreads();
+  for (int w = 0; w < 4; ++w) {
+    const int kind = bc_kind[w];
+    if (kind == BC_PERIODIC) continue;
+    const int axis = w < 2 ? 0 : 1;
+    const int ghost = (w == W_LEFT || w == W_BOTTOM) ? 0 : (axis == 0 ? nx + 1 : ny + 1);
+    const int inner = (w == W_LEFT || w == W_BOTTOM) ? 1 : (axis == 0 ? nx : ny);
+    const double pref = w == W_LEFT ? g.pref_w : w == W_RIGHT ? g.pref_e : w == W_BOTTOM ? g.pref_s : g.pref_n;
+    const int len = axis == 0 ? ny + 2 : nx + 2;
+    for (int k = threadIdx.x; k < len; k += blockDim.x) {
+      // interior value of the line (may itself be a ghost set earlier: read p)
+      const int ii = axis == 0 ? inner : k, jj = axis == 0 ? k : inner;
+      double in;
+      if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) in = x[(long)(ii - 1) * ny + (jj - 1)];
+      else in = p[(long)ii * WP + jj];
+      const double val = (kind == BC_PRESSURE_OUTLET) ? 2.0 * pref - in : in;
+      const int gi = axis == 0 ? ghost : k, gj = axis == 0 ? k : ghost;
+      p[(long)gi * WP + gj] = val;
+    }
+    __syncthreads();
+  }
+  if (g.periodic_x) {
+    for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
+      const double a = (k >= 1 && k <= ny) ? x[(long)(nx - 1) * ny + k - 1] : p[(long)nx * WP + k];
+      p[k] = a;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
+      const double a = (k >= 1 && k <= ny) ? x[(long)(k - 1)] : p[WP + k];
+      p[(long)(nx + 1) * WP + k] = a;
+    }
+    __syncthreads();
+  }
+  if (g.periodic_y) {
+    for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
+      const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny + ny - 1] : p[(long)k * WP + ny];
+      p[(long)k * WP] = a;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
+      const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny] : p[(long)k * WP + 1];
+      p[(long)k * WP + ny + 1] = a;
+    }
+  }
+}
+
 // Velocity correction u -= dt*(p[m]-p[m-1])/dx on exactly the solvable faces
 // (pycfd/core/solver.py:665-682), plus the ghosted pressure output.  The last
 // block fills the pressure ghost layer wall by wall in the reference's order
@@ -194,61 +256,8 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
   const int nx = g.nx, ny = g.ny;
   const double dt = dt_override > 0.0 ? dt_override : S[S_DT];
   if (blockIdx.x == gridDim.x - 1) {
-    // The other blocks copy the interior.  This block rebuilds the ghost ring
-    // from zero (the reference fills a fresh zero array) wall by wall.
-    const long WP = ny + 2;
-    for (int k = threadIdx.x; k < 2 * (nx + 2) + 2 * ny; k += blockDim.x) {
-      long idx;
-      if (k < ny + 2) idx = k;                                         // row 0
-      else if (k < 2 * (ny + 2)) idx = (long)(nx + 1) * WP + (k - (ny + 2));  // row nx+1
-      else if (k < 2 * (ny + 2) + nx) idx = (long)(k - 2 * (ny + 2) + 1) * WP;  // col 0
-      else idx = (long)(k - 2 * (ny + 2) - nx + 1) * WP + ny + 1;            // col ny+1
-      p[idx] = 0.0;
-    }
-    __syncthreads();
-    for (int w = 0; w < 4; ++w) {
-      const int kind = bc_kind[w];
-      if (kind == BC_PERIODIC) continue;
-      const int axis = w < 2 ? 0 : 1;
-      const int ghost = (w == W_LEFT || w == W_BOTTOM) ? 0 : (axis == 0 ? nx + 1 : ny + 1);
-      const int inner = (w == W_LEFT || w == W_BOTTOM) ? 1 : (axis == 0 ? nx : ny);
-      const double pref = w == W_LEFT ? g.pref_w : w == W_RIGHT ? g.pref_e : w == W_BOTTOM ? g.pref_s : g.pref_n;
-      const int len = axis == 0 ? ny + 2 : nx + 2;
-      for (int k = threadIdx.x; k < len; k += blockDim.x) {
-        // interior value of the line (may itself be a ghost set earlier: read p)
-        const int ii = axis == 0 ? inner : k, jj = axis == 0 ? k : inner;
-        double in;
-        if (ii >= 1 && ii <= nx && jj >= 1 && jj <= ny) in = x[(long)(ii - 1) * ny + (jj - 1)];
-        else in = p[(long)ii * WP + jj];
-        const double val = (kind == BC_PRESSURE_OUTLET) ? 2.0 * pref - in : in;
-        const int gi = axis == 0 ? ghost : k, gj = axis == 0 ? k : ghost;
-        p[(long)gi * WP + gj] = val;
-      }
-      __syncthreads();
-    }
-    if (g.periodic_x) {
-      for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
-        const double a = (k >= 1 && k <= ny) ? x[(long)(nx - 1) * ny + k - 1] : p[(long)nx * WP + k];
-        p[k] = a;
-      }
-      __syncthreads();
-      for (int k = threadIdx.x; k < ny + 2; k += blockDim.x) {
-        const double a = (k >= 1 && k <= ny) ? x[(long)(k - 1)] : p[WP + k];
-        p[(long)(nx + 1) * WP + k] = a;
-      }
-      __syncthreads();
-    }
-    if (g.periodic_y) {
-      for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
-        const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny + ny - 1] : p[(long)k * WP + ny];
-        p[(long)k * WP] = a;
-      }
-      __syncthreads();
-      for (int k = threadIdx.x; k < nx + 2; k += blockDim.x) {
-        const double a = (k >= 1 && k <= nx) ? x[(long)(k - 1) * ny] : p[(long)k * WP + 1];
-        p[(long)k * WP + ny + 1] = a;
-      }
-    }
+    // The other blocks copy the interior and update the faces.
+    p_ghost_ring(p, x, g, bc_kind);
     return;
   }
   // 2D sweep over rows i = 0..nx+1 (blocks in y), columns j = 0..ny+1 (threads)

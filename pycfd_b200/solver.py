@@ -106,6 +106,116 @@ class BoundaryInfo:
         return full
 
 
+def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind, options,
+                levels=None, cinv=None):
+    """The ``pycfd_solver_desc`` of one problem and the host arrays it points into.
+
+    Keep the returned list alive until the native call that reads the descriptor returns.
+    """
+    cfg = config
+    nx, ny = mesh.shape
+    d = _lib.SolverDesc()
+    d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, mesh.dx, mesh.dy, config.nu
+    d.body_fx, d.body_fy = cfg.body_force
+    keep = []
+    for w, wall in enumerate(WALLS):
+        spec = boundaries.specs[wall]
+        d.bc_kind[w] = _lib.BC_CODES[boundaries.kinds[wall].value]
+        d.bc_velocity[w] = spec.velocity
+        d.bc_p_ref[w] = spec.p_ref
+        if boundaries.kinds[wall] is BCKind.INLET and spec.profile == "parabolic":
+            prof = boundaries.profile(wall)
+            keep.append(prof)
+            d.bc_profile[w] = _lib.cast(prof, C.c_double)
+        else:
+            d.bc_profile[w] = _lib.cast(None, C.c_double)
+    solid_u8 = np.ascontiguousarray(solid.astype(np.uint8))
+    keep.append(solid_u8)
+    d.solid = _lib.cast(solid_u8 if has_obstacle else None, C.c_uint8)
+    if body_masks:
+        bid = np.zeros((nx, ny), np.uint8)
+        for kb, b in enumerate(body_masks):
+            bid[b] = kb + 1
+        keep.append(bid)
+        d.body_id = _lib.cast(bid, C.c_uint8)
+        d.n_bodies = len(body_masks)
+    else:
+        d.body_id = _lib.cast(None, C.c_uint8)
+        d.n_bodies = 0
+    d.solver_kind = _lib.SOLVER_CODES[kind.value]
+    d.tol = cfg.poisson_tol
+    d.maxiter = cfg.poisson_maxiter
+    d.sor_omega = cfg.sor_omega
+    d.mg_sweeps = cfg.mg_sweeps
+    d.time_scheme = _lib.SCHEME_CODES[TimeScheme(cfg.time_scheme).value]
+    d.precision = 1 if options.precision == "mixed" else 0
+    d.inner_tol = options.inner_tol
+    d.coarse_cluster_rows = int(options.coarse_cluster_rows)
+    d.sequential_launch = 0 if options.programmatic_launch else 1
+    if levels is not None:
+        arr = (_lib.MgLevel * len(levels))()
+        for l, lv in enumerate(levels):
+            e = arr[l]
+            e.n, e.shape_x, e.shape_y, e.weight = lv.n, lv.shape[0], lv.shape[1], lv.weight
+            wd = np.ascontiguousarray(lv.weighted_dinv, dtype=np.float64)
+            act = np.ascontiguousarray(lv.active.astype(np.uint8))
+            keep += [wd, act]
+            e.weighted_dinv = _lib.cast(wd, C.c_double)
+            e.active = _lib.cast(act, C.c_uint8)
+            A = lv.A.tocsr()
+            ap = np.ascontiguousarray(A.indptr, np.int64)
+            ai = np.ascontiguousarray(A.indices, np.int32)
+            ad = np.ascontiguousarray(A.data, np.float64)
+            keep += [ap, ai, ad]
+            e.a_indptr, e.a_indices, e.a_data = (_lib.cast(ap, C.c_int64), _lib.cast(ai, C.c_int32),
+                                                 _lib.cast(ad, C.c_double))
+            if lv.P is not None:
+                P = lv.P.tocsr()
+                pp = np.ascontiguousarray(P.indptr, np.int64)
+                pi = np.ascontiguousarray(P.indices, np.int32)
+                pd = np.ascontiguousarray(P.data, np.float64)
+                keep += [pp, pi, pd]
+                e.p_indptr, e.p_indices, e.p_data = (_lib.cast(pp, C.c_int64),
+                                                     _lib.cast(pi, C.c_int32),
+                                                     _lib.cast(pd, C.c_double))
+            else:
+                e.p_indptr = _lib.cast(None, C.c_int64)
+                e.p_indices = _lib.cast(None, C.c_int32)
+                e.p_data = _lib.cast(None, C.c_double)
+        cinv = np.ascontiguousarray(cinv, np.float64)
+        keep.append(cinv)
+        d.n_levels = len(levels)
+        d.levels = arr
+        d.coarsest_inverse = _lib.cast(cinv, C.c_double)
+        keep.append(arr)
+    else:
+        d.n_levels = 0
+        d.levels = C.cast(C.c_void_p(0), C.POINTER(_lib.MgLevel))
+        d.coarsest_inverse = _lib.cast(None, C.c_double)
+    return d, keep
+
+
+def dt_control_for(config, mesh, t_end: float = float("inf")):
+    """Device-side time-step control matching :class:`TimeStepper` for ``config``.
+
+    ``pycfd/core/timestepper.py:94-142``: CFL and viscous limits capped by ``config.dt``
+    (fixed ``config.dt`` when ``adaptive_dt`` is off), donor-cell blend policy.
+    """
+    nu = config.nu
+    dx, dy = mesh.dx, mesh.dy
+    visc = float("inf") if nu <= 0 else 0.8 / (2.0 * nu * (1.0 / dx ** 2 + 1.0 / dy ** 2))
+    c = _lib.DtControl()
+    c.adaptive = int(bool(config.adaptive_dt))
+    c.cfl = config.cfl_max
+    c.visc_limit = visc
+    c.dt_cap = config.dt
+    c.t_end = float(t_end)
+    central = AdvectionScheme(config.advection_scheme) is AdvectionScheme.CENTRAL
+    c.blend_mode = 0 if (central or config.upwind_blend is not None) else 1
+    c.blend = 0.0 if central else float(config.upwind_blend or 0.0)
+    return c
+
+
 class GpuPoissonSolver:
     """``PoissonSolverBase`` surface over the native solve (``pycfd/core/pressure.py:273-327``)."""
 
@@ -218,85 +328,9 @@ class ProjectionSolver:
             self.u_face_solid = self.v_face_solid = None
 
     def _create_native(self, kind: PressureSolver) -> None:
-        cfg, mesh = self.config, self.mesh
-        nx, ny = mesh.shape
-        d = _lib.SolverDesc()
-        d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, mesh.dx, mesh.dy, self.nu
-        d.body_fx, d.body_fy = cfg.body_force
-        keep = []
-        for w, wall in enumerate(WALLS):
-            spec = self.boundaries.specs[wall]
-            d.bc_kind[w] = _lib.BC_CODES[self.boundaries.kinds[wall].value]
-            d.bc_velocity[w] = spec.velocity
-            d.bc_p_ref[w] = spec.p_ref
-            if self.boundaries.kinds[wall] is BCKind.INLET and spec.profile == "parabolic":
-                prof = self.boundaries.profile(wall)
-                keep.append(prof)
-                d.bc_profile[w] = _lib.cast(prof, C.c_double)
-            else:
-                d.bc_profile[w] = _lib.cast(None, C.c_double)
-        solid_u8 = np.ascontiguousarray(self.solid.astype(np.uint8))
-        keep.append(solid_u8)
-        d.solid = _lib.cast(solid_u8 if self.has_obstacle else None, C.c_uint8)
-        if self.body_masks:
-            bid = np.zeros((nx, ny), np.uint8)
-            for kb, b in enumerate(self.body_masks):
-                bid[b] = kb + 1
-            keep.append(bid)
-            d.body_id = _lib.cast(bid, C.c_uint8)
-            d.n_bodies = len(self.body_masks)
-        else:
-            d.body_id = _lib.cast(None, C.c_uint8)
-            d.n_bodies = 0
-        d.solver_kind = _lib.SOLVER_CODES[kind.value]
-        d.tol = cfg.poisson_tol
-        d.maxiter = cfg.poisson_maxiter
-        d.sor_omega = cfg.sor_omega
-        d.mg_sweeps = cfg.mg_sweeps
-        d.time_scheme = _lib.SCHEME_CODES[TimeScheme(cfg.time_scheme).value]
-        d.precision = 1 if self.options.precision == "mixed" else 0
-        d.inner_tol = self.options.inner_tol
-        d.coarse_cluster_rows = int(self.options.coarse_cluster_rows)
-        d.sequential_launch = 0 if self.options.programmatic_launch else 1
-        if self._levels is not None:
-            arr = (_lib.MgLevel * len(self._levels))()
-            for l, lv in enumerate(self._levels):
-                e = arr[l]
-                e.n, e.shape_x, e.shape_y, e.weight = lv.n, lv.shape[0], lv.shape[1], lv.weight
-                wd = np.ascontiguousarray(lv.weighted_dinv, dtype=np.float64)
-                act = np.ascontiguousarray(lv.active.astype(np.uint8))
-                keep += [wd, act]
-                e.weighted_dinv = _lib.cast(wd, C.c_double)
-                e.active = _lib.cast(act, C.c_uint8)
-                A = lv.A.tocsr()
-                ap = np.ascontiguousarray(A.indptr, np.int64)
-                ai = np.ascontiguousarray(A.indices, np.int32)
-                ad = np.ascontiguousarray(A.data, np.float64)
-                keep += [ap, ai, ad]
-                e.a_indptr, e.a_indices, e.a_data = (_lib.cast(ap, C.c_int64), _lib.cast(ai, C.c_int32),
-                                                     _lib.cast(ad, C.c_double))
-                if lv.P is not None:
-                    P = lv.P.tocsr()
-                    pp = np.ascontiguousarray(P.indptr, np.int64)
-                    pi = np.ascontiguousarray(P.indices, np.int32)
-                    pd = np.ascontiguousarray(P.data, np.float64)
-                    keep += [pp, pi, pd]
-                    e.p_indptr, e.p_indices, e.p_data = (_lib.cast(pp, C.c_int64),
-                                                         _lib.cast(pi, C.c_int32),
-                                                         _lib.cast(pd, C.c_double))
-                else:
-                    e.p_indptr = _lib.cast(None, C.c_int64)
-                    e.p_indices = _lib.cast(None, C.c_int32)
-                    e.p_data = _lib.cast(None, C.c_double)
-            cinv = np.ascontiguousarray(self._cinv, np.float64)
-            keep.append(cinv)
-            d.n_levels = len(self._levels)
-            d.levels = arr
-            d.coarsest_inverse = _lib.cast(cinv, C.c_double)
-        else:
-            d.n_levels = 0
-            d.levels = C.cast(C.c_void_p(0), C.POINTER(_lib.MgLevel))
-            d.coarsest_inverse = _lib.cast(None, C.c_double)
+        d, keep = native_desc(self.config, self.mesh, self.boundaries, self.solid,
+                              self.has_obstacle, self.body_masks, kind, self.options,
+                              self._levels, self._cinv)
         h = C.c_void_p()
         _lib.check(self._L.pycfd_solver_create(C.byref(d), C.byref(h)))
         self._h = h
@@ -443,20 +477,7 @@ class ProjectionSolver:
 
     def dt_control(self):
         """Device-side time-step control matching :class:`TimeStepper` for this configuration."""
-        cfg = self.config
-        nu = self.nu
-        dx, dy = self.mesh.dx, self.mesh.dy
-        visc = float("inf") if nu <= 0 else 0.8 / (2.0 * nu * (1.0 / dx ** 2 + 1.0 / dy ** 2))
-        c = _lib.DtControl()
-        c.adaptive = int(bool(cfg.adaptive_dt))
-        c.cfl = cfg.cfl_max
-        c.visc_limit = visc
-        c.dt_cap = cfg.dt
-        c.t_end = float("inf")
-        central = AdvectionScheme(cfg.advection_scheme) is AdvectionScheme.CENTRAL
-        c.blend_mode = 0 if (central or cfg.upwind_blend is not None) else 1
-        c.blend = 0.0 if central else float(cfg.upwind_blend or 0.0)
-        return c
+        return dt_control_for(self.config, self.mesh)
 
     def set_clock(self, t: float = 0.0) -> None:
         """Reset the device clock, step counter and health flags of device-side stepping."""
