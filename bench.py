@@ -203,47 +203,172 @@ def cpu_baseline(steps=3):
                       f"({el:.1f} s; setup {setup:.1f} s excluded); NumPy/SciPy, one thread"}
 
 
+def batch_cpu_baseline(cfgs, steps=1):
+    """The oracle on one cavity of each grid size of the batch (bounded sample),
+    extrapolated to the batch by cell count."""
+    from oracle import OracleSolver
+    from oracle.projection import OracleStepper
+    sample, seen = [], set()
+    for c in cfgs:
+        if c.nx not in seen:
+            seen.add(c.nx)
+            sample.append(c)
+    cells = el = 0.0
+    for c in sample:
+        s = OracleSolver(c)
+        u, v, p = s.initialize()
+        stp = OracleStepper(s)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            u, v, p = s.step(u, v, stp.compute_dt(u, v))
+        el += time.perf_counter() - t0
+        cells += c.nx * c.ny * steps
+    return {"value": cells / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} adaptive RK3 step(s) of one cavity per grid size "
+                      f"({', '.join(str(c.nx) for c in sample)}) after initialisation, "
+                      f"{el:.1f} s; NumPy/SciPy, one thread; batch figure = sample cells/s"}
+
+
 def run_batch(args, world, rank, local):
-    """Batched cavities: aggregate cell-updates/s of the whole batch (replicas across ranks)."""
+    """256 seeded lid-driven cavities of uneven size, Re and lid speed: the batched engine
+    (every stage one launch over the whole batch), with the plain FP64 path -- one
+    single-problem solver per cavity, graphs replayed on a pool of streams -- beside it."""
     import torch
     torch.cuda.set_device(local)
-    from pycfd_b200.batch import Autotuner, BatchRunner, cavity_batch_configs
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from pycfd_b200 import _lib
+    from pycfd_b200.batch import (BatchAutotuner, BatchedSolver, BatchOptions, BatchRunner,
+                                  cavity_batch_configs)
+    from pycfd_b200.solver import GpuOptions
     cfgs = cavity_batch_configs(count=args.batch, seed=0)
     t0 = time.perf_counter()
-    tuner = Autotuner(allowed_precisions=("mixed", "fp64") if args.precision == "mixed" else ("fp64",))
-    runner = BatchRunner(cfgs, streams=args.streams, autotuner=tuner)
+    if args.autotune:
+        opts = BatchAutotuner(allowed_precisions=(args.precision,)).choose(cfgs)
+    else:
+        opts = BatchOptions(precision=args.precision, tile_rows=args.tile_rows,
+                            mg_sweeps=args.mg_sweeps, inner_tol=args.inner_tol,
+                            coarse_level=args.coarse_level)
+    b = BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
-    runner.step(args.warmup)
+    rec = not args.eager
+    b.step(args.warmup, record=rec)
     torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = Clocks(local)
-    a.record()
-    runner.step(args.steps)
-    b.record()
+    b.launches(0)
+    n_launch0 = _lib.load().pycfd_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local) if rank == 0 else None
+    if dist:
+        dist.barrier()
     torch.cuda.synchronize()
-    ck = clocks.stop()
-    ms = a.elapsed_time(b)
-    rep = runner.report()
-    value = runner.cells * args.steps / (ms / 1e3)
-    choices = {}
-    for cfg, ch in zip(cfgs, runner.choices):
-        choices.setdefault(f"{cfg.nx}", ch)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-            "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)",
-                       "cells": runner.cells, "sizes": sorted({c.nx for c in cfgs}),
-                       "streams": args.streams, "autotuned": choices, "setup_s": setup,
-                       "diverged": sum(r["diverged"] for r in rep),
-                       "cell_update": "one cell advanced by one RK3 step, summed over the batch"},
-            "clocks": ck}
-    print(json.dumps(line), flush=True)
+    ev0.record()
+    b.step(args.steps, record=rec)
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ck = clocks.stop() if clocks else None
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+    launches = b.launches(args.steps) if rec else int(_lib.load().pycfd_launch_count() - n_launch0)
+    value = world * b.cells * args.steps / (ms / 1e3)
+    st = b.status()
+    its = st["iterations"]
+    max_div = max(b.field_stats(k).max_div for k in range(len(b)))
+    # roofline: the batched CG direction kernel over one eager step
+    s_bytes = 4 if opts.precision == "mixed" else 8
+    pq_ms, pq_n, pq_its = b.profile(1)
+    cells = np.array([c.nx * c.ny for c in cfgs], dtype=np.float64)
+    pq_bytes = float((pq_its * cells).sum()) * (4 * s_bytes + 1)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = pq_bytes / (pq_ms / 1e3) / 1e9 if pq_ms > 0 else None
+    roof = {"bound": "hbm", "kernel": "k_b_cg_pq (batched CG direction p = z + beta p, q = A p, p.q)",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "traffic": None,
+            "bytes_per_launch": pq_bytes / max(pq_n, 1), "us_per_launch": 1e3 * pq_ms / max(pq_n, 1),
+            "launches": pq_n, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "timing": "CUDA events around each eager launch over one step; bytes = sum over "
+                      "problems of CG iterations x cells x (4 vectors x element + 1 flag byte)"}
+    # end to end: (u, v) of every cavity from pinned host memory, one step, (u, v, p) back
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
+    e2e = None
+    if e2e_steps:
+        b.step_host(1)
+        t0 = time.perf_counter()
+        b.step_host(e2e_steps)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        h2d, d2h = b.state_bytes()
+        e2e = {"value": world * b.cells * e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    plain = None
+    if not args.no_plain:
+        # the plain FP64 path on the same batch: per-problem recorded steps on 16 streams
+        runner = BatchRunner(cfgs, streams=16, options=GpuOptions(precision="fp64"))
+        runner.step(2)
+        torch.cuda.synchronize()
+        k_plain = max(2, min(args.steps, 5))
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        runner.step(k_plain)
+        p1.record()
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain = {"value": b.cells * k_plain / (pms / 1e3), "ms_per_step": pms / k_plain,
+                 "steps": k_plain, "form": "fp64, one single-problem solver per cavity, "
+                                           "recorded steps replayed on 16 streams"}
+        del runner
+    if rank == 0:
+        sizes = {}
+        for c in cfgs:
+            sizes[str(c.nx)] = sizes.get(str(c.nx), 0) + 1
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64/f32" if opts.precision == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)",
+                           "cells": b.cells, "sizes": sizes, "re": "log-uniform 100..2000",
+                           "lid": "uniform 0.5..1.5", "pressure_solver": "mgcg",
+                           "poisson_tol": cfgs[0].poisson_tol, "dt": "adaptive, CFL 0.5, per cavity",
+                           "options": opts.__dict__, "autotuned": bool(args.autotune),
+                           "setup_s": setup, "structures": b.structures,
+                           "cg_iterations_per_step": float(np.mean(its)),
+                           "stopped": int((st["frozen"] != 0).sum()), "max_div": max_div,
+                           "parallelism": f"replicas x{world}",
+                           "l2": "working set larger than L2 (no flush needed)",
+                           "cell_update": "one cell advanced by one RK3 step, summed over the batch",
+                           "plain_fp64_path": plain},
+                "e2e": e2e, "clocks": ck, "roofline": roof, "gpu_launches": launches}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = batch_cpu_baseline(cfgs)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     import torch  # noqa: F401  (same process layout as the GPU arm)
+    if args.workload == "batch":
+        from pycfd_b200.batch import cavity_batch_configs
+        cb = batch_cpu_baseline(cavity_batch_configs(count=args.batch, seed=0))
+        line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     steps = max(1, min(args.steps, 4))
     cb = cpu_baseline(steps)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
@@ -348,15 +473,27 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="default: fp64 for the vortex, mixed for the batch")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--eager", action="store_true", help="launch kernels one by one (no CUDA graph)")
     ap.add_argument("--workload", default="tgv512", choices=["tgv512", "batch"],
                     help="tgv512: the headline single-domain workload; batch: seeded cavity batch")
     ap.add_argument("--batch", type=int, default=256, help="problems in the batch workload")
-    ap.add_argument("--streams", type=int, default=16, help="streams the batch is spread over")
+    ap.add_argument("--autotune", action="store_true",
+                    help="batch: pick tiles, sweeps, coarse level and inner tolerance by timing (cached)")
+    ap.add_argument("--tile-rows", type=int, default=32, choices=[8, 16, 32, 64],
+                    help="batch: rows per fine-level tile")
+    ap.add_argument("--mg-sweeps", type=int, default=1, help="batch: smoothing sweeps per level")
+    ap.add_argument("--coarse-level", type=int, default=0,
+                    help="batch: multigrid levels from this one down in one block per problem (0: off)")
+    ap.add_argument("--inner-tol", type=float, default=1e-4, help="batch, mixed: inner tolerance")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batch: skip the plain per-problem FP64 comparison leg")
     args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "mixed" if args.workload == "batch" else "fp64"
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -270,6 +270,9 @@ typedef struct {
     double inner_tol;   /* mixed: relative tolerance of each FP32 inner solve     */
     int mg_sweeps;      /* damped-Jacobi sweeps before and after each coarse step */
     int tile_rows;      /* rows of x per fine-level block: 8, 16, 32 or 64        */
+    int coarse_level;   /* multigrid levels from this one down run in one thread
+                           block per problem (one launch per V-cycle); 0: one
+                           launch per phase on every level                      */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver
@@ -299,6 +302,12 @@ pycfd_solver* pycfd_batch_problem(pycfd_batch* b, int i);
  * status, clock and last dt.  Any pointer may be NULL. */
 int pycfd_batch_status(pycfd_batch* b, int* frozen, int* steps, int* iterations, int* status,
                        double* t, double* dt, void* stream);
+/* Measurement support: bracket every eager launch (record = 0) of one kernel
+ * kind with CUDA events, then read the summed device time.  Ids: 1 CG
+ * direction/A-product, 2 last fine V-cycle sweep, 3 first fine sweep +
+ * residual, 4 coarse levels, 5 CG update, 6 predictor; 0 off. */
+int pycfd_batch_profile(pycfd_batch* b, int kernel_id);
+int pycfd_batch_profile_read(pycfd_batch* b, double* total_ms, int* launches, void* stream);
 /* Kernel launches the device executed for `steps` recorded steps since the
  * last call (fixed part per step plus the loop bodies times the passes run). */
 int pycfd_batch_launches(pycfd_batch* b, int steps, long long* launches, void* stream);

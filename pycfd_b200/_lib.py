@@ -30,6 +30,7 @@ EXPORTS = (
     "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_launch_count",
     "pycfd_profile_read", "pycfd_batch_create", "pycfd_batch_destroy", "pycfd_batch_initialize",
     "pycfd_batch_step", "pycfd_batch_problem", "pycfd_batch_status", "pycfd_batch_launches",
+    "pycfd_batch_profile", "pycfd_batch_profile_read",
 )
 
 _dp = C.POINTER(C.c_double)
@@ -65,7 +66,8 @@ class DtControl(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("maxiter", C.c_int),
-                ("inner_tol", C.c_double), ("mg_sweeps", C.c_int), ("tile_rows", C.c_int)]
+                ("inner_tol", C.c_double), ("mg_sweeps", C.c_int), ("tile_rows", C.c_int),
+                ("coarse_level", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -139,6 +141,8 @@ def load(path: str = LIB_PATH):
                                          C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
         "pycfd_batch_launches": (C.c_int, [vp, C.c_int, C.POINTER(C.c_longlong), vp]),
+        "pycfd_batch_profile": (C.c_int, [vp, C.c_int]),
+        "pycfd_batch_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -27,7 +27,7 @@ import numpy as np
 from . import _lib
 from .config import BCKind, BCSpec, PressureSolver, SimulationConfig, SolverType, TimeScheme
 from .fields import FlowField
-from .hierarchy import assemble, build_hierarchy
+from .hierarchy import hierarchy_for
 from .mesh import StructuredMesh
 from .solver import (BoundaryInfo, GpuOptions, ProjectionSolver, _stream, _torch, dt_control_for,
                      native_desc)
@@ -184,9 +184,6 @@ class BatchRunner:
 # ---------------------------------------------------------------------------
 # Batched engine
 # ---------------------------------------------------------------------------
-_HIERARCHIES: dict = {}
-
-
 class _Problem:
     """Host set-up of one problem of a batch (the host half of ``ProjectionSolver.__init__``)."""
 
@@ -217,14 +214,11 @@ class _Problem:
                     self.solid.tobytes() if self.has_obstacle else None)
 
     def hierarchy(self):
-        """Multigrid hierarchy of this problem's structure (built once per process)."""
-        h = _HIERARCHIES.get(self.key)
-        if h is None:
-            nx, ny = self.mesh.shape
-            b = self.boundaries
-            A = assemble(nx, ny, self.mesh.dx, self.mesh.dy, b.periodic_x, b.periodic_y,
-                         self.solid if self.has_obstacle else None, self.dirichlet or None)
-            h = _HIERARCHIES[self.key] = build_hierarchy(A)
+        """Multigrid hierarchy of this problem's structure (built once per structure)."""
+        nx, ny = self.mesh.shape
+        b = self.boundaries
+        _, h = hierarchy_for(nx, ny, self.mesh.dx, self.mesh.dy, b.periodic_x, b.periodic_y,
+                             self.solid if self.has_obstacle else None, self.dirichlet or None)
         return h
 
 
@@ -236,6 +230,7 @@ class BatchOptions:
     inner_tol: float = 1e-4      #: mixed: relative tolerance of each inner FP32 solve
     mg_sweeps: int = 1           #: damped-Jacobi sweeps before/after each coarse correction
     tile_rows: int = 32          #: rows of x per fine-level block (8, 16, 32, 64)
+    coarse_level: int = 0        #: multigrid levels from this one down: one block per problem (0: off)
 
 
 class BatchedSolver:
@@ -287,9 +282,19 @@ class BatchedSolver:
             te = t_end[k] if isinstance(t_end, (list, tuple, np.ndarray)) else t_end
             ctl[k] = dt_control_for(pb.config, pb.mesh, float(te))
         self.structures = len(leader)
+        # state in three flat pools (one host<->device copy per array kind), one view per problem
+        shapes = [(pb.mesh.u_shape, pb.mesh.v_shape, pb.mesh.p_shape) for pb in self.problems]
+        sizes = [[int(np.prod(sh)) for sh in trio] for trio in shapes]
+        self._pools = [torch.zeros(sum(sz[a] for sz in sizes), dtype=torch.float64, device="cuda")
+                       for a in range(3)]
+        self._offsets = np.zeros((n + 1, 3), dtype=np.int64)
+        for k in range(n):
+            self._offsets[k + 1] = self._offsets[k] + sizes[k]
         self.fields = []
         for k, pb in enumerate(self.problems):
-            f = FlowField.zeros(pb.mesh)
+            views = [self._pools[a][self._offsets[k, a]:self._offsets[k + 1, a]].view(shapes[k][a])
+                     for a in range(3)]
+            f = FlowField(pb.mesh, *views)
             for init, view in ((u_init, "u_phys"), (v_init, "v_phys")):
                 if init is None:
                     continue
@@ -301,11 +306,13 @@ class BatchedSolver:
                     np.asarray(val, np.float64) if not isinstance(val, torch.Tensor) else val,
                     dtype=torch.float64, device="cuda")
             self.fields.append(f)
+        self._host = None
         U = (C.c_void_p * n)(*[f.u.data_ptr() for f in self.fields])
         V = (C.c_void_p * n)(*[f.v.data_ptr() for f in self.fields])
         P = (C.c_void_p * n)(*[f.p.data_ptr() for f in self.fields])
         bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
-                            float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows))
+                            float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows),
+                            int(opts.coarse_level))
         if max_steps is None:
             ms = None
         else:
@@ -368,6 +375,39 @@ class BatchedSolver:
         _lib.check(self._L.pycfd_get_stats(C.c_void_p(hk), C.byref(st), _stream()))
         return st.fx, st.fy
 
+    def state_bytes(self):
+        """Bytes of the (u, v) inputs and (u, v, p) outputs of one host round trip."""
+        return (8 * int(self._offsets[-1, 0] + self._offsets[-1, 1]),
+                8 * int(self._offsets[-1].sum()))
+
+    def step_host(self, count: int = 1) -> None:
+        """``count`` times: (u, v) of every problem from pinned host memory, one recorded
+        step, (u, v, p) back to pinned host memory -- the host-buffer call of
+        ``pycfd_step_host`` for the whole batch.  The host copies start as the state."""
+        torch = _torch()
+        if self._host is None:
+            self._host = [torch.empty(p.numel(), dtype=torch.float64, pin_memory=True)
+                          for p in self._pools]
+            for h, p in zip(self._host, self._pools):
+                h.copy_(p)
+        for _ in range(count):
+            self._pools[0].copy_(self._host[0], non_blocking=True)
+            self._pools[1].copy_(self._host[1], non_blocking=True)
+            self.step(1)
+            for h, p in zip(self._host, self._pools):
+                h.copy_(p, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    def profile(self, kernel_id: int, steps: int = 1):
+        """Device time (ms) and launch count of one kernel kind over ``steps`` eager steps,
+        plus the CG iterations per problem of the last step (ids in the C header)."""
+        _lib.check(self._L.pycfd_batch_profile(self._h, int(kernel_id)))
+        self.step(steps, record=False)
+        ms, cnt = C.c_double(), C.c_int()
+        _lib.check(self._L.pycfd_batch_profile_read(self._h, C.byref(ms), C.byref(cnt), _stream()))
+        _lib.check(self._L.pycfd_batch_profile(self._h, 0))
+        return ms.value, cnt.value, self.status()["iterations"]
+
     def launches(self, steps: int) -> int:
         """Kernel launches the device ran for the last ``steps`` recorded steps."""
         n = C.c_longlong()
@@ -380,6 +420,7 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=16),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, coarse_level=3),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
 )
 

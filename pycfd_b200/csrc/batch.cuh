@@ -29,7 +29,7 @@ constexpr int kBMaxLevels = 12;
 constexpr int kBTileJ = 32;      // fine tile width along y (contiguous) = threads along y
 constexpr int kBThreadsI = 8;    // threads along x in a fine tile block
 constexpr int kBThreads = 256;   // every batched kernel runs 256-thread blocks
-constexpr int kBRows = 256;      // multigrid rows per block of an ELL launch
+constexpr int kBEllRounds = 8;   // ELL blocks: rounds of kBThreads / L rows each
 
 // One coarse level (l >= 1) of a hierarchy shared by the problems of one
 // structure (same grid, boundary kinds and solid mask).
@@ -60,6 +60,7 @@ struct BProb {
   int hier, nlev, singular;
   int max_steps;                         // the problem stops after this many steps
   int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
+  int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
   int red_base;                          // first partial row of this problem
   const uint8_t* flags;
   const uint8_t* solid;
@@ -72,6 +73,10 @@ struct BProb {
   double *b, *x;                         // FP64 right-hand side and solution (warm start)
   T *xs, *r, *z, *pa, *pb, *q;           // (inner) CG iterate and vectors
   T *lb[kBMaxLevels], *lxa[kBMaxLevels], *lxb[kBMaxLevels], *lres[kBMaxLevels];
+  // the problem's copy of its structure's hierarchy (read with the record)
+  double w0;
+  const T* C;                            // coarsest pseudo-inverse, row-major
+  BLevel<T> lv[kBMaxLevels];
 };
 
 // Launch-wide state of a batch (device pointers).
@@ -82,16 +87,17 @@ struct BShared {
   long long* passes;     // per site: how often it let its loop body run (launch accounting)
   unsigned* iters;       // per site: passes of the loop now running (the cap below)
   int* capped;           // per site: set when a loop was ended by its pass cap
+  // Per-problem flags indexed by problem, mirrored from the scalar block by the
+  // kernels that change them: a block learns whether its problem takes part
+  // from one load beside its map entry instead of a chain through the record.
+  uint8_t* frozen;       // I_FROZEN != 0
+  uint8_t* solving;      // not frozen and the current solve not done
 };
 
 enum BTicket { TK_CG = 0, TK_IR = 1, TK_ARM = 2, TK_COUNT = 4 };
 
-template <class T>
-__device__ __forceinline__ bool b_frozen(const BProb<T>& P) { return P.I[I_FROZEN] != 0; }
-template <class T>
-__device__ __forceinline__ bool b_solving(const BProb<T>& P) {
-  return P.I[I_FROZEN] == 0 && P.I[I_DONE] == 0;
-}
+__device__ __forceinline__ bool b_frozen(const BShared& sh, int p) { return sh.frozen[p] != 0; }
+__device__ __forceinline__ bool b_solving(const BShared& sh, int p) { return sh.solving[p] != 0; }
 
 // Per-problem reduction over the tiles of one launch.  Every block of the
 // problem contributes NV values at row `tile`; the last to arrive combines them
@@ -194,6 +200,13 @@ __device__ void b_loop_ticket(const BProb<T>* __restrict__ probs, int nprob, con
   for (int i = ti_ * (P).tile_i + (int)threadIdx.y; i < i1_; i += kBThreadsI)                \
     for (int j = tj_ * kBTileJ + (int)threadIdx.x; j < j1_; j += kBTileJ)
 
+// The tiles of chunk `chunk` of problem P (one block of a fine launch takes a
+// chunk, so the per-block set-up -- map entry, record, flags -- is paid once
+// for several tiles).
+#define B_CHUNK_TILES(P, chunk)                                                             \
+  for (int tile_ = (chunk) * (P).chunk_tiles, tend_ = min((P).tiles, tile_ + (P).chunk_tiles); \
+       tile_ < tend_; ++tile_)
+
 // Stage arrays: 0 the state, 1 the first stage buffer, 2 the second.
 template <class T>
 __device__ __forceinline__ double* b_arr_u(const BProb<T>& P, int code) {
@@ -212,27 +225,29 @@ __global__ void __launch_bounds__(kBThreads) k_b_stats(const BProb<T>* __restric
                                                         const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const int nx = P.g.nx, ny = P.g.ny;
   const long W = ny + 2, WV = ny + 3;
   const double *u = P.u, *v = P.v, *p = P.p;
   double acc[3] = {0, 0, 0};
   {
-    B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
-      if (j < ny + 2) {
-        const double a = u[(long)i * W + j];
-        if (!isfinite(a)) acc[2] += 1.0;
-        if (i >= 1 && i <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
-      }
-      if (i < nx + 2) {
-        const double a = v[(long)i * WV + j];
-        if (!isfinite(a)) acc[2] += 1.0;
-        if (i >= 1 && i <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
-        if (j < ny + 2 && !isfinite(p[(long)i * W + j])) acc[2] += 1.0;
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_EXT(P, tile_, nx + 3, ny + 3) {
+        if (j < ny + 2) {
+          const double a = u[(long)i * W + j];
+          if (!isfinite(a)) acc[2] += 1.0;
+          if (i >= 1 && i <= nx + 1 && j >= 1 && j <= ny) acc[0] = fmax(acc[0], fabs(a));
+        }
+        if (i < nx + 2) {
+          const double a = v[(long)i * WV + j];
+          if (!isfinite(a)) acc[2] += 1.0;
+          if (i >= 1 && i <= nx && j >= 1 && j <= ny + 1) acc[1] = fmax(acc[1], fabs(a));
+          if (j < ny + 2 && !isfinite(p[(long)i * W + j])) acc[2] += 1.0;
+        }
       }
     }
   }
-  b_reduce<3, 0x3u>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+  b_reduce<3, 0x3u>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
     P.S[S_STAT0] = t[0];
     P.S[S_STAT0 + 1] = t[1];
     P.S[S_STAT0 + 7] = t[2];
@@ -243,18 +258,22 @@ __global__ void __launch_bounds__(kBThreads) k_b_stats(const BProb<T>* __restric
 // a problem whose health flags trip, or whose end time or step count is
 // reached, freezes.
 template <class T>
-__global__ void k_b_dt(const BProb<T>* __restrict__ probs, int nprob) {
+__global__ void k_b_dt(const BProb<T>* __restrict__ probs, int nprob, BShared sh) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nprob) return;
   const BProb<T>& P = probs[k];
   if (P.I[I_FROZEN]) return;
   if (P.dtc.t_end - P.S[S_T] <= 0.0 || P.I[I_STEPS] >= P.max_steps) {
     P.I[I_FROZEN] = 2;
+    sh.frozen[k] = 1;
+    sh.solving[k] = 0;
     return;
   }
   adaptive_dt_update(P.S, P.I, P.dtc);
   if (P.I[I_HEALTH] != 0) {   // the step is not taken: state stays at the last good step
     P.I[I_FROZEN] = 1;
+    sh.frozen[k] = 1;
+    sh.solving[k] = 0;
     P.S[S_T] -= P.S[S_DT];
     P.I[I_STEPS] -= 1;
   }
@@ -278,10 +297,11 @@ __global__ void k_b_set_dt(const BProb<T>* __restrict__ probs, int nprob, double
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, int src_a,
-                                                            int src_b, double ca, double cb, int dst) {
+                                                            int src_b, double ca, double cb, int dst,
+                                                            BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const Geo& g = P.g;
   const int nx = g.nx, ny = g.ny;
   const StageIn u{b_arr_u(P, src_a), src_b >= 0 ? b_arr_u(P, src_b) : nullptr, ca, cb};
@@ -289,20 +309,22 @@ __global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __res
   double* us = b_arr_u(P, dst);
   double* vs = b_arr_v(P, dst);
   const double dt = P.S[S_DT], blend = P.S[S_BLEND];
-  B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
-    if (j < ny + 2) {
-      const long k = (long)i * (ny + 2) + j;
-      double val = u[k];
-      if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-        val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
-      us[k] = val;
-    }
-    if (i < nx + 2) {
-      const long k = (long)i * (ny + 3) + j;
-      double val = v[k];
-      if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-        val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
-      vs[k] = val;
+  B_CHUNK_TILES(P, e.y) {
+    B_TILE_EXT(P, tile_, nx + 3, ny + 3) {
+      if (j < ny + 2) {
+        const long k = (long)i * (ny + 2) + j;
+        double val = u[k];
+        if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
+          val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
+        us[k] = val;
+      }
+      if (i < nx + 2) {
+        const long k = (long)i * (ny + 3) + j;
+        double val = v[k];
+        if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
+          val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
+        vs[k] = val;
+      }
     }
   }
 }
@@ -312,9 +334,9 @@ __global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __res
 // in the correction's last block).
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_boundary(const BProb<T>* __restrict__ probs, int arr,
-                                                           BcProgram prog, int p_ghosts) {
+                                                           BcProgram prog, int p_ghosts, BShared sh) {
   const BProb<T>& P = probs[blockIdx.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, blockIdx.x)) return;
   double* u = b_arr_u(P, arr);
   double* v = b_arr_v(P, arr);
   if (p_ghosts) {
@@ -343,25 +365,27 @@ __global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restr
                                                           BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const Geo& g = P.g;
   const double* u = b_arr_u(P, arr);
   const double* v = b_arr_v(P, arr);
   const double dt = P.S[S_DT];
   double acc[1] = {0.0};
   {
-    B_TILE_CELLS(P, e.y) {
-      const int c = i * g.ny + j;
-      const uint8_t f = P.flags[c];
-      double val = 0.0;
-      if (f & F_SOLV) {
-        val = (cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt) * 1.0 + fine_bc(f, i, j, g);
-        acc[0] += val;
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_CELLS(P, tile_) {
+        const int c = i * g.ny + j;
+        const uint8_t f = P.flags[c];
+        double val = 0.0;
+        if (f & F_SOLV) {
+          val = (cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt) * 1.0 + fine_bc(f, i, j, g);
+          acc[0] += val;
+        }
+        P.b[c] = val;
       }
-      P.b[c] = val;
     }
   }
-  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles,
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks,
               [&](double* t) { P.S[S_MEAN_B] = g.n_fluid ? t[0] / g.n_fluid : 0.0; });
 }
 
@@ -369,10 +393,11 @@ __global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restr
 // (pycfd/core/solver.py:665-682); the ghost ring follows in k_b_boundary.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_correct(const BProb<T>* __restrict__ probs,
-                                                          const int2* __restrict__ map, int arr) {
+                                                          const int2* __restrict__ map, int arr,
+                                                          BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const Geo& g = P.g;
   const int nx = g.nx, ny = g.ny;
   double* u = b_arr_u(P, arr);
@@ -380,15 +405,17 @@ __global__ void __launch_bounds__(kBThreads) k_b_correct(const BProb<T>* __restr
   const double* x = P.x;
   double* p = P.p;
   const double dt = P.S[S_DT];
-  B_TILE_EXT(P, e.y, nx + 2, ny + 3) {
-    if (i >= 1 && i <= nx && j >= 1 && j <= ny) p[(long)i * (ny + 2) + j] = x[(long)(i - 1) * ny + (j - 1)];
-    if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny) {
-      const long k = (long)i * (ny + 2) + j;
-      u[k] = u[k] - dt * (p_at(x, i, j, g) - p_at(x, i - 1, j, g)) / g.dx;
-    }
-    if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi) {
-      const long k = (long)i * (ny + 3) + j;
-      v[k] = v[k] - dt * (p_at(x, i, j, g) - p_at(x, i, j - 1, g)) / g.dy;
+  B_CHUNK_TILES(P, e.y) {
+    B_TILE_EXT(P, tile_, nx + 2, ny + 3) {
+      if (i >= 1 && i <= nx && j >= 1 && j <= ny) p[(long)i * (ny + 2) + j] = x[(long)(i - 1) * ny + (j - 1)];
+      if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny) {
+        const long k = (long)i * (ny + 2) + j;
+        u[k] = u[k] - dt * (p_at(x, i, j, g) - p_at(x, i - 1, j, g)) / g.dx;
+      }
+      if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi) {
+        const long k = (long)i * (ny + 3) + j;
+        v[k] = v[k] - dt * (p_at(x, i, j, g) - p_at(x, i, j - 1, g)) / g.dy;
+      }
     }
   }
 }
@@ -398,21 +425,23 @@ __global__ void __launch_bounds__(kBThreads) k_b_correct(const BProb<T>* __restr
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_combine(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int src_b,
-                                                          double ca, double cb) {
+                                                          double ca, double cb, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const int nx = P.g.nx, ny = P.g.ny;
   const double* bu = b_arr_u(P, src_b);
   const double* bv = b_arr_v(P, src_b);
-  B_TILE_EXT(P, e.y, nx + 3, ny + 3) {
-    if (j < ny + 2) {
-      const long k = (long)i * (ny + 2) + j;
-      P.u[k] = ca * P.u[k] + cb * bu[k];
-    }
-    if (i < nx + 2) {
-      const long k = (long)i * (ny + 3) + j;
-      P.v[k] = ca * P.v[k] + cb * bv[k];
+  B_CHUNK_TILES(P, e.y) {
+    B_TILE_EXT(P, tile_, nx + 3, ny + 3) {
+      if (j < ny + 2) {
+        const long k = (long)i * (ny + 2) + j;
+        P.u[k] = ca * P.u[k] + cb * bu[k];
+      }
+      if (i < nx + 2) {
+        const long k = (long)i * (ny + 3) + j;
+        P.v[k] = ca * P.v[k] + cb * bv[k];
+      }
     }
   }
 }
@@ -427,25 +456,27 @@ __global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __rest
                                                            LoopCtl loop) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (!b_frozen(P)) {
+  if (!b_frozen(sh, e.x)) {
     const Geo& g = P.g;
     const double mean = P.singular ? P.S[S_MEAN_B] : 0.0;
     double acc[3] = {0, 0, 0};
     {
-      B_TILE_CELLS(P, e.y) {
-        const int c = i * g.ny + j;
-        const uint8_t f = P.flags[c];
-        const double bc = (f & F_SOLV) ? P.b[c] - mean : 0.0;
-        P.b[c] = bc;
-        const double ax = fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return (double)P.xs[k]; });
-        const double rc = bc - ax;
-        P.r[c] = (T)rc;
-        acc[0] += bc * bc;
-        acc[1] += rc * rc;
-        if (f & F_SOLV) acc[2] += rc;
+      B_CHUNK_TILES(P, e.y) {
+        B_TILE_CELLS(P, tile_) {
+          const int c = i * g.ny + j;
+          const uint8_t f = P.flags[c];
+          const double bc = (f & F_SOLV) ? P.b[c] - mean : 0.0;
+          P.b[c] = bc;
+          const double ax = fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return (double)P.xs[k]; });
+          const double rc = bc - ax;
+          P.r[c] = (T)rc;
+          acc[0] += bc * bc;
+          acc[1] += rc * rc;
+          if (f & F_SOLV) acc[2] += rc;
+        }
       }
     }
-    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       S[S_BNORM2] = t[0];
@@ -460,6 +491,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __rest
       I[I_CONVERGED] = conv;
       I[I_DONE] = conv || maxiter <= 0;
       I[I_STATUS] = 0;
+      sh.solving[e.x] = !I[I_DONE];
     });
   }
   b_loop_ticket(probs, nprob, sh, TK_CG, I_DONE, 1, maxiter + 1, loop);
@@ -471,7 +503,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
                                                         const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (!b_solving(P)) return;
+  if (!b_solving(sh, e.x)) return;
   const Geo& g = P.g;
   const bool first = P.I[I_IT] == 0;
   const double beta = first ? 0.0 : P.S[S_RHO] / P.S[S_RHO_PREV];
@@ -486,16 +518,18 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
   };
   double acc[1] = {0.0};
   {
-    B_TILE_CELLS(P, e.y) {
-      const int c = i * g.ny + j;
-      const double pc = pval(c, i, j);
-      const double qc = fine_apply<double>(flags[c], i, j, c, g, pval);
-      P.pb[c] = (T)pc;
-      P.q[c] = (T)qc;
-      acc[0] += pc * qc;
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_CELLS(P, tile_) {
+        const int c = i * g.ny + j;
+        const double pc = pval(c, i, j);
+        const double qc = fine_apply<double>(flags[c], i, j, c, g, pval);
+        P.pb[c] = (T)pc;
+        P.q[c] = (T)qc;
+        acc[0] += pc * qc;
+      }
     }
   }
-  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
     P.S[S_PQ] = t[0];
     P.S[S_ALPHA] = P.S[S_RHO] / t[0];
   });
@@ -509,24 +543,26 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
                                                         BShared sh, LoopCtl loop) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_solving(P)) {
+  if (b_solving(sh, e.x)) {
     const Geo& g = P.g;
     const double alpha = P.S[S_ALPHA];
     double acc[2] = {0, 0};
     {
-      B_TILE_CELLS(P, e.y) {
-        const int c = i * g.ny + j;
-        const T pc = P.pb[c];
-        const double xc = (double)P.xs[c] + alpha * (double)pc;
-        const double rc = (double)(T)((double)P.r[c] - alpha * (double)P.q[c]);
-        P.pa[c] = pc;
-        P.xs[c] = (T)xc;
-        P.r[c] = (T)rc;
-        acc[0] += rc * rc;
-        if (P.flags[c] & F_SOLV) acc[1] += rc;
+      B_CHUNK_TILES(P, e.y) {
+        B_TILE_CELLS(P, tile_) {
+          const int c = i * g.ny + j;
+          const T pc = P.pb[c];
+          const double xc = (double)P.xs[c] + alpha * (double)pc;
+          const double rc = (double)(T)((double)P.r[c] - alpha * (double)P.q[c]);
+          P.pa[c] = pc;
+          P.xs[c] = (T)xc;
+          P.r[c] = (T)rc;
+          acc[0] += rc * rc;
+          if (P.flags[c] & F_SOLV) acc[1] += rc;
+        }
       }
     }
-    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       const int it = I[I_IT] + 1;
@@ -538,6 +574,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
       const bool conv = sqrt(t[0]) < S[S_ATOL];
       I[I_CONVERGED] = conv;
       I[I_DONE] = conv || it >= maxiter;
+      sh.solving[e.x] = !I[I_DONE];
     });
   }
   b_loop_ticket(probs, nprob, sh, TK_CG, I_DONE, 0, maxiter + 1, loop);
@@ -550,22 +587,24 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __
                                                                BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const Geo& g = P.g;
   const bool zero = P.I[I_ZERO_RHS] != 0;
   const double* x = P.x;
   auto xv = [&](int k, int, int) -> double { return zero ? 0.0 : x[k]; };
   double acc[2] = {0, 0};
   {
-    B_TILE_CELLS(P, e.y) {
-      const int c = i * g.ny + j;
-      const uint8_t f = P.flags[c];
-      const double rc = P.b[c] - fine_apply<double>(f, i, j, c, g, xv);
-      acc[0] += rc * rc;
-      if (f & F_SOLV) acc[1] += xv(c, i, j);
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_CELLS(P, tile_) {
+        const int c = i * g.ny + j;
+        const uint8_t f = P.flags[c];
+        const double rc = P.b[c] - fine_apply<double>(f, i, j, c, g, xv);
+        acc[0] += rc * rc;
+        if (f & F_SOLV) acc[1] += xv(c, i, j);
+      }
     }
   }
-  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
     double* S = P.S;
     const double nb = sqrt(S[S_BNORM2]);
     S[S_RESID] = sqrt(t[0]) / (nb > 1e-300 ? nb : 1.0);
@@ -577,15 +616,17 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __
 // x <- x - mean on solvable rows, 0 elsewhere.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_finish_apply(const BProb<T>* __restrict__ probs,
-                                                               const int2* __restrict__ map) {
+                                                               const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P)) return;
+  if (b_frozen(sh, e.x)) return;
   const bool zero = P.I[I_ZERO_RHS] != 0;
   const double m = P.S[S_MEAN_X];
-  B_TILE_CELLS(P, e.y) {
-    const int c = i * P.g.ny + j;
-    P.x[c] = (!zero && (P.flags[c] & F_SOLV)) ? P.x[c] - m : 0.0;
+  B_CHUNK_TILES(P, e.y) {
+    B_TILE_CELLS(P, tile_) {
+      const int c = i * P.g.ny + j;
+      P.x[c] = (!zero && (P.flags[c] & F_SOLV)) ? P.x[c] - m : 0.0;
+    }
   }
 }
 
@@ -600,28 +641,30 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __r
                                                               LoopCtl outer) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (!b_frozen(P) && (first || !P.I[I_IR_DONE])) {
+  if (!b_frozen(sh, e.x) && (first || !P.I[I_IR_DONE])) {
     const Geo& g = P.g;
     const double mean = (first && P.singular) ? P.S[S_MEAN_B] : 0.0;
     double acc[3] = {0, 0, 0};
     {
-      B_TILE_CELLS(P, e.y) {
-        const int c = i * g.ny + j;
-        const uint8_t f = P.flags[c];
-        double bc = P.b[c];
-        if (first) {
-          bc = (f & F_SOLV) ? bc - mean : 0.0;
-          P.b[c] = bc;
+      B_CHUNK_TILES(P, e.y) {
+        B_TILE_CELLS(P, tile_) {
+          const int c = i * g.ny + j;
+          const uint8_t f = P.flags[c];
+          double bc = P.b[c];
+          if (first) {
+            bc = (f & F_SOLV) ? bc - mean : 0.0;
+            P.b[c] = bc;
+          }
+          const double rc = bc - fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return P.x[k]; });
+          P.r[c] = (T)rc;
+          P.xs[c] = (T)0;
+          acc[0] += rc * rc;
+          if (f & F_SOLV) acc[1] += (double)(T)rc;
+          if (first) acc[2] += bc * bc;
         }
-        const double rc = bc - fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return P.x[k]; });
-        P.r[c] = (T)rc;
-        P.xs[c] = (T)0;
-        acc[0] += rc * rc;
-        if (f & F_SOLV) acc[1] += (double)(T)rc;
-        if (first) acc[2] += bc * bc;
       }
     }
-    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       if (first) {
@@ -644,6 +687,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __r
       S[S_MEAN_R] = g.n_fluid ? t[1] / g.n_fluid : 0.0;
       I[I_IT] = 0;
       I[I_DONE] = done;
+      sh.solving[e.x] = !done;
     });
   }
   b_loop_ticket(probs, nprob, sh, TK_IR, I_IR_DONE, first, max_passes + 1, outer);
@@ -654,7 +698,7 @@ template <class T>
 __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShared sh, LoopCtl inner) {
   int any = 0;
   for (int p = threadIdx.x; p < nprob; p += blockDim.x)
-    if (b_solving(probs[p])) any = 1;
+    if (b_solving(sh, p)) any = 1;
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
     sh.any[TK_ARM] = any;
@@ -667,14 +711,16 @@ __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShare
 // x += e on solvable rows for the problems that ran this pass; count the pass.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_ir_update(const BProb<T>* __restrict__ probs,
-                                                            const int2* __restrict__ map) {
+                                                            const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (b_frozen(P) || P.I[I_IR_DONE]) return;
+  if (b_frozen(sh, e.x) || P.I[I_IR_DONE]) return;
   {
-    B_TILE_CELLS(P, e.y) {
-      const int c = i * P.g.ny + j;
-      if (P.flags[c] & F_SOLV) P.x[c] = P.x[c] + (double)P.xs[c];
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_CELLS(P, tile_) {
+        const int c = i * P.g.ny + j;
+        if (P.flags[c] & F_SOLV) P.x[c] = P.x[c] + (double)P.xs[c];
+      }
     }
   }
   if (e.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) P.I[I_IR_IT] += 1;
@@ -698,9 +744,9 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
                                                        BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
-  if (!b_solving(P)) return;
+  if (!b_solving(sh, e.x)) return;
   const Geo& g = P.g;
-  const double w = hiers[P.hier].w0;
+  const double w = P.w0;
   const uint8_t* flags = P.flags;
   const T* r = P.r;
   const double mr = P.singular ? P.S[S_MEAN_R] : 0.0;
@@ -709,34 +755,36 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   T* xo = b_fine_buf(P, dst);
   double acc[2] = {0, 0};
   {
-    B_TILE_CELLS(P, e.y) {
-      const int c = i * g.ny + j;
-      const uint8_t f = flags[c];
-      if (MODE == FM_PRE) {
-        auto xv = [&](int k, int ii, int jj) -> double {
-          return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
-        };
-        xo[c] = (T)xv(c, i, j);
-        P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
-      } else if (MODE == FM_WDB) {
-        xo[c] = (T)(fine_wdinv(f, i, j, g, w) * bf(c));
-      } else if (MODE == FM_RESID) {
-        auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
-        P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
-      } else {
-        auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
-        const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
-                                      (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
-        xo[c] = (T)xn;
-        if (MODE == FM_LAST && (f & F_SOLV)) {
-          acc[0] += xn;
-          acc[1] += (double)r[c] * xn;
+    B_CHUNK_TILES(P, e.y) {
+      B_TILE_CELLS(P, tile_) {
+        const int c = i * g.ny + j;
+        const uint8_t f = flags[c];
+        if (MODE == FM_PRE) {
+          auto xv = [&](int k, int ii, int jj) -> double {
+            return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
+          };
+          xo[c] = (T)xv(c, i, j);
+          P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+        } else if (MODE == FM_WDB) {
+          xo[c] = (T)(fine_wdinv(f, i, j, g, w) * bf(c));
+        } else if (MODE == FM_RESID) {
+          auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
+          P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+        } else {
+          auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
+          const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
+                                        (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
+          xo[c] = (T)xn;
+          if (MODE == FM_LAST && (f & F_SOLV)) {
+            acc[0] += xn;
+            acc[1] += (double)r[c] * xn;
+          }
         }
       }
     }
   }
   if (MODE != FM_LAST) return;
-  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.tiles, [&](double* t) {
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
     double* S = P.S;
     const double m = (P.singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
     S[S_MEAN_Z] = m;
@@ -745,9 +793,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   });
 }
 
-// ELL phases of coarse level d (and prolongation into level 0).  Row blocks of
-// kBRows rows; lanes per row from the hierarchy (runtime), so problems of
-// different structures share one launch.
+// ELL phases of coarse level d (and prolongation into level 0).  A block takes
+// kBEllRounds x kBThreads / L rows, L lanes per row from the problem's
+// hierarchy (runtime), so problems of different structures share one launch
+// and wide rows spread over many blocks.
 enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG };
 
 template <class T>
@@ -764,8 +813,10 @@ __device__ __forceinline__ double b_ell_row(const Ell<T>& E, int L, int row, int
   if (row < E.n) {
     if (E.rowmajor) {
       const long base = (long)row * E.K;
+#pragma unroll 4
       for (int k = lane; k < E.K; k += L) acc += (double)E.val[base + k] * x(E.col[base + k]);
     } else {
+#pragma unroll 4
       for (int k = lane; k < E.K; k += L) {
         const long at = (long)k * E.n + row;
         acc += (double)E.val[at] * x(E.col[at]);
@@ -778,17 +829,15 @@ __device__ __forceinline__ double b_ell_row(const Ell<T>& E, int L, int row, int
 
 template <class T, int OP>
 __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict__ probs,
-                                                      const BHier<T>* __restrict__ hiers,
                                                       const int2* __restrict__ map, int d, int src,
-                                                      int dst) {
+                                                      int dst, BShared sh) {
   extern __shared__ double sb[];
   const int2 e = map[blockIdx.x];
+  if (!b_solving(sh, e.x)) return;
   const BProb<T>& P = probs[e.x];
-  if (!b_solving(P)) return;
-  const BHier<T>& H = hiers[P.hier];
   if (OP == EO_RESTRICT && e.y < 0) {
     // coarsest level d: restriction and dense solve in this block
-    const BLevel<T>& Lc = H.lv[d];
+    const BLevel<T>& Lc = P.lv[d];
     const T* res = P.lres[d - 1];
     const int L = Lc.lr, lane = threadIdx.x & (L - 1);
     const int per = kBThreads / L;
@@ -805,61 +854,191 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     const int n = Lc.R.n;
     for (int row = warp; row < n; row += nw) {
       double acc = 0.0;
-      for (int k = wl; k < n; k += 32) acc += (double)H.C[(long)row * n + k] * sb[k];
+      for (int k = wl; k < n; k += 32) acc += (double)P.C[(long)row * n + k] * sb[k];
       acc = warp_sum(acc);
       if (wl == 0) P.lxa[d][row] = (T)acc;
     }
     return;
   }
-  // rows [r0, r1) of level d
-  const int n = (d == 0) ? P.g.nx * P.g.ny : H.lv[d].n;
-  const int r0 = e.y * kBRows, r1 = min(n, r0 + kBRows);
+  // rows [r0, r1) of level d: kBEllRounds rounds of kBThreads / L rows each
+  // (L: lanes of the block's matrix), the rounds unrolled so their loads overlap
+  const int n = (d == 0) ? P.g.nx * P.g.ny : P.lv[d].n;
+  const int Lop = OP == EO_PROLONG ? P.lv[d + 1].lp : OP == EO_RESTRICT ? P.lv[d].lr : P.lv[d].la;
+  const int per = kBThreads / Lop;
+  const int r0 = e.y * per * kBEllRounds;
+  const int r1 = min(n, r0 + per * kBEllRounds);
+  const int lane = threadIdx.x & (Lop - 1);
   if (OP == EO_PROLONG) {
     // x_d += P_{d+1} x_{d+1}
-    const BLevel<T>& Lc = H.lv[d + 1];
-    const int L = Lc.lp, lane = threadIdx.x & (L - 1), per = kBThreads / L;
-    const T* xc = b_lvl_x(P, d + 1, src);
-    T* xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
-    for (int base = r0; base < r1; base += per) {
-      const int row = base + (int)threadIdx.x / L;
-      const double s = b_ell_row(Lc.P, L, row < r1 ? row : Lc.P.n, lane, [&](int c) { return (double)xc[c]; });
+    const BLevel<T>& Lc = P.lv[d + 1];
+    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
+    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
+#pragma unroll
+    for (int rd = 0; rd < kBEllRounds; ++rd) {
+      const int row = r0 + rd * per + (int)threadIdx.x / Lop;
+      const double s = b_ell_row(Lc.P, Lop, row < r1 ? row : Lc.P.n, lane, [&](int c) { return (double)xc[c]; });
       if (lane == 0 && row < r1) xf[row] = (T)((double)xf[row] + s);
     }
     return;
   }
-  const BLevel<T>& Lv = H.lv[d];
+  const BLevel<T>& Lv = P.lv[d];
   if (OP == EO_RESTRICT) {
-    const T* res = (d == 1) ? P.lres[0] : P.lres[d - 1];
-    const int L = Lv.lr, lane = threadIdx.x & (L - 1), per = kBThreads / L;
-    for (int base = r0; base < r1; base += per) {
-      const int row = base + (int)threadIdx.x / L;
-      const double s = b_ell_row(Lv.R, L, row < r1 ? row : Lv.R.n, lane, [&](int c) { return (double)res[c]; });
-      if (lane == 0 && row < r1) P.lb[d][row] = (T)s;
+    const T* __restrict__ res = P.lres[d - 1];
+    T* __restrict__ bo = P.lb[d];
+#pragma unroll
+    for (int rd = 0; rd < kBEllRounds; ++rd) {
+      const int row = r0 + rd * per + (int)threadIdx.x / Lop;
+      const double s = b_ell_row(Lv.R, Lop, row < r1 ? row : Lv.R.n, lane, [&](int c) { return (double)res[c]; });
+      if (lane == 0 && row < r1) bo[row] = (T)s;
     }
     return;
   }
-  const int L = Lv.la, lane = threadIdx.x & (L - 1), per = kBThreads / L;
-  const T* b = P.lb[d];
-  const T* wd = Lv.wd;
-  const T* x = b_lvl_x(P, d, src);
-  T* xo = b_lvl_x(P, d, dst);
-  for (int base = r0; base < r1; base += per) {
-    const int row = base + (int)threadIdx.x / L;
+  const T* __restrict__ b = P.lb[d];
+  const T* __restrict__ wd = Lv.wd;
+  const T* __restrict__ x = b_lvl_x(P, d, src);
+  T* __restrict__ xo = b_lvl_x(P, d, dst);
+  T* __restrict__ xa = P.lxa[d];
+  T* __restrict__ ro = P.lres[d];
+#pragma unroll
+  for (int rd = 0; rd < kBEllRounds; ++rd) {
+    const int row = r0 + rd * per + (int)threadIdx.x / Lop;
     const int rr = row < r1 ? row : Lv.A.n;
     if (OP == EO_PRE) {
-      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
+      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
       if (lane == 0 && row < r1) {
         const double bx = (double)b[row];
-        P.lxa[d][row] = (T)((double)wd[row] * bx);
-        P.lres[d][row] = (T)(bx - s);
+        xa[row] = (T)((double)wd[row] * bx);
+        ro[row] = (T)(bx - s);
       }
     } else if (OP == EO_SMOOTH) {
-      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)x[c]; });
+      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)x[c]; });
       if (lane == 0 && row < r1) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
     } else {   // EO_RESID
-      const double s = b_ell_row(Lv.A, L, rr, lane, [&](int c) { return (double)x[c]; });
-      if (lane == 0 && row < r1) P.lres[d][row] = (T)((double)b[row] - s);
+      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)x[c]; });
+      if (lane == 0 && row < r1) ro[row] = (T)((double)b[row] - s);
     }
+  }
+}
+
+// Coarse levels of the V-cycle, one thread block per problem: levels
+// d0 = min(dc, coarsest) .. coarsest of every solving problem run inside one
+// block, phases separated by __syncthreads -- restriction from the residual of
+// level d0 - 1, first sweep + residual (more sweeps if asked), down to the
+// coarsest dense solve, then prolongation and smoothing back up to d0.  These
+// levels hold few rows, so one launch for all problems replaces a launch per
+// phase and level; their vectors and the shared matrices stay in L2.  The
+// result at d0 lands in the buffer the per-level path would leave it in
+// (b_coarse_final), so the prolongation into d0 - 1 is unchanged.  Measured on
+// the 256-cavity batch this form is slower than per-level launches (one SM
+// carries a problem's whole coarse cycle, and the largest problems set the
+// launch's length), so it is an option, not the default.
+constexpr int kBCoarseThreads = 512;
+
+__host__ __device__ inline int b_coarse_final(int sweeps) {
+  // down: the first sweep writes xa, each further one swaps; up: every sweep swaps
+  return (((sweeps - 1) & 1) + sweeps) & 1;
+}
+
+template <class T, class X, class W>
+__device__ __forceinline__ void b_blk_ell(const Ell<T>& E, int L, X x, W write) {
+  const int lane = threadIdx.x & (L - 1), per = blockDim.x / L;
+  for (int base = 0; base < E.n; base += per) {
+    const int row = base + (int)threadIdx.x / L;
+    const double s = b_ell_row(E, L, row, lane, x);
+    if (lane == 0 && row < E.n) write(row, s);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __restrict__ probs,
+                                                               const int* __restrict__ order, int dc,
+                                                               int sweeps, BShared sh) {
+  extern __shared__ double sb[];
+  const int p = order[blockIdx.x];
+  if (!b_solving(sh, p)) return;
+  const BProb<T>& P = probs[p];
+  const int c = P.nlev - 1;
+  const int d0 = min(dc, c);
+  int cur[kBMaxLevels];
+  // ---- down ----
+  for (int l = d0; l <= c; ++l) {
+    const BLevel<T>& Lv = P.lv[l];
+    const T* __restrict__ src = P.lres[l - 1];
+    T* __restrict__ bl = P.lb[l];
+    const bool coarsest = l == c;
+    b_blk_ell(Lv.R, Lv.lr, [&](int k) { return (double)src[k]; }, [&](int row, double s) {
+      bl[row] = (T)s;
+      if (coarsest) sb[row] = (double)(T)s;
+    });
+    __syncthreads();
+    if (coarsest) {
+      const int wl = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      const int n = Lv.R.n;
+      T* __restrict__ xo = P.lxa[l];
+      for (int row = warp; row < n; row += nw) {
+        double acc = 0.0;
+        for (int k = wl; k < n; k += 32) acc += (double)P.C[(long)row * n + k] * sb[k];
+        acc = warp_sum(acc);
+        if (wl == 0) xo[row] = (T)acc;
+      }
+      __syncthreads();
+      cur[l] = 0;
+      break;
+    }
+    const T* __restrict__ wd = Lv.wd;
+    T* __restrict__ xa = P.lxa[l];
+    T* __restrict__ xb = P.lxb[l];
+    T* __restrict__ rs = P.lres[l];
+    b_blk_ell(Lv.A, Lv.la, [&](int k) { return (double)wd[k] * (double)bl[k]; }, [&](int row, double s) {
+      const double bx = (double)bl[row];
+      xa[row] = (T)((double)wd[row] * bx);
+      rs[row] = (T)(bx - s);
+    });
+    __syncthreads();
+    int a = 0;
+    if (sweeps > 1) {
+      for (int k = 1; k < sweeps; ++k) {
+        const T* xi = a == 0 ? xa : xb;
+        T* xn = a == 0 ? xb : xa;
+        b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; }, [&](int row, double s) {
+          xn[row] = (T)((double)xi[row] + (double)wd[row] * ((double)bl[row] - s));
+        });
+        __syncthreads();
+        a ^= 1;
+      }
+      const T* xi = a == 0 ? xa : xb;
+      b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; },
+                [&](int row, double s) { rs[row] = (T)((double)bl[row] - s); });
+      __syncthreads();
+    }
+    cur[l] = a;
+  }
+  // ---- up ----
+  for (int l = c - 1; l >= d0; --l) {
+    const BLevel<T>& Lv = P.lv[l];
+    const BLevel<T>& Lc = P.lv[l + 1];
+    const T* __restrict__ xc = (l + 1 == c || cur[l + 1] == 0) ? P.lxa[l + 1] : P.lxb[l + 1];
+    T* xa = P.lxa[l];
+    T* xb = P.lxb[l];
+    int a = cur[l];
+    {
+      T* __restrict__ xf = a == 0 ? xa : xb;
+      b_blk_ell(Lc.P, Lc.lp, [&](int k) { return (double)xc[k]; },
+                [&](int row, double s) { xf[row] = (T)((double)xf[row] + s); });
+      __syncthreads();
+    }
+    const T* __restrict__ wd = Lv.wd;
+    const T* __restrict__ bl = P.lb[l];
+    for (int k = 1; k <= sweeps; ++k) {
+      const T* xi = a == 0 ? xa : xb;
+      T* xn = a == 0 ? xb : xa;
+      b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; }, [&](int row, double s) {
+        xn[row] = (T)((double)xi[row] + (double)wd[row] * ((double)bl[row] - s));
+      });
+      __syncthreads();
+      a ^= 1;
+    }
+    cur[l] = a;
   }
 }
 

@@ -21,15 +21,19 @@ struct pycfd_batch {
   int precision = PCFD_FP64;
   double tol = 1e-10, inner_tol = 1e-4;
   int maxiter = 1000, sweeps = 1, tile_i = 32;
+  int coarse = 0;                          // levels >= coarse: one block per problem (0: per level)
+  int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
   void* probs = nullptr;                   // BProb<T>[n] (device)
   void* hiers = nullptr;                   // BHier<T>[nh] (device)
   std::vector<int> nlev;
   int depth = 0;                           // most levels of any problem
-  BMapHost fine;                           // every tile of every problem
-  std::vector<BMapHost> rows;              // rows[d]: row blocks of level d (non-coarsest; d = 0: all)
-  std::vector<BMapHost> restr;             // restr[d]: rows[d] + one coarsest block per problem ending at d
+  BMapHost fine;                           // every chunk of tiles of every problem
+  // row-block maps per depth d (problems whose level d runs per level):
+  std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
+  std::vector<BMapHost> mapR;              // restriction into d (+ coarsest blocks when coarse == 0)
+  std::vector<BMapHost> mapP;              // prolongation into d with P_{d+1}
   size_t smem_dense = 0;
   BShared sh{};
   int* h_any = nullptr;                    // pinned mirror of sh.any
@@ -48,6 +52,7 @@ namespace {
 
 constexpr int kIrMaxPassesB = 40;
 constexpr int kInnerMaxIterB = 200;
+constexpr int kBChunkCells = 4096;   // fine cells per block of a fine launch
 
 int upload_map(pycfd_batch* B, BMapHost* m, const std::vector<int2>& h) {
   m->n = (int)h.size();
@@ -167,8 +172,10 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.tiles_i = (s->g.nx + B->tile_i - 1) / B->tile_i;
     P.tiles_j = (s->g.ny + kBTileJ - 1) / kBTileJ;
     P.tiles = P.tiles_i * P.tiles_j;
+    P.chunk_tiles = std::max(1, kBChunkCells / (B->tile_i * kBTileJ));
+    P.chunks = (P.tiles + P.chunk_tiles - 1) / P.chunk_tiles;
     P.red_base = red_rows;
-    red_rows += P.tiles;
+    red_rows += P.chunks;
     P.flags = s->flags;
     P.solid = s->solid;
     P.bc_kind = s->bc_kind_dev;
@@ -210,29 +217,54 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       TRY(dalloc(B->mem, &P.lxb[l], K[l].n));
       TRY(dalloc(B->mem, &P.lres[l], K[l].n));
     }
-    for (int t = 0; t < P.tiles; ++t) fine.push_back(make_int2(i, t));
+    P.w0 = hh[hid[i]].w0;
+    P.C = hh[hid[i]].C;
+    for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
+    for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
-  // row maps per depth
-  B->rows.assign(B->depth, BMapHost{});
-  B->restr.assign(B->depth, BMapHost{});
+  // row-block maps per depth: a block takes kBEllRounds x kBThreads / L rows
+  // (L: lanes of its matrix).  With the coarse kernel, a problem's levels from
+  // min(coarse, coarsest) on run there and take no per-level blocks.
+  B->mapA.assign(B->depth, BMapHost{});
+  B->mapR.assign(B->depth, BMapHost{});
+  B->mapP.assign(B->depth, BMapHost{});
   for (int d = 0; d < B->depth; ++d) {
-    std::vector<int2> rows, restr;
+    std::vector<int2> ma, mr, mp;
     for (int i = 0; i < n; ++i) {
-      const int c = B->nlev[i] - 1;   // coarsest level index
-      if (d > c) continue;
-      if (d == c) {
-        if (d >= 1) restr.push_back(make_int2(i, -1));
-        continue;
+      const int c = B->nlev[i] - 1;
+      const BHier<T>& H = hh[hid[i]];
+      if (B->coarse > 0) {
+        if (d >= std::min(B->coarse, c)) continue;
+      } else {
+        if (d > c) continue;
+        if (d == c) {
+          if (d >= 1) mr.push_back(make_int2(i, -1));
+          continue;
+        }
       }
       const int nrow = d == 0 ? pr[i].g.nx * pr[i].g.ny : keep[hid[i]][d].n;
-      for (int rb = 0; rb * kBRows < nrow; ++rb) {
-        rows.push_back(make_int2(i, rb));
-        restr.push_back(make_int2(i, rb));
+      auto add = [&](std::vector<int2>& m, int lanes) {
+        const int rpb = kBThreads / lanes * kBEllRounds;
+        for (int rb = 0; rb * rpb < nrow; ++rb) m.push_back(make_int2(i, rb));
+      };
+      add(mp, H.lv[d + 1].lp);
+      if (d >= 1) {
+        add(ma, H.lv[d].la);
+        add(mr, H.lv[d].lr);
       }
     }
-    TRY(upload_map(B, &B->rows[d], rows));
-    TRY(upload_map(B, &B->restr[d], restr));
+    TRY(upload_map(B, &B->mapA[d], ma));
+    TRY(upload_map(B, &B->mapR[d], mr));
+    TRY(upload_map(B, &B->mapP[d], mp));
+  }
+  {
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; ++i) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+      return (long)pr[a].g.nx * pr[a].g.ny > (long)pr[b].g.nx * pr[b].g.ny;
+    });
+    TRY(upload(B->mem, &B->order, ord.data(), ord.size()));
   }
   void* pd = nullptr;
   TRY(upload(B->mem, (uint8_t**)&pd, (const uint8_t*)pr.data(), pr.size() * sizeof(BProb<T>)));
@@ -243,6 +275,8 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   TRY(dalloc(B->mem, &B->sh.passes, TK_COUNT));
   TRY(dalloc(B->mem, &B->sh.iters, TK_COUNT));
   TRY(dalloc(B->mem, &B->sh.capped, TK_COUNT));
+  TRY(dalloc(B->mem, &B->sh.frozen, n));
+  TRY(dalloc(B->mem, &B->sh.solving, n));
   TRY(dalloc(B->mem, &B->d_iout, (size_t)4 * n));
   TRY(dalloc(B->mem, &B->d_dout, (size_t)2 * n));
   return 0;
@@ -257,6 +291,13 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 
 const dim3 kBFineBlock(kBTileJ, kBThreadsI);
 
+// Event pair around eager launches of one kernel kind (measurement support;
+// ids: 1 k_b_cg_pq, 2 last fine V-cycle sweep, 3 first fine sweep, 4 coarse
+// levels (ELL phases and the per-problem coarse block), 5 k_b_cg_xr, 6 predictor).
+inline void b_prof(pycfd_batch* B, int id, cudaStream_t st) {
+  if (id != 0 && !B->capturing) prof_mark(B->mem, id, st);
+}
+
 template <class T>
 const BProb<T>* probs_of(pycfd_batch* B) { return (const BProb<T>*)B->probs; }
 template <class T>
@@ -268,7 +309,7 @@ int b_boundary(pycfd_batch* B, int arr, std::initializer_list<int> ops, int p_gh
   int k = 0;
   for (int op : ops) prog.op[k++] = op;
   prog.op[k] = OP_END;
-  BLAUNCH(k_b_boundary<T>, B->n, kBThreads, 0, st, probs_of<T>(B), arr, prog, p_ghosts);
+  BLAUNCH(k_b_boundary<T>, B->n, kBThreads, 0, st, probs_of<T>(B), arr, prog, p_ghosts, B->sh);
   return 0;
 }
 
@@ -276,22 +317,29 @@ template <class T, int OP>
 int b_ell(pycfd_batch* B, const BMapHost& m, int d, int src, int dst, cudaStream_t st) {
   if (m.n == 0) return 0;
   const size_t smem = OP == EO_RESTRICT ? B->smem_dense : 0;
-  BLAUNCH((k_b_ell<T, OP>), m.n, kBThreads, smem, st, probs_of<T>(B), hiers_of<T>(B), m.e, d, src, dst);
+  b_prof(B, 4, st);
+  BLAUNCH((k_b_ell<T, OP>), m.n, kBThreads, smem, st, probs_of<T>(B), m.e, d, src, dst, B->sh);
+  b_prof(B, 4, st);
   return 0;
 }
 
 template <class T, int MODE>
 int b_fine(pycfd_batch* B, int src, int dst, cudaStream_t st) {
+  const int id = MODE == FM_LAST ? 2 : MODE == FM_PRE ? 3 : 0;
+  b_prof(B, id, st);
   BLAUNCH((k_b_fine<T, MODE>), B->fine.n, kBFineBlock, 0, st, probs_of<T>(B), hiers_of<T>(B), B->fine.e, src,
           dst, B->sh);
+  b_prof(B, id, st);
   return 0;
 }
 
 // One V-cycle from zero on every solving problem, levels in lockstep by depth:
-// z <- M r, with mean(z) and r.z left in each problem's scalar block.
+// z <- M r, with mean(z) and r.z left in each problem's scalar block.  With
+// B->coarse > 0 the levels from there down run in one block per problem.
 template <class T>
 int b_vcycle(pycfd_batch* B, cudaStream_t st) {
-  const int sw = B->sweeps, D = B->depth;
+  const int sw = B->sweeps;
+  const int D = B->coarse > 0 ? std::min(B->coarse, B->depth) : B->depth;   // depths run per level
   // ---- down ----
   int cur0 = 0;
   if (sw == 1) {
@@ -306,34 +354,40 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
     TRY((b_fine<T, FM_RESID>(B, a, a, st)));
     cur0 = a;
   }
-  std::vector<int> cur(D, 0);
+  std::vector<int> cur(B->depth + 1, 0), fin(B->depth + 1, 0);
   for (int d = 1; d < D; ++d) {
-    TRY((b_ell<T, EO_RESTRICT>(B, B->restr[d], d, 0, 0, st)));
-    if (B->rows[d].n == 0) continue;
-    TRY((b_ell<T, EO_PRE>(B, B->rows[d], d, 0, 0, st)));
+    TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+    if (B->mapA[d].n == 0) continue;
+    TRY((b_ell<T, EO_PRE>(B, B->mapA[d], d, 0, 0, st)));
     int a = 0, o = 1;
     if (sw > 1) {
       for (int k = 1; k < sw; ++k) {
-        TRY((b_ell<T, EO_SMOOTH>(B, B->rows[d], d, a, o, st)));
+        TRY((b_ell<T, EO_SMOOTH>(B, B->mapA[d], d, a, o, st)));
         std::swap(a, o);
       }
-      TRY((b_ell<T, EO_RESID>(B, B->rows[d], d, a, a, st)));
+      TRY((b_ell<T, EO_RESID>(B, B->mapA[d], d, a, a, st)));
     }
     cur[d] = a;
   }
+  if (B->coarse > 0) {
+    b_prof(B, 4, st);
+    BLAUNCH(k_b_coarse<T>, B->n, kBCoarseThreads, B->smem_dense, st, probs_of<T>(B), B->order, B->coarse, sw,
+            B->sh);
+    b_prof(B, 4, st);
+    fin[D] = b_coarse_final(sw);
+  }
   // ---- up ----
-  std::vector<int> fin(D, 0);
-  for (int d = D - 2; d >= 1; --d) {
-    if (B->rows[d].n == 0) continue;
-    TRY((b_ell<T, EO_PROLONG>(B, B->rows[d], d, fin[d + 1], cur[d], st)));
+  for (int d = D - (B->coarse > 0 ? 1 : 2); d >= 1; --d) {
+    if (B->mapA[d].n == 0) continue;
+    TRY((b_ell<T, EO_PROLONG>(B, B->mapP[d], d, fin[d + 1], cur[d], st)));
     int xf = cur[d], o = 1 - cur[d];
     for (int k = 1; k <= sw; ++k) {
-      TRY((b_ell<T, EO_SMOOTH>(B, B->rows[d], d, xf, o, st)));
+      TRY((b_ell<T, EO_SMOOTH>(B, B->mapA[d], d, xf, o, st)));
       std::swap(xf, o);
     }
     fin[d] = xf;
   }
-  TRY((b_ell<T, EO_PROLONG>(B, B->rows[0], 0, fin[1], cur0, st)));
+  TRY((b_ell<T, EO_PROLONG>(B, B->mapP[0], 0, fin[1], cur0, st)));
   int xf = cur0, o = 1 - cur0;
   for (int k = 1; k <= sw; ++k) {
     if (k == sw) {
@@ -402,8 +456,12 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
   BLAUNCH(k_b_rhs_init<T>, B->fine.n, kBFineBlock, 0, st, P, B->n, B->fine.e, B->tol, B->maxiter, B->sh, ctl);
   auto pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
+    b_prof(B, 1, s2);
     BLAUNCH(k_b_cg_pq<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
+    b_prof(B, 1, s2);
+    b_prof(B, 5, s2);
     BLAUNCH(k_b_cg_xr<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, B->maxiter, B->sh, ctl);
+    b_prof(B, 5, s2);
     return 0;
   };
   if (B->capturing) {
@@ -421,7 +479,7 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
     }
   }
   BLAUNCH(k_b_finish_stats<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->tol, B->sh);
-  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e);
+  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->sh);
   return 0;
 }
 
@@ -435,12 +493,16 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
           kIrMaxPassesB, 1, B->sh, outer);
   auto inner_pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
+    b_prof(B, 1, s2);
     BLAUNCH(k_b_cg_pq<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
+    b_prof(B, 1, s2);
+    b_prof(B, 5, s2);
     BLAUNCH(k_b_cg_xr<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, kInnerMaxIterB, B->sh, inner);
+    b_prof(B, 5, s2);
     return 0;
   };
   auto refine = [&](cudaStream_t s2) -> int {
-    BLAUNCH(k_b_ir_update<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e);
+    BLAUNCH(k_b_ir_update<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
     BLAUNCH(k_b_ir_residual<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, B->tol, B->inner_tol,
             kIrMaxPassesB, 0, B->sh, outer);
     return 0;
@@ -475,7 +537,7 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
     }
   }
   BLAUNCH(k_b_finish_stats<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->tol, B->sh);
-  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e);
+  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->sh);
   return 0;
 }
 
@@ -486,14 +548,16 @@ int b_project(pycfd_batch* B, int arr, cudaStream_t st) {
   BLAUNCH(k_b_div_rhs<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, arr, B->sh);
   if (B->precision == PCFD_MIXED) TRY(b_solve_mixed(B, st));
   else TRY(b_solve_fp64(B, st));
-  BLAUNCH(k_b_correct<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, arr);
+  BLAUNCH(k_b_correct<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, arr, B->sh);
   return 0;
 }
 
 // One projected Euler substep of every problem: stage input ca*a + cb*b into dst.
 template <class T>
 int b_substep(pycfd_batch* B, int a, int b, double ca, double cb, int dst, cudaStream_t st) {
-  BLAUNCH(k_b_predictor<T>, B->fine.n, kBFineBlock, 0, st, probs_of<T>(B), B->fine.e, a, b, ca, cb, dst);
+  b_prof(B, 6, st);
+  BLAUNCH(k_b_predictor<T>, B->fine.n, kBFineBlock, 0, st, probs_of<T>(B), B->fine.e, a, b, ca, cb, dst, B->sh);
+  b_prof(B, 6, st);
   TRY(b_boundary<T>(B, dst, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, 0, st));
   TRY(b_project<T>(B, dst, st));
   TRY(b_boundary<T>(B, dst, {OP_MASK_ACC, OP_WRAP_FACES, OP_VEL_CORR}, 1, st));
@@ -506,11 +570,11 @@ template <class T>
 int b_step(pycfd_batch* B, cudaStream_t st) {
   const BProb<T>* P = probs_of<T>(B);
   BLAUNCH(k_b_stats<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->sh);
-  BLAUNCH(k_b_dt<T>, (B->n + 127) / 128, 128, 0, st, P, B->n);
+  BLAUNCH(k_b_dt<T>, (B->n + 127) / 128, 128, 0, st, P, B->n, B->sh);
   TRY(b_substep<T>(B, 0, -1, 1.0, 0.0, 1, st));
   TRY(b_substep<T>(B, 1, -1, 1.0, 0.0, 2, st));
   TRY(b_substep<T>(B, 0, 2, 0.75, 0.25, 1, st));
-  BLAUNCH(k_b_combine<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, 1, 1.0 / 3.0, 2.0 / 3.0);
+  BLAUNCH(k_b_combine<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, 1, 1.0 / 3.0, 2.0 / 3.0, B->sh);
   TRY(b_boundary<T>(B, 0, {OP_VEL_CORR, OP_WRAP_FACES}, 0, st));
   return 0;
 }
@@ -559,6 +623,8 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   if (opts->tile_rows != 8 && opts->tile_rows != 16 && opts->tile_rows != 32 && opts->tile_rows != 64)
     return fail(PCFD_E_ARG, "tile_rows must be 8, 16, 32 or 64");
   if (opts->mg_sweeps < 1 || opts->mg_sweeps > 4) return fail(PCFD_E_ARG, "mg_sweeps must be 1..4");
+  if (opts->coarse_level < 0 || opts->coarse_level >= kBMaxLevels)
+    return fail(PCFD_E_ARG, "coarse_level must be 0..%d", kBMaxLevels - 1);
   if (!(opts->tol > 0) || opts->maxiter < 1) return fail(PCFD_E_ARG, "bad tolerance or iteration limit");
   for (int i = 0; i < n; ++i) {
     if (!u[i] || !v[i] || !p[i]) return fail(PCFD_E_ARG, "problem %d: null state pointer", i);
@@ -573,6 +639,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->inner_tol = opts->inner_tol > 0 ? opts->inner_tol : 1e-4;
   B->sweeps = opts->mg_sweeps;
   B->tile_i = opts->tile_rows;
+  B->coarse = opts->coarse_level;
   B->mem = new pycfd_solver();
   B->solvers.assign(n, nullptr);
   for (int i = 0; i < n; ++i) {
@@ -637,6 +704,16 @@ int pycfd_batch_step(pycfd_batch* B, int steps, int record, void* stream) {
   }
   for (int k = 0; k < steps; ++k) CU(cudaGraphLaunch(B->exec, sm));
   return 0;
+}
+
+int pycfd_batch_profile(pycfd_batch* B, int kernel_id) {
+  if (!B || kernel_id < 0 || kernel_id > 6) return fail(PCFD_E_ARG, "bad arguments");
+  return pycfd_profile_kernel(B->mem, kernel_id);
+}
+
+int pycfd_batch_profile_read(pycfd_batch* B, double* total_ms, int* launches, void* stream) {
+  if (!B) return fail(PCFD_E_ARG, "bad arguments");
+  return pycfd_profile_read(B->mem, total_ms, launches, stream);
 }
 
 pycfd_solver* pycfd_batch_problem(pycfd_batch* B, int i) {

@@ -192,3 +192,28 @@ def coarsest_pseudo_inverse(level: MgLevelHost, singular: bool) -> np.ndarray:
     if singular and act.any():
         X[act, :] -= X[act, :].mean(axis=0)
     return np.ascontiguousarray(X)
+
+
+_CACHE: dict = {}
+_CACHE_ORDER: list = []
+_CACHE_MAX = 8
+
+
+def hierarchy_for(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None):
+    """``(fine operator, (levels, coarsest inverse))`` of one Poisson structure.
+
+    The hierarchy is a deterministic function of the assembled operator, so
+    problems that share grid, periodicity, Dirichlet walls and solid mask share
+    one build (kept for the last few structures of the process).
+    """
+    key = (nx, ny, dx, dy, bool(periodic_x), bool(periodic_y),
+           tuple(sorted((dirichlet or {}).items())),
+           None if solid is None else np.asarray(solid, bool).tobytes())
+    hit = _CACHE.get(key)
+    if hit is None:
+        op = assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid, dirichlet)
+        hit = _CACHE[key] = (op, build_hierarchy(op))
+        _CACHE_ORDER.append(key)
+        while len(_CACHE_ORDER) > _CACHE_MAX:
+            _CACHE.pop(_CACHE_ORDER.pop(0), None)
+    return hit

@@ -20,7 +20,7 @@ from . import _lib
 from .config import (AdvectionScheme, BCKind, PressureSolver, SimulationConfig, SolverType,
                      TimeScheme, WALLS)
 from .fields import FlowField
-from .hierarchy import assemble, build_hierarchy
+from .hierarchy import assemble, hierarchy_for
 from .mesh import StructuredMesh
 
 
@@ -292,12 +292,13 @@ class ProjectionSolver:
                     raise ValueError(f"body {k} mask must have shape {(nx, ny)}, got {b.shape}")
         self._build_slices()
         self.dirichlet_pressure = self.boundaries.dirichlet_pressure()
-        self.poisson = assemble(nx, ny, self.mesh.dx, self.mesh.dy, self.periodic_x,
-                                self.periodic_y, self.solid if self.has_obstacle else None,
-                                self.dirichlet_pressure or None)
+        args = (nx, ny, self.mesh.dx, self.mesh.dy, self.periodic_x, self.periodic_y,
+                self.solid if self.has_obstacle else None, self.dirichlet_pressure or None)
         self._levels, self._cinv = (None, None)
         if kind in (PressureSolver.MULTIGRID, PressureSolver.MGCG):
-            self._levels, self._cinv = build_hierarchy(self.poisson)
+            self.poisson, (self._levels, self._cinv) = hierarchy_for(*args)
+        else:
+            self.poisson = assemble(*args)
         self._create_native(kind)
         self.pressure_solver = GpuPoissonSolver(self, kind)
         self.turbulence = None
