@@ -289,9 +289,15 @@ def run_batch(args, world, rank, local):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     achieved = pq_bytes / (pq_ms / 1e3) / 1e9 if pq_ms > 0 else None
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
+        traffic = prof.get("batch_" + opts.precision, {}).get("1")
+    except Exception:
+        pass
     roof = {"bound": "hbm", "kernel": "k_b_cg_pq (batched CG direction p = z + beta p, q = A p, p.q)",
             "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "traffic": None,
+            "frac": achieved / hbm if achieved else None, "traffic": traffic,
             "bytes_per_launch": pq_bytes / max(pq_n, 1), "us_per_launch": 1e3 * pq_ms / max(pq_n, 1),
             "launches": pq_n, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
             "timing": "CUDA events around each eager launch over one step; bytes = sum over "
@@ -350,6 +356,127 @@ def run_batch(args, world, rank, local):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def run_tgv_validation(args, local):
+    """The 512x512 vortex over 500 steps in the FP64 path and in the mixed form: error of
+    each against the analytic decay (u, v ~ exp(-2 nu t), p ~ exp(-4 nu t), mean-free)
+    and of the mixed form against FP64."""
+    import torch
+    torch.cuda.set_device(local)
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    cfg = tgv_config()
+    steps = args.val_steps
+    out, fields = {}, {}
+    for prec in ("fp64", "mixed"):
+        s = ProjectionSolver(cfg, options=GpuOptions(precision=prec))
+        f = s.initialize(*tgv_init(s.mesh))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            f = s.advance(f, cfg.dt)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        t = steps * cfg.dt
+        nu = cfg.nu
+        Xu, Yu = s.mesh.u_grid()
+        Xv, Yv = s.mesh.v_grid()
+        ue = np.sin(Xu) * np.cos(Yu) * np.exp(-2 * nu * t)
+        ve = -np.cos(Xv) * np.sin(Yv) * np.exp(-2 * nu * t)
+        xc, yc = s.mesh.xc, s.mesh.yc
+        pe = 0.25 * (np.cos(2 * xc)[:, None] + np.cos(2 * yc)[None, :]) * np.exp(-4 * nu * t)
+        pe -= pe.mean()
+        u = f.u_phys.cpu().numpy()
+        v = f.v_phys.cpu().numpy()
+        p = f.p[1:-1, 1:-1].cpu().numpy()
+        p = p - p.mean()
+        st = s.field_stats(f)
+        fields[prec] = (u, v, p)
+        out[prec] = {"ms_per_step": ms, "cell_updates_per_s": N * N / (ms / 1e3),
+                     "err_u": float(np.abs(u - ue).max() / np.abs(ue).max()),
+                     "err_v": float(np.abs(v - ve).max() / np.abs(ve).max()),
+                     "err_p": float(np.abs(p - pe).max() / np.abs(pe).max()), "max_div": st.max_div}
+        del s
+    uf, vf, pf = fields["fp64"]
+    um, vm, pm = fields["mixed"]
+    scale = max(np.abs(uf).max(), np.abs(vf).max())
+    out["mixed_vs_fp64"] = {"velocity": float(max(np.abs(um - uf).max(), np.abs(vm - vf).max()) / scale),
+                            "pressure": float(np.abs(pm - pf).max() / np.abs(pf).max())}
+    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"validation": out, "t_end": steps * cfg.dt})}
+    print(json.dumps(line), flush=True)
+
+
+def run_cylinder(args, local):
+    """Flow past a cylinder on the 2048x1024 channel (Re 100, D 0.1 at (0.5, 0.5), uniform
+    inflow 1, convective outlet, slip walls, 1e-3 seeded noise), MG-PCG 1e-10, adaptive dt:
+    Cd and Cl histories in the FP64 path and in the mixed form."""
+    import torch
+    torch.cuda.set_device(local)
+    from pycfd_b200.config import BCKind, BCSpec, SimulationConfig
+    from pycfd_b200.mesh import StructuredMesh
+    from pycfd_b200.obstacles import circle_mask
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    nx, ny = 2048, 1024
+    walls = {"left": BCSpec(BCKind.INLET, velocity=1.0), "right": BCSpec(BCKind.OUTLET),
+             "bottom": BCSpec(BCKind.SYMMETRY), "top": BCSpec(BCKind.SYMMETRY)}
+    cfg = SimulationConfig(nx=nx, ny=ny, lx=2.0, ly=1.0, re=100.0, u_ref=1.0, l_ref=0.1, dt=1.0,
+                           t_end=1e9, cfl_max=0.5, pressure_solver="mgcg", poisson_tol=1e-10,
+                           boundary_config=walls, name="cylinder")
+    mesh = StructuredMesh.from_config(cfg)
+    obstacle = circle_mask(mesh, (0.5, 0.5), 0.05)
+    rng = np.random.default_rng(0)
+    u0 = 1.0 + 1e-3 * rng.standard_normal((nx + 1, ny))
+    v0 = 1e-3 * rng.standard_normal((nx, ny + 1))
+    steps, every = args.cyl_steps, 20
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = ProjectionSolver(cfg, mesh, obstacle, options=GpuOptions(precision=prec))
+        f = s.initialize(u0, v0)
+        s.set_clock(0.0)
+        ts, cd, cl = [], [], []
+        dev_ms = 0.0
+        for k in range(steps // every):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(every):
+                f = s.advance_adaptive(f)
+            b.record()
+            torch.cuda.synchronize()
+            dev_ms += a.elapsed_time(b)
+            st = s._read_stats()
+            t, dt, n, h = s.clock()
+            if h:
+                break
+            ts.append(t)
+            cd.append(st.fx / 0.05)
+            cl.append(st.fy / 0.05)
+        ts, cd, cl = np.array(ts), np.array(cd), np.array(cl)
+        half = ts >= 0.5 * ts[-1]
+        clh = cl[half] - cl[half].mean()
+        crossings = np.where(np.diff(np.sign(clh)) > 0)[0]
+        st_num = None
+        if len(crossings) >= 2:
+            period = (ts[half][crossings[-1]] - ts[half][crossings[0]]) / (len(crossings) - 1)
+            st_num = 0.1 / period
+        fs = s.field_stats(f)
+        out[prec] = {"steps": int(n), "t_end": float(ts[-1]), "ms_per_step": dev_ms / max(n, 1),
+                     "cell_updates_per_s": nx * ny * n / (dev_ms / 1e3),
+                     "cd_mean_second_half": float(cd[half].mean()), "cl_amplitude_second_half":
+                     float(0.5 * (cl[half].max() - cl[half].min())), "strouhal": st_num,
+                     "max_div": fs.max_div, "health": int(h),
+                     "cd_every_20": [round(float(x), 6) for x in cd[::10]],
+                     "cl_every_20": [round(float(x), 6) for x in cl[::10]]}
+        del s
+    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cylinder channel 2048x1024, Re 100", "runs": out}}
+    print(json.dumps(line), flush=True)
 
 
 def run_adjoint(args, world, rank, local):
@@ -529,9 +656,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--eager", action="store_true", help="launch kernels one by one (no CUDA graph)")
-    ap.add_argument("--workload", default="tgv512", choices=["tgv512", "batch", "adjoint"],
+    ap.add_argument("--workload", default="tgv512",
+                    choices=["tgv512", "batch", "adjoint", "tgv-validation", "cylinder"],
                     help="tgv512: the headline single-domain workload; batch: seeded cavity batch")
     ap.add_argument("--batch", type=int, default=256, help="problems in the batch workload")
+    ap.add_argument("--val-steps", type=int, default=500, help="tgv-validation: steps")
+    ap.add_argument("--cyl-steps", type=int, default=20000, help="cylinder: steps per precision")
     ap.add_argument("--autotune", action="store_true",
                     help="batch: pick tiles, sweeps, coarse level and inner tolerance by timing (cached)")
     ap.add_argument("--tile-rows", type=int, default=32, choices=[8, 16, 32, 64],
@@ -553,6 +683,12 @@ def main():
     elif args.workload == "adjoint":
         if rank == 0:
             run_adjoint(args, world, rank, local)
+    elif args.workload == "tgv-validation":
+        if rank == 0:
+            run_tgv_validation(args, local)
+    elif args.workload == "cylinder":
+        if rank == 0:
+            run_cylinder(args, local)
     else:
         run_ours(args, world, rank, local)
 
