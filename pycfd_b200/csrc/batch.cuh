@@ -73,6 +73,10 @@ struct BProb {
   double *b, *x;                         // FP64 right-hand side and solution (warm start)
   T *xs, *r, *z, *pa, *pb, *q;           // (inner) CG iterate and vectors
   T *lb[kBMaxLevels], *lxa[kBMaxLevels], *lxb[kBMaxLevels], *lres[kBMaxLevels];
+  // fine-operator diagonal and weighted inverse per face-flag pattern (F_W..F_N),
+  // formed at set-up with fine_diag's operations; Dirichlet edges use fine_diag
+  double dtab[16], wtab[16];
+  int any_dir;
   // the problem's copy of its structure's hierarchy (read with the record)
   double w0;
   const T* C;                            // coarsest pseudo-inverse, row-major
@@ -215,6 +219,37 @@ __device__ __forceinline__ double* b_arr_u(const BProb<T>& P, int code) {
 template <class T>
 __device__ __forceinline__ double* b_arr_v(const BProb<T>& P, int code) {
   return code == 0 ? P.v : code == 1 ? P.vs1 : P.vs2;
+}
+
+// Diagonal and weighted inverse diagonal of the fine operator at a cell: the
+// set-up table (the same subtractions as fine_diag, in its order, so the same
+// value), or fine_diag itself on an edge cell of a problem with Dirichlet walls.
+template <class T>
+__device__ __forceinline__ double b_diag(const BProb<T>& P, uint8_t f, int i, int j) {
+  if (!(f & F_SOLV)) return 1.0;
+  if (P.any_dir && (i == 0 || j == 0 || i == P.g.nx - 1 || j == P.g.ny - 1)) return fine_diag(f, i, j, P.g);
+  return P.dtab[f & 15];
+}
+template <class T>
+__device__ __forceinline__ double b_wdinv(const BProb<T>& P, uint8_t f, int i, int j) {
+  if (!(f & F_SOLV)) return P.w0 * (1.0 / 1.0);
+  if (P.any_dir && (i == 0 || j == 0 || i == P.g.nx - 1 || j == P.g.ny - 1))
+    return P.w0 * (1.0 / fine_diag(f, i, j, P.g));
+  return P.wtab[f & 15];
+}
+
+// (A x)_c in arithmetic type A: fine_apply's terms in its order, the diagonal
+// from the table.  A = double for the FP64 kernels; the mixed form's inner
+// solve uses A = float (FP32 accumulation, dot products stay FP64).
+template <class A, class T, class X>
+__device__ __forceinline__ A b_apply(const BProb<T>& P, uint8_t f, int i, int j, int c, X x) {
+  const Geo& g = P.g;
+  A acc = (A)b_diag(P, f, i, j) * x(c, i, j);
+  if (f & F_W) { const int a = wrap_w(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_E) { const int a = wrap_e(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_S) { const int b = wrap_s(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
+  if (f & F_N) { const int b = wrap_n(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
+  return acc;
 }
 
 // ---- step bookkeeping -------------------------------------------------------
@@ -467,7 +502,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __rest
           const uint8_t f = P.flags[c];
           const double bc = (f & F_SOLV) ? P.b[c] - mean : 0.0;
           P.b[c] = bc;
-          const double ax = fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return (double)P.xs[k]; });
+          const double ax = b_apply<double>(P, f, i, j, c, [&](int k, int, int) { return (double)P.xs[k]; });
           const double rc = bc - ax;
           P.r[c] = (T)rc;
           acc[0] += bc * bc;
@@ -511,21 +546,23 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
   const uint8_t* flags = P.flags;
   const T* zraw = P.z;
   const T* p_old = P.pa;
-  auto pval = [&](int k, int, int) -> double {
-    const double z = (flags[k] & F_SOLV) ? (double)zraw[k] - mz : 0.0;
-    if (first) return (double)(T)z;
-    return (double)(T)((double)p_old[k] * beta + z);
+  // arithmetic in T (FP32 in the mixed form's inner solve), p.q summed in FP64
+  const T tb = (T)beta, tm = (T)mz;
+  auto pval = [&](int k, int, int) -> T {
+    const T z = (flags[k] & F_SOLV) ? zraw[k] - tm : (T)0;
+    if (first) return z;
+    return p_old[k] * tb + z;
   };
   double acc[1] = {0.0};
   {
     B_CHUNK_TILES(P, e.y) {
       B_TILE_CELLS(P, tile_) {
         const int c = i * g.ny + j;
-        const double pc = pval(c, i, j);
-        const double qc = fine_apply<double>(flags[c], i, j, c, g, pval);
-        P.pb[c] = (T)pc;
-        P.q[c] = (T)qc;
-        acc[0] += pc * qc;
+        const T pc = pval(c, i, j);
+        const T qc = b_apply<T>(P, flags[c], i, j, c, pval);
+        P.pb[c] = pc;
+        P.q[c] = qc;
+        acc[0] += (double)pc * (double)qc;
       }
     }
   }
@@ -598,7 +635,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __
       B_TILE_CELLS(P, tile_) {
         const int c = i * g.ny + j;
         const uint8_t f = P.flags[c];
-        const double rc = P.b[c] - fine_apply<double>(f, i, j, c, g, xv);
+        const double rc = P.b[c] - b_apply<double>(P, f, i, j, c, xv);
         acc[0] += rc * rc;
         if (f & F_SOLV) acc[1] += xv(c, i, j);
       }
@@ -655,7 +692,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __r
             bc = (f & F_SOLV) ? bc - mean : 0.0;
             P.b[c] = bc;
           }
-          const double rc = bc - fine_apply<double>(f, i, j, c, g, [&](int k, int, int) { return P.x[k]; });
+          const double rc = bc - b_apply<double>(P, f, i, j, c, [&](int k, int, int) { return P.x[k]; });
           P.r[c] = (T)rc;
           P.xs[c] = (T)0;
           acc[0] += rc * rc;
@@ -746,13 +783,14 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
   const Geo& g = P.g;
-  const double w = P.w0;
-  const uint8_t* flags = P.flags;
-  const T* r = P.r;
-  const double mr = P.singular ? P.S[S_MEAN_R] : 0.0;
-  auto bf = [&](int k) -> double { return (flags[k] & F_SOLV) ? (double)r[k] - mr : 0.0; };
+  // arithmetic in T (FP32 in the mixed form's inner solve), sums in FP64
+  const uint8_t* __restrict__ flags = P.flags;
+  const T* __restrict__ r = P.r;
+  const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
+  auto bf = [&](int k) -> T { return (flags[k] & F_SOLV) ? r[k] - mr : (T)0; };
   const T* x = b_fine_buf(P, src);
   T* xo = b_fine_buf(P, dst);
+  T* __restrict__ lres0 = P.lres[0];
   double acc[2] = {0, 0};
   {
     B_CHUNK_TILES(P, e.y) {
@@ -760,24 +798,21 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
         const int c = i * g.ny + j;
         const uint8_t f = flags[c];
         if (MODE == FM_PRE) {
-          auto xv = [&](int k, int ii, int jj) -> double {
-            return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
-          };
-          xo[c] = (T)xv(c, i, j);
-          P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+          auto xv = [&](int k, int ii, int jj) -> T { return (T)b_wdinv(P, flags[k], ii, jj) * bf(k); };
+          xo[c] = xv(c, i, j);
+          lres0[c] = bf(c) - b_apply<T>(P, f, i, j, c, xv);
         } else if (MODE == FM_WDB) {
-          xo[c] = (T)(fine_wdinv(f, i, j, g, w) * bf(c));
+          xo[c] = (T)b_wdinv(P, f, i, j) * bf(c);
         } else if (MODE == FM_RESID) {
-          auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
-          P.lres[0][c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
+          auto xv = [&](int k, int, int) -> T { return x[k]; };
+          lres0[c] = bf(c) - b_apply<T>(P, f, i, j, c, xv);
         } else {
-          auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
-          const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
-                                        (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
-          xo[c] = (T)xn;
+          auto xv = [&](int k, int, int) -> T { return x[k]; };
+          const T xn = x[c] + (T)b_wdinv(P, f, i, j) * (bf(c) - b_apply<T>(P, f, i, j, c, xv));
+          xo[c] = xn;
           if (MODE == FM_LAST && (f & F_SOLV)) {
-            acc[0] += xn;
-            acc[1] += (double)r[c] * xn;
+            acc[0] += (double)xn;
+            acc[1] += (double)r[c] * (double)xn;
           }
         }
       }
@@ -808,18 +843,18 @@ __device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
 // Row dot product of E by L lanes (L a power of two, runtime), rows past the
 // end contribute nothing; every lane of the warp calls it.
 template <class T, class X>
-__device__ __forceinline__ double b_ell_row(const Ell<T>& E, int L, int row, int lane, X x) {
-  double acc = 0.0;
+__device__ __forceinline__ T b_ell_row(const Ell<T>& E, int L, int row, int lane, X x) {
+  T acc = (T)0;
   if (row < E.n) {
     if (E.rowmajor) {
       const long base = (long)row * E.K;
 #pragma unroll 4
-      for (int k = lane; k < E.K; k += L) acc += (double)E.val[base + k] * x(E.col[base + k]);
+      for (int k = lane; k < E.K; k += L) acc += E.val[base + k] * x(E.col[base + k]);
     } else {
 #pragma unroll 4
       for (int k = lane; k < E.K; k += L) {
         const long at = (long)k * E.n + row;
-        acc += (double)E.val[at] * x(E.col[at]);
+        acc += E.val[at] * x(E.col[at]);
       }
     }
   }
@@ -843,10 +878,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     const int per = kBThreads / L;
     for (int base = 0; base < Lc.R.n; base += per) {
       const int row = base + (int)threadIdx.x / L;
-      const double s = b_ell_row(Lc.R, L, row, lane, [&](int c) { return (double)res[c]; });
+      const T s = b_ell_row(Lc.R, L, row, lane, [&](int c) { return res[c]; });
       if (lane == 0 && row < Lc.R.n) {
-        sb[row] = (double)(T)s;
-        P.lb[d][row] = (T)s;
+        sb[row] = (double)s;
+        P.lb[d][row] = s;
       }
     }
     __syncthreads();
@@ -876,8 +911,8 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
 #pragma unroll
     for (int rd = 0; rd < kBEllRounds; ++rd) {
       const int row = r0 + rd * per + (int)threadIdx.x / Lop;
-      const double s = b_ell_row(Lc.P, Lop, row < r1 ? row : Lc.P.n, lane, [&](int c) { return (double)xc[c]; });
-      if (lane == 0 && row < r1) xf[row] = (T)((double)xf[row] + s);
+      const T s = b_ell_row(Lc.P, Lop, row < r1 ? row : Lc.P.n, lane, [&](int c) { return xc[c]; });
+      if (lane == 0 && row < r1) xf[row] = xf[row] + s;
     }
     return;
   }
@@ -888,8 +923,8 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
 #pragma unroll
     for (int rd = 0; rd < kBEllRounds; ++rd) {
       const int row = r0 + rd * per + (int)threadIdx.x / Lop;
-      const double s = b_ell_row(Lv.R, Lop, row < r1 ? row : Lv.R.n, lane, [&](int c) { return (double)res[c]; });
-      if (lane == 0 && row < r1) bo[row] = (T)s;
+      const T s = b_ell_row(Lv.R, Lop, row < r1 ? row : Lv.R.n, lane, [&](int c) { return res[c]; });
+      if (lane == 0 && row < r1) bo[row] = s;
     }
     return;
   }
@@ -904,18 +939,18 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     const int row = r0 + rd * per + (int)threadIdx.x / Lop;
     const int rr = row < r1 ? row : Lv.A.n;
     if (OP == EO_PRE) {
-      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
+      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return wd[c] * b[c]; });
       if (lane == 0 && row < r1) {
-        const double bx = (double)b[row];
-        xa[row] = (T)((double)wd[row] * bx);
-        ro[row] = (T)(bx - s);
+        const T bx = b[row];
+        xa[row] = wd[row] * bx;
+        ro[row] = bx - s;
       }
     } else if (OP == EO_SMOOTH) {
-      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)x[c]; });
-      if (lane == 0 && row < r1) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return x[c]; });
+      if (lane == 0 && row < r1) xo[row] = x[row] + wd[row] * (b[row] - s);
     } else {   // EO_RESID
-      const double s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return (double)x[c]; });
-      if (lane == 0 && row < r1) ro[row] = (T)((double)b[row] - s);
+      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return x[c]; });
+      if (lane == 0 && row < r1) ro[row] = b[row] - s;
     }
   }
 }
@@ -944,7 +979,7 @@ __device__ __forceinline__ void b_blk_ell(const Ell<T>& E, int L, X x, W write) 
   const int lane = threadIdx.x & (L - 1), per = blockDim.x / L;
   for (int base = 0; base < E.n; base += per) {
     const int row = base + (int)threadIdx.x / L;
-    const double s = b_ell_row(E, L, row, lane, x);
+    const T s = b_ell_row(E, L, row, lane, x);
     if (lane == 0 && row < E.n) write(row, s);
   }
 }
@@ -966,9 +1001,9 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
     const T* __restrict__ src = P.lres[l - 1];
     T* __restrict__ bl = P.lb[l];
     const bool coarsest = l == c;
-    b_blk_ell(Lv.R, Lv.lr, [&](int k) { return (double)src[k]; }, [&](int row, double s) {
-      bl[row] = (T)s;
-      if (coarsest) sb[row] = (double)(T)s;
+    b_blk_ell(Lv.R, Lv.lr, [&](int k) { return src[k]; }, [&](int row, T s) {
+      bl[row] = s;
+      if (coarsest) sb[row] = (double)s;
     });
     __syncthreads();
     if (coarsest) {
@@ -989,10 +1024,10 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
     T* __restrict__ xa = P.lxa[l];
     T* __restrict__ xb = P.lxb[l];
     T* __restrict__ rs = P.lres[l];
-    b_blk_ell(Lv.A, Lv.la, [&](int k) { return (double)wd[k] * (double)bl[k]; }, [&](int row, double s) {
-      const double bx = (double)bl[row];
-      xa[row] = (T)((double)wd[row] * bx);
-      rs[row] = (T)(bx - s);
+    b_blk_ell(Lv.A, Lv.la, [&](int k) { return wd[k] * bl[k]; }, [&](int row, T s) {
+      const T bx = bl[row];
+      xa[row] = wd[row] * bx;
+      rs[row] = bx - s;
     });
     __syncthreads();
     int a = 0;
@@ -1000,15 +1035,15 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
       for (int k = 1; k < sweeps; ++k) {
         const T* xi = a == 0 ? xa : xb;
         T* xn = a == 0 ? xb : xa;
-        b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; }, [&](int row, double s) {
-          xn[row] = (T)((double)xi[row] + (double)wd[row] * ((double)bl[row] - s));
+        b_blk_ell(Lv.A, Lv.la, [&](int q) { return xi[q]; }, [&](int row, T s) {
+          xn[row] = xi[row] + wd[row] * (bl[row] - s);
         });
         __syncthreads();
         a ^= 1;
       }
       const T* xi = a == 0 ? xa : xb;
-      b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; },
-                [&](int row, double s) { rs[row] = (T)((double)bl[row] - s); });
+      b_blk_ell(Lv.A, Lv.la, [&](int q) { return xi[q]; },
+                [&](int row, T s) { rs[row] = bl[row] - s; });
       __syncthreads();
     }
     cur[l] = a;
@@ -1023,8 +1058,8 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
     int a = cur[l];
     {
       T* __restrict__ xf = a == 0 ? xa : xb;
-      b_blk_ell(Lc.P, Lc.lp, [&](int k) { return (double)xc[k]; },
-                [&](int row, double s) { xf[row] = (T)((double)xf[row] + s); });
+      b_blk_ell(Lc.P, Lc.lp, [&](int k) { return xc[k]; },
+                [&](int row, T s) { xf[row] = xf[row] + s; });
       __syncthreads();
     }
     const T* __restrict__ wd = Lv.wd;
@@ -1032,8 +1067,8 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
     for (int k = 1; k <= sweeps; ++k) {
       const T* xi = a == 0 ? xa : xb;
       T* xn = a == 0 ? xb : xa;
-      b_blk_ell(Lv.A, Lv.la, [&](int q) { return (double)xi[q]; }, [&](int row, double s) {
-        xn[row] = (T)((double)xi[row] + (double)wd[row] * ((double)bl[row] - s));
+      b_blk_ell(Lv.A, Lv.la, [&](int q) { return xi[q]; }, [&](int row, T s) {
+        xn[row] = xi[row] + wd[row] * (bl[row] - s);
       });
       __syncthreads();
       a ^= 1;

@@ -218,6 +218,18 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       TRY(dalloc(B->mem, &P.lres[l], K[l].n));
     }
     P.w0 = hh[hid[i]].w0;
+    // diagonal per face-flag pattern: fine_diag's subtractions in its order (an
+    // interior cell gets no Dirichlet terms), and w / diag as in fine_wdinv
+    P.any_dir = s->g.dir_w || s->g.dir_e || s->g.dir_s || s->g.dir_n;
+    for (int f = 0; f < 16; ++f) {
+      double dg = 0.0;
+      if (f & F_W) dg -= s->g.cx;
+      if (f & F_E) dg -= s->g.cx;
+      if (f & F_S) dg -= s->g.cy;
+      if (f & F_N) dg -= s->g.cy;
+      P.dtab[f] = dg;
+      P.wtab[f] = dg != 0.0 ? P.w0 * (1.0 / dg) : 0.0;
+    }
     P.C = hh[hid[i]].C;
     for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
