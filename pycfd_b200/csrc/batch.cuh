@@ -862,6 +862,90 @@ __device__ __forceinline__ T b_ell_row(const Ell<T>& E, int L, int row, int lane
   return acc;
 }
 
+// Row dot product of E with L lanes fixed at compile time (L > 1: row-major
+// entries, L = 1: column-major), the same summation order as b_ell_row.
+template <int L, class T, class X>
+__device__ __forceinline__ T b_ell_row_c(const Ell<T>& E, int row, int lane, X x) {
+  T acc = (T)0;
+  if (row < E.n) {
+    if (L > 1) {
+      const long base = (long)row * E.K;
+#pragma unroll 4
+      for (int k = lane; k < E.K; k += L) acc += E.val[base + k] * x(E.col[base + k]);
+    } else {
+#pragma unroll 4
+      for (int k = 0; k < E.K; ++k) {
+        const long at = (long)k * E.n + row;
+        acc += E.val[at] * x(E.col[at]);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
+  return acc;
+}
+
+// Rows [r0, r1) of level d for one ELL op: kBEllRounds rounds of kBThreads / L
+// rows, the rounds unrolled so their loads overlap.
+template <int L, int OP, class T>
+__device__ __forceinline__ void b_ell_rows(const BProb<T>& P, int d, int src, int dst, int blk) {
+  constexpr int per = kBThreads / L;
+  const int n = (d == 0) ? P.g.nx * P.g.ny : P.lv[d].n;
+  const int r0 = blk * per * kBEllRounds;
+  const int r1 = min(n, r0 + per * kBEllRounds);
+  const int lane = threadIdx.x & (L - 1);
+  if (OP == EO_PROLONG) {
+    // x_d += P_{d+1} x_{d+1}
+    const BLevel<T>& Lc = P.lv[d + 1];
+    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
+    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
+#pragma unroll
+    for (int rd = 0; rd < kBEllRounds; ++rd) {
+      const int row = r0 + rd * per + (int)threadIdx.x / L;
+      const T s = b_ell_row_c<L>(Lc.P, row < r1 ? row : Lc.P.n, lane, [&](int c) { return xc[c]; });
+      if (lane == 0 && row < r1) xf[row] = xf[row] + s;
+    }
+    return;
+  }
+  const BLevel<T>& Lv = P.lv[d];
+  if (OP == EO_RESTRICT) {
+    const T* __restrict__ res = P.lres[d - 1];
+    T* __restrict__ bo = P.lb[d];
+#pragma unroll
+    for (int rd = 0; rd < kBEllRounds; ++rd) {
+      const int row = r0 + rd * per + (int)threadIdx.x / L;
+      const T s = b_ell_row_c<L>(Lv.R, row < r1 ? row : Lv.R.n, lane, [&](int c) { return res[c]; });
+      if (lane == 0 && row < r1) bo[row] = s;
+    }
+    return;
+  }
+  const T* __restrict__ b = P.lb[d];
+  const T* __restrict__ wd = Lv.wd;
+  const T* __restrict__ x = b_lvl_x(P, d, src);
+  T* __restrict__ xo = b_lvl_x(P, d, dst);
+  T* __restrict__ xa = P.lxa[d];
+  T* __restrict__ ro = P.lres[d];
+#pragma unroll
+  for (int rd = 0; rd < kBEllRounds; ++rd) {
+    const int row = r0 + rd * per + (int)threadIdx.x / L;
+    const int rr = row < r1 ? row : Lv.A.n;
+    if (OP == EO_PRE) {
+      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return wd[c] * b[c]; });
+      if (lane == 0 && row < r1) {
+        const T bx = b[row];
+        xa[row] = wd[row] * bx;
+        ro[row] = bx - s;
+      }
+    } else if (OP == EO_SMOOTH) {
+      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return x[c]; });
+      if (lane == 0 && row < r1) xo[row] = x[row] + wd[row] * (b[row] - s);
+    } else {   // EO_RESID
+      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return x[c]; });
+      if (lane == 0 && row < r1) ro[row] = b[row] - s;
+    }
+  }
+}
+
 template <class T, int OP>
 __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict__ probs,
                                                       const int2* __restrict__ map, int d, int src,
@@ -895,63 +979,14 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     }
     return;
   }
-  // rows [r0, r1) of level d: kBEllRounds rounds of kBThreads / L rows each
-  // (L: lanes of the block's matrix), the rounds unrolled so their loads overlap
-  const int n = (d == 0) ? P.g.nx * P.g.ny : P.lv[d].n;
+  // the rows of this block, with the lane count of its matrix fixed at compile time
   const int Lop = OP == EO_PROLONG ? P.lv[d + 1].lp : OP == EO_RESTRICT ? P.lv[d].lr : P.lv[d].la;
-  const int per = kBThreads / Lop;
-  const int r0 = e.y * per * kBEllRounds;
-  const int r1 = min(n, r0 + per * kBEllRounds);
-  const int lane = threadIdx.x & (Lop - 1);
-  if (OP == EO_PROLONG) {
-    // x_d += P_{d+1} x_{d+1}
-    const BLevel<T>& Lc = P.lv[d + 1];
-    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
-    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
-#pragma unroll
-    for (int rd = 0; rd < kBEllRounds; ++rd) {
-      const int row = r0 + rd * per + (int)threadIdx.x / Lop;
-      const T s = b_ell_row(Lc.P, Lop, row < r1 ? row : Lc.P.n, lane, [&](int c) { return xc[c]; });
-      if (lane == 0 && row < r1) xf[row] = xf[row] + s;
-    }
-    return;
-  }
-  const BLevel<T>& Lv = P.lv[d];
-  if (OP == EO_RESTRICT) {
-    const T* __restrict__ res = P.lres[d - 1];
-    T* __restrict__ bo = P.lb[d];
-#pragma unroll
-    for (int rd = 0; rd < kBEllRounds; ++rd) {
-      const int row = r0 + rd * per + (int)threadIdx.x / Lop;
-      const T s = b_ell_row(Lv.R, Lop, row < r1 ? row : Lv.R.n, lane, [&](int c) { return res[c]; });
-      if (lane == 0 && row < r1) bo[row] = s;
-    }
-    return;
-  }
-  const T* __restrict__ b = P.lb[d];
-  const T* __restrict__ wd = Lv.wd;
-  const T* __restrict__ x = b_lvl_x(P, d, src);
-  T* __restrict__ xo = b_lvl_x(P, d, dst);
-  T* __restrict__ xa = P.lxa[d];
-  T* __restrict__ ro = P.lres[d];
-#pragma unroll
-  for (int rd = 0; rd < kBEllRounds; ++rd) {
-    const int row = r0 + rd * per + (int)threadIdx.x / Lop;
-    const int rr = row < r1 ? row : Lv.A.n;
-    if (OP == EO_PRE) {
-      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return wd[c] * b[c]; });
-      if (lane == 0 && row < r1) {
-        const T bx = b[row];
-        xa[row] = wd[row] * bx;
-        ro[row] = bx - s;
-      }
-    } else if (OP == EO_SMOOTH) {
-      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return x[c]; });
-      if (lane == 0 && row < r1) xo[row] = x[row] + wd[row] * (b[row] - s);
-    } else {   // EO_RESID
-      const T s = b_ell_row(Lv.A, Lop, rr, lane, [&](int c) { return x[c]; });
-      if (lane == 0 && row < r1) ro[row] = b[row] - s;
-    }
+  switch (Lop) {
+    case 1: b_ell_rows<1, OP>(P, d, src, dst, e.y); break;
+    case 4: b_ell_rows<4, OP>(P, d, src, dst, e.y); break;
+    case 8: b_ell_rows<8, OP>(P, d, src, dst, e.y); break;
+    case 16: b_ell_rows<16, OP>(P, d, src, dst, e.y); break;
+    default: b_ell_rows<32, OP>(P, d, src, dst, e.y); break;
   }
 }
 
