@@ -113,6 +113,14 @@ typedef struct {
                                                  0 = one kernel per phase    */
     int sequential_launch;                    /* 1: plain stream order between kernels;
                                                  0: programmatic dependent launch */
+    int persistent_solve;                     /* CG / MG-PCG: 1 = the whole solve as one
+                                                 cooperative launch (phases separated by
+                                                 grid barriers); 0 = one kernel per phase */
+    int tail_level;                           /* multigrid: level l >= 1 above the coarsest
+                                                 whose cycle (sweeps, coarser levels,
+                                                 sweeps back) is applied as one dense
+                                                 operator; 0 = level by level      */
+    const double* tail_operator;              /* n_l x n_l row-major, x_l = M b_l   */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */
@@ -236,9 +244,20 @@ int pycfd_step_host(pycfd_solver* s, const double* u0_host, const double* v0_hos
  * launch of one kernel with CUDA events on its stream, then read the summed
  * device time.  Ids: 1 CG direction/A-product (k_cg_pq), 2 last fine smoothing
  * sweep of the V-cycle, 3 first fine sweep + residual, 4 coarse-level cluster
- * cycle, 6 momentum predictor, 7 projection correction; 0 switches it off.
+ * cycle, 6 momentum predictor, 7 projection correction, 8 whole persistent
+ * solve (k_solve_persistent); 0 switches it off.
  * Steps replayed from a recorded graph are not bracketed. */
 int pycfd_profile_kernel(pycfd_solver* s, int kernel_id);
+/* CTAs of the cooperative launch that runs each CG / MG-PCG solve whole
+ * (0: the solver launches one kernel per phase). */
+int pycfd_solver_persistent(pycfd_solver* s, int* ctas);
+/* Phase trace of the persistent solve (measurement support).  enable 1 turns
+ * it on (each later solve overwrites it), 0 off, -1 leaves it as it is.  With
+ * out != NULL: waits for `stream`, then copies the last solve's trace -- out[0]
+ * = entries n, then n pairs (globaltimer ns when the barrier ending a phase
+ * released, phase tag: low byte the phase kind, next byte the level) -- at
+ * most cap words. */
+int pycfd_solve_trace(pycfd_solver* s, int enable, unsigned long long* out, int cap, void* stream);
 /* Kernel launches issued by this library so far (eager launches; a recorded
  * step counts its launches once, when it is recorded). */
 long long pycfd_launch_count(void);

@@ -27,7 +27,7 @@ EXPORTS = (
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
     "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
-    "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_launch_count",
+    "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_solver_persistent", "pycfd_solve_trace", "pycfd_launch_count",
     "pycfd_profile_read", "pycfd_batch_create", "pycfd_batch_destroy", "pycfd_batch_initialize",
     "pycfd_batch_step", "pycfd_batch_problem", "pycfd_batch_status", "pycfd_batch_launches",
     "pycfd_batch_profile", "pycfd_batch_profile_read",
@@ -55,7 +55,8 @@ class SolverDesc(C.Structure):
                 ("mg_sweeps", C.c_int), ("time_scheme", C.c_int), ("precision", C.c_int),
                 ("inner_tol", C.c_double), ("n_levels", C.c_int),
                 ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp),
-                ("coarse_cluster_rows", C.c_int), ("sequential_launch", C.c_int)]
+                ("coarse_cluster_rows", C.c_int), ("sequential_launch", C.c_int),
+                ("persistent_solve", C.c_int), ("tail_level", C.c_int), ("tail_operator", _dp)]
 
 
 class DtControl(C.Structure):
@@ -123,6 +124,8 @@ def load(path: str = LIB_PATH):
                                       C.POINTER(C.c_int), C.POINTER(C.c_int), vp]),
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
         "pycfd_profile_kernel": (C.c_int, [vp, C.c_int]),
+        "pycfd_solver_persistent": (C.c_int, [vp, C.POINTER(C.c_int)]),
+        "pycfd_solve_trace": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ulonglong), C.c_int, vp]),
         "pycfd_launch_count": (C.c_longlong, []),
         "pycfd_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),

@@ -20,7 +20,7 @@ import ctypes as C
 import json
 import os
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 
 import numpy as np
 
@@ -147,6 +147,8 @@ class BatchRunner:
             else:
                 ch = None
                 opts = options or GpuOptions()
+            if streams > 1:   # concurrent solves: one kernel per phase, no grid-filling launch
+                opts = replace(opts, persistent_solve=False)
             self.choices.append(ch)
             s = ProjectionSolver(cfg, options=opts)
             self.solvers.append(s)

@@ -160,6 +160,46 @@ __global__ void k_restrict_dense(Ell<T> R, int L, const T* __restrict__ res, con
   }
 }
 
+// Dense close of the V-cycle: x = M b, M (row-major n x n) the cycle's map at
+// and below one level (the host builds it from the hierarchy).  kTailWarps
+// warps per row, their lanes striding the columns eight loads at a time; the
+// warps' sums are added in warp order.  256-thread blocks, two rows each.
+constexpr int kTailWarps = 4;
+constexpr int kTailRowsPerBlock = 256 / 32 / kTailWarps;
+template <class T>
+__global__ void __launch_bounds__(256) k_tail(const T* __restrict__ M, int n, const T* __restrict__ b,
+                                              T* __restrict__ x) {
+  pdl_begin();
+  __shared__ double part[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * kTailRowsPerBlock + warp / kTailWarps;
+  const int w = warp % kTailWarps;
+  double acc = 0.0;
+  if (row < n) {
+    const T* m = M + (long)row * n;
+    constexpr int stride = 32 * kTailWarps;
+    for (int k0 = w * 32 + lane; k0 < n; k0 += 8 * stride) {
+      T mm[8], bb[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = k0 + u * stride;
+        mm[u] = k < n ? __ldg(m + k) : (T)0;
+        bb[u] = k < n ? b[k] : (T)0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc += (double)mm[u] * (double)bb[u];
+    }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (row < n && w == 0 && lane == 0) {
+    double t = 0.0;
+    for (int k = 0; k < kTailWarps; ++k) t += part[warp + k];
+    x[row] = (T)t;
+  }
+}
+
 // ---- level 0 (matrix-free) --------------------------------------------------
 // Right-hand side of the fine level: the CG residual projected onto the
 // active set (multigrid.py:453-458), or a stored vector.

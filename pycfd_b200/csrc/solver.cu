@@ -15,6 +15,7 @@
 #include "boundary.cuh"
 #include "common.cuh"
 #include "multigrid.cuh"
+#include "persistent.cuh"
 #include "poisson.cuh"
 #include "stencil.cuh"
 
@@ -126,6 +127,9 @@ struct pycfd_solver {
   double* C = nullptr;
   float* Cf = nullptr;
   int nc = 0;
+  int tail_level = 0;           // level whose cycle is one dense operator (0: none)
+  double* tail = nullptr;
+  float* tailf = nullptr;
   int last_ir = 0;
   // per-kernel timing of eager launches (measurement support)
   int prof_id = 0;
@@ -134,6 +138,12 @@ struct pycfd_solver {
   int pdl = 1;                  // programmatic dependent launch between step kernels
   int cluster_from = 1 << 30;   // first level run inside the coarse cluster kernel
   int cluster_size = 0;         // CTAs per cluster (0: not used)
+  // whole CG / MG-PCG solves as one cooperative launch
+  int persistent = 0;           // CTAs of that launch (0: one kernel per phase)
+  unsigned* pbar = nullptr;     // barrier words, zeroed before every launch
+  double* ppart = nullptr;      // per-CTA partial sums
+  unsigned long long* ptrace = nullptr;   // phase trace (measurement support)
+  int trace_on = 0;
   // CUDA-graph recording of whole steps
   bool capturing = false;
   cudaStream_t aux = nullptr;   // records the bodies of the solve loops
@@ -320,6 +330,12 @@ double* lvWd<double>(Level& l) { return l.wd; }
 template <>
 float* lvWd<float>(Level& l) { return l.wdf; }
 template <class T>
+const T* tailM(pycfd_solver* s);
+template <>
+const double* tailM<double>(pycfd_solver* s) { return s->tail; }
+template <>
+const float* tailM<float>(pycfd_solver* s) { return s->tailf; }
+template <class T>
 const T* coarseC(pycfd_solver* s);
 template <>
 const double* coarseC<double>(pycfd_solver* s) { return s->C; }
@@ -429,9 +445,11 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     cur[0] = a;
   }
   const int lc = std::max(1, std::min(s->cluster_from, Lv));
+  int bottom = Lv - 1;   // level where the down sweep ends
   for (int l = 1; l < Lv; ++l) {
     if (l >= lc) {   // the rest of the cycle below l runs in one cluster
       TRY(launch_coarse_cluster<T>(s, l, lvB<T>(s->lv[l - 1]).res, &cur[l], stream));
+      bottom = l;
       break;
     }
     Level& Lc = s->lv[l];
@@ -447,6 +465,14 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     }
     ELL_DISPATCH(R.lanes, (pdl_launch(s, k_ell_spmv<L, false, T>, ell_grid(R.n, L), 256, 0, stream, R.view(), res_f, Bc.b)));
     CHECK_LAUNCH();
+    if (l == s->tail_level) {   // the cycle at and below l as one dense operator
+      pdl_launch(s, k_tail<T>, (Lc.n + kTailRowsPerBlock - 1) / kTailRowsPerBlock, 256, 0, stream, tailM<T>(s), Lc.n,
+                 (const T*)Bc.b, Bc.xa);
+      CHECK_LAUNCH();
+      cur[l] = Bc.xa;
+      bottom = l;
+      break;
+    }
     const DevEll<T>& A = lvA<T>(Lc);
     T* wd = lvWd<T>(Lc);
     ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_pre<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bc.b, Bc.xa, Bc.res)));
@@ -465,7 +491,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     cur[l] = a;
   }
   // ---- up ----
-  for (int l = std::min(Lv - 2, lc - 1); l >= 0; --l) {
+  for (int l = bottom - 1; l >= 0; --l) {
     Level& Lf = s->lv[l];
     LevelBuf<T>& Bf = lvB<T>(Lf);
     const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
@@ -729,6 +755,78 @@ int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
   return 0;
 }
 
+// ---- CG / MG-PCG as one cooperative launch ---------------------------------
+// The kernel conditions b, runs the passes, leaves ||b - A x|| and the mean of
+// x in the scalar slots and removes the mean (k_rhs_init ... k_finish_apply);
+// the barrier
+// words start at zero for every launch, so a wait that gave up in an earlier
+// launch leaves no trace.
+int solve_persistent(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
+  PSolve<double> t{};
+  const int Lv = (int)s->lv.size();
+  const bool mg = s->solver_kind == PCFD_SOLVER_MGCG;
+  if (mg) {
+    t.nlev = Lv;
+    for (int l = 0; l < Lv; ++l) {
+      Level& L = s->lv[l];
+      PLevel<double>& c = t.lv[l];
+      if (l >= 1) {
+        if (l < Lv - 1) {
+          c.A = L.A.view();
+          c.la = L.A.lanes;
+        }
+        c.R = L.R.view();
+        c.lr = L.R.lanes;
+        c.P = L.P.view();
+        c.lp = L.P.lanes;
+        c.wd = L.wd;
+      }
+      c.b = L.d.b;
+      c.xa = L.d.xa;
+      c.xb = L.d.xb;
+      c.res = L.d.res;
+    }
+    t.C = s->C;
+    t.nc = s->nc;
+    t.tail = s->tail;
+    t.tail_level = s->tail_level;
+    t.w0 = s->lv[0].weight;
+  }
+  t.flags = s->flags;
+  t.g = s->g;
+  t.sweeps = s->mg_sweeps;
+  t.cfg = s->cfg();
+  t.has_x0 = has_x0 ? 1 : 0;
+  t.b = s->b;
+  t.x = x;
+  t.r = s->r;
+  t.z = s->z;
+  t.pa = s->pa;
+  t.pb = s->pb;
+  t.q = s->q;
+  t.S = s->S;
+  t.I = s->I;
+  t.partials = s->ppart;
+  t.bar = s->pbar;
+  t.trace = s->trace_on ? s->ptrace : nullptr;
+  CU(cudaMemsetAsync(s->pbar, 0, 64 * sizeof(unsigned), stream));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(s->persistent);
+  cfg.blockDim = dim3(kPThreads);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  prof_mark(s, 8, stream);
+  if (mg) CU(cudaLaunchKernelEx(&cfg, k_solve_persistent<double, PC_MG>, t));
+  else CU(cudaLaunchKernelEx(&cfg, k_solve_persistent<double, PC_JACOBI>, t));
+  prof_mark(s, 8, stream);
+  CHECK_LAUNCH();
+  return 0;
+}
+
 // ---- Poisson solve on the prepared raw right-hand side s->b --------------
 // Result (normalised) in x.  has_x0: x holds the warm start on entry.
 int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
@@ -737,6 +835,9 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
   const SolveCfg cfg = s->cfg();
   const int kind = s->solver_kind;
   const bool cap = s->capturing;
+  if (s->persistent && (kind == PCFD_SOLVER_CG || kind == PCFD_SOLVER_MGCG)) {
+    return solve_persistent(s, x, has_x0, stream);   // mean removal included
+  }
   if (kind == PCFD_SOLVER_CG || kind == PCFD_SOLVER_MGCG) {
     Loop L;
     TRY(loop_handle(s, stream, &L));
@@ -1183,6 +1284,17 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
     }
     if ((rc = upload(s, &s->C, cm.data(), cm.size())) || (rc = upload(s, &s->Cf, cf.data(), cf.size())))
       return bail(rc);
+    const int tl = d->tail_level;
+    if (tl > 0) {
+      if (tl >= (int)s->lv.size() - 1 || !d->tail_operator)
+        return bail(fail(PCFD_E_ARG, "tail_level must name a level above the coarsest, with its operator"));
+      const size_t nt = (size_t)s->lv[tl].n;
+      std::vector<float> tf(nt * nt);
+      for (size_t e = 0; e < nt * nt; ++e) tf[e] = (float)d->tail_operator[e];
+      if ((rc = upload(s, &s->tail, d->tail_operator, nt * nt)) || (rc = upload(s, &s->tailf, tf.data(), nt * nt)))
+        return bail(rc);
+      s->tail_level = tl;
+    }
   }
   if (mg && d->coarse_cluster_rows > 0 && s->lv.size() > 1) {
     // coarse levels: first level (>= 1) with at most coarse_cluster_rows rows
@@ -1222,6 +1334,21 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
     }
     s->cluster_size = best;
     if (!best) s->cluster_from = 1 << 30;
+  }
+  if (d->persistent_solve && s->precision != PCFD_MIXED &&
+      (s->solver_kind == PCFD_SOLVER_CG || s->solver_kind == PCFD_SOLVER_MGCG) &&
+      (int)s->lv.size() <= kPMaxLevels) {
+    // one CTA pair per SM at most: the grid is resident at once by construction
+    int dev = 0, nsm = 0, occ_j = 0, occ_m = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_j, k_solve_persistent<double, PC_JACOBI>, kPThreads, 0));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_solve_persistent<double, PC_MG>, kPThreads, 0));
+    const int per_sm = std::min(2, std::min(occ_j, occ_m));
+    if (per_sm < 1) return bail(fail(PCFD_E_CUDA, "persistent solve: no CTA fits an SM"));
+    s->persistent = nsm * per_sm;
+    if ((rc = dalloc(s, &s->pbar, 64)) || (rc = dalloc(s, &s->ppart, (size_t)s->persistent * 2 * kPMaxNV)))
+      return bail(rc);
   }
   if (s->precision == PCFD_MIXED) {
     if ((rc = dalloc(s, &s->r32, n)) || (rc = dalloc(s, &s->x32, n)) || (rc = dalloc(s, &s->pa32, n)) ||
@@ -1474,8 +1601,28 @@ int pycfd_step_host(pycfd_solver* s, const double* u0h, const double* v0h, doubl
 
 long long pycfd_launch_count(void) { return g_launches.load(); }
 
+int pycfd_solve_trace(pycfd_solver* s, int enable, unsigned long long* out, int cap, void* stream) {
+  if (!s || (out && cap < 1)) return fail(PCFD_E_ARG, "bad arguments");
+  if (!s->persistent) return fail(PCFD_E_UNSUPPORTED, "the solver does not run persistent solves");
+  if (enable == 1 && !s->ptrace) TRY(dalloc(s, &s->ptrace, (size_t)kPTraceCap));
+  if (enable == 0 || enable == 1) s->trace_on = enable;
+  if (out) {
+    if (!s->ptrace) return fail(PCFD_E_ARG, "no trace recorded");
+    CU(cudaStreamSynchronize(st(stream)));
+    CU(cudaMemcpy(out, s->ptrace, sizeof(unsigned long long) * (size_t)std::min(cap, kPTraceCap),
+                  cudaMemcpyDeviceToHost));
+  }
+  return 0;
+}
+
+int pycfd_solver_persistent(pycfd_solver* s, int* ctas) {
+  if (!s || !ctas) return fail(PCFD_E_ARG, "bad arguments");
+  *ctas = s->persistent;
+  return 0;
+}
+
 int pycfd_profile_kernel(pycfd_solver* s, int kernel_id) {
-  if (!s || kernel_id < 0 || kernel_id > 7) return fail(PCFD_E_ARG, "bad arguments");
+  if (!s || kernel_id < 0 || kernel_id > 8) return fail(PCFD_E_ARG, "bad arguments");
   s->prof_id = kernel_id;
   s->prof_n = 0;
   return 0;

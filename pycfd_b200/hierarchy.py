@@ -95,6 +95,7 @@ class MgLevelHost:
     A: sp.csr_matrix
     P: sp.csr_matrix | None = None
     arrays: list = field(default_factory=list)   # keeps ctypes-backed buffers alive
+    tails: dict = field(default_factory=dict)    # dense cycle operators from this level, by sweeps
 
 
 def _rho(A, dinv):
@@ -192,6 +193,59 @@ def coarsest_pseudo_inverse(level: MgLevelHost, singular: bool) -> np.ndarray:
     if singular and act.any():
         X[act, :] -= X[act, :].mean(axis=0)
     return np.ascontiguousarray(X)
+
+
+# Levels of at most this many rows may close the V-cycle as one dense operator.
+TAIL_MAX_ROWS = 2048
+
+
+def tail_level(levels) -> int:
+    """First level above the coarsest (index >= 1) with at most TAIL_MAX_ROWS rows, or 0."""
+    for l in range(1, len(levels) - 1):
+        if levels[l].n <= TAIL_MAX_ROWS:
+            return l
+    return 0
+
+
+def tail_operator(levels, cinv: np.ndarray, t: int, sweeps: int) -> np.ndarray:
+    """Dense matrix of the V-cycle from level ``t`` down, as a map of its right-hand side.
+
+    From a zero start the part of the cycle at and below a level -- damped-
+    Jacobi sweeps, restriction, the coarser levels, the coarsest pseudo-inverse,
+    prolongation and the sweeps back up (``pycfd/core/multigrid.py:430-474``) --
+    is linear in that level's right-hand side b, so it equals one matrix M with
+    x = M b.  M is built here by running those steps on the identity (columns
+    of b at once); the device then replaces the phases below ``t`` by one mat-
+    vec.  Row-major, ``n_t x n_t``.
+    """
+    def cycle(l, B):
+        lv = levels[l]
+        W = np.asarray(lv.weighted_dinv)[:, None]
+        A = lv.A
+        x = W * B
+        for _ in range(1, sweeps):
+            x = x + W * (B - A @ x)
+        res = B - A @ x
+        nxt = levels[l + 1]
+        bc = nxt.P.T @ res
+        xc = cinv @ bc if l + 1 == len(levels) - 1 else cycle(l + 1, bc)
+        x = x + nxt.P @ xc
+        for _ in range(sweeps):
+            x = x + W * (B - A @ x)
+        return x
+    return np.ascontiguousarray(cycle(t, np.eye(levels[t].n)))
+
+
+def tail_for(levels, cinv: np.ndarray, sweeps: int):
+    """``(level, operator)`` closing the V-cycle of this hierarchy, or ``(0, None)``;
+    built once per hierarchy and sweep count."""
+    t = tail_level(levels)
+    if t == 0:
+        return 0, None
+    ops = levels[t].tails
+    if sweeps not in ops:
+        ops[sweeps] = tail_operator(levels, cinv, t, sweeps)
+    return t, ops[sweeps]
 
 
 _CACHE: dict = {}

@@ -20,7 +20,7 @@ from . import _lib
 from .config import (AdvectionScheme, BCKind, PressureSolver, SimulationConfig, SolverType,
                      TimeScheme, WALLS)
 from .fields import FlowField
-from .hierarchy import assemble, hierarchy_for
+from .hierarchy import assemble, hierarchy_for, tail_for
 from .mesh import StructuredMesh
 
 
@@ -45,6 +45,15 @@ class GpuOptions:
     #: let each step kernel be scheduled while its predecessor runs
     #: (programmatic dependent launch); False keeps plain stream order.
     programmatic_launch: bool = True
+    #: CG and MG-PCG solves (FP64) as one cooperative launch whose phases are
+    #: separated by grid barriers; False launches one kernel per phase.  The
+    #: launch fills the GPU, so solvers stepped concurrently on several streams
+    #: use the per-phase form.
+    persistent_solve: bool = False
+    #: MG-PCG: apply the V-cycle at and below the first level of at most 2048
+    #: rows as one precomputed dense operator (the same linear map, so the same
+    #: preconditioner up to rounding) instead of level by level.
+    coarse_tail: bool = True
 
 
 def _torch():
@@ -152,6 +161,7 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     d.inner_tol = options.inner_tol
     d.coarse_cluster_rows = int(options.coarse_cluster_rows)
     d.sequential_launch = 0 if options.programmatic_launch else 1
+    d.persistent_solve = 1 if options.persistent_solve else 0
     if levels is not None:
         arr = (_lib.MgLevel * len(levels))()
         for l, lv in enumerate(levels):
@@ -188,10 +198,17 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
         d.levels = arr
         d.coarsest_inverse = _lib.cast(cinv, C.c_double)
         keep.append(arr)
+        tl, top = (0, None)
+        if options.coarse_tail and kind is PressureSolver.MGCG:
+            tl, top = tail_for(levels, cinv, cfg.mg_sweeps)
+        d.tail_level = tl
+        d.tail_operator = _lib.cast(top, C.c_double)
     else:
         d.n_levels = 0
         d.levels = C.cast(C.c_void_p(0), C.POINTER(_lib.MgLevel))
         d.coarsest_inverse = _lib.cast(None, C.c_double)
+        d.tail_level = 0
+        d.tail_operator = _lib.cast(None, C.c_double)
     return d, keep
 
 
@@ -336,6 +353,10 @@ class ProjectionSolver:
         _lib.check(self._L.pycfd_solver_create(C.byref(d), C.byref(h)))
         self._h = h
         del keep
+        ctas = C.c_int()
+        _lib.check(self._L.pycfd_solver_persistent(h, C.byref(ctas)))
+        #: CTAs of the cooperative launch of each CG / MG-PCG solve (0: per-phase kernels)
+        self._persistent = int(ctas.value)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -23,14 +23,14 @@ def _cavities():
 
 def test_batch_matches_individual_time_loops_bitwise():
     from pycfd_b200.batch import BatchRunner
-    from pycfd_b200.solver import ProjectionSolver
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
     from pycfd_b200.timestepper import TimeStepper
     cfgs = _cavities()
-    batch = BatchRunner(cfgs, streams=3)
+    batch = BatchRunner(cfgs, streams=3)   # concurrent streams: one kernel per solve phase
     batch.step(12)
     rep = batch.report()
     for k, cfg in enumerate(cfgs):
-        s = ProjectionSolver(cfg)
+        s = ProjectionSolver(cfg, options=GpuOptions(persistent_solve=False))
         res = TimeStepper(s).run(s.initialize(), max_steps=12)
         ua, va, pa = batch.fields[k].numpy()
         ub, vb, pb = res.fields.numpy()
