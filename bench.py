@@ -606,7 +606,7 @@ def run_ours(args, world, rank, local):
     from pycfd_b200.mesh import StructuredMesh
     cfg = tgv_config()
     opts = GpuOptions(precision=args.precision, graphs=not args.eager, persistent_solve=args.persistent,
-                      coarse_tail=not args.no_tail)
+                      coarse_tail=not args.no_tail, ell_thread_budget=args.ell_budget)
     solver = ProjectionSolver(cfg, options=opts)
     f = solver.initialize(*tgv_init(solver.mesh))
     dt = cfg.dt
@@ -697,6 +697,8 @@ def main():
     ap.add_argument("--eager", action="store_true", help="launch kernels one by one (no CUDA graph)")
     ap.add_argument("--persistent", action="store_true",
                     help="tgv512: each CG solve as one cooperative launch (phases between grid barriers)")
+    ap.add_argument("--ell-budget", type=int, default=0,
+                    help="tgv512: resident threads per coarse-level pass (0 default, -1 storage lanes)")
     ap.add_argument("--no-tail", action="store_true",
                     help="tgv512: V-cycle level by level down to the coarsest (no dense tail operator)")
     ap.add_argument("--workload", default="tgv512",

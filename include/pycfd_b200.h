@@ -80,6 +80,12 @@ typedef struct {
     const int64_t* p_indptr;     /* CSR of P_l (l >= 1)                      */
     const int32_t* p_indices;
     const double* p_data;
+    const int64_t* m_indptr;     /* optional, 1 <= l <= tail level: CSR of the
+                                    fused restriction R_l (I - A_{l-1} W_{l-1})
+                                    (n_l x n_{l-1}; one sweep from zero and the
+                                    restriction of its residual in one pass) */
+    const int32_t* m_indices;
+    const double* m_data;
 } pycfd_mg_level;
 
 typedef struct {
@@ -121,6 +127,10 @@ typedef struct {
                                                  sweeps back) is applied as one dense
                                                  operator; 0 = level by level      */
     const double* tail_operator;              /* n_l x n_l row-major, x_l = M b_l   */
+    int ell_thread_budget;                    /* resident threads one coarse-level pass
+                                                 may spread its rows over (lanes per row
+                                                 follow from it); 0 = 5 blocks of 256 per
+                                                 SM, -1 = the storage lane count   */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */

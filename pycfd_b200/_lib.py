@@ -42,7 +42,9 @@ class MgLevel(C.Structure):
                 ("weight", C.c_double), ("weighted_dinv", _dp), ("active", _u8p),
                 ("a_indptr", C.POINTER(C.c_int64)), ("a_indices", C.POINTER(C.c_int32)),
                 ("a_data", _dp), ("p_indptr", C.POINTER(C.c_int64)),
-                ("p_indices", C.POINTER(C.c_int32)), ("p_data", _dp)]
+                ("p_indices", C.POINTER(C.c_int32)), ("p_data", _dp),
+                ("m_indptr", C.POINTER(C.c_int64)), ("m_indices", C.POINTER(C.c_int32)),
+                ("m_data", _dp)]
 
 
 class SolverDesc(C.Structure):
@@ -56,7 +58,8 @@ class SolverDesc(C.Structure):
                 ("inner_tol", C.c_double), ("n_levels", C.c_int),
                 ("levels", C.POINTER(MgLevel)), ("coarsest_inverse", _dp),
                 ("coarse_cluster_rows", C.c_int), ("sequential_launch", C.c_int),
-                ("persistent_solve", C.c_int), ("tail_level", C.c_int), ("tail_operator", _dp)]
+                ("persistent_solve", C.c_int), ("tail_level", C.c_int), ("tail_operator", _dp),
+                ("ell_thread_budget", C.c_int)]
 
 
 class DtControl(C.Structure):

@@ -125,15 +125,7 @@ __device__ __forceinline__ void b_reduce(double (&v)[NV], double* partials, unsi
   if (last) {
     __threadfence();
     double acc[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
-    for (int b = tid; b < ntiles; b += nthr) {
-#pragma unroll
-      for (int k = 0; k < NV; ++k) {
-        const double p = ((volatile double*)partials)[(long)b * NV + k];
-        acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], p) : acc[k] + p;
-      }
-    }
+    sum_partials<NV, MAXMASK>(partials, ntiles, tid, nthr, acc);
     block_reduce<NV, MAXMASK>(acc);
     if (tid == 0) {
       fin(acc);

@@ -110,6 +110,34 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV]) {
   __syncthreads();
 }
 
+// The last block's pass over every block's NV partials (row b at b*NV): L2
+// loads (ld.global.cg, coherent with the other blocks' fenced writes), several
+// blocks' rows in flight per thread; each thread adds its rows in block order,
+// so the totals are those of a plain strided loop.
+template <int NV, unsigned MAXMASK = 0u>
+__device__ __forceinline__ void sum_partials(const double* __restrict__ partials, int n, int tid, int nthr,
+                                             double (&acc)[NV]) {
+  constexpr int U = NV <= 2 ? 4 : (NV <= 4 ? 2 : 1);
+#pragma unroll
+  for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
+  for (int b0 = tid; b0 < n; b0 += U * nthr) {
+    double p[U][NV];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int b = b0 + u * nthr;
+#pragma unroll
+      for (int k = 0; k < NV; ++k) p[u][k] = b < n ? __ldcg(partials + (long)b * NV + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (b0 + u * nthr < n) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], p[u][k]) : acc[k] + p[u][k];
+      }
+    }
+  }
+}
+
 // Grid-wide reduction.  Every block contributes NV values; the last block to
 // arrive (ticket counter) combines the partials in block order and calls
 // fin(totals) on its thread 0.  Returns true in that thread.
@@ -132,15 +160,7 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin)
   if (!last) return;
   __threadfence();
   double acc[NV];
-#pragma unroll
-  for (int k = 0; k < NV; ++k) acc[k] = ((MAXMASK >> k) & 1u) ? -INFINITY : 0.0;
-  for (int b = tid; b < nblk; b += nthr) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double p = ((volatile double*)rb.partials)[b * NV + k];
-      acc[k] = ((MAXMASK >> k) & 1u) ? fmax(acc[k], p) : acc[k] + p;
-    }
-  }
+  sum_partials<NV, MAXMASK>(rb.partials, nblk, tid, nthr, acc);
   block_reduce<NV, MAXMASK>(acc);
   if (tid == 0) {
     fin(acc);

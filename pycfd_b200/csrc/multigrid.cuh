@@ -25,51 +25,88 @@ struct Ell {
   int rowmajor;   // 1: [row*K + k], 0: [k*n + row]
 };
 
-// Row dot product by L lanes.  Every lane of the warp must call this (the
-// lane shuffle uses the full mask); rows past the end contribute nothing.
+// Per-phase ELL passes (blockDim 256).  A row's entries are split over L
+// lanes -- L <= 32: a group within a warp, combined by shuffles; L > 32: L/32
+// warps, their sums combined in shared memory in warp order.  A lane gathers
+// its entries kEllGather at a time (indices and values, then the vector
+// values, then the products added in entry order), so several gathers are in
+// flight.  Rows past the end contribute nothing; every thread of a block runs
+// the same rounds (the shuffles and the block barrier need them all).
+constexpr int kEllGather = 4;
+
 template <int L, class T, class X>
-__device__ __forceinline__ double ell_row(const Ell<T>& E, int row, int lane, X x) {
+__device__ __forceinline__ double ell_lane_sum(const Ell<T>& E, int row, int lane, X x) {
   double acc = 0.0;
-  if (row >= E.n) {
-  } else if (E.rowmajor) {
-    const long base = (long)row * E.K;
-    for (int k = lane; k < E.K; k += L) {
-      const T a = E.val[base + k];
-      acc += (double)a * x(E.col[base + k]);
-    }
-  } else {
-    for (int k = lane; k < E.K; k += L) {
-      const long e = (long)k * E.n + row;
-      acc += (double)E.val[e] * x(E.col[e]);
-    }
-  }
+  if (row >= E.n) return acc;
+  for (int k0 = lane; k0 < E.K; k0 += kEllGather * L) {
+    int cc[kEllGather];
+    T vv[kEllGather];
 #pragma unroll
-  for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
+    for (int u = 0; u < kEllGather; ++u) {
+      const int k = k0 + u * L;
+      cc[u] = 0;
+      vv[u] = (T)0;
+      if (k < E.K) {
+        const long e = E.rowmajor ? (long)row * E.K + k : (long)k * E.n + row;
+        cc[u] = __ldg(E.col + e);
+        vv[u] = __ldg(E.val + e);
+      }
+    }
+    double xx[kEllGather];
+#pragma unroll
+    for (int u = 0; u < kEllGather; ++u) xx[u] = (k0 + u * L < E.K) ? x(cc[u]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < kEllGather; ++u)
+      if (k0 + u * L < E.K) acc += (double)vv[u] * xx[u];
+  }
   return acc;
 }
 
-// Rows of an ELL pass, L lanes each, grid-stride over one wave of blocks.
-// A warp's row groups share `base`, so every lane of a warp runs the same
-// number of rounds (the lane shuffle needs them all).
-#define FOR_ELL_ROWS(E, L)                                                                   \
-  const int lane = (int)(threadIdx.x % (L));                                                 \
-  const int per = (int)(gridDim.x * blockDim.x / (L));                                       \
-  for (int base = (int)(blockIdx.x * blockDim.x / (L)); base < (E).n; base += per)            \
-    for (int row = base + (int)(threadIdx.x / (L)), once_ = 1; once_; once_ = 0)
+template <int L, class T, class X, class W>
+__device__ __forceinline__ void ell_pass(const Ell<T>& E, X x, W write) {
+  static_assert(L >= 1 && L <= 256 && (L & (L - 1)) == 0, "lanes per row: a power of two up to 256");
+  if constexpr (L <= 32) {
+    const int lane = (int)(threadIdx.x % L);
+    const int per = (int)(gridDim.x * blockDim.x / L);
+    for (int base = (int)(blockIdx.x * blockDim.x / L); base < E.n; base += per) {
+      const int row = base + (int)(threadIdx.x / L);
+      double acc = ell_lane_sum<L>(E, row, lane, x);
+#pragma unroll
+      for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
+      if (lane == 0 && row < E.n) write(row, acc);
+    }
+  } else {
+    constexpr int kW = L / 32;              // warps per row
+    constexpr int kRows = 256 / L;          // rows per block and round
+    __shared__ double part[8];
+    const int warp = (int)(threadIdx.x >> 5), wl = (int)(threadIdx.x & 31);
+    const int lane = (int)(threadIdx.x % L), rloc = (int)(threadIdx.x / L);
+    for (int base = (int)blockIdx.x * kRows; base < E.n; base += (int)gridDim.x * kRows) {
+      const int row = base + rloc;
+      const double acc = warp_sum(ell_lane_sum<L>(E, row, lane, x));
+      if (wl == 0) part[warp] = acc;
+      __syncthreads();
+      if (lane == 0 && row < E.n) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kW; ++w) t += part[warp + w];
+        write(row, t);
+      }
+      __syncthreads();
+    }
+  }
+}
 
 // x = wd*b; res = b - A(wd*b)          (first sweep from zero + residual)
 template <int L, class T>
 __global__ void k_ell_pre(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                           T* __restrict__ x, T* __restrict__ res) {
   pdl_begin();
-  FOR_ELL_ROWS(A, L) {
-    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)wd[c] * (double)b[c]; });
-    if (lane == 0 && row < A.n) {
-      const double bx = (double)b[row];
-      x[row] = (T)((double)wd[row] * bx);
-      res[row] = (T)(bx - s);
-    }
-  }
+  ell_pass<L>(A, [&](int c) { return (double)wd[c] * (double)b[c]; }, [&](int row, double s) {
+    const double bx = (double)b[row];
+    x[row] = (T)((double)wd[row] * bx);
+    res[row] = (T)(bx - s);
+  });
 }
 
 // xo = x + wd*(b - A x)
@@ -77,10 +114,9 @@ template <int L, class T>
 __global__ void k_ell_smooth(Ell<T> A, const T* __restrict__ wd, const T* __restrict__ b,
                              const T* __restrict__ x, T* __restrict__ xo) {
   pdl_begin();
-  FOR_ELL_ROWS(A, L) {
-    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
-    if (lane == 0 && row < A.n) xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
-  }
+  ell_pass<L>(A, [&](int c) { return (double)x[c]; }, [&](int row, double s) {
+    xo[row] = (T)((double)x[row] + (double)wd[row] * ((double)b[row] - s));
+  });
 }
 
 // res = b - A x
@@ -88,20 +124,16 @@ template <int L, class T>
 __global__ void k_ell_resid(Ell<T> A, const T* __restrict__ b, const T* __restrict__ x,
                             T* __restrict__ res) {
   pdl_begin();
-  FOR_ELL_ROWS(A, L) {
-    const double s = ell_row<L>(A, row, lane, [&](int c) { return (double)x[c]; });
-    if (lane == 0 && row < A.n) res[row] = (T)((double)b[row] - s);
-  }
+  ell_pass<L>(A, [&](int c) { return (double)x[c]; },
+              [&](int row, double s) { res[row] = (T)((double)b[row] - s); });
 }
 
 // y = M x (restriction with M = R), or y += M x (prolongation with M = P).
 template <int L, bool ADD, class T>
 __global__ void k_ell_spmv(Ell<T> M, const T* __restrict__ x, T* __restrict__ y) {
   pdl_begin();
-  FOR_ELL_ROWS(M, L) {
-    const double s = ell_row<L>(M, row, lane, [&](int c) { return (double)x[c]; });
-    if (lane == 0 && row < M.n) y[row] = ADD ? (T)((double)y[row] + s) : (T)s;
-  }
+  ell_pass<L>(M, [&](int c) { return (double)x[c]; },
+              [&](int row, double s) { y[row] = ADD ? (T)((double)y[row] + s) : (T)s; });
 }
 
 // Coarsest level: x = C b with C the precomputed pseudo-inverse (pinned LU
@@ -236,6 +268,41 @@ struct BStored {
 
 __device__ __forceinline__ double fine_wdinv(uint8_t f, int i, int j, const Geo& g, double w) {
   return w * (1.0 / fine_diag(f, i, j, g));
+}
+
+// ---- fused down sweep (one sweep per level, from zero) ------------------------
+// b_l = M_l b_{l-1} with M_l = R_l (I - A_{l-1} W_{l-1}): the first sweep on
+// level l-1 and the restriction of its residual in one pass.  From level 0 the
+// right-hand side is the projected CG residual (bf).
+template <int L, class T, class B>
+__global__ void k_ell_fused_restrict0(Ell<T> M, B bf, T* __restrict__ y) {
+  pdl_begin();
+  bf.load();
+  ell_pass<L>(M, [&](int c) { return bf(c); }, [&](int row, double s) { y[row] = (T)s; });
+}
+
+// Up sweep after a fused down sweep: the level's first-sweep iterate W b was
+// not stored, so the prolongation forms it on the fly -- x = (T)(W b), then
+// x + P x_c, the same two roundings as the stored form.
+template <int L, class T>
+__global__ void k_ell_prolong_wb(Ell<T> P, const T* __restrict__ wd, const T* __restrict__ b,
+                                 const T* __restrict__ xc, T* __restrict__ xf) {
+  pdl_begin();
+  ell_pass<L>(P, [&](int c) { return (double)xc[c]; }, [&](int row, double s) {
+    xf[row] = (T)((double)(T)((double)wd[row] * (double)b[row]) + s);
+  });
+}
+
+// The same onto level 0, whose W b is fine_wdinv * (projected residual).
+template <int L, class T, class B>
+__global__ void k_ell_prolong0_wb(Ell<T> P, B bf, const uint8_t* __restrict__ flags, Geo g, double w,
+                                  const T* __restrict__ xc, T* __restrict__ xf) {
+  pdl_begin();
+  bf.load();
+  ell_pass<L>(P, [&](int c) { return (double)xc[c]; }, [&](int row, double s) {
+    const int i = row / g.ny, j = row - i * g.ny;
+    xf[row] = (T)((double)(T)(fine_wdinv(flags[row], i, j, g, w) * bf(row)) + s);
+  });
 }
 
 // x = wd*b and res = b - A(wd*b) on level 0.

@@ -197,7 +197,7 @@ __device__ __forceinline__ double p_apply(const double* dtab, uint8_t f, int i, 
 // One ELL pass over all rows, L lanes per row, every thread the same number
 // of rounds.  A lane's entries are gathered four at a time -- indices and
 // values first, then the vector values, then the products added in entry
-// order -- so the sums are those of ell_row while four gathers are in flight.
+// order -- so the sums are those of a lane's plain loop with four gathers in flight.
 constexpr int kPGather = 4;
 template <class T, class X, class W>
 __device__ __forceinline__ void p_ell(const Ell<T>& E, int L, int gtid, int nthr, X x, W write) {

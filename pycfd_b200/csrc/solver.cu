@@ -62,6 +62,7 @@ struct DevEll {
   int* col = nullptr;
   T* val = nullptr;
   int n = 0, K = 0, rowmajor = 0, lanes = 1;
+  int xl = 1;   // lanes per row of the per-phase kernels (1 with the column-major layout)
   Ell<T> view() const { return Ell<T>{col, val, n, K, rowmajor}; }
 };
 
@@ -75,6 +76,8 @@ struct Level {
   double weight = 1.0;
   DevEll<double> A, P, R;   // P: rows of the finer level; R = P^T: rows of this level
   DevEll<float> Af, Pf, Rf;
+  DevEll<double> M;          // fused restriction R (I - A W) from the finer level (optional)
+  DevEll<float> Mf;
   double* wd = nullptr;
   float* wdf = nullptr;
   LevelBuf<double> d;
@@ -87,6 +90,19 @@ int choose_lanes(int K) {
   if (K <= 96) return 8;
   if (K <= 200) return 16;
   return 32;
+}
+
+// Lanes per row of the per-phase ELL kernels (row-major layouts; the column-
+// major one is read by one lane per row): about four entries per lane -- one
+// round of gathers -- up to eight warps per row, but no more lanes than keep
+// all rows x lanes within `budget` resident threads, so a pass is one round.
+// budget < 0: the storage lane count.
+int exec_lanes(int K, int rowmajor, int lanes, int n, long budget) {
+  if (!rowmajor) return 1;
+  if (budget < 0) return lanes;
+  int L = 2;
+  while (L < 256 && L * 4 < K && (long)n * L * 2 <= budget) L <<= 1;
+  return L;
 }
 
 }  // namespace
@@ -128,6 +144,9 @@ struct pycfd_solver {
   float* Cf = nullptr;
   int nc = 0;
   int tail_level = 0;           // level whose cycle is one dense operator (0: none)
+  int fused = 0;                // down sweep by fused restrictions onto levels 1..tail_level
+  long ell_budget = 0;          // resident threads a per-phase ELL pass may use (< 0: storage lanes)
+  int ell_blocks = kWaveBlocks; // grid cap of the per-phase ELL kernels
   double* tail = nullptr;
   float* tailf = nullptr;
   int last_ir = 0;
@@ -219,6 +238,7 @@ int make_ell(pycfd_solver* s, DevEll<T>* E, int n, const int64_t* indptr, const 
   E->K = Kp;
   E->rowmajor = rowmajor;
   E->lanes = L;
+  E->xl = exec_lanes(Kp, rowmajor, L, n, s->ell_budget);
   return 0;
 }
 
@@ -288,16 +308,22 @@ int launch_boundary(pycfd_solver* s, double* u, double* v, std::initializer_list
 int grid1(pycfd_solver* s) { return grid_for(s->ncell(), kRedThreads, kMaxRedBlocks); }
 
 // Generic dispatcher over the lane count of an ELL block.
-#define ELL_DISPATCH(LANES, CALL)                 \
-  switch (LANES) {                                \
-    case 1: { constexpr int L = 1; CALL; } break;  \
-    case 4: { constexpr int L = 4; CALL; } break;  \
-    case 8: { constexpr int L = 8; CALL; } break;  \
-    case 16: { constexpr int L = 16; CALL; } break; \
-    default: { constexpr int L = 32; CALL; } break; \
+#define ELL_DISPATCH(LANES, CALL)                   \
+  switch (LANES) {                                  \
+    case 1: { constexpr int L = 1; CALL; } break;    \
+    case 2: { constexpr int L = 2; CALL; } break;    \
+    case 4: { constexpr int L = 4; CALL; } break;    \
+    case 8: { constexpr int L = 8; CALL; } break;    \
+    case 16: { constexpr int L = 16; CALL; } break;  \
+    case 32: { constexpr int L = 32; CALL; } break;  \
+    case 64: { constexpr int L = 64; CALL; } break;  \
+    case 128: { constexpr int L = 128; CALL; } break; \
+    default: { constexpr int L = 256; CALL; } break;  \
   }
 
-inline int ell_grid(int n, int L) { return (int)std::min<long>(((long)n * L + 255) / 256, kWaveBlocks); }
+inline int ell_grid(const pycfd_solver* s, int n, int L) {
+  return (int)std::min<long>(((long)n * L + 255) / 256, s->ell_blocks);
+}
 
 template <class T>
 const DevEll<T>& lvA(const Level& l);
@@ -329,6 +355,12 @@ template <>
 double* lvWd<double>(Level& l) { return l.wd; }
 template <>
 float* lvWd<float>(Level& l) { return l.wdf; }
+template <class T>
+const DevEll<T>& lvM(const Level& l);
+template <>
+const DevEll<double>& lvM<double>(const Level& l) { return l.M; }
+template <>
+const DevEll<float>& lvM<float>(const Level& l) { return l.Mf; }
 template <class T>
 const T* tailM(pycfd_solver* s);
 template <>
@@ -421,6 +453,51 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     return 0;
   }
   const double w0 = s->lv[0].weight;
+  if (s->fused && sw == 1 && s->tail_level > 0 && s->tail_level < std::min(s->cluster_from, Lv)) {
+    // ---- down: b_l = M_l b_{l-1} (first sweep + restriction in one pass), then the tail
+    const int tl = s->tail_level;
+    {
+      const DevEll<T>& M = lvM<T>(s->lv[1]);
+      ELL_DISPATCH(M.xl, (pdl_launch(s, k_ell_fused_restrict0<L, T, BFromRS<T>>, ell_grid(s, M.n, L), 256, 0, stream,
+                                        M.view(), bf0, lvB<T>(s->lv[1]).b)));
+      CHECK_LAUNCH();
+    }
+    for (int l = 2; l <= tl; ++l) {
+      const DevEll<T>& M = lvM<T>(s->lv[l]);
+      ELL_DISPATCH(M.xl, (pdl_launch(s, k_ell_spmv<L, false, T>, ell_grid(s, M.n, L), 256, 0, stream, M.view(),
+                                        (const T*)lvB<T>(s->lv[l - 1]).b, lvB<T>(s->lv[l]).b)));
+      CHECK_LAUNCH();
+    }
+    LevelBuf<T>& Bt = lvB<T>(s->lv[tl]);
+    pdl_launch(s, k_tail<T>, (s->lv[tl].n + kTailRowsPerBlock - 1) / kTailRowsPerBlock, 256, 0, stream, tailM<T>(s),
+               s->lv[tl].n, (const T*)Bt.b, Bt.xa);
+    CHECK_LAUNCH();
+    // ---- up: x_l = (T)(W b_l) + P x_{l+1}, one sweep
+    const T* xc = Bt.xa;
+    for (int l = tl - 1; l >= 1; --l) {
+      Level& Lf = s->lv[l];
+      LevelBuf<T>& Bf = lvB<T>(Lf);
+      const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
+      ELL_DISPATCH(P.xl, (pdl_launch(s, k_ell_prolong_wb<L, T>, ell_grid(s, P.n, L), 256, 0, stream, P.view(),
+                                        (const T*)lvWd<T>(Lf), (const T*)Bf.b, xc, Bf.xa)));
+      CHECK_LAUNCH();
+      const DevEll<T>& A = lvA<T>(Lf);
+      ELL_DISPATCH(A.xl, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(s, A.n, L), 256, 0, stream, A.view(),
+                                        (const T*)lvWd<T>(Lf), (const T*)Bf.b, (const T*)Bf.xa, Bf.xb)));
+      CHECK_LAUNCH();
+      xc = Bf.xb;
+    }
+    const DevEll<T>& P1 = lvP<T>(s->lv[1]);
+    ELL_DISPATCH(P1.xl, (pdl_launch(s, k_ell_prolong0_wb<L, T, BFromRS<T>>, ell_grid(s, P1.n, L), 256, 0, stream,
+                                       P1.view(), bf0, s->flags, g, w0, xc, B0.xa)));
+    CHECK_LAUNCH();
+    prof_mark(s, 2, stream);
+    pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0,
+               (const T*)B0.xa, z_out, r, s->singular, s->S, s->rb());
+    prof_mark(s, 2, stream);
+    CHECK_LAUNCH();
+    return 0;
+  }
   // ---- down ----
   T* cur[32];
   if (sw == 1) {
@@ -463,7 +540,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
       cur[l] = Bc.xa;
       break;
     }
-    ELL_DISPATCH(R.lanes, (pdl_launch(s, k_ell_spmv<L, false, T>, ell_grid(R.n, L), 256, 0, stream, R.view(), res_f, Bc.b)));
+    ELL_DISPATCH(R.xl, (pdl_launch(s, k_ell_spmv<L, false, T>, ell_grid(s, R.n, L), 256, 0, stream, R.view(), res_f, Bc.b)));
     CHECK_LAUNCH();
     if (l == s->tail_level) {   // the cycle at and below l as one dense operator
       pdl_launch(s, k_tail<T>, (Lc.n + kTailRowsPerBlock - 1) / kTailRowsPerBlock, 256, 0, stream, tailM<T>(s), Lc.n,
@@ -475,17 +552,17 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     }
     const DevEll<T>& A = lvA<T>(Lc);
     T* wd = lvWd<T>(Lc);
-    ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_pre<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bc.b, Bc.xa, Bc.res)));
+    ELL_DISPATCH(A.xl, (pdl_launch(s, k_ell_pre<L, T>, ell_grid(s, A.n, L), 256, 0, stream, A.view(), wd, Bc.b, Bc.xa, Bc.res)));
     CHECK_LAUNCH();
     T* a = Bc.xa;
     T* bb = Bc.xb;
     if (sw > 1) {
       for (int k = 1; k < sw; ++k) {
-        ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bc.b, a, bb)));
+        ELL_DISPATCH(A.xl, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(s, A.n, L), 256, 0, stream, A.view(), wd, Bc.b, a, bb)));
         CHECK_LAUNCH();
         std::swap(a, bb);
       }
-      ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_resid<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), Bc.b, a, Bc.res)));
+      ELL_DISPATCH(A.xl, (pdl_launch(s, k_ell_resid<L, T>, ell_grid(s, A.n, L), 256, 0, stream, A.view(), Bc.b, a, Bc.res)));
       CHECK_LAUNCH();
     }
     cur[l] = a;
@@ -496,7 +573,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     LevelBuf<T>& Bf = lvB<T>(Lf);
     const DevEll<T>& P = lvP<T>(s->lv[l + 1]);
     T* xf = cur[l];
-    ELL_DISPATCH(P.lanes, (pdl_launch(s, k_ell_spmv<L, true, T>, ell_grid(P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
+    ELL_DISPATCH(P.xl, (pdl_launch(s, k_ell_spmv<L, true, T>, ell_grid(s, P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
     CHECK_LAUNCH();
     T* other = (xf == Bf.xa) ? Bf.xb : Bf.xa;
     for (int k = 1; k <= sw; ++k) {
@@ -518,7 +595,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
       } else {
         const DevEll<T>& A = lvA<T>(Lf);
         T* wd = lvWd<T>(Lf);
-        ELL_DISPATCH(A.lanes, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(A.n, L), 256, 0, stream, A.view(), wd, Bf.b, xf, other)));
+        ELL_DISPATCH(A.xl, (pdl_launch(s, k_ell_smooth<L, T>, ell_grid(s, A.n, L), 256, 0, stream, A.view(), wd, Bf.b, xf, other)));
         CHECK_LAUNCH();
         std::swap(xf, other);
       }
@@ -560,7 +637,7 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   for (int l = 1; l < Lv; ++l) {
     Level& Lc = s->lv[l];
     const double* res_f = s->lv[l - 1].d.res;
-    ELL_DISPATCH(Lc.R.lanes, (pdl_launch(s, k_ell_spmv<L, false, double>, ell_grid(Lc.R.n, L), 256, 0, stream, Lc.R.view(), res_f, Lc.d.b)));
+    ELL_DISPATCH(Lc.R.xl, (pdl_launch(s, k_ell_spmv<L, false, double>, ell_grid(s, Lc.R.n, L), 256, 0, stream, Lc.R.view(), res_f, Lc.d.b)));
     CHECK_LAUNCH();
     if (l == Lv - 1) {
       pdl_launch(s, k_dense<double>, 1, 256, 0, stream, s->C, s->nc, Lc.d.b, Lc.d.xa);
@@ -568,17 +645,17 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
       cur[l] = Lc.d.xa;
       break;
     }
-    ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_pre<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, Lc.d.xa, Lc.d.res)));
+    ELL_DISPATCH(Lc.A.xl, (pdl_launch(s, k_ell_pre<L, double>, ell_grid(s, Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, Lc.d.xa, Lc.d.res)));
     CHECK_LAUNCH();
     double* p = Lc.d.xa;
     double* o = Lc.d.xb;
     if (sw > 1) {
       for (int k = 1; k < sw; ++k) {
-        ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, p, o)));
+        ELL_DISPATCH(Lc.A.xl, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(s, Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.wd, Lc.d.b, p, o)));
         CHECK_LAUNCH();
         std::swap(p, o);
       }
-      ELL_DISPATCH(Lc.A.lanes, (pdl_launch(s, k_ell_resid<L, double>, ell_grid(Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.d.b, p, Lc.d.res)));
+      ELL_DISPATCH(Lc.A.xl, (pdl_launch(s, k_ell_resid<L, double>, ell_grid(s, Lc.A.n, L), 256, 0, stream, Lc.A.view(), Lc.d.b, p, Lc.d.res)));
       CHECK_LAUNCH();
     }
     cur[l] = p;
@@ -587,7 +664,7 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
     Level& Lf = s->lv[l];
     const DevEll<double>& P = s->lv[l + 1].P;
     double* xf = cur[l];
-    ELL_DISPATCH(P.lanes, (pdl_launch(s, k_ell_spmv<L, true, double>, ell_grid(P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
+    ELL_DISPATCH(P.xl, (pdl_launch(s, k_ell_spmv<L, true, double>, ell_grid(s, P.n, L), 256, 0, stream, P.view(), cur[l + 1], xf)));
     CHECK_LAUNCH();
     if (l == 0) {
       double* o = (xf == x) ? s->xtmp : x;
@@ -605,7 +682,7 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
     } else {
       double* o = (xf == Lf.d.xa) ? Lf.d.xb : Lf.d.xa;
       for (int k = 1; k <= sw; ++k) {
-        ELL_DISPATCH(Lf.A.lanes, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(Lf.A.n, L), 256, 0, stream, Lf.A.view(), Lf.wd, Lf.d.b, xf, o)));
+        ELL_DISPATCH(Lf.A.xl, (pdl_launch(s, k_ell_smooth<L, double>, ell_grid(s, Lf.A.n, L), 256, 0, stream, Lf.A.view(), Lf.wd, Lf.d.b, xf, o)));
         CHECK_LAUNCH();
         std::swap(xf, o);
       }
@@ -1099,6 +1176,13 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->precision = d->precision;
   s->inner_tol = d->inner_tol > 0 ? d->inner_tol : 1e-4;
   s->pdl = d->sequential_launch ? 0 : 1;
+  {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // default: five resident 256-thread blocks per SM (the ELL kernels keep <= 48 registers)
+    s->ell_budget = d->ell_thread_budget ? (long)d->ell_thread_budget : (long)nsm * 5 * 256;
+    s->ell_blocks = s->ell_budget > 0 ? (int)std::max<long>(1, s->ell_budget / 256) : kWaveBlocks;
+  }
 
   // ---- cell flags of the fine operator (pycfd/core/pressure.py:209-247) ----
   const long n = (long)nx * ny;
@@ -1272,6 +1356,10 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
         if ((rc = make_ell(s, &L.R, L.n, tp.data(), ti.data(), td.data())) ||
             (rc = make_ell(s, &L.Rf, L.n, tp.data(), ti.data(), td.data())))
           return bail(rc);
+        if (in.m_indptr &&
+            ((rc = make_ell(s, &L.M, L.n, in.m_indptr, in.m_indices, in.m_data)) ||
+             (rc = make_ell(s, &L.Mf, L.n, in.m_indptr, in.m_indices, in.m_data))))
+          return bail(rc);
       }
     }
     const int ncs = d->levels[d->n_levels - 1].n;
@@ -1294,6 +1382,9 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
       if ((rc = upload(s, &s->tail, d->tail_operator, nt * nt)) || (rc = upload(s, &s->tailf, tf.data(), nt * nt)))
         return bail(rc);
       s->tail_level = tl;
+      s->fused = 1;
+      for (int l = 1; l <= tl; ++l)
+        if (!d->levels[l].m_indptr) s->fused = 0;
     }
   }
   if (mg && d->coarse_cluster_rows > 0 && s->lv.size() > 1) {

@@ -236,6 +236,18 @@ def tail_operator(levels, cinv: np.ndarray, t: int, sweeps: int) -> np.ndarray:
     return np.ascontiguousarray(cycle(t, np.eye(levels[t].n)))
 
 
+def fused_restriction(levels, l: int) -> sp.csr_matrix:
+    """``R_l (I - A_{l-1} W_{l-1})``: from a zero start, the first damped-Jacobi
+    sweep on level l-1 (x = W b) and the restriction of its residual b - A x
+    (``pycfd/core/multigrid.py:436-447``) are one linear map of b onto level l."""
+    f = levels[l - 1]
+    A = f.A.tocsr()
+    W = sp.diags(np.asarray(f.weighted_dinv))
+    M = (levels[l].P.T.tocsr() @ (sp.identity(A.shape[0], format="csr") - A @ W)).tocsr()
+    M.sort_indices()
+    return M
+
+
 def tail_for(levels, cinv: np.ndarray, sweeps: int):
     """``(level, operator)`` closing the V-cycle of this hierarchy, or ``(0, None)``;
     built once per hierarchy and sweep count."""
@@ -246,6 +258,17 @@ def tail_for(levels, cinv: np.ndarray, sweeps: int):
     if sweeps not in ops:
         ops[sweeps] = tail_operator(levels, cinv, t, sweeps)
     return t, ops[sweeps]
+
+
+def fused_for(levels, t: int):
+    """Fused restrictions onto levels 1..t (one sweep per level), built once."""
+    out = []
+    for l in range(1, t + 1):
+        ops = levels[l].tails
+        if "M" not in ops:
+            ops["M"] = fused_restriction(levels, l)
+        out.append(ops["M"])
+    return out
 
 
 _CACHE: dict = {}

@@ -20,7 +20,7 @@ from . import _lib
 from .config import (AdvectionScheme, BCKind, PressureSolver, SimulationConfig, SolverType,
                      TimeScheme, WALLS)
 from .fields import FlowField
-from .hierarchy import assemble, hierarchy_for, tail_for
+from .hierarchy import assemble, fused_for, hierarchy_for, tail_for
 from .mesh import StructuredMesh
 
 
@@ -40,7 +40,7 @@ class GpuOptions:
     graphs: bool = True
     #: multigrid levels with at most this many rows run inside one thread-block
     #: cluster per V-cycle (0, the default: one kernel per phase on every level;
-    #: the cluster form is bit-identical but slower while coarse stencils are wide).
+    #: the cluster form agrees to rounding but is slower while coarse stencils are wide).
     coarse_cluster_rows: int = 0
     #: let each step kernel be scheduled while its predecessor runs
     #: (programmatic dependent launch); False keeps plain stream order.
@@ -54,6 +54,15 @@ class GpuOptions:
     #: rows as one precomputed dense operator (the same linear map, so the same
     #: preconditioner up to rounding) instead of level by level.
     coarse_tail: bool = True
+    #: MG-PCG with a dense tail and one sweep per level: the first sweep of each
+    #: level above the tail and the restriction of its residual as one sparse
+    #: product R (I - A W) (the same map), so the down sweep takes one launch per
+    #: level.
+    fused_restriction: bool = True
+    #: resident threads a coarse-level pass may spread its rows over (lanes per
+    #: row follow from it); 0 = five 256-thread blocks per SM, -1 = the lane
+    #: count of the stored layout.
+    ell_thread_budget: int = 0
 
 
 def _torch():
@@ -162,6 +171,7 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     d.coarse_cluster_rows = int(options.coarse_cluster_rows)
     d.sequential_launch = 0 if options.programmatic_launch else 1
     d.persistent_solve = 1 if options.persistent_solve else 0
+    d.ell_thread_budget = int(options.ell_thread_budget)
     if levels is not None:
         arr = (_lib.MgLevel * len(levels))()
         for l, lv in enumerate(levels):
@@ -203,6 +213,15 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
             tl, top = tail_for(levels, cinv, cfg.mg_sweeps)
         d.tail_level = tl
         d.tail_operator = _lib.cast(top, C.c_double)
+        if tl and options.fused_restriction and cfg.mg_sweeps == 1:
+            for l, M in enumerate(fused_for(levels, tl), start=1):
+                mp = np.ascontiguousarray(M.indptr, np.int64)
+                mi = np.ascontiguousarray(M.indices, np.int32)
+                md = np.ascontiguousarray(M.data, np.float64)
+                keep += [mp, mi, md]
+                e = arr[l]
+                e.m_indptr, e.m_indices, e.m_data = (_lib.cast(mp, C.c_int64), _lib.cast(mi, C.c_int32),
+                                                     _lib.cast(md, C.c_double))
     else:
         d.n_levels = 0
         d.levels = C.cast(C.c_void_p(0), C.POINTER(_lib.MgLevel))

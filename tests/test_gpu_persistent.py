@@ -124,14 +124,16 @@ def test_persistent_solve_is_one_launch():
 @pytest.mark.parametrize("n,sweeps", [(64, 1), (256, 1), (256, 2)])
 def test_dense_tail_matches_level_by_level(n, sweeps, persistent):
     """The V-cycle closed by the dense operator of its tail (levels of at most 2048
-    rows down to the coarsest) against the level-by-level cycle."""
+    rows down to the coarsest), with and without the fused restrictions above it,
+    against the level-by-level cycle."""
     from pycfd_b200.hierarchy import tail_level
     from pycfd_b200.solver import GpuOptions, ProjectionSolver
     cfg = _cfg(dict(nx=n, ny=n, re=400.0, pressure_solver="mgcg", poisson_tol=1e-12, mg_sweeps=sweeps,
                     boundary_config=cases.bcs(top=("moving_wall", 1.0))))
     out, its = [], []
-    for tail in (True, False):
-        s = ProjectionSolver(cfg, options=GpuOptions(coarse_tail=tail, persistent_solve=persistent))
+    for tail, fused in ((True, True), (True, False), (False, False)):
+        s = ProjectionSolver(cfg, options=GpuOptions(coarse_tail=tail, fused_restriction=fused,
+                                                     persistent_solve=persistent))
         f = s.initialize()
         k = []
         for _ in range(5):
@@ -140,6 +142,7 @@ def test_dense_tail_matches_level_by_level(n, sweeps, persistent):
         out.append(f.numpy())
         its.append(k)
     assert tail_level(s._levels) > 0
-    for x, y in zip(*out):
-        assert _rel(x, y) < 1e-9
-    assert all(abs(p - q) <= 2 for p, q in zip(*its)), its
+    for k in (0, 1):
+        for x, y in zip(out[k], out[2]):
+            assert _rel(x, y) < 1e-9
+        assert all(abs(p - q) <= 2 for p, q in zip(its[k], its[2])), its
