@@ -351,10 +351,14 @@ def run_batch(args, world, rank, local):
     plain = None
     if not args.no_plain:
         # the plain FP64 path on the same batch: per-problem recorded steps on 16 streams
-        runner = BatchRunner(cfgs, streams=16, options=GpuOptions(precision="fp64"))
-        runner.step(2)
+        popts = {"auto": GpuOptions(precision="fp64"),
+                 "compact": GpuOptions(precision="fp64", tail_ratio=4.0),
+                 "off": GpuOptions(precision="fp64", coarse_tail=False)}[args.plain_tail]
+        runner = BatchRunner(cfgs, streams=16, options=popts)
+        # the same steps of the flow as the batched leg: W untimed, then K timed
+        runner.step(args.warmup)
         torch.cuda.synchronize()
-        k_plain = max(2, min(args.steps, 5))
+        k_plain = args.steps
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record()
         runner.step(k_plain)
@@ -363,7 +367,8 @@ def run_batch(args, world, rank, local):
         pms = p0.elapsed_time(p1)
         plain = {"value": b.cells * k_plain / (pms / 1e3), "ms_per_step": pms / k_plain,
                  "steps": k_plain, "form": "fp64, one single-problem solver per cavity, "
-                                           "recorded steps replayed on 16 streams"}
+                                           "recorded steps replayed on 16 streams",
+                 "dense_tail": args.plain_tail}
         del runner
     if rank == 0:
         sizes = {}
@@ -715,6 +720,8 @@ def main():
     ap.add_argument("--coarse-level", type=int, default=0,
                     help="batch: multigrid levels from this one down in one block per problem (0: off)")
     ap.add_argument("--inner-tol", type=float, default=1e-4, help="batch, mixed: inner tolerance")
+    ap.add_argument("--plain-tail", default="compact", choices=["auto", "compact", "off"],
+                    help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
     ap.add_argument("--no-plain", action="store_true",
                     help="batch: skip the plain per-problem FP64 comparison leg")
     args = ap.parse_args()

@@ -233,6 +233,7 @@ class BatchOptions:
     mg_sweeps: int = 1           #: damped-Jacobi sweeps before/after each coarse correction
     tile_rows: int = 32          #: rows of x per fine-level block (8, 16, 32, 64)
     coarse_level: int = 0        #: multigrid levels from this one down: one block per problem (0: off)
+    coarse_tail: bool = True     #: close each structure's V-cycle with its dense tail operator
 
 
 class BatchedSolver:
@@ -270,14 +271,16 @@ class BatchedSolver:
         descs = (_lib.SolverDesc * n)()
         ctl = (_lib.DtControl * n)()
         keep = []
-        gopts = GpuOptions(precision=opts.precision, inner_tol=opts.inner_tol)
+        gopts = GpuOptions(precision=opts.precision, inner_tol=opts.inner_tol,
+                           coarse_tail=opts.coarse_tail and opts.coarse_level == 0, fused_restriction=False)
         for k, pb in enumerate(self.problems):
             first = pb.key not in leader
             if first:
                 leader[pb.key] = k
             levels, cinv = pb.hierarchy() if first else (None, None)
-            d, kp = native_desc(pb.config, pb.mesh, pb.boundaries, pb.solid, pb.has_obstacle, (),
-                                PressureSolver.MGCG, gopts, levels, cinv)
+            # the tail operator is built for the batch's sweep count
+            d, kp = native_desc(pb.config.replace(mg_sweeps=opts.mg_sweeps), pb.mesh, pb.boundaries, pb.solid,
+                                pb.has_obstacle, (), PressureSolver.MGCG, gopts, levels, cinv)
             keep.append((d, kp))
             descs[k] = d
             structure[k] = leader[pb.key]

@@ -48,6 +48,9 @@ struct BHier {
   const T* C;       // coarsest pseudo-inverse, row-major nc x nc
   int nc;
   int nlev;
+  const T* tail;    // dense operator of the cycle at and below tail_level (row-major), or null
+  int tail_level, tail_n;
+  int sp0, spn;     // this structure's problems: sprobs[sp0 .. sp0 + spn)
 };
 
 // Device record of one problem.  T is the storage type of the (inner) CG and
@@ -58,6 +61,7 @@ struct BProb {
   BcTable bc;
   DtControl dtc;
   int hier, nlev, singular;
+  int tail;                              // depth closed by the structure's dense operator (0: none)
   int max_steps;                         // the problem stops after this many steps
   int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
   int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
@@ -828,7 +832,7 @@ enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG };
 
 template <class T>
 __device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
-  if (d == P.nlev - 1) return P.lxa[d];   // the coarsest result is always in xa
+  if (d == P.nlev - 1 || d == P.tail) return P.lxa[d];   // coarsest and tail results are in xa
   return sel == 0 ? P.lxa[d] : P.lxb[d];
 }
 
@@ -979,6 +983,69 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     case 8: b_ell_rows<8, OP>(P, d, src, dst, e.y); break;
     case 16: b_ell_rows<16, OP>(P, d, src, dst, e.y); break;
     default: b_ell_rows<32, OP>(P, d, src, dst, e.y); break;
+  }
+}
+
+// Dense close of the V-cycle at depth d: x_d = M b_d for the problems whose
+// structure's tail is at d, M the structure's operator (n x n, row-major; the
+// cycle at and below d as one linear map).  A block takes kBTailRows rows of M
+// (one warp each) for a group of kBTailGroup problems of one structure: each
+// lane loads its entries of M once and applies them to every problem of the
+// group (independent accumulators), so M crosses from L2 once per group and a
+// row's sum is a fixed lane-strided order plus the warp tree.
+constexpr int kBTailRows = kBThreads / 32;
+constexpr int kBTailGroup = 8;
+
+template <class T>
+__device__ __forceinline__ T b_warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_tail(const BProb<T>* __restrict__ probs,
+                                                       const BHier<T>* __restrict__ hiers,
+                                                       const int2* __restrict__ map,
+                                                       const int* __restrict__ sprobs, int d, BShared sh) {
+  const int2 e = map[blockIdx.x];   // (structure, row block * 64 + problem group)
+  const BHier<T>& H = hiers[e.x];
+  const int n = H.tail_n;
+  const int rb = e.y >> 6, grp = e.y & 63;
+  __shared__ const T* sb[kBTailGroup];
+  __shared__ T* sx[kBTailGroup];
+  if (threadIdx.x < kBTailGroup) {
+    const int k = grp * kBTailGroup + (int)threadIdx.x;
+    const T* b = nullptr;
+    T* x = nullptr;
+    if (k < H.spn) {
+      const int pi = sprobs[H.sp0 + k];
+      if (b_solving(sh, pi)) {
+        b = probs[pi].lb[d];
+        x = probs[pi].lxa[d];
+      }
+    }
+    sb[threadIdx.x] = b;
+    sx[threadIdx.x] = x;
+  }
+  __syncthreads();
+  const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+  const int row = rb * kBTailRows + warp;
+  if (row >= n) return;   // warp-uniform, no block barrier follows
+  const T* m = H.tail + (long)row * n;
+  T acc[kBTailGroup];
+#pragma unroll
+  for (int g = 0; g < kBTailGroup; ++g) acc[g] = (T)0;
+  for (int c = lane; c < n; c += 32) {
+    const T mv = __ldg(m + c);
+#pragma unroll
+    for (int g = 0; g < kBTailGroup; ++g)
+      if (sb[g]) acc[g] += mv * sb[g][c];
+  }
+#pragma unroll
+  for (int g = 0; g < kBTailGroup; ++g) {
+    const T t = b_warp_sum(acc[g]);
+    if (lane == 0 && sx[g]) sx[g][row] = t;
   }
 }
 

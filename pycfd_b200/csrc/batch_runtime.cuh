@@ -34,6 +34,8 @@ struct pycfd_batch {
   std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
   std::vector<BMapHost> mapR;              // restriction into d (+ coarsest blocks when coarse == 0)
   std::vector<BMapHost> mapP;              // prolongation into d with P_{d+1}
+  std::vector<BMapHost> mapT;              // dense tail at d: (structure, row block x 64 + problem group)
+  int* sprobs = nullptr;                   // problems grouped by structure
   size_t smem_dense = 0;
   BShared sh{};
   int* h_any = nullptr;                    // pinned mirror of sh.any
@@ -99,6 +101,16 @@ int upload_hier(pycfd_batch* B, const pycfd_solver_desc* d, BHier<T>* H, std::ve
     bl.wd = wd;
     bl.n = in.n;
   }
+  if (B->coarse == 0 && d->tail_level > 0 && d->tail_level < Lv - 1 && d->tail_operator) {
+    const int nt = d->levels[d->tail_level].n;
+    std::vector<T> m((size_t)nt * nt);
+    for (size_t e = 0; e < m.size(); ++e) m[e] = (T)d->tail_operator[e];
+    T* md = nullptr;
+    TRY(upload(B->mem, &md, m.data(), m.size()));
+    H->tail = md;
+    H->tail_level = d->tail_level;
+    H->tail_n = nt;
+  }
   const int nc = d->levels[Lv - 1].n;
   std::vector<T> c((size_t)nc * nc);
   for (size_t e = 0; e < c.size(); ++e) c[e] = (T)d->coarsest_inverse[e];
@@ -144,9 +156,6 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   }
   if (B->smem_dense > 48 * 1024)
     return fail(PCFD_E_UNSUPPORTED, "coarsest level too large for the one-block dense solve");
-  void* hd = nullptr;
-  TRY(upload(B->mem, (uint8_t**)&hd, (const uint8_t*)hh.data(), hh.size() * sizeof(BHier<T>)));
-  B->hiers = hd;
 
   // per-problem records
   std::vector<BProb<T>> pr(n);
@@ -164,6 +173,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.dtc = DtControl{c.adaptive, c.cfl, c.visc_limit, c.dt_cap, c.t_end, s->g.dx, s->g.dy, c.blend_mode, c.blend};
     P.hier = hid[i];
     P.nlev = descs[leaders[hid[i]]].n_levels;
+    P.tail = hh[hid[i]].tail_level;
     B->nlev[i] = P.nlev;
     B->depth = std::max(B->depth, P.nlev);
     P.singular = s->singular;
@@ -235,19 +245,47 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
+  // problems grouped by structure (the dense tail's block groups)
+  {
+    std::vector<int> sp;
+    for (size_t h = 0; h < leaders.size(); ++h) {
+      hh[h].sp0 = (int)sp.size();
+      for (int i = 0; i < n; ++i)
+        if (hid[i] == (int)h) sp.push_back(i);
+      hh[h].spn = (int)sp.size() - hh[h].sp0;
+    }
+    TRY(upload(B->mem, &B->sprobs, sp.data(), sp.size()));
+    void* hd = nullptr;
+    TRY(upload(B->mem, (uint8_t**)&hd, (const uint8_t*)hh.data(), hh.size() * sizeof(BHier<T>)));
+    B->hiers = hd;
+  }
   // row-block maps per depth: a block takes kBEllRounds x kBThreads / L rows
   // (L: lanes of its matrix).  With the coarse kernel, a problem's levels from
-  // min(coarse, coarsest) on run there and take no per-level blocks.
+  // min(coarse, coarsest) on run there and take no per-level blocks.  A problem
+  // whose structure has a dense tail at depth t takes the restriction into t
+  // and no level below it; the tail blocks cover t.
   B->mapA.assign(B->depth, BMapHost{});
   B->mapR.assign(B->depth, BMapHost{});
   B->mapP.assign(B->depth, BMapHost{});
+  B->mapT.assign(B->depth, BMapHost{});
   for (int d = 0; d < B->depth; ++d) {
-    std::vector<int2> ma, mr, mp;
+    std::vector<int2> ma, mr, mp, mt;
+    for (size_t h = 0; h < leaders.size(); ++h) {
+      if (hh[h].tail_level != d || hh[h].tail_n == 0) continue;
+      const int rbs = (hh[h].tail_n + kBTailRows - 1) / kBTailRows;
+      const int grps = (hh[h].spn + kBTailGroup - 1) / kBTailGroup;
+      if (grps > 64) return fail(PCFD_E_UNSUPPORTED, "at most %d problems share a structure", 64 * kBTailGroup);
+      for (int rb = 0; rb < rbs; ++rb)
+        for (int g = 0; g < grps; ++g) mt.push_back(make_int2((int)h, rb * 64 + g));
+    }
     for (int i = 0; i < n; ++i) {
       const int c = B->nlev[i] - 1;
+      const int t = pr[i].tail;
       const BHier<T>& H = hh[hid[i]];
       if (B->coarse > 0) {
         if (d >= std::min(B->coarse, c)) continue;
+      } else if (t > 0) {
+        if (d > t) continue;
       } else {
         if (d > c) continue;
         if (d == c) {
@@ -260,6 +298,10 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
         const int rpb = kBThreads / lanes * kBEllRounds;
         for (int rb = 0; rb * rpb < nrow; ++rb) m.push_back(make_int2(i, rb));
       };
+      if (t > 0 && d == t) {   // restriction into the tail level only
+        add(mr, H.lv[d].lr);
+        continue;
+      }
       add(mp, H.lv[d + 1].lp);
       if (d >= 1) {
         add(ma, H.lv[d].la);
@@ -269,6 +311,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     TRY(upload_map(B, &B->mapA[d], ma));
     TRY(upload_map(B, &B->mapR[d], mr));
     TRY(upload_map(B, &B->mapP[d], mp));
+    TRY(upload_map(B, &B->mapT[d], mt));
   }
   {
     std::vector<int> ord(n);
@@ -369,6 +412,12 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
   std::vector<int> cur(B->depth + 1, 0), fin(B->depth + 1, 0);
   for (int d = 1; d < D; ++d) {
     TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+    if (B->mapT[d].n) {
+      b_prof(B, 4, st);
+      BLAUNCH(k_b_tail<T>, B->mapT[d].n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT[d].e, B->sprobs,
+              d, B->sh);
+      b_prof(B, 4, st);
+    }
     if (B->mapA[d].n == 0) continue;
     TRY((b_ell<T, EO_PRE>(B, B->mapA[d], d, 0, 0, st)));
     int a = 0, o = 1;
@@ -662,6 +711,9 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
     d.levels = nullptr;
     d.coarsest_inverse = nullptr;
     d.coarse_cluster_rows = 0;
+    d.persistent_solve = 0;
+    d.tail_level = 0;
+    d.tail_operator = nullptr;
     d.precision = opts->precision;
     d.tol = opts->tol;
     d.maxiter = opts->maxiter;

@@ -199,10 +199,17 @@ def coarsest_pseudo_inverse(level: MgLevelHost, singular: bool) -> np.ndarray:
 TAIL_MAX_ROWS = 2048
 
 
-def tail_level(levels) -> int:
-    """First level above the coarsest (index >= 1) with at most TAIL_MAX_ROWS rows, or 0."""
+def tail_level(levels, ratio: float | None = None) -> int:
+    """First level above the coarsest (index >= 1) with at most TAIL_MAX_ROWS rows, or 0.
+
+    ``ratio``: also require n_l^2 <= ratio * n_0, so the dense operator's bytes stay
+    within a few fine-level vectors (for many small solves sharing the GPU, where
+    bytes count more than launches).
+    """
+    n0 = levels[0].n
     for l in range(1, len(levels) - 1):
-        if levels[l].n <= TAIL_MAX_ROWS:
+        n = levels[l].n
+        if n <= TAIL_MAX_ROWS and (ratio is None or n * n <= ratio * n0):
             return l
     return 0
 
@@ -248,10 +255,10 @@ def fused_restriction(levels, l: int) -> sp.csr_matrix:
     return M
 
 
-def tail_for(levels, cinv: np.ndarray, sweeps: int):
+def tail_for(levels, cinv: np.ndarray, sweeps: int, ratio: float | None = None):
     """``(level, operator)`` closing the V-cycle of this hierarchy, or ``(0, None)``;
-    built once per hierarchy and sweep count."""
-    t = tail_level(levels)
+    built once per hierarchy, sweep count and level."""
+    t = tail_level(levels, ratio)
     if t == 0:
         return 0, None
     ops = levels[t].tails

@@ -54,6 +54,10 @@ class GpuOptions:
     #: rows as one precomputed dense operator (the same linear map, so the same
     #: preconditioner up to rounding) instead of level by level.
     coarse_tail: bool = True
+    #: with ``coarse_tail``: also keep the dense operator within ``tail_ratio``
+    #: fine-level vectors (n_t^2 <= tail_ratio * n_0); None takes the first level
+    #: of at most 2048 rows (fewest launches: best for one solve on the GPU).
+    tail_ratio: float | None = None
     #: MG-PCG with a dense tail and one sweep per level: the first sweep of each
     #: level above the tail and the restriction of its residual as one sparse
     #: product R (I - A W) (the same map), so the down sweep takes one launch per
@@ -210,7 +214,7 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
         keep.append(arr)
         tl, top = (0, None)
         if options.coarse_tail and kind is PressureSolver.MGCG:
-            tl, top = tail_for(levels, cinv, cfg.mg_sweeps)
+            tl, top = tail_for(levels, cinv, cfg.mg_sweeps, options.tail_ratio)
         d.tail_level = tl
         d.tail_operator = _lib.cast(top, C.c_double)
         if tl and options.fused_restriction and cfg.mg_sweeps == 1:

@@ -167,3 +167,21 @@ def test_stopped_problems_leave_the_others_running():
     assert st["frozen"][2] == 0 and st["steps"][2] == 30
     for k in (0, 2):
         assert b.field_stats(k).finite
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dense_tail_matches_level_by_level(precision):
+    """Each structure's V-cycle closed by its dense tail operator (one blocked mat-vec
+    over the structure's problems) against the level-by-level cycle."""
+    from pycfd_b200.batch import BatchedSolver, BatchOptions
+    cfgs = _cavities(count=7, seed=3)
+    out = []
+    for tail in (True, False):
+        b = BatchedSolver(cfgs, BatchOptions(precision=precision, coarse_tail=tail))
+        b.step(6)
+        out.append([b.fields[k].numpy() for k in range(len(cfgs))])
+        assert all(f == 0 for f in b.status()["frozen"])
+    bound = 1e-9 if precision == "fp64" else 1e-7
+    for fa, fb in zip(*out):
+        for x, y in zip(fa[:2], fb[:2]):
+            assert rel(x, y) < bound
