@@ -248,6 +248,145 @@ __device__ __forceinline__ A b_apply(const BProb<T>& P, uint8_t f, int i, int j,
   return acc;
 }
 
+// A block's copy of what a fine cell loop reads from its problem's record: the
+// geometry and tile shape in registers, the diagonal tables in shared memory.
+// The record lives in global memory, and a loop that stores to the problem's
+// vectors cannot keep record fields in registers by itself (the stores might
+// alias it), so without the copy every cell would reload them.
+struct BView {
+  Geo g;
+  int any_dir;
+  double w0;
+  const double* dtab;
+  const double* wtab;
+  int tile_i, tiles_i, tiles_j, tiles, chunk_tiles;
+};
+
+// Declares `V` for problem record P; every thread of the block must reach it.
+#define B_VIEW(V, P)                                                                           \
+  __shared__ double V##_dt[16], V##_wt[16];                                                    \
+  if (threadIdx.y == 0 && threadIdx.x < 16) {                                                  \
+    V##_dt[threadIdx.x] = (P).dtab[threadIdx.x];                                               \
+    V##_wt[threadIdx.x] = (P).wtab[threadIdx.x];                                               \
+  }                                                                                            \
+  __syncthreads();                                                                             \
+  const BView V{(P).g, (P).any_dir, (P).w0, V##_dt, V##_wt, (P).tile_i, (P).tiles_i, (P).tiles_j, \
+                (P).tiles, (P).chunk_tiles}
+
+__device__ __forceinline__ double b_diag(const BView& V, uint8_t f, int i, int j) {
+  if (!(f & F_SOLV)) return 1.0;
+  if (V.any_dir && (i == 0 || j == 0 || i == V.g.nx - 1 || j == V.g.ny - 1)) return fine_diag(f, i, j, V.g);
+  return V.dtab[f & 15];
+}
+__device__ __forceinline__ double b_wdinv(const BView& V, uint8_t f, int i, int j) {
+  if (!(f & F_SOLV)) return V.w0 * (1.0 / 1.0);
+  if (V.any_dir && (i == 0 || j == 0 || i == V.g.nx - 1 || j == V.g.ny - 1))
+    return V.w0 * (1.0 / fine_diag(f, i, j, V.g));
+  return V.wtab[f & 15];
+}
+template <class A, class X>
+__device__ __forceinline__ A b_apply(const BView& V, uint8_t f, int i, int j, int c, X x) {
+  const Geo& g = V.g;
+  A acc = (A)b_diag(V, f, i, j) * x(c, i, j);
+  if (f & F_W) { const int a = wrap_w(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_E) { const int a = wrap_e(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
+  if (f & F_S) { const int b = wrap_s(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
+  if (f & F_N) { const int b = wrap_n(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
+  return acc;
+}
+
+// ---- staged fine tiles --------------------------------------------------------
+// The stencil kernels stage a tile's values once in shared memory, with a one-
+// cell halo, instead of rebuilding every neighbour's value per cell: sm[li][lj]
+// holds v at cell (i0 + li - 1, j0 + lj - 1).  Outside the domain the halo
+// wraps where the axis is periodic; elsewhere it holds 0 -- a face flag is
+// clear there, so the value is never read.
+constexpr int kBHaloJ = kBTileJ + 2;
+constexpr int kBHaloRows = 64 + 2;   // the largest tile height, plus the halo
+
+template <class T, class F>
+__device__ __forceinline__ void b_stage(T (*sm)[kBHaloJ], const BView& V, int i0, int j0, int rows, F v) {
+  const int nx = V.g.nx, ny = V.g.ny;
+  const int total = (rows + 2) * kBHaloJ;
+#pragma unroll 4
+  for (int idx = (int)(threadIdx.y * kBTileJ + threadIdx.x); idx < total; idx += kBThreads) {
+    const int li = idx / kBHaloJ, lj = idx - li * kBHaloJ;
+    int i = i0 + li - 1, j = j0 + lj - 1;
+    bool ok = true;
+    if (i < 0) {
+      ok = V.g.periodic_x != 0;
+      i = nx - 1;
+    } else if (i >= nx) {
+      ok = V.g.periodic_x && i == nx;
+      i = 0;
+    }
+    if (j < 0) {
+      ok = ok && V.g.periodic_y;
+      j = ny - 1;
+    } else if (j >= ny) {
+      ok = ok && V.g.periodic_y && j == ny;
+      j = 0;
+    }
+    sm[li][lj] = ok ? v(i * ny + j, i, j) : (T)0;
+  }
+}
+
+// (A x)_c from a staged tile, fine_apply's terms in its order.
+template <class A, class T>
+__device__ __forceinline__ A b_apply_sm(const BView& V, uint8_t f, int i, int j, const T (*sm)[kBHaloJ], int li,
+                                        int lj) {
+  A acc = (A)b_diag(V, f, i, j) * (A)sm[li][lj];
+  if (f & F_W) acc += (A)V.g.cx * (A)sm[li - 1][lj];
+  if (f & F_E) acc += (A)V.g.cx * (A)sm[li + 1][lj];
+  if (f & F_S) acc += (A)V.g.cy * (A)sm[li][lj - 1];
+  if (f & F_N) acc += (A)V.g.cy * (A)sm[li][lj + 1];
+  return acc;
+}
+
+// A thread's cells of a tile in batches of kBCellBatch rows: load(u, c) for
+// every cell of the batch first (independent loads in flight), then body(u, c,
+// i, j, li, lj) in row order -- the order a plain row loop visits them.
+constexpr int kBCellBatch = 4;
+
+template <class Load, class Body>
+__device__ __forceinline__ void b_tile_cells(const BView& V, int i0, int j0, int rows, Load load, Body body) {
+  const int j = j0 + (int)threadIdx.x, lj = (int)threadIdx.x + 1;
+  if (j >= V.g.ny) return;
+  for (int l0 = 1 + (int)threadIdx.y; l0 <= rows; l0 += kBCellBatch * kBThreadsI) {
+    int c[kBCellBatch];
+#pragma unroll
+    for (int u = 0; u < kBCellBatch; ++u) {
+      const int li = l0 + u * kBThreadsI;
+      c[u] = (i0 + li - 1) * V.g.ny + j;
+      if (li <= rows) load(u, c[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kBCellBatch; ++u) {
+      const int li = l0 + u * kBThreadsI;
+      if (li <= rows) body(u, c[u], i0 + li - 1, j, li, lj);
+    }
+  }
+}
+
+// The tiles of a chunk (block-uniform), optionally staged: with a value
+// function `val`, each tile's values and halo go to `sm` first.  Every thread
+// of the block runs the same tiles (the barriers need them all).
+template <bool STAGE, class T, class Val, class Load, class Body>
+__device__ __forceinline__ void b_chunk_cells(const BView& V, int chunk, T (*sm)[kBHaloJ], Val val, Load load,
+                                              Body body) {
+  for (int tile = chunk * V.chunk_tiles, tend = min(V.tiles, tile + V.chunk_tiles); tile < tend; ++tile) {
+    const int ti = tile / V.tiles_j, tj = tile - ti * V.tiles_j;
+    const int i0 = ti * V.tile_i, j0 = tj * kBTileJ;
+    const int rows = min(V.tile_i, V.g.nx - i0);
+    if (STAGE) {
+      __syncthreads();
+      b_stage(sm, V, i0, j0, rows, val);
+      __syncthreads();
+    }
+    b_tile_cells(V, i0, j0, rows, load, body);
+  }
+}
+
 // ---- step bookkeeping -------------------------------------------------------
 // max|u|, max|v| over the physical faces and the non-finite count of u, v, p:
 // the inputs of the time-step control (pycfd/core/timestepper.py:94-142).
@@ -535,33 +674,38 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
-  const Geo& g = P.g;
+  B_VIEW(V, P);
+  const int ny = V.g.ny;
   const bool first = P.I[I_IT] == 0;
   const double beta = first ? 0.0 : P.S[S_RHO] / P.S[S_RHO_PREV];
   const double mz = P.S[S_MEAN_Z];
-  const uint8_t* flags = P.flags;
-  const T* zraw = P.z;
-  const T* p_old = P.pa;
+  const uint8_t* __restrict__ flags = P.flags;
+  const T* __restrict__ zraw = P.z;
+  const T* __restrict__ p_old = P.pa;
+  T* __restrict__ pn = P.pb;
+  T* __restrict__ q = P.q;
   // arithmetic in T (FP32 in the mixed form's inner solve), p.q summed in FP64
   const T tb = (T)beta, tm = (T)mz;
-  auto pval = [&](int k, int, int) -> T {
-    const T z = (flags[k] & F_SOLV) ? zraw[k] - tm : (T)0;
+  auto pval = [&](int k, int, int) -> T {   // all loads issued, then selected
+    const uint8_t fk = flags[k];
+    const T zk = zraw[k];
+    const T pk = first ? (T)0 : p_old[k];
+    const T z = (fk & F_SOLV) ? zk - tm : (T)0;
     if (first) return z;
-    return p_old[k] * tb + z;
+    return pk * tb + z;
   };
   double acc[1] = {0.0};
-  {
-    B_CHUNK_TILES(P, e.y) {
-      B_TILE_CELLS(P, tile_) {
-        const int c = i * g.ny + j;
-        const T pc = pval(c, i, j);
-        const T qc = b_apply<T>(P, flags[c], i, j, c, pval);
-        P.pb[c] = pc;
-        P.q[c] = qc;
-        acc[0] += (double)pc * (double)qc;
-      }
-    }
-  }
+  __shared__ T sm[kBHaloRows][kBHaloJ];
+  uint8_t fv[kBCellBatch];
+  b_chunk_cells<true>(V, e.y, sm, pval, [&](int u, int c) { fv[u] = flags[c]; },
+                      [&](int u, int c, int i, int j, int li, int lj) {
+                        const T pc = sm[li][lj];
+                        const T qc = b_apply_sm<T>(V, fv[u], i, j, sm, li, lj);
+                        pn[c] = pc;
+                        q[c] = qc;
+                        acc[0] += (double)pc * (double)qc;
+                      });
+  (void)ny;
   b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
     P.S[S_PQ] = t[0];
     P.S[S_ALPHA] = P.S[S_RHO] / t[0];
@@ -578,23 +722,38 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
   const BProb<T>& P = probs[e.x];
   if (b_solving(sh, e.x)) {
     const Geo& g = P.g;
+    B_VIEW(V, P);
+    const int ny = V.g.ny;
     const double alpha = P.S[S_ALPHA];
+    const uint8_t* __restrict__ flags = P.flags;
+    const T* __restrict__ pn = P.pb;
+    const T* __restrict__ q = P.q;
+    T* __restrict__ pa = P.pa;
+    T* __restrict__ xs = P.xs;
+    T* __restrict__ r = P.r;
     double acc[2] = {0, 0};
-    {
-      B_CHUNK_TILES(P, e.y) {
-        B_TILE_CELLS(P, tile_) {
-          const int c = i * g.ny + j;
-          const T pc = P.pb[c];
-          const double xc = (double)P.xs[c] + alpha * (double)pc;
-          const double rc = (double)(T)((double)P.r[c] - alpha * (double)P.q[c]);
-          P.pa[c] = pc;
-          P.xs[c] = (T)xc;
-          P.r[c] = (T)rc;
+    T pv[kBCellBatch], xv[kBCellBatch], rv[kBCellBatch], qv[kBCellBatch];
+    uint8_t fv[kBCellBatch];
+    b_chunk_cells<false, T>(
+        V, e.y, nullptr, [](int, int, int) { return (T)0; },
+        [&](int u, int c) {
+          pv[u] = pn[c];
+          xv[u] = xs[c];
+          rv[u] = r[c];
+          qv[u] = q[c];
+          fv[u] = flags[c];
+        },
+        [&](int u, int c, int, int, int, int) {
+          const T pc = pv[u];
+          const double xc = (double)xv[u] + alpha * (double)pc;
+          const double rc = (double)(T)((double)rv[u] - alpha * (double)qv[u]);
+          pa[c] = pc;
+          xs[c] = (T)xc;
+          r[c] = (T)rc;
           acc[0] += rc * rc;
-          if (P.flags[c] & F_SOLV) acc[1] += rc;
-        }
-      }
-    }
+          if (fv[u] & F_SOLV) acc[1] += rc;
+        });
+    (void)ny;
     b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
@@ -779,39 +938,62 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
   const Geo& g = P.g;
+  B_VIEW(V, P);
+  const int ny = V.g.ny;
   // arithmetic in T (FP32 in the mixed form's inner solve), sums in FP64
   const uint8_t* __restrict__ flags = P.flags;
   const T* __restrict__ r = P.r;
   const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
-  auto bf = [&](int k) -> T { return (flags[k] & F_SOLV) ? r[k] - mr : (T)0; };
-  const T* x = b_fine_buf(P, src);
-  T* xo = b_fine_buf(P, dst);
+  auto bf = [&](int k) -> T {   // both loads issued, then selected
+    const uint8_t fk = flags[k];
+    const T rk = r[k];
+    return (fk & F_SOLV) ? rk - mr : (T)0;
+  };
+  const T* __restrict__ x = b_fine_buf(P, src);
+  T* __restrict__ xo = b_fine_buf(P, dst);
   T* __restrict__ lres0 = P.lres[0];
   double acc[2] = {0, 0};
-  {
-    B_CHUNK_TILES(P, e.y) {
-      B_TILE_CELLS(P, tile_) {
-        const int c = i * g.ny + j;
-        const uint8_t f = flags[c];
-        if (MODE == FM_PRE) {
-          auto xv = [&](int k, int ii, int jj) -> T { return (T)b_wdinv(P, flags[k], ii, jj) * bf(k); };
-          xo[c] = xv(c, i, j);
-          lres0[c] = bf(c) - b_apply<T>(P, f, i, j, c, xv);
-        } else if (MODE == FM_WDB) {
-          xo[c] = (T)b_wdinv(P, f, i, j) * bf(c);
-        } else if (MODE == FM_RESID) {
-          auto xv = [&](int k, int, int) -> T { return x[k]; };
-          lres0[c] = bf(c) - b_apply<T>(P, f, i, j, c, xv);
+  __shared__ T sm[kBHaloRows][kBHaloJ];
+  if (MODE == FM_WDB) {
+    B_CHUNK_TILES(V, e.y) {
+      B_TILE_CELLS(V, tile_) {
+        const int c = i * ny + j;
+        xo[c] = (T)b_wdinv(V, flags[c], i, j) * bf(c);
+      }
+    }
+  } else {
+    uint8_t fv[kBCellBatch];
+    T rv[kBCellBatch];
+    auto load = [&](int u, int c) {
+      fv[u] = flags[c];
+      rv[u] = r[c];
+    };
+    auto bfv = [&](int u) -> T { return (fv[u] & F_SOLV) ? rv[u] - mr : (T)0; };   // bf at the cell
+    if (MODE == FM_PRE) {
+      auto xw = [&](int k, int ii, int jj) -> T {
+        const uint8_t fk = flags[k];
+        const T bk = bf(k);
+        return (T)b_wdinv(V, fk, ii, jj) * bk;
+      };
+      b_chunk_cells<true>(V, e.y, sm, xw, load, [&](int u, int c, int i, int j, int li, int lj) {
+        xo[c] = sm[li][lj];
+        lres0[c] = bfv(u) - b_apply_sm<T>(V, fv[u], i, j, sm, li, lj);
+      });
+    } else {
+      auto xw = [&](int k, int, int) -> T { return x[k]; };
+      b_chunk_cells<true>(V, e.y, sm, xw, load, [&](int u, int c, int i, int j, int li, int lj) {
+        const uint8_t f = fv[u];
+        if (MODE == FM_RESID) {
+          lres0[c] = bfv(u) - b_apply_sm<T>(V, f, i, j, sm, li, lj);
         } else {
-          auto xv = [&](int k, int, int) -> T { return x[k]; };
-          const T xn = x[c] + (T)b_wdinv(P, f, i, j) * (bf(c) - b_apply<T>(P, f, i, j, c, xv));
+          const T xn = sm[li][lj] + (T)b_wdinv(V, f, i, j) * (bfv(u) - b_apply_sm<T>(V, f, i, j, sm, li, lj));
           xo[c] = xn;
           if (MODE == FM_LAST && (f & F_SOLV)) {
             acc[0] += (double)xn;
-            acc[1] += (double)r[c] * (double)xn;
+            acc[1] += (double)rv[u] * (double)xn;
           }
         }
-      }
+      });
     }
   }
   if (MODE != FM_LAST) return;
@@ -892,31 +1074,32 @@ __device__ __forceinline__ void b_ell_rows(const BProb<T>& P, int d, int src, in
   const int lane = threadIdx.x & (L - 1);
   if (OP == EO_PROLONG) {
     // x_d += P_{d+1} x_{d+1}
-    const BLevel<T>& Lc = P.lv[d + 1];
+    const Ell<T> Pm = P.lv[d + 1].P;
     const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
     T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
 #pragma unroll
     for (int rd = 0; rd < kBEllRounds; ++rd) {
       const int row = r0 + rd * per + (int)threadIdx.x / L;
-      const T s = b_ell_row_c<L>(Lc.P, row < r1 ? row : Lc.P.n, lane, [&](int c) { return xc[c]; });
+      const T s = b_ell_row_c<L>(Pm, row < r1 ? row : Pm.n, lane, [&](int c) { return xc[c]; });
       if (lane == 0 && row < r1) xf[row] = xf[row] + s;
     }
     return;
   }
-  const BLevel<T>& Lv = P.lv[d];
   if (OP == EO_RESTRICT) {
+    const Ell<T> R = P.lv[d].R;
     const T* __restrict__ res = P.lres[d - 1];
     T* __restrict__ bo = P.lb[d];
 #pragma unroll
     for (int rd = 0; rd < kBEllRounds; ++rd) {
       const int row = r0 + rd * per + (int)threadIdx.x / L;
-      const T s = b_ell_row_c<L>(Lv.R, row < r1 ? row : Lv.R.n, lane, [&](int c) { return res[c]; });
+      const T s = b_ell_row_c<L>(R, row < r1 ? row : R.n, lane, [&](int c) { return res[c]; });
       if (lane == 0 && row < r1) bo[row] = s;
     }
     return;
   }
+  const Ell<T> A = P.lv[d].A;
   const T* __restrict__ b = P.lb[d];
-  const T* __restrict__ wd = Lv.wd;
+  const T* __restrict__ wd = P.lv[d].wd;
   const T* __restrict__ x = b_lvl_x(P, d, src);
   T* __restrict__ xo = b_lvl_x(P, d, dst);
   T* __restrict__ xa = P.lxa[d];
@@ -924,19 +1107,19 @@ __device__ __forceinline__ void b_ell_rows(const BProb<T>& P, int d, int src, in
 #pragma unroll
   for (int rd = 0; rd < kBEllRounds; ++rd) {
     const int row = r0 + rd * per + (int)threadIdx.x / L;
-    const int rr = row < r1 ? row : Lv.A.n;
+    const int rr = row < r1 ? row : A.n;
     if (OP == EO_PRE) {
-      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return wd[c] * b[c]; });
+      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return wd[c] * b[c]; });
       if (lane == 0 && row < r1) {
         const T bx = b[row];
         xa[row] = wd[row] * bx;
         ro[row] = bx - s;
       }
     } else if (OP == EO_SMOOTH) {
-      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return x[c]; });
+      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return x[c]; });
       if (lane == 0 && row < r1) xo[row] = x[row] + wd[row] * (b[row] - s);
     } else {   // EO_RESID
-      const T s = b_ell_row_c<L>(Lv.A, rr, lane, [&](int c) { return x[c]; });
+      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return x[c]; });
       if (lane == 0 && row < r1) ro[row] = b[row] - s;
     }
   }
