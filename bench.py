@@ -284,9 +284,11 @@ def run_batch(args, world, rank, local):
     if args.autotune:
         opts = BatchAutotuner(allowed_precisions=(args.precision,)).choose(cfgs)
     else:
+        tail = args.batch_tail
         opts = BatchOptions(precision=args.precision, tile_rows=args.tile_rows,
                             mg_sweeps=args.mg_sweeps, inner_tol=args.inner_tol,
-                            coarse_level=args.coarse_level)
+                            coarse_level=args.coarse_level, coarse_tail=tail != "off",
+                            tail_ratio=None if tail in ("none", "off") else float(tail))
     b = BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
     rec = not args.eager
@@ -712,14 +714,17 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="problems in the batch workload")
     ap.add_argument("--val-steps", type=int, default=500, help="tgv-validation: steps")
     ap.add_argument("--cyl-steps", type=int, default=20000, help="cylinder: steps per precision")
-    ap.add_argument("--autotune", action="store_true",
-                    help="batch: pick tiles, sweeps, coarse level and inner tolerance by timing (cached)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="batch: take the options below instead of the autotuner's choice (tiles, sweeps, "
+                         "tail bound, coarse level, inner tolerance; timed on the batch, cached)")
     ap.add_argument("--tile-rows", type=int, default=32, choices=[8, 16, 32, 64],
                     help="batch: rows per fine-level tile")
     ap.add_argument("--mg-sweeps", type=int, default=1, help="batch: smoothing sweeps per level")
     ap.add_argument("--coarse-level", type=int, default=0,
                     help="batch: multigrid levels from this one down in one block per problem (0: off)")
     ap.add_argument("--inner-tol", type=float, default=1e-4, help="batch, mixed: inner tolerance")
+    ap.add_argument("--batch-tail", default="16",
+                    help="batch: dense V-cycle tail per structure -- a bound r (n_t^2 <= r n_0), none, or off")
     ap.add_argument("--plain-tail", default="compact", choices=["auto", "compact", "off"],
                     help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
     ap.add_argument("--no-plain", action="store_true",

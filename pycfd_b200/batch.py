@@ -234,6 +234,7 @@ class BatchOptions:
     tile_rows: int = 32          #: rows of x per fine-level block (8, 16, 32, 64)
     coarse_level: int = 0        #: multigrid levels from this one down: one block per problem (0: off)
     coarse_tail: bool = True     #: close each structure's V-cycle with its dense tail operator
+    tail_ratio: float | None = 16.0   #: bound the tail operator: n_t^2 <= tail_ratio * n_0 (None: none)
 
 
 class BatchedSolver:
@@ -272,7 +273,8 @@ class BatchedSolver:
         ctl = (_lib.DtControl * n)()
         keep = []
         gopts = GpuOptions(precision=opts.precision, inner_tol=opts.inner_tol,
-                           coarse_tail=opts.coarse_tail and opts.coarse_level == 0, fused_restriction=False)
+                           coarse_tail=opts.coarse_tail and opts.coarse_level == 0, tail_ratio=opts.tail_ratio,
+                           fused_restriction=False)
         for k, pb in enumerate(self.problems):
             first = pb.key not in leader
             if first:
@@ -425,6 +427,8 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=16),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=None),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=4.0),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, coarse_level=3),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
 )
