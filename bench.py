@@ -725,7 +725,7 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=1e-4, help="batch, mixed: inner tolerance")
     ap.add_argument("--batch-tail", default="16",
                     help="batch: dense V-cycle tail per structure -- a bound r (n_t^2 <= r n_0), none, or off")
-    ap.add_argument("--plain-tail", default="compact", choices=["auto", "compact", "off"],
+    ap.add_argument("--plain-tail", default="auto", choices=["auto", "compact", "off"],
                     help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
     ap.add_argument("--no-plain", action="store_true",
                     help="batch: skip the plain per-problem FP64 comparison leg")

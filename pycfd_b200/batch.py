@@ -235,6 +235,7 @@ class BatchOptions:
     coarse_level: int = 0        #: multigrid levels from this one down: one block per problem (0: off)
     coarse_tail: bool = True     #: close each structure's V-cycle with its dense tail operator
     tail_ratio: float | None = 16.0   #: bound the tail operator: n_t^2 <= tail_ratio * n_0 (None: none)
+    fused_restriction: bool = False   #: down sweep by R (I - A W) products (one sweep, every structure tailed)
 
 
 class BatchedSolver:
@@ -274,7 +275,7 @@ class BatchedSolver:
         keep = []
         gopts = GpuOptions(precision=opts.precision, inner_tol=opts.inner_tol,
                            coarse_tail=opts.coarse_tail and opts.coarse_level == 0, tail_ratio=opts.tail_ratio,
-                           fused_restriction=False)
+                           fused_restriction=opts.fused_restriction)
         for k, pb in enumerate(self.problems):
             first = pb.key not in leader
             if first:
@@ -430,7 +431,9 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=None),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=4.0),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, coarse_level=3),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
+    BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True),
 )
 
 

@@ -39,6 +39,8 @@ struct BLevel {
   int la, lr, lp;   // lanes per row of each block
   const T* wd;      // weighted inverse diagonal
   int n;
+  Ell<T> M;         // fused restriction R (I - A W) from the finer level (rows of this level), optional
+  int lm;
 };
 
 template <class T>
@@ -50,6 +52,7 @@ struct BHier {
   int nlev;
   const T* tail;    // dense operator of the cycle at and below tail_level (row-major), or null
   int tail_level, tail_n;
+  int fused;        // levels 1..tail_level carry their fused restriction M
   int sp0, spn;     // this structure's problems: sprobs[sp0 .. sp0 + spn)
 };
 
@@ -1010,7 +1013,11 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
 // kBEllRounds x kBThreads / L rows, L lanes per row from the problem's
 // hierarchy (runtime), so problems of different structures share one launch
 // and wide rows spread over many blocks.
-enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG };
+// EO_FRESTRICT: b_d = M_d b_{d-1} (first sweep on d-1 and restriction of its
+// residual in one product; from level 0 the right-hand side is the projected CG
+// residual).  EO_PROLONGW: prolongation onto a level whose first-sweep iterate
+// W b was not stored -- it is formed again, with the same T roundings.
+enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG, EO_FRESTRICT, EO_PROLONGW };
 
 template <class T>
 __device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
@@ -1082,6 +1089,65 @@ __device__ __forceinline__ void b_ell_rows(const BProb<T>& P, int d, int src, in
       const int row = r0 + rd * per + (int)threadIdx.x / L;
       const T s = b_ell_row_c<L>(Pm, row < r1 ? row : Pm.n, lane, [&](int c) { return xc[c]; });
       if (lane == 0 && row < r1) xf[row] = xf[row] + s;
+    }
+    return;
+  }
+  if (OP == EO_PROLONGW) {
+    // x_d = W b_d + P_{d+1} x_{d+1}; on level 0 W b is fine_wdinv * (projected residual)
+    const Ell<T> Pm = P.lv[d + 1].P;
+    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
+    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
+    const T* __restrict__ b = P.lb[d];
+    const T* __restrict__ wd = P.lv[d].wd;
+    const uint8_t* __restrict__ flags = P.flags;
+    const T* __restrict__ r = P.r;
+    const T mr = (T)(d == 0 && P.singular ? P.S[S_MEAN_R] : 0.0);
+    const int ny = P.g.ny;
+#pragma unroll
+    for (int rd = 0; rd < kBEllRounds; ++rd) {
+      const int row = r0 + rd * per + (int)threadIdx.x / L;
+      const T s = b_ell_row_c<L>(Pm, row < r1 ? row : Pm.n, lane, [&](int c) { return xc[c]; });
+      if (lane == 0 && row < r1) {
+        T wb;
+        if (d == 0) {
+          const uint8_t f = flags[row];
+          const int i = row / ny, j = row - i * ny;
+          const T bfr = (f & F_SOLV) ? r[row] - mr : (T)0;
+          wb = (T)b_wdinv(P, f, i, j) * bfr;
+        } else {
+          wb = wd[row] * b[row];
+        }
+        xf[row] = wb + s;
+      }
+    }
+    return;
+  }
+  if (OP == EO_FRESTRICT) {
+    // b_d = M_d b_{d-1}, from level 0 the projected CG residual
+    const Ell<T> M = P.lv[d].M;
+    T* __restrict__ bo = P.lb[d];
+    if (d == 1) {
+      const uint8_t* __restrict__ flags = P.flags;
+      const T* __restrict__ r = P.r;
+      const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
+#pragma unroll
+      for (int rd = 0; rd < kBEllRounds; ++rd) {
+        const int row = r0 + rd * per + (int)threadIdx.x / L;
+        const T s = b_ell_row_c<L>(M, row < r1 ? row : M.n, lane, [&](int c) {
+          const uint8_t fc = flags[c];
+          const T rc = r[c];
+          return (fc & F_SOLV) ? rc - mr : (T)0;
+        });
+        if (lane == 0 && row < r1) bo[row] = s;
+      }
+    } else {
+      const T* __restrict__ bi = P.lb[d - 1];
+#pragma unroll
+      for (int rd = 0; rd < kBEllRounds; ++rd) {
+        const int row = r0 + rd * per + (int)threadIdx.x / L;
+        const T s = b_ell_row_c<L>(M, row < r1 ? row : M.n, lane, [&](int c) { return bi[c]; });
+        if (lane == 0 && row < r1) bo[row] = s;
+      }
     }
     return;
   }
@@ -1159,7 +1225,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
     return;
   }
   // the rows of this block, with the lane count of its matrix fixed at compile time
-  const int Lop = OP == EO_PROLONG ? P.lv[d + 1].lp : OP == EO_RESTRICT ? P.lv[d].lr : P.lv[d].la;
+  const int Lop = (OP == EO_PROLONG || OP == EO_PROLONGW) ? P.lv[d + 1].lp
+                  : OP == EO_RESTRICT                    ? P.lv[d].lr
+                  : OP == EO_FRESTRICT                   ? P.lv[d].lm
+                                                         : P.lv[d].la;
   switch (Lop) {
     case 1: b_ell_rows<1, OP>(P, d, src, dst, e.y); break;
     case 4: b_ell_rows<4, OP>(P, d, src, dst, e.y); break;

@@ -22,6 +22,7 @@ struct pycfd_batch {
   double tol = 1e-10, inner_tol = 1e-4;
   int maxiter = 1000, sweeps = 1, tile_i = 32;
   int coarse = 0;                          // levels >= coarse: one block per problem (0: per level)
+  int fused = 0;                           // down sweep by fused restrictions (every structure has them)
   int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
@@ -92,6 +93,12 @@ int upload_hier(pycfd_batch* B, const pycfd_solver_desc* d, BHier<T>* H, std::ve
     csr_transpose(up.n, in.n, in.p_indptr, in.p_indices, in.p_data, tp, ti, td);
     TRY(make_ell(B->mem, &R, in.n, tp.data(), ti.data(), td.data()));
     BLevel<T>& bl = H->lv[l];
+    if (in.m_indptr) {
+      DevEll<T> M;
+      TRY(make_ell(B->mem, &M, in.n, in.m_indptr, in.m_indices, in.m_data));
+      bl.M = M.view();
+      bl.lm = M.lanes;
+    }
     bl.A = A.view();
     bl.la = A.lanes;
     bl.P = P.view();
@@ -110,6 +117,9 @@ int upload_hier(pycfd_batch* B, const pycfd_solver_desc* d, BHier<T>* H, std::ve
     H->tail = md;
     H->tail_level = d->tail_level;
     H->tail_n = nt;
+    H->fused = 1;
+    for (int l = 1; l <= d->tail_level; ++l)
+      if (!d->levels[l].m_indptr) H->fused = 0;
   }
   const int nc = d->levels[Lv - 1].n;
   std::vector<T> c((size_t)nc * nc);
@@ -264,6 +274,11 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   // min(coarse, coarsest) on run there and take no per-level blocks.  A problem
   // whose structure has a dense tail at depth t takes the restriction into t
   // and no level below it; the tail blocks cover t.
+  // fused down sweep: every structure closes its cycle with a tail and carries
+  // the fused restrictions above it, one sweep per level
+  B->fused = (B->coarse == 0 && B->sweeps == 1) ? 1 : 0;
+  for (size_t h = 0; h < leaders.size(); ++h)
+    if (!hh[h].fused || hh[h].tail_level == 0) B->fused = 0;
   B->mapA.assign(B->depth, BMapHost{});
   B->mapR.assign(B->depth, BMapHost{});
   B->mapP.assign(B->depth, BMapHost{});
@@ -298,14 +313,15 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
         const int rpb = kBThreads / lanes * kBEllRounds;
         for (int rb = 0; rb * rpb < nrow; ++rb) m.push_back(make_int2(i, rb));
       };
+      const int lres = B->fused ? H.lv[d].lm : H.lv[d].lr;   // lanes of the restriction into d
       if (t > 0 && d == t) {   // restriction into the tail level only
-        add(mr, H.lv[d].lr);
+        add(mr, lres);
         continue;
       }
       add(mp, H.lv[d + 1].lp);
       if (d >= 1) {
         add(ma, H.lv[d].la);
-        add(mr, H.lv[d].lr);
+        add(mr, lres);
       }
     }
     TRY(upload_map(B, &B->mapA[d], ma));
@@ -395,6 +411,27 @@ template <class T>
 int b_vcycle(pycfd_batch* B, cudaStream_t st) {
   const int sw = B->sweeps;
   const int D = B->coarse > 0 ? std::min(B->coarse, B->depth) : B->depth;   // depths run per level
+  if (B->fused) {
+    // ---- down: b_d = M_d b_{d-1} at every depth above each problem's tail, then the tails
+    for (int d = 1; d < D; ++d) {
+      TRY((b_ell<T, EO_FRESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+      if (B->mapT[d].n) {
+        b_prof(B, 4, st);
+        BLAUNCH(k_b_tail<T>, B->mapT[d].n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT[d].e,
+                B->sprobs, d, B->sh);
+        b_prof(B, 4, st);
+      }
+    }
+    // ---- up: x_d = W b_d + P x_{d+1} into xa, one sweep into xb
+    for (int d = D - 2; d >= 1; --d) {
+      if (B->mapA[d].n == 0) continue;
+      TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[d], d, 1, 0, st)));
+      TRY((b_ell<T, EO_SMOOTH>(B, B->mapA[d], d, 0, 1, st)));
+    }
+    TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[0], 0, 1, 0, st)));
+    TRY((b_fine<T, FM_LAST>(B, 0, 2, st)));
+    return 0;
+  }
   // ---- down ----
   int cur0 = 0;
   if (sw == 1) {
