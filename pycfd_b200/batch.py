@@ -269,6 +269,7 @@ class BatchedSolver:
         self.problems = [_Problem(cfg, None if obstacles is None else obstacles[k])
                          for k, cfg in enumerate(self.configs)]
         leader: dict = {}
+        tailed: dict = {}
         structure = (C.c_int * n)()
         descs = (_lib.SolverDesc * n)()
         ctl = (_lib.DtControl * n)()
@@ -287,9 +288,17 @@ class BatchedSolver:
             keep.append((d, kp))
             descs[k] = d
             structure[k] = leader[pb.key]
+            if first:
+                tailed[pb.key] = d.tail_level > 0
             te = t_end[k] if isinstance(t_end, (list, tuple, np.ndarray)) else t_end
             ctl[k] = dt_control_for(pb.config, pb.mesh, float(te))
         self.structures = len(leader)
+        #: problems whose structure closes its V-cycle with a dense tail
+        self._tailed = sum(1 for pb in self.problems if tailed[pb.key])
+        #: the down sweep runs by fused restrictions (the engine's rule: every
+        #: structure tailed, one sweep per level, per-level coarse launches)
+        self._fused = bool(opts.fused_restriction and opts.mg_sweeps == 1 and opts.coarse_level == 0
+                           and self._tailed == n)
         # state in three flat pools (one host<->device copy per array kind), one view per problem
         shapes = [(pb.mesh.u_shape, pb.mesh.v_shape, pb.mesh.p_shape) for pb in self.problems]
         sizes = [[int(np.prod(sh)) for sh in trio] for trio in shapes]

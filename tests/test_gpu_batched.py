@@ -177,7 +177,8 @@ def test_dense_tail_matches_level_by_level(precision):
     cfgs = _cavities(count=7, seed=3)
     out = []
     for tail in (True, False):
-        b = BatchedSolver(cfgs, BatchOptions(precision=precision, coarse_tail=tail))
+        b = BatchedSolver(cfgs, BatchOptions(precision=precision, coarse_tail=tail, tail_ratio=None))
+        assert not tail or b._tailed == len(cfgs)
         b.step(6)
         out.append([b.fields[k].numpy() for k in range(len(cfgs))])
         assert all(f == 0 for f in b.status()["frozen"])
@@ -194,7 +195,9 @@ def test_fused_restriction_matches_two_phase_down_sweep(precision):
     cfgs = _cavities(count=7, seed=4)
     out = []
     for fused in (True, False):
-        b = BatchedSolver(cfgs, BatchOptions(precision=precision, fused_restriction=fused))
+        # unbounded tail: these small cavities all get one (a tail bound would leave them none)
+        b = BatchedSolver(cfgs, BatchOptions(precision=precision, fused_restriction=fused, tail_ratio=None))
+        assert b._fused == fused
         b.step(6)
         out.append([b.fields[k].numpy() for k in range(len(cfgs))])
         assert all(f == 0 for f in b.status()["frozen"])
