@@ -220,27 +220,30 @@ def live_roofline(solver, f, dt, hbm_gbs, steps=3):
             "share_of_candidates": {KERNELS[k]: v[0] for k, v in shares.items()}}
 
 
-def cpu_baseline(steps=3):
-    """The oracle (NumPy/SciPy restatement of the reference) on a bounded sample."""
+def cpu_baseline(steps=3, warmup=0):
+    """The oracle (NumPy/SciPy restatement of the reference) on a bounded sample,
+    after `warmup` untimed steps."""
     from oracle import OracleSolver
     from pycfd_b200.mesh import StructuredMesh
     cfg = tgv_config()
     t0 = time.perf_counter()
     s = OracleSolver(cfg)
     u, v, p = s.initialize(*tgv_init(StructuredMesh.from_config(cfg)))
+    for _ in range(warmup):
+        u, v, p = s.step(u, v, cfg.dt)
     setup = time.perf_counter() - t0
     t0 = time.perf_counter()
     for _ in range(steps):
         u, v, p = s.step(u, v, cfg.dt)
     el = time.perf_counter() - t0
     return {"value": N * N * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} RK3 steps of the 512x512 vortex after initialisation "
-                      f"({el:.1f} s; setup {setup:.1f} s excluded); NumPy/SciPy, one thread"}
+            "sample": f"{steps} RK3 steps of the 512x512 vortex after initialisation and {warmup} "
+                      f"untimed steps ({el:.1f} s; {setup:.1f} s before excluded); NumPy/SciPy, one thread"}
 
 
-def batch_cpu_baseline(cfgs, steps=1):
-    """The oracle on one cavity of each grid size of the batch (bounded sample),
-    extrapolated to the batch by cell count."""
+def batch_cpu_baseline(cfgs, steps=1, warmup=0):
+    """The oracle on one cavity of each grid size of the batch (bounded sample, after
+    `warmup` untimed steps per cavity), extrapolated to the batch by cell count."""
     from oracle import OracleSolver
     from oracle.projection import OracleStepper
     sample, seen = [], set()
@@ -253,6 +256,8 @@ def batch_cpu_baseline(cfgs, steps=1):
         s = OracleSolver(c)
         u, v, p = s.initialize()
         stp = OracleStepper(s)
+        for _ in range(warmup):
+            u, v, p = s.step(u, v, stp.compute_dt(u, v))
         t0 = time.perf_counter()
         for _ in range(steps):
             u, v, p = s.step(u, v, stp.compute_dt(u, v))
@@ -260,7 +265,8 @@ def batch_cpu_baseline(cfgs, steps=1):
         cells += c.nx * c.ny * steps
     return {"value": cells / el, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{steps} adaptive RK3 step(s) of one cavity per grid size "
-                      f"({', '.join(str(c.nx) for c in sample)}) after initialisation, "
+                      f"({', '.join(str(c.nx) for c in sample)}) after initialisation and {warmup} "
+                      f"untimed step(s), "
                       f"{el:.1f} s; NumPy/SciPy, one thread; batch figure = sample cells/s"}
 
 
@@ -578,9 +584,10 @@ def run_reference(args, world, rank):
     import torch  # noqa: F401  (same process layout as the GPU arm)
     if args.workload == "batch":
         from pycfd_b200.batch import cavity_batch_configs
-        cb = batch_cpu_baseline(cavity_batch_configs(count=args.batch, seed=0))
+        w = min(args.warmup, 3)
+        cb = batch_cpu_baseline(cavity_batch_configs(count=args.batch, seed=0), warmup=w)
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+                "steps": 1, "warmup": w, "ms_per_step": None, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "impl": "reference",
                 "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)"},
@@ -590,9 +597,10 @@ def run_reference(args, world, rank):
         print(json.dumps(line), flush=True)
         return
     steps = max(1, min(args.steps, 4))
-    cb = cpu_baseline(steps)
+    w = min(args.warmup, 3)   # each oracle step of the 512x512 vortex takes about a second
+    cb = cpu_baseline(steps, warmup=w)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": 0, "ms_per_step": 1e3 * N * N / cb["value"],
+            "steps": steps, "warmup": w, "ms_per_step": 1e3 * N * N / cb["value"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference", "config": workload_config(),
             "cpu_baseline": cb,
