@@ -244,8 +244,10 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
 int pycfd_set_clock(pycfd_solver* s, double t, void* stream);
 int pycfd_get_clock(pycfd_solver* s, double* t, double* dt, int* steps, int* health, void* stream);
 
-/* The same step on HOST buffers: copies the inputs in, steps, copies u, v, p
- * back, all on `stream`, and returns after the stream has finished. */
+/* The same step on HOST buffers: copies the inputs in, steps (the step is
+ * recorded on the first call and replayed after, as pycfd_step_graph), copies
+ * u, v, p back, all on `stream`, and returns after the stream has finished.
+ * Pinned host buffers make the copies asynchronous DMA. */
 int pycfd_step_host(pycfd_solver* s, const double* u0_host, const double* v0_host,
                     double* u_host, double* v_host, double* p_host, double dt, double blend,
                     void* stream);

@@ -1682,7 +1682,8 @@ int pycfd_step_host(pycfd_solver* s, const double* u0h, const double* v0h, doubl
   }
   CU(cudaMemcpyAsync(s->hu0, u0h, nu * sizeof(double), cudaMemcpyHostToDevice, sm));
   CU(cudaMemcpyAsync(s->hv0, v0h, nv * sizeof(double), cudaMemcpyHostToDevice, sm));
-  TRY(pycfd_step(s, s->hu0, s->hv0, s->hu, s->hv, s->hp, dt, blend, stream));
+  // the device buffers are the solver's own, so the recorded step is replayed
+  TRY(pycfd_step_graph(s, s->hu0, s->hv0, s->hu, s->hv, s->hp, dt, blend, stream));
   CU(cudaMemcpyAsync(uh, s->hu, nu * sizeof(double), cudaMemcpyDeviceToHost, sm));
   CU(cudaMemcpyAsync(vh, s->hv, nv * sizeof(double), cudaMemcpyDeviceToHost, sm));
   CU(cudaMemcpyAsync(ph, s->hp, np * sizeof(double), cudaMemcpyDeviceToHost, sm));

@@ -563,12 +563,23 @@ class ProjectionSolver:
         self.step(fields, dt)
         return int(self._L.pycfd_launch_count() - before)
 
-    def step_host(self, u0: np.ndarray, v0: np.ndarray, dt: float):
-        """The same step on host arrays: copies in, steps, copies ``(u, v, p)`` out."""
+    def step_host(self, u0: np.ndarray, v0: np.ndarray, dt: float, out=None):
+        """The same step on host arrays: copies in, steps, copies ``(u, v, p)`` out.
+
+        ``out``: three contiguous float64 arrays of the state shapes to write into
+        (pinned ones, e.g. ``torch.empty(...).pin_memory().numpy()``, make the copies
+        asynchronous DMA); new arrays otherwise.
+        """
         u0 = np.ascontiguousarray(u0, np.float64)
         v0 = np.ascontiguousarray(v0, np.float64)
-        u, v, p = (np.empty(self.mesh.u_shape), np.empty(self.mesh.v_shape),
-                   np.empty(self.mesh.p_shape))
+        if out is None:
+            u, v, p = (np.empty(self.mesh.u_shape), np.empty(self.mesh.v_shape),
+                       np.empty(self.mesh.p_shape))
+        else:
+            u, v, p = out
+            for a, shape in ((u, self.mesh.u_shape), (v, self.mesh.v_shape), (p, self.mesh.p_shape)):
+                if a.shape != tuple(shape) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError(f"out arrays must be contiguous float64 of shape {tuple(shape)}")
         _lib.check(self._L.pycfd_step_host(self._h, _lib.ptr(u0), _lib.ptr(v0), _lib.ptr(u),
                                            _lib.ptr(v), _lib.ptr(p), float(dt), float(self._blend),
                                            _stream()))

@@ -169,6 +169,27 @@ def test_rejected_configurations():
         ProjectionSolver(_cfg(base, pressure_solver="cg"), obstacle=np.zeros((4, 4), bool))
 
 
+@pytest.mark.parametrize("solver", ["cg", "mgcg", "sor"])
+def test_host_buffer_step_matches_device_step_bitwise(solver):
+    """pycfd_step_host (copies in, the recorded step, copies out) against the device step of
+    an identically prepared solver, over three steps (the first records, the rest replay)."""
+    from pycfd_b200.solver import GpuOptions
+    d = dict(nx=40, ny=32, re=100.0, pressure_solver=solver, poisson_tol=1e-12,
+             boundary_config=cases.bcs(top=("moving_wall", 1.0)))
+    a = _solver(_cfg(d), options=GpuOptions(graphs=False))
+    b = _solver(_cfg(d))
+    fa = a.initialize()
+    fb = b.initialize()
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64).pin_memory().numpy()
+    out = [(pin(fb.u.shape), pin(fb.v.shape), pin(fb.p.shape)) for _ in range(2)]
+    u, v = fb.u.cpu().numpy().copy(), fb.v.cpu().numpy().copy()
+    for k in range(3):
+        fa = a.step(fa, 2e-3)
+        u, v, p = b.step_host(u, v, 2e-3, out=out[k % 2])
+        ua, va, pa = fa.numpy()
+        assert np.array_equal(ua, u) and np.array_equal(va, v) and np.array_equal(pa, p), k
+
+
 @pytest.mark.parametrize("solver", ["cg", "mgcg", "multigrid"])
 def test_graph_replay_matches_eager_bitwise(solver):
     """A step recorded into a CUDA graph (device-side solve loops) replays the eager launches."""
