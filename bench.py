@@ -378,6 +378,18 @@ def run_batch(args, world, rank, local):
                                            "recorded steps replayed on 16 streams",
                  "dense_tail": args.plain_tail}
         del runner
+        # the same solvers one problem after another on one stream (a loop over the cavities)
+        runner = BatchRunner(cfgs, streams=1, options=popts)
+        runner.step(args.warmup)
+        torch.cuda.synchronize()
+        p0.record()
+        runner.step(k_plain)
+        p1.record()
+        torch.cuda.synchronize()
+        pms1 = p0.elapsed_time(p1)
+        plain["one_stream"] = {"value": b.cells * k_plain / (pms1 / 1e3), "ms_per_step": pms1 / k_plain,
+                               "form": "the same solvers, one problem after another on one stream"}
+        del runner
     if rank == 0:
         sizes = {}
         for c in cfgs:
