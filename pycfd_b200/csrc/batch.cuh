@@ -875,7 +875,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __r
       const bool done = conv || I[I_IR_IT] >= max_passes;
       I[I_CONVERGED] = conv;
       I[I_IR_DONE] = done;
-      S[S_ATOL] = inner_tol * sqrt(t[0]);
+      S[S_ATOL] = fmax(inner_tol * sqrt(t[0]), kIrLastFraction * tol * nb);   // as k_ir_residual
       S[S_RNORM2] = t[0];
       S[S_RHO_PREV] = 1.0;
       S[S_SUM_R] = t[1];

@@ -354,7 +354,12 @@ __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
 // One refinement pass: r = b - A x in FP64 (first pass: finalise b from the raw
 // right-hand side and take x from the warm start or zero), the outer stopping
 // rule ||r|| < tol ||b|| on this true residual, and the set-up of the inner
-// FP32 solve A e = r from e = 0 (r32 = r, inner atol = inner_tol ||r||).
+// FP32 solve A e = r from e = 0 (r32 = r).  The inner solve stops at
+// max(inner_tol ||r||, kIrLastFraction tol ||b||): a pass that only has to take
+// the residual the rest of the way to the outer target stops there instead of
+// reducing it by the full inner_tol (the outer test on the true residual stays
+// the judge).
+constexpr double kIrLastFraction = 0.5;
 __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
                               float* __restrict__ r32, float* __restrict__ e32,
                               const uint8_t* __restrict__ flags, Geo g, SolveCfg cfg,
@@ -398,7 +403,7 @@ __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
     I[I_CONVERGED] = conv;
     I[I_IR_DONE] = done;
     // inner solve from e = 0: its residual is r itself
-    S[S_ATOL] = inner_tol * sqrt(t[0]);
+    S[S_ATOL] = fmax(inner_tol * sqrt(t[0]), kIrLastFraction * cfg.tol * nb);
     S[S_RNORM2] = t[0];
     S[S_SUM_R] = t[1];
     S[S_MEAN_R] = g.n_fluid ? t[1] / g.n_fluid : 0.0;
