@@ -304,6 +304,10 @@ typedef struct {
     int coarse_level;   /* multigrid levels from this one down run in one thread
                            block per problem (one launch per V-cycle); 0: one
                            launch per phase on every level                      */
+    int fused_from;     /* with fused restrictions in the hierarchies: the first
+                           level restricted by R (I - A W) (1: from the fine level;
+                           2: the fine sweep and restriction stay separate); 0
+                           reads as 1                                           */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver

@@ -23,6 +23,7 @@ struct pycfd_batch {
   int maxiter = 1000, sweeps = 1, tile_i = 32;
   int coarse = 0;                          // levels >= coarse: one block per problem (0: per level)
   int fused = 0;                           // down sweep by fused restrictions (every structure has them)
+  int fused_from = 1;                      // first level restricted by the fused product (1 or 2)
   int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
@@ -313,7 +314,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
         const int rpb = kBThreads / lanes * kBEllRounds;
         for (int rb = 0; rb * rpb < nrow; ++rb) m.push_back(make_int2(i, rb));
       };
-      const int lres = B->fused ? H.lv[d].lm : H.lv[d].lr;   // lanes of the restriction into d
+      const int lres = (B->fused && d >= B->fused_from) ? H.lv[d].lm : H.lv[d].lr;   // lanes of the restriction into d
       if (t > 0 && d == t) {   // restriction into the tail level only
         add(mr, lres);
         continue;
@@ -412,9 +413,13 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
   const int sw = B->sweeps;
   const int D = B->coarse > 0 ? std::min(B->coarse, B->depth) : B->depth;   // depths run per level
   if (B->fused) {
-    // ---- down: b_d = M_d b_{d-1} at every depth above each problem's tail, then the tails
+    // ---- down: b_d = M_d b_{d-1} at every depth from fused_from above each problem's
+    // tail (below it the fine sweep and R), then the tails
+    const bool fine_kept = B->fused_from == 2;
+    if (fine_kept) TRY((b_fine<T, FM_PRE>(B, 0, 0, st)));
     for (int d = 1; d < D; ++d) {
-      TRY((b_ell<T, EO_FRESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+      if (d < B->fused_from) TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+      else TRY((b_ell<T, EO_FRESTRICT>(B, B->mapR[d], d, 0, 0, st)));
       if (B->mapT[d].n) {
         b_prof(B, 4, st);
         BLAUNCH(k_b_tail<T>, B->mapT[d].n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT[d].e,
@@ -428,7 +433,8 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
       TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[d], d, 1, 0, st)));
       TRY((b_ell<T, EO_SMOOTH>(B, B->mapA[d], d, 0, 1, st)));
     }
-    TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[0], 0, 1, 0, st)));
+    if (fine_kept) TRY((b_ell<T, EO_PROLONG>(B, B->mapP[0], 0, 1, 0, st)));   // x_0 stored by FM_PRE
+    else TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[0], 0, 1, 0, st)));
     TRY((b_fine<T, FM_LAST>(B, 0, 2, st)));
     return 0;
   }
@@ -721,6 +727,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   if (opts->tile_rows != 8 && opts->tile_rows != 16 && opts->tile_rows != 32 && opts->tile_rows != 64)
     return fail(PCFD_E_ARG, "tile_rows must be 8, 16, 32 or 64");
   if (opts->mg_sweeps < 1 || opts->mg_sweeps > 4) return fail(PCFD_E_ARG, "mg_sweeps must be 1..4");
+  if (opts->fused_from < 0 || opts->fused_from > 2) return fail(PCFD_E_ARG, "fused_from must be 0, 1 or 2");
   if (opts->coarse_level < 0 || opts->coarse_level >= kBMaxLevels)
     return fail(PCFD_E_ARG, "coarse_level must be 0..%d", kBMaxLevels - 1);
   if (!(opts->tol > 0) || opts->maxiter < 1) return fail(PCFD_E_ARG, "bad tolerance or iteration limit");
@@ -738,6 +745,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->sweeps = opts->mg_sweeps;
   B->tile_i = opts->tile_rows;
   B->coarse = opts->coarse_level;
+  B->fused_from = opts->fused_from == 2 ? 2 : 1;
   B->mem = new pycfd_solver();
   B->solvers.assign(n, nullptr);
   for (int i = 0; i < n; ++i) {

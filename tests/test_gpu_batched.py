@@ -190,18 +190,21 @@ def test_dense_tail_matches_level_by_level(precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_restriction_matches_two_phase_down_sweep(precision):
-    """The down sweep by fused restrictions R (I - A W) against restriction + first sweep."""
+    """The down sweep by fused restrictions R (I - A W) -- from the fine level, or from
+    level 2 with the fine sweep and restriction kept -- against restriction + first sweep."""
     from pycfd_b200.batch import BatchedSolver, BatchOptions
     cfgs = _cavities(count=7, seed=4)
     out = []
-    for fused in (True, False):
+    for fused, start in ((True, 1), (True, 2), (False, 1)):
         # unbounded tail: these small cavities all get one (a tail bound would leave them none)
-        b = BatchedSolver(cfgs, BatchOptions(precision=precision, fused_restriction=fused, tail_ratio=None))
+        b = BatchedSolver(cfgs, BatchOptions(precision=precision, fused_restriction=fused, fused_from=start,
+                                             tail_ratio=None))
         assert b._fused == fused
         b.step(6)
         out.append([b.fields[k].numpy() for k in range(len(cfgs))])
         assert all(f == 0 for f in b.status()["frozen"])
     bound = 1e-9 if precision == "fp64" else 1e-7
-    for fa, fb in zip(*out):
-        for x, y in zip(fa[:2], fb[:2]):
-            assert rel(x, y) < bound
+    for k in (0, 1):
+        for fa, fb in zip(out[k], out[2]):
+            for x, y in zip(fa[:2], fb[:2]):
+                assert rel(x, y) < bound
