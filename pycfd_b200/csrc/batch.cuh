@@ -1238,9 +1238,10 @@ __global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict_
   }
 }
 
-// Dense close of the V-cycle at depth d: x_d = M b_d for the problems whose
-// structure's tail is at d, M the structure's operator (n x n, row-major; the
-// cycle at and below d as one linear map).  A block takes kBTailRows rows of M
+// Dense close of the V-cycle: x_t = M b_t for every problem whose structure has
+// a tail, t the structure's tail depth and M its operator (n x n, row-major; the
+// cycle at and below t as one linear map).  One launch after the down sweep
+// covers every structure, whatever its tail depth.  A block takes kBTailRows rows of M
 // (one warp each) for a group of kBTailGroup problems of one structure: each
 // lane loads its entries of M once and applies them to every problem of the
 // group (independent accumulators), so M crosses from L2 once per group and a
@@ -1259,9 +1260,10 @@ template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_tail(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map,
-                                                       const int* __restrict__ sprobs, int d, BShared sh) {
+                                                       const int* __restrict__ sprobs, BShared sh) {
   const int2 e = map[blockIdx.x];   // (structure, row block * 64 + problem group)
   const BHier<T>& H = hiers[e.x];
+  const int d = H.tail_level;
   const int n = H.tail_n;
   const int rb = e.y >> 6, grp = e.y & 63;
   __shared__ const T* sb[kBTailGroup];

@@ -36,7 +36,7 @@ struct pycfd_batch {
   std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
   std::vector<BMapHost> mapR;              // restriction into d (+ coarsest blocks when coarse == 0)
   std::vector<BMapHost> mapP;              // prolongation into d with P_{d+1}
-  std::vector<BMapHost> mapT;              // dense tail at d: (structure, row block x 64 + problem group)
+  BMapHost mapT;                           // dense tails: (structure, row block x 64 + problem group)
   int* sprobs = nullptr;                   // problems grouped by structure
   size_t smem_dense = 0;
   BShared sh{};
@@ -283,9 +283,9 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   B->mapA.assign(B->depth, BMapHost{});
   B->mapR.assign(B->depth, BMapHost{});
   B->mapP.assign(B->depth, BMapHost{});
-  B->mapT.assign(B->depth, BMapHost{});
+  std::vector<int2> mt;
   for (int d = 0; d < B->depth; ++d) {
-    std::vector<int2> ma, mr, mp, mt;
+    std::vector<int2> ma, mr, mp;
     for (size_t h = 0; h < leaders.size(); ++h) {
       if (hh[h].tail_level != d || hh[h].tail_n == 0) continue;
       const int rbs = (hh[h].tail_n + kBTailRows - 1) / kBTailRows;
@@ -328,8 +328,8 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     TRY(upload_map(B, &B->mapA[d], ma));
     TRY(upload_map(B, &B->mapR[d], mr));
     TRY(upload_map(B, &B->mapP[d], mp));
-    TRY(upload_map(B, &B->mapT[d], mt));
   }
+  TRY(upload_map(B, &B->mapT, mt));
   {
     std::vector<int> ord(n);
     for (int i = 0; i < n; ++i) ord[i] = i;
@@ -405,6 +405,17 @@ int b_fine(pycfd_batch* B, int src, int dst, cudaStream_t st) {
   return 0;
 }
 
+// The dense tails of every tailed structure, one launch after the down sweep
+// (each block reads its structure's tail depth).
+template <class T>
+int b_tails(pycfd_batch* B, cudaStream_t st) {
+  if (B->mapT.n == 0) return 0;
+  b_prof(B, 4, st);
+  BLAUNCH(k_b_tail<T>, B->mapT.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT.e, B->sprobs, B->sh);
+  b_prof(B, 4, st);
+  return 0;
+}
+
 // One V-cycle from zero on every solving problem, levels in lockstep by depth:
 // z <- M r, with mean(z) and r.z left in each problem's scalar block.  With
 // B->coarse > 0 the levels from there down run in one block per problem.
@@ -420,13 +431,8 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
     for (int d = 1; d < D; ++d) {
       if (d < B->fused_from) TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
       else TRY((b_ell<T, EO_FRESTRICT>(B, B->mapR[d], d, 0, 0, st)));
-      if (B->mapT[d].n) {
-        b_prof(B, 4, st);
-        BLAUNCH(k_b_tail<T>, B->mapT[d].n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT[d].e,
-                B->sprobs, d, B->sh);
-        b_prof(B, 4, st);
-      }
     }
+    TRY(b_tails<T>(B, st));
     // ---- up: x_d = W b_d + P x_{d+1} into xa, one sweep into xb
     for (int d = D - 2; d >= 1; --d) {
       if (B->mapA[d].n == 0) continue;
@@ -455,12 +461,6 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
   std::vector<int> cur(B->depth + 1, 0), fin(B->depth + 1, 0);
   for (int d = 1; d < D; ++d) {
     TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
-    if (B->mapT[d].n) {
-      b_prof(B, 4, st);
-      BLAUNCH(k_b_tail<T>, B->mapT[d].n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT[d].e, B->sprobs,
-              d, B->sh);
-      b_prof(B, 4, st);
-    }
     if (B->mapA[d].n == 0) continue;
     TRY((b_ell<T, EO_PRE>(B, B->mapA[d], d, 0, 0, st)));
     int a = 0, o = 1;
@@ -473,6 +473,7 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
     }
     cur[d] = a;
   }
+  TRY(b_tails<T>(B, st));
   if (B->coarse > 0) {
     b_prof(B, 4, st);
     BLAUNCH(k_b_coarse<T>, B->n, kBCoarseThreads, B->smem_dense, st, probs_of<T>(B), B->order, B->coarse, sw,
