@@ -129,7 +129,7 @@ typedef struct {
     const double* tail_operator;              /* n_l x n_l row-major, x_l = M b_l   */
     int ell_thread_budget;                    /* resident threads one coarse-level pass
                                                  may spread its rows over (lanes per row
-                                                 follow from it); 0 = 5 blocks of 256 per
+                                                 follow from it); 0 = 8 blocks of 256 per
                                                  SM, -1 = the storage lane count   */
 } pycfd_solver_desc;
 

@@ -1179,8 +1179,9 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   {
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    // default: five resident 256-thread blocks per SM (the ELL kernels keep <= 48 registers)
-    s->ell_budget = d->ell_thread_budget ? (long)d->ell_thread_budget : (long)nsm * 5 * 256;
+    // default: eight 256-thread blocks per SM (measured best of 4..12 on the 512^2 vortex;
+    // with the ELL kernels' <= 48 registers five are resident, the rest follow as they end)
+    s->ell_budget = d->ell_thread_budget ? (long)d->ell_thread_budget : (long)nsm * 8 * 256;
     s->ell_blocks = s->ell_budget > 0 ? (int)std::max<long>(1, s->ell_budget / 256) : kWaveBlocks;
   }
 

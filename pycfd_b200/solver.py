@@ -64,7 +64,7 @@ class GpuOptions:
     #: level.
     fused_restriction: bool = True
     #: resident threads a coarse-level pass may spread its rows over (lanes per
-    #: row follow from it); 0 = five 256-thread blocks per SM, -1 = the lane
+    #: row follow from it); 0 = eight 256-thread blocks per SM, -1 = the lane
     #: count of the stored layout.
     ell_thread_budget: int = 0
 
