@@ -79,3 +79,31 @@ def test_tail_level_rule():
     # a grid with no level above the coarsest gets no tail
     small, _ = _hierarchy(8, True)
     assert tail_level(small) == 0
+
+
+@pytest.mark.parametrize("tail,ratio,fused,sweeps", [(True, None, True, 1), (True, 4.0, True, 1),
+                                                     (True, None, False, 1), (True, None, True, 2),
+                                                     (False, None, True, 1)])
+def test_solver_descriptor_carries_the_cycle_options(tail, ratio, fused, sweeps):
+    """The options reach the native descriptor: the tail level and its operator, and the
+    fused restrictions onto levels 1..tail (one sweep per level only)."""
+    import cases
+    from pycfd_b200.config import BCKind, BCSpec, PressureSolver, SimulationConfig
+    from pycfd_b200.mesh import StructuredMesh
+    from pycfd_b200.solver import BoundaryInfo, GpuOptions, native_desc
+    from pycfd_b200.hierarchy import hierarchy_for
+    cfg = cases.to_config(dict(nx=128, ny=128, re=100.0, pressure_solver="mgcg", mg_sweeps=sweeps,
+                               boundary_config=cases.bcs(top=("moving_wall", 1.0))),
+                          SimulationConfig, BCSpec, BCKind)
+    mesh = StructuredMesh.from_config(cfg)
+    bnd = BoundaryInfo(cfg.boundary_config, mesh)
+    solid = np.zeros(mesh.shape, bool)
+    _, (levels, cinv) = hierarchy_for(cfg.nx, cfg.ny, mesh.dx, mesh.dy, False, False, None, {})
+    opts = GpuOptions(coarse_tail=tail, tail_ratio=ratio, fused_restriction=fused)
+    d, keep = native_desc(cfg, mesh, bnd, solid, False, (), PressureSolver.MGCG, opts, levels, cinv)
+    expect = tail_level(levels, ratio) if tail else 0
+    assert d.tail_level == expect
+    assert bool(d.tail_operator) == (expect > 0)
+    for l in range(1, d.n_levels):
+        has_m = bool(d.levels[l].m_indptr)
+        assert has_m == (expect > 0 and fused and sweeps == 1 and l <= expect), l
