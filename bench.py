@@ -241,353 +241,73 @@ def cpu_baseline(steps=3, warmup=0):
                       f"untimed steps ({el:.1f} s; {setup:.1f} s before excluded); NumPy/SciPy, one thread"}
 
 
-def batch_cpu_baseline(cfgs, steps=1, warmup=0):
-    """The oracle on one cavity of each grid size of the batch (bounded sample, after
-    `warmup` untimed steps per cavity), extrapolated to the batch by cell count."""
+def host_cores():
+    """Host threads this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _oracle_cavity(cfg, warmup, steps, barrier, out):
+    """One worker process: the oracle's adaptive RK3 steps of one cavity.  Set-up and
+    `warmup` steps untimed; then wait at the barrier, so all workers time together."""
     from oracle import OracleSolver
     from oracle.projection import OracleStepper
-    sample, seen = [], set()
+    s = OracleSolver(cfg)
+    u, v, p = s.initialize()
+    stp = OracleStepper(s)
+    for _ in range(warmup):
+        u, v, p = s.step(u, v, stp.compute_dt(u, v))
+    barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u, v, p = s.step(u, v, stp.compute_dt(u, v))
+    out.put((cfg.nx * cfg.ny * steps, time.perf_counter() - t0, time.time()))
+
+
+def batch_cpu_baseline(cfgs, steps=1, warmup=0, workers=None):
+    """The oracle (the reference's algorithm restated in NumPy/SciPy) on the host cores:
+    one single-threaded process per cavity, `workers` cavities at once (default all
+    host threads, capped by the batch), drawn round-robin over the grid sizes so the
+    sample keeps the batch's size mix.  Every process sets up and runs `warmup`
+    untimed steps, then all time `steps` steps together (barrier); value = the
+    sample's cell-updates / the wall time from the barrier to the last finisher."""
+    import multiprocessing as mp
+    by_size = {}
     for c in cfgs:
-        if c.nx not in seen:
-            seen.add(c.nx)
-            sample.append(c)
-    cells = el = 0.0
+        by_size.setdefault(c.nx, []).append(c)
+    order = []
+    while any(by_size.values()):
+        for n in sorted(by_size):
+            if by_size[n]:
+                order.append(by_size[n].pop(0))
+    cores = host_cores()
+    workers = min(workers or cores, len(order), cores)
+    sample = order[:workers]
+    for var in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS", "NUMBA_NUM_THREADS"):
+        os.environ[var] = "1"   # one thread per process, inherited by the spawned workers
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(workers + 1)
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_oracle_cavity, args=(c, warmup, steps, barrier, out)) for c in sample]
+    for pr in procs:
+        pr.start()
+    barrier.wait(timeout=900)
+    t0 = time.time()
+    res = [out.get(timeout=1800) for _ in procs]
+    for pr in procs:
+        pr.join(timeout=60)
+    wall = max(r[2] for r in res) - t0
+    cells = sum(r[0] for r in res)
+    sizes = {}
     for c in sample:
-        s = OracleSolver(c)
-        u, v, p = s.initialize()
-        stp = OracleStepper(s)
-        for _ in range(warmup):
-            u, v, p = s.step(u, v, stp.compute_dt(u, v))
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            u, v, p = s.step(u, v, stp.compute_dt(u, v))
-        el += time.perf_counter() - t0
-        cells += c.nx * c.ny * steps
-    return {"value": cells / el, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{steps} adaptive RK3 step(s) of one cavity per grid size "
-                      f"({', '.join(str(c.nx) for c in sample)}) after initialisation and {warmup} "
-                      f"untimed step(s), "
-                      f"{el:.1f} s; NumPy/SciPy, one thread; batch figure = sample cells/s"}
-
-
-def run_batch(args, world, rank, local):
-    """256 seeded lid-driven cavities of uneven size, Re and lid speed: the batched engine
-    (every stage one launch over the whole batch), with the plain FP64 path -- one
-    single-problem solver per cavity, graphs replayed on a pool of streams -- beside it."""
-    import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-    from pycfd_b200 import _lib
-    from pycfd_b200.batch import (BatchAutotuner, BatchedSolver, BatchOptions, BatchRunner,
-                                  cavity_batch_configs)
-    from pycfd_b200.solver import GpuOptions
-    cfgs = cavity_batch_configs(count=args.batch, seed=0)
-    t0 = time.perf_counter()
-    if args.autotune:
-        opts = BatchAutotuner(allowed_precisions=(args.precision,)).choose(cfgs)
-    else:
-        tail = args.batch_tail
-        opts = BatchOptions(precision=args.precision, tile_rows=args.tile_rows,
-                            mg_sweeps=args.mg_sweeps, inner_tol=args.inner_tol,
-                            coarse_level=args.coarse_level, coarse_tail=tail != "off",
-                            tail_ratio=None if tail in ("none", "off") else float(tail))
-    b = BatchedSolver(cfgs, opts)
-    setup = time.perf_counter() - t0
-    rec = not args.eager
-    b.step(args.warmup, record=rec)
-    torch.cuda.synchronize()
-    b.launches(0)
-    n_launch0 = _lib.load().pycfd_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clocks = Clocks(local) if rank == 0 else None
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0.record()
-    b.step(args.steps, record=rec)
-    ev1.record()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ck = clocks.stop() if clocks else None
-    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
-    launches = b.launches(args.steps) if rec else int(_lib.load().pycfd_launch_count() - n_launch0)
-    value = world * b.cells * args.steps / (ms / 1e3)
-    st = b.status()
-    its = st["iterations"]
-    max_div = max(b.field_stats(k).max_div for k in range(len(b)))
-    # roofline: the batched CG direction kernel over one eager step
-    s_bytes = 4 if opts.precision == "mixed" else 8
-    pq_ms, pq_n, pq_its = b.profile(1)
-    cells = np.array([c.nx * c.ny for c in cfgs], dtype=np.float64)
-    pq_bytes = float((pq_its * cells).sum()) * (4 * s_bytes + 1)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except Exception:
-        pass
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    achieved = pq_bytes / (pq_ms / 1e3) / 1e9 if pq_ms > 0 else None
-    traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
-        traffic = prof.get("batch_" + opts.precision, {}).get("1")
-    except Exception:
-        pass
-    roof = {"bound": "hbm", "kernel": "k_b_cg_pq (batched CG direction p = z + beta p, q = A p, p.q)",
-            "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "traffic": traffic,
-            "bytes_per_launch": pq_bytes / max(pq_n, 1), "us_per_launch": 1e3 * pq_ms / max(pq_n, 1),
-            "launches": pq_n, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-            "timing": "CUDA events around each eager launch over one step; bytes = sum over "
-                      "problems of CG iterations x cells x (4 vectors x element + 1 flag byte)"}
-    # end to end: (u, v) of every cavity from pinned host memory, one step, (u, v, p) back
-    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
-    e2e = None
-    if e2e_steps:
-        b.step_host(1)
-        t0 = time.perf_counter()
-        b.step_host(e2e_steps)
-        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-        h2d, d2h = b.state_bytes()
-        e2e = {"value": world * b.cells * e2e_steps / e2e_s, "unit": UNIT,
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
-    plain = None
-    if not args.no_plain:
-        # the plain FP64 path on the same batch: per-problem recorded steps on 16 streams
-        popts = {"auto": GpuOptions(precision="fp64"),
-                 "compact": GpuOptions(precision="fp64", tail_ratio=4.0),
-                 "off": GpuOptions(precision="fp64", coarse_tail=False)}[args.plain_tail]
-        runner = BatchRunner(cfgs, streams=16, options=popts)
-        # the same steps of the flow as the batched leg: W untimed, then K timed
-        runner.step(args.warmup)
-        torch.cuda.synchronize()
-        k_plain = args.steps
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        p0.record()
-        runner.step(k_plain)
-        p1.record()
-        torch.cuda.synchronize()
-        pms = p0.elapsed_time(p1)
-        plain = {"value": b.cells * k_plain / (pms / 1e3), "ms_per_step": pms / k_plain,
-                 "steps": k_plain, "form": "fp64, one single-problem solver per cavity, "
-                                           "recorded steps replayed on 16 streams",
-                 "dense_tail": args.plain_tail}
-        del runner
-        # the same solvers one problem after another on one stream (a loop over the cavities)
-        runner = BatchRunner(cfgs, streams=1, options=popts)
-        runner.step(args.warmup)
-        torch.cuda.synchronize()
-        p0.record()
-        runner.step(k_plain)
-        p1.record()
-        torch.cuda.synchronize()
-        pms1 = p0.elapsed_time(p1)
-        plain["one_stream"] = {"value": b.cells * k_plain / (pms1 / 1e3), "ms_per_step": pms1 / k_plain,
-                               "form": "the same solvers, one problem after another on one stream"}
-        del runner
-    if rank == 0:
-        sizes = {}
-        for c in cfgs:
-            sizes[str(c.nx)] = sizes.get(str(c.nx), 0) + 1
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64/f32" if opts.precision == "mixed" else "f64", "data": "synthetic",
-                "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)",
-                           "cells": b.cells, "sizes": sizes, "re": "log-uniform 100..2000",
-                           "lid": "uniform 0.5..1.5", "pressure_solver": "mgcg",
-                           "poisson_tol": cfgs[0].poisson_tol, "dt": "adaptive, CFL 0.5, per cavity",
-                           "options": opts.__dict__, "autotuned": bool(args.autotune),
-                           "setup_s": setup, "structures": b.structures,
-                           "cg_iterations_per_step": float(np.mean(its)),
-                           "stopped": int((st["frozen"] != 0).sum()), "max_div": max_div,
-                           "parallelism": f"replicas x{world}",
-                           "l2": "working set larger than L2 (no flush needed)",
-                           "cell_update": "one cell advanced by one RK3 step, summed over the batch",
-                           "plain_fp64_path": plain},
-                "e2e": e2e, "clocks": ck, "roofline": roof, "gpu_launches": launches}
-        if not args.no_cpu_baseline:
-            line["cpu_baseline"] = batch_cpu_baseline(cfgs)
-        print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
-
-
-def run_tgv_validation(args, local):
-    """The 512x512 vortex over 500 steps in the FP64 path and in the mixed form: error of
-    each against the analytic decay (u, v ~ exp(-2 nu t), p ~ exp(-4 nu t), mean-free)
-    and of the mixed form against FP64."""
-    import torch
-    torch.cuda.set_device(local)
-    from pycfd_b200.solver import GpuOptions, ProjectionSolver
-    cfg = tgv_config()
-    steps = args.val_steps
-    out, fields = {}, {}
-    for prec in ("fp64", "mixed"):
-        s = ProjectionSolver(cfg, options=GpuOptions(precision=prec))
-        f = s.initialize(*tgv_init(s.mesh))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record()
-        for _ in range(steps):
-            f = s.advance(f, cfg.dt)
-        b.record()
-        torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / steps
-        t = steps * cfg.dt
-        nu = cfg.nu
-        Xu, Yu = s.mesh.u_grid()
-        Xv, Yv = s.mesh.v_grid()
-        ue = np.sin(Xu) * np.cos(Yu) * np.exp(-2 * nu * t)
-        ve = -np.cos(Xv) * np.sin(Yv) * np.exp(-2 * nu * t)
-        xc, yc = s.mesh.xc, s.mesh.yc
-        pe = 0.25 * (np.cos(2 * xc)[:, None] + np.cos(2 * yc)[None, :]) * np.exp(-4 * nu * t)
-        pe -= pe.mean()
-        u = f.u_phys.cpu().numpy()
-        v = f.v_phys.cpu().numpy()
-        p = f.p[1:-1, 1:-1].cpu().numpy()
-        p = p - p.mean()
-        st = s.field_stats(f)
-        fields[prec] = (u, v, p)
-        out[prec] = {"ms_per_step": ms, "cell_updates_per_s": N * N / (ms / 1e3),
-                     "err_u": float(np.abs(u - ue).max() / np.abs(ue).max()),
-                     "err_v": float(np.abs(v - ve).max() / np.abs(ve).max()),
-                     "err_p": float(np.abs(p - pe).max() / np.abs(pe).max()), "max_div": st.max_div}
-        del s
-    uf, vf, pf = fields["fp64"]
-    um, vm, pm = fields["mixed"]
-    scale = max(np.abs(uf).max(), np.abs(vf).max())
-    out["mixed_vs_fp64"] = {"velocity": float(max(np.abs(um - uf).max(), np.abs(vm - vf).max()) / scale),
-                            "pressure": float(np.abs(pm - pf).max() / np.abs(pf).max())}
-    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
-            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config({"validation": out, "t_end": steps * cfg.dt})}
-    print(json.dumps(line), flush=True)
-
-
-def run_cylinder(args, local):
-    """Flow past a cylinder on the 2048x1024 channel (Re 100, D 0.1 at (0.5, 0.5), uniform
-    inflow 1, convective outlet, slip walls, 1e-3 seeded noise), MG-PCG 1e-10, adaptive dt:
-    Cd and Cl histories in the FP64 path and in the mixed form."""
-    import torch
-    torch.cuda.set_device(local)
-    from pycfd_b200.config import BCKind, BCSpec, SimulationConfig
-    from pycfd_b200.mesh import StructuredMesh
-    from pycfd_b200.obstacles import circle_mask
-    from pycfd_b200.solver import GpuOptions, ProjectionSolver
-    nx, ny = 2048, 1024
-    walls = {"left": BCSpec(BCKind.INLET, velocity=1.0), "right": BCSpec(BCKind.OUTLET),
-             "bottom": BCSpec(BCKind.SYMMETRY), "top": BCSpec(BCKind.SYMMETRY)}
-    cfg = SimulationConfig(nx=nx, ny=ny, lx=2.0, ly=1.0, re=100.0, u_ref=1.0, l_ref=0.1, dt=1.0,
-                           t_end=1e9, cfl_max=0.5, pressure_solver="mgcg", poisson_tol=1e-10,
-                           boundary_config=walls, name="cylinder")
-    mesh = StructuredMesh.from_config(cfg)
-    obstacle = circle_mask(mesh, (0.5, 0.5), 0.05)
-    rng = np.random.default_rng(0)
-    u0 = 1.0 + 1e-3 * rng.standard_normal((nx + 1, ny))
-    v0 = 1e-3 * rng.standard_normal((nx, ny + 1))
-    steps, every = args.cyl_steps, 20
-    out = {}
-    for prec in ("fp64", "mixed"):
-        s = ProjectionSolver(cfg, mesh, obstacle, options=GpuOptions(precision=prec))
-        f = s.initialize(u0, v0)
-        s.set_clock(0.0)
-        ts, cd, cl = [], [], []
-        dev_ms = 0.0
-        for k in range(steps // every):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            for _ in range(every):
-                f = s.advance_adaptive(f)
-            b.record()
-            torch.cuda.synchronize()
-            dev_ms += a.elapsed_time(b)
-            st = s._read_stats()
-            t, dt, n, h = s.clock()
-            if h:
-                break
-            ts.append(t)
-            cd.append(st.fx / 0.05)
-            cl.append(st.fy / 0.05)
-        ts, cd, cl = np.array(ts), np.array(cd), np.array(cl)
-        half = ts >= 0.5 * ts[-1]
-        clh = cl[half] - cl[half].mean()
-        crossings = np.where(np.diff(np.sign(clh)) > 0)[0]
-        st_num = None
-        if len(crossings) >= 2:
-            period = (ts[half][crossings[-1]] - ts[half][crossings[0]]) / (len(crossings) - 1)
-            st_num = 0.1 / period
-        fs = s.field_stats(f)
-        out[prec] = {"steps": int(n), "t_end": float(ts[-1]), "ms_per_step": dev_ms / max(n, 1),
-                     "cell_updates_per_s": nx * ny * n / (dev_ms / 1e3),
-                     "cd_mean_second_half": float(cd[half].mean()), "cl_amplitude_second_half":
-                     float(0.5 * (cl[half].max() - cl[half].min())), "strouhal": st_num,
-                     "max_div": fs.max_div, "health": int(h),
-                     "cd_every_20": [round(float(x), 6) for x in cd[::10]],
-                     "cl_every_20": [round(float(x), 6) for x in cl[::10]]}
-        del s
-    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
-            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cylinder channel 2048x1024, Re 100", "runs": out}}
-    print(json.dumps(line), flush=True)
-
-
-def run_adjoint(args, world, rank, local):
-    """Gradient of the lower-half kinetic energy of the 256x256 Re 400 cavity after 200
-    steps w.r.t. 32 lid modes and the smoothed-disk radius: hand-written adjoint with
-    10-step checkpoints, checked against central differences (h = 1e-6) on 3 components."""
-    import torch
-    torch.cuda.set_device(local)
-    from pycfd_b200.adjoint import AdjointCavity, Geometry, MultigridSolve, gradient, rollout
-    cav = AdjointCavity()
-    g = Geometry(cav, device="cuda")
-    solve = MultigridSolve(cav.n, tol=cav.tol)
-    theta = torch.tensor(cav.default_theta(), dtype=torch.float64, device="cuda")
-    radius = torch.tensor(cav.radius, dtype=torch.float64, device="cuda")
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    solve.calls = 0
-    J, gt, gr = gradient(theta, radius, g, solve)
-    torch.cuda.synchronize()
-    t_grad = time.perf_counter() - t0
-    grad_solves = solve.calls
-    t0 = time.perf_counter()
-    J0, _ = rollout(theta, radius, g, solve)
-    torch.cuda.synchronize()
-    t_fwd = time.perf_counter() - t0
-    h = 1e-6
-    checks = []
-    with torch.no_grad():
-        for k in (0, 7):
-            e = torch.zeros_like(theta)
-            e[k] = h
-            fd = float((rollout(theta + e, radius, g, solve)[0] - rollout(theta - e, radius, g, solve)[0]) / (2 * h))
-            checks.append({"param": f"theta_{k + 1}", "adjoint": float(gt[k]), "fd": fd,
-                           "rel_err": abs(fd - float(gt[k])) / max(abs(fd), 1e-300)})
-        fd = float((rollout(theta, radius + h, g, solve)[0] - rollout(theta, radius - h, g, solve)[0]) / (2 * h))
-        checks.append({"param": "radius", "adjoint": float(gr), "fd": fd,
-                       "rel_err": abs(fd - float(gr)) / max(abs(fd), 1e-300)})
-    cells = cav.n * cav.n
-    line = {"metric": "gradient of J (lower-half kinetic energy) w.r.t. 33 parameters, adjoint",
-            "value": cells * cav.steps / t_grad, "unit": "cell-updates/s (forward + adjoint sweep)",
-            "n_gpus": 1, "steps": cav.steps, "warmup": 0, "ms_per_step": 1e3 * t_grad / cav.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "lid-driven cavity 256x256, Re 400, 200 steps, dt 1.2e-3, "
-                                   "32 sine lid modes (seeded) + tanh disk radius at (0.5, 0.3), "
-                                   "r 0.08, width 2 cells",
-                       "poisson_tol": cav.tol, "checkpoint_every": cav.checkpoint,
-                       "J": float(J), "forward_s": t_fwd, "gradient_s": t_grad,
-                       "gradient_over_forward": t_grad / t_fwd, "poisson_solves_in_gradient": grad_solves,
-                       "fd_checks": checks, "max_fd_rel_err": max(c["rel_err"] for c in checks)}}
-    print(json.dumps(line), flush=True)
+        sizes[c.nx] = sizes.get(c.nx, 0) + 1
+    return {"value": cells / wall, "unit": UNIT, "cores": workers, "kind": "port",
+            "host_threads": cores, "wall_s": wall, "steps": steps,
+            "sample": f"{workers} cavities of the batch (by grid size: {sizes}), one single-threaded "
+                      f"NumPy/SciPy process each, {steps} adaptive RK3 step(s) each after set-up and "
+                      f"{warmup} untimed step(s), timed together ({wall:.1f} s wall)"}
 
 
 def run_reference(args, world, rank):
@@ -596,13 +316,17 @@ def run_reference(args, world, rank):
     import torch  # noqa: F401  (same process layout as the GPU arm)
     if args.workload == "batch":
         from pycfd_b200.batch import cavity_batch_configs
+        # the 256 cavities of one GPU's share at N = 1; each timed step of this arm is one
+        # RK3 step of as many of them as there are host threads, all processes at once
         w = min(args.warmup, 3)
-        cb = batch_cpu_baseline(cavity_batch_configs(count=args.batch, seed=0), warmup=w)
+        k = max(1, min(args.steps, 5))
+        cb = batch_cpu_baseline(cavity_batch_configs(count=args.batch, seed=0), steps=k, warmup=w)
         line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-                "steps": 1, "warmup": w, "ms_per_step": None, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "impl": "reference",
-                "config": {"workload": f"batch of {args.batch} lid-driven cavities (seed 0)"},
+                "steps": k, "warmup": w, "ms_per_step": 1e3 * cb["wall_s"] / k,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": f"batch of {args.batch} lid-driven cavities per GPU (seed 0)",
+                           "sample": cb["sample"]},
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -730,9 +454,12 @@ def main():
                     help="tgv512: resident threads per coarse-level pass (0 default, -1 storage lanes)")
     ap.add_argument("--no-tail", action="store_true",
                     help="tgv512: V-cycle level by level down to the coarsest (no dense tail operator)")
-    ap.add_argument("--workload", default="tgv512",
+    ap.add_argument("--workload", default="batch",
                     choices=["tgv512", "batch", "adjoint", "tgv-validation", "cylinder"],
-                    help="tgv512: the headline single-domain workload; batch: seeded cavity batch")
+                    help="batch: the seeded 256-cavity batch (the headline); tgv512: the 512x512 "
+                         "vortex on the single-problem path")
+    ap.add_argument("--spinup", type=int, default=0,
+                    help="batch: untimed steps before the warm-up (later steps of the same flow)")
     ap.add_argument("--batch", type=int, default=256, help="problems in the batch workload")
     ap.add_argument("--val-steps", type=int, default=500, help="tgv-validation: steps")
     ap.add_argument("--cyl-steps", type=int, default=20000, help="cylinder: steps per precision")

@@ -263,6 +263,14 @@ int pycfd_profile_kernel(pycfd_solver* s, int kernel_id);
 /* CTAs of the cooperative launch that runs each CG / MG-PCG solve whole
  * (0: the solver launches one kernel per phase). */
 int pycfd_solver_persistent(pycfd_solver* s, int* ctas);
+/* No counterpart in the reference (failure detection of the persistent solve).
+ * Limit, in nanoseconds, of one grid-barrier wait of the cooperative solve
+ * (default 2 s).  A CTA that waits longer sets the launch's error word; every
+ * CTA then leaves its waits, the kernel ends, and the solve reports status -6
+ * (pycfd_get_stats) -- the context stays usable.  Applies to solves launched
+ * after the call (a step graph recorded earlier keeps the limit it was recorded
+ * with).  PCFD_E_UNSUPPORTED when the solver runs one kernel per phase. */
+int pycfd_solver_set_wait_limit(pycfd_solver* s, unsigned long long ns);
 /* Phase trace of the persistent solve (measurement support).  enable 1 turns
  * it on (each later solve overwrites it), 0 off, -1 leaves it as it is.  With
  * out != NULL: waits for `stream`, then copies the last solve's trace -- out[0]
@@ -277,6 +285,47 @@ int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* s
 
 /* Results of the last solve/step (synchronises `stream`). */
 int pycfd_get_stats(pycfd_solver* s, pycfd_stats* out, void* stream);
+
+/* The masked-face lists the device applies the direct forcing to
+ * (ProjectionSolver._build_slices' u_face_solid / v_face_solid and the per-body
+ * u_face_body / v_face_body, pycfd/core/solver.py:62-79, :280-296): linear
+ * indices into u (nx+3, ny+2) and v (nx+2, ny+3), grouped by body;
+ * body_*_start[b] .. body_*_start[b+1] are body b's entries (PCFD_MAX_BODIES + 1
+ * slots each), *n_bodies the count (0: the total only).  Copies at most u_cap /
+ * v_cap entries; *n_u / *n_v get the full counts.  The face ranges u_lo/u_hi,
+ * v_lo/v_hi (solver.py:250-258) go to lohi[4]. */
+int pycfd_face_lists(pycfd_solver* s, int* u_faces, int u_cap, int* v_faces, int v_cap, int* n_u,
+                     int* n_v, int* body_u_start, int* body_v_start, int* n_bodies, int* lohi);
+
+/* ---- Immersed bodies rasterised on the device (circle_mask, rectangle_mask,
+ * polygon_mask, mask_from_image; pycfd/geometry/obstacles.py:87-367).  The solid
+ * fraction of a cell is the mean of a subsamples x subsamples midpoint
+ * supersample of the shape's inside test, sample coordinates
+ * xf[i] + ((a + 0.5) / S) * dx_cells[i] (and the same in y) from the mesh's
+ * face coordinates; mask = fraction > 0.5.  Bit-identical to the reference's
+ * fraction and mask on the same mesh.  All arrays are device memory:
+ * xf, dx_cells (nx), yf, dy_cells (ny), fraction (nx*ny doubles), mask (nx*ny
+ * bytes). */
+#define PCFD_SHAPE_CIRCLE 0      /* p = cx, cy, r                                     */
+#define PCFD_SHAPE_RECTANGLE 1   /* p = x0, y0, x1, y1 (closed box)                    */
+#define PCFD_SHAPE_POLYGON 2     /* p = bounding box x0, y0, x1, y1 of the vertices;
+                                    verts: n_verts (x, y) pairs, even-odd ray test    */
+#define PCFD_SHAPE_IMAGE 3       /* image: rows x cols luminance, row 0 at y = 0,
+                                    stretched over [0, lx] x [0, ly]; solid where
+                                    luminance < threshold (the opposite if invert)    */
+typedef struct {
+    int kind;
+    double p[4];
+    const double* verts;
+    int n_verts;
+    const double* image;
+    int rows, cols;
+    double threshold;
+    int invert;
+} pycfd_shape;
+int pycfd_rasterize(const pycfd_shape* shape, const double* xf, const double* dx_cells, const double* yf,
+                    const double* dy_cells, int nx, int ny, double lx, double ly, int subsamples,
+                    double* fraction, uint8_t* mask, void* stream);
 
 /* Field reductions (synchronises `stream`).  u_prev/v_prev may be NULL. */
 int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const double* p,
@@ -346,23 +395,36 @@ int pycfd_batch_profile_read(pycfd_batch* b, double* total_ms, int* launches, vo
 /* Kernel launches the device executed for `steps` recorded steps since the
  * last call (fixed part per step plus the loop bodies times the passes run). */
 int pycfd_batch_launches(pycfd_batch* b, int steps, long long* launches, void* stream);
+/* No counterpart in the reference (failure detection of the device loops).
+ * Every device-side WHILE loop of a batched solve ends after a pass cap, above
+ * the problems' own iteration limits, so the loop always ends.  cap > 0 sets
+ * that cap for the CG and refinement loops of later steps (recorded or eager;
+ * the device reads it at every pass), 0 restores the built-in caps.  A solve
+ * cut short leaves its problems unconverged: status PCFD_E_NOCONV in
+ * pycfd_batch_status when the residual is above the solver's bound, and the
+ * step goes on.  pycfd_batch_capped reports (and clears) which loops a cap
+ * ended since the last call: bit 0 the CG loop, bit 1 the refinement loop. */
+int pycfd_batch_set_loop_cap(pycfd_batch* b, int cap, void* stream);
+int pycfd_batch_capped(pycfd_batch* b, int* capped, void* stream);
 
 /* No counterpart in the reference.  The reductions of pycfd_reduce_fields for
  * callers that cannot allocate device memory at the moment they need them: a
- * host whose own allocator owns all device memory, a real-time loop that cannot
- * afford the implicit device synchronisation of cudaMalloc, code that issues its
- * work while a stream is being captured.  It needs no solver handle and calls
- * no allocator.  Its scratch is a static device array of
+ * host whose own allocator owns all device memory (cudaMalloc would fail or
+ * steal from its pool), or a loop that cannot afford the device-wide
+ * synchronisation a cudaMalloc/cudaFree pair may impose.  It needs no solver
+ * handle and calls no allocator.  Its scratch is a static device array of
  * PCFD_NOALLOC_MAX_ROWS*8 + 66 doubles (about 258 KiB) that every GPU which
  * loads the library holds until the process exits; one thread block runs per
  * row of u, so nx may be at most PCFD_NOALLOC_MAX_ROWS - 3 (larger grids are
  * refused with PCFD_E_ARG).  Every call on a device shares that scratch and it
- * keeps the last call's contents: calls whose work overlaps on the GPU (for
- * instance on two streams) race, so serialise them.  The first call on a
- * device looks up the scratch's device address with that device current; make
- * that first call before any stream capture.  u, v, p, u_prev, v_prev and solid
- * (nx*ny bytes, or NULL) are device pointers; *out is written once the stream
- * has finished the reduction. */
+ * keeps the last call's contents (the call clears its ticket counter itself):
+ * calls whose work overlaps on the GPU (for instance on two streams) race, so
+ * serialise them.  The first call on a device looks up the scratch's device
+ * address with that device current and keeps it for the life of the process;
+ * after a cudaDeviceReset that address is stale, so do not call this entry
+ * point again in that process.  The call waits for its stream to finish the
+ * reduction before it returns.  u, v, p, u_prev, v_prev and solid (nx*ny
+ * bytes, or NULL) are device pointers. */
 #define PCFD_NOALLOC_MAX_ROWS 4096
 int pycfd_reduce_fields_noalloc(const double* u, const double* v, const double* p,
                                 const double* u_prev, const double* v_prev, const uint8_t* solid,

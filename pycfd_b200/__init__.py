@@ -27,7 +27,8 @@ def __getattr__(name):
     if name in ("TimeStepper", "DivergenceError", "SimulationResult"):
         from . import timestepper
         return getattr(timestepper, name)
-    if name in ("circle_mask", "Obstacle", "ObstacleGroup"):
+    if name in ("circle_mask", "rectangle_mask", "polygon_mask", "mask_from_image", "mask_from_function",
+                "load_polygon", "transform_polygon", "Obstacle", "ObstacleGroup"):
         from . import obstacles
         return getattr(obstacles, name)
     raise AttributeError(name)

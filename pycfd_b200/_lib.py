@@ -26,15 +26,23 @@ EXPORTS = (
     "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
-    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields",
-    "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_solver_persistent", "pycfd_solve_trace", "pycfd_launch_count",
+    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields", "pycfd_face_lists", "pycfd_rasterize",
+    "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_solver_persistent",
+    "pycfd_solver_set_wait_limit", "pycfd_solve_trace", "pycfd_launch_count",
     "pycfd_profile_read", "pycfd_batch_create", "pycfd_batch_destroy", "pycfd_batch_initialize",
     "pycfd_batch_step", "pycfd_batch_problem", "pycfd_batch_status", "pycfd_batch_launches",
-    "pycfd_batch_profile", "pycfd_batch_profile_read",
+    "pycfd_batch_profile", "pycfd_batch_profile_read", "pycfd_batch_set_loop_cap",
+    "pycfd_batch_capped",
 )
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
+
+
+class Shape(C.Structure):
+    _fields_ = [("kind", C.c_int), ("p", C.c_double * 4), ("verts", C.c_void_p), ("n_verts", C.c_int),
+                ("image", C.c_void_p), ("rows", C.c_int), ("cols", C.c_int), ("threshold", C.c_double),
+                ("invert", C.c_int)]
 
 
 class MgLevel(C.Structure):
@@ -128,10 +136,15 @@ def load(path: str = LIB_PATH):
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),
         "pycfd_profile_kernel": (C.c_int, [vp, C.c_int]),
         "pycfd_solver_persistent": (C.c_int, [vp, C.POINTER(C.c_int)]),
+        "pycfd_solver_set_wait_limit": (C.c_int, [vp, C.c_ulonglong]),
         "pycfd_solve_trace": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ulonglong), C.c_int, vp]),
         "pycfd_launch_count": (C.c_longlong, []),
         "pycfd_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),
+        "pycfd_rasterize": (C.c_int, [C.POINTER(Shape), vp, vp, vp, vp, C.c_int, C.c_int, C.c_double,
+                                      C.c_double, C.c_int, vp, vp, vp]),
+        "pycfd_face_lists": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int), vp, vp, C.POINTER(C.c_int), vp]),
         "pycfd_reduce_fields_noalloc": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_int, C.c_int,
                                                   C.c_double, C.c_double, C.POINTER(FieldStats),
                                                   vp]),
@@ -148,6 +161,8 @@ def load(path: str = LIB_PATH):
                                          C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
         "pycfd_batch_launches": (C.c_int, [vp, C.c_int, C.POINTER(C.c_longlong), vp]),
         "pycfd_batch_profile": (C.c_int, [vp, C.c_int]),
+        "pycfd_batch_set_loop_cap": (C.c_int, [vp, C.c_int, vp]),
+        "pycfd_batch_capped": (C.c_int, [vp, C.POINTER(C.c_int), vp]),
         "pycfd_batch_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
     }
     for name, (res, args) in sig.items():

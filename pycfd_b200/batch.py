@@ -56,6 +56,27 @@ def cavity_batch_configs(count: int = 256, seed: int = 0, sizes=(64, 96, 128, 19
     return out
 
 
+def partition_by_cells(configs, parts: int):
+    """Split independent problems over ``parts`` ranks by cell count.
+
+    Largest problem first, each to the rank with the fewest cells so far (ties to
+    the lower rank): every problem lands on exactly one rank, and the ranks'
+    totals differ by at most the largest problem's cells.  Returns one sorted
+    list of problem indices per rank.  Deterministic, so every rank computes the
+    same split without communicating.
+    """
+    if parts < 1:
+        raise ValueError(f"parts must be >= 1, got {parts}")
+    order = sorted(range(len(configs)), key=lambda k: (-configs[k].nx * configs[k].ny, k))
+    load = [0] * parts
+    out = [[] for _ in range(parts)]
+    for k in order:
+        r = min(range(parts), key=lambda q: (load[q], q))
+        out[r].append(k)
+        load[r] += configs[k].nx * configs[k].ny
+    return [sorted(o) for o in out]
+
+
 CANDIDATES = (
     dict(precision="fp64", inner_tol=1e-4, mg_sweeps=1),
     dict(precision="mixed", inner_tol=1e-4, mg_sweeps=1),
@@ -425,6 +446,16 @@ class BatchedSolver:
         _lib.check(self._L.pycfd_batch_profile_read(self._h, C.byref(ms), C.byref(cnt), _stream()))
         _lib.check(self._L.pycfd_batch_profile(self._h, 0))
         return ms.value, cnt.value, self.status()["iterations"]
+
+    def set_loop_cap(self, cap: int = 0) -> None:
+        """Pass cap of the device loops of later steps (0: the built-in caps)."""
+        _lib.check(self._L.pycfd_batch_set_loop_cap(self._h, int(cap), _stream()))
+
+    def capped(self) -> int:
+        """Which device loops a pass cap ended since the last call (bit 0 CG, bit 1 refinement)."""
+        out = C.c_int()
+        _lib.check(self._L.pycfd_batch_capped(self._h, C.byref(out), _stream()))
+        return int(out.value)
 
     def launches(self, steps: int) -> int:
         """Kernel launches the device ran for the last ``steps`` recorded steps."""

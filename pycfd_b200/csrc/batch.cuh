@@ -29,7 +29,6 @@ constexpr int kBMaxLevels = 12;
 constexpr int kBTileJ = 32;      // fine tile width along y (contiguous) = threads along y
 constexpr int kBThreadsI = 8;    // threads along x in a fine tile block
 constexpr int kBThreads = 256;   // every batched kernel runs 256-thread blocks
-constexpr int kBEllRounds = 8;   // ELL blocks: rounds of kBThreads / L rows each
 
 // One coarse level (l >= 1) of a hierarchy shared by the problems of one
 // structure (same grid, boundary kinds and solid mask).
@@ -68,6 +67,7 @@ struct BProb {
   int max_steps;                         // the problem stops after this many steps
   int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
   int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
+  int s_segs, s_items, s_chunks;         // warp strips of the solver kernels (b_strips)
   int red_base;                          // first partial row of this problem
   const uint8_t* flags;
   const uint8_t* solid;
@@ -98,6 +98,7 @@ struct BShared {
   long long* passes;     // per site: how often it let its loop body run (launch accounting)
   unsigned* iters;       // per site: passes of the loop now running (the cap below)
   int* capped;           // per site: set when a loop was ended by its pass cap
+  unsigned* cap_set;     // per site: pass cap set by the host (0: the loop's own cap)
   // Per-problem flags indexed by problem, mirrored from the scalar block by the
   // kernels that change them: a block learns whether its problem takes part
   // from one load beside its map entry instead of a chain through the record.
@@ -145,8 +146,9 @@ __device__ __forceinline__ void b_reduce(double (&v)[NV], double* partials, unsi
 // block sets the loop condition to "some unfrozen problem has flag `slot`
 // still 0", mirrors it into the site's `any` and rearms the ticket.  The
 // launch that opens a loop passes reset = 1; every later one counts a pass,
-// and at `cap` passes the loop ends whatever the flags say (each problem's
-// own iteration limit ends it first; the cap only bounds the device loop).
+// and at `cap` passes (or the host's sh.cap_set[site] when nonzero) the loop
+// ends whatever the flags say (each problem's own iteration limit ends it
+// first; the cap only bounds the device loop) and sh.capped[site] is set.
 template <class T>
 __device__ void b_loop_ticket(const BProb<T>* __restrict__ probs, int nprob, const BShared& sh,
                               int site, int slot, int reset, int cap, LoopCtl loop) {
@@ -173,7 +175,8 @@ __device__ void b_loop_ticket(const BProb<T>* __restrict__ probs, int nprob, con
   if (tid == 0) {
     const unsigned it = reset ? 0u : sh.iters[site] + 1u;
     sh.iters[site] = it;
-    if (any && it >= (unsigned)cap) {
+    const unsigned cs = sh.cap_set[site];
+    if (any && it >= (cs ? cs : (unsigned)cap)) {
       any = 0;
       sh.capped[site] = 1;
     }
@@ -252,7 +255,7 @@ __device__ __forceinline__ A b_apply(const BProb<T>& P, uint8_t f, int i, int j,
 }
 
 // A block's copy of what a fine cell loop reads from its problem's record: the
-// geometry and tile shape in registers, the diagonal tables in shared memory.
+// geometry and strip shape in registers, the diagonal tables in shared memory.
 // The record lives in global memory, and a loop that stores to the problem's
 // vectors cannot keep record fields in registers by itself (the stores might
 // alias it), so without the copy every cell would reload them.
@@ -262,19 +265,18 @@ struct BView {
   double w0;
   const double* dtab;
   const double* wtab;
-  int tile_i, tiles_i, tiles_j, tiles, chunk_tiles;
+  int segs, items;   // warp strips: 32-column segments per row, strips x segments
 };
 
 // Declares `V` for problem record P; every thread of the block must reach it.
 #define B_VIEW(V, P)                                                                           \
   __shared__ double V##_dt[16], V##_wt[16];                                                    \
-  if (threadIdx.y == 0 && threadIdx.x < 16) {                                                  \
+  if (threadIdx.x < 16) {                                                                      \
     V##_dt[threadIdx.x] = (P).dtab[threadIdx.x];                                               \
     V##_wt[threadIdx.x] = (P).wtab[threadIdx.x];                                               \
   }                                                                                            \
   __syncthreads();                                                                             \
-  const BView V{(P).g, (P).any_dir, (P).w0, V##_dt, V##_wt, (P).tile_i, (P).tiles_i, (P).tiles_j, \
-                (P).tiles, (P).chunk_tiles}
+  const BView V{(P).g, (P).any_dir, (P).w0, V##_dt, V##_wt, (P).s_segs, (P).s_items}
 
 __device__ __forceinline__ double b_diag(const BView& V, uint8_t f, int i, int j) {
   if (!(f & F_SOLV)) return 1.0;
@@ -287,106 +289,99 @@ __device__ __forceinline__ double b_wdinv(const BView& V, uint8_t f, int i, int 
     return V.w0 * (1.0 / fine_diag(f, i, j, V.g));
   return V.wtab[f & 15];
 }
-template <class A, class X>
-__device__ __forceinline__ A b_apply(const BView& V, uint8_t f, int i, int j, int c, X x) {
-  const Geo& g = V.g;
-  A acc = (A)b_diag(V, f, i, j) * x(c, i, j);
-  if (f & F_W) { const int a = wrap_w(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
-  if (f & F_E) { const int a = wrap_e(i, g); acc += (A)g.cx * x(a * g.ny + j, a, j); }
-  if (f & F_S) { const int b = wrap_s(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
-  if (f & F_N) { const int b = wrap_n(j, g); acc += (A)g.cy * x(i * g.ny + b, i, b); }
-  return acc;
-}
 
-// ---- staged fine tiles --------------------------------------------------------
-// The stencil kernels stage a tile's values once in shared memory, with a one-
-// cell halo, instead of rebuilding every neighbour's value per cell: sm[li][lj]
-// holds v at cell (i0 + li - 1, j0 + lj - 1).  Outside the domain the halo
-// wraps where the axis is periodic; elsewhere it holds 0 -- a face flag is
-// clear there, so the value is never read.
-constexpr int kBHaloJ = kBTileJ + 2;
-constexpr int kBHaloRows = 64 + 2;   // the largest tile height, plus the halo
-
-template <class T, class F>
-__device__ __forceinline__ void b_stage(T (*sm)[kBHaloJ], const BView& V, int i0, int j0, int rows, F v) {
-  const int nx = V.g.nx, ny = V.g.ny;
-  const int total = (rows + 2) * kBHaloJ;
-#pragma unroll 4
-  for (int idx = (int)(threadIdx.y * kBTileJ + threadIdx.x); idx < total; idx += kBThreads) {
-    const int li = idx / kBHaloJ, lj = idx - li * kBHaloJ;
-    int i = i0 + li - 1, j = j0 + lj - 1;
-    bool ok = true;
-    if (i < 0) {
-      ok = V.g.periodic_x != 0;
-      i = nx - 1;
-    } else if (i >= nx) {
-      ok = V.g.periodic_x && i == nx;
-      i = 0;
-    }
-    if (j < 0) {
-      ok = ok && V.g.periodic_y;
-      j = ny - 1;
-    } else if (j >= ny) {
-      ok = ok && V.g.periodic_y && j == ny;
-      j = 0;
-    }
-    sm[li][lj] = ok ? v(i * ny + j, i, j) : (T)0;
-  }
-}
-
-// (A x)_c from a staged tile, fine_apply's terms in its order.
+// (A x) at a cell from its value and its four neighbours' values, fine_apply's
+// terms in its order (diagonal, west, east, south, north), in arithmetic type A.
 template <class A, class T>
-__device__ __forceinline__ A b_apply_sm(const BView& V, uint8_t f, int i, int j, const T (*sm)[kBHaloJ], int li,
-                                        int lj) {
-  A acc = (A)b_diag(V, f, i, j) * (A)sm[li][lj];
-  if (f & F_W) acc += (A)V.g.cx * (A)sm[li - 1][lj];
-  if (f & F_E) acc += (A)V.g.cx * (A)sm[li + 1][lj];
-  if (f & F_S) acc += (A)V.g.cy * (A)sm[li][lj - 1];
-  if (f & F_N) acc += (A)V.g.cy * (A)sm[li][lj + 1];
+__device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T c, T w, T e, T s, T n) {
+  A acc = (A)b_diag(V, f, i, j) * (A)c;
+  if (f & F_W) acc += (A)V.g.cx * (A)w;
+  if (f & F_E) acc += (A)V.g.cx * (A)e;
+  if (f & F_S) acc += (A)V.g.cy * (A)s;
+  if (f & F_N) acc += (A)V.g.cy * (A)n;
   return acc;
 }
 
-// A thread's cells of a tile in batches of kBCellBatch rows: load(u, c) for
-// every cell of the batch first (independent loads in flight), then body(u, c,
-// i, j, li, lj) in row order -- the order a plain row loop visits them.
-constexpr int kBCellBatch = 4;
+// ---- warp strips -----------------------------------------------------------------
+// The fine-level solver kernels (CG direction and operator, CG update, the
+// level-0 multigrid sweeps) walk a problem's cells in warp strips: a warp takes
+// one 32-column segment of y (lane = column, so each row of a vector is one
+// coalesced 128-byte access in FP32, 256 bytes in FP64) over kBStripRows rows of
+// x.  The stencil operand of the strip and its two halo rows go to registers
+// first, with every per-cell load of the strip, before any arithmetic (a thread
+// keeps tens of independent loads in flight); the y-neighbours then come from
+// the adjacent lanes by shuffle, the segment's two edge lanes fetching theirs.
+// No shared-memory staging and no block barrier until the block's reduction.
+// A block (8 warps) takes kBStripItems consecutive (strip, segment) items of one
+// problem, adjacent segments of the same rows first.
+constexpr int kBStripRows = 8;
+constexpr int kBStripItems = 16;
 
-template <class Load, class Body>
-__device__ __forceinline__ void b_tile_cells(const BView& V, int i0, int j0, int rows, Load load, Body body) {
-  const int j = j0 + (int)threadIdx.x, lj = (int)threadIdx.x + 1;
-  if (j >= V.g.ny) return;
-  for (int l0 = 1 + (int)threadIdx.y; l0 <= rows; l0 += kBCellBatch * kBThreadsI) {
-    int c[kBCellBatch];
+// op(k, i, j): the operand at cell (i, j), k = i*ny + j (issues its loads).
+// load(u, c): the per-cell loads of body row u.
+// body(u, c, i, j, centre, west, east, south, north).
+// STENCIL = false: no operand (pointwise kernels); body gets zeros.
+template <bool STENCIL, class T, class Op, class Load, class Body>
+__device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load load, Body body) {
+  constexpr int RS = kBStripRows;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  const int nx = V.g.nx, ny = V.g.ny;
+  const int it1 = min(V.items, (chunk + 1) * kBStripItems);
+  for (int it = chunk * kBStripItems + warp; it < it1; it += kBThreads / 32) {
+    const int strip = it / V.segs, seg = it - strip * V.segs;
+    const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
+    const bool jv = j < ny;
+    T ov[STENCIL ? RS + 2 : 1];
+    T es[STENCIL ? RS : 1], en[STENCIL ? RS : 1];
+    if (STENCIL) {
 #pragma unroll
-    for (int u = 0; u < kBCellBatch; ++u) {
-      const int li = l0 + u * kBThreadsI;
-      c[u] = (i0 + li - 1) * V.g.ny + j;
-      if (li <= rows) load(u, c[u]);
+      for (int u = 0; u < RS + 2; ++u) {
+        int r = i0 - 1 + u;
+        if (r < 0) r = V.g.periodic_x ? nx - 1 : -1;
+        else if (r >= nx) r = (r == nx && V.g.periodic_x) ? 0 : -1;
+        ov[u] = (jv && r >= 0) ? op(r * ny + j, r, j) : (T)0;
+      }
     }
 #pragma unroll
-    for (int u = 0; u < kBCellBatch; ++u) {
-      const int li = l0 + u * kBThreadsI;
-      if (li <= rows) body(u, c[u], i0 + li - 1, j, li, lj);
+    for (int u = 0; u < RS; ++u) {
+      const int i = i0 + u;
+      if (jv && i < nx) load(u, i * ny + j);
     }
-  }
-}
-
-// The tiles of a chunk (block-uniform), optionally staged: with a value
-// function `val`, each tile's values and halo go to `sm` first.  Every thread
-// of the block runs the same tiles (the barriers need them all).
-template <bool STAGE, class T, class Val, class Load, class Body>
-__device__ __forceinline__ void b_chunk_cells(const BView& V, int chunk, T (*sm)[kBHaloJ], Val val, Load load,
-                                              Body body) {
-  for (int tile = chunk * V.chunk_tiles, tend = min(V.tiles, tile + V.chunk_tiles); tile < tend; ++tile) {
-    const int ti = tile / V.tiles_j, tj = tile - ti * V.tiles_j;
-    const int i0 = ti * V.tile_i, j0 = tj * kBTileJ;
-    const int rows = min(V.tile_i, V.g.nx - i0);
-    if (STAGE) {
-      __syncthreads();
-      b_stage(sm, V, i0, j0, rows, val);
-      __syncthreads();
+    const int last = min(31, ny - 1 - j0);   // the segment's last valid lane
+    if (STENCIL) {
+      // the edge lanes' outer neighbours (wrapped on a periodic y axis, absent otherwise)
+      if (lane == 0) {
+        const int js = j0 > 0 ? j0 - 1 : (V.g.periodic_y ? ny - 1 : -1);
+#pragma unroll
+        for (int u = 0; u < RS; ++u) {
+          const int i = i0 + u;
+          es[u] = (js >= 0 && i < nx) ? op(i * ny + js, i, js) : (T)0;
+        }
+      }
+      if (lane == last) {
+        const int jn = j + 1 < ny ? j + 1 : (V.g.periodic_y ? 0 : -1);
+#pragma unroll
+        for (int u = 0; u < RS; ++u) {
+          const int i = i0 + u;
+          en[u] = (jn >= 0 && i < nx) ? op(i * ny + jn, i, jn) : (T)0;
+        }
+      }
     }
-    b_tile_cells(V, i0, j0, rows, load, body);
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      T c = (T)0, w = (T)0, e = (T)0, sv = (T)0, nv = (T)0;
+      if (STENCIL) {
+        c = ov[u + 1];
+        w = ov[u];
+        e = ov[u + 2];
+        sv = __shfl_up_sync(0xffffffffu, c, 1);
+        nv = __shfl_down_sync(0xffffffffu, c, 1);
+        if (lane == 0) sv = es[u];
+        if (lane == last) nv = en[u];
+      }
+      const int i = i0 + u;
+      if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
+    }
   }
 }
 
@@ -670,6 +665,13 @@ __global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __rest
   b_loop_ticket(probs, nprob, sh, TK_CG, I_DONE, 1, maxiter + 1, loop);
 }
 
+// The CG direction of pass `it` lives in pa (it even) or pb (it odd), the
+// previous one in the other buffer, so no pass copies p.
+template <class T>
+__device__ __forceinline__ T* b_pdir(const BProb<T>& P, int it) {
+  return (it & 1) ? P.pb : P.pa;
+}
+
 // p = (z - mean z) + beta p_old on solvable rows, q = A p, p.q -> alpha.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restrict__ probs,
@@ -678,14 +680,14 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
   B_VIEW(V, P);
-  const int ny = V.g.ny;
-  const bool first = P.I[I_IT] == 0;
+  const int it = P.I[I_IT];
+  const bool first = it == 0;
   const double beta = first ? 0.0 : P.S[S_RHO] / P.S[S_RHO_PREV];
   const double mz = P.S[S_MEAN_Z];
   const uint8_t* __restrict__ flags = P.flags;
   const T* __restrict__ zraw = P.z;
-  const T* __restrict__ p_old = P.pa;
-  T* __restrict__ pn = P.pb;
+  const T* __restrict__ p_old = b_pdir(P, it + 1);
+  T* __restrict__ pn = b_pdir(P, it);
   T* __restrict__ q = P.q;
   // arithmetic in T (FP32 in the mixed form's inner solve), p.q summed in FP64
   const T tb = (T)beta, tm = (T)mz;
@@ -698,25 +700,22 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
     return pk * tb + z;
   };
   double acc[1] = {0.0};
-  __shared__ T sm[kBHaloRows][kBHaloJ];
-  uint8_t fv[kBCellBatch];
-  b_chunk_cells<true>(V, e.y, sm, pval, [&](int u, int c) { fv[u] = flags[c]; },
-                      [&](int u, int c, int i, int j, int li, int lj) {
-                        const T pc = sm[li][lj];
-                        const T qc = b_apply_sm<T>(V, fv[u], i, j, sm, li, lj);
-                        pn[c] = pc;
-                        q[c] = qc;
-                        acc[0] += (double)pc * (double)qc;
-                      });
-  (void)ny;
-  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+  uint8_t fv[kBStripRows];
+  b_strips<true, T>(V, e.y, pval, [&](int u, int c) { fv[u] = flags[c]; },
+                    [&](int u, int c, int i, int j, T pc, T pw, T pe, T ps, T pnn) {
+                      const T qc = b_apply5<T>(V, fv[u], i, j, pc, pw, pe, ps, pnn);
+                      pn[c] = pc;
+                      q[c] = qc;
+                      acc[0] += (double)pc * (double)qc;
+                    });
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
     P.S[S_PQ] = t[0];
     P.S[S_ALPHA] = P.S[S_RHO] / t[0];
   });
 }
 
-// x += alpha p, r -= alpha q, p kept for the next pass; ||r||^2 and sum(r);
-// the next pass's convergence test; launch-wide loop decision.
+// x += alpha p, r -= alpha q; ||r||^2 and sum(r); the next pass's convergence
+// test; launch-wide loop decision.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
                                                         const int2* __restrict__ map, int maxiter,
@@ -726,19 +725,17 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
   if (b_solving(sh, e.x)) {
     const Geo& g = P.g;
     B_VIEW(V, P);
-    const int ny = V.g.ny;
     const double alpha = P.S[S_ALPHA];
     const uint8_t* __restrict__ flags = P.flags;
-    const T* __restrict__ pn = P.pb;
+    const T* __restrict__ pn = b_pdir(P, P.I[I_IT]);
     const T* __restrict__ q = P.q;
-    T* __restrict__ pa = P.pa;
     T* __restrict__ xs = P.xs;
     T* __restrict__ r = P.r;
     double acc[2] = {0, 0};
-    T pv[kBCellBatch], xv[kBCellBatch], rv[kBCellBatch], qv[kBCellBatch];
-    uint8_t fv[kBCellBatch];
-    b_chunk_cells<false, T>(
-        V, e.y, nullptr, [](int, int, int) { return (T)0; },
+    T pv[kBStripRows], xv[kBStripRows], rv[kBStripRows], qv[kBStripRows];
+    uint8_t fv[kBStripRows];
+    b_strips<false, T>(
+        V, e.y, [](int, int, int) { return (T)0; },
         [&](int u, int c) {
           pv[u] = pn[c];
           xv[u] = xs[c];
@@ -746,18 +743,15 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
           qv[u] = q[c];
           fv[u] = flags[c];
         },
-        [&](int u, int c, int, int, int, int) {
-          const T pc = pv[u];
-          const double xc = (double)xv[u] + alpha * (double)pc;
+        [&](int u, int c, int, int, T, T, T, T, T) {
+          const double xc = (double)xv[u] + alpha * (double)pv[u];
           const double rc = (double)(T)((double)rv[u] - alpha * (double)qv[u]);
-          pa[c] = pc;
           xs[c] = (T)xc;
           r[c] = (T)rc;
           acc[0] += rc * rc;
           if (fv[u] & F_SOLV) acc[1] += rc;
         });
-    (void)ny;
-    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       const int it = I[I_IT] + 1;
@@ -942,65 +936,56 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   if (!b_solving(sh, e.x)) return;
   const Geo& g = P.g;
   B_VIEW(V, P);
-  const int ny = V.g.ny;
   // arithmetic in T (FP32 in the mixed form's inner solve), sums in FP64
   const uint8_t* __restrict__ flags = P.flags;
   const T* __restrict__ r = P.r;
   const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
-  auto bf = [&](int k) -> T {   // both loads issued, then selected
-    const uint8_t fk = flags[k];
-    const T rk = r[k];
-    return (fk & F_SOLV) ? rk - mr : (T)0;
-  };
   const T* __restrict__ x = b_fine_buf(P, src);
   T* __restrict__ xo = b_fine_buf(P, dst);
   T* __restrict__ lres0 = P.lres[0];
   double acc[2] = {0, 0};
-  __shared__ T sm[kBHaloRows][kBHaloJ];
+  uint8_t fv[kBStripRows];
+  T rv[kBStripRows];
+  auto load = [&](int u, int c) {
+    fv[u] = flags[c];
+    rv[u] = r[c];
+  };
+  auto bfv = [&](int u) -> T { return (fv[u] & F_SOLV) ? rv[u] - mr : (T)0; };   // right-hand side at the cell
   if (MODE == FM_WDB) {
-    B_CHUNK_TILES(V, e.y) {
-      B_TILE_CELLS(V, tile_) {
-        const int c = i * ny + j;
-        xo[c] = (T)b_wdinv(V, flags[c], i, j) * bf(c);
-      }
-    }
-  } else {
-    uint8_t fv[kBCellBatch];
-    T rv[kBCellBatch];
-    auto load = [&](int u, int c) {
-      fv[u] = flags[c];
-      rv[u] = r[c];
+    b_strips<false, T>(V, e.y, [](int, int, int) { return (T)0; }, load,
+                       [&](int u, int c, int i, int j, T, T, T, T, T) {
+                         xo[c] = (T)b_wdinv(V, fv[u], i, j) * bfv(u);
+                       });
+  } else if (MODE == FM_PRE) {
+    // first sweep from zero, x = W b, and the residual b - A W b
+    auto xw = [&](int k, int ii, int jj) -> T {   // both loads issued, then selected
+      const uint8_t fk = flags[k];
+      const T rk = r[k];
+      const T bk = (fk & F_SOLV) ? rk - mr : (T)0;
+      return (T)b_wdinv(V, fk, ii, jj) * bk;
     };
-    auto bfv = [&](int u) -> T { return (fv[u] & F_SOLV) ? rv[u] - mr : (T)0; };   // bf at the cell
-    if (MODE == FM_PRE) {
-      auto xw = [&](int k, int ii, int jj) -> T {
-        const uint8_t fk = flags[k];
-        const T bk = bf(k);
-        return (T)b_wdinv(V, fk, ii, jj) * bk;
-      };
-      b_chunk_cells<true>(V, e.y, sm, xw, load, [&](int u, int c, int i, int j, int li, int lj) {
-        xo[c] = sm[li][lj];
-        lres0[c] = bfv(u) - b_apply_sm<T>(V, fv[u], i, j, sm, li, lj);
-      });
-    } else {
-      auto xw = [&](int k, int, int) -> T { return x[k]; };
-      b_chunk_cells<true>(V, e.y, sm, xw, load, [&](int u, int c, int i, int j, int li, int lj) {
-        const uint8_t f = fv[u];
-        if (MODE == FM_RESID) {
-          lres0[c] = bfv(u) - b_apply_sm<T>(V, f, i, j, sm, li, lj);
-        } else {
-          const T xn = sm[li][lj] + (T)b_wdinv(V, f, i, j) * (bfv(u) - b_apply_sm<T>(V, f, i, j, sm, li, lj));
-          xo[c] = xn;
-          if (MODE == FM_LAST && (f & F_SOLV)) {
-            acc[0] += (double)xn;
-            acc[1] += (double)rv[u] * (double)xn;
-          }
+    b_strips<true, T>(V, e.y, xw, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
+      xo[c] = xc;
+      lres0[c] = bfv(u) - b_apply5<T>(V, fv[u], i, j, xc, xw_, xe, xs_, xn);
+    });
+  } else {
+    auto xv = [&](int k, int, int) -> T { return x[k]; };
+    b_strips<true, T>(V, e.y, xv, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
+      const uint8_t f = fv[u];
+      if (MODE == FM_RESID) {
+        lres0[c] = bfv(u) - b_apply5<T>(V, f, i, j, xc, xw_, xe, xs_, xn);
+      } else {
+        const T xnew = xc + (T)b_wdinv(V, f, i, j) * (bfv(u) - b_apply5<T>(V, f, i, j, xc, xw_, xe, xs_, xn));
+        xo[c] = xnew;
+        if (MODE == FM_LAST && (f & F_SOLV)) {
+          acc[0] += (double)xnew;
+          acc[1] += (double)rv[u] * (double)xnew;
         }
-      });
-    }
+      }
+    });
   }
   if (MODE != FM_LAST) return;
-  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
     double* S = P.S;
     const double m = (P.singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
     S[S_MEAN_Z] = m;
@@ -1009,10 +994,9 @@ __global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict
   });
 }
 
-// ELL phases of coarse level d (and prolongation into level 0).  A block takes
-// kBEllRounds x kBThreads / L rows, L lanes per row from the problem's
-// hierarchy (runtime), so problems of different structures share one launch
-// and wide rows spread over many blocks.
+// ELL phases of coarse level d (and prolongation into level 0), applied to
+// groups of a structure's problems (k_b_ellg below); one launch covers every
+// structure, whatever its hierarchy.
 // EO_FRESTRICT: b_d = M_d b_{d-1} (first sweep on d-1 and restriction of its
 // residual in one product; from level 0 the right-hand side is the projected CG
 // residual).  EO_PROLONGW: prolongation onto a level whose first-sweep iterate
@@ -1047,229 +1031,314 @@ __device__ __forceinline__ T b_ell_row(const Ell<T>& E, int L, int row, int lane
   return acc;
 }
 
-// Row dot product of E with L lanes fixed at compile time (L > 1: row-major
-// entries, L = 1: column-major), the same summation order as b_ell_row.
-template <int L, class T, class X>
-__device__ __forceinline__ T b_ell_row_c(const Ell<T>& E, int row, int lane, X x) {
-  T acc = (T)0;
-  if (row < E.n) {
-    if (L > 1) {
-      const long base = (long)row * E.K;
-#pragma unroll 4
-      for (int k = lane; k < E.K; k += L) acc += E.val[base + k] * x(E.col[base + k]);
-    } else {
-#pragma unroll 4
-      for (int k = 0; k < E.K; ++k) {
-        const long at = (long)k * E.n + row;
-        acc += E.val[at] * x(E.col[at]);
-      }
-    }
-  }
-#pragma unroll
-  for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, L);
-  return acc;
-}
+// ---- grouped ELL phases ------------------------------------------------------------
+// The problems of one structure share its hierarchy, so a block of a coarse-
+// level launch applies one row block of a structure's matrix to a GROUP of up
+// to kBGroup of its problems: each lane loads an entry (value, column) once and
+// multiplies it into every problem's gathered vector with its own accumulator.
+// The shared matrices cross from L2 once per group instead of once per problem,
+// and the per-entry index arithmetic is paid once per group.  Each problem's row
+// sum keeps the per-problem order (lane-strided entries, then the lane tree).
+constexpr int kBGroup = 8;         // problems per block of a grouped launch (also the tail's group)
+constexpr int kBEllGRounds = 2;    // rounds of kBThreads / L rows per block
 
-// Rows [r0, r1) of level d for one ELL op: kBEllRounds rounds of kBThreads / L
-// rows, the rounds unrolled so their loads overlap.
-template <int L, int OP, class T>
-__device__ __forceinline__ void b_ell_rows(const BProb<T>& P, int d, int src, int dst, int blk) {
-  constexpr int per = kBThreads / L;
-  const int n = (d == 0) ? P.g.nx * P.g.ny : P.lv[d].n;
-  const int r0 = blk * per * kBEllRounds;
-  const int r1 = min(n, r0 + per * kBEllRounds);
-  const int lane = threadIdx.x & (L - 1);
-  if (OP == EO_PROLONG) {
-    // x_d += P_{d+1} x_{d+1}
-    const Ell<T> Pm = P.lv[d + 1].P;
-    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
-    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
-#pragma unroll
-    for (int rd = 0; rd < kBEllRounds; ++rd) {
-      const int row = r0 + rd * per + (int)threadIdx.x / L;
-      const T s = b_ell_row_c<L>(Pm, row < r1 ? row : Pm.n, lane, [&](int c) { return xc[c]; });
-      if (lane == 0 && row < r1) xf[row] = xf[row] + s;
-    }
-    return;
-  }
-  if (OP == EO_PROLONGW) {
-    // x_d = W b_d + P_{d+1} x_{d+1}; on level 0 W b is fine_wdinv * (projected residual)
-    const Ell<T> Pm = P.lv[d + 1].P;
-    const T* __restrict__ xc = b_lvl_x(P, d + 1, src);
-    T* __restrict__ xf = (d == 0) ? b_fine_buf(P, dst) : b_lvl_x(P, d, dst);
-    const T* __restrict__ b = P.lb[d];
-    const T* __restrict__ wd = P.lv[d].wd;
-    const uint8_t* __restrict__ flags = P.flags;
-    const T* __restrict__ r = P.r;
-    const T mr = (T)(d == 0 && P.singular ? P.S[S_MEAN_R] : 0.0);
-    const int ny = P.g.ny;
-#pragma unroll
-    for (int rd = 0; rd < kBEllRounds; ++rd) {
-      const int row = r0 + rd * per + (int)threadIdx.x / L;
-      const T s = b_ell_row_c<L>(Pm, row < r1 ? row : Pm.n, lane, [&](int c) { return xc[c]; });
-      if (lane == 0 && row < r1) {
-        T wb;
-        if (d == 0) {
-          const uint8_t f = flags[row];
-          const int i = row / ny, j = row - i * ny;
-          const T bfr = (f & F_SOLV) ? r[row] - mr : (T)0;
-          wb = (T)b_wdinv(P, f, i, j) * bfr;
-        } else {
-          wb = wd[row] * b[row];
-        }
-        xf[row] = wb + s;
-      }
-    }
-    return;
-  }
-  if (OP == EO_FRESTRICT) {
-    // b_d = M_d b_{d-1}, from level 0 the projected CG residual
-    const Ell<T> M = P.lv[d].M;
-    T* __restrict__ bo = P.lb[d];
-    if (d == 1) {
-      const uint8_t* __restrict__ flags = P.flags;
-      const T* __restrict__ r = P.r;
-      const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
-#pragma unroll
-      for (int rd = 0; rd < kBEllRounds; ++rd) {
-        const int row = r0 + rd * per + (int)threadIdx.x / L;
-        const T s = b_ell_row_c<L>(M, row < r1 ? row : M.n, lane, [&](int c) {
-          const uint8_t fc = flags[c];
-          const T rc = r[c];
-          return (fc & F_SOLV) ? rc - mr : (T)0;
-        });
-        if (lane == 0 && row < r1) bo[row] = s;
-      }
-    } else {
-      const T* __restrict__ bi = P.lb[d - 1];
-#pragma unroll
-      for (int rd = 0; rd < kBEllRounds; ++rd) {
-        const int row = r0 + rd * per + (int)threadIdx.x / L;
-        const T s = b_ell_row_c<L>(M, row < r1 ? row : M.n, lane, [&](int c) { return bi[c]; });
-        if (lane == 0 && row < r1) bo[row] = s;
-      }
-    }
-    return;
-  }
-  if (OP == EO_RESTRICT) {
-    const Ell<T> R = P.lv[d].R;
-    const T* __restrict__ res = P.lres[d - 1];
-    T* __restrict__ bo = P.lb[d];
-#pragma unroll
-    for (int rd = 0; rd < kBEllRounds; ++rd) {
-      const int row = r0 + rd * per + (int)threadIdx.x / L;
-      const T s = b_ell_row_c<L>(R, row < r1 ? row : R.n, lane, [&](int c) { return res[c]; });
-      if (lane == 0 && row < r1) bo[row] = s;
-    }
-    return;
-  }
-  const Ell<T> A = P.lv[d].A;
-  const T* __restrict__ b = P.lb[d];
-  const T* __restrict__ wd = P.lv[d].wd;
-  const T* __restrict__ x = b_lvl_x(P, d, src);
-  T* __restrict__ xo = b_lvl_x(P, d, dst);
-  T* __restrict__ xa = P.lxa[d];
-  T* __restrict__ ro = P.lres[d];
-#pragma unroll
-  for (int rd = 0; rd < kBEllRounds; ++rd) {
-    const int row = r0 + rd * per + (int)threadIdx.x / L;
-    const int rr = row < r1 ? row : A.n;
-    if (OP == EO_PRE) {
-      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return wd[c] * b[c]; });
-      if (lane == 0 && row < r1) {
-        const T bx = b[row];
-        xa[row] = wd[row] * bx;
-        ro[row] = bx - s;
-      }
-    } else if (OP == EO_SMOOTH) {
-      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return x[c]; });
-      if (lane == 0 && row < r1) xo[row] = x[row] + wd[row] * (b[row] - s);
-    } else {   // EO_RESID
-      const T s = b_ell_row_c<L>(A, rr, lane, [&](int c) { return x[c]; });
-      if (lane == 0 && row < r1) ro[row] = b[row] - s;
-    }
-  }
-}
+// The group's vectors for one op, filled from the problem records by the first
+// kBGroup threads; a null output marks a member that is absent or not solving.
+template <class T>
+struct BGroup {
+  const T* src[kBGroup];   // gathered vector
+  const T* b[kBGroup];     // the level's right-hand side (or r on level 0)
+  T* out[kBGroup];
+  T* out2[kBGroup];
+  T mr[kBGroup];           // fluid mean of r (projected level-0 right-hand side)
+};
 
+// Fill member g (thread g of the block) for op OP at depth d.
 template <class T, int OP>
-__global__ void __launch_bounds__(kBThreads) k_b_ell(const BProb<T>* __restrict__ probs,
-                                                      const int2* __restrict__ map, int d, int src,
-                                                      int dst, BShared sh) {
+__device__ __forceinline__ void b_group_fill(BGroup<T>& G, int g, const BProb<T>* P, int d, int src, int dst) {
+  G.src[g] = nullptr;
+  G.b[g] = nullptr;
+  G.out[g] = nullptr;
+  G.out2[g] = nullptr;
+  G.mr[g] = (T)0;
+  if (!P) return;
+  if ((OP == EO_PROLONGW && d == 0) || (OP == EO_FRESTRICT && d == 1)) {
+    G.b[g] = P->r;
+    G.mr[g] = (T)(P->singular ? P->S[S_MEAN_R] : 0.0);
+  }
+  switch (OP) {
+    case EO_PROLONG:
+    case EO_PROLONGW:
+      G.src[g] = b_lvl_x(*P, d + 1, src);
+      G.out[g] = d == 0 ? b_fine_buf(*P, dst) : b_lvl_x(*P, d, dst);
+      if (OP == EO_PROLONGW && d > 0) G.b[g] = P->lb[d];
+      break;
+    case EO_FRESTRICT:
+      G.out[g] = P->lb[d];
+      if (d > 1) G.src[g] = P->lb[d - 1];
+      break;
+    case EO_RESTRICT:
+      G.out[g] = P->lb[d];
+      G.src[g] = P->lres[d - 1];
+      break;
+    case EO_PRE:
+      G.b[g] = P->lb[d];
+      G.out[g] = P->lxa[d];
+      G.out2[g] = P->lres[d];
+      break;
+    case EO_SMOOTH:
+      G.src[g] = b_lvl_x(*P, d, src);
+      G.b[g] = P->lb[d];
+      G.out[g] = b_lvl_x(*P, d, dst);
+      break;
+    default:   // EO_RESID
+      G.src[g] = b_lvl_x(*P, d, src);
+      G.b[g] = P->lb[d];
+      G.out[g] = P->lres[d];
+      break;
+  }
+}
+
+// kBEllGRounds rounds of kBThreads / L rows of row block rb of matrix E, for
+// every member of the group.  L lanes per row fixed at compile time (L > 1:
+// row-major entries, L = 1: column-major).
+template <int L, int OP, class T>
+__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T>& G, const Ell<T>& E,
+                                            const T* __restrict__ wd, int d, int rb) {
+  constexpr int per = kBThreads / L;
+  const int lane = (int)threadIdx.x & (L - 1);
+  const uint8_t* __restrict__ flags = P0.flags;
+  bool on[kBGroup];
+#pragma unroll
+  for (int g = 0; g < kBGroup; ++g) on[g] = G.out[g] != nullptr;
+#pragma unroll
+  for (int rd = 0; rd < kBEllGRounds; ++rd) {
+    const int row = (rb * kBEllGRounds + rd) * per + (int)threadIdx.x / L;
+    T acc[kBGroup];
+#pragma unroll
+    for (int g = 0; g < kBGroup; ++g) acc[g] = (T)0;
+    if (row < E.n) {
+      const int kb = L > 1 ? lane : 0;
+#pragma unroll 2
+      for (int k = kb; k < E.K; k += L) {
+        const long at = L > 1 ? (long)row * E.K + k : (long)k * E.n + row;
+        const T v = E.val[at];
+        const int c = E.col[at];
+        if (OP == EO_PRE) {
+          const T w = wd[c];
+#pragma unroll
+          for (int g = 0; g < kBGroup; ++g)
+            if (on[g]) acc[g] += v * (w * G.b[g][c]);
+        } else if ((OP == EO_FRESTRICT && d == 1)) {
+          const bool solv = (flags[c] & F_SOLV) != 0;
+#pragma unroll
+          for (int g = 0; g < kBGroup; ++g)
+            if (on[g]) {
+              const T rc = G.b[g][c];
+              acc[g] += v * (solv ? rc - G.mr[g] : (T)0);
+            }
+        } else {
+#pragma unroll
+          for (int g = 0; g < kBGroup; ++g)
+            if (on[g]) acc[g] += v * G.src[g][c];
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kBGroup; ++g)
+#pragma unroll
+      for (int o = L / 2; o > 0; o >>= 1) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], o, L);
+    if (lane != 0 || row >= E.n) continue;
+#pragma unroll
+    for (int g = 0; g < kBGroup; ++g) {
+      if (!on[g]) continue;
+      const T s = acc[g];
+      T* __restrict__ o = G.out[g];
+      switch (OP) {
+        case EO_PROLONG: o[row] = o[row] + s; break;
+        case EO_PROLONGW: {
+          T wb;
+          if (d == 0) {
+            const uint8_t f = flags[row];
+            const int i = row / P0.g.ny, j = row - i * P0.g.ny;
+            const T bfr = (f & F_SOLV) ? G.b[g][row] - G.mr[g] : (T)0;
+            wb = (T)b_wdinv(P0, f, i, j) * bfr;
+          } else {
+            wb = wd[row] * G.b[g][row];
+          }
+          o[row] = wb + s;
+          break;
+        }
+        case EO_FRESTRICT:
+        case EO_RESTRICT: o[row] = s; break;
+        case EO_PRE: {
+          const T bx = G.b[g][row];
+          o[row] = wd[row] * bx;
+          G.out2[g][row] = bx - s;
+          break;
+        }
+        case EO_SMOOTH: {
+          const T xr = G.src[g][row];
+          o[row] = xr + wd[row] * (G.b[g][row] - s);
+          break;
+        }
+        default: o[row] = G.b[g][row] - s; break;   // EO_RESID
+      }
+    }
+  }
+}
+
+// One ELL op at depth d over the map's (structure, row block x 64 + group)
+// entries.  Members: sprobs[H.sp0 + group * kBGroup + g], g < kBGroup.
+template <class T, int OP>
+__global__ void __launch_bounds__(kBThreads) k_b_ellg(const BProb<T>* __restrict__ probs,
+                                                       const BHier<T>* __restrict__ hiers,
+                                                       const int2* __restrict__ map,
+                                                       const int* __restrict__ sprobs, int d, int src,
+                                                       int dst, BShared sh) {
+  const int2 e = map[blockIdx.x];
+  const BHier<T>& H = hiers[e.x];
+  const int rb = e.y >> 6, grp = e.y & 63;
+  __shared__ BGroup<T> G;
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  if (threadIdx.x < kBGroup) {
+    const int k = grp * kBGroup + (int)threadIdx.x;
+    const BProb<T>* P = nullptr;
+    if (k < H.spn) {
+      const int pi = sprobs[H.sp0 + k];
+      if (b_solving(sh, pi)) P = probs + pi;
+    }
+    b_group_fill<T, OP>(G, (int)threadIdx.x, P, d, src, dst);
+    if (P) any = 1;
+  }
+  __syncthreads();
+  if (!any) return;
+  const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * kBGroup]];   // the structure's geometry and flags
+  const bool pl = OP == EO_PROLONG || OP == EO_PROLONGW;
+  const BLevel<T>& Lm = pl ? H.lv[d + 1] : H.lv[d];
+  const Ell<T>& E = pl ? Lm.P : OP == EO_RESTRICT ? Lm.R : OP == EO_FRESTRICT ? Lm.M : Lm.A;
+  const int Lop = pl ? Lm.lp : OP == EO_RESTRICT ? Lm.lr : OP == EO_FRESTRICT ? Lm.lm : Lm.la;
+  const T* wd = d > 0 ? H.lv[d].wd : nullptr;
+  switch (Lop) {
+    case 1: b_ellg_rows<1, OP>(P0, G, E, wd, d, rb); break;
+    case 4: b_ellg_rows<4, OP>(P0, G, E, wd, d, rb); break;
+    case 8: b_ellg_rows<8, OP>(P0, G, E, wd, d, rb); break;
+    case 16: b_ellg_rows<16, OP>(P0, G, E, wd, d, rb); break;
+    default: b_ellg_rows<32, OP>(P0, G, E, wd, d, rb); break;
+  }
+}
+
+// Coarsest level d of the problems whose structure has no dense tail: the
+// restriction from level d - 1 and the dense pseudo-inverse, one block per problem.
+template <class T>
+__global__ void __launch_bounds__(kBThreads) k_b_coarsest(const BProb<T>* __restrict__ probs,
+                                                           const int2* __restrict__ map, int d, BShared sh) {
   extern __shared__ double sb[];
   const int2 e = map[blockIdx.x];
   if (!b_solving(sh, e.x)) return;
   const BProb<T>& P = probs[e.x];
-  if (OP == EO_RESTRICT && e.y < 0) {
-    // coarsest level d: restriction and dense solve in this block
-    const BLevel<T>& Lc = P.lv[d];
-    const T* res = P.lres[d - 1];
-    const int L = Lc.lr, lane = threadIdx.x & (L - 1);
-    const int per = kBThreads / L;
-    for (int base = 0; base < Lc.R.n; base += per) {
-      const int row = base + (int)threadIdx.x / L;
-      const T s = b_ell_row(Lc.R, L, row, lane, [&](int c) { return res[c]; });
-      if (lane == 0 && row < Lc.R.n) {
-        sb[row] = (double)s;
-        P.lb[d][row] = s;
-      }
+  const BLevel<T>& Lc = P.lv[d];
+  const T* res = P.lres[d - 1];
+  const int L = Lc.lr, lane = threadIdx.x & (L - 1);
+  const int per = kBThreads / L;
+  for (int base = 0; base < Lc.R.n; base += per) {
+    const int row = base + (int)threadIdx.x / L;
+    const T s = b_ell_row(Lc.R, L, row, lane, [&](int c) { return res[c]; });
+    if (lane == 0 && row < Lc.R.n) {
+      sb[row] = (double)s;
+      P.lb[d][row] = s;
     }
-    __syncthreads();
-    const int wl = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kBThreads >> 5;
-    const int n = Lc.R.n;
-    for (int row = warp; row < n; row += nw) {
-      double acc = 0.0;
-      for (int k = wl; k < n; k += 32) acc += (double)P.C[(long)row * n + k] * sb[k];
-      acc = warp_sum(acc);
-      if (wl == 0) P.lxa[d][row] = (T)acc;
-    }
-    return;
   }
-  // the rows of this block, with the lane count of its matrix fixed at compile time
-  const int Lop = (OP == EO_PROLONG || OP == EO_PROLONGW) ? P.lv[d + 1].lp
-                  : OP == EO_RESTRICT                    ? P.lv[d].lr
-                  : OP == EO_FRESTRICT                   ? P.lv[d].lm
-                                                         : P.lv[d].la;
-  switch (Lop) {
-    case 1: b_ell_rows<1, OP>(P, d, src, dst, e.y); break;
-    case 4: b_ell_rows<4, OP>(P, d, src, dst, e.y); break;
-    case 8: b_ell_rows<8, OP>(P, d, src, dst, e.y); break;
-    case 16: b_ell_rows<16, OP>(P, d, src, dst, e.y); break;
-    default: b_ell_rows<32, OP>(P, d, src, dst, e.y); break;
+  __syncthreads();
+  const int wl = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kBThreads >> 5;
+  const int n = Lc.R.n;
+  for (int row = warp; row < n; row += nw) {
+    double acc = 0.0;
+    for (int k = wl; k < n; k += 32) acc += (double)P.C[(long)row * n + k] * sb[k];
+    acc = warp_sum(acc);
+    if (wl == 0) P.lxa[d][row] = (T)acc;
   }
 }
 
-// Dense close of the V-cycle: x_t = M b_t for every problem whose structure has
-// a tail, t the structure's tail depth and M its operator (n x n, row-major; the
-// cycle at and below t as one linear map).  One launch after the down sweep
-// covers every structure, whatever its tail depth.  A block takes kBTailRows rows of M
-// (one warp each) for a group of kBTailGroup problems of one structure: each
-// lane loads its entries of M once and applies them to every problem of the
-// group (independent accumulators), so M crosses from L2 once per group and a
-// row's sum is a fixed lane-strided order plus the warp tree.
-constexpr int kBTailRows = kBThreads / 32;
-constexpr int kBTailGroup = 8;
+// Dense close of the V-cycle on the tensor cores: X_t = M B_t for every tailed
+// structure, where M (n x n, row-major) is the structure's operator of the cycle
+// at and below its tail depth t and the columns of B_t are the level-t
+// right-hand sides of its problems -- a matrix product with the problems as the
+// N dimension.  One launch after the down sweep covers every structure; a block
+// (4 warps) takes a kTailBM-row tile of M against a kTailBN-problem column tile,
+// the K dimension in kTailBK chunks staged in shared memory (M rows and the
+// problems' vectors loaded coalesced along K).  FP64 form: DMMA (mma m8n8k4
+// f64, FP64 products and sums).  Mixed form: three TF32 MMAs per product
+// (m16n8k8; each FP32 operand split into a TF32 head and a TF32 remainder,
+// head*head + head*rem + rem*head) so the result keeps FP32 accuracy and the
+// preconditioner its FP32 behaviour.
+constexpr int kTailBM = 64, kTailBN = 32, kTailThreads = 128;
+constexpr int kBTailGroup = kTailBN;   // problems per column tile of the tail launch
 
+template <class T> struct TailTile;
+template <> struct TailTile<float> { static constexpr int BK = 32, PA = 4, PB = 8; };
+template <> struct TailTile<double> { static constexpr int BK = 16, PA = 2, PB = 4; };
+
+__device__ __forceinline__ uint32_t b_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void b_mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void b_mma_f64(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+// Stage K chunk [k0, k0 + BK) of the block's M rows and of its problems' vectors.
 template <class T>
-__device__ __forceinline__ T b_warp_sum(T v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+__device__ __forceinline__ void b_tail_stage(T (*As)[TailTile<T>::BK + TailTile<T>::PA],
+                                             T (*Bs)[kTailBN + TailTile<T>::PB], const T* __restrict__ M,
+                                             const T* const* sb, int n, int r0, int k0) {
+  constexpr int BK = TailTile<T>::BK;
+  for (int idx = threadIdx.x; idx < kTailBM * BK; idx += kTailThreads) {
+    const int r = idx / BK, k = idx - r * BK;
+    const int row = r0 + r, col = k0 + k;
+    As[r][k] = (row < n && col < n) ? __ldg(M + (long)row * n + col) : (T)0;
+  }
+  for (int idx = threadIdx.x; idx < kTailBN * BK; idx += kTailThreads) {
+    const int c = idx / BK, k = idx - c * BK;
+    const T* v = sb[c];
+    Bs[k][c] = (v && k0 + k < n) ? v[k0 + k] : (T)0;
+  }
 }
 
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_tail(const BProb<T>* __restrict__ probs,
-                                                       const BHier<T>* __restrict__ hiers,
-                                                       const int2* __restrict__ map,
-                                                       const int* __restrict__ sprobs, BShared sh) {
-  const int2 e = map[blockIdx.x];   // (structure, row block * 64 + problem group)
+__global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restrict__ probs,
+                                                          const BHier<T>* __restrict__ hiers,
+                                                          const int2* __restrict__ map,
+                                                          const int* __restrict__ sprobs, BShared sh) {
+  constexpr int BK = TailTile<T>::BK;
+  const int2 e = map[blockIdx.x];   // (structure, row tile * 64 + column tile)
   const BHier<T>& H = hiers[e.x];
   const int d = H.tail_level;
   const int n = H.tail_n;
-  const int rb = e.y >> 6, grp = e.y & 63;
-  __shared__ const T* sb[kBTailGroup];
-  __shared__ T* sx[kBTailGroup];
-  if (threadIdx.x < kBTailGroup) {
-    const int k = grp * kBTailGroup + (int)threadIdx.x;
+  const int r0 = (e.y >> 6) * kTailBM, ct = e.y & 63;
+  __shared__ const T* sb[kTailBN];
+  __shared__ T* sx[kTailBN];
+  __shared__ int any;
+  __shared__ __align__(16) T As[kTailBM][BK + TailTile<T>::PA];
+  __shared__ __align__(16) T Bs[BK][kTailBN + TailTile<T>::PB];
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  if (threadIdx.x < kTailBN) {
+    const int k = ct * kTailBN + (int)threadIdx.x;
     const T* b = nullptr;
     T* x = nullptr;
     if (k < H.spn) {
@@ -1277,29 +1346,91 @@ __global__ void __launch_bounds__(kBThreads) k_b_tail(const BProb<T>* __restrict
       if (b_solving(sh, pi)) {
         b = probs[pi].lb[d];
         x = probs[pi].lxa[d];
+        any = 1;
       }
     }
     sb[threadIdx.x] = b;
     sx[threadIdx.x] = x;
   }
   __syncthreads();
+  if (!any) return;   // block-uniform
   const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
-  const int row = rb * kBTailRows + warp;
-  if (row >= n) return;   // warp-uniform, no block barrier follows
-  const T* m = H.tail + (long)row * n;
-  T acc[kBTailGroup];
+  const int g = lane >> 2, t = lane & 3;
+  const T* __restrict__ M = H.tail;
+  if constexpr (sizeof(T) == 4) {
+    float acc[4][4];   // [n tile][fragment]
 #pragma unroll
-  for (int g = 0; g < kBTailGroup; ++g) acc[g] = (T)0;
-  for (int c = lane; c < n; c += 32) {
-    const T mv = __ldg(m + c);
+    for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int g = 0; g < kBTailGroup; ++g)
-      if (sb[g]) acc[g] += mv * sb[g][c];
-  }
+      for (int i = 0; i < 4; ++i) acc[q][i] = 0.f;
+    const int wr = warp * 16;
+    for (int k0 = 0; k0 < n; k0 += BK) {
+      __syncthreads();
+      b_tail_stage<T>(As, Bs, M, sb, n, r0, k0);
+      __syncthreads();
 #pragma unroll
-  for (int g = 0; g < kBTailGroup; ++g) {
-    const T t = b_warp_sum(acc[g]);
-    if (lane == 0 && sx[g]) sx[g][row] = t;
+      for (int kk = 0; kk < BK; kk += 8) {
+        const float av[4] = {As[wr + g][kk + t], As[wr + g + 8][kk + t], As[wr + g][kk + t + 4],
+                             As[wr + g + 8][kk + t + 4]};
+        uint32_t ah[4], al[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          ah[i] = b_tf32(av[i]);
+          al[i] = b_tf32(av[i] - __uint_as_float(ah[i]));
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float bv0 = Bs[kk + t][q * 8 + g], bv1 = Bs[kk + t + 4][q * 8 + g];
+          const uint32_t bh0 = b_tf32(bv0), bh1 = b_tf32(bv1);
+          const uint32_t bl0 = b_tf32(bv0 - __uint_as_float(bh0)), bl1 = b_tf32(bv1 - __uint_as_float(bh1));
+          b_mma_tf32(acc[q], al, bh0, bh1);
+          b_mma_tf32(acc[q], ah, bl0, bl1);
+          b_mma_tf32(acc[q], ah, bh0, bh1);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int row = r0 + wr + g + ((i & 2) ? 8 : 0);
+        const int col = q * 8 + 2 * t + (i & 1);
+        T* x = sx[col];
+        if (x && row < n) x[row] = acc[q][i];
+      }
+  } else {
+    double acc[2][4][2];   // [m tile][n tile][fragment]
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[m][q][0] = acc[m][q][1] = 0.0;
+    const int wr = warp * 16;
+    for (int k0 = 0; k0 < n; k0 += BK) {
+      __syncthreads();
+      b_tail_stage<T>(As, Bs, M, sb, n, r0, k0);
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 4) {
+        const double a0 = As[wr + g][kk + t], a1 = As[wr + 8 + g][kk + t];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double bv = Bs[kk + t][q * 8 + g];
+          b_mma_f64(acc[0][q], a0, bv);
+          b_mma_f64(acc[1][q], a1, bv);
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int row = r0 + wr + 8 * m + g;
+          const int col = q * 8 + 2 * t + i;
+          T* x = sx[col];
+          if (x && row < n) x[row] = acc[m][q][i];
+        }
   }
 }
 

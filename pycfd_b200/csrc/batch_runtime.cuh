@@ -32,10 +32,13 @@ struct pycfd_batch {
   std::vector<int> nlev;
   int depth = 0;                           // most levels of any problem
   BMapHost fine;                           // every chunk of tiles of every problem
+  BMapHost strip;                          // every chunk of warp strips of every problem (solver kernels)
   // row-block maps per depth d (problems whose level d runs per level):
+  // grouped maps per depth d, entries (structure, row block x 64 + group of kBGroup problems):
   std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
-  std::vector<BMapHost> mapR;              // restriction into d (+ coarsest blocks when coarse == 0)
+  std::vector<BMapHost> mapR;              // restriction into d
   std::vector<BMapHost> mapP;              // prolongation into d with P_{d+1}
+  std::vector<BMapHost> mapC;              // (problem, -1): coarsest level d of an untailed structure
   BMapHost mapT;                           // dense tails: (structure, row block x 64 + problem group)
   int* sprobs = nullptr;                   // problems grouped by structure
   size_t smem_dense = 0;
@@ -170,7 +173,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 
   // per-problem records
   std::vector<BProb<T>> pr(n);
-  std::vector<int2> fine;
+  std::vector<int2> fine, strip;
   B->nlev.assign(n, 0);
   B->depth = 0;
   int red_rows = 0;
@@ -195,8 +198,11 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.tiles = P.tiles_i * P.tiles_j;
     P.chunk_tiles = std::max(1, kBChunkCells / (B->tile_i * kBTileJ));
     P.chunks = (P.tiles + P.chunk_tiles - 1) / P.chunk_tiles;
+    P.s_segs = (s->g.ny + 31) / 32;
+    P.s_items = ((s->g.nx + kBStripRows - 1) / kBStripRows) * P.s_segs;
+    P.s_chunks = (P.s_items + kBStripItems - 1) / kBStripItems;
     P.red_base = red_rows;
-    red_rows += P.chunks;
+    red_rows += std::max(P.chunks, P.s_chunks);
     P.flags = s->flags;
     P.solid = s->solid;
     P.bc_kind = s->bc_kind_dev;
@@ -254,8 +260,10 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.C = hh[hid[i]].C;
     for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
+    for (int c = 0; c < P.s_chunks; ++c) strip.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
+  TRY(upload_map(B, &B->strip, strip));
   // problems grouped by structure (the dense tail's block groups)
   {
     std::vector<int> sp;
@@ -283,21 +291,23 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   B->mapA.assign(B->depth, BMapHost{});
   B->mapR.assign(B->depth, BMapHost{});
   B->mapP.assign(B->depth, BMapHost{});
+  B->mapC.assign(B->depth, BMapHost{});
   std::vector<int2> mt;
   for (int d = 0; d < B->depth; ++d) {
-    std::vector<int2> ma, mr, mp;
+    std::vector<int2> ma, mr, mp, mc;
     for (size_t h = 0; h < leaders.size(); ++h) {
-      if (hh[h].tail_level != d || hh[h].tail_n == 0) continue;
-      const int rbs = (hh[h].tail_n + kBTailRows - 1) / kBTailRows;
-      const int grps = (hh[h].spn + kBTailGroup - 1) / kBTailGroup;
-      if (grps > 64) return fail(PCFD_E_UNSUPPORTED, "at most %d problems share a structure", 64 * kBTailGroup);
-      for (int rb = 0; rb < rbs; ++rb)
-        for (int g = 0; g < grps; ++g) mt.push_back(make_int2((int)h, rb * 64 + g));
-    }
-    for (int i = 0; i < n; ++i) {
-      const int c = B->nlev[i] - 1;
-      const int t = pr[i].tail;
-      const BHier<T>& H = hh[hid[i]];
+      const BHier<T>& H = hh[h];
+      const int grps = (H.spn + kBGroup - 1) / kBGroup;
+      if (grps > 64) return fail(PCFD_E_UNSUPPORTED, "at most %d problems share a structure", 64 * kBGroup);
+      if (H.tail_level == d && H.tail_n > 0) {
+        const int rts = (H.tail_n + kTailBM - 1) / kTailBM;
+        const int cts = (H.spn + kTailBN - 1) / kTailBN;
+        for (int rt = 0; rt < rts; ++rt)
+          for (int c = 0; c < cts; ++c) mt.push_back(make_int2((int)h, rt * 64 + c));
+      }
+      const int lead = leaders[h];
+      const int c = B->nlev[lead] - 1;
+      const int t = pr[lead].tail;
       if (B->coarse > 0) {
         if (d >= std::min(B->coarse, c)) continue;
       } else if (t > 0) {
@@ -305,14 +315,17 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       } else {
         if (d > c) continue;
         if (d == c) {
-          if (d >= 1) mr.push_back(make_int2(i, -1));
+          if (d >= 1)
+            for (int i = 0; i < n; ++i)
+              if (hid[i] == (int)h) mc.push_back(make_int2(i, -1));
           continue;
         }
       }
-      const int nrow = d == 0 ? pr[i].g.nx * pr[i].g.ny : keep[hid[i]][d].n;
+      const int nrow = d == 0 ? pr[lead].g.nx * pr[lead].g.ny : keep[h][d].n;
       auto add = [&](std::vector<int2>& m, int lanes) {
-        const int rpb = kBThreads / lanes * kBEllRounds;
-        for (int rb = 0; rb * rpb < nrow; ++rb) m.push_back(make_int2(i, rb));
+        const int rpb = kBThreads / lanes * kBEllGRounds;
+        for (int rb = 0; rb * rpb < nrow; ++rb)
+          for (int g = 0; g < grps; ++g) m.push_back(make_int2((int)h, rb * 64 + g));
       };
       const int lres = (B->fused && d >= B->fused_from) ? H.lv[d].lm : H.lv[d].lr;   // lanes of the restriction into d
       if (t > 0 && d == t) {   // restriction into the tail level only
@@ -328,6 +341,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     TRY(upload_map(B, &B->mapA[d], ma));
     TRY(upload_map(B, &B->mapR[d], mr));
     TRY(upload_map(B, &B->mapP[d], mp));
+    TRY(upload_map(B, &B->mapC[d], mc));
   }
   TRY(upload_map(B, &B->mapT, mt));
   {
@@ -347,6 +361,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   TRY(dalloc(B->mem, &B->sh.passes, TK_COUNT));
   TRY(dalloc(B->mem, &B->sh.iters, TK_COUNT));
   TRY(dalloc(B->mem, &B->sh.capped, TK_COUNT));
+  TRY(dalloc(B->mem, &B->sh.cap_set, TK_COUNT));
   TRY(dalloc(B->mem, &B->sh.frozen, n));
   TRY(dalloc(B->mem, &B->sh.solving, n));
   TRY(dalloc(B->mem, &B->d_iout, (size_t)4 * n));
@@ -385,12 +400,17 @@ int b_boundary(pycfd_batch* B, int arr, std::initializer_list<int> ops, int p_gh
   return 0;
 }
 
+// One grouped ELL op at depth d; a restriction also closes the untailed
+// structures whose coarsest level is d (restriction + dense solve per problem).
 template <class T, int OP>
 int b_ell(pycfd_batch* B, const BMapHost& m, int d, int src, int dst, cudaStream_t st) {
-  if (m.n == 0) return 0;
-  const size_t smem = OP == EO_RESTRICT ? B->smem_dense : 0;
+  const BMapHost* mc = (OP == EO_RESTRICT && d < (int)B->mapC.size()) ? &B->mapC[d] : nullptr;
+  if (m.n == 0 && !(mc && mc->n)) return 0;
   b_prof(B, 4, st);
-  BLAUNCH((k_b_ell<T, OP>), m.n, kBThreads, smem, st, probs_of<T>(B), m.e, d, src, dst, B->sh);
+  if (m.n)
+    BLAUNCH((k_b_ellg<T, OP>), m.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), m.e, B->sprobs, d, src,
+            dst, B->sh);
+  if (mc && mc->n) BLAUNCH(k_b_coarsest<T>, mc->n, kBThreads, B->smem_dense, st, probs_of<T>(B), mc->e, d, B->sh);
   b_prof(B, 4, st);
   return 0;
 }
@@ -399,7 +419,7 @@ template <class T, int MODE>
 int b_fine(pycfd_batch* B, int src, int dst, cudaStream_t st) {
   const int id = MODE == FM_LAST ? 2 : MODE == FM_PRE ? 3 : 0;
   b_prof(B, id, st);
-  BLAUNCH((k_b_fine<T, MODE>), B->fine.n, kBFineBlock, 0, st, probs_of<T>(B), hiers_of<T>(B), B->fine.e, src,
+  BLAUNCH((k_b_fine<T, MODE>), B->strip.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->strip.e, src,
           dst, B->sh);
   b_prof(B, id, st);
   return 0;
@@ -411,7 +431,8 @@ template <class T>
 int b_tails(pycfd_batch* B, cudaStream_t st) {
   if (B->mapT.n == 0) return 0;
   b_prof(B, 4, st);
-  BLAUNCH(k_b_tail<T>, B->mapT.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT.e, B->sprobs, B->sh);
+  BLAUNCH(k_b_tail<T>, B->mapT.n, kTailThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->mapT.e, B->sprobs,
+          B->sh);
   b_prof(B, 4, st);
   return 0;
 }
@@ -562,10 +583,10 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
   auto pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
     b_prof(B, 1, s2);
-    BLAUNCH(k_b_cg_pq<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
+    BLAUNCH(k_b_cg_pq<T>, B->strip.n, kBThreads, 0, s2, P, B->strip.e, B->sh);
     b_prof(B, 1, s2);
     b_prof(B, 5, s2);
-    BLAUNCH(k_b_cg_xr<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, B->maxiter, B->sh, ctl);
+    BLAUNCH(k_b_cg_xr<T>, B->strip.n, kBThreads, 0, s2, P, B->n, B->strip.e, B->maxiter, B->sh, ctl);
     b_prof(B, 5, s2);
     return 0;
   };
@@ -599,10 +620,10 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
   auto inner_pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
     b_prof(B, 1, s2);
-    BLAUNCH(k_b_cg_pq<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
+    BLAUNCH(k_b_cg_pq<T>, B->strip.n, kBThreads, 0, s2, P, B->strip.e, B->sh);
     b_prof(B, 1, s2);
     b_prof(B, 5, s2);
-    BLAUNCH(k_b_cg_xr<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, kInnerMaxIterB, B->sh, inner);
+    BLAUNCH(k_b_cg_xr<T>, B->strip.n, kBThreads, 0, s2, P, B->n, B->strip.e, kInnerMaxIterB, B->sh, inner);
     b_prof(B, 5, s2);
     return 0;
   };
@@ -824,6 +845,28 @@ int pycfd_batch_profile(pycfd_batch* B, int kernel_id) {
 int pycfd_batch_profile_read(pycfd_batch* B, double* total_ms, int* launches, void* stream) {
   if (!B) return fail(PCFD_E_ARG, "bad arguments");
   return pycfd_profile_read(B->mem, total_ms, launches, stream);
+}
+
+int pycfd_batch_set_loop_cap(pycfd_batch* B, int cap, void* stream) {
+  if (!B || cap < 0) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  std::vector<unsigned> c(TK_COUNT, 0u);
+  c[TK_CG] = c[TK_IR] = (unsigned)cap;
+  CU(cudaMemcpyAsync(B->sh.cap_set, c.data(), TK_COUNT * sizeof(unsigned), cudaMemcpyHostToDevice, sm));
+  CU(cudaStreamSynchronize(sm));
+  return 0;
+}
+
+int pycfd_batch_capped(pycfd_batch* B, int* capped, void* stream) {
+  if (!B || !capped) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  int h[TK_COUNT];
+  CU(cudaMemcpyAsync(h, B->sh.capped, sizeof h, cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  *capped = (h[TK_CG] ? 1 : 0) | (h[TK_IR] ? 2 : 0);
+  CU(cudaMemsetAsync(B->sh.capped, 0, sizeof h, sm));
+  CU(cudaStreamSynchronize(sm));
+  return 0;
 }
 
 pycfd_solver* pycfd_batch_problem(pycfd_batch* B, int i) {

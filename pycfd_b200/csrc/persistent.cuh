@@ -33,7 +33,7 @@ constexpr int kPThreads = 512;
 constexpr int kPMaxLevels = 12;
 constexpr int kPDenseMax = 1024;                            // coarsest rows solved in CTA 0
 constexpr int kPMaxNV = 4;                                  // sums per all-reduce
-constexpr unsigned long long kPWaitLimitNs = 2000000000ull;  // 2 s per barrier wait
+constexpr unsigned long long kPWaitLimitNs = 2000000000ull;  // default limit of one barrier wait: 2 s
 constexpr int kPStatusTimeout = -6;
 constexpr int kPTraceCap = 8192;                            // words of the phase trace
 
@@ -70,6 +70,7 @@ struct PSolve {
   double* partials;            // 2 x kPMaxNV x gridDim.x (alternating slots)
   unsigned* bar;               // [0] arrivals, [32] error word; zeroed before every launch
   unsigned long long* trace;   // optional: [0] count, then (globaltimer, tag) pairs
+  unsigned long long wait_ns;  // limit of one barrier wait (kPWaitLimitNs unless set)
 };
 
 __device__ __forceinline__ unsigned p_ld_relaxed(const unsigned* p) {
@@ -90,6 +91,7 @@ struct PBar {
   unsigned red;                // all-reduces so far (selects the partials slot)
   unsigned long long* trace;   // CTA 0 only
   int ntr;
+  unsigned long long wait_ns;  // limit of one barrier wait
 };
 
 __device__ __forceinline__ bool p_failed(const PBar& pb) { return p_ld_relaxed(pb.bar + 32) != 0u; }
@@ -107,7 +109,7 @@ __device__ __forceinline__ void p_sync(PBar& pb, int tag) {
     while (p_ld_relaxed(pb.bar) < pb.target) {
       if ((++k & 63) == 0) {
         if (p_failed(pb)) break;                      // another CTA gave up
-        if (p_clock_ns() - t0 > kPWaitLimitNs) {
+        if (p_clock_ns() - t0 > pb.wait_ns) {
           atomicExch(pb.bar + 32, 1u);
           break;
         }
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(kPThreads, 2) k_solve_persistent(PSolve<T> t) 
   const uint8_t* fl = t.flags;
   const SolveCfg cfg = t.cfg;
   const int nf = g.n_fluid;
-  PBar pb{t.bar, 0u, 0u, (blockIdx.x == 0) ? t.trace : nullptr, 0};
+  PBar pb{t.bar, 0u, 0u, (blockIdx.x == 0) ? t.trace : nullptr, 0, t.wait_ns};
   if (threadIdx.x < 32) {
     Geo g0 = g;   // fine_diag's sums without the Dirichlet terms
     g0.dir_w = g0.dir_e = g0.dir_s = g0.dir_n = 0;

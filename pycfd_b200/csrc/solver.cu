@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "multigrid.cuh"
 #include "persistent.cuh"
+#include "masks.cuh"
 #include "poisson.cuh"
 #include "stencil.cuh"
 
@@ -159,6 +160,7 @@ struct pycfd_solver {
   int cluster_size = 0;         // CTAs per cluster (0: not used)
   // whole CG / MG-PCG solves as one cooperative launch
   int persistent = 0;           // CTAs of that launch (0: one kernel per phase)
+  unsigned long long wait_ns = kPWaitLimitNs;   // limit of one grid-barrier wait of that launch
   unsigned* pbar = nullptr;     // barrier words, zeroed before every launch
   double* ppart = nullptr;      // per-CTA partial sums
   unsigned long long* ptrace = nullptr;   // phase trace (measurement support)
@@ -886,6 +888,7 @@ int solve_persistent(pycfd_solver* s, double* x, bool has_x0, cudaStream_t strea
   t.partials = s->ppart;
   t.bar = s->pbar;
   t.trace = s->trace_on ? s->ptrace : nullptr;
+  t.wait_ns = s->wait_ns;
   CU(cudaMemsetAsync(s->pbar, 0, 64 * sizeof(unsigned), stream));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(s->persistent);
@@ -1708,6 +1711,13 @@ int pycfd_solve_trace(pycfd_solver* s, int enable, unsigned long long* out, int 
   return 0;
 }
 
+int pycfd_solver_set_wait_limit(pycfd_solver* s, unsigned long long ns) {
+  if (!s || ns == 0) return fail(PCFD_E_ARG, "bad arguments");
+  if (!s->persistent) return fail(PCFD_E_UNSUPPORTED, "the solver does not run persistent solves");
+  s->wait_ns = ns;
+  return 0;
+}
+
 int pycfd_solver_persistent(pycfd_solver* s, int* ctas) {
   if (!s || !ctas) return fail(PCFD_E_ARG, "bad arguments");
   *ctas = s->persistent;
@@ -1733,6 +1743,69 @@ int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* s
   *total_ms = t;
   *launches = s->prof_n / 2;
   s->prof_n = 0;
+  return 0;
+}
+
+int pycfd_rasterize(const pycfd_shape* shape, const double* xf, const double* dx_cells, const double* yf,
+                    const double* dy_cells, int nx, int ny, double lx, double ly, int subsamples,
+                    double* fraction, uint8_t* mask, void* stream) {
+  if (!shape || !xf || !dx_cells || !yf || !dy_cells || !fraction || !mask || nx < 1 || ny < 1)
+    return fail(PCFD_E_ARG, "bad arguments");
+  if (subsamples < 1 || subsamples > 64) return fail(PCFD_E_ARG, "subsamples must be 1..64, got %d", subsamples);
+  ShapeDev d{};
+  d.kind = shape->kind;
+  d.p0 = shape->p[0];
+  d.p1 = shape->p[1];
+  d.p2 = shape->p[2];
+  d.p3 = shape->p[3];
+  d.lx = lx;
+  d.ly = ly;
+  switch (shape->kind) {
+    case PCFD_SHAPE_CIRCLE:
+    case PCFD_SHAPE_RECTANGLE: break;
+    case PCFD_SHAPE_POLYGON:
+      if (!shape->verts || shape->n_verts < 3) return fail(PCFD_E_ARG, "a polygon needs at least 3 vertices");
+      d.verts = shape->verts;
+      d.n_verts = shape->n_verts;
+      break;
+    case PCFD_SHAPE_IMAGE:
+      if (!shape->image || shape->rows < 1 || shape->cols < 1 || !(lx > 0) || !(ly > 0))
+        return fail(PCFD_E_ARG, "bad image");
+      d.image = shape->image;
+      d.rows = shape->rows;
+      d.cols = shape->cols;
+      d.threshold = shape->threshold;
+      d.invert = shape->invert;
+      break;
+    default: return fail(PCFD_E_ARG, "unknown shape kind %d", shape->kind);
+  }
+  const long n = (long)nx * ny;
+  k_solid_fraction<<<grid_for(n, 256, 148 * 8), 256, 0, st(stream)>>>(d, xf, dx_cells, yf, dy_cells, nx, ny,
+                                                                         subsamples, fraction, mask);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_face_lists(pycfd_solver* s, int* u_faces, int u_cap, int* v_faces, int v_cap, int* n_u,
+                     int* n_v, int* body_u_start, int* body_v_start, int* n_bodies, int* lohi) {
+  if (!s || !n_u || !n_v || u_cap < 0 || v_cap < 0) return fail(PCFD_E_ARG, "bad arguments");
+  *n_u = s->bc.n_mask_u;
+  *n_v = s->bc.n_mask_v;
+  const int cu = std::min(u_cap, s->bc.n_mask_u), cv = std::min(v_cap, s->bc.n_mask_v);
+  if (cu > 0 && u_faces) CU(cudaMemcpy(u_faces, s->mask_u, sizeof(int) * cu, cudaMemcpyDeviceToHost));
+  if (cv > 0 && v_faces) CU(cudaMemcpy(v_faces, s->mask_v, sizeof(int) * cv, cudaMemcpyDeviceToHost));
+  const int nb = s->bc.n_bodies;
+  if (n_bodies) *n_bodies = nb;
+  for (int b = 0; b <= std::max(nb, 1) && b <= PCFD_MAX_BODIES; ++b) {
+    if (body_u_start) body_u_start[b] = s->bc.body_u_start[b];
+    if (body_v_start) body_v_start[b] = s->bc.body_v_start[b];
+  }
+  if (lohi) {
+    lohi[0] = s->g.u_lo;
+    lohi[1] = s->g.u_hi;
+    lohi[2] = s->g.v_lo;
+    lohi[3] = s->g.v_hi;
+  }
   return 0;
 }
 
@@ -1785,10 +1858,9 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
 // Field reduction without device allocation
 // ============================================================================
 // Some hosts cannot call cudaMalloc at the moment they want a reduction: an
-// application that hands every byte of device memory to its own allocator, a
-// real-time loop that must not take the implicit device synchronisation of an
-// allocation, or code that builds its work while a stream is being captured.
-// This entry point serves them.  Its scratch -- one block of scalar slots laid
+// application that hands every byte of device memory to its own allocator, or a
+// loop that must not take the device-wide synchronisation an allocation may
+// impose.  This entry point serves them.  Its scratch -- one block of scalar slots laid
 // out like a solver's (the results land in the statistics slots), one row of 8
 // partial sums per thread block and the ticket counter of the grid reduction --
 // is the file-scope array below: PCFD_NOALLOC_MAX_ROWS*8 + S_COUNT + 2 doubles
@@ -1803,7 +1875,8 @@ double* g_noalloc_addr[128] = {};   // device address of the scratch, per device
 
 // Host code must not use the array's name as a device address (it names a
 // host-side stand-in); the address is looked up once per device, with that
-// device current, and cached.
+// device current, and cached for the life of the process (a cudaDeviceReset
+// makes the cached address stale).
 int noalloc_scratch(double** out) {
   int dev = 0;
   CU(cudaGetDevice(&dev));
@@ -1825,7 +1898,7 @@ extern "C" int pycfd_reduce_fields_noalloc(const double* u, const double* v, con
                                            pycfd_field_stats* o, void* stream) {
   if (!u || !v || !o || nx < 1 || ny < 1 || !(dx > 0) || !(dy > 0))
     return fail(PCFD_E_ARG, "bad arguments");
-  if (nx + 3 > PCFD_NOALLOC_MAX_ROWS)
+  if (nx > PCFD_NOALLOC_MAX_ROWS - 3)
     return fail(PCFD_E_ARG,
                 "pycfd_reduce_fields_noalloc handles nx <= %d (its static scratch holds %d block rows); "
                 "got nx = %d -- use pycfd_reduce_fields for larger grids",

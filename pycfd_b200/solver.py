@@ -23,6 +23,9 @@ from .fields import FlowField
 from .hierarchy import assemble, fused_for, hierarchy_for, tail_for
 from .mesh import StructuredMesh
 
+#: solve status of a persistent (cooperative) solve whose grid barrier ran out of time
+PERSISTENT_TIMEOUT = -6
+
 
 @dataclass
 class GpuOptions:
@@ -381,6 +384,13 @@ class ProjectionSolver:
         #: CTAs of the cooperative launch of each CG / MG-PCG solve (0: per-phase kernels)
         self._persistent = int(ctas.value)
 
+    def set_wait_limit(self, seconds: float) -> None:
+        """Limit of one grid-barrier wait of the persistent solve (default 2 s).  A
+        wait that runs out ends the solve with a ``RuntimeError``; the solver stays
+        usable.  Only solvers built with ``GpuOptions(persistent_solve=True)``."""
+        ns = max(1, int(round(seconds * 1e9)))
+        _lib.check(self._L.pycfd_solver_set_wait_limit(self._h, C.c_ulonglong(ns)))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
@@ -410,6 +420,10 @@ class ProjectionSolver:
             if self.body_masks:
                 self.body_force_reactions = tuple((st.body_fx[k], st.body_fy[k])
                                                   for k in range(len(self.body_masks)))
+        if raise_on_error and st.status == PERSISTENT_TIMEOUT:
+            raise RuntimeError(
+                "the persistent pressure solve stopped: a grid barrier waited longer than its limit "
+                "(a CTA did not arrive); the result of this solve is not valid")
         if raise_on_error and st.status != 0:
             kind = self.config.pressure_solver
             raise RuntimeError(

@@ -99,34 +99,49 @@ class TimeStepper:
         max_steps = self.config.max_steps if max_steps is None else max_steps
         history = {k: [] for k in ("step", "t", "dt", "cfl", "max_div", "kinetic_energy",
                                    "residual", "fx", "fy")}
+        bar = None
+        if progress:
+            # a bar over simulated time, as the reference shows (timestepper.py:174-181)
+            try:
+                from tqdm.auto import tqdm
+                bar = tqdm(total=float(t_end), initial=float(fields.t), unit="s",
+                           desc=self.config.name, dynamic_ncols=True)
+            except ImportError:
+                log.warning("tqdm not installed; running without a progress bar")
         wall_start = time.perf_counter()
         converged = False
         steps_taken = 0
-        while fields.t < t_end - 1e-12:
-            if max_steps is not None and steps_taken >= max_steps:
-                break
-            dt = self.compute_dt(fields)
-            self._check_health(fields, dt)
-            dt = min(dt, t_end - fields.t)
-            self.solver.set_upwind_blend(self.solver.upwind_blend_for(fields, dt))
-            previous = fields
-            fields = self.solver.advance(previous, dt)
-            steps_taken += 1
-            st = self.solver.field_stats(fields, previous)
-            fields._stats = st
-            rate_of_change = max(st.max_du, st.max_dv) / dt
-            if steps_taken % record_every == 0:
-                info = self._diagnostics(fields, dt, rate_of_change)
-                for k, val in info.items():
-                    if k in history:
-                        history[k].append(val)
-                fields.diagnostics = info
-            if callback is not None and steps_taken % callback_every == 0:
-                callback(fields, fields.diagnostics or self._diagnostics(fields, dt, rate_of_change))
-            if self.config.steady_tol is not None and rate_of_change < self.config.steady_tol:
-                converged = True
-                break
-        self._check_health(fields, self.config.dt)
+        try:
+            while fields.t < t_end - 1e-12:
+                if max_steps is not None and steps_taken >= max_steps:
+                    break
+                dt = self.compute_dt(fields)
+                self._check_health(fields, dt)
+                dt = min(dt, t_end - fields.t)
+                self.solver.set_upwind_blend(self.solver.upwind_blend_for(fields, dt))
+                previous = fields
+                fields = self.solver.advance(previous, dt)
+                steps_taken += 1
+                st = self.solver.field_stats(fields, previous)
+                fields._stats = st
+                rate_of_change = max(st.max_du, st.max_dv) / dt
+                if steps_taken % record_every == 0:
+                    info = self._diagnostics(fields, dt, rate_of_change)
+                    for k, val in info.items():
+                        if k in history:
+                            history[k].append(val)
+                    fields.diagnostics = info
+                if callback is not None and steps_taken % callback_every == 0:
+                    callback(fields, fields.diagnostics or self._diagnostics(fields, dt, rate_of_change))
+                if bar is not None:
+                    bar.update(float(dt))
+                if self.config.steady_tol is not None and rate_of_change < self.config.steady_tol:
+                    converged = True
+                    break
+            self._check_health(fields, self.config.dt)
+        finally:
+            if bar is not None:
+                bar.close()
         wall = time.perf_counter() - wall_start
         if callback is not None:
             callback(fields, fields.diagnostics or self._diagnostics(fields, self.config.dt,

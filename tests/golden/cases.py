@@ -138,3 +138,57 @@ def step_init(spec, nx, ny, lx, ly):
         u_init = 0.1 * rng.standard_normal((nx + 1, ny))
         v_init = 0.1 * rng.standard_normal((nx, ny + 1))
     return u_init, v_init
+
+
+# Face-flag layouts: bodies as index boxes (i0, i1, j0, j1) of solid cells, so both
+# packages build the same masks without any rasterisation.  Each body is one
+# connected set; a body may span a periodic seam (cells on both sides of it).
+FACE_CASES = {
+    "seam_x": dict(cfg=dict(nx=24, ny=16, re=50.0, pressure_solver="cg", poisson_tol=1e-10,
+                            boundary_config=bcs(left=("periodic",), right=("periodic",))),
+                   bodies=[[(0, 3, 5, 9), (21, 24, 5, 9)]]),
+    "seam_y": dict(cfg=dict(nx=20, ny=24, re=50.0, pressure_solver="cg", poisson_tol=1e-10,
+                            boundary_config=bcs(left=("inlet", 1.0), right=("outlet",),
+                                                bottom=("periodic",), top=("periodic",))),
+                   bodies=[[(6, 10, 0, 2), (6, 10, 22, 24)]]),
+    "outlet_touch": dict(cfg=dict(nx=28, ny=16, re=50.0, pressure_solver="cg", poisson_tol=1e-10,
+                                  boundary_config=bcs(left=("inlet", 1.0),
+                                                      right=("pressure_outlet", 0.0, "uniform", 0.0),
+                                                      bottom=("symmetry",), top=("symmetry",))),
+                         bodies=[[(25, 28, 6, 10)], [(8, 12, 3, 7)]]),
+    "walls_two_bodies": dict(cfg=dict(nx=18, ny=18, re=50.0, pressure_solver="cg", poisson_tol=1e-10,
+                                      boundary_config=bcs(top=("moving_wall", 1.0))),
+                             bodies=[[(0, 4, 0, 3)], [(9, 12, 8, 13)], [(14, 18, 15, 18)]]),
+}
+
+
+def face_bodies(case, nx, ny):
+    """Per-body boolean masks of a face case."""
+    out = []
+    for boxes in case["bodies"]:
+        m = np.zeros((nx, ny), dtype=bool)
+        for i0, i1, j0, j1 in boxes:
+            m[i0:i1, j0:j1] = True
+        out.append(m)
+    return out
+
+
+# Shapes for the rasteriser fixtures (plain data).
+STAR = [(0.55 + (0.28 if k % 2 == 0 else 0.12) * np.cos(np.pi * k / 6),
+         0.45 + (0.28 if k % 2 == 0 else 0.12) * np.sin(np.pi * k / 6)) for k in range(12)]
+SHAPE_MESH = dict(nx=200, ny=120, lx=1.6, ly=1.0)
+
+
+def shape_image(rows=37, cols=53, seed=4):
+    """An RGBA 8-bit picture: a dark ellipse and a dark bar on a light, noisy background."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:rows, 0:cols]
+    lum = 0.85 + 0.1 * rng.random((rows, cols))
+    lum[((xx - 20) / 9.0) ** 2 + ((yy - 14) / 6.0) ** 2 <= 1.0] = 0.1
+    lum[28:32, 30:48] = 0.3
+    img = np.empty((rows, cols, 4), dtype=np.uint8)
+    img[..., 0] = np.round(255 * lum)
+    img[..., 1] = np.round(255 * np.clip(lum * 0.9, 0, 1))
+    img[..., 2] = np.round(255 * np.clip(lum * 1.05, 0, 1))
+    img[..., 3] = 255
+    return img

@@ -1,11 +1,11 @@
 """Generate the golden fixtures in this folder by running the reference itself.
 
 The reference (kiliancmd/pycfd, pure Python) is imported from a source tree given
-on the command line (default ``/root/reference``) and driven through its own
+given as the first command-line argument, and driven through its own
 public API.  Nothing here runs on the GPU host: the fixtures it writes are the
 committed ``*.npz`` files beside this script, which the tests read.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 Cases (all seeded, all synthetic):
   rhs.npz        momentum RHS (Numba kernel) on random ghosted fields, blend 0 / 0.6
@@ -16,6 +16,9 @@ Cases (all seeded, all synthetic):
   cavity64.npz   64x64 lid cavity, Re 100, CG 1e-10, adaptive dt: steps 100/500/2000
   cylinder.npz   256x128 cylinder channel, MG-PCG, 30 steps with Cd/Cl history
   masks.npz      circle_mask at 2048x1024 (packed bits) and at 256x128
+  faces.npz      face ranges and face solid flags (total, per body) for four layouts
+  cylinder_long.npz  512x256 cylinder, MG-PCG, 2000 steps: Cd/Cl/t history
+  shapes.npz     polygon, rectangle and image masks with their fractions (200x120)
 """
 
 from __future__ import annotations
@@ -26,7 +29,9 @@ import time
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python tests/golden/make_golden.py <path to the reference source tree>")
+REF = sys.argv[1]
 sys.path.insert(0, REF)
 
 from pycfd.config import BCKind, BCSpec, SimulationConfig  # noqa: E402
@@ -233,6 +238,82 @@ def gen_cylinder():
          cl=np.array(cl), mask=ob.mask)
 
 
+def gen_faces():
+    """Solvable face ranges and face solid flags, total and per body
+    (pycfd/core/solver.py:62-79, :235-296), for bodies on periodic seams, at a
+    pressure outlet and against walls."""
+    out = {}
+    for name, case in cases.FACE_CASES.items():
+        cfg = ref_config({**dict(dt=1e-3, t_end=1.0, adaptive_dt=False, name=name), **case["cfg"]})
+        bodies = cases.face_bodies(case, cfg.nx, cfg.ny)
+        solid = np.logical_or.reduce(bodies)
+        s = ProjectionSolver(cfg, None, solid, bodies=bodies)
+        out[f"{name}_upd"] = np.array([s.u_upd[0].start, s.u_upd[0].stop, s.v_upd[1].start,
+                                       s.v_upd[1].stop])
+        out[f"{name}_u_face_solid"] = s.u_face_solid
+        out[f"{name}_v_face_solid"] = s.v_face_solid
+        if s.u_face_body:                      # kept only for two or more bodies
+            out[f"{name}_u_face_body"] = np.stack(s.u_face_body)
+            out[f"{name}_v_face_body"] = np.stack(s.v_face_body)
+    save("faces.npz", **out)
+
+
+def gen_cylinder_long():
+    """512x256 cylinder channel (the 2048x1024 case at reduced grid), MG-PCG 1e-10,
+    adaptive dt: Cd, Cl and t after each of 2000 steps, and every 16th value of the
+    final u, v, p."""
+    nx, ny, steps = 512, 256, 2000
+    cfg = ref_config(cases.cylinder_cfg(nx, ny))
+    ob = circle_mask(StructuredMesh.from_config(cfg), (0.5, 0.5), 0.05)
+    u0, v0 = cases.cylinder_init(nx, ny)
+    sim = Simulation(cfg, obstacle=ob, u_init=u0, v_init=v0)
+    cd, cl, t = [], [], []
+    for k in range(steps):
+        sim.run(max_steps=1)
+        c = sim.force_coefficients()
+        cd.append(c[0])
+        cl.append(c[1])
+        t.append(sim.fields.t)
+        if (k + 1) % 200 == 0:
+            print(f"  cylinder_long step {k + 1}: t={t[-1]:.5f} cd={cd[-1]:.8f} cl={cl[-1]:.3e}",
+                  flush=True)
+    f = sim.fields
+    save("cylinder_long.npz", cd=np.array(cd), cl=np.array(cl), t=np.array(t),
+         u16=f.u[::16, ::16], v16=f.v[::16, ::16], p16=f.p[::16, ::16])
+
+
+def gen_shapes():
+    """polygon_mask (a 12-point star), rectangle_mask and mask_from_image (the
+    picture of cases.shape_image, handed to the reference through a stand-in for
+    matplotlib.image.imread, which is not installed here) on a 200x120 mesh:
+    fraction and mask of each (pycfd/geometry/obstacles.py:87-367)."""
+    import types
+    from pycfd.geometry import obstacles as ob
+    img = cases.shape_image()
+    mpl = types.ModuleType("matplotlib")
+    mpl_image = types.ModuleType("matplotlib.image")
+    mpl_image.imread = lambda path: img
+    mpl.image = mpl_image
+    sys.modules.setdefault("matplotlib", mpl)
+    sys.modules["matplotlib.image"] = mpl_image
+    m = cases.SHAPE_MESH
+    mesh = StructuredMesh(m["nx"], m["ny"], m["lx"], m["ly"])
+    star = np.array(cases.STAR)
+    pg = ob.polygon_mask(mesh, star)
+    rc = ob.rectangle_mask(mesh, (0.31, 0.22), (0.93, 0.61))
+    path = os.path.join(os.path.dirname(__file__), "_unused.png")
+    open(path, "wb").close()                 # the reference checks that the path exists
+    try:
+        im = ob.mask_from_image(mesh, path, threshold=0.5)
+        im2 = ob.mask_from_image(mesh, path, threshold=0.5, invert=True, subsamples=3)
+    finally:
+        os.remove(path)
+    save("shapes.npz", star=star, poly_frac=pg.fraction, poly_mask=pg.mask,
+         poly_len=np.array(pg.characteristic_length), rect_frac=rc.fraction, rect_mask=rc.mask,
+         image=img, img_frac=im.fraction, img_mask=im.mask, img_len=np.array(im.characteristic_length),
+         img_inv_frac=im2.fraction, img_inv_mask=im2.mask)
+
+
 def gen_masks():
     big = StructuredMesh(2048, 1024, 2.0, 1.0)
     m = circle_mask(big, (0.5, 0.5), 0.05).mask
@@ -244,9 +325,9 @@ def gen_masks():
 
 if __name__ == "__main__":
     which = set(sys.argv[2:]) or {"rhs", "poisson", "multigrid", "solvers", "steps",
-                                  "cavity64", "cylinder", "masks"}
+                                  "cavity64", "cylinder", "masks", "faces", "cylinder_long", "shapes"}
     for name in ("rhs", "poisson", "multigrid", "solvers", "steps", "cavity64",
-                 "cylinder", "masks"):
+                 "cylinder", "masks", "faces", "cylinder_long", "shapes"):
         if name in which:
             t0 = time.perf_counter()
             globals()["gen_" + name]()

@@ -175,17 +175,21 @@ def test_dense_tail_matches_level_by_level(precision):
     over the structure's problems) against the level-by-level cycle."""
     from pycfd_b200.batch import BatchedSolver, BatchOptions
     cfgs = _cavities(count=7, seed=3)
-    out = []
+    out, its = [], []
     for tail in (True, False):
         b = BatchedSolver(cfgs, BatchOptions(precision=precision, coarse_tail=tail, tail_ratio=None))
         assert not tail or b._tailed == len(cfgs)
         b.step(6)
         out.append([b.fields[k].numpy() for k in range(len(cfgs))])
-        assert all(f == 0 for f in b.status()["frozen"])
+        st = b.status()
+        assert all(f == 0 for f in st["frozen"])
+        its.append(st["iterations"])
     bound = 1e-9 if precision == "fp64" else 1e-7
     for fa, fb in zip(*out):
         for x, y in zip(fa[:2], fb[:2]):
             assert rel(x, y) < bound
+    # the same preconditioner up to rounding: the same CG passes per step (within one per solve)
+    assert np.abs(its[0] - its[1]).max() <= 3, its
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -208,3 +212,26 @@ def test_fused_restriction_matches_two_phase_down_sweep(precision):
         for fa, fb in zip(out[k], out[2]):
             for x, y in zip(fa[:2], fb[:2]):
                 assert rel(x, y) < bound
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_loop_cap_ends_device_loops_and_the_batch_goes_on(precision):
+    """The pass cap of the device-side WHILE loops, set low from the host, ends every
+    solve of a step early (reported per loop, problems unconverged, no hang); with
+    the built-in cap restored the next steps converge again."""
+    from pycfd_b200.batch import BatchedSolver, BatchOptions
+    cfgs = _cavities(count=3, seed=5)
+    b = BatchedSolver(cfgs, BatchOptions(precision=precision))
+    b.step(2)
+    assert b.capped() == 0
+    assert (b.status()["status"] == 0).all()
+    b.set_loop_cap(2)
+    b.step(1)
+    assert b.capped() & 1
+    st = b.status()
+    assert (st["status"] == -3).any() and (st["frozen"] == 0).all()
+    b.set_loop_cap(0)
+    b.step(2)
+    assert b.capped() == 0
+    st = b.status()
+    assert (st["status"] == 0).all() and (st["steps"] == 5).all()

@@ -251,3 +251,35 @@ def test_cylinder_force_history(lib, golden):
     assert np.abs(np.array(cl) - g["cl"]).max() < 1e-8 * np.abs(g["cd"]).max()
     u, v, p = sim.fields.numpy()
     assert rel(u, g["u"]) < 1e-10 and rel(v, g["v"]) < 1e-10 and rel(p, g["p"]) < 1e-10
+
+
+def test_cylinder_long_force_history(lib, golden):
+    """512x256 cylinder channel (the 2048x1024 case at reduced grid), MG-PCG 1e-10,
+    adaptive dt: Cd/Cl after each of 2000 steps against the reference's own history,
+    the clock step for step, and a 1-in-16 sample of the final u, v, p."""
+    from pycfd_b200.obstacles import circle_mask
+    from pycfd_b200.simulation import Simulation
+    from pycfd_b200.mesh import StructuredMesh
+    g = golden("cylinder_long.npz")
+    cfg = _cfg(cases.cylinder_cfg(512, 256))
+    ob = circle_mask(StructuredMesh.from_config(cfg), (0.5, 0.5), 0.05)
+    u0, v0 = cases.cylinder_init(512, 256)
+    sim = Simulation(cfg, obstacle=ob, u_init=u0, v_init=v0)
+    cd, cl, t = [], [], []
+    for _ in range(len(g["cd"])):
+        sim.run(max_steps=1)
+        c = sim.force_coefficients()
+        cd.append(c[0])
+        cl.append(c[1])
+        t.append(sim.fields.t)
+    cd, cl, t = np.array(cd), np.array(cl), np.array(t)
+    scale = np.abs(g["cd"]).max()
+    print(f"cylinder 512x256, 2000 steps: max|dCd| {np.abs(cd - g['cd']).max():.3e}, "
+          f"max|dCl| {np.abs(cl - g['cl']).max():.3e}, max|dt| {np.abs(t - g['t']).max():.3e}")
+    assert np.abs(t - g["t"]).max() <= 1e-12 * g["t"][-1]
+    assert np.abs(cd - g["cd"]).max() <= 1e-8 * scale
+    assert np.abs(cl - g["cl"]).max() <= 1e-8 * scale
+    u, v, p = sim.fields.numpy()
+    assert rel(u[::16, ::16], g["u16"]) < 1e-8
+    assert rel(v[::16, ::16], g["v16"]) < 1e-8
+    assert rel(p[::16, ::16], g["p16"]) < 1e-8

@@ -146,3 +146,27 @@ def test_dense_tail_matches_level_by_level(n, sweeps, persistent):
         for x, y in zip(out[k], out[2]):
             assert _rel(x, y) < 1e-9
         assert all(abs(p - q) <= 2 for p, q in zip(its[k], its[2])), its
+
+
+def test_barrier_wait_limit_ends_the_solve_and_the_solver_stays_usable():
+    """A grid-barrier wait that runs out (limit set to 1 ns, so the first CTA that has
+    to wait gives up) ends the persistent solve with status -6 -- reported as a
+    RuntimeError, no fault, no hang -- and the next solve with the default limit
+    is correct."""
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    cfg = _cfg(dict(nx=64, ny=64, re=100.0, pressure_solver="mgcg", poisson_tol=1e-12,
+                    boundary_config=FAMILIES["cavity"]))
+    s = ProjectionSolver(cfg, options=GpuOptions(persistent_solve=True, graphs=False))
+    assert s._persistent
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((64, 64))
+    rhs -= rhs.mean()
+    ref = s.pressure_solver.solve(rhs).cpu().numpy()
+    s.set_wait_limit(1e-9)
+    with pytest.raises(RuntimeError, match="grid barrier"):
+        s.pressure_solver.solve(rhs)
+    assert s.last_stats.status == -6
+    s.set_wait_limit(2.0)
+    again = s.pressure_solver.solve(rhs).cpu().numpy()
+    assert s.last_stats.status == 0
+    assert _rel(again, ref) < 1e-12
