@@ -192,3 +192,8 @@ def shape_image(rows=37, cols=53, seed=4):
     img[..., 2] = np.round(255 * np.clip(lum * 1.05, 0, 1))
     img[..., 3] = 255
     return img
+
+
+CKPT_CAVITY = dict(nx=32, ny=32, re=100.0, dt=1.0, t_end=1e9, cfl_max=0.5, adaptive_dt=True,
+                   pressure_solver="mgcg", poisson_tol=1e-12,
+                   boundary_config=bcs(top=("moving_wall", 1.0)), name="ckpt_cavity")

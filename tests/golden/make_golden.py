@@ -19,6 +19,8 @@ Cases (all seeded, all synthetic):
   faces.npz      face ranges and face solid flags (total, per body) for four layouts
   cylinder_long.npz  512x256 cylinder, MG-PCG, 2000 steps: Cd/Cl/t history
   shapes.npz     polygon, rectangle and image masks with their fractions (200x120)
+  ref_checkpoint.npz (+ _continued)  a reference checkpoint and the state 10 steps on
+  interchange.npz  this package's checkpoint writer read back by the reference's loader
 """
 
 from __future__ import annotations
@@ -314,6 +316,56 @@ def gen_shapes():
          img_inv_frac=im2.fraction, img_inv_mask=im2.mask)
 
 
+def gen_checkpoint():
+    """A checkpoint written by the reference's own save_checkpoint (cavity 32x32,
+    Re 100, MG-PCG 1e-12, 20 adaptive steps) and the reference's state 10 steps
+    after resuming from it (pycfd/analysis/export.py:214-276)."""
+    cfg = ref_config(cases.CKPT_CAVITY)
+    sim = Simulation(cfg)
+    sim.run(max_steps=20)
+    path = os.path.join(os.path.dirname(__file__), "ref_checkpoint.npz")
+    sim.save_checkpoint(path)
+    side = os.path.join(os.path.dirname(__file__), "ref_checkpoint.provenance.json")
+    if os.path.exists(side):
+        os.remove(side)                      # the archive embeds the same record
+    sim2 = Simulation.from_checkpoint(path)
+    sim2.run(max_steps=10)
+    f = sim2.fields
+    save("ref_checkpoint_continued.npz", u=f.u, v=f.v, p=f.p, t=np.array(f.t), step=np.array(f.step))
+
+
+def gen_interchange():
+    """A checkpoint written by THIS package's writer (from host arrays, the same code
+    path a GPU run takes after its device-to-host copy), loaded with the
+    reference's own load_checkpoint (pycfd/analysis/export.py:253-276); records
+    that it loaded and matched.  Needs pycfd_b200 importable beside the reference."""
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    sys.path.insert(0, root)
+    import json
+    from pycfd.analysis.export import load_checkpoint
+    from pycfd_b200 import export as ours
+    from pycfd_b200.config import BCKind as OK, BCSpec as OS, SimulationConfig as OC
+    from pycfd_b200.fields import FlowField as OF
+    from pycfd_b200.mesh import StructuredMesh as OM
+    g = np.load(os.path.join(os.path.dirname(__file__), "ref_checkpoint_continued.npz"))
+    cfg = cases.to_config(cases.CKPT_CAVITY, OC, OS, OK)
+    f = OF.from_numpy(OM.from_config(cfg), g["u"], g["v"], g["p"], float(g["t"]), int(g["step"]),
+                      device="cpu")
+    tmp = os.path.join(os.path.dirname(__file__), "_ours_tmp.npz")
+    try:
+        ours.save_checkpoint(f, cfg, tmp)
+        rf, rcfg = load_checkpoint(tmp)
+        same = (np.array_equal(rf.u, g["u"]) and np.array_equal(rf.v, g["v"])
+                and np.array_equal(rf.p, g["p"]) and rf.t == float(g["t"]) and rf.step == int(g["step"]))
+        cfg_same = rcfg.to_dict() == json.loads(cfg.to_json())
+    finally:
+        for x in (tmp, tmp.replace(".npz", ".provenance.json")):
+            if os.path.exists(x):
+                os.remove(x)
+    assert same and cfg_same
+    save("interchange.npz", loaded_by_reference=np.array(bool(same and cfg_same)))
+
+
 def gen_masks():
     big = StructuredMesh(2048, 1024, 2.0, 1.0)
     m = circle_mask(big, (0.5, 0.5), 0.05).mask
@@ -325,9 +377,10 @@ def gen_masks():
 
 if __name__ == "__main__":
     which = set(sys.argv[2:]) or {"rhs", "poisson", "multigrid", "solvers", "steps",
-                                  "cavity64", "cylinder", "masks", "faces", "cylinder_long", "shapes"}
+                                  "cavity64", "cylinder", "masks", "faces", "cylinder_long", "shapes",
+                                  "checkpoint", "interchange"}
     for name in ("rhs", "poisson", "multigrid", "solvers", "steps", "cavity64",
-                 "cylinder", "masks", "faces", "cylinder_long", "shapes"):
+                 "cylinder", "masks", "faces", "cylinder_long", "shapes", "checkpoint", "interchange"):
         if name in which:
             t0 = time.perf_counter()
             globals()["gen_" + name]()
