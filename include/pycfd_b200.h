@@ -232,6 +232,8 @@ typedef struct {
     double t_end;          /* dt is clamped so the clock lands on t_end            */
     int blend_mode;        /* 0: fixed blend below; 1: 1.2 x Courant number (upwind) */
     double blend;
+    double steady_tol;     /* history runs: stop once max|du|/dt < steady_tol (0: never) */
+    int history;           /* 1: gated step with a device history row (see below)     */
 } pycfd_dt_control;
 
 /* One step whose dt is computed on the device from the current state, with
@@ -242,6 +244,20 @@ typedef struct {
 int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
                         double* p, const pycfd_dt_control* ctl, void* stream);
 int pycfd_set_clock(pycfd_solver* s, double t, void* stream);
+
+/* Device-side run loop (TimeStepper.run, pycfd/core/timestepper.py:145-266).
+ * With ctl->history = 1 the recorded step is gated on the device: a run whose
+ * clock has reached t_end (frozen 2), that tripped a health check on the
+ * unclamped dt (frozen 1: the step is not taken and the clock stays at the last
+ * good step, as the reference raises DivergenceError before it), or that went
+ * steady (frozen 3: max|du|/dt < steady_tol after a step, which is kept) takes
+ * no further steps; every step taken appends a row to a device history: step,
+ * t, dt, CFL number, max|div u|, kinetic energy, last Poisson residual, fx, fy,
+ * max|du|/dt (timestepper.py:251-266).  pycfd_history_read copies the rows
+ * appended since the last read (at most 4096 between reads) into rows (10
+ * doubles each), gives their count and the frozen state, and clears the
+ * history; pycfd_set_clock clears the clock, health, frozen state and history. */
+int pycfd_history_read(pycfd_solver* s, double* rows, int max_rows, int* n_rows, int* frozen, void* stream);
 int pycfd_get_clock(pycfd_solver* s, double* t, double* dt, int* steps, int* health, void* stream);
 
 /* The same step on HOST buffers: copies the inputs in, steps (the step is

@@ -26,6 +26,7 @@ EXPORTS = (
     "pycfd_momentum_rhs", "pycfd_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
+    "pycfd_history_read",
     "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields", "pycfd_face_lists", "pycfd_rasterize",
     "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_solver_persistent",
     "pycfd_solver_set_wait_limit", "pycfd_solve_trace", "pycfd_launch_count",
@@ -73,7 +74,7 @@ class SolverDesc(C.Structure):
 class DtControl(C.Structure):
     _fields_ = [("adaptive", C.c_int), ("cfl", C.c_double), ("visc_limit", C.c_double),
                 ("dt_cap", C.c_double), ("t_end", C.c_double), ("blend_mode", C.c_int),
-                ("blend", C.c_double)]
+                ("blend", C.c_double), ("steady_tol", C.c_double), ("history", C.c_int)]
 
 
 class BatchOpts(C.Structure):
@@ -131,6 +132,7 @@ def load(path: str = LIB_PATH):
         "pycfd_step_host": (C.c_int, [vp, vp, vp, vp, vp, vp, C.c_double, C.c_double, vp]),
         "pycfd_step_adaptive": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(DtControl), vp]),
         "pycfd_set_clock": (C.c_int, [vp, C.c_double, vp]),
+        "pycfd_history_read": (C.c_int, [vp, vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), vp]),
         "pycfd_get_clock": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(C.c_int), C.POINTER(C.c_int), vp]),
         "pycfd_get_stats": (C.c_int, [vp, C.POINTER(Stats), vp]),

@@ -36,7 +36,8 @@ enum Slot {
 enum ISlot {
   I_IT = 0, I_DONE, I_CONVERGED, I_STATUS, I_STALLED, I_TOTAL_IT, I_ZERO_RHS, I_MAXITER,
   I_IR_IT, I_IR_DONE, I_FINITE, I_HEALTH, I_STEPS,
-  I_FROZEN,        // batched runs: 1 stopped by a health flag, 2 reached its end time
+  I_FROZEN,        // 1 stopped by a health flag, 2 reached its end time, 3 steady (device loops)
+  I_HIST,          // rows appended to the device history since it was last read
   I_COUNT = 16
 };
 

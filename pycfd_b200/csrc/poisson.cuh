@@ -441,6 +441,8 @@ struct DtControl {
   double cfl, visc_limit, dt_cap, t_end, dx, dy;
   int blend_mode;     // 0 fixed blend (below), 1 follow the Courant number
   double blend;
+  double steady_tol;  // device loop: stop once max|du|/dt falls below it (0: never)
+  int history;        // 1: the step is gated and appends a row to the device history
 };
 
 __device__ __forceinline__ void adaptive_dt_update(double* S, int* I, const DtControl& c) {
@@ -471,12 +473,78 @@ __global__ void k_adaptive_dt(double* __restrict__ S, int* __restrict__ I, DtCon
   adaptive_dt_update(S, I, c);
 }
 
+// Gate of a device-loop step (TimeStepper.run, pycfd/core/timestepper.py:183-231):
+// a frozen run takes no more steps; once the clock is within 1e-12 of the end
+// time (the reference's loop condition) it freezes (2); the dt and health
+// checks run on the unclamped dt as in k_adaptive_dt, and a health flag freezes
+// the run (1) with the clock left at the last good step -- the step the
+// reference refuses with DivergenceError.  `gate` is the condition of the
+// graph's IF node around the step.
+__global__ void k_step_gate(double* __restrict__ S, int* __restrict__ I, DtControl c, LoopCtl gate) {
+  if (threadIdx.x != 0) return;
+  if (I[I_FROZEN]) {
+    gate.set(false);
+    return;
+  }
+  if (!(S[S_T] < c.t_end - 1e-12)) {
+    I[I_FROZEN] = 2;
+    gate.set(false);
+    return;
+  }
+  const double t0 = S[S_T], dt0 = S[S_DT];
+  const int n0 = I[I_STEPS];
+  adaptive_dt_update(S, I, c);
+  if (I[I_HEALTH] != 0) {
+    S[S_T] = t0;
+    S[S_DT] = dt0;
+    I[I_STEPS] = n0;
+    I[I_FROZEN] = 1;
+    gate.set(false);
+    return;
+  }
+  gate.set(true);
+}
+
+// One row of the device history after a step (timestepper.py:251-266): step,
+// t, dt, CFL number, max|div u|, kinetic energy, last Poisson residual, body
+// force (fx, fy), max|du|/dt.  The field statistics of the new state (and its
+// change over the step) are in the stats slots.  A run whose rate of change
+// falls below steady_tol freezes (3) after this step, as the reference stops.
+constexpr int kHistCols = 10;
+constexpr int kHistRows = 4096;   // rows the device history holds between reads
+
+__global__ void k_history_append(double* __restrict__ S, int* __restrict__ I, double* __restrict__ hist,
+                                 int cap, DtControl c) {
+  if (threadIdx.x != 0) return;
+  const double dt = S[S_DT];
+  const double umax = S[S_STAT0], vmax = S[S_STAT0 + 1];
+  const double rate = fmax(S[S_STAT0 + 2], S[S_STAT0 + 3]) / dt;
+  const int row = I[I_HIST];
+  if (row < cap) {
+    double* h = hist + (long)row * kHistCols;
+    h[0] = (double)I[I_STEPS];
+    h[1] = S[S_T];
+    h[2] = dt;
+    h[3] = dt * (umax / c.dx + vmax / c.dy);
+    h[4] = S[S_STAT0 + 4];
+    h[5] = S[S_STAT0 + 5] * (c.dx * c.dy);
+    h[6] = S[S_RESID];
+    h[7] = S[S_FX];
+    h[8] = S[S_FY];
+    h[9] = rate;
+  }
+  I[I_HIST] = row + 1;
+  if (c.steady_tol > 0.0 && rate < c.steady_tol) I[I_FROZEN] = 3;
+}
+
 __global__ void k_set_clock(double* __restrict__ S, int* __restrict__ I, double t) {
   pdl_begin();
   if (threadIdx.x == 0) {
     S[S_T] = t;
     I[I_STEPS] = 0;
     I[I_HEALTH] = 0;
+    I[I_FROZEN] = 0;
+    I[I_HIST] = 0;
   }
 }
 

@@ -165,10 +165,12 @@ struct pycfd_solver {
   double* ppart = nullptr;      // per-CTA partial sums
   unsigned long long* ptrace = nullptr;   // phase trace (measurement support)
   int trace_on = 0;
+  double* hist = nullptr;       // device history of a device-side run loop (kHistRows x kHistCols)
   // CUDA-graph recording of whole steps
   bool capturing = false;
   cudaStream_t aux = nullptr;   // records the bodies of the solve loops
   cudaStream_t aux2 = nullptr;  // records loop bodies nested one level deeper
+  cudaStream_t gate = nullptr;  // records the gated body of a device-loop step
   cudaStream_t rec = nullptr;   // records whole steps
   struct GraphEntry {
     const void* key[5];
@@ -1123,6 +1125,7 @@ int pycfd_solver_destroy(pycfd_solver* s) {
   if (s->aux) cudaStreamDestroy(s->aux);
   if (s->rec) cudaStreamDestroy(s->rec);
   if (s->aux2) cudaStreamDestroy(s->aux2);
+  if (s->gate) cudaStreamDestroy(s->gate);
   for (void* p : s->allocs) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
   if (s->hI) cudaFreeHost(s->hI);
@@ -1596,6 +1599,60 @@ int pycfd_step_graph(pycfd_solver* s, const double* u0, const double* v0, double
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The body of a device-loop step, captured on s->rec after the statistics of
+// the input state: the gate kernel sets the condition of an IF node whose body
+// is the step, the statistics of its result (and its change) and the history
+// row.  A frozen run replays the graph without touching the state.
+int record_gated_step(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v, double* p,
+                      const DtControl& c) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamGetCaptureInfo(s->rec, &cs, nullptr, &g, nullptr, nullptr));
+  cudaGraphConditionalHandle h;
+  CU(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  const LoopCtl gate{h, 1};
+  k_step_gate<<<1, 32, 0, s->rec>>>(s->S, s->I, c, gate);
+  CHECK_LAUNCH();
+  g_launches.fetch_add(1);
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  CU(cudaStreamGetCaptureInfo(s->rec, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams np{};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeIf;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CU(cudaGraphAddNode(&node, g, deps, nd, &np));
+  CU(cudaStreamUpdateCaptureDependencies(s->rec, &node, 1, cudaStreamSetCaptureDependencies));
+  if (!s->gate) CU(cudaStreamCreateWithFlags(&s->gate, cudaStreamNonBlocking));
+  // the IF body, recorded on its own stream (the step's solve loops nest inside it)
+  CU(cudaStreamBeginCaptureToGraph(s->gate, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeRelaxed));
+  int rc = step_impl(s, u0, v0, u, v, p, s->gate);
+  if (!rc) {
+    k_field_stats<<<std::min(s->g.nx + 3, kMaxRedBlocks), kRedThreads, 0, s->gate>>>(
+        u, v, p, u0, v0, s->solid, s->g, s->rb(), s->S);
+    if (cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "stats launch failed");
+    k_history_append<<<1, 32, 0, s->gate>>>(s->S, s->I, s->hist, kHistRows, c);
+    if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "history launch failed");
+    g_launches.fetch_add(2);
+  }
+  cudaGraph_t body = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s->gate, &body);
+  if (rc) return rc;
+  if (ec != cudaSuccess) return fail(PCFD_E_CUDA, "gated step capture failed: %s", cudaGetErrorString(ec));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, double* u, double* v,
                         double* p, const pycfd_dt_control* ctl, void* stream) {
   if (!s || !u0 || !v0 || !u || !v || !p || !ctl) return fail(PCFD_E_ARG, "bad arguments");
@@ -1603,8 +1660,20 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
   if (s->solver_kind == PCFD_SOLVER_JACOBI || s->solver_kind == PCFD_SOLVER_SOR)
     return fail(PCFD_E_UNSUPPORTED, "device-side stepping needs a cg, multigrid or mgcg solver");
   cudaStream_t sm = st(stream);
-  DtControl c{ctl->adaptive, ctl->cfl, ctl->visc_limit, ctl->dt_cap, ctl->t_end, s->g.dx, s->g.dy,
-              ctl->blend_mode, ctl->blend};
+  DtControl c;
+  memset(&c, 0, sizeof c);   // compared bytewise below
+  c.adaptive = ctl->adaptive;
+  c.cfl = ctl->cfl;
+  c.visc_limit = ctl->visc_limit;
+  c.dt_cap = ctl->dt_cap;
+  c.t_end = ctl->t_end;
+  c.dx = s->g.dx;
+  c.dy = s->g.dy;
+  c.blend_mode = ctl->blend_mode;
+  c.blend = ctl->blend;
+  c.steady_tol = ctl->steady_tol;
+  c.history = ctl->history ? 1 : 0;
+  if (c.history && !s->hist) TRY(dalloc(s, &s->hist, (size_t)kHistRows * kHistCols));
   // key: the five addresses plus the control values (recorded into the graph)
   const void* key[5] = {u0, v0, u, v, p};
   pycfd_solver::GraphEntry* hit = nullptr;
@@ -1621,10 +1690,15 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
         u0, v0, nullptr, nullptr, nullptr, s->solid, s->g, s->rb(), s->S);
     if (cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "stats launch failed");
     g_launches.fetch_add(1);
-    pdl_launch(s, k_adaptive_dt, 1, 32, 0, s->rec, s->S, s->I, c);
-    if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "dt launch failed");
-    g_launches.fetch_add(1);
-    if (!rc) rc = step_impl(s, u0, v0, u, v, p, s->rec);
+    if (!c.history) {
+      pdl_launch(s, k_adaptive_dt, 1, 32, 0, s->rec, s->S, s->I, c);
+      if (!rc && cudaGetLastError() != cudaSuccess) rc = fail(PCFD_E_CUDA, "dt launch failed");
+      g_launches.fetch_add(1);
+      if (!rc) rc = step_impl(s, u0, v0, u, v, p, s->rec);
+    } else if (!rc) {
+      // gated step: [gate] -> IF { step, statistics of the new state, history row }
+      rc = record_gated_step(s, u0, v0, u, v, p, c);
+    }
     s->capturing = false;
     const cudaError_t ec = cudaStreamEndCapture(s->rec, &graph);
     if (rc) {
@@ -1649,6 +1723,23 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
     hit = &s->graphs.back();
   }
   CU(cudaGraphLaunch(hit->exec, sm));
+  return 0;
+}
+
+int pycfd_history_read(pycfd_solver* s, double* rows, int max_rows, int* n_rows, int* frozen, void* stream) {
+  if (!s || !n_rows || !frozen || max_rows < 0) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  CU(cudaMemcpyAsync(s->hI, s->I, sizeof(int) * I_COUNT, cudaMemcpyDeviceToHost, sm));
+  CU(cudaStreamSynchronize(sm));
+  const int n = s->hI[I_HIST];
+  *frozen = s->hI[I_FROZEN];
+  if (n > kHistRows) return fail(PCFD_E_ARG, "%d steps since the history was last read; it holds %d", n, kHistRows);
+  *n_rows = n;
+  const int c = std::min(n, max_rows);
+  if (c > 0 && rows && s->hist)
+    CU(cudaMemcpyAsync(rows, s->hist, sizeof(double) * kHistCols * c, cudaMemcpyDeviceToHost, sm));
+  CU(cudaMemsetAsync(s->I + I_HIST, 0, sizeof(int), sm));
+  CU(cudaStreamSynchronize(sm));
   return 0;
 }
 

@@ -38,6 +38,11 @@ class GpuOptions:
 
     precision: str = "fp64"
     inner_tol: float = 1e-4
+    #: TimeStepper.run on the device: dt, health checks, the end-time clamp and the
+    #: steady test run in the recorded step, each step appends a row to a device
+    #: history, and the host reads the rows every ``device_loop`` steps (0: the
+    #: host-driven loop, one small read per step).  cg / multigrid / mgcg only.
+    device_loop: int = 64
     #: record each step once into a CUDA graph (device-side Poisson loops) and
     #: replay it; ``advance()`` and the time stepper use it.
     graphs: bool = True
@@ -238,7 +243,7 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     return d, keep
 
 
-def dt_control_for(config, mesh, t_end: float = float("inf")):
+def dt_control_for(config, mesh, t_end: float = float("inf"), history: bool = False):
     """Device-side time-step control matching :class:`TimeStepper` for ``config``.
 
     ``pycfd/core/timestepper.py:94-142``: CFL and viscous limits capped by ``config.dt``
@@ -256,6 +261,8 @@ def dt_control_for(config, mesh, t_end: float = float("inf")):
     central = AdvectionScheme(config.advection_scheme) is AdvectionScheme.CENTRAL
     c.blend_mode = 0 if (central or config.upwind_blend is not None) else 1
     c.blend = 0.0 if central else float(config.upwind_blend or 0.0)
+    c.steady_tol = float(config.steady_tol) if (history and config.steady_tol is not None) else 0.0
+    c.history = int(bool(history))
     return c
 
 
@@ -537,6 +544,16 @@ class ProjectionSolver:
     def dt_control(self):
         """Device-side time-step control matching :class:`TimeStepper` for this configuration."""
         return dt_control_for(self.config, self.mesh)
+
+    def read_history(self):
+        """Rows the device history gained since the last read (step, t, dt, cfl, max_div,
+        kinetic energy, residual, fx, fy, max|du|/dt) and the frozen state (0 running,
+        1 health stop, 2 end time, 3 steady); clears the history (synchronises)."""
+        rows = np.empty((4096, 10), dtype=np.float64)
+        n, fr = C.c_int(), C.c_int()
+        _lib.check(self._L.pycfd_history_read(self._h, _lib.ptr(rows), 4096, C.byref(n), C.byref(fr),
+                                              _stream()))
+        return rows[:n.value].copy(), fr.value
 
     def set_clock(self, t: float = 0.0) -> None:
         """Reset the device clock, step counter and health flags of device-side stepping."""

@@ -97,6 +97,9 @@ class TimeStepper:
         """Integrate until ``t_end`` (``pycfd/core/timestepper.py:145-248``)."""
         t_end = self.config.t_end if t_end is None else t_end
         max_steps = self.config.max_steps if max_steps is None else max_steps
+        if self._device_loop() > 0:
+            return self._run_device(fields, t_end, max_steps, callback, callback_every, progress,
+                                    record_every)
         history = {k: [] for k in ("step", "t", "dt", "cfl", "max_div", "kinetic_energy",
                                    "residual", "fx", "fy")}
         bar = None
@@ -146,6 +149,98 @@ class TimeStepper:
         if callback is not None:
             callback(fields, fields.diagnostics or self._diagnostics(fields, self.config.dt,
                                                                      float("nan")))
+        result = SimulationResult(fields, steps_taken, fields.t, wall, converged, history)
+        log.info(result.summary())
+        return result
+
+    # ------------------------------------------------------------------ #
+    def _device_loop(self) -> int:
+        from .config import PressureSolver
+        opts = getattr(self.solver, "options", None)
+        k = int(getattr(opts, "device_loop", 0) or 0)
+        kind = PressureSolver(self.config.pressure_solver)
+        if k <= 0 or kind in (PressureSolver.SOR, PressureSolver.JACOBI):
+            return 0
+        return min(k, 4096)
+
+    def _run_device(self, fields, t_end, max_steps, callback, callback_every, progress, record_every):
+        """The run loop with the step, its dt, health checks, end-time clamp and steady
+        test on the device (one recorded, gated step per step), the per-step
+        diagnostics kept in a device history read every ``device_loop`` steps (and
+        at each callback step)."""
+        from .solver import dt_control_for
+        K = self._device_loop()
+        keys = ("step", "t", "dt", "cfl", "max_div", "kinetic_energy", "residual", "fx", "fy")
+        names = keys + ("rate_of_change",)
+        history = {k: [] for k in keys}
+        bar = None
+        if progress:
+            try:
+                from tqdm.auto import tqdm
+                bar = tqdm(total=float(t_end), initial=float(fields.t), unit="s",
+                           desc=self.config.name, dynamic_ncols=True)
+            except ImportError:
+                log.warning("tqdm not installed; running without a progress bar")
+        s = self.solver
+        ctl = dt_control_for(self.config, self.mesh, t_end, history=True)
+        s.set_clock(fields.t)
+        wall_start = time.perf_counter()
+        converged = False
+        steps_taken = 0
+        step0 = fields.step
+        cur = fields
+        frozen = 0
+        try:
+            while frozen == 0 and fields.t < t_end - 1e-12:
+                n = K
+                if max_steps is not None:
+                    n = min(n, max_steps - steps_taken)
+                if callback is not None:
+                    n = min(n, callback_every - steps_taken % callback_every)
+                if n <= 0:
+                    break
+                outs = []
+                for _ in range(n):
+                    cur = s.advance_adaptive(cur, ctl)
+                    outs.append(cur)
+                rows, frozen = s.read_history()
+                done = len(rows)
+                if done:
+                    cur = outs[done - 1]
+                    fields = FlowField(self.mesh, cur.u, cur.v, cur.p, float(rows[-1][1]),
+                                       step0 + int(rows[-1][0]))
+                    s._read_stats(raise_on_error=False)
+                    if bar is not None:
+                        bar.update(float(rows[:, 2].sum()))
+                else:
+                    cur = fields      # the gate refused the window's first step
+                for r in rows:
+                    k = int(r[0])
+                    if k % record_every == 0:
+                        info = dict(zip(names, (float(x) for x in r)))
+                        info["step"] = step0 + k
+                        for key in keys:
+                            history[key].append(info[key])
+                        fields.diagnostics = info
+                steps_taken += done
+                if frozen == 1:
+                    fields._stats = None
+                    self._check_health(fields, self.compute_dt(fields))
+                    raise DivergenceError(f"the device health check stopped the run at step {fields.step}")
+                if callback is not None and done and steps_taken % callback_every == 0:
+                    callback(fields, fields.diagnostics or self._diagnostics(fields, float(rows[-1][2]),
+                                                                              float(rows[-1][9])))
+                if frozen == 3:
+                    converged = True
+            fields = FlowField(self.mesh, fields.u.clone(), fields.v.clone(), fields.p.clone(), fields.t,
+                               fields.step, fields.diagnostics)
+            self._check_health(fields, self.config.dt)
+        finally:
+            if bar is not None:
+                bar.close()
+        wall = time.perf_counter() - wall_start
+        if callback is not None:
+            callback(fields, fields.diagnostics or self._diagnostics(fields, self.config.dt, float("nan")))
         result = SimulationResult(fields, steps_taken, fields.t, wall, converged, history)
         log.info(result.summary())
         return result
