@@ -343,6 +343,43 @@ int pycfd_rasterize(const pycfd_shape* shape, const double* xf, const double* dx
                     const double* dy_cells, int nx, int ny, double lx, double ly, int subsamples,
                     double* fraction, uint8_t* mask, void* stream);
 
+/* ---- Discrete adjoint of the cavity step (no counterpart in the reference,
+ * whose step has no adjoint): the primitives of one SSP-RK3 step of the
+ * lid-driven cavity with a lid profile U(x) and a smoothed obstacle chi, and
+ * their exact transposes, as hand-written kernels.  The forward primitives are
+ * the library step's arithmetic for the cavity (pycfd/core/solver.py:612-731,
+ * kernels.py:54-110, boundary.py:141-164 with a profile on the moving lid,
+ * solver.py:553-599 with u <- (1 - chi) u on the solvable faces); the Poisson
+ * solves of the projection and its transpose go through pycfd_poisson_solve.
+ * Arrays are device pointers in the ghosted layout (u (n+3) x (n+2), v
+ * (n+2) x (n+3)); cell arrays are n x n. */
+#define PCFD_ADJ_PREDICTOR 1    /* out_u, out_v = u, v + dt rhs(u, v) on solvable faces      */
+#define PCFD_ADJ_WALLS 2        /* out_u, out_v (in place): cavity walls, lid[n+3] on top     */
+#define PCFD_ADJ_MASK 3         /* out_u, out_v = (1 - cu, cv) (u, v) on solvable faces       */
+#define PCFD_ADJ_DIV 4          /* out[n*n] = div(u, v) / dt                                  */
+#define PCFD_ADJ_CORRECT 5      /* out_u, out_v (in place) -= dt grad(a), a = p (n*n)         */
+#define PCFD_ADJ_LINCOMB 6      /* out[count] = ca a + cb b                                   */
+#define PCFD_ADJ_OBJECTIVE 7    /* out[0] = h^2 sum 0.5 (uc^2 + vc^2) lower[j]                */
+#define PCFD_ADJ_PREDICTOR_T 8  /* out_u, out_v = predictor^T at (u, v) applied to (gu, gv)   */
+#define PCFD_ADJ_WALLS_T 9      /* out_u, out_v (in place) = walls^T; acc_u[n+3] += d/dlid   */
+#define PCFD_ADJ_MASK_T 10      /* out_u, out_v (in place) = mask^T at input (u, v); acc_u,
+                                   acc_v += d/dchi                                         */
+#define PCFD_ADJ_GRAD_T 11      /* out[n*n] = G^T (gu, gv) (transposed face gradient)         */
+#define PCFD_ADJ_DIV_T 12       /* out_u, out_v (in place) -= D^T a (a = psi, n*n)            */
+#define PCFD_ADJ_OBJECTIVE_T 13 /* out_u, out_v = d objective / d(u, v) at (u, v)             */
+typedef struct {
+    int n;                       /* cells per side                                   */
+    double h, nu, dt;            /* spacing, viscosity, time step                    */
+    double ca, cb;               /* lincomb weights                                  */
+    long count;                  /* lincomb length                                   */
+    const double *u, *v;         /* state the primitive (or its transpose) is taken at */
+    const double *gu, *gv;       /* incoming gradients (predictor_T, grad_T)         */
+    const double *a, *b;         /* extra operands (lincomb, correct/div_T field)   */
+    const double *lid, *cu, *cv, *lower;
+    double *out_u, *out_v, *out, *acc_u, *acc_v;
+} pycfd_adj_args;
+int pycfd_adjoint_apply(int op, const pycfd_adj_args* args, void* stream);
+
 /* Field reductions (synchronises `stream`).  u_prev/v_prev may be NULL. */
 int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const double* p,
                       const double* u_prev, const double* v_prev, pycfd_field_stats* out,

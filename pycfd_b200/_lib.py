@@ -27,7 +27,7 @@ EXPORTS = (
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
     "pycfd_history_read",
-    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields", "pycfd_face_lists", "pycfd_rasterize",
+    "pycfd_step_host", "pycfd_get_stats", "pycfd_reduce_fields", "pycfd_face_lists", "pycfd_rasterize", "pycfd_adjoint_apply",
     "pycfd_reduce_fields_noalloc", "pycfd_profile_kernel", "pycfd_solver_persistent",
     "pycfd_solver_set_wait_limit", "pycfd_solve_trace", "pycfd_launch_count",
     "pycfd_profile_read", "pycfd_batch_create", "pycfd_batch_destroy", "pycfd_batch_initialize",
@@ -44,6 +44,15 @@ class Shape(C.Structure):
     _fields_ = [("kind", C.c_int), ("p", C.c_double * 4), ("verts", C.c_void_p), ("n_verts", C.c_int),
                 ("image", C.c_void_p), ("rows", C.c_int), ("cols", C.c_int), ("threshold", C.c_double),
                 ("invert", C.c_int)]
+
+
+class AdjArgs(C.Structure):
+    _fields_ = [("n", C.c_int), ("h", C.c_double), ("nu", C.c_double), ("dt", C.c_double),
+                ("ca", C.c_double), ("cb", C.c_double), ("count", C.c_long),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("gu", C.c_void_p), ("gv", C.c_void_p),
+                ("a", C.c_void_p), ("b", C.c_void_p), ("lid", C.c_void_p), ("cu", C.c_void_p),
+                ("cv", C.c_void_p), ("lower", C.c_void_p), ("out_u", C.c_void_p), ("out_v", C.c_void_p),
+                ("out", C.c_void_p), ("acc_u", C.c_void_p), ("acc_v", C.c_void_p)]
 
 
 class MgLevel(C.Structure):
@@ -143,6 +152,7 @@ def load(path: str = LIB_PATH):
         "pycfd_launch_count": (C.c_longlong, []),
         "pycfd_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int), vp]),
         "pycfd_reduce_fields": (C.c_int, [vp, vp, vp, vp, vp, vp, C.POINTER(FieldStats), vp]),
+        "pycfd_adjoint_apply": (C.c_int, [C.c_int, C.POINTER(AdjArgs), vp]),
         "pycfd_rasterize": (C.c_int, [C.POINTER(Shape), vp, vp, vp, vp, C.c_int, C.c_int, C.c_double,
                                       C.c_double, C.c_int, vp, vp, vp]),
         "pycfd_face_lists": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int),

@@ -19,15 +19,19 @@ the cell grid, gradient correction of the solvable faces), mask, wall pass.
 Arrays are float64 tensors in the reference's ghosted layout: ``u`` is
 ``(nx+3, ny+2)``, ``v`` is ``(nx+2, ny+3)``.
 
-The forward functions are written with tensor slicing only, so autograd can run
-through them when the Poisson solve is a differentiable dense solve (the small
-dense reference).  The backward is hand-written: each primitive has its
-transpose (:func:`rhs_adjoint` is the transposed Jacobian of the advection-
-diffusion operator; :func:`walls_adjoint` reverses the ordered line
-assignments; :func:`project_adjoint` applies the transposed projection with the
-same Poisson solver -- the operator is symmetric, so the adjoint solve is one
-more solve with the same multigrid).  Long rollouts keep a checkpoint every
-``checkpoint`` steps and recompute each segment during the backward pass.
+Every primitive exists twice.  On CUDA tensors it runs as a hand-written kernel
+of the library (``pycfd_adjoint_apply``: the forward with the library step's own
+arithmetic, each transpose in gather form); on CPU tensors it runs as tensor
+slicing, so that autograd can run through the forward when the Poisson solve is
+a differentiable dense solve (the small dense reference the kernels and the
+hand-written backward are checked against).  The backward is hand-written:
+each primitive has its transpose (:func:`rhs_adjoint` is the transposed
+Jacobian of the advection-diffusion operator; :func:`walls_adjoint` reverses the
+ordered line assignments; :func:`project_adjoint` applies the transposed
+projection with the same Poisson solver -- the operator is symmetric, so the
+adjoint solve is one more solve with the same multigrid).  Long rollouts keep a
+checkpoint every ``checkpoint`` steps and recompute each segment during the
+backward pass.
 """
 
 from __future__ import annotations
@@ -41,6 +45,47 @@ import numpy as np
 def _torch():
     import torch
     return torch
+
+
+# ---------------------------------------------------------------------------
+# the kernels (CUDA tensors)
+# ---------------------------------------------------------------------------
+OP = dict(predictor=1, walls=2, mask=3, div=4, correct=5, lincomb=6, objective=7, predictor_t=8,
+          walls_t=9, mask_t=10, grad_t=11, div_t=12, objective_t=13)
+
+
+def _on_device(t) -> bool:
+    return getattr(t, "is_cuda", False)
+
+
+def _k(op, **kw):
+    """One adjoint-primitive kernel launch on the current stream."""
+    import ctypes as C
+    from . import _lib
+    torch = _torch()
+    L = _lib.load()
+    a = _lib.AdjArgs()
+    for k, val in kw.items():
+        if isinstance(val, torch.Tensor):
+            if val.dtype != torch.float64 or not val.is_contiguous():
+                raise ValueError(f"{k}: contiguous float64 tensors only")
+            setattr(a, k, val.data_ptr())
+        else:
+            setattr(a, k, val)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(L.pycfd_adjoint_apply(OP[op], C.byref(a), stream))
+
+
+def lincomb(a, ca, b=None, cb=0.0):
+    """``ca a + cb b`` (``b`` absent: ``ca a``)."""
+    if b is None:
+        b, cb = a, 0.0
+    if _on_device(a):
+        out = _torch().empty_like(a)
+        _k("lincomb", out=out, a=a.contiguous(), b=b.contiguous(), ca=float(ca), cb=float(cb),
+           count=a.numel())
+        return out
+    return ca * a + cb * b if cb != 0.0 else ca * a
 
 
 # ---------------------------------------------------------------------------
@@ -144,6 +189,10 @@ def rhs(u, v, n, h, nu):
 
 def predictor(U, V, n, h, nu, dt):
     """u* = U + dt rhs(U) on the solvable faces (u: m = 2..n, v: k = 2..n), U elsewhere."""
+    if _on_device(U):
+        us, vs = _torch().empty_like(U), _torch().empty_like(V)
+        _k("predictor", n=n, h=h, nu=nu, dt=dt, u=U, v=V, out_u=us, out_v=vs)
+        return us, vs
     ru, rv = rhs(U, V, n, h, nu)
     us, vs = U.clone(), V.clone()
     us[2:n + 1, 1:n + 1] = U[2:n + 1, 1:n + 1] + dt * ru[1:n]
@@ -155,6 +204,9 @@ def walls(u, v, lid, n):
     """Wall pass of the cavity, walls in the reference's order (left, right,
     bottom, top), each line assignment in sequence so corner ghosts agree."""
     u, v = u.clone(), v.clone()
+    if _on_device(u):
+        _k("walls", n=n, h=1.0, out_u=u, out_v=v, lid=lid.contiguous())
+        return u, v
     # left: normal face, normal ghost, tangential ghost
     u[1, :] = 0.0
     u[0, :] = 2.0 * u[1, :] - u[2, :]
@@ -176,6 +228,10 @@ def walls(u, v, lid, n):
 
 def mask(u, v, cu, cv, n):
     """Direct forcing: solvable faces times (1 - chi)."""
+    if _on_device(u):
+        uo, vo = _torch().empty_like(u), _torch().empty_like(v)
+        _k("mask", n=n, h=1.0, u=u, v=v, out_u=uo, out_v=vo, cu=cu, cv=cv)
+        return uo, vo
     uo, vo = u.clone(), v.clone()
     uo[2:n + 1, 1:n + 1] = (1.0 - cu[2:n + 1, 1:n + 1]) * u[2:n + 1, 1:n + 1]
     vo[1:n + 1, 2:n + 1] = (1.0 - cv[1:n + 1, 2:n + 1]) * v[1:n + 1, 2:n + 1]
@@ -189,6 +245,14 @@ def divergence(u, v, n, h):
 def project(u, v, n, h, dt, solve):
     """Projection: p from lap p = div(u)/dt (``solve``: mean-free, singular
     Neumann system), then u -= dt grad p on the solvable faces."""
+    if _on_device(u):
+        torch = _torch()
+        b = torch.empty((n, n), dtype=u.dtype, device=u.device)
+        _k("div", n=n, h=h, dt=dt, u=u, v=v, out=b)
+        p = solve(b).contiguous()
+        u, v = u.clone(), v.clone()
+        _k("correct", n=n, h=h, dt=dt, out_u=u, out_v=v, a=p)
+        return u, v
     p = solve(divergence(u, v, n, h) / dt)
     u, v = u.clone(), v.clone()
     u[2:n + 1, 1:n + 1] = u[2:n + 1, 1:n + 1] - dt * (p[1:n] - p[0:n - 1]) / h
@@ -219,8 +283,9 @@ def step(u, v, lid, cu, cv, g, dt, solve, tape=None):
         return substep(U, V, lid, cu, cv, g, dt, solve, tape)
     u1, v1 = sub(u, v)
     u2, v2 = sub(u1, v1)
-    u3, v3 = sub(0.75 * u + 0.25 * u2, 0.75 * v + 0.25 * v2)
-    return walls(u / 3.0 + 2.0 * u3 / 3.0, v / 3.0 + 2.0 * v3 / 3.0, lid, g.n)
+    u3, v3 = sub(lincomb(u, 0.75, u2, 0.25), lincomb(v, 0.75, v2, 0.25))
+    # the library step's weights (pycfd/core/solver.py:716-721)
+    return walls(lincomb(u, 1.0 / 3.0, u3, 2.0 / 3.0), lincomb(v, 1.0 / 3.0, v3, 2.0 / 3.0), lid, g.n)
 
 
 def initial(lid, cu, cv, g, solve, tape=None):
@@ -242,6 +307,10 @@ def initial(lid, cu, cv, g, solve, tape=None):
 def objective(u, v, g):
     """Kinetic energy of the cells with yc below the split (``pycfd/analysis/postprocess.py:73-79``)."""
     n, h = g.n, g.h
+    if _on_device(u):
+        out = _torch().empty((), dtype=u.dtype, device=u.device)
+        _k("objective", n=n, h=h, u=u, v=v, lower=g.lower, out=out)
+        return out
     uc = 0.5 * (u[1:n + 1, 1:n + 1] + u[2:n + 2, 1:n + 1])
     vc = 0.5 * (v[1:n + 1, 1:n + 1] + v[1:n + 1, 2:n + 2])
     return (0.5 * (uc * uc + vc * vc) * g.lower[None, :]).sum() * h * h
@@ -308,6 +377,11 @@ def rhs_adjoint(u, v, gru, grv, n, h, nu):
 def predictor_adjoint(U, V, gus, gvs, n, h, nu, dt):
     """Transpose of :func:`predictor` at (U, V)."""
     torch = _torch()
+    if _on_device(U):
+        gU, gV = torch.empty_like(U), torch.empty_like(V)
+        _k("predictor_t", n=n, h=h, nu=nu, dt=dt, u=U, v=V, gu=gus.contiguous(), gv=gvs.contiguous(),
+           out_u=gU, out_v=gV)
+        return gU, gV
     gru = torch.zeros(n + 1, n, dtype=U.dtype, device=U.device)
     grv = torch.zeros(n, n + 1, dtype=U.dtype, device=U.device)
     gru[1:n] = dt * gus[2:n + 1, 1:n + 1]
@@ -372,6 +446,13 @@ def project_adjoint(gu, gv, n, h, solve):
     """Transpose of :func:`project`.  With u_out = u - G A^+ D u (dt cancels), the
     transpose is g - D^T A^+ G^T g: one solve with the same (symmetric) operator."""
     torch = _torch()
+    if _on_device(gu):
+        q = torch.empty((n, n), dtype=gu.dtype, device=gu.device)
+        _k("grad_t", n=n, h=h, gu=gu.contiguous(), gv=gv.contiguous(), out=q)
+        psi = solve(q).contiguous()
+        gu, gv = gu.clone(), gv.clone()
+        _k("div_t", n=n, h=h, out_u=gu, out_v=gv, a=psi)
+        return gu, gv
     gui, gvi = gu[2:n + 1, 1:n + 1], gv[1:n + 1, 2:n + 1]
     q = torch.zeros(n, n, dtype=gu.dtype, device=gu.device)      # G^T g on the cells
     q[1:n] += gui / h
@@ -388,61 +469,77 @@ def project_adjoint(gu, gv, n, h, solve):
     return gu, gv
 
 
+def walls_adjoint_acc(gu, gv, n, acc):
+    """:func:`walls_adjoint` with the lid gradient added into ``acc["lid"]``."""
+    if _on_device(gu):
+        gu, gv = gu.clone(), gv.clone()
+        _k("walls_t", n=n, h=1.0, out_u=gu, out_v=gv, acc_u=acc["lid"])
+        return gu, gv
+    gu, gv, gl = walls_adjoint(gu, gv, n)
+    acc["lid"] += gl
+    return gu, gv
+
+
+def mask_adjoint_acc(u_in, v_in, gu, gv, cu, cv, n, acc):
+    """:func:`mask_adjoint` with the chi gradients added into ``acc["cu"]``, ``acc["cv"]``."""
+    if _on_device(gu):
+        gu, gv = gu.clone(), gv.clone()
+        _k("mask_t", n=n, h=1.0, u=u_in, v=v_in, out_u=gu, out_v=gv, cu=cu, cv=cv, acc_u=acc["cu"],
+           acc_v=acc["cv"])
+        return gu, gv
+    gu, gv, gcu, gcv = mask_adjoint(u_in, v_in, gu, gv, cu, cv, n)
+    acc["cu"] += gcu
+    acc["cv"] += gcv
+    return gu, gv
+
+
 def substep_adjoint(U, V, pre1, pre2, gu, gv, lid, cu, cv, g, dt, solve, acc):
     """Adjoint of :func:`substep`; ``pre1``/``pre2`` are the states in front of its
     masks (from the tape).  Lid and chi gradients accumulate into ``acc``."""
     n, h, nu = g.n, g.h, g.cav.nu
-    gu, gv, gl = walls_adjoint(gu, gv, n)
-    acc["lid"] += gl
-    gu, gv, gcu, gcv = mask_adjoint(pre2[0], pre2[1], gu, gv, cu, cv, n)
-    acc["cu"] += gcu
-    acc["cv"] += gcv
+    gu, gv = walls_adjoint_acc(gu, gv, n, acc)
+    gu, gv = mask_adjoint_acc(pre2[0], pre2[1], gu, gv, cu, cv, n, acc)
     gu, gv = project_adjoint(gu, gv, n, h, solve)
-    gu, gv, gcu, gcv = mask_adjoint(pre1[0], pre1[1], gu, gv, cu, cv, n)
-    acc["cu"] += gcu
-    acc["cv"] += gcv
-    gu, gv, gl = walls_adjoint(gu, gv, n)
-    acc["lid"] += gl
+    gu, gv = mask_adjoint_acc(pre1[0], pre1[1], gu, gv, cu, cv, n, acc)
+    gu, gv = walls_adjoint_acc(gu, gv, n, acc)
     return predictor_adjoint(U, V, gu, gv, n, h, nu, dt)
 
 
 def step_adjoint(tape, gu, gv, lid, cu, cv, g, dt, solve, acc):
     """Adjoint of :func:`step` from its tape (9 entries: per substep its input and
     the two pre-mask states); returns the gradient at the step's input."""
-    gu, gv, gl = walls_adjoint(gu, gv, g.n)
-    acc["lid"] += gl
-    gu0, gv0 = gu / 3.0, gv / 3.0
-    gu3, gv3 = 2.0 * gu / 3.0, 2.0 * gv / 3.0
+    gu, gv = walls_adjoint_acc(gu, gv, g.n, acc)
+    gu0, gv0 = lincomb(gu, 1.0 / 3.0), lincomb(gv, 1.0 / 3.0)
+    gu3, gv3 = lincomb(gu, 2.0 / 3.0), lincomb(gv, 2.0 / 3.0)
     (U3, V3), p31, p32 = tape[6], tape[7], tape[8]
     gU3, gV3 = substep_adjoint(U3, V3, p31, p32, gu3, gv3, lid, cu, cv, g, dt, solve, acc)
-    gu0 = gu0 + 0.75 * gU3
-    gv0 = gv0 + 0.75 * gV3
+    gu0 = lincomb(gu0, 1.0, gU3, 0.75)
+    gv0 = lincomb(gv0, 1.0, gV3, 0.75)
     (U2, V2), p21, p22 = tape[3], tape[4], tape[5]
-    gU2, gV2 = substep_adjoint(U2, V2, p21, p22, 0.25 * gU3, 0.25 * gV3, lid, cu, cv, g, dt, solve, acc)
+    gU2, gV2 = substep_adjoint(U2, V2, p21, p22, lincomb(gU3, 0.25), lincomb(gV3, 0.25), lid, cu, cv, g, dt,
+                               solve, acc)
     (U1, V1), p11, p12 = tape[0], tape[1], tape[2]
     gU1, gV1 = substep_adjoint(U1, V1, p11, p12, gU2, gV2, lid, cu, cv, g, dt, solve, acc)
-    return gu0 + gU1, gv0 + gV1
+    return lincomb(gu0, 1.0, gU1, 1.0), lincomb(gv0, 1.0, gV1, 1.0)
 
 
 def initial_adjoint(tape, gu, gv, cu, cv, g, solve, acc):
     """Adjoint of :func:`initial` (its tape: the two pre-mask states)."""
     n = g.n
-    gu, gv, gl = walls_adjoint(gu, gv, n)
-    acc["lid"] += gl
-    gu, gv, gcu, gcv = mask_adjoint(tape[1][0], tape[1][1], gu, gv, cu, cv, n)
-    acc["cu"] += gcu
-    acc["cv"] += gcv
+    gu, gv = walls_adjoint_acc(gu, gv, n, acc)
+    gu, gv = mask_adjoint_acc(tape[1][0], tape[1][1], gu, gv, cu, cv, n, acc)
     gu, gv = project_adjoint(gu, gv, n, g.h, solve)
-    gu, gv, gcu, gcv = mask_adjoint(tape[0][0], tape[0][1], gu, gv, cu, cv, n)
-    acc["cu"] += gcu
-    acc["cv"] += gcv
-    _, _, gl = walls_adjoint(gu, gv, n)   # from rest: only the lid carries on
-    acc["lid"] += gl
+    gu, gv = mask_adjoint_acc(tape[0][0], tape[0][1], gu, gv, cu, cv, n, acc)
+    walls_adjoint_acc(gu, gv, n, acc)   # from rest: only the lid carries on
 
 
 def objective_adjoint(u, v, g):
     torch = _torch()
     n, h = g.n, g.h
+    if _on_device(u):
+        gu, gv = torch.empty_like(u), torch.empty_like(v)
+        _k("objective_t", n=n, h=h, u=u, v=v, lower=g.lower, out_u=gu, out_v=gv)
+        return gu, gv
     uc = 0.5 * (u[1:n + 1, 1:n + 1] + u[2:n + 2, 1:n + 1])
     vc = 0.5 * (v[1:n + 1, 1:n + 1] + v[1:n + 1, 2:n + 2])
     w = g.lower[None, :] * h * h

@@ -107,13 +107,11 @@ __device__ __forceinline__ void p_sync(PBar& pb, int tag) {
     const unsigned long long t0 = p_clock_ns();
     int k = 0;
     while (p_ld_relaxed(pb.bar) < pb.target) {
-      if ((++k & 63) == 0) {
-        if (p_failed(pb)) break;                      // another CTA gave up
-        if (p_clock_ns() - t0 > pb.wait_ns) {
-          atomicExch(pb.bar + 32, 1u);
-          break;
-        }
+      if (p_clock_ns() - t0 > pb.wait_ns) {           // checked on every poll
+        atomicExch(pb.bar + 32, 1u);
+        break;
       }
+      if ((++k & 63) == 0 && p_failed(pb)) break;     // another CTA gave up
     }
     __threadfence();
     if (pb.trace && blockIdx.x == 0 && 2 * pb.ntr + 2 < kPTraceCap) {

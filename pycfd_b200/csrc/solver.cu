@@ -17,6 +17,7 @@
 #include "multigrid.cuh"
 #include "persistent.cuh"
 #include "masks.cuh"
+#include "adjoint.cuh"
 #include "poisson.cuh"
 #include "stencil.cuh"
 
@@ -1834,6 +1835,80 @@ int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* s
   *total_ms = t;
   *launches = s->prof_n / 2;
   s->prof_n = 0;
+  return 0;
+}
+
+int pycfd_adjoint_apply(int op, const pycfd_adj_args* a, void* stream) {
+  if (!a || a->n < 2 || !(a->h > 0)) return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  const AdjGeo G{a->n, a->h, a->nu};
+  const long nf = (long)(a->n + 3) * (a->n + 2) * 2;   // u and v faces
+  const int grid = grid_for(nf, 256);
+  auto need = [](std::initializer_list<const void*> ps) {
+    for (const void* p : ps)
+      if (!p) return false;
+    return true;
+  };
+  switch (op) {
+    case PCFD_ADJ_PREDICTOR:
+      if (!need({a->u, a->v, a->out_u, a->out_v})) return fail(PCFD_E_ARG, "predictor: null array");
+      k_adj_predictor<<<grid, 256, 0, sm>>>(G, a->u, a->v, a->out_u, a->out_v, a->dt);
+      break;
+    case PCFD_ADJ_WALLS:
+      if (!need({a->out_u, a->out_v, a->lid})) return fail(PCFD_E_ARG, "walls: null array");
+      k_adj_walls<<<1, 512, 0, sm>>>(G, a->out_u, a->out_v, a->lid);
+      break;
+    case PCFD_ADJ_MASK:
+      if (!need({a->u, a->v, a->out_u, a->out_v, a->cu, a->cv})) return fail(PCFD_E_ARG, "mask: null array");
+      k_adj_mask<<<grid, 256, 0, sm>>>(G, a->u, a->v, a->out_u, a->out_v, a->cu, a->cv);
+      break;
+    case PCFD_ADJ_DIV:
+      if (!need({a->u, a->v, a->out}) || !(a->dt > 0)) return fail(PCFD_E_ARG, "div: bad arguments");
+      k_adj_div<<<grid, 256, 0, sm>>>(G, a->u, a->v, a->out, a->dt);
+      break;
+    case PCFD_ADJ_CORRECT:
+      if (!need({a->out_u, a->out_v, a->a})) return fail(PCFD_E_ARG, "correct: null array");
+      k_adj_correct<<<grid, 256, 0, sm>>>(G, a->out_u, a->out_v, a->a, a->dt);
+      break;
+    case PCFD_ADJ_LINCOMB:
+      if (!need({a->out, a->a, a->b}) || a->count < 0) return fail(PCFD_E_ARG, "lincomb: bad arguments");
+      k_adj_lincomb<<<grid_for(a->count, 256), 256, 0, sm>>>(a->out, a->a, a->ca, a->b, a->cb, a->count);
+      break;
+    case PCFD_ADJ_OBJECTIVE:
+      if (!need({a->u, a->v, a->lower, a->out})) return fail(PCFD_E_ARG, "objective: null array");
+      k_adj_objective<<<1, 1024, 0, sm>>>(G, a->u, a->v, a->lower, a->out);
+      break;
+    case PCFD_ADJ_PREDICTOR_T: {
+      if (!need({a->u, a->v, a->gu, a->gv, a->out_u, a->out_v})) return fail(PCFD_E_ARG, "predictor_T: null array");
+      const AdjRhs R{G, a->u, a->v, a->gu, a->gv, a->dt};
+      k_adj_predictor_T<<<grid, 256, 0, sm>>>(R, a->out_u, a->out_v);
+      break;
+    }
+    case PCFD_ADJ_WALLS_T:
+      if (!need({a->out_u, a->out_v, a->acc_u})) return fail(PCFD_E_ARG, "walls_T: null array");
+      k_adj_walls_T<<<1, 512, 0, sm>>>(G, a->out_u, a->out_v, a->acc_u);
+      break;
+    case PCFD_ADJ_MASK_T:
+      if (!need({a->u, a->v, a->out_u, a->out_v, a->cu, a->cv, a->acc_u, a->acc_v}))
+        return fail(PCFD_E_ARG, "mask_T: null array");
+      k_adj_mask_T<<<grid, 256, 0, sm>>>(G, a->u, a->v, a->out_u, a->out_v, a->cu, a->cv, a->acc_u, a->acc_v);
+      break;
+    case PCFD_ADJ_GRAD_T:
+      if (!need({a->gu, a->gv, a->out})) return fail(PCFD_E_ARG, "grad_T: null array");
+      k_adj_grad_T<<<grid, 256, 0, sm>>>(G, a->gu, a->gv, a->out);
+      break;
+    case PCFD_ADJ_DIV_T:
+      if (!need({a->out_u, a->out_v, a->a})) return fail(PCFD_E_ARG, "div_T: null array");
+      k_adj_div_T<<<grid, 256, 0, sm>>>(G, a->out_u, a->out_v, a->a);
+      break;
+    case PCFD_ADJ_OBJECTIVE_T:
+      if (!need({a->u, a->v, a->lower, a->out_u, a->out_v})) return fail(PCFD_E_ARG, "objective_T: null array");
+      k_adj_objective_T<<<grid, 256, 0, sm>>>(G, a->u, a->v, a->lower, a->out_u, a->out_v);
+      break;
+    default: return fail(PCFD_E_ARG, "unknown adjoint op %d", op);
+  }
+  CHECK_LAUNCH();
+  g_launches.fetch_add(1);
   return 0;
 }
 
