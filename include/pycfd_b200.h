@@ -131,6 +131,9 @@ typedef struct {
                                                  may spread its rows over (lanes per row
                                                  follow from it); 0 = 8 blocks of 256 per
                                                  SM, -1 = the storage lane count   */
+    int use_les;                              /* config.use_les: Smagorinsky closure, viscous
+                                                 term in stress-divergence form   */
+    double les_coeff;                         /* (Cs Delta)^2, Delta = sqrt(dx dy) */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */
@@ -177,6 +180,17 @@ int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double 
 
 /* Cell divergence, stateless: out nx*ny.  ProjectionSolver.divergence
  * (pycfd/core/solver.py:532-543). */
+/* The momentum RHS with the Smagorinsky closure (ProjectionSolver.momentum_rhs
+ * with config.use_les, pycfd/core/solver.py:501-529, :467-499, and
+ * SmagorinskyModel.eddy_viscosity, pycfd/physics/turbulence.py:68-118), uniform
+ * mesh: the effective viscosity nu + les_coeff |S| on the ghosted cell grid
+ * into nu_c ((nx+2) x (ny+2)), its corner average into nu_corner
+ * ((nx+1) x (ny+1)), and the right-hand side with the viscous term in
+ * stress-divergence form, bit-identical to the reference's array path. */
+int pycfd_momentum_rhs_les(const double* u, const double* v, int nx, int ny, double dx, double dy, double nu,
+                           double les_coeff, double blend, double fx, double fy, double* nu_c, double* nu_corner,
+                           double* rhs_u, double* rhs_v, void* stream);
+
 int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy,
                      double* out, void* stream);
 

@@ -167,6 +167,10 @@ struct pycfd_solver {
   unsigned long long* ptrace = nullptr;   // phase trace (measurement support)
   int trace_on = 0;
   double* hist = nullptr;       // device history of a device-side run loop (kHistRows x kHistCols)
+  int les = 0;                  // Smagorinsky closure on
+  double les_coeff = 0.0;       // (Cs Delta)^2
+  double* les_nu_c = nullptr;   // (nx+2) x (ny+2) effective viscosity of the current stage
+  double* les_nu_k = nullptr;   // (nx+1) x (ny+1) its corner average
   // CUDA-graph recording of whole steps
   bool capturing = false;
   cudaStream_t aux = nullptr;   // records the bodies of the solve loops
@@ -1065,9 +1069,23 @@ int substep_impl(pycfd_solver* s, StageIn uin, StageIn vin, double* us, double* 
   const Geo& g = s->g;
   dim3 blk(TJ, TI);
   dim3 grd((g.ny + 3 + TJ - 1) / TJ, (g.nx + 3 + TI - 1) / TI);
-  prof_mark(s, 6, stream);
-  pdl_launch(s, k_predictor, grd, blk, 0, stream, uin, vin, us, vs, g, s->S);
-  prof_mark(s, 6, stream);
+  if (s->les) {
+    // the stage input's effective viscosity, then the predictor in stress-divergence form
+    pdl_launch(s, k_les_nu, grid_for((long)(g.nx + 2) * (g.ny + 2), 256, kWaveBlocks), 256, 0, stream, uin, vin, g,
+               s->les_coeff, s->les_nu_c);
+    CHECK_LAUNCH();
+    pdl_launch(s, k_les_corner, grid_for((long)(g.nx + 1) * (g.ny + 1), 256, kWaveBlocks), 256, 0, stream,
+               (const double*)s->les_nu_c, g, s->les_nu_k);
+    CHECK_LAUNCH();
+    prof_mark(s, 6, stream);
+    pdl_launch(s, k_predictor_les, grd, blk, 0, stream, uin, vin, us, vs, g, (const double*)s->S,
+               (const double*)s->les_nu_c, (const double*)s->les_nu_k);
+    prof_mark(s, 6, stream);
+  } else {
+    prof_mark(s, 6, stream);
+    pdl_launch(s, k_predictor, grd, blk, 0, stream, uin, vin, us, vs, g, s->S);
+    prof_mark(s, 6, stream);
+  }
   CHECK_LAUNCH();
   TRY(launch_boundary(s, us, vs, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, stream));
   TRY(project_impl(s, us, vs, p, -1.0, stream));
@@ -1180,6 +1198,15 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->omega = d->sor_omega;
   s->mg_sweeps = std::max(1, d->mg_sweeps);
   s->scheme = d->time_scheme;
+  if (d->use_les) {
+    if (!(d->les_coeff >= 0.0)) return bail(fail(PCFD_E_ARG, "les_coeff must be non-negative"));
+    s->les = 1;
+    s->les_coeff = d->les_coeff;
+    int lrc;
+    if ((lrc = dalloc(s, &s->les_nu_c, (size_t)(d->nx + 2) * (d->ny + 2))) ||
+        (lrc = dalloc(s, &s->les_nu_k, (size_t)(d->nx + 1) * (d->ny + 1))))
+      return bail(lrc);
+  }
   s->precision = d->precision;
   s->inner_tol = d->inner_tol > 0 ? d->inner_tol : 1e-4;
   s->pdl = d->sequential_launch ? 0 : 1;
@@ -1464,6 +1491,29 @@ int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double 
   if (!u || !v || !rhs_u || !rhs_v || nx < 1 || ny < 1) return fail(PCFD_E_ARG, "bad arguments");
   dim3 blk(TJ, TI), grd((ny + 1 + TJ - 1) / TJ, (nx + 1 + TI - 1) / TI);
   k_rhs<<<grd, blk, 0, st(stream)>>>(u, v, nx, ny, dx, dy, nu, blend, fx, fy, rhs_u, rhs_v);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_momentum_rhs_les(const double* u, const double* v, int nx, int ny, double dx, double dy, double nu,
+                           double les_coeff, double blend, double fx, double fy, double* nu_c, double* nu_corner,
+                           double* rhs_u, double* rhs_v, void* stream) {
+  if (!u || !v || !nu_c || !nu_corner || !rhs_u || !rhs_v || nx < 1 || ny < 1 || !(les_coeff >= 0.0))
+    return fail(PCFD_E_ARG, "bad arguments");
+  cudaStream_t sm = st(stream);
+  Geo g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.dx = dx;
+  g.dy = dy;
+  g.nu = nu;
+  const StageIn U{u, nullptr, 1.0, 0.0}, V{v, nullptr, 1.0, 0.0};
+  k_les_nu<<<grid_for((long)(nx + 2) * (ny + 2), 256, kWaveBlocks), 256, 0, sm>>>(U, V, g, les_coeff, nu_c);
+  CHECK_LAUNCH();
+  k_les_corner<<<grid_for((long)(nx + 1) * (ny + 1), 256, kWaveBlocks), 256, 0, sm>>>(nu_c, g, nu_corner);
+  CHECK_LAUNCH();
+  dim3 blk(TJ, TI), grd((ny + 1 + TJ - 1) / TJ, (nx + 1 + TI - 1) / TI);
+  k_rhs_les<<<grd, blk, 0, sm>>>(u, v, nx, ny, dx, dy, blend, fx, fy, nu_c, nu_corner, rhs_u, rhs_v);
   CHECK_LAUNCH();
   return 0;
 }

@@ -76,6 +76,155 @@ __device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n,
   return -(duvdx + dvvdy) + nu * lap + fy;
 }
 
+// ---- Smagorinsky large-eddy closure (pycfd/physics/turbulence.py:25-118) -------
+// Effective viscosity nu + (Cs Delta)^2 |S| on the ghosted cell grid (nx+2, ny+2)
+// and its corner average on (nx+1, ny+1), then the viscous term in
+// stress-divergence form (pycfd/core/solver.py:467-499), uniform mesh.  The
+// expressions follow the reference's array code term by term, so the
+// viscosities and the right-hand side are bit-identical to it.
+template <class U, class V>
+__device__ __forceinline__ double les_s12_corner(const U& u, const V& v, int i, int j, int ny, double dx,
+                                                 double dy) {
+  const long W = ny + 2, WV = ny + 3;
+  const double dudy = (u[(long)(i + 1) * W + j + 1] - u[(long)(i + 1) * W + j]) / dy;
+  const double dvdx = (v[(long)(i + 1) * WV + j + 1] - v[(long)i * WV + j + 1]) / dx;
+  return 0.5 * (dudy + dvdx);
+}
+
+// nu_c at every ghosted cell: |S| = sqrt(2 s11^2 + 2 s22^2 + 4 s12^2), s11 and s22
+// across the cell, s12 the mean of the cell's four corner shear rates (ghost
+// cells take the nearest interior cell's mean, as the reference extends it).
+__global__ void k_les_nu(StageIn u, StageIn v, Geo g, double coeff, double* __restrict__ nu_c) {
+  pdl_begin();
+  const int nx = g.nx, ny = g.ny;
+  const long W = ny + 2, WV = ny + 3;
+  const long total = (long)(nx + 2) * (ny + 2);
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / (ny + 2)), j = (int)(e % (ny + 2));
+    const double s11 = (u[(long)(i + 1) * W + j] - u[(long)i * W + j]) / g.dx;
+    const double s22 = (v[(long)i * WV + j + 1] - v[(long)i * WV + j]) / g.dy;
+    const int ic = i < 1 ? 1 : (i > nx ? nx : i), jc = j < 1 ? 1 : (j > ny ? ny : j);
+    const double s12 = 0.25 * (les_s12_corner(u, v, ic - 1, jc - 1, ny, g.dx, g.dy) +
+                               les_s12_corner(u, v, ic, jc - 1, ny, g.dx, g.dy) +
+                               les_s12_corner(u, v, ic - 1, jc, ny, g.dx, g.dy) +
+                               les_s12_corner(u, v, ic, jc, ny, g.dx, g.dy));
+    const double smag = sqrt(2.0 * (s11 * s11) + 2.0 * (s22 * s22) + 4.0 * (s12 * s12));
+    nu_c[e] = g.nu + coeff * smag;
+  }
+}
+
+__global__ void k_les_corner(const double* __restrict__ nu_c, Geo g, double* __restrict__ nu_k) {
+  pdl_begin();
+  const int nx = g.nx, ny = g.ny;
+  const long W = ny + 2;
+  const long total = (long)(nx + 1) * (ny + 1);
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / (ny + 1)), j = (int)(e % (ny + 1));
+    nu_k[e] = 0.25 * (nu_c[(long)i * W + j] + nu_c[(long)(i + 1) * W + j] + nu_c[(long)i * W + j + 1] +
+                      nu_c[(long)(i + 1) * W + j + 1]);
+  }
+}
+
+// Advection as rhs_u_at, diffusion in stress-divergence form with the cell
+// viscosities nu_c (nx+2, ny+2) and corner viscosities nu_k (nx+1, ny+1).
+template <class U, class V>
+__device__ __forceinline__ double rhs_u_les_at(const U& u, const V& v, int m, int j, int ny, double dx, double dy,
+                                               double blend, double fx, const double* nu_c,
+                                               const double* nu_k) {
+  const long W = ny + 2, WV = ny + 3, WK = ny + 1;
+  const double u0 = u[m * W + j];
+  const double ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
+  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+  const double u_right = 0.5 * (u0 + ue);
+  const double u_left = 0.5 * (uw + u0);
+  double duudx = (u_right * u_right - u_left * u_left) / dx;
+  const double u_top = 0.5 * (u0 + un);
+  const double v_top = 0.5 * (v[(m - 1) * WV + j + 1] + v[m * WV + j + 1]);
+  const double u_bot = 0.5 * (us + u0);
+  const double v_bot = 0.5 * (v[(m - 1) * WV + j] + v[m * WV + j]);
+  double duvdy = (u_top * v_top - u_bot * v_bot) / dy;
+  if (blend > 0.0) {
+    duudx += blend / dx * (fabs(u_right) * (u0 - ue) * 0.5 - fabs(u_left) * (uw - u0) * 0.5);
+    duvdy += blend / dy * (fabs(v_top) * (u0 - un) * 0.5 - fabs(v_bot) * (us - u0) * 0.5);
+  }
+  const double dudx_r = (ue - u0) / dx, dudx_l = (u0 - uw) / dx;
+  const double tau_t = nu_k[(long)(m - 1) * WK + j] * ((un - u0) / dy + (v[(long)m * WV + j + 1] - v[(long)(m - 1) * WV + j + 1]) / dx);
+  const double tau_b = nu_k[(long)(m - 1) * WK + j - 1] * ((u0 - us) / dy + (v[(long)m * WV + j] - v[(long)(m - 1) * WV + j]) / dx);
+  const double d = 2.0 * (nu_c[(long)m * W + j] * dudx_r - nu_c[(long)(m - 1) * W + j] * dudx_l) / dx +
+                   (tau_t - tau_b) / dy;
+  return -(duudx + duvdy) + d + fx;
+}
+
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_les_at(const U& u, const V& v, int i, int n, int ny, double dx, double dy,
+                                               double blend, double fy, const double* nu_c,
+                                               const double* nu_k) {
+  const long W = ny + 2, WV = ny + 3, WK = ny + 1;
+  const double v0 = v[i * WV + n];
+  const double vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
+  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+  const double v_top = 0.5 * (v0 + vn);
+  const double v_bot = 0.5 * (vs + v0);
+  double dvvdy = (v_top * v_top - v_bot * v_bot) / dy;
+  const double u_right = 0.5 * (u[(i + 1) * W + n - 1] + u[(i + 1) * W + n]);
+  const double v_right = 0.5 * (v0 + ve);
+  const double u_left = 0.5 * (u[i * W + n - 1] + u[i * W + n]);
+  const double v_left = 0.5 * (vw + v0);
+  double duvdx = (u_right * v_right - u_left * v_left) / dx;
+  if (blend > 0.0) {
+    dvvdy += blend / dy * (fabs(v_top) * (v0 - vn) * 0.5 - fabs(v_bot) * (vs - v0) * 0.5);
+    duvdx += blend / dx * (fabs(u_right) * (v0 - ve) * 0.5 - fabs(u_left) * (vw - v0) * 0.5);
+  }
+  // corners (i, n-1) and (i-1, n-1) of the v face
+  const double tau_r = nu_k[(long)i * WK + n - 1] *
+                       ((u[(long)(i + 1) * W + n] - u[(long)(i + 1) * W + n - 1]) / dy + (ve - v0) / dx);
+  const double tau_l = nu_k[(long)(i - 1) * WK + n - 1] *
+                       ((u[(long)i * W + n] - u[(long)i * W + n - 1]) / dy + (v0 - vw) / dx);
+  const double dvdy_t = (vn - v0) / dy, dvdy_b = (v0 - vs) / dy;
+  const double d = (tau_r - tau_l) / dx +
+                   2.0 * (nu_c[(long)i * W + n] * dvdy_t - nu_c[(long)i * W + n - 1] * dvdy_b) / dy;
+  return -(duvdx + dvvdy) + d + fy;
+}
+
+// Stateless LES RHS into (nx+1, ny) and (nx, ny+1) blocks.
+__global__ void k_rhs_les(const double* __restrict__ u, const double* __restrict__ v, int nx, int ny, double dx,
+                          double dy, double blend, double fx, double fy, const double* __restrict__ nu_c,
+                          const double* __restrict__ nu_k, double* __restrict__ rhs_u,
+                          double* __restrict__ rhs_v) {
+  pdl_begin();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i <= nx && j < ny)
+    rhs_u[(long)i * ny + j] = rhs_u_les_at(u, v, i + 1, j + 1, ny, dx, dy, blend, fx, nu_c, nu_k);
+  if (i < nx && j <= ny)
+    rhs_v[(long)i * (ny + 1) + j] = rhs_v_les_at(u, v, i + 1, j + 1, ny, dx, dy, blend, fy, nu_c, nu_k);
+}
+
+// Predictor with the LES right-hand side (the stage input's viscosities precomputed).
+__global__ void k_predictor_les(StageIn u, StageIn v, double* __restrict__ us, double* __restrict__ vs, Geo g,
+                                const double* __restrict__ S, const double* __restrict__ nu_c,
+                                const double* __restrict__ nu_k) {
+  pdl_begin();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nx = g.nx, ny = g.ny;
+  const double dt = S[S_DT], blend = S[S_BLEND];
+  if (i < nx + 3 && j < ny + 2) {
+    const long k = (long)i * (ny + 2) + j;
+    double val = u[k];
+    if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
+      val = val + dt * rhs_u_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k);
+    us[k] = val;
+  }
+  if (i < nx + 2 && j < ny + 3) {
+    const long k = (long)i * (ny + 3) + j;
+    double val = v[k];
+    if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
+      val = val + dt * rhs_v_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k);
+    vs[k] = val;
+  }
+}
+
 // Stateless RHS into (nx+1, ny) and (nx, ny+1) blocks.
 __global__ void k_rhs(const double* __restrict__ u, const double* __restrict__ v, int nx, int ny,
                       double dx, double dy, double nu, double blend, double fx, double fy,

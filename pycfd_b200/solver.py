@@ -136,6 +136,35 @@ class BoundaryInfo:
         return full
 
 
+def les_coefficient(cs: float, mesh) -> float:
+    """``(Cs Delta)^2`` with the filter width Delta = sqrt(dx dy) of a uniform mesh
+    (``pycfd/physics/turbulence.py:38-52``)."""
+    delta = float(np.sqrt(mesh.dx * mesh.dy))
+    return (float(cs) * delta) ** 2
+
+
+class GpuSmagorinsky:
+    """The Smagorinsky closure of a GPU solver (``pycfd/physics/turbulence.py:25-118``):
+    its constant, filter width and the eddy viscosity evaluated on the device."""
+
+    def __init__(self, solver, cs: float) -> None:
+        self.solver = solver
+        self.mesh = solver.mesh
+        self.cs = float(cs)
+        self.delta = float(np.sqrt(self.mesh.dx * self.mesh.dy))
+        self._coeff = les_coefficient(cs, self.mesh)
+        self.last_nu_t_max = 0.0
+
+    def eddy_viscosity(self, u, v, nu_molecular: float):
+        """``(nu_c, nu_corner)``: nu + nu_t at the ghosted cell centres and at the corners."""
+        nu_c, nu_k, _, _ = self.solver._les_rhs(u, v, 0.0)
+        self.last_nu_t_max = float((nu_c - nu_molecular).max())
+        return nu_c, nu_k
+
+    def __repr__(self) -> str:
+        return f"SmagorinskyModel(cs={self.cs:g}, delta={self.delta:.4g})"
+
+
 def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind, options,
                 levels=None, cinv=None):
     """The ``pycfd_solver_desc`` of one problem and the host arrays it points into.
@@ -147,6 +176,9 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     d = _lib.SolverDesc()
     d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, mesh.dx, mesh.dy, config.nu
     d.body_fx, d.body_fy = cfg.body_force
+    if cfg.use_les:
+        d.use_les = 1
+        d.les_coeff = les_coefficient(cfg.smagorinsky_cs, mesh)
     keep = []
     for w, wall in enumerate(WALLS):
         spec = boundaries.specs[wall]
@@ -304,8 +336,6 @@ class ProjectionSolver:
             raise NotImplementedError(
                 "solver_type='simple' is reserved for a future SIMPLE implementation; only "
                 "'projection' is available. Set solver_type='projection'.")
-        if config.use_les:
-            raise NotImplementedError("the GPU projection path is laminar; use_les=True is not provided")
         kind = PressureSolver(config.pressure_solver)
         if kind is PressureSolver.DIRECT:
             raise NotImplementedError(
@@ -351,7 +381,7 @@ class ProjectionSolver:
             self.poisson = assemble(*args)
         self._create_native(kind)
         self.pressure_solver = GpuPoissonSolver(self, kind)
-        self.turbulence = None
+        self.turbulence = GpuSmagorinsky(self, config.smagorinsky_cs) if config.use_les else None
         self.body_force_reaction = (0.0, 0.0)
         self.body_force_reactions = tuple((0.0, 0.0) for _ in self.body_masks)
         self._blend = 0.0
@@ -458,9 +488,26 @@ class ProjectionSolver:
         self._read_stats()
         return fields
 
-    def momentum_rhs(self, u, v, blend: float = 0.0):
-        """``-A(u) + nu lap(u) + f`` as ``(nx+1, ny)`` and ``(nx, ny+1)`` tensors."""
+    def _les_rhs(self, u, v, blend):
         torch = _torch()
+        u, v = self._dev(u).contiguous(), self._dev(v).contiguous()
+        nx, ny = self.mesh.shape
+        f64 = dict(dtype=torch.float64, device="cuda")
+        nu_c, nu_k = torch.empty((nx + 2, ny + 2), **f64), torch.empty((nx + 1, ny + 1), **f64)
+        ru, rv = torch.empty((nx + 1, ny), **f64), torch.empty((nx, ny + 1), **f64)
+        fx, fy = self.config.body_force
+        _lib.check(self._L.pycfd_momentum_rhs_les(
+            _lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx, self.mesh.dy, self.nu, self.turbulence._coeff,
+            float(blend), fx, fy, _lib.ptr(nu_c), _lib.ptr(nu_k), _lib.ptr(ru), _lib.ptr(rv), _stream()))
+        return nu_c, nu_k, ru, rv
+
+    def momentum_rhs(self, u, v, blend: float = 0.0):
+        """``-A(u) + D(u) + f`` as ``(nx+1, ny)`` and ``(nx, ny+1)`` tensors; D is
+        ``nu lap(u)``, or the stress divergence of ``nu + nu_t`` with the Smagorinsky
+        closure (``pycfd/core/solver.py:501-529``)."""
+        torch = _torch()
+        if self.turbulence is not None:
+            return self._les_rhs(u, v, blend)[2:]
         u, v = self._dev(u).contiguous(), self._dev(v).contiguous()
         nx, ny = self.mesh.shape
         ru = torch.empty((nx + 1, ny), dtype=torch.float64, device="cuda")

@@ -197,3 +197,8 @@ def shape_image(rows=37, cols=53, seed=4):
 CKPT_CAVITY = dict(nx=32, ny=32, re=100.0, dt=1.0, t_end=1e9, cfl_max=0.5, adaptive_dt=True,
                    pressure_solver="mgcg", poisson_tol=1e-12,
                    boundary_config=bcs(top=("moving_wall", 1.0)), name="ckpt_cavity")
+
+
+LES_CAVITY = dict(nx=40, ny=40, re=5000.0, use_les=True, smagorinsky_cs=0.17, dt=2e-3, t_end=10.0,
+                  adaptive_dt=False, pressure_solver="cg", poisson_tol=1e-12,
+                  boundary_config=bcs(top=("moving_wall", 1.0)), name="les_cavity")

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder by running the reference itself.
 
-The reference (kiliancmd/pycfd, pure Python) is imported from a source tree given
+The reference (kiliancmd/pycfd, pure Python) is imported from a source tree
 given as the first command-line argument, and driven through its own
 public API.  Nothing here runs on the GPU host: the fixtures it writes are the
 committed ``*.npz`` files beside this script, which the tests read.
@@ -21,6 +21,7 @@ Cases (all seeded, all synthetic):
   shapes.npz     polygon, rectangle and image masks with their fractions (200x120)
   ref_checkpoint.npz (+ _continued)  a reference checkpoint and the state 10 steps on
   interchange.npz  this package's checkpoint writer read back by the reference's loader
+  les.npz        Smagorinsky eddy viscosity, LES momentum RHS, and 10 LES cavity steps
 """
 
 from __future__ import annotations
@@ -366,6 +367,34 @@ def gen_interchange():
     save("interchange.npz", loaded_by_reference=np.array(bool(same and cfg_same)))
 
 
+def gen_les():
+    """The Smagorinsky closure (pycfd/physics/turbulence.py:25-118 and the
+    stress-divergence viscous term, pycfd/core/solver.py:467-529): eddy
+    viscosities and the momentum RHS on random fields (blend 0 and 0.6), and a
+    cavity run with use_les=True for 10 steps."""
+    out = {}
+    for k, (nx, ny, blend) in enumerate(((20, 16, 0.0), (13, 22, 0.6))):
+        c = dict(nx=nx, ny=ny, lx=1.0 + 0.1 * k, ly=1.0, re=2000.0, use_les=True, smagorinsky_cs=0.17,
+                 body_force=(0.1, -0.2), dt=1e-3, t_end=1.0, adaptive_dt=False, pressure_solver="cg",
+                 boundary_config=cases.bcs(top=("moving_wall", 1.0)), name="les")
+        cfg = ref_config(c)
+        s = ProjectionSolver(cfg)
+        rng = np.random.default_rng(30 + k)
+        u = rng.standard_normal((nx + 3, ny + 2))
+        v = rng.standard_normal((nx + 2, ny + 3))
+        nu_c, nu_k = s.turbulence.eddy_viscosity(u, v, s.nu)
+        ru, rv = s.momentum_rhs(u, v, blend)
+        out.update({f"c{k}_u": u, f"c{k}_v": v, f"c{k}_blend": np.array(blend), f"c{k}_nu_c": nu_c,
+                    f"c{k}_nu_k": nu_k, f"c{k}_rhs_u": np.array(ru), f"c{k}_rhs_v": np.array(rv)})
+    cfg = ref_config(cases.LES_CAVITY)
+    s = ProjectionSolver(cfg)
+    f = s.initialize()
+    for _ in range(10):
+        f = s.step(f, cfg.dt)
+    out.update({"cav_u": f.u, "cav_v": f.v, "cav_p": f.p})
+    save("les.npz", **out)
+
+
 def gen_masks():
     big = StructuredMesh(2048, 1024, 2.0, 1.0)
     m = circle_mask(big, (0.5, 0.5), 0.05).mask
@@ -378,9 +407,10 @@ def gen_masks():
 if __name__ == "__main__":
     which = set(sys.argv[2:]) or {"rhs", "poisson", "multigrid", "solvers", "steps",
                                   "cavity64", "cylinder", "masks", "faces", "cylinder_long", "shapes",
-                                  "checkpoint", "interchange"}
+                                  "checkpoint", "interchange", "les"}
     for name in ("rhs", "poisson", "multigrid", "solvers", "steps", "cavity64",
-                 "cylinder", "masks", "faces", "cylinder_long", "shapes", "checkpoint", "interchange"):
+                 "cylinder", "masks", "faces", "cylinder_long", "shapes", "checkpoint", "interchange",
+                 "les"):
         if name in which:
             t0 = time.perf_counter()
             globals()["gen_" + name]()
