@@ -1,20 +1,29 @@
-"""Throughput of the projection step: cell-updates/s on the 512x512 Taylor-Green vortex.
+"""Throughput of the projection step in cell-updates/s: the 256-cavity batch (default).
 
-One step = one SSP-RK3 time step of the whole 512x512 doubly periodic vortex
-(Re 1000, fixed dt = 0.4*2pi/512, MG-PCG to 1e-10, three projections).
-value = cells x steps / device time of the timed steps (CUDA events on the
-launching stream, barrier + synchronise on both sides, max over ranks).  The
-working set (~60 MB) fits in the 126 MB L2, so L2 is flushed between timed
-steps by writing a 256 MB buffer outside the timed events.
+Workload (default, ``--workload batch``): 256 seeded lid-driven cavities per GPU,
+N in {64, 96, 128, 192, 256}, Re log-uniform in [100, 2000], lid speed uniform
+in [0.5, 1.5], adaptive dt at CFL 0.5, MG-PCG to 1e-10, advanced by the batched
+engine in the mixed form (FP32 MG-PCG inside FP64 refinement).  One step = one
+SSP-RK3 step of every cavity; value = cells of all ranks x steps / device time
+(CUDA events on the launching stream, barrier + synchronise on both sides,
+max over ranks).  The working set (~0.5 GB) exceeds L2.  Beside it the line
+carries the batched engine in FP64 and the plain FP64 path (one single-problem
+solver per cavity, recorded steps on 16 streams), their ratios, the per-kernel
+roofline of one eager step, the end-to-end figure through host buffers and the
+CPU baseline.  Under torchrun the 256*N cavities of one seeded draw are split
+over the ranks by cell count (no exchange on the data path).
+
+``--workload tgv512``: one SSP-RK3 step of the 512x512 Taylor-Green vortex on the
+single-problem path (L2 flushed between steps).  Other workloads: adjoint,
+tgv-validation, cylinder.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed]
+                    [--workload batch|tgv512|...] [--precision fp64|mixed]
 
 --impl reference times the reference algorithm's CPU implementation (the NumPy/
 SciPy restatement in oracle/, which only this arm and the cpu_baseline leg run)
-on the host cores, on the same workload and metric.  Under torchrun every rank
-advances its own replica of the vortex (the path does not shard: replicas only)
-and rank 0 prints one JSON line.
+on the host cores, one single-threaded process per cavity, on the same workload
+and metric; under torchrun rank 0 alone runs it.
 """
 
 from __future__ import annotations
@@ -310,6 +319,378 @@ def batch_cpu_baseline(cfgs, steps=1, warmup=0, workers=None):
                       f"{warmup} untimed step(s), timed together ({wall:.1f} s wall)"}
 
 
+def batch_kernel_bytes(kid, cells, its, s_bytes):
+    """Algorithmic bytes of one eager step's launches of kernel kind `kid` (ids of
+    pycfd_batch_profile), from each problem's CG passes in that step."""
+    passes = float((its * cells).sum())
+    if kid == 1:     # k_b_cg_pq: read z, p_old, flags; write p, q
+        return passes * (4 * s_bytes + 1)
+    if kid == 5:     # k_b_cg_xr: read p, x, r, q, flags; write x, r
+        return passes * (6 * s_bytes + 1)
+    if kid == 2:     # k_b_fine (last sweep): read x0, r, flags; write z
+        return passes * (3 * s_bytes + 1)
+    if kid == 3:     # k_b_fine (first sweep): read r, flags; write x0, lres0
+        return passes * (3 * s_bytes + 1)
+    if kid == 6:     # k_b_predictor, 3 per step: read u, v; write u*, v* (FP64 state)
+        return 3.0 * float(cells.sum()) * 32
+    return None
+
+
+KERNEL_NAMES = {1: "k_b_cg_pq (batched CG direction p = z + beta p, q = A p, p.q)",
+                2: "k_b_fine<FM_LAST> (last level-0 V-cycle sweep, z and r.z)",
+                3: "k_b_fine<FM_PRE> (first level-0 sweep and residual)",
+                5: "k_b_cg_xr (batched CG update x, r, norms)",
+                6: "k_b_predictor (momentum RHS + Runge-Kutta stage, FP64 state)"}
+
+
+def run_batch(args, world, rank, local):
+    """The cavity batch: 256 seeded lid-driven cavities of uneven size, Re and lid
+    speed per GPU.  At N GPUs the 256*N cavities of one seeded draw are split over
+    the ranks by cell count (no exchange on the data path); every rank advances its
+    share with the batched engine (every stage one launch over all its problems).
+    Beside it, on the same problems and steps: the plain FP64 path (one
+    single-problem solver per cavity, recorded steps replayed on 16 streams) and
+    the batched engine in FP64."""
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    from pycfd_b200 import _lib
+    from pycfd_b200.batch import (BatchAutotuner, BatchedSolver, BatchOptions, BatchRunner,
+                                  cavity_batch_configs, partition_by_cells)
+    from pycfd_b200.solver import GpuOptions
+    all_cfgs = cavity_batch_configs(count=args.batch * world, seed=0)
+    cfgs = [all_cfgs[k] for k in partition_by_cells(all_cfgs, world)[rank]]
+    my_cells = sum(c.nx * c.ny for c in cfgs)
+    total_cells = sum(c.nx * c.ny for c in all_cfgs)
+    t0 = time.perf_counter()
+    if args.autotune:
+        opts = BatchAutotuner(allowed_precisions=(args.precision,)).choose(cfgs)
+    else:
+        tail = args.batch_tail
+        opts = BatchOptions(precision=args.precision, tile_rows=args.tile_rows,
+                            mg_sweeps=args.mg_sweeps, inner_tol=args.inner_tol,
+                            coarse_level=args.coarse_level, coarse_tail=tail != "off",
+                            tail_ratio=None if tail in ("none", "off") else float(tail),
+                            fused_restriction=args.fused_from > 0, fused_from=max(1, args.fused_from))
+    b = BatchedSolver(cfgs, opts)
+    setup = time.perf_counter() - t0
+    rec = not args.eager
+
+    def timed(step_fn, k):
+        """Device ms of k steps (events on the launching stream, barrier + sync both sides)."""
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        step_fn(k)
+        ev1.record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1), dist, "cuda")
+
+    b.step(args.spinup, record=rec)
+    b.step(args.warmup, record=rec)
+    torch.cuda.synchronize()
+    b.launches(0)
+    n_launch0 = _lib.load().pycfd_launch_count()
+    clocks = Clocks(local) if rank == 0 else None
+    ms = timed(lambda k: b.step(k, record=rec), args.steps)
+    ck = clocks.stop() if clocks else None
+    launches = b.launches(args.steps) if rec else int(_lib.load().pycfd_launch_count() - n_launch0)
+    value = total_cells * args.steps / (ms / 1e3)
+    st = b.status()
+    its = st["iterations"]
+    divs = np.array([b.field_stats(k).max_div for k in range(len(b))])
+    # roofline: the kernel kind with the largest share of one eager step
+    s_bytes = 4 if opts.precision == "mixed" else 8
+    cells = np.array([c.nx * c.ny for c in cfgs], dtype=np.float64)
+    prof = {}
+    if not args.no_profile:
+        for kid in (1, 2, 3, 5, 6):
+            kms, kn, kits = b.profile(kid, 1)
+            prof[kid] = (kms, kn, batch_kernel_bytes(kid, cells, kits, s_bytes))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if hbm is None:
+        hbm, peak_src = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+    roof = None
+    if prof:
+        top = max(prof, key=lambda k: prof[k][0])
+        kms, kn, kbytes = prof[top]
+        achieved = kbytes / (kms / 1e3) / 1e9 if kms > 0 else None
+        traffic = None
+        try:
+            tr = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic.json")))
+            traffic = tr.get("batch_" + opts.precision, {}).get(str(top))
+        except Exception:
+            pass
+        roof = {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm if achieved else None, "traffic": traffic,
+                "bytes_per_launch": kbytes / max(kn, 1), "us_per_launch": 1e3 * kms / max(kn, 1),
+                "launches": kn, "peak_source": peak_src,
+                "timing": "CUDA events around each eager launch of the kernel over one step; bytes = "
+                          "sum over problems of its passes x cells x bytes per cell",
+                "kernels": {KERNEL_NAMES[k].split(" ")[0] + ("" if k not in (2, 3) else f"[{k}]"):
+                            {"ms": v[0], "launches": v[1],
+                             "gb_s": (v[2] / (v[0] / 1e3) / 1e9) if v[0] > 0 and v[2] else None}
+                            for k, v in prof.items()},
+                "traffic_source": "profiles/roofline_traffic.json (one ncu capture of this kernel)"}
+    # end to end: (u, v) of every cavity from pinned host memory, one step, (u, v, p) back
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
+    e2e = None
+    if e2e_steps:
+        b.step_host(1)
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        b.step_host(e2e_steps)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
+        h2d, d2h = b.state_bytes()
+        e2e = {"value": total_cells * e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "note": "per rank; every cavity's (u, v) H2D and (u, v, p) D2H inside each timed step"}
+    del b
+    fp64b = plain = None
+    if not args.no_plain:
+        # the batched engine in FP64 on the same problems and steps
+        o64 = BatchAutotuner(allowed_precisions=("fp64",)).choose(cfgs) if args.autotune else \
+            BatchOptions(precision="fp64")
+        b64 = BatchedSolver(cfgs, o64)
+        b64.step(args.spinup + args.warmup)
+        ms64 = timed(lambda k: b64.step(k), args.steps)
+        fp64b = {"value": total_cells * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                 "max_div": max(b64.field_stats(k).max_div for k in range(len(b64))),
+                 "options": o64.__dict__}
+        del b64
+        # the plain FP64 path on the same problems: per-problem recorded steps on 16 streams
+        popts = {"auto": GpuOptions(precision="fp64"),
+                 "compact": GpuOptions(precision="fp64", tail_ratio=4.0),
+                 "off": GpuOptions(precision="fp64", coarse_tail=False)}[args.plain_tail]
+        runner = BatchRunner(cfgs, streams=16, options=popts)
+        runner.step(args.spinup + args.warmup)
+        pms = timed(runner.step, args.steps)
+        plain = {"value": total_cells * args.steps / (pms / 1e3), "ms_per_step": pms / args.steps,
+                 "steps": args.steps, "form": "fp64, one single-problem solver per cavity, "
+                                             "recorded steps replayed on 16 streams",
+                 "dense_tail": args.plain_tail}
+        del runner
+    if rank == 0:
+        sizes = {}
+        for c in all_cfgs:
+            sizes[str(c.nx)] = sizes.get(str(c.nx), 0) + 1
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64/f32" if opts.precision == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": f"batch of {args.batch} lid-driven cavities per GPU "
+                                       f"(seed 0, {args.batch * world} in all, split over ranks by cells)",
+                           "cells": total_cells, "cells_rank0": my_cells, "sizes": sizes,
+                           "re": "log-uniform 100..2000", "lid": "uniform 0.5..1.5",
+                           "pressure_solver": "mgcg", "poisson_tol": cfgs[0].poisson_tol,
+                           "dt": "adaptive, CFL 0.5, per cavity",
+                           "precision": opts.precision, "options": opts.__dict__,
+                           "autotuned": bool(args.autotune), "setup_s": setup,
+                           "spinup_steps": args.spinup,
+                           "cg_iterations_per_step": float(np.mean(its)),
+                           "stopped": int((st["frozen"] != 0).sum()),
+                           "max_div": float(divs.max()), "cavities_div_le_1e-8": int((divs <= 1e-8).sum()),
+                           "parallelism": f"problem partition x{world}",
+                           "l2": "working set larger than L2 (no flush needed)",
+                           "cell_update": "one cell advanced by one RK3 step, summed over the batch",
+                           "batched_fp64": fp64b, "plain_fp64_path": plain,
+                           "mixed_batched_vs_plain_fp64": value / plain["value"] if plain else None,
+                           "mixed_batched_vs_batched_fp64": value / fp64b["value"] if fp64b else None},
+                "e2e": e2e, "clocks": ck, "roofline": roof, "gpu_launches": launches}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = batch_cpu_baseline(cfgs, steps=1, workers=16)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_tgv_validation(args, local):
+    """The 512x512 vortex over 500 steps in the FP64 path and in the mixed form: error of
+    each against the analytic decay (u, v ~ exp(-2 nu t), p ~ exp(-4 nu t), mean-free)
+    and of the mixed form against FP64."""
+    import torch
+    torch.cuda.set_device(local)
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    cfg = tgv_config()
+    steps = args.val_steps
+    out, fields = {}, {}
+    for prec in ("fp64", "mixed"):
+        s = ProjectionSolver(cfg, options=GpuOptions(precision=prec))
+        f = s.initialize(*tgv_init(s.mesh))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(steps):
+            f = s.advance(f, cfg.dt)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        t = steps * cfg.dt
+        nu = cfg.nu
+        Xu, Yu = s.mesh.u_grid()
+        Xv, Yv = s.mesh.v_grid()
+        ue = np.sin(Xu) * np.cos(Yu) * np.exp(-2 * nu * t)
+        ve = -np.cos(Xv) * np.sin(Yv) * np.exp(-2 * nu * t)
+        xc, yc = s.mesh.xc, s.mesh.yc
+        pe = 0.25 * (np.cos(2 * xc)[:, None] + np.cos(2 * yc)[None, :]) * np.exp(-4 * nu * t)
+        pe -= pe.mean()
+        u = f.u_phys.cpu().numpy()
+        v = f.v_phys.cpu().numpy()
+        p = f.p[1:-1, 1:-1].cpu().numpy()
+        p = p - p.mean()
+        st = s.field_stats(f)
+        fields[prec] = (u, v, p)
+        out[prec] = {"ms_per_step": ms, "cell_updates_per_s": N * N / (ms / 1e3),
+                     "err_u": float(np.abs(u - ue).max() / np.abs(ue).max()),
+                     "err_v": float(np.abs(v - ve).max() / np.abs(ve).max()),
+                     "err_p": float(np.abs(p - pe).max() / np.abs(pe).max()), "max_div": st.max_div}
+        del s
+    uf, vf, pf = fields["fp64"]
+    um, vm, pm = fields["mixed"]
+    scale = max(np.abs(uf).max(), np.abs(vf).max())
+    out["mixed_vs_fp64"] = {"velocity": float(max(np.abs(um - uf).max(), np.abs(vm - vf).max()) / scale),
+                            "pressure": float(np.abs(pm - pf).max() / np.abs(pf).max())}
+    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config({"validation": out, "t_end": steps * cfg.dt})}
+    print(json.dumps(line), flush=True)
+
+
+def run_cylinder(args, local):
+    """Flow past a cylinder on the 2048x1024 channel (Re 100, D 0.1 at (0.5, 0.5), uniform
+    inflow 1, convective outlet, slip walls, 1e-3 seeded noise), MG-PCG 1e-10, adaptive dt:
+    Cd and Cl histories in the FP64 path and in the mixed form."""
+    import torch
+    torch.cuda.set_device(local)
+    from pycfd_b200.config import BCKind, BCSpec, SimulationConfig
+    from pycfd_b200.mesh import StructuredMesh
+    from pycfd_b200.obstacles import circle_mask
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    nx, ny = 2048, 1024
+    walls = {"left": BCSpec(BCKind.INLET, velocity=1.0), "right": BCSpec(BCKind.OUTLET),
+             "bottom": BCSpec(BCKind.SYMMETRY), "top": BCSpec(BCKind.SYMMETRY)}
+    cfg = SimulationConfig(nx=nx, ny=ny, lx=2.0, ly=1.0, re=100.0, u_ref=1.0, l_ref=0.1, dt=1.0,
+                           t_end=1e9, cfl_max=0.5, pressure_solver="mgcg", poisson_tol=1e-10,
+                           boundary_config=walls, name="cylinder")
+    mesh = StructuredMesh.from_config(cfg)
+    obstacle = circle_mask(mesh, (0.5, 0.5), 0.05)
+    rng = np.random.default_rng(0)
+    u0 = 1.0 + 1e-3 * rng.standard_normal((nx + 1, ny))
+    v0 = 1e-3 * rng.standard_normal((nx, ny + 1))
+    steps, every = args.cyl_steps, 20
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = ProjectionSolver(cfg, mesh, obstacle, options=GpuOptions(precision=prec))
+        f = s.initialize(u0, v0)
+        s.set_clock(0.0)
+        ts, cd, cl = [], [], []
+        dev_ms = 0.0
+        for k in range(steps // every):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(every):
+                f = s.advance_adaptive(f)
+            b.record()
+            torch.cuda.synchronize()
+            dev_ms += a.elapsed_time(b)
+            st = s._read_stats()
+            t, dt, n, h = s.clock()
+            if h:
+                break
+            ts.append(t)
+            cd.append(st.fx / 0.05)
+            cl.append(st.fy / 0.05)
+        ts, cd, cl = np.array(ts), np.array(cd), np.array(cl)
+        half = ts >= 0.5 * ts[-1]
+        clh = cl[half] - cl[half].mean()
+        crossings = np.where(np.diff(np.sign(clh)) > 0)[0]
+        st_num = None
+        if len(crossings) >= 2:
+            period = (ts[half][crossings[-1]] - ts[half][crossings[0]]) / (len(crossings) - 1)
+            st_num = 0.1 / period
+        fs = s.field_stats(f)
+        out[prec] = {"steps": int(n), "t_end": float(ts[-1]), "ms_per_step": dev_ms / max(n, 1),
+                     "cell_updates_per_s": nx * ny * n / (dev_ms / 1e3),
+                     "cd_mean_second_half": float(cd[half].mean()), "cl_amplitude_second_half":
+                     float(0.5 * (cl[half].max() - cl[half].min())), "strouhal": st_num,
+                     "max_div": fs.max_div, "health": int(h),
+                     "cd_every_20": [round(float(x), 6) for x in cd[::10]],
+                     "cl_every_20": [round(float(x), 6) for x in cl[::10]]}
+        del s
+    line = {"metric": METRIC, "value": out["fp64"]["cell_updates_per_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": 0, "ms_per_step": out["fp64"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cylinder channel 2048x1024, Re 100", "runs": out}}
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, world, rank, local):
+    """Gradient of the lower-half kinetic energy of the 256x256 Re 400 cavity after 200
+    steps w.r.t. 32 lid modes and the smoothed-disk radius: hand-written adjoint with
+    10-step checkpoints, checked against central differences (h = 1e-6) on 3 components."""
+    import torch
+    torch.cuda.set_device(local)
+    from pycfd_b200.adjoint import AdjointCavity, Geometry, MultigridSolve, gradient, rollout
+    cav = AdjointCavity()
+    g = Geometry(cav, device="cuda")
+    solve = MultigridSolve(cav.n, tol=cav.tol)
+    theta = torch.tensor(cav.default_theta(), dtype=torch.float64, device="cuda")
+    radius = torch.tensor(cav.radius, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    solve.calls = 0
+    J, gt, gr = gradient(theta, radius, g, solve)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    grad_solves = solve.calls
+    t0 = time.perf_counter()
+    J0, _ = rollout(theta, radius, g, solve)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    h = 1e-6
+    checks = []
+    with torch.no_grad():
+        for k in (0, 7):
+            e = torch.zeros_like(theta)
+            e[k] = h
+            fd = float((rollout(theta + e, radius, g, solve)[0] - rollout(theta - e, radius, g, solve)[0]) / (2 * h))
+            checks.append({"param": f"theta_{k + 1}", "adjoint": float(gt[k]), "fd": fd,
+                           "rel_err": abs(fd - float(gt[k])) / max(abs(fd), 1e-300)})
+        fd = float((rollout(theta, radius + h, g, solve)[0] - rollout(theta, radius - h, g, solve)[0]) / (2 * h))
+        checks.append({"param": "radius", "adjoint": float(gr), "fd": fd,
+                       "rel_err": abs(fd - float(gr)) / max(abs(fd), 1e-300)})
+    cells = cav.n * cav.n
+    line = {"metric": "gradient of J (lower-half kinetic energy) w.r.t. 33 parameters, adjoint",
+            "value": cells * cav.steps / t_grad, "unit": "cell-updates/s (forward + adjoint sweep)",
+            "n_gpus": 1, "steps": cav.steps, "warmup": 0, "ms_per_step": 1e3 * t_grad / cav.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "lid-driven cavity 256x256, Re 400, 200 steps, dt 1.2e-3, "
+                                   "32 sine lid modes (seeded) + tanh disk radius at (0.5, 0.3), "
+                                   "r 0.08, width 2 cells",
+                       "poisson_tol": cav.tol, "checkpoint_every": cav.checkpoint,
+                       "J": float(J), "forward_s": t_fwd, "gradient_s": t_grad,
+                       "gradient_over_forward": t_grad / t_fwd, "poisson_solves_in_gradient": grad_solves,
+                       "fd_checks": checks, "max_fd_rel_err": max(c["rel_err"] for c in checks)}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -476,6 +857,10 @@ def main():
                     help="batch: dense V-cycle tail per structure -- a bound r (n_t^2 <= r n_0), none, or off")
     ap.add_argument("--plain-tail", default="auto", choices=["auto", "compact", "off"],
                     help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
+    ap.add_argument("--fused-from", type=int, default=0, choices=[0, 1, 2],
+                    help="batch, --no-autotune: down sweep by fused restrictions from this level (0: off)")
+    ap.add_argument("--no-profile", action="store_true",
+                    help="batch: skip the per-kernel eager timing of the roofline block")
     ap.add_argument("--no-plain", action="store_true",
                     help="batch: skip the plain per-problem FP64 comparison leg")
     args = ap.parse_args()
