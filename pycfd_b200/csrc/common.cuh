@@ -227,6 +227,104 @@ __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Ge
   for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < (g).nx; i += gridDim.y * blockDim.y) \
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < (g).ny; j += gridDim.x * blockDim.x)
 
+// ---- warp strips of one grid ------------------------------------------------
+// The fine-level solver kernels walk the grid in warp strips: a warp takes one
+// 32-column segment of y (lane = column: every row load is one coalesced
+// access) over kStripRows rows of x.  The stencil operand of the strip and its
+// two halo rows are formed once, into registers, before any arithmetic (each
+// thread keeps tens of independent loads in flight); the y-neighbours come
+// from the adjacent lanes by shuffle, the segment's edge lanes forming theirs.
+// Blocks of 256 threads (8 warps) stride over the items (strip x segment).
+constexpr int kStripRows = 8;
+constexpr int kStripThreads = 256;
+
+inline int strip_items(const Geo& g) { return ((g.ny + 31) / 32) * ((g.nx + kStripRows - 1) / kStripRows); }
+inline int strip_grid(const Geo& g) {
+  const int b = (strip_items(g) + kStripThreads / 32 - 1) / (kStripThreads / 32);
+  return b < kMaxRedBlocks ? (b < 1 ? 1 : b) : kMaxRedBlocks;
+}
+
+// op(k, i, j): the operand at cell (i, j) (issues its loads); load(u, c): the
+// per-cell loads of body row u; body(u, c, i, j, centre, west, east, south, north).
+// STENCIL = false: no operand (pointwise kernels).  Neighbours off the grid are
+// wrapped on periodic axes and 0 otherwise (their face flags are clear).
+template <bool STENCIL, class Op, class Load, class Body>
+__device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body body) {
+  constexpr int RS = kStripRows;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  const int nx = g.nx, ny = g.ny;
+  const int segs = (ny + 31) / 32;
+  const int items = segs * ((nx + RS - 1) / RS);
+  const int wpb = (int)(blockDim.x >> 5);
+  for (int it = (int)blockIdx.x * wpb + warp; it < items; it += (int)gridDim.x * wpb) {
+    const int strip = it / segs, seg = it - strip * segs;
+    const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
+    const bool jv = j < ny;
+    double ov[STENCIL ? RS + 2 : 1];
+    double es[STENCIL ? RS : 1], en[STENCIL ? RS : 1];
+    if (STENCIL) {
+#pragma unroll
+      for (int u = 0; u < RS + 2; ++u) {
+        int r = i0 - 1 + u;
+        if (r < 0) r = g.periodic_x ? nx - 1 : -1;
+        else if (r >= nx) r = (r == nx && g.periodic_x) ? 0 : -1;
+        ov[u] = (jv && r >= 0) ? op(r * ny + j, r, j) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      const int i = i0 + u;
+      if (jv && i < nx) load(u, i * ny + j);
+    }
+    const int last = min(31, ny - 1 - j0);
+    if (STENCIL) {
+      if (lane == 0) {
+        const int js = j0 > 0 ? j0 - 1 : (g.periodic_y ? ny - 1 : -1);
+#pragma unroll
+        for (int u = 0; u < RS; ++u) {
+          const int i = i0 + u;
+          es[u] = (js >= 0 && i < nx) ? op(i * ny + js, i, js) : 0.0;
+        }
+      }
+      if (lane == last) {
+        const int jn = j + 1 < ny ? j + 1 : (g.periodic_y ? 0 : -1);
+#pragma unroll
+        for (int u = 0; u < RS; ++u) {
+          const int i = i0 + u;
+          en[u] = (jn >= 0 && i < nx) ? op(i * ny + jn, i, jn) : 0.0;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      double c = 0.0, w = 0.0, e = 0.0, sv = 0.0, nv = 0.0;
+      if (STENCIL) {
+        c = ov[u + 1];
+        w = ov[u];
+        e = ov[u + 2];
+        sv = __shfl_up_sync(0xffffffffu, c, 1);
+        nv = __shfl_down_sync(0xffffffffu, c, 1);
+        if (lane == 0) sv = es[u];
+        if (lane == last) nv = en[u];
+      }
+      const int i = i0 + u;
+      if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
+    }
+  }
+}
+
+// (A x) at a cell from its value and its neighbours', fine_apply's terms in its
+// order (diagonal, west, east, south, north).
+__device__ __forceinline__ double fine_apply5(uint8_t f, int i, int j, const Geo& g, double c, double w, double e,
+                                              double s, double n) {
+  double acc = fine_diag(f, i, j, g) * c;
+  if (f & F_W) acc += g.cx * w;
+  if (f & F_E) acc += g.cx * e;
+  if (f & F_S) acc += g.cy * s;
+  if (f & F_N) acc += g.cy * n;
+  return acc;
+}
+
 constexpr int kCellTJ = 32, kCellTI = 8;
 
 // 2D launch shape over nx x ny cells with at most kMaxRedBlocks blocks.

@@ -314,13 +314,13 @@ __global__ void k_fine_pre(B bf, const uint8_t* __restrict__ flags, Geo g, doubl
   auto xv = [&](int k, int ii, int jj) -> double {
     return (double)(T)(fine_wdinv(flags[k], ii, jj, g, w) * bf(k));
   };
-  FOR_CELLS(g) {
-    const int c = i * g.ny + j;
-    const uint8_t f = flags[c];
-    const double xc = xv(c, i, j);
-    x[c] = (T)xc;
-    res[c] = (T)(bf(c) - fine_apply<double>(f, i, j, c, g, xv));
-  }
+  uint8_t fv[kStripRows];
+  double bv[kStripRows];
+  strip_cells<true>(g, xv, [&](int u, int c) { fv[u] = flags[c]; bv[u] = bf(c); },
+                    [&](int u, int c, int i, int j, double xc, double xw, double xe, double xs, double xn) {
+                      x[c] = (T)xc;
+                      res[c] = (T)(bv[u] - fine_apply5(fv[u], i, j, g, xc, xw, xe, xs, xn));
+                    });
 }
 
 // xo = x + wd*(b - A x) on level 0.  MODE 0: plain; MODE 1: last sweep of the
@@ -336,17 +336,24 @@ __global__ void k_fine_smooth(B bf, const uint8_t* __restrict__ flags, Geo g, do
   bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
   double acc[2] = {0, 0};
-  FOR_CELLS(g) {
-    const int c = i * g.ny + j;
-    const uint8_t f = flags[c];
-    const double xn = (double)(T)((double)x[c] + fine_wdinv(f, i, j, g, w) *
-                                  (bf(c) - fine_apply<double>(f, i, j, c, g, xv)));
-    xo[c] = (T)xn;
-    if (MODE != 0 && (f & F_SOLV)) {
-      acc[0] += xn;
-      if (MODE == 1) acc[1] += (double)rcg[c] * xn;
-    }
-  }
+  uint8_t fv[kStripRows];
+  double bv[kStripRows], rv[kStripRows];
+  strip_cells<true>(g, xv,
+                    [&](int u, int c) {
+                      fv[u] = flags[c];
+                      bv[u] = bf(c);
+                      if (MODE == 1) rv[u] = (double)rcg[c];
+                    },
+                    [&](int u, int c, int i, int j, double xc, double xw, double xe, double xs, double xn_) {
+                      const uint8_t f = fv[u];
+                      const double xn = (double)(T)(xc + fine_wdinv(f, i, j, g, w) *
+                                                    (bv[u] - fine_apply5(f, i, j, g, xc, xw, xe, xs, xn_)));
+                      xo[c] = (T)xn;
+                      if (MODE != 0 && (f & F_SOLV)) {
+                        acc[0] += xn;
+                        if (MODE == 1) acc[1] += rv[u] * xn;
+                      }
+                    });
   if (MODE == 0) return;
   grid_reduce<2>(acc, rb, [&](double* t) {
     const double m = (singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
@@ -367,10 +374,12 @@ __global__ void k_fine_resid(B bf, const uint8_t* __restrict__ flags, Geo g,
   pdl_begin();
   bf.load();
   auto xv = [&](int k, int, int) -> double { return (double)x[k]; };
-  FOR_CELLS(g) {
-    const int c = i * g.ny + j;
-    res[c] = (T)(bf(c) - fine_apply<double>(flags[c], i, j, c, g, xv));
-  }
+  uint8_t fv[kStripRows];
+  double bv[kStripRows];
+  strip_cells<true>(g, xv, [&](int u, int c) { fv[u] = flags[c]; bv[u] = bf(c); },
+                    [&](int u, int c, int i, int j, double xc, double xw, double xe, double xs, double xn) {
+                      res[c] = (T)(bv[u] - fine_apply5(fv[u], i, j, g, xc, xw, xe, xs, xn));
+                    });
 }
 
 // x = wd*b on level 0 (first sweep from zero when more sweeps follow).

@@ -105,15 +105,14 @@ __global__ void k_cg_pq(const T* __restrict__ r, const T* __restrict__ zraw,
     return (double)(T)((double)p_old[k] * beta + z);
   };
   double acc[1] = {0.0};
-  FOR_CELLS(g) {
-    const int c = i * g.ny + j;
-    const uint8_t f = flags[c];
-    const double pc = pval(c, i, j);
-    const double qc = fine_apply<double>(f, i, j, c, g, pval);
-    p_new[c] = (T)pc;
-    q[c] = (T)qc;
-    acc[0] += pc * qc;
-  }
+  uint8_t fv[kStripRows];
+  strip_cells<true>(g, pval, [&](int u, int c) { fv[u] = flags[c]; },
+                    [&](int u, int c, int i, int j, double pc, double pw, double pe, double ps, double pn) {
+                      const double qc = fine_apply5(fv[u], i, j, g, pc, pw, pe, ps, pn);
+                      p_new[c] = (T)pc;
+                      q[c] = (T)qc;
+                      acc[0] += pc * qc;
+                    });
   grid_reduce<1>(acc, rb, [&](double* t) {
     S[S_PQ] = t[0];
     S[S_ALPHA] = S[S_RHO] / t[0];
@@ -132,19 +131,28 @@ __global__ void k_cg_xr(T* __restrict__ x, T* __restrict__ r, const T* __restric
   pdl_begin();
   const double alpha = S[S_ALPHA];
   double acc[3] = {0, 0, 0};
-  FOR_CELLS(g) {
-    const int c = i * g.ny + j;
-    const uint8_t f = flags[c];
-    const T pc = p[c];
-    const double xc = (double)x[c] + alpha * (double)pc;
-    const double rc = (double)(T)((double)r[c] - alpha * (double)q[c]);
-    if (p_keep) p_keep[c] = pc;
-    x[c] = (T)xc;
-    r[c] = (T)rc;
-    acc[0] += rc * rc;
-    if (PC == PC_JACOBI) acc[1] += rc * (rc / fine_diag(f, i, j, g));
-    if (f & F_SOLV) acc[2] += rc;
-  }
+  T pv[kStripRows], xv[kStripRows], rv[kStripRows], qv[kStripRows];
+  uint8_t fv[kStripRows];
+  strip_cells<false>(
+      g, [](int, int, int) { return 0.0; },
+      [&](int u, int c) {
+        pv[u] = p[c];
+        xv[u] = x[c];
+        rv[u] = r[c];
+        qv[u] = q[c];
+        fv[u] = flags[c];
+      },
+      [&](int u, int c, int i, int j, double, double, double, double, double) {
+        const T pc = pv[u];
+        const double xc = (double)xv[u] + alpha * (double)pc;
+        const double rc = (double)(T)((double)rv[u] - alpha * (double)qv[u]);
+        if (p_keep) p_keep[c] = pc;
+        x[c] = (T)xc;
+        r[c] = (T)rc;
+        acc[0] += rc * rc;
+        if (PC == PC_JACOBI) acc[1] += rc * (rc / fine_diag(fv[u], i, j, g));
+        if (fv[u] & F_SOLV) acc[2] += rc;
+      });
   grid_reduce<3>(acc, rb, [&](double* t) {
     const int it = I[I_IT] + 1;
     I[I_IT] = it;

@@ -501,7 +501,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
                                        P1.view(), bf0, s->flags, g, w0, xc, B0.xa)));
     CHECK_LAUNCH();
     prof_mark(s, 2, stream);
-    pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0,
+    pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, w0,
                (const T*)B0.xa, z_out, r, s->singular, s->S, s->rb());
     prof_mark(s, 2, stream);
     CHECK_LAUNCH();
@@ -511,7 +511,7 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
   T* cur[32];
   if (sw == 1) {
     prof_mark(s, 3, stream);
-    pdl_launch(s, k_fine_pre<T, BFromRS<T>>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, B0.xa, B0.res);
+    pdl_launch(s, k_fine_pre<T, BFromRS<T>>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, w0, B0.xa, B0.res);
     prof_mark(s, 3, stream);
     CHECK_LAUNCH();
     cur[0] = B0.xa;
@@ -521,12 +521,12 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
     T* a = B0.xa;
     T* bb = B0.xb;
     for (int k = 1; k < sw; ++k) {
-      pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, a, bb, r,
+      pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, w0, a, bb, r,
                                                                       s->singular, s->S, s->rb());
       CHECK_LAUNCH();
       std::swap(a, bb);
     }
-    pdl_launch(s, k_fine_resid<T, BFromRS<T>>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, a, B0.res);
+    pdl_launch(s, k_fine_resid<T, BFromRS<T>>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, a, B0.res);
     CHECK_LAUNCH();
     cur[0] = a;
   }
@@ -591,12 +591,12 @@ int vcycle_pcg(pycfd_solver* s, const T* r, T* z_out, cudaStream_t stream) {
         if (k == sw)
           {
             prof_mark(s, 2, stream);
-            pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, xf, dst, r,
+            pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 1>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, w0, xf, dst, r,
                                                                           s->singular, s->S, s->rb());
             prof_mark(s, 2, stream);
           }
         else
-          pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, s->cgrid, s->cblock, 0, stream, bf0, s->flags, g, w0, xf, dst, r,
+          pdl_launch(s, k_fine_smooth<T, BFromRS<T>, 0>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf0, s->flags, g, w0, xf, dst, r,
                                                                           s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         other = xf;
@@ -634,12 +634,12 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
   double* a = x;
   double* t = s->xtmp;
   for (int k = 0; k < sw; ++k) {
-    pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, a, t, nullptr,
+    pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf, s->flags, g, w0, a, t, nullptr,
                                                                              s->singular, s->S, s->rb());
     CHECK_LAUNCH();
     std::swap(a, t);
   }
-  pdl_launch(s, k_fine_resid<double, BStored<double>>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, a, B0.res);
+  pdl_launch(s, k_fine_resid<double, BStored<double>>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf, s->flags, g, a, B0.res);
   CHECK_LAUNCH();
   double* cur[32];
   cur[0] = a;
@@ -679,10 +679,10 @@ int vcycle_standalone(pycfd_solver* s, double* b, double* x, cudaStream_t stream
       double* o = (xf == x) ? s->xtmp : x;
       for (int k = 1; k <= sw; ++k) {
         if (k == sw)
-          pdl_launch(s, k_fine_smooth<double, BStored<double>, 2>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
+          pdl_launch(s, k_fine_smooth<double, BStored<double>, 2>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         else
-          pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, s->cgrid, s->cblock, 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
+          pdl_launch(s, k_fine_smooth<double, BStored<double>, 0>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, stream, bf, s->flags, g, w0, xf, o, nullptr,
                                                                                    s->singular, s->S, s->rb());
         CHECK_LAUNCH();
         std::swap(xf, o);
@@ -775,10 +775,10 @@ int solve_mixed(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream) {
   CHECK_LAUNCH();
   auto inner_pass = [&](cudaStream_t st) -> int {
     TRY(vcycle_pcg<float>(s, s->r32, s->z32, st));
-    pdl_launch(s, k_cg_pq<float, PC_MG>, s->cgrid, s->cblock, 0, st, s->r32, s->z32, s->pa32, s->pb32, s->q32, s->flags,
+    pdl_launch(s, k_cg_pq<float, PC_MG>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, s->r32, s->z32, s->pa32, s->pb32, s->q32, s->flags,
                                                           g, s->S, s->I, s->rb());
     CHECK_LAUNCH();
-    pdl_launch(s, k_cg_xr<float, PC_MG>, s->cgrid, s->cblock, 0, st, s->x32, s->r32, s->pb32, s->q32, s->pa32, s->flags,
+    pdl_launch(s, k_cg_xr<float, PC_MG>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, s->x32, s->r32, s->pb32, s->q32, s->pa32, s->flags,
                                                           g, icfg, s->S, s->I, s->rb(), inner.ctl);
     CHECK_LAUNCH();
     return 0;
@@ -934,19 +934,19 @@ int solve_prepared(pycfd_solver* s, double* x, bool has_x0, cudaStream_t stream)
     // one pass of the recurrence on stream `st`; p_old -> p_new
     auto pass = [&](cudaStream_t st, double* p_old, double* p_new, double* keep) -> int {
       if (kind == PCFD_SOLVER_CG) {
-        pdl_launch(s, k_cg_pq<double, PC_JACOBI>, s->cgrid, s->cblock, 0, st, s->r, nullptr, p_old, p_new, s->q, s->flags,
+        pdl_launch(s, k_cg_pq<double, PC_JACOBI>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, s->r, nullptr, p_old, p_new, s->q, s->flags,
                                                               g, s->S, s->I, s->rb());
         CHECK_LAUNCH();
-        pdl_launch(s, k_cg_xr<double, PC_JACOBI>, s->cgrid, s->cblock, 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+        pdl_launch(s, k_cg_xr<double, PC_JACOBI>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
                                                               s->S, s->I, s->rb(), L.ctl);
       } else {
         TRY(vcycle_pcg<double>(s, s->r, s->z, st));
         prof_mark(s, 1, st);
-        pdl_launch(s, k_cg_pq<double, PC_MG>, s->cgrid, s->cblock, 0, st, s->r, s->z, p_old, p_new, s->q, s->flags, g,
+        pdl_launch(s, k_cg_pq<double, PC_MG>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, s->r, s->z, p_old, p_new, s->q, s->flags, g,
                                                           s->S, s->I, s->rb());
         prof_mark(s, 1, st);
         CHECK_LAUNCH();
-        pdl_launch(s, k_cg_xr<double, PC_MG>, s->cgrid, s->cblock, 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
+        pdl_launch(s, k_cg_xr<double, PC_MG>, dim3(strip_grid(s->g)), dim3(kStripThreads), 0, st, x, s->r, p_new, s->q, keep, s->flags, g, cfg,
                                                           s->S, s->I, s->rb(), L.ctl);
       }
       CHECK_LAUNCH();
