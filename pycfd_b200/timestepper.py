@@ -205,6 +205,8 @@ class TimeStepper:
                     outs.append(cur)
                 rows, frozen = s.read_history()
                 done = len(rows)
+                if done == 0 and frozen == 0:
+                    raise RuntimeError("the device run loop took no step and reported no stop reason")
                 if done:
                     cur = outs[done - 1]
                     fields = FlowField(self.mesh, cur.u, cur.v, cur.p, float(rows[-1][1]),

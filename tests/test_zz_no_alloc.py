@@ -83,7 +83,7 @@ def test_noalloc_reduction_wide_grid_without_optional_inputs():
     walls = {w: BCSpec(BCKind.NO_SLIP) for w in ("left", "right", "bottom")}
     walls["top"] = BCSpec(BCKind.MOVING_WALL, velocity=1.0)
     cfg = SimulationConfig(nx=nx, ny=6, lx=float(nx) / 6.0, ly=1.0, re=100.0,
-                           pressure_solver="cg", poisson_tol=1e-8, boundary_config=walls, name="wide")
+                           pressure_solver="mgcg", poisson_tol=1e-8, boundary_config=walls, name="wide")
     s = ProjectionSolver(cfg)
     f1 = s.step(s.initialize(), 1e-3)
     f2 = s.step(f1, 1e-3)
