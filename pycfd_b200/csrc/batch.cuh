@@ -68,6 +68,7 @@ struct BProb {
   int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
   int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
   int s_segs, s_items, s_chunks;         // warp strips of the solver kernels (b_strips)
+  int p_chunks;                          // warp-strip chunks of the predictor (ghosted arrays)
   int red_base;                          // first partial row of this problem
   const uint8_t* flags;
   const uint8_t* solid;
@@ -462,36 +463,68 @@ __global__ void k_b_set_dt(const BProb<T>* __restrict__ probs, int nprob, double
 // ---- stencils ----------------------------------------------------------------
 // Predictor of one Runge-Kutta stage: out = U + dt*rhs on the solvable faces,
 // U elsewhere, U = ca*a + cb*b (b absent: U = a) (pycfd/core/solver.py:619-622).
+// Warp strips over the ghosted arrays: a warp loads 32 adjacent columns of
+// kBStripRows + 2 rows of u and of v (the stage input formed on the fly) into
+// registers and writes the 30 inner columns -- the outer two lanes only carry
+// the halo, so every neighbour comes from a register or a shuffle.  The RHS is
+// rhs_u_core / rhs_v_core, the single-problem predictor's arithmetic.
+constexpr int kBPredCols = 30;   // output columns per warp segment (32 lanes, one halo lane each side)
+
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, int src_a,
                                                             int src_b, double ca, double cb, int dst,
                                                             BShared sh) {
+  constexpr int RS = kBStripRows;
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
-  const Geo& g = P.g;
+  const Geo g = P.g;
   const int nx = g.nx, ny = g.ny;
+  const long W = ny + 2, WV = ny + 3;
   const StageIn u{b_arr_u(P, src_a), src_b >= 0 ? b_arr_u(P, src_b) : nullptr, ca, cb};
   const StageIn v{b_arr_v(P, src_a), src_b >= 0 ? b_arr_v(P, src_b) : nullptr, ca, cb};
-  double* us = b_arr_u(P, dst);
-  double* vs = b_arr_v(P, dst);
+  double* __restrict__ us = b_arr_u(P, dst);
+  double* __restrict__ vs = b_arr_v(P, dst);
   const double dt = P.S[S_DT], blend = P.S[S_BLEND];
-  B_CHUNK_TILES(P, e.y) {
-    B_TILE_EXT(P, tile_, nx + 3, ny + 3) {
-      if (j < ny + 2) {
-        const long k = (long)i * (ny + 2) + j;
-        double val = u[k];
-        if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-          val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
-        us[k] = val;
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  const int segs = (ny + 3 + kBPredCols - 1) / kBPredCols;
+  const int items = segs * ((nx + 3 + RS - 1) / RS);
+  const int it1 = min(items, (e.y + 1) * kBStripItems);
+  for (int it = e.y * kBStripItems + warp; it < it1; it += kBThreads / 32) {
+    const int strip = it / segs, seg = it - strip * segs;
+    const int i0 = strip * RS, j = seg * kBPredCols - 1 + lane;
+    const bool ju = j >= 0 && j < ny + 2, jv = j >= 0 && j < ny + 3;
+    double U[RS + 2], V[RS + 2];
+#pragma unroll
+    for (int r = 0; r < RS + 2; ++r) {
+      const int row = i0 - 1 + r;
+      U[r] = (ju && row >= 0 && row < nx + 3) ? u[(long)row * W + j] : 0.0;
+      V[r] = (jv && row >= 0 && row < nx + 2) ? v[(long)row * WV + j] : 0.0;
+    }
+    const bool out = lane >= 1 && lane <= kBPredCols;
+#pragma unroll
+    for (int q = 0; q < RS; ++q) {
+      const int m = i0 + q;
+      const double un = __shfl_down_sync(0xffffffffu, U[q + 1], 1);
+      const double usv = __shfl_up_sync(0xffffffffu, U[q + 1], 1);
+      const double us2 = __shfl_up_sync(0xffffffffu, U[q + 2], 1);
+      const double vn0 = __shfl_down_sync(0xffffffffu, V[q], 1);
+      const double vn1 = __shfl_down_sync(0xffffffffu, V[q + 1], 1);
+      const double vsv = __shfl_up_sync(0xffffffffu, V[q + 1], 1);
+      if (out && ju && m < nx + 3) {
+        double val = U[q + 1];
+        if (m >= g.u_lo && m < g.u_hi && j >= 1 && j <= ny)
+          val = val + dt * rhs_u_core(U[q + 1], U[q + 2], U[q], un, usv, vn0, vn1, V[q], V[q + 1], g.dx, g.dy,
+                                      g.nu, blend, g.fx);
+        us[(long)m * W + j] = val;
       }
-      if (i < nx + 2) {
-        const long k = (long)i * (ny + 3) + j;
-        double val = v[k];
-        if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-          val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
-        vs[k] = val;
+      if (out && jv && m < nx + 2) {
+        double val = V[q + 1];
+        if (m >= 1 && m <= nx && j >= g.v_lo && j < g.v_hi)
+          val = val + dt * rhs_v_core(V[q + 1], vn1, vsv, V[q + 2], V[q], us2, U[q + 2], usv, U[q + 1], g.dx,
+                                      g.dy, g.nu, blend, g.fy);
+        vs[(long)m * WV + j] = val;
       }
     }
   }
@@ -527,6 +560,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_boundary(const BProb<T>* __rest
 
 // Poisson right-hand side b = div(u*)/dt + Dirichlet terms on solvable rows and
 // its fluid mean (pycfd/core/solver.py:659-661, pycfd/core/pressure.py:300-308).
+// Warp strips: the four face values of each of a thread's cells loaded first.
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int arr,
@@ -534,26 +568,38 @@ __global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restr
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
-  const Geo& g = P.g;
-  const double* u = b_arr_u(P, arr);
-  const double* v = b_arr_v(P, arr);
+  B_VIEW(V, P);
+  const Geo& g = V.g;
+  const long W = g.ny + 2, WV = g.ny + 3;
+  const double* __restrict__ u = b_arr_u(P, arr);
+  const double* __restrict__ v = b_arr_v(P, arr);
+  const uint8_t* __restrict__ flags = P.flags;
+  double* __restrict__ b = P.b;
   const double dt = P.S[S_DT];
   double acc[1] = {0.0};
-  {
-    B_CHUNK_TILES(P, e.y) {
-      B_TILE_CELLS(P, tile_) {
-        const int c = i * g.ny + j;
-        const uint8_t f = P.flags[c];
+  uint8_t fv[kBStripRows];
+  double ue[kBStripRows], uw[kBStripRows], vn[kBStripRows], vs[kBStripRows];
+  b_strips<false, double>(
+      V, e.y, [](int, int, int) { return 0.0; },
+      [&](int q, int c) {
+        const int i = c / g.ny, j = c - i * g.ny;
+        fv[q] = flags[c];
+        ue[q] = u[(long)(i + 2) * W + j + 1];
+        uw[q] = u[(long)(i + 1) * W + j + 1];
+        vn[q] = v[(long)(i + 1) * WV + j + 2];
+        vs[q] = v[(long)(i + 1) * WV + j + 1];
+      },
+      [&](int q, int c, int i, int j, double, double, double, double, double) {
+        const uint8_t f = fv[q];
         double val = 0.0;
         if (f & F_SOLV) {
-          val = (cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt) * 1.0 + fine_bc(f, i, j, g);
+          const double div = (ue[q] - uw[q]) / g.dx + (vn[q] - vs[q]) / g.dy;   // cell_div's expression
+          val = (div / dt) * 1.0 + fine_bc(f, i, j, g);
           acc[0] += val;
         }
-        P.b[c] = val;
-      }
-    }
-  }
-  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks,
+        b[c] = val;
+      });
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks,
               [&](double* t) { P.S[S_MEAN_B] = g.n_fluid ? t[0] / g.n_fluid : 0.0; });
 }
 
@@ -625,26 +671,34 @@ __global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __rest
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_frozen(sh, e.x)) {
-    const Geo& g = P.g;
+    B_VIEW(V, P);
+    const Geo& g = V.g;
     const double mean = P.singular ? P.S[S_MEAN_B] : 0.0;
+    const uint8_t* __restrict__ flags = P.flags;
+    const T* __restrict__ xs = P.xs;
+    double* __restrict__ b = P.b;
+    T* __restrict__ r = P.r;
     double acc[3] = {0, 0, 0};
-    {
-      B_CHUNK_TILES(P, e.y) {
-        B_TILE_CELLS(P, tile_) {
-          const int c = i * g.ny + j;
-          const uint8_t f = P.flags[c];
-          const double bc = (f & F_SOLV) ? P.b[c] - mean : 0.0;
-          P.b[c] = bc;
-          const double ax = b_apply<double>(P, f, i, j, c, [&](int k, int, int) { return (double)P.xs[k]; });
+    uint8_t fv[kBStripRows];
+    double bv[kBStripRows];
+    b_strips<true, double>(
+        V, e.y, [&](int k, int, int) { return (double)xs[k]; },
+        [&](int q, int c) {
+          fv[q] = flags[c];
+          bv[q] = b[c];
+        },
+        [&](int q, int c, int i, int j, double xc, double xw, double xe, double xsv, double xn) {
+          const uint8_t f = fv[q];
+          const double bc = (f & F_SOLV) ? bv[q] - mean : 0.0;
+          b[c] = bc;
+          const double ax = b_apply5<double>(V, f, i, j, xc, xw, xe, xsv, xn);
           const double rc = bc - ax;
-          P.r[c] = (T)rc;
+          r[c] = (T)rc;
           acc[0] += bc * bc;
           acc[1] += rc * rc;
           if (f & F_SOLV) acc[2] += rc;
-        }
-      }
-    }
-    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+        });
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       S[S_BNORM2] = t[0];
@@ -777,23 +831,28 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
-  const Geo& g = P.g;
+  B_VIEW(V, P);
+  const Geo& g = V.g;
   const bool zero = P.I[I_ZERO_RHS] != 0;
-  const double* x = P.x;
-  auto xv = [&](int k, int, int) -> double { return zero ? 0.0 : x[k]; };
+  const double* __restrict__ x = P.x;
+  const double* __restrict__ b = P.b;
+  const uint8_t* __restrict__ flags = P.flags;
   double acc[2] = {0, 0};
-  {
-    B_CHUNK_TILES(P, e.y) {
-      B_TILE_CELLS(P, tile_) {
-        const int c = i * g.ny + j;
-        const uint8_t f = P.flags[c];
-        const double rc = P.b[c] - b_apply<double>(P, f, i, j, c, xv);
+  uint8_t fv[kBStripRows];
+  double bv[kBStripRows];
+  b_strips<true, double>(
+      V, e.y, [&](int k, int, int) { return zero ? 0.0 : x[k]; },
+      [&](int q, int c) {
+        fv[q] = flags[c];
+        bv[q] = b[c];
+      },
+      [&](int q, int, int i, int j, double xc, double xw, double xe, double xsv, double xn) {
+        const uint8_t f = fv[q];
+        const double rc = bv[q] - b_apply5<double>(V, f, i, j, xc, xw, xe, xsv, xn);
         acc[0] += rc * rc;
-        if (f & F_SOLV) acc[1] += xv(c, i, j);
-      }
-    }
-  }
-  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+        if (f & F_SOLV) acc[1] += xc;
+      });
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
     double* S = P.S;
     const double nb = sqrt(S[S_BNORM2]);
     S[S_RESID] = sqrt(t[0]) / (nb > 1e-300 ? nb : 1.0);
@@ -809,14 +868,22 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_apply(const BProb<T>* __
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
+  B_VIEW(V, P);
   const bool zero = P.I[I_ZERO_RHS] != 0;
   const double m = P.S[S_MEAN_X];
-  B_CHUNK_TILES(P, e.y) {
-    B_TILE_CELLS(P, tile_) {
-      const int c = i * P.g.ny + j;
-      P.x[c] = (!zero && (P.flags[c] & F_SOLV)) ? P.x[c] - m : 0.0;
-    }
-  }
+  double* __restrict__ x = P.x;
+  const uint8_t* __restrict__ flags = P.flags;
+  uint8_t fv[kBStripRows];
+  double xv[kBStripRows];
+  b_strips<false, double>(
+      V, e.y, [](int, int, int) { return 0.0; },
+      [&](int q, int c) {
+        fv[q] = flags[c];
+        xv[q] = x[c];
+      },
+      [&](int q, int c, int, int, double, double, double, double, double) {
+        x[c] = (!zero && (fv[q] & F_SOLV)) ? xv[q] - m : 0.0;
+      });
 }
 
 // ---- mixed form: FP64 iterative refinement around the FP32 MG-PCG -----------
@@ -831,29 +898,38 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __r
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_frozen(sh, e.x) && (first || !P.I[I_IR_DONE])) {
-    const Geo& g = P.g;
+    B_VIEW(V, P);
+    const Geo& g = V.g;
     const double mean = (first && P.singular) ? P.S[S_MEAN_B] : 0.0;
+    const uint8_t* __restrict__ flags = P.flags;
+    const double* __restrict__ x = P.x;
+    double* __restrict__ b = P.b;
+    T* __restrict__ r = P.r;
+    T* __restrict__ xs = P.xs;
     double acc[3] = {0, 0, 0};
-    {
-      B_CHUNK_TILES(P, e.y) {
-        B_TILE_CELLS(P, tile_) {
-          const int c = i * g.ny + j;
-          const uint8_t f = P.flags[c];
-          double bc = P.b[c];
+    uint8_t fv[kBStripRows];
+    double bv[kBStripRows];
+    b_strips<true, double>(
+        V, e.y, [&](int k, int, int) { return x[k]; },
+        [&](int q, int c) {
+          fv[q] = flags[c];
+          bv[q] = b[c];
+        },
+        [&](int q, int c, int i, int j, double xc, double xw, double xe, double xsv, double xn) {
+          const uint8_t f = fv[q];
+          double bc = bv[q];
           if (first) {
             bc = (f & F_SOLV) ? bc - mean : 0.0;
-            P.b[c] = bc;
+            b[c] = bc;
           }
-          const double rc = bc - b_apply<double>(P, f, i, j, c, [&](int k, int, int) { return P.x[k]; });
-          P.r[c] = (T)rc;
-          P.xs[c] = (T)0;
+          const double rc = bc - b_apply5<double>(V, f, i, j, xc, xw, xe, xsv, xn);
+          r[c] = (T)rc;
+          xs[c] = (T)0;
           acc[0] += rc * rc;
           if (f & F_SOLV) acc[1] += (double)(T)rc;
           if (first) acc[2] += bc * bc;
-        }
-      }
-    }
-    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.chunks, [&](double* t) {
+        });
+    b_reduce<3>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       if (first) {
@@ -904,15 +980,24 @@ __global__ void __launch_bounds__(kBThreads) k_b_ir_update(const BProb<T>* __res
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x) || P.I[I_IR_DONE]) return;
-  {
-    B_CHUNK_TILES(P, e.y) {
-      B_TILE_CELLS(P, tile_) {
-        const int c = i * P.g.ny + j;
-        if (P.flags[c] & F_SOLV) P.x[c] = P.x[c] + (double)P.xs[c];
-      }
-    }
-  }
-  if (e.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) P.I[I_IR_IT] += 1;
+  B_VIEW(V, P);
+  double* __restrict__ x = P.x;
+  const T* __restrict__ xs = P.xs;
+  const uint8_t* __restrict__ flags = P.flags;
+  uint8_t fv[kBStripRows];
+  double xv[kBStripRows];
+  T ev[kBStripRows];
+  b_strips<false, double>(
+      V, e.y, [](int, int, int) { return 0.0; },
+      [&](int q, int c) {
+        fv[q] = flags[c];
+        xv[q] = x[c];
+        ev[q] = xs[c];
+      },
+      [&](int q, int c, int, int, double, double, double, double, double) {
+        if (fv[q] & F_SOLV) x[c] = xv[q] + (double)ev[q];
+      });
+  if (e.y == 0 && threadIdx.x == 0) P.I[I_IR_IT] += 1;
 }
 
 // ---- V-cycle ---------------------------------------------------------------------

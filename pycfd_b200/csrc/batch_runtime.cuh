@@ -33,6 +33,7 @@ struct pycfd_batch {
   int depth = 0;                           // most levels of any problem
   BMapHost fine;                           // every chunk of tiles of every problem
   BMapHost strip;                          // every chunk of warp strips of every problem (solver kernels)
+  BMapHost pstrip;                         // every chunk of predictor strips of every problem
   // row-block maps per depth d (problems whose level d runs per level):
   // grouped maps per depth d, entries (structure, row block x 64 + group of kBGroup problems):
   std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
@@ -173,7 +174,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 
   // per-problem records
   std::vector<BProb<T>> pr(n);
-  std::vector<int2> fine, strip;
+  std::vector<int2> fine, strip, pstrip;
   B->nlev.assign(n, 0);
   B->depth = 0;
   int red_rows = 0;
@@ -201,6 +202,11 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.s_segs = (s->g.ny + 31) / 32;
     P.s_items = ((s->g.nx + kBStripRows - 1) / kBStripRows) * P.s_segs;
     P.s_chunks = (P.s_items + kBStripItems - 1) / kBStripItems;
+    {
+      const int segs = (s->g.ny + 3 + kBPredCols - 1) / kBPredCols;
+      const int items = segs * ((s->g.nx + 3 + kBStripRows - 1) / kBStripRows);
+      P.p_chunks = (items + kBStripItems - 1) / kBStripItems;
+    }
     P.red_base = red_rows;
     red_rows += std::max(P.chunks, P.s_chunks);
     P.flags = s->flags;
@@ -261,9 +267,11 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
     for (int c = 0; c < P.s_chunks; ++c) strip.push_back(make_int2(i, c));
+    for (int c = 0; c < P.p_chunks; ++c) pstrip.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
   TRY(upload_map(B, &B->strip, strip));
+  TRY(upload_map(B, &B->pstrip, pstrip));
   // problems grouped by structure (the dense tail's block groups)
   {
     std::vector<int> sp;
@@ -579,7 +587,7 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
   const BProb<T>* P = probs_of<T>(B);
   LoopCtl ctl{0, 0};
   if (B->capturing) TRY(b_loop_handle(st, nullptr, &ctl));
-  BLAUNCH(k_b_rhs_init<T>, B->fine.n, kBFineBlock, 0, st, P, B->n, B->fine.e, B->tol, B->maxiter, B->sh, ctl);
+  BLAUNCH(k_b_rhs_init<T>, B->strip.n, kBThreads, 0, st, P, B->n, B->strip.e, B->tol, B->maxiter, B->sh, ctl);
   auto pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
     b_prof(B, 1, s2);
@@ -604,8 +612,8 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
       TRY(pass(st));
     }
   }
-  BLAUNCH(k_b_finish_stats<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->tol, B->sh);
-  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->sh);
+  BLAUNCH(k_b_finish_stats<T>, B->strip.n, kBThreads, 0, st, P, B->strip.e, B->tol, B->sh);
+  BLAUNCH(k_b_finish_apply<T>, B->strip.n, kBThreads, 0, st, P, B->strip.e, B->sh);
   return 0;
 }
 
@@ -615,7 +623,7 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
   const BProb<T>* P = probs_of<T>(B);
   LoopCtl outer{0, 0}, inner{0, 0};
   if (B->capturing) TRY(b_loop_handle(st, nullptr, &outer));
-  BLAUNCH(k_b_ir_residual<T>, B->fine.n, kBFineBlock, 0, st, P, B->n, B->fine.e, B->tol, B->inner_tol,
+  BLAUNCH(k_b_ir_residual<T>, B->strip.n, kBThreads, 0, st, P, B->n, B->strip.e, B->tol, B->inner_tol,
           kIrMaxPassesB, 1, B->sh, outer);
   auto inner_pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
@@ -628,8 +636,8 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
     return 0;
   };
   auto refine = [&](cudaStream_t s2) -> int {
-    BLAUNCH(k_b_ir_update<T>, B->fine.n, kBFineBlock, 0, s2, P, B->fine.e, B->sh);
-    BLAUNCH(k_b_ir_residual<T>, B->fine.n, kBFineBlock, 0, s2, P, B->n, B->fine.e, B->tol, B->inner_tol,
+    BLAUNCH(k_b_ir_update<T>, B->strip.n, kBThreads, 0, s2, P, B->strip.e, B->sh);
+    BLAUNCH(k_b_ir_residual<T>, B->strip.n, kBThreads, 0, s2, P, B->n, B->strip.e, B->tol, B->inner_tol,
             kIrMaxPassesB, 0, B->sh, outer);
     return 0;
   };
@@ -662,8 +670,8 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
       TRY(refine(st));
     }
   }
-  BLAUNCH(k_b_finish_stats<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->tol, B->sh);
-  BLAUNCH(k_b_finish_apply<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, B->sh);
+  BLAUNCH(k_b_finish_stats<T>, B->strip.n, kBThreads, 0, st, P, B->strip.e, B->tol, B->sh);
+  BLAUNCH(k_b_finish_apply<T>, B->strip.n, kBThreads, 0, st, P, B->strip.e, B->sh);
   return 0;
 }
 
@@ -671,7 +679,7 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
 template <class T>
 int b_project(pycfd_batch* B, int arr, cudaStream_t st) {
   const BProb<T>* P = probs_of<T>(B);
-  BLAUNCH(k_b_div_rhs<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, arr, B->sh);
+  BLAUNCH(k_b_div_rhs<T>, B->strip.n, kBThreads, 0, st, P, B->strip.e, arr, B->sh);
   if (B->precision == PCFD_MIXED) TRY(b_solve_mixed(B, st));
   else TRY(b_solve_fp64(B, st));
   BLAUNCH(k_b_correct<T>, B->fine.n, kBFineBlock, 0, st, P, B->fine.e, arr, B->sh);
@@ -682,7 +690,7 @@ int b_project(pycfd_batch* B, int arr, cudaStream_t st) {
 template <class T>
 int b_substep(pycfd_batch* B, int a, int b, double ca, double cb, int dst, cudaStream_t st) {
   b_prof(B, 6, st);
-  BLAUNCH(k_b_predictor<T>, B->fine.n, kBFineBlock, 0, st, probs_of<T>(B), B->fine.e, a, b, ca, cb, dst, B->sh);
+  BLAUNCH(k_b_predictor<T>, B->pstrip.n, kBThreads, 0, st, probs_of<T>(B), B->pstrip.e, a, b, ca, cb, dst, B->sh);
   b_prof(B, 6, st);
   TRY(b_boundary<T>(B, dst, {OP_VEL_PRED, OP_MASS, OP_MASK_RESET, OP_WRAP_FACES}, 0, st));
   TRY(b_project<T>(B, dst, st));

@@ -24,23 +24,19 @@ struct StageIn {
   }
 };
 
-// u-momentum RHS at u-face (m, j), 1<=m<=nx+1, 1<=j<=ny
-// (pycfd/core/kernels.py:54-80).
-template <class U, class V>
-__device__ __forceinline__ double rhs_u_at(const U& u, const V& v, int m, int j, int ny,
-                                           double dx, double dy, double nu, double blend,
-                                           double fx) {
-  const long W = ny + 2, WV = ny + 3;
-  const double u0 = u[m * W + j];
-  const double ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
-  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+// u-momentum RHS at a u face from the values it reads (pycfd/core/kernels.py:54-80):
+// the face's own value, its east/west/north/south neighbours, and the four v faces
+// around it (v_tl = v[m-1, j+1], v_tr = v[m, j+1], v_bl = v[m-1, j], v_br = v[m, j]).
+__device__ __forceinline__ double rhs_u_core(double u0, double ue, double uw, double un, double us, double v_tl,
+                                             double v_tr, double v_bl, double v_br, double dx, double dy,
+                                             double nu, double blend, double fx) {
   const double u_right = 0.5 * (u0 + ue);
   const double u_left = 0.5 * (uw + u0);
   double duudx = (u_right * u_right - u_left * u_left) / dx;
   const double u_top = 0.5 * (u0 + un);
-  const double v_top = 0.5 * (v[(m - 1) * WV + j + 1] + v[m * WV + j + 1]);
+  const double v_top = 0.5 * (v_tl + v_tr);
   const double u_bot = 0.5 * (us + u0);
-  const double v_bot = 0.5 * (v[(m - 1) * WV + j] + v[m * WV + j]);
+  const double v_bot = 0.5 * (v_bl + v_br);
   double duvdy = (u_top * v_top - u_bot * v_bot) / dy;
   if (blend > 0.0) {
     duudx += blend / dx * (fabs(u_right) * (u0 - ue) * 0.5 - fabs(u_left) * (uw - u0) * 0.5);
@@ -50,22 +46,18 @@ __device__ __forceinline__ double rhs_u_at(const U& u, const V& v, int m, int j,
   return -(duudx + duvdy) + nu * lap + fx;
 }
 
-// v-momentum RHS at v-face (i, n), 1<=i<=nx, 1<=n<=ny+1
-// (pycfd/core/kernels.py:83-110).
-template <class U, class V>
-__device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n, int ny,
-                                           double dx, double dy, double nu, double blend,
-                                           double fy) {
-  const long W = ny + 2, WV = ny + 3;
-  const double v0 = v[i * WV + n];
-  const double vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
-  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+// v-momentum RHS at a v face from its values (pycfd/core/kernels.py:83-110): the
+// face, its north/south/east/west neighbours, and the four u faces around it
+// (u_rb = u[i+1, n-1], u_rt = u[i+1, n], u_lb = u[i, n-1], u_lt = u[i, n]).
+__device__ __forceinline__ double rhs_v_core(double v0, double vn, double vs, double ve, double vw, double u_rb,
+                                             double u_rt, double u_lb, double u_lt, double dx, double dy,
+                                             double nu, double blend, double fy) {
   const double v_top = 0.5 * (v0 + vn);
   const double v_bot = 0.5 * (vs + v0);
   double dvvdy = (v_top * v_top - v_bot * v_bot) / dy;
-  const double u_right = 0.5 * (u[(i + 1) * W + n - 1] + u[(i + 1) * W + n]);
+  const double u_right = 0.5 * (u_rb + u_rt);
   const double v_right = 0.5 * (v0 + ve);
-  const double u_left = 0.5 * (u[i * W + n - 1] + u[i * W + n]);
+  const double u_left = 0.5 * (u_lb + u_lt);
   const double v_left = 0.5 * (vw + v0);
   double duvdx = (u_right * v_right - u_left * v_left) / dx;
   if (blend > 0.0) {
@@ -74,6 +66,28 @@ __device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n,
   }
   const double lap = ((vw - 2.0 * v0 + ve) / (dx * dx) + (vs - 2.0 * v0 + vn) / (dy * dy));
   return -(duvdx + dvvdy) + nu * lap + fy;
+}
+
+// u-momentum RHS at u-face (m, j), 1<=m<=nx+1, 1<=j<=ny.
+template <class U, class V>
+__device__ __forceinline__ double rhs_u_at(const U& u, const V& v, int m, int j, int ny,
+                                           double dx, double dy, double nu, double blend,
+                                           double fx) {
+  const long W = ny + 2, WV = ny + 3;
+  return rhs_u_core(u[m * W + j], u[(m + 1) * W + j], u[(m - 1) * W + j], u[m * W + j + 1], u[m * W + j - 1],
+                    v[(m - 1) * WV + j + 1], v[m * WV + j + 1], v[(m - 1) * WV + j], v[m * WV + j], dx, dy, nu,
+                    blend, fx);
+}
+
+// v-momentum RHS at v-face (i, n), 1<=i<=nx, 1<=n<=ny+1.
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n, int ny,
+                                           double dx, double dy, double nu, double blend,
+                                           double fy) {
+  const long W = ny + 2, WV = ny + 3;
+  return rhs_v_core(v[i * WV + n], v[i * WV + n + 1], v[i * WV + n - 1], v[(i + 1) * WV + n], v[(i - 1) * WV + n],
+                    u[(i + 1) * W + n - 1], u[(i + 1) * W + n], u[i * W + n - 1], u[i * W + n], dx, dy, nu,
+                    blend, fy);
 }
 
 // ---- Smagorinsky large-eddy closure (pycfd/physics/turbulence.py:25-118) -------
