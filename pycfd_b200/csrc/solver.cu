@@ -1668,7 +1668,6 @@ int record_gated_step(pycfd_solver* s, const double* u0, const double* v0, doubl
   const LoopCtl gate{h, 1};
   k_step_gate<<<1, 32, 0, s->rec>>>(s->S, s->I, c, gate);
   CHECK_LAUNCH();
-  g_launches.fetch_add(1);
   const cudaGraphNode_t* deps = nullptr;
   size_t nd = 0;
   CU(cudaStreamGetCaptureInfo(s->rec, &cs, nullptr, &g, &deps, &nd));
@@ -1889,8 +1888,17 @@ int pycfd_profile_read(pycfd_solver* s, double* total_ms, int* launches, void* s
 }
 
 int pycfd_adjoint_apply(int op, const pycfd_adj_args* a, void* stream) {
-  if (!a || a->n < 2 || !(a->h > 0)) return fail(PCFD_E_ARG, "bad arguments");
+  if (!a) return fail(PCFD_E_ARG, "bad arguments");
   cudaStream_t sm = st(stream);
+  if (op == PCFD_ADJ_LINCOMB) {   // elementwise: no grid
+    if (!a->out || !a->a || !a->b || a->count < 0) return fail(PCFD_E_ARG, "lincomb: bad arguments");
+    if (a->count > 0) {
+      k_adj_lincomb<<<grid_for(a->count, 256), 256, 0, sm>>>(a->out, a->a, a->ca, a->b, a->cb, a->count);
+      CHECK_LAUNCH();
+    }
+    return 0;
+  }
+  if (a->n < 2 || !(a->h > 0)) return fail(PCFD_E_ARG, "bad arguments");
   const AdjGeo G{a->n, a->h, a->nu};
   const long nf = (long)(a->n + 3) * (a->n + 2) * 2;   // u and v faces
   const int grid = grid_for(nf, 256);
@@ -1919,10 +1927,6 @@ int pycfd_adjoint_apply(int op, const pycfd_adj_args* a, void* stream) {
     case PCFD_ADJ_CORRECT:
       if (!need({a->out_u, a->out_v, a->a})) return fail(PCFD_E_ARG, "correct: null array");
       k_adj_correct<<<grid, 256, 0, sm>>>(G, a->out_u, a->out_v, a->a, a->dt);
-      break;
-    case PCFD_ADJ_LINCOMB:
-      if (!need({a->out, a->a, a->b}) || a->count < 0) return fail(PCFD_E_ARG, "lincomb: bad arguments");
-      k_adj_lincomb<<<grid_for(a->count, 256), 256, 0, sm>>>(a->out, a->a, a->ca, a->b, a->cb, a->count);
       break;
     case PCFD_ADJ_OBJECTIVE:
       if (!need({a->u, a->v, a->lower, a->out})) return fail(PCFD_E_ARG, "objective: null array");
@@ -1958,7 +1962,6 @@ int pycfd_adjoint_apply(int op, const pycfd_adj_args* a, void* stream) {
     default: return fail(PCFD_E_ARG, "unknown adjoint op %d", op);
   }
   CHECK_LAUNCH();
-  g_launches.fetch_add(1);
   return 0;
 }
 

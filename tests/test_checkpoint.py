@@ -77,9 +77,18 @@ def test_gpu_state_round_trips_through_a_checkpoint(tmp_path):
     sim.run(max_steps=5)
     path = sim.save_checkpoint(tmp_path / "gpu.npz")
     back = Simulation.from_checkpoint(path)
+    again = Simulation.from_checkpoint(path)
     for a, b in zip(back.fields.numpy(), sim.fields.numpy()):
         assert np.array_equal(a, b)
     sim.run(max_steps=3)
     back.run(max_steps=3)
-    for a, b in zip(back.fields.numpy(), sim.fields.numpy()):
-        assert np.array_equal(a, b)
+    again.run(max_steps=3)
+    # The Poisson warm start is solver state, not checkpoint content (the
+    # reference keeps it in the solver object, pycfd/core/solver.py:659-663), so
+    # a restored run starts its first solve cold: it agrees with the
+    # uninterrupted run to the solve tolerance, and bit for bit with another
+    # restore of the same file.
+    assert back.fields.step == sim.fields.step and back.fields.t == sim.fields.t
+    for a, b, c in zip(back.fields.numpy(), sim.fields.numpy(), again.fields.numpy()):
+        assert np.array_equal(a, c)
+        assert np.abs(a - b).max() <= 1e-8 * max(np.abs(b).max(), 1.0)
