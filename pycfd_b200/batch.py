@@ -466,9 +466,7 @@ class BatchedSolver:
 
 BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
-    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=16),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32),
-    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=16),
     BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=None),

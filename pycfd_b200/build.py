@@ -45,7 +45,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     """Compile the library unless it is newer than every source; return its path."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB, *SOURCES]
+    # PYCFD_B200_DEFINES: extra -D options (strip heights PCFD_STRIP_ROWS and
+    # PCFD_BSTRIP_ROWS), e.g. "-DPCFD_BSTRIP_ROWS=4"
+    extra = os.environ.get("PYCFD_B200_DEFINES", "").split()
+    if any(not d.startswith("-D") for d in extra):
+        raise ValueError("PYCFD_B200_DEFINES takes -D options only")
+    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", LIB, *SOURCES]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)

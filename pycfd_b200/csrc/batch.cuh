@@ -309,19 +309,26 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
 // one 32-column segment of y (lane = column, so each row of a vector is one
 // coalesced 128-byte access in FP32, 256 bytes in FP64) over kBStripRows rows of
 // x.  The stencil operand of the strip and its two halo rows go to registers
-// first, with every per-cell load of the strip, before any arithmetic (a thread
-// keeps tens of independent loads in flight); the y-neighbours then come from
-// the adjacent lanes by shuffle, the segment's two edge lanes fetching theirs.
+// first, with every per-cell load of the strip, before any arithmetic; the
+// y-neighbours then come from the adjacent lanes by shuffle.  The columns just
+// west and east of the segment are the same for the whole warp: every lane forms
+// them (one broadcast load per row) and lanes 0 and `last` use them, so no load
+// sits under a lane-dependent branch and none waits for another.  Off-grid rows
+// and columns are read at a clamped (valid) index and the value dropped.
 // No shared-memory staging and no block barrier until the block's reduction.
 // A block (8 warps) takes kBStripItems consecutive (strip, segment) items of one
 // problem, adjacent segments of the same rows first.
-constexpr int kBStripRows = 8;
+#ifndef PCFD_BSTRIP_ROWS
+#define PCFD_BSTRIP_ROWS 8
+#endif
+constexpr int kBStripRows = PCFD_BSTRIP_ROWS;
 constexpr int kBStripItems = 16;
 
-// op(k, i, j): the operand at cell (i, j), k = i*ny + j (issues its loads).
-// load(u, c): the per-cell loads of body row u.
-// body(u, c, i, j, centre, west, east, south, north).
-// STENCIL = false: no operand (pointwise kernels); body gets zeros.
+// op(k, i, j): the operand at cell (i, j), k = i*ny + j (issues its loads; k is
+// always a valid cell).  load(u, c): the per-cell loads of body row u (c valid;
+// the values unused past the grid).  body(u, c, i, j, centre, west, east,
+// south, north).  STENCIL = false: no operand (pointwise kernels); body gets
+// zeros.
 template <bool STENCIL, class T, class Op, class Load, class Body>
 __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load load, Body body) {
   constexpr int RS = kBStripRows;
@@ -332,41 +339,33 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
     const int strip = it / V.segs, seg = it - strip * V.segs;
     const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
     const bool jv = j < ny;
+    const int jc = jv ? j : ny - 1;
+    const int last = min(31, ny - 1 - j0);   // the segment's last valid lane
     T ov[STENCIL ? RS + 2 : 1];
-    T es[STENCIL ? RS : 1], en[STENCIL ? RS : 1];
+    T ew[STENCIL ? RS : 1], ee[STENCIL ? RS : 1];
     if (STENCIL) {
 #pragma unroll
       for (int u = 0; u < RS + 2; ++u) {
-        int r = i0 - 1 + u;
-        if (r < 0) r = V.g.periodic_x ? nx - 1 : -1;
-        else if (r >= nx) r = (r == nx && V.g.periodic_x) ? 0 : -1;
-        ov[u] = (jv && r >= 0) ? op(r * ny + j, r, j) : (T)0;
+        const int r = strip_row(i0 - 1 + u, nx, V.g.periodic_x);
+        const int rc = r >= 0 ? r : 0;
+        const T val = op(rc * ny + jc, rc, jc);
+        ov[u] = (jv && r >= 0) ? val : (T)0;
+      }
+      int jw, je;
+      strip_edges(j0, last, ny, V.g.periodic_y, &jw, &je);
+      const int jwc = jw >= 0 ? jw : 0, jec = je >= 0 ? je : 0;
+#pragma unroll
+      for (int u = 0; u < RS; ++u) {
+        const int i = i0 + u, ic = i < nx ? i : nx - 1;
+        const T vw = op(ic * ny + jwc, ic, jwc), ve = op(ic * ny + jec, ic, jec);
+        ew[u] = (jw >= 0 && i < nx) ? vw : (T)0;
+        ee[u] = (je >= 0 && i < nx) ? ve : (T)0;
       }
     }
 #pragma unroll
     for (int u = 0; u < RS; ++u) {
-      const int i = i0 + u;
-      if (jv && i < nx) load(u, i * ny + j);
-    }
-    const int last = min(31, ny - 1 - j0);   // the segment's last valid lane
-    if (STENCIL) {
-      // the edge lanes' outer neighbours (wrapped on a periodic y axis, absent otherwise)
-      if (lane == 0) {
-        const int js = j0 > 0 ? j0 - 1 : (V.g.periodic_y ? ny - 1 : -1);
-#pragma unroll
-        for (int u = 0; u < RS; ++u) {
-          const int i = i0 + u;
-          es[u] = (js >= 0 && i < nx) ? op(i * ny + js, i, js) : (T)0;
-        }
-      }
-      if (lane == last) {
-        const int jn = j + 1 < ny ? j + 1 : (V.g.periodic_y ? 0 : -1);
-#pragma unroll
-        for (int u = 0; u < RS; ++u) {
-          const int i = i0 + u;
-          en[u] = (jn >= 0 && i < nx) ? op(i * ny + jn, i, jn) : (T)0;
-        }
-      }
+      const int i = i0 + u, ic = i < nx ? i : nx - 1;
+      load(u, ic * ny + jc);
     }
 #pragma unroll
     for (int u = 0; u < RS; ++u) {
@@ -377,8 +376,8 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
         e = ov[u + 2];
         sv = __shfl_up_sync(0xffffffffu, c, 1);
         nv = __shfl_down_sync(0xffffffffu, c, 1);
-        if (lane == 0) sv = es[u];
-        if (lane == last) nv = en[u];
+        if (lane == 0) sv = ew[u];
+        if (lane == last) nv = ee[u];
       }
       const int i = i0 + u;
       if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
@@ -748,7 +747,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
   auto pval = [&](int k, int, int) -> T {   // all loads issued, then selected
     const uint8_t fk = flags[k];
     const T zk = zraw[k];
-    const T pk = first ? (T)0 : p_old[k];
+    const T pk = p_old[k];                   // unused (and possibly unset) on the first pass
     const T z = (fk & F_SOLV) ? zk - tm : (T)0;
     if (first) return z;
     return pk * tb + z;
@@ -1351,20 +1350,23 @@ __global__ void __launch_bounds__(kBThreads) k_b_coarsest(const BProb<T>* __rest
 // structure, where M (n x n, row-major) is the structure's operator of the cycle
 // at and below its tail depth t and the columns of B_t are the level-t
 // right-hand sides of its problems -- a matrix product with the problems as the
-// N dimension.  One launch after the down sweep covers every structure; a block
-// (4 warps) takes a kTailBM-row tile of M against a kTailBN-problem column tile,
-// the K dimension in kTailBK chunks staged in shared memory (M rows and the
-// problems' vectors loaded coalesced along K).  FP64 form: DMMA (mma m8n8k4
-// f64, FP64 products and sums).  Mixed form: three TF32 MMAs per product
-// (m16n8k8; each FP32 operand split into a TF32 head and a TF32 remainder,
+// N dimension.  One launch after the down sweep covers every structure.  A block
+// takes a kTailBM = 16-row tile of M against a kTailBN = 32-problem column tile;
+// its 8 warps split K (warp w takes the K chunks w, w + 8, ...) and load their
+// MMA fragments straight from global memory (M and the vectors sit in L2; each
+// chunk's loads are all issued before its MMAs, and no barrier is taken inside
+// the K loop), then the eight partial tiles are summed through shared memory in
+// warp order, so the result is deterministic.  FP64 form: DMMA (mma m8n8k4 f64,
+// FP64 products and sums).  Mixed form: three TF32 MMAs per product (m16n8k8;
+// each FP32 operand split into a TF32 head and a TF32 remainder,
 // head*head + head*rem + rem*head) so the result keeps FP32 accuracy and the
 // preconditioner its FP32 behaviour.
-constexpr int kTailBM = 64, kTailBN = 32, kTailThreads = 128;
+constexpr int kTailBM = 16, kTailBN = 32, kTailThreads = 256;
 constexpr int kBTailGroup = kTailBN;   // problems per column tile of the tail launch
 
-template <class T> struct TailTile;
-template <> struct TailTile<float> { static constexpr int BK = 32, PA = 4, PB = 8; };
-template <> struct TailTile<double> { static constexpr int BK = 16, PA = 2, PB = 4; };
+template <class T> struct TailK;
+template <> struct TailK<float> { static constexpr int KW = 32; };    // K per warp chunk: 4 m16n8k8 steps
+template <> struct TailK<double> { static constexpr int KW = 16; };   // 4 m8n8k4 steps
 
 __device__ __forceinline__ uint32_t b_tf32(float x) {
   uint32_t r;
@@ -1386,22 +1388,9 @@ __device__ __forceinline__ void b_mma_f64(double (&c)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-// Stage K chunk [k0, k0 + BK) of the block's M rows and of its problems' vectors.
 template <class T>
-__device__ __forceinline__ void b_tail_stage(T (*As)[TailTile<T>::BK + TailTile<T>::PA],
-                                             T (*Bs)[kTailBN + TailTile<T>::PB], const T* __restrict__ M,
-                                             const T* const* sb, int n, int r0, int k0) {
-  constexpr int BK = TailTile<T>::BK;
-  for (int idx = threadIdx.x; idx < kTailBM * BK; idx += kTailThreads) {
-    const int r = idx / BK, k = idx - r * BK;
-    const int row = r0 + r, col = k0 + k;
-    As[r][k] = (row < n && col < n) ? __ldg(M + (long)row * n + col) : (T)0;
-  }
-  for (int idx = threadIdx.x; idx < kTailBN * BK; idx += kTailThreads) {
-    const int c = idx / BK, k = idx - c * BK;
-    const T* v = sb[c];
-    Bs[k][c] = (v && k0 + k < n) ? v[k0 + k] : (T)0;
-  }
+__device__ __forceinline__ T b_ld_or0(const T* p, bool ok) {
+  return ok ? __ldg(p) : (T)0;
 }
 
 template <class T>
@@ -1409,7 +1398,8 @@ __global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restr
                                                           const BHier<T>* __restrict__ hiers,
                                                           const int2* __restrict__ map,
                                                           const int* __restrict__ sprobs, BShared sh) {
-  constexpr int BK = TailTile<T>::BK;
+  constexpr int KW = TailK<T>::KW;
+  constexpr int NW = kTailThreads / 32;
   const int2 e = map[blockIdx.x];   // (structure, row tile * 64 + column tile)
   const BHier<T>& H = hiers[e.x];
   const int d = H.tail_level;
@@ -1418,8 +1408,7 @@ __global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restr
   __shared__ const T* sb[kTailBN];
   __shared__ T* sx[kTailBN];
   __shared__ int any;
-  __shared__ __align__(16) T As[kTailBM][BK + TailTile<T>::PA];
-  __shared__ __align__(16) T Bs[BK][kTailBN + TailTile<T>::PB];
+  __shared__ __align__(16) T red[NW][16 * 32];   // each warp's partial 16 x 32 tile, fragment order
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
   if (threadIdx.x < kTailBN) {
@@ -1442,32 +1431,47 @@ __global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restr
   const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
   const int g = lane >> 2, t = lane & 3;
   const T* __restrict__ M = H.tail;
+  const bool ok0 = r0 + g < n, ok1 = r0 + g + 8 < n;
+  const T* m0 = M + (long)(ok0 ? r0 + g : 0) * n;
+  const T* m1 = M + (long)(ok1 ? r0 + g + 8 : 0) * n;
+  const T* bq[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) bq[q] = sb[q * 8 + g];
+  T* out = &red[warp][0];
   if constexpr (sizeof(T) == 4) {
     float acc[4][4];   // [n tile][fragment]
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[q][i] = 0.f;
-    const int wr = warp * 16;
-    for (int k0 = 0; k0 < n; k0 += BK) {
-      __syncthreads();
-      b_tail_stage<T>(As, Bs, M, sb, n, r0, k0);
-      __syncthreads();
+    for (int k0 = warp * KW; k0 < n; k0 += NW * KW) {
+      float av[4][4], bv[4][4][2];
 #pragma unroll
-      for (int kk = 0; kk < BK; kk += 8) {
-        const float av[4] = {As[wr + g][kk + t], As[wr + g + 8][kk + t], As[wr + g][kk + t + 4],
-                             As[wr + g + 8][kk + t + 4]};
+      for (int s = 0; s < 4; ++s) {
+        const int ka = k0 + s * 8 + t, kb = ka + 4;
+        av[s][0] = b_ld_or0(m0 + ka, ok0 && ka < n);
+        av[s][1] = b_ld_or0(m1 + ka, ok1 && ka < n);
+        av[s][2] = b_ld_or0(m0 + kb, ok0 && kb < n);
+        av[s][3] = b_ld_or0(m1 + kb, ok1 && kb < n);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          bv[s][q][0] = b_ld_or0(bq[q] + ka, bq[q] && ka < n);
+          bv[s][q][1] = b_ld_or0(bq[q] + kb, bq[q] && kb < n);
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
         uint32_t ah[4], al[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          ah[i] = b_tf32(av[i]);
-          al[i] = b_tf32(av[i] - __uint_as_float(ah[i]));
+          ah[i] = b_tf32(av[s][i]);
+          al[i] = b_tf32(av[s][i] - __uint_as_float(ah[i]));
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const float bv0 = Bs[kk + t][q * 8 + g], bv1 = Bs[kk + t + 4][q * 8 + g];
-          const uint32_t bh0 = b_tf32(bv0), bh1 = b_tf32(bv1);
-          const uint32_t bl0 = b_tf32(bv0 - __uint_as_float(bh0)), bl1 = b_tf32(bv1 - __uint_as_float(bh1));
+          const uint32_t bh0 = b_tf32(bv[s][q][0]), bh1 = b_tf32(bv[s][q][1]);
+          const uint32_t bl0 = b_tf32(bv[s][q][0] - __uint_as_float(bh0));
+          const uint32_t bl1 = b_tf32(bv[s][q][1] - __uint_as_float(bh1));
           b_mma_tf32(acc[q], al, bh0, bh1);
           b_mma_tf32(acc[q], ah, bl0, bl1);
           b_mma_tf32(acc[q], ah, bh0, bh1);
@@ -1477,45 +1481,57 @@ __global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restr
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int row = r0 + wr + g + ((i & 2) ? 8 : 0);
-        const int col = q * 8 + 2 * t + (i & 1);
-        T* x = sx[col];
-        if (x && row < n) x[row] = acc[q][i];
-      }
+      for (int i = 0; i < 4; ++i) out[(q * 4 + i) * 32 + lane] = acc[q][i];
   } else {
     double acc[2][4][2];   // [m tile][n tile][fragment]
 #pragma unroll
     for (int m = 0; m < 2; ++m)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[m][q][0] = acc[m][q][1] = 0.0;
-    const int wr = warp * 16;
-    for (int k0 = 0; k0 < n; k0 += BK) {
-      __syncthreads();
-      b_tail_stage<T>(As, Bs, M, sb, n, r0, k0);
-      __syncthreads();
+    for (int k0 = warp * KW; k0 < n; k0 += NW * KW) {
+      double av[4][2], bv[4][4];
 #pragma unroll
-      for (int kk = 0; kk < BK; kk += 4) {
-        const double a0 = As[wr + g][kk + t], a1 = As[wr + 8 + g][kk + t];
+      for (int s = 0; s < 4; ++s) {
+        const int k = k0 + s * 4 + t;
+        av[s][0] = b_ld_or0(m0 + k, ok0 && k < n);
+        av[s][1] = b_ld_or0(m1 + k, ok1 && k < n);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bv[s][q] = b_ld_or0(bq[q] + k, bq[q] && k < n);
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const double bv = Bs[kk + t][q * 8 + g];
-          b_mma_f64(acc[0][q], a0, bv);
-          b_mma_f64(acc[1][q], a1, bv);
+          b_mma_f64(acc[0][q], av[s][0], bv[s][q]);
+          b_mma_f64(acc[1][q], av[s][1], bv[s][q]);
         }
-      }
     }
 #pragma unroll
     for (int m = 0; m < 2; ++m)
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int row = r0 + wr + 8 * m + g;
-          const int col = q * 8 + 2 * t + i;
-          T* x = sx[col];
-          if (x && row < n) x[row] = acc[m][q][i];
-        }
+        for (int i = 0; i < 2; ++i) out[((m * 4 + q) * 2 + i) * 32 + lane] = acc[m][q][i];
+  }
+  __syncthreads();
+  // the partial tiles summed in warp order; slot -> (lane, fragment) -> (row, problem)
+  for (int idx = threadIdx.x; idx < 16 * 32; idx += kTailThreads) {
+    T v = red[0][idx];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) v += red[w][idx];
+    const int f = idx >> 5, l = idx & 31, lg = l >> 2, lt = l & 3;
+    int row, col;
+    if constexpr (sizeof(T) == 4) {   // f = q * 4 + i: rows g, g + 8; columns 2t, 2t + 1 of n tile q
+      const int q = f >> 2, i = f & 3;
+      row = lg + ((i & 2) ? 8 : 0);
+      col = q * 8 + 2 * lt + (i & 1);
+    } else {                          // f = (m * 4 + q) * 2 + i: row 8m + g; columns 2t, 2t + 1 of n tile q
+      const int m = f >> 3, q = (f >> 1) & 3, i = f & 1;
+      row = 8 * m + lg;
+      col = q * 8 + 2 * lt + i;
+    }
+    T* x = sx[col];
+    if (x && r0 + row < n) x[r0 + row] = v;
   }
 }
 

@@ -231,11 +231,18 @@ __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Ge
 // The fine-level solver kernels walk the grid in warp strips: a warp takes one
 // 32-column segment of y (lane = column: every row load is one coalesced
 // access) over kStripRows rows of x.  The stencil operand of the strip and its
-// two halo rows are formed once, into registers, before any arithmetic (each
-// thread keeps tens of independent loads in flight); the y-neighbours come
-// from the adjacent lanes by shuffle, the segment's edge lanes forming theirs.
+// two halo rows are formed once, into registers, before any arithmetic; the
+// y-neighbours come from the adjacent lanes by shuffle.  The columns just west
+// and east of the segment are the same for the whole warp, so every lane forms
+// them (one broadcast load per row) and lanes 0 and `last` use them: no load
+// sits under a lane-dependent branch, none waits for another, and the whole
+// strip's loads are in flight at once.  Off-grid rows and columns are read at a
+// clamped (valid) index and the value dropped.
 // Blocks of 256 threads (8 warps) stride over the items (strip x segment).
-constexpr int kStripRows = 8;
+#ifndef PCFD_STRIP_ROWS
+#define PCFD_STRIP_ROWS 4
+#endif
+constexpr int kStripRows = PCFD_STRIP_ROWS;
 constexpr int kStripThreads = 256;
 
 inline int strip_items(const Geo& g) { return ((g.ny + 31) / 32) * ((g.nx + kStripRows - 1) / kStripRows); }
@@ -244,10 +251,27 @@ inline int strip_grid(const Geo& g) {
   return b < kMaxRedBlocks ? (b < 1 ? 1 : b) : kMaxRedBlocks;
 }
 
-// op(k, i, j): the operand at cell (i, j) (issues its loads); load(u, c): the
-// per-cell loads of body row u; body(u, c, i, j, centre, west, east, south, north).
-// STENCIL = false: no operand (pointwise kernels).  Neighbours off the grid are
-// wrapped on periodic axes and 0 otherwise (their face flags are clear).
+// Row of the operand at strip row r (halo rows included): wrapped on a periodic
+// x axis, -1 off the grid.
+__device__ __forceinline__ int strip_row(int r, int nx, int periodic_x) {
+  if (r < 0) return periodic_x ? nx - 1 : -1;
+  if (r >= nx) return (r == nx && periodic_x) ? 0 : -1;
+  return r;
+}
+
+// The columns west and east of segment [j0, j0 + last]: wrapped on a periodic y
+// axis, -1 off the grid.
+__device__ __forceinline__ void strip_edges(int j0, int last, int ny, int periodic_y, int* jw, int* je) {
+  *jw = j0 > 0 ? j0 - 1 : (periodic_y ? ny - 1 : -1);
+  *je = j0 + last + 1 < ny ? j0 + last + 1 : (periodic_y ? 0 : -1);
+}
+
+// op(k, i, j): the operand at cell (i, j) (issues its loads; k always a valid
+// cell, the value dropped where the cell is off the grid); load(u, c): the
+// per-cell loads of body row u (c valid; the values unused past the grid);
+// body(u, c, i, j, centre, west, east, south, north).  STENCIL = false: no
+// operand (pointwise kernels).  Neighbours off the grid are wrapped on periodic
+// axes and 0 otherwise (their face flags are clear).
 template <bool STENCIL, class Op, class Load, class Body>
 __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body body) {
   constexpr int RS = kStripRows;
@@ -260,40 +284,33 @@ __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body
     const int strip = it / segs, seg = it - strip * segs;
     const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
     const bool jv = j < ny;
+    const int jc = jv ? j : ny - 1;
+    const int last = min(31, ny - 1 - j0);
     double ov[STENCIL ? RS + 2 : 1];
-    double es[STENCIL ? RS : 1], en[STENCIL ? RS : 1];
+    double ew[STENCIL ? RS : 1], ee[STENCIL ? RS : 1];
     if (STENCIL) {
 #pragma unroll
       for (int u = 0; u < RS + 2; ++u) {
-        int r = i0 - 1 + u;
-        if (r < 0) r = g.periodic_x ? nx - 1 : -1;
-        else if (r >= nx) r = (r == nx && g.periodic_x) ? 0 : -1;
-        ov[u] = (jv && r >= 0) ? op(r * ny + j, r, j) : 0.0;
+        const int r = strip_row(i0 - 1 + u, nx, g.periodic_x);
+        const int rc = r >= 0 ? r : 0;
+        const double val = op(rc * ny + jc, rc, jc);
+        ov[u] = (jv && r >= 0) ? val : 0.0;
+      }
+      int jw, je;
+      strip_edges(j0, last, ny, g.periodic_y, &jw, &je);
+      const int jwc = jw >= 0 ? jw : 0, jec = je >= 0 ? je : 0;
+#pragma unroll
+      for (int u = 0; u < RS; ++u) {
+        const int i = i0 + u, ic = i < nx ? i : nx - 1;
+        const double vw = op(ic * ny + jwc, ic, jwc), ve = op(ic * ny + jec, ic, jec);
+        ew[u] = (jw >= 0 && i < nx) ? vw : 0.0;
+        ee[u] = (je >= 0 && i < nx) ? ve : 0.0;
       }
     }
 #pragma unroll
     for (int u = 0; u < RS; ++u) {
-      const int i = i0 + u;
-      if (jv && i < nx) load(u, i * ny + j);
-    }
-    const int last = min(31, ny - 1 - j0);
-    if (STENCIL) {
-      if (lane == 0) {
-        const int js = j0 > 0 ? j0 - 1 : (g.periodic_y ? ny - 1 : -1);
-#pragma unroll
-        for (int u = 0; u < RS; ++u) {
-          const int i = i0 + u;
-          es[u] = (js >= 0 && i < nx) ? op(i * ny + js, i, js) : 0.0;
-        }
-      }
-      if (lane == last) {
-        const int jn = j + 1 < ny ? j + 1 : (g.periodic_y ? 0 : -1);
-#pragma unroll
-        for (int u = 0; u < RS; ++u) {
-          const int i = i0 + u;
-          en[u] = (jn >= 0 && i < nx) ? op(i * ny + jn, i, jn) : 0.0;
-        }
-      }
+      const int i = i0 + u, ic = i < nx ? i : nx - 1;
+      load(u, ic * ny + jc);
     }
 #pragma unroll
     for (int u = 0; u < RS; ++u) {
@@ -304,8 +321,8 @@ __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body
         e = ov[u + 2];
         sv = __shfl_up_sync(0xffffffffu, c, 1);
         nv = __shfl_down_sync(0xffffffffu, c, 1);
-        if (lane == 0) sv = es[u];
-        if (lane == last) nv = en[u];
+        if (lane == 0) sv = ew[u];
+        if (lane == last) nv = ee[u];
       }
       const int i = i0 + u;
       if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);

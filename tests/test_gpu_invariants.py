@@ -154,12 +154,12 @@ def test_nonfinite_state_raises_divergence_error():
 
 
 def test_rejected_configurations():
-    from pycfd_b200.solver import ProjectionSolver
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
     base = dict(nx=16, ny=16, re=100.0, boundary_config=cases.bcs())
     with pytest.raises(NotImplementedError, match="direct"):
         ProjectionSolver(_cfg(base, pressure_solver="direct"))
-    with pytest.raises(NotImplementedError):
-        ProjectionSolver(_cfg(base, pressure_solver="cg", use_les=True))
+    with pytest.raises(NotImplementedError, match="mixed-precision"):
+        ProjectionSolver(_cfg(base, pressure_solver="cg"), options=GpuOptions(precision="mixed"))
     with pytest.raises(NotImplementedError, match="simple"):
         ProjectionSolver(_cfg(base, pressure_solver="cg", solver_type="simple"))
     with pytest.raises(ValueError, match="red/black"):
