@@ -424,6 +424,9 @@ typedef struct {
                            level restricted by R (I - A W) (1: from the fine level;
                            2: the fine sweep and restriction stay separate); 0
                            reads as 1                                           */
+    int ell_group;      /* problems of one structure per block of a coarse-level
+                           launch, sharing each matrix entry's load: 1 or 8 (0
+                           reads as 8)                                          */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver

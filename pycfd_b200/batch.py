@@ -258,6 +258,7 @@ class BatchOptions:
     tail_ratio: float | None = 16.0   #: bound the tail operator: n_t^2 <= tail_ratio * n_0 (None: none)
     fused_restriction: bool = False   #: down sweep by R (I - A W) products (one sweep, every structure tailed)
     fused_from: int = 1               #: first level so restricted (2: the fine level's restriction stays)
+    ell_group: int = 8                #: problems per coarse-level block sharing the matrix loads (1 or 8)
 
 
 class BatchedSolver:
@@ -351,7 +352,7 @@ class BatchedSolver:
         P = (C.c_void_p * n)(*[f.p.data_ptr() for f in self.fields])
         bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
                             float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows),
-                            int(opts.coarse_level), int(opts.fused_from))
+                            int(opts.coarse_level), int(opts.fused_from), int(opts.ell_group))
         if max_steps is None:
             ms = None
         else:
@@ -475,8 +476,16 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True),
     BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
                  fused_from=2),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, ell_group=1),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, ell_group=1),
+    BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32, ell_group=1),
+    BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 fused_from=2, ell_group=1),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True),
+    BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, ell_group=1),
+    BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 ell_group=1),
 )
 
 

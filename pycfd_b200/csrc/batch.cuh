@@ -1118,28 +1118,31 @@ __device__ __forceinline__ T b_ell_row(const Ell<T>& E, int L, int row, int lane
 // ---- grouped ELL phases ------------------------------------------------------------
 // The problems of one structure share its hierarchy, so a block of a coarse-
 // level launch applies one row block of a structure's matrix to a GROUP of up
-// to kBGroup of its problems: each lane loads an entry (value, column) once and
+// to GS of its problems: each lane loads an entry (value, column) once and
 // multiplies it into every problem's gathered vector with its own accumulator.
-// The shared matrices cross from L2 once per group instead of once per problem,
-// and the per-entry index arithmetic is paid once per group.  Each problem's row
-// sum keeps the per-problem order (lane-strided entries, then the lane tree).
-constexpr int kBGroup = 8;         // problems per block of a grouped launch (also the tail's group)
-constexpr int kBEllGRounds = 2;    // rounds of kBThreads / L rows per block
+// GS = 8: the shared matrices cross from L2 once per group instead of once per
+// problem, and the per-entry index arithmetic is paid once per group.  GS = 1:
+// one problem per block, more blocks and eight rows per lane group in flight
+// (the per-problem form).  Each problem's row sum keeps the per-problem order
+// (lane-strided entries, then the lane tree) in both.
+constexpr int kBGroup = 8;         // problems per block of the grouped form
+template <int GS>
+__host__ __device__ constexpr int b_ell_rounds() { return GS == 1 ? 8 : 2; }   // rounds of kBThreads / L rows
 
 // The group's vectors for one op, filled from the problem records by the first
-// kBGroup threads; a null output marks a member that is absent or not solving.
-template <class T>
+// GS threads; a null output marks a member that is absent or not solving.
+template <class T, int GS>
 struct BGroup {
-  const T* src[kBGroup];   // gathered vector
-  const T* b[kBGroup];     // the level's right-hand side (or r on level 0)
-  T* out[kBGroup];
-  T* out2[kBGroup];
-  T mr[kBGroup];           // fluid mean of r (projected level-0 right-hand side)
+  const T* src[GS];   // gathered vector
+  const T* b[GS];     // the level's right-hand side (or r on level 0)
+  T* out[GS];
+  T* out2[GS];
+  T mr[GS];           // fluid mean of r (projected level-0 right-hand side)
 };
 
 // Fill member g (thread g of the block) for op OP at depth d.
-template <class T, int OP>
-__device__ __forceinline__ void b_group_fill(BGroup<T>& G, int g, const BProb<T>* P, int d, int src, int dst) {
+template <class T, int OP, int GS>
+__device__ __forceinline__ void b_group_fill(BGroup<T, GS>& G, int g, const BProb<T>* P, int d, int src, int dst) {
   G.src[g] = nullptr;
   G.b[g] = nullptr;
   G.out[g] = nullptr;
@@ -1183,24 +1186,25 @@ __device__ __forceinline__ void b_group_fill(BGroup<T>& G, int g, const BProb<T>
   }
 }
 
-// kBEllGRounds rounds of kBThreads / L rows of row block rb of matrix E, for
-// every member of the group.  L lanes per row fixed at compile time (L > 1:
+// b_ell_rounds<GS>() rounds of kBThreads / L rows of row block rb of matrix E,
+// for every member of the group.  L lanes per row fixed at compile time (L > 1:
 // row-major entries, L = 1: column-major).
-template <int L, int OP, class T>
-__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T>& G, const Ell<T>& E,
+template <int L, int OP, int GS, class T>
+__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T, GS>& G, const Ell<T>& E,
                                             const T* __restrict__ wd, int d, int rb) {
   constexpr int per = kBThreads / L;
   const int lane = (int)threadIdx.x & (L - 1);
   const uint8_t* __restrict__ flags = P0.flags;
-  bool on[kBGroup];
+  constexpr int ROUNDS = b_ell_rounds<GS>();
+  bool on[GS];
 #pragma unroll
-  for (int g = 0; g < kBGroup; ++g) on[g] = G.out[g] != nullptr;
+  for (int g = 0; g < GS; ++g) on[g] = G.out[g] != nullptr;
 #pragma unroll
-  for (int rd = 0; rd < kBEllGRounds; ++rd) {
-    const int row = (rb * kBEllGRounds + rd) * per + (int)threadIdx.x / L;
-    T acc[kBGroup];
+  for (int rd = 0; rd < ROUNDS; ++rd) {
+    const int row = (rb * ROUNDS + rd) * per + (int)threadIdx.x / L;
+    T acc[GS];
 #pragma unroll
-    for (int g = 0; g < kBGroup; ++g) acc[g] = (T)0;
+    for (int g = 0; g < GS; ++g) acc[g] = (T)0;
     if (row < E.n) {
       const int kb = L > 1 ? lane : 0;
 #pragma unroll 2
@@ -1211,30 +1215,30 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T>&
         if (OP == EO_PRE) {
           const T w = wd[c];
 #pragma unroll
-          for (int g = 0; g < kBGroup; ++g)
+          for (int g = 0; g < GS; ++g)
             if (on[g]) acc[g] += v * (w * G.b[g][c]);
         } else if ((OP == EO_FRESTRICT && d == 1)) {
           const bool solv = (flags[c] & F_SOLV) != 0;
 #pragma unroll
-          for (int g = 0; g < kBGroup; ++g)
+          for (int g = 0; g < GS; ++g)
             if (on[g]) {
               const T rc = G.b[g][c];
               acc[g] += v * (solv ? rc - G.mr[g] : (T)0);
             }
         } else {
 #pragma unroll
-          for (int g = 0; g < kBGroup; ++g)
+          for (int g = 0; g < GS; ++g)
             if (on[g]) acc[g] += v * G.src[g][c];
         }
       }
     }
 #pragma unroll
-    for (int g = 0; g < kBGroup; ++g)
+    for (int g = 0; g < GS; ++g)
 #pragma unroll
       for (int o = L / 2; o > 0; o >>= 1) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], o, L);
     if (lane != 0 || row >= E.n) continue;
 #pragma unroll
-    for (int g = 0; g < kBGroup; ++g) {
+    for (int g = 0; g < GS; ++g) {
       if (!on[g]) continue;
       const T s = acc[g];
       T* __restrict__ o = G.out[g];
@@ -1272,9 +1276,9 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T>&
   }
 }
 
-// One ELL op at depth d over the map's (structure, row block x 64 + group)
-// entries.  Members: sprobs[H.sp0 + group * kBGroup + g], g < kBGroup.
-template <class T, int OP>
+// One ELL op at depth d over the map's (structure, row block x 1024 + group)
+// entries.  Members: sprobs[H.sp0 + group * GS + g], g < GS.
+template <class T, int OP, int GS>
 __global__ void __launch_bounds__(kBThreads) k_b_ellg(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map,
@@ -1282,35 +1286,35 @@ __global__ void __launch_bounds__(kBThreads) k_b_ellg(const BProb<T>* __restrict
                                                        int dst, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BHier<T>& H = hiers[e.x];
-  const int rb = e.y >> 6, grp = e.y & 63;
-  __shared__ BGroup<T> G;
+  const int rb = e.y >> 10, grp = e.y & 1023;
+  __shared__ BGroup<T, GS> G;
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
-  if (threadIdx.x < kBGroup) {
-    const int k = grp * kBGroup + (int)threadIdx.x;
+  if (threadIdx.x < GS) {
+    const int k = grp * GS + (int)threadIdx.x;
     const BProb<T>* P = nullptr;
     if (k < H.spn) {
       const int pi = sprobs[H.sp0 + k];
       if (b_solving(sh, pi)) P = probs + pi;
     }
-    b_group_fill<T, OP>(G, (int)threadIdx.x, P, d, src, dst);
+    b_group_fill<T, OP, GS>(G, (int)threadIdx.x, P, d, src, dst);
     if (P) any = 1;
   }
   __syncthreads();
   if (!any) return;
-  const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * kBGroup]];   // the structure's geometry and flags
+  const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * GS]];   // the structure's geometry and flags
   const bool pl = OP == EO_PROLONG || OP == EO_PROLONGW;
   const BLevel<T>& Lm = pl ? H.lv[d + 1] : H.lv[d];
   const Ell<T>& E = pl ? Lm.P : OP == EO_RESTRICT ? Lm.R : OP == EO_FRESTRICT ? Lm.M : Lm.A;
   const int Lop = pl ? Lm.lp : OP == EO_RESTRICT ? Lm.lr : OP == EO_FRESTRICT ? Lm.lm : Lm.la;
   const T* wd = d > 0 ? H.lv[d].wd : nullptr;
   switch (Lop) {
-    case 1: b_ellg_rows<1, OP>(P0, G, E, wd, d, rb); break;
-    case 4: b_ellg_rows<4, OP>(P0, G, E, wd, d, rb); break;
-    case 8: b_ellg_rows<8, OP>(P0, G, E, wd, d, rb); break;
-    case 16: b_ellg_rows<16, OP>(P0, G, E, wd, d, rb); break;
-    default: b_ellg_rows<32, OP>(P0, G, E, wd, d, rb); break;
+    case 1: b_ellg_rows<1, OP, GS>(P0, G, E, wd, d, rb); break;
+    case 4: b_ellg_rows<4, OP, GS>(P0, G, E, wd, d, rb); break;
+    case 8: b_ellg_rows<8, OP, GS>(P0, G, E, wd, d, rb); break;
+    case 16: b_ellg_rows<16, OP, GS>(P0, G, E, wd, d, rb); break;
+    default: b_ellg_rows<32, OP, GS>(P0, G, E, wd, d, rb); break;
   }
 }
 

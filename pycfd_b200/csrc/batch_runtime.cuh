@@ -24,6 +24,7 @@ struct pycfd_batch {
   int coarse = 0;                          // levels >= coarse: one block per problem (0: per level)
   int fused = 0;                           // down sweep by fused restrictions (every structure has them)
   int fused_from = 1;                      // first level restricted by the fused product (1 or 2)
+  int ell_group = kBGroup;                 // problems per block of the coarse-level launches (1 or kBGroup)
   int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
@@ -35,7 +36,7 @@ struct pycfd_batch {
   BMapHost strip;                          // every chunk of warp strips of every problem (solver kernels)
   BMapHost pstrip;                         // every chunk of predictor strips of every problem
   // row-block maps per depth d (problems whose level d runs per level):
-  // grouped maps per depth d, entries (structure, row block x 64 + group of kBGroup problems):
+  // grouped maps per depth d, entries (structure, row block x 1024 + group of ell_group problems):
   std::vector<BMapHost> mapA;              // smoothing/residual with A_d (d >= 1)
   std::vector<BMapHost> mapR;              // restriction into d
   std::vector<BMapHost> mapP;              // prolongation into d with P_{d+1}
@@ -305,8 +306,9 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     std::vector<int2> ma, mr, mp, mc;
     for (size_t h = 0; h < leaders.size(); ++h) {
       const BHier<T>& H = hh[h];
-      const int grps = (H.spn + kBGroup - 1) / kBGroup;
-      if (grps > 64) return fail(PCFD_E_UNSUPPORTED, "at most %d problems share a structure", 64 * kBGroup);
+      const int gs = B->ell_group;
+      const int grps = (H.spn + gs - 1) / gs;
+      if (grps > 1024) return fail(PCFD_E_UNSUPPORTED, "at most %d problems share a structure", 1024 * gs);
       if (H.tail_level == d && H.tail_n > 0) {
         const int rts = (H.tail_n + kTailBM - 1) / kTailBM;
         const int cts = (H.spn + kTailBN - 1) / kTailBN;
@@ -331,9 +333,9 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       }
       const int nrow = d == 0 ? pr[lead].g.nx * pr[lead].g.ny : keep[h][d].n;
       auto add = [&](std::vector<int2>& m, int lanes) {
-        const int rpb = kBThreads / lanes * kBEllGRounds;
+        const int rpb = kBThreads / lanes * (gs == 1 ? b_ell_rounds<1>() : b_ell_rounds<kBGroup>());
         for (int rb = 0; rb * rpb < nrow; ++rb)
-          for (int g = 0; g < grps; ++g) m.push_back(make_int2((int)h, rb * 64 + g));
+          for (int g = 0; g < grps; ++g) m.push_back(make_int2((int)h, rb * 1024 + g));
       };
       const int lres = (B->fused && d >= B->fused_from) ? H.lv[d].lm : H.lv[d].lr;   // lanes of the restriction into d
       if (t > 0 && d == t) {   // restriction into the tail level only
@@ -415,9 +417,12 @@ int b_ell(pycfd_batch* B, const BMapHost& m, int d, int src, int dst, cudaStream
   const BMapHost* mc = (OP == EO_RESTRICT && d < (int)B->mapC.size()) ? &B->mapC[d] : nullptr;
   if (m.n == 0 && !(mc && mc->n)) return 0;
   b_prof(B, 4, st);
-  if (m.n)
-    BLAUNCH((k_b_ellg<T, OP>), m.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), m.e, B->sprobs, d, src,
+  if (m.n && B->ell_group == 1)
+    BLAUNCH((k_b_ellg<T, OP, 1>), m.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), m.e, B->sprobs, d, src,
             dst, B->sh);
+  else if (m.n)
+    BLAUNCH((k_b_ellg<T, OP, kBGroup>), m.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), m.e, B->sprobs, d,
+            src, dst, B->sh);
   if (mc && mc->n) BLAUNCH(k_b_coarsest<T>, mc->n, kBThreads, B->smem_dense, st, probs_of<T>(B), mc->e, d, B->sh);
   b_prof(B, 4, st);
   return 0;
@@ -758,6 +763,8 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
     return fail(PCFD_E_ARG, "tile_rows must be 8, 16, 32 or 64");
   if (opts->mg_sweeps < 1 || opts->mg_sweeps > 4) return fail(PCFD_E_ARG, "mg_sweeps must be 1..4");
   if (opts->fused_from < 0 || opts->fused_from > 2) return fail(PCFD_E_ARG, "fused_from must be 0, 1 or 2");
+  if (opts->ell_group != 0 && opts->ell_group != 1 && opts->ell_group != kBGroup)
+    return fail(PCFD_E_ARG, "ell_group must be 0, 1 or %d", kBGroup);
   if (opts->coarse_level < 0 || opts->coarse_level >= kBMaxLevels)
     return fail(PCFD_E_ARG, "coarse_level must be 0..%d", kBMaxLevels - 1);
   if (!(opts->tol > 0) || opts->maxiter < 1) return fail(PCFD_E_ARG, "bad tolerance or iteration limit");
@@ -776,6 +783,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->tile_i = opts->tile_rows;
   B->coarse = opts->coarse_level;
   B->fused_from = opts->fused_from == 2 ? 2 : 1;
+  B->ell_group = opts->ell_group == 1 ? 1 : kBGroup;
   B->mem = new pycfd_solver();
   B->solvers.assign(n, nullptr);
   for (int i = 0; i < n; ++i) {
