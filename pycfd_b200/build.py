@@ -3,8 +3,9 @@
     python -m pycfd_b200.build        (or __graft_entry__.build())
 
 The library is the C ABI of include/pycfd_b200.h: one translation unit
-(csrc/solver.cu including the kernel headers), compiled for sm_100a only, with
-FMA contraction disabled so the stencils keep the reference's rounding.
+(csrc/solver.cu including the kernel headers), compiled for sm_100a only.  FMA
+contraction is on; the stencils that must keep the reference's rounding form
+their products with rmul (csrc/common.cuh), which is never fused.
 """
 
 from __future__ import annotations
@@ -23,7 +24,7 @@ HEADERS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "--extended-lambda",
-    "-fmad=false", "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC", "-shared",
 ]
 
 

@@ -40,13 +40,13 @@ __global__ void k_adj_predictor(AdjGeo G, const double* __restrict__ U, const do
     if (e < nu) {
       const int m = (int)(e / (n + 2)), j = (int)(e % (n + 2));
       double val = U[e];
-      if (G.u_solv(m, j)) val = val + dt * rhs_u_at(U, V, m, j, n, G.h, G.h, G.nu, 0.0, 0.0);
+      if (G.u_solv(m, j)) val = val + rmul(dt, rhs_u_at(U, V, m, j, n, G.h, G.h, G.nu, 0.0, 0.0));
       us[e] = val;
     } else {
       const long f = e - nu;
       const int i = (int)(f / (n + 3)), k = (int)(f % (n + 3));
       double val = V[f];
-      if (G.v_solv(i, k)) val = val + dt * rhs_v_at(U, V, i, k, n, G.h, G.h, G.nu, 0.0, 0.0);
+      if (G.v_solv(i, k)) val = val + rmul(dt, rhs_v_at(U, V, i, k, n, G.h, G.h, G.nu, 0.0, 0.0));
       vs[f] = val;
     }
   }
@@ -131,7 +131,7 @@ __global__ void k_adj_correct(AdjGeo G, double* __restrict__ u, double* __restri
 // out = ca a + cb b, elementwise (the Runge-Kutta combinations and their transposes).
 __global__ void k_adj_lincomb(double* __restrict__ out, const double* __restrict__ a, double ca,
                               const double* __restrict__ b, double cb, long count) {
-  ADJ_FOR(count) out[e] = ca * a[e] + cb * b[e];
+  ADJ_FOR(count) out[e] = rmul(ca, a[e]) + rmul(cb, b[e]);
 }
 
 // Kinetic energy of the cells below the split, one block: 0.5 (uc^2 + vc^2)
@@ -144,7 +144,7 @@ __global__ void k_adj_objective(AdjGeo G, const double* __restrict__ u, const do
     const int i = (int)(e / n), j = (int)(e % n);
     const double uc = 0.5 * (u[G.U(i + 1, j + 1)] + u[G.U(i + 2, j + 1)]);
     const double vc = 0.5 * (v[G.V(i + 1, j + 1)] + v[G.V(i + 1, j + 2)]);
-    acc += 0.5 * (uc * uc + vc * vc) * lower[j];
+    acc += rmul(0.5 * (rmul(uc, uc) + rmul(vc, vc)), lower[j]);
   }
   double a[1] = {acc};
   block_reduce<1>(a);

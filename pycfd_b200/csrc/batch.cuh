@@ -514,15 +514,15 @@ __global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __res
       if (out && ju && m < nx + 3) {
         double val = U[q + 1];
         if (m >= g.u_lo && m < g.u_hi && j >= 1 && j <= ny)
-          val = val + dt * rhs_u_core(U[q + 1], U[q + 2], U[q], un, usv, vn0, vn1, V[q], V[q + 1], g.dx, g.dy,
-                                      g.nu, blend, g.fx);
+          val = val + rmul(dt, rhs_u_core(U[q + 1], U[q + 2], U[q], un, usv, vn0, vn1, V[q], V[q + 1], g.dx,
+                                          g.dy, g.nu, blend, g.fx));
         us[(long)m * W + j] = val;
       }
       if (out && jv && m < nx + 2) {
         double val = V[q + 1];
         if (m >= 1 && m <= nx && j >= g.v_lo && j < g.v_hi)
-          val = val + dt * rhs_v_core(V[q + 1], vn1, vsv, V[q + 2], V[q], us2, U[q + 2], usv, U[q + 1], g.dx,
-                                      g.dy, g.nu, blend, g.fy);
+          val = val + rmul(dt, rhs_v_core(V[q + 1], vn1, vsv, V[q + 2], V[q], us2, U[q + 2], usv, U[q + 1],
+                                          g.dx, g.dy, g.nu, blend, g.fy));
         vs[(long)m * WV + j] = val;
       }
     }

@@ -142,13 +142,13 @@ __device__ void bc_mass_balance(double* u, double* v, const Geo& g, const BcTabl
       s += axis == 0 ? u[(long)n_face * WU + k] : v[(long)k * WV + n_face];
     s = block_sum_bcast(s);
     const double width = axis == 0 ? g.dy : g.dx;
-    const double flux_out = (low ? -1.0 : 1.0) * (s * width);
+    const double flux_out = (low ? -1.0 : 1.0) * rmul(s, width);
     if (T.kind[w] == BC_OUTLET) outflux += flux_out;
     else influx -= flux_out;
   }
   double total = 0.0;
   for (int w = 0; w < 4; ++w)
-    if (T.kind[w] == BC_OUTLET) total += (w < 2 ? ny : nx) * (w < 2 ? g.dy : g.dx);
+    if (T.kind[w] == BC_OUTLET) total += rmul((double)(w < 2 ? ny : nx), w < 2 ? g.dy : g.dx);
   const bool scale_mode = outflux > 1.0e-12;
   const double scale = influx / outflux;
   const double deficit = influx - outflux;

@@ -5,6 +5,14 @@
 
 namespace pcfd {
 
+// A product rounded on its own: never fused with the add or subtract it feeds.
+// The library is compiled with FMA contraction on (the solver kernels gain from
+// it); the momentum stencil, the stage combinations, the boundary sums and the
+// rasteriser form their products through rmul so that every product rounds
+// before it is summed, as the reference's array arithmetic does, and stay
+// bit-identical to it.  Products by 0.5, 2 or 4 are exact and need no guard.
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+
 #define PCFD_MAX_BODIES_DEV 8
 
 // Wall order of every boundary pass (pycfd/core/boundary.py:375-379).

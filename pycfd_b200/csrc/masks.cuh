@@ -29,7 +29,7 @@ __device__ __forceinline__ bool shape_inside(const ShapeDev& s, double X, double
   switch (s.kind) {
     case SH_CIRCLE: {
       const double ax = X - s.p0, ay = Y - s.p1;
-      return ax * ax + ay * ay <= s.p2 * s.p2;
+      return rmul(ax, ax) + rmul(ay, ay) <= rmul(s.p2, s.p2);
     }
     case SH_RECTANGLE:
       return (X >= s.p0) && (X <= s.p2) && (Y >= s.p1) && (Y <= s.p3);
@@ -68,9 +68,9 @@ __global__ void k_solid_fraction(ShapeDev s, const double* __restrict__ xf, cons
     const double x0 = xf[i], hx = dxc[i], y0 = yf[j], hy = dyc[j];
     int hits = 0;
     for (int a = 0; a < S; ++a) {
-      const double X = x0 + (((double)a + 0.5) / (double)S) * hx;
+      const double X = x0 + rmul(((double)a + 0.5) / (double)S, hx);
       for (int b = 0; b < S; ++b) {
-        const double Y = y0 + (((double)b + 0.5) / (double)S) * hy;
+        const double Y = y0 + rmul(((double)b + 0.5) / (double)S, hy);
         hits += shape_inside(s, X, Y) ? 1 : 0;
       }
     }

@@ -1,10 +1,10 @@
 // MAC-grid stencils: momentum predictor, divergence, projection correction,
 // Runge-Kutta stage combination, field statistics.
 //
-// Arithmetic follows the reference expression by expression (no FMA
-// contraction: the library is built with -fmad=false), so the predictor, the
-// divergence and the correction are bit-identical to the reference's
-// NumPy/Numba path on the same inputs.
+// Arithmetic follows the reference expression by expression (every product
+// that feeds a sum is formed with rmul, so no multiply-add is fused), so the
+// predictor, the divergence and the correction are bit-identical to the
+// reference's NumPy/Numba path on the same inputs.
 #pragma once
 #include "common.cuh"
 
@@ -20,7 +20,7 @@ struct StageIn {
   const double* b;   // nullptr: plain read of a
   double ca, cb;
   __device__ __forceinline__ double operator[](long k) const {
-    return b ? ca * a[k] + cb * b[k] : a[k];
+    return b ? rmul(ca, a[k]) + rmul(cb, b[k]) : a[k];
   }
 };
 
@@ -32,18 +32,18 @@ __device__ __forceinline__ double rhs_u_core(double u0, double ue, double uw, do
                                              double nu, double blend, double fx) {
   const double u_right = 0.5 * (u0 + ue);
   const double u_left = 0.5 * (uw + u0);
-  double duudx = (u_right * u_right - u_left * u_left) / dx;
+  double duudx = (rmul(u_right, u_right) - rmul(u_left, u_left)) / dx;
   const double u_top = 0.5 * (u0 + un);
   const double v_top = 0.5 * (v_tl + v_tr);
   const double u_bot = 0.5 * (us + u0);
   const double v_bot = 0.5 * (v_bl + v_br);
-  double duvdy = (u_top * v_top - u_bot * v_bot) / dy;
+  double duvdy = (rmul(u_top, v_top) - rmul(u_bot, v_bot)) / dy;
   if (blend > 0.0) {
-    duudx += blend / dx * (fabs(u_right) * (u0 - ue) * 0.5 - fabs(u_left) * (uw - u0) * 0.5);
-    duvdy += blend / dy * (fabs(v_top) * (u0 - un) * 0.5 - fabs(v_bot) * (us - u0) * 0.5);
+    duudx += rmul(blend / dx, rmul(fabs(u_right), u0 - ue) * 0.5 - rmul(fabs(u_left), uw - u0) * 0.5);
+    duvdy += rmul(blend / dy, rmul(fabs(v_top), u0 - un) * 0.5 - rmul(fabs(v_bot), us - u0) * 0.5);
   }
   const double lap = ((uw - 2.0 * u0 + ue) / (dx * dx) + (us - 2.0 * u0 + un) / (dy * dy));
-  return -(duudx + duvdy) + nu * lap + fx;
+  return -(duudx + duvdy) + rmul(nu, lap) + fx;
 }
 
 // v-momentum RHS at a v face from its values (pycfd/core/kernels.py:83-110): the
@@ -54,18 +54,18 @@ __device__ __forceinline__ double rhs_v_core(double v0, double vn, double vs, do
                                              double nu, double blend, double fy) {
   const double v_top = 0.5 * (v0 + vn);
   const double v_bot = 0.5 * (vs + v0);
-  double dvvdy = (v_top * v_top - v_bot * v_bot) / dy;
+  double dvvdy = (rmul(v_top, v_top) - rmul(v_bot, v_bot)) / dy;
   const double u_right = 0.5 * (u_rb + u_rt);
   const double v_right = 0.5 * (v0 + ve);
   const double u_left = 0.5 * (u_lb + u_lt);
   const double v_left = 0.5 * (vw + v0);
-  double duvdx = (u_right * v_right - u_left * v_left) / dx;
+  double duvdx = (rmul(u_right, v_right) - rmul(u_left, v_left)) / dx;
   if (blend > 0.0) {
-    dvvdy += blend / dy * (fabs(v_top) * (v0 - vn) * 0.5 - fabs(v_bot) * (vs - v0) * 0.5);
-    duvdx += blend / dx * (fabs(u_right) * (v0 - ve) * 0.5 - fabs(u_left) * (vw - v0) * 0.5);
+    dvvdy += rmul(blend / dy, rmul(fabs(v_top), v0 - vn) * 0.5 - rmul(fabs(v_bot), vs - v0) * 0.5);
+    duvdx += rmul(blend / dx, rmul(fabs(u_right), v0 - ve) * 0.5 - rmul(fabs(u_left), vw - v0) * 0.5);
   }
   const double lap = ((vw - 2.0 * v0 + ve) / (dx * dx) + (vs - 2.0 * v0 + vn) / (dy * dy));
-  return -(duvdx + dvvdy) + nu * lap + fy;
+  return -(duvdx + dvvdy) + rmul(nu, lap) + fy;
 }
 
 // u-momentum RHS at u-face (m, j), 1<=m<=nx+1, 1<=j<=ny.
@@ -122,8 +122,8 @@ __global__ void k_les_nu(StageIn u, StageIn v, Geo g, double coeff, double* __re
                                les_s12_corner(u, v, ic, jc - 1, ny, g.dx, g.dy) +
                                les_s12_corner(u, v, ic - 1, jc, ny, g.dx, g.dy) +
                                les_s12_corner(u, v, ic, jc, ny, g.dx, g.dy));
-    const double smag = sqrt(2.0 * (s11 * s11) + 2.0 * (s22 * s22) + 4.0 * (s12 * s12));
-    nu_c[e] = g.nu + coeff * smag;
+    const double smag = sqrt(2.0 * rmul(s11, s11) + 2.0 * rmul(s22, s22) + 4.0 * rmul(s12, s12));
+    nu_c[e] = g.nu + rmul(coeff, smag);
   }
 }
 
@@ -151,20 +151,22 @@ __device__ __forceinline__ double rhs_u_les_at(const U& u, const V& v, int m, in
   const double un = u[m * W + j + 1], us = u[m * W + j - 1];
   const double u_right = 0.5 * (u0 + ue);
   const double u_left = 0.5 * (uw + u0);
-  double duudx = (u_right * u_right - u_left * u_left) / dx;
+  double duudx = (rmul(u_right, u_right) - rmul(u_left, u_left)) / dx;
   const double u_top = 0.5 * (u0 + un);
   const double v_top = 0.5 * (v[(m - 1) * WV + j + 1] + v[m * WV + j + 1]);
   const double u_bot = 0.5 * (us + u0);
   const double v_bot = 0.5 * (v[(m - 1) * WV + j] + v[m * WV + j]);
-  double duvdy = (u_top * v_top - u_bot * v_bot) / dy;
+  double duvdy = (rmul(u_top, v_top) - rmul(u_bot, v_bot)) / dy;
   if (blend > 0.0) {
-    duudx += blend / dx * (fabs(u_right) * (u0 - ue) * 0.5 - fabs(u_left) * (uw - u0) * 0.5);
-    duvdy += blend / dy * (fabs(v_top) * (u0 - un) * 0.5 - fabs(v_bot) * (us - u0) * 0.5);
+    duudx += rmul(blend / dx, rmul(fabs(u_right), u0 - ue) * 0.5 - rmul(fabs(u_left), uw - u0) * 0.5);
+    duvdy += rmul(blend / dy, rmul(fabs(v_top), u0 - un) * 0.5 - rmul(fabs(v_bot), us - u0) * 0.5);
   }
   const double dudx_r = (ue - u0) / dx, dudx_l = (u0 - uw) / dx;
-  const double tau_t = nu_k[(long)(m - 1) * WK + j] * ((un - u0) / dy + (v[(long)m * WV + j + 1] - v[(long)(m - 1) * WV + j + 1]) / dx);
-  const double tau_b = nu_k[(long)(m - 1) * WK + j - 1] * ((u0 - us) / dy + (v[(long)m * WV + j] - v[(long)(m - 1) * WV + j]) / dx);
-  const double d = 2.0 * (nu_c[(long)m * W + j] * dudx_r - nu_c[(long)(m - 1) * W + j] * dudx_l) / dx +
+  const double tau_t = rmul(nu_k[(long)(m - 1) * WK + j],
+                            (un - u0) / dy + (v[(long)m * WV + j + 1] - v[(long)(m - 1) * WV + j + 1]) / dx);
+  const double tau_b = rmul(nu_k[(long)(m - 1) * WK + j - 1],
+                            (u0 - us) / dy + (v[(long)m * WV + j] - v[(long)(m - 1) * WV + j]) / dx);
+  const double d = 2.0 * (rmul(nu_c[(long)m * W + j], dudx_r) - rmul(nu_c[(long)(m - 1) * W + j], dudx_l)) / dx +
                    (tau_t - tau_b) / dy;
   return -(duudx + duvdy) + d + fx;
 }
@@ -179,24 +181,24 @@ __device__ __forceinline__ double rhs_v_les_at(const U& u, const V& v, int i, in
   const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
   const double v_top = 0.5 * (v0 + vn);
   const double v_bot = 0.5 * (vs + v0);
-  double dvvdy = (v_top * v_top - v_bot * v_bot) / dy;
+  double dvvdy = (rmul(v_top, v_top) - rmul(v_bot, v_bot)) / dy;
   const double u_right = 0.5 * (u[(i + 1) * W + n - 1] + u[(i + 1) * W + n]);
   const double v_right = 0.5 * (v0 + ve);
   const double u_left = 0.5 * (u[i * W + n - 1] + u[i * W + n]);
   const double v_left = 0.5 * (vw + v0);
-  double duvdx = (u_right * v_right - u_left * v_left) / dx;
+  double duvdx = (rmul(u_right, v_right) - rmul(u_left, v_left)) / dx;
   if (blend > 0.0) {
-    dvvdy += blend / dy * (fabs(v_top) * (v0 - vn) * 0.5 - fabs(v_bot) * (vs - v0) * 0.5);
-    duvdx += blend / dx * (fabs(u_right) * (v0 - ve) * 0.5 - fabs(u_left) * (vw - v0) * 0.5);
+    dvvdy += rmul(blend / dy, rmul(fabs(v_top), v0 - vn) * 0.5 - rmul(fabs(v_bot), vs - v0) * 0.5);
+    duvdx += rmul(blend / dx, rmul(fabs(u_right), v0 - ve) * 0.5 - rmul(fabs(u_left), vw - v0) * 0.5);
   }
   // corners (i, n-1) and (i-1, n-1) of the v face
-  const double tau_r = nu_k[(long)i * WK + n - 1] *
-                       ((u[(long)(i + 1) * W + n] - u[(long)(i + 1) * W + n - 1]) / dy + (ve - v0) / dx);
-  const double tau_l = nu_k[(long)(i - 1) * WK + n - 1] *
-                       ((u[(long)i * W + n] - u[(long)i * W + n - 1]) / dy + (v0 - vw) / dx);
+  const double tau_r = rmul(nu_k[(long)i * WK + n - 1],
+                            (u[(long)(i + 1) * W + n] - u[(long)(i + 1) * W + n - 1]) / dy + (ve - v0) / dx);
+  const double tau_l = rmul(nu_k[(long)(i - 1) * WK + n - 1],
+                            (u[(long)i * W + n] - u[(long)i * W + n - 1]) / dy + (v0 - vw) / dx);
   const double dvdy_t = (vn - v0) / dy, dvdy_b = (v0 - vs) / dy;
   const double d = (tau_r - tau_l) / dx +
-                   2.0 * (nu_c[(long)i * W + n] * dvdy_t - nu_c[(long)i * W + n - 1] * dvdy_b) / dy;
+                   2.0 * (rmul(nu_c[(long)i * W + n], dvdy_t) - rmul(nu_c[(long)i * W + n - 1], dvdy_b)) / dy;
   return -(duvdx + dvvdy) + d + fy;
 }
 
@@ -227,14 +229,14 @@ __global__ void k_predictor_les(StageIn u, StageIn v, double* __restrict__ us, d
     const long k = (long)i * (ny + 2) + j;
     double val = u[k];
     if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-      val = val + dt * rhs_u_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k);
+      val = val + rmul(dt, rhs_u_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k));
     us[k] = val;
   }
   if (i < nx + 2 && j < ny + 3) {
     const long k = (long)i * (ny + 3) + j;
     double val = v[k];
     if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-      val = val + dt * rhs_v_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k);
+      val = val + rmul(dt, rhs_v_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k));
     vs[k] = val;
   }
 }
@@ -264,14 +266,14 @@ __global__ void k_predictor(StageIn u, StageIn v, double* __restrict__ us, doubl
     const long k = (long)i * (ny + 2) + j;
     double val = u[k];
     if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-      val = val + dt * rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx);
+      val = val + rmul(dt, rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx));
     us[k] = val;
   }
   if (i < nx + 2 && j < ny + 3) {
     const long k = (long)i * (ny + 3) + j;
     double val = v[k];
     if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-      val = val + dt * rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy);
+      val = val + rmul(dt, rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy));
     vs[k] = val;
   }
 }
