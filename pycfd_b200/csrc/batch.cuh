@@ -323,6 +323,12 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
 #endif
 constexpr int kBStripRows = PCFD_BSTRIP_ROWS;
 constexpr int kBStripItems = 16;
+// Resident blocks per SM the strip kernels are compiled for (register bound
+// 65536 / (256 x this)); 1 leaves the register count to the compiler.
+#ifndef PCFD_BSTRIP_MINB
+#define PCFD_BSTRIP_MINB 1
+#endif
+#define B_STRIP_KERNEL __global__ void __launch_bounds__(kBThreads, PCFD_BSTRIP_MINB)
 
 // op(k, i, j): the operand at cell (i, j), k = i*ny + j (issues its loads; k is
 // always a valid cell).  load(u, c): the per-cell loads of body row u (c valid;
@@ -470,7 +476,7 @@ __global__ void k_b_set_dt(const BProb<T>* __restrict__ probs, int nprob, double
 constexpr int kBPredCols = 30;   // output columns per warp segment (32 lanes, one halo lane each side)
 
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_predictor(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_predictor(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, int src_a,
                                                             int src_b, double ca, double cb, int dst,
                                                             BShared sh) {
@@ -561,7 +567,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_boundary(const BProb<T>* __rest
 // its fluid mean (pycfd/core/solver.py:659-661, pycfd/core/pressure.py:300-308).
 // Warp strips: the four face values of each of a thread's cells loaded first.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_div_rhs(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_div_rhs(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int arr,
                                                           BShared sh) {
   const int2 e = map[blockIdx.x];
@@ -663,7 +669,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_combine(const BProb<T>* __restr
 // b <- b - mean (solvable rows), r = b - A x from the warm start x, norms and
 // the convergence test before the first pass (scipy cg, pressure.py:300-308).
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_rhs_init(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_rhs_init(const BProb<T>* __restrict__ probs,
                                                            int nprob, const int2* __restrict__ map,
                                                            double tol, int maxiter, BShared sh,
                                                            LoopCtl loop) {
@@ -727,7 +733,7 @@ __device__ __forceinline__ T* b_pdir(const BProb<T>& P, int it) {
 
 // p = (z - mean z) + beta p_old on solvable rows, q = A p, p.q -> alpha.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
                                                         const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -770,7 +776,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_pq(const BProb<T>* __restric
 // x += alpha p, r -= alpha q; ||r||^2 and sum(r); the next pass's convergence
 // test; launch-wide loop decision.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
+B_STRIP_KERNEL k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
                                                         const int2* __restrict__ map, int maxiter,
                                                         BShared sh, LoopCtl loop) {
   const int2 e = map[blockIdx.x];
@@ -824,7 +830,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_cg_xr(const BProb<T>* __restric
 
 // ||b - A x||/||b|| and the fluid mean of x (pycfd/core/pressure.py:310-322).
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, double tol,
                                                                BShared sh) {
   const int2 e = map[blockIdx.x];
@@ -862,7 +868,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_stats(const BProb<T>* __
 
 // x <- x - mean on solvable rows, 0 elsewhere.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_finish_apply(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_finish_apply(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -889,7 +895,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_finish_apply(const BProb<T>* __
 // One refinement pass per problem (see k_ir_residual): r = b - A x in FP64, the
 // outer test ||r|| < tol ||b||, and the inner solve A e = r set up from e = 0.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_ir_residual(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_ir_residual(const BProb<T>* __restrict__ probs,
                                                               int nprob, const int2* __restrict__ map,
                                                               double tol, double inner_tol,
                                                               int max_passes, int first, BShared sh,
@@ -974,7 +980,7 @@ __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShare
 
 // x += e on solvable rows for the problems that ran this pass; count the pass.
 template <class T>
-__global__ void __launch_bounds__(kBThreads) k_b_ir_update(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_ir_update(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, BShared sh) {
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -1011,7 +1017,7 @@ __device__ __forceinline__ T* b_fine_buf(const BProb<T>& P, int sel) {
 }
 
 template <class T, int MODE>
-__global__ void __launch_bounds__(kBThreads) k_b_fine(const BProb<T>* __restrict__ probs,
+B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map, int src, int dst,
                                                        BShared sh) {
@@ -1188,60 +1194,86 @@ __device__ __forceinline__ void b_group_fill(BGroup<T, GS>& G, int g, const BPro
 
 // b_ell_rounds<GS>() rounds of kBThreads / L rows of row block rb of matrix E,
 // for every member of the group.  L lanes per row fixed at compile time (L > 1:
-// row-major entries, L = 1: column-major).
+// row-major entries, L = 1: column-major).  All rounds gather first and store
+// after: the group's vectors are reached through pointers the compiler cannot
+// prove disjoint from the outputs, so a store between rounds would hold back
+// the next round's loads.  A lane takes its entries four at a time, the four
+// (value, column) pairs loaded together and then every member's four gathers,
+// so a row costs one dependent load pair per four entries per lane.
 template <int L, int OP, int GS, class T>
 __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T, GS>& G, const Ell<T>& E,
                                             const T* __restrict__ wd, int d, int rb) {
   constexpr int per = kBThreads / L;
+  constexpr int ROUNDS = b_ell_rounds<GS>();
   const int lane = (int)threadIdx.x & (L - 1);
   const uint8_t* __restrict__ flags = P0.flags;
-  constexpr int ROUNDS = b_ell_rounds<GS>();
-  bool on[GS];
+  const bool fr1 = OP == EO_FRESTRICT && d == 1;   // gathers the projected fine CG residual
+  const T* src[GS];
+  T mr[GS];
 #pragma unroll
-  for (int g = 0; g < GS; ++g) on[g] = G.out[g] != nullptr;
+  for (int g = 0; g < GS; ++g) {
+    const bool on = G.out[g] != nullptr;
+    src[g] = on ? (OP == EO_PRE || fr1 ? G.b[g] : G.src[g]) : nullptr;
+    mr[g] = G.mr[g];
+  }
+  const int K = E.K, n = E.n;
+  T acc[ROUNDS][GS];
 #pragma unroll
   for (int rd = 0; rd < ROUNDS; ++rd) {
     const int row = (rb * ROUNDS + rd) * per + (int)threadIdx.x / L;
-    T acc[GS];
 #pragma unroll
-    for (int g = 0; g < GS; ++g) acc[g] = (T)0;
-    if (row < E.n) {
-      const int kb = L > 1 ? lane : 0;
-#pragma unroll 2
-      for (int k = kb; k < E.K; k += L) {
-        const long at = L > 1 ? (long)row * E.K + k : (long)k * E.n + row;
-        const T v = E.val[at];
-        const int c = E.col[at];
-        if (OP == EO_PRE) {
-          const T w = wd[c];
+    for (int g = 0; g < GS; ++g) acc[rd][g] = (T)0;
+    if (row >= n) continue;
+    for (int k0 = L > 1 ? lane : 0; k0 < K; k0 += 4 * L) {
+      T vv[4];
+      int cc[4];
 #pragma unroll
-          for (int g = 0; g < GS; ++g)
-            if (on[g]) acc[g] += v * (w * G.b[g][c]);
-        } else if ((OP == EO_FRESTRICT && d == 1)) {
-          const bool solv = (flags[c] & F_SOLV) != 0;
+      for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q * L;
+        const bool ok = k < K;
+        const long at = L > 1 ? (long)row * K + k : (long)k * n + row;
+        vv[q] = ok ? E.val[at] : (T)0;
+        cc[q] = ok ? E.col[at] : 0;
+      }
+      T sc[4];   // the per-column factor shared by the group (W on a coarse level)
+      bool sv[4];
 #pragma unroll
-          for (int g = 0; g < GS; ++g)
-            if (on[g]) {
-              const T rc = G.b[g][c];
-              acc[g] += v * (solv ? rc - G.mr[g] : (T)0);
-            }
-        } else {
+      for (int q = 0; q < 4; ++q) {
+        sc[q] = OP == EO_PRE ? wd[cc[q]] : (T)1;
+        sv[q] = fr1 ? (flags[cc[q]] & F_SOLV) != 0 : true;
+      }
 #pragma unroll
-          for (int g = 0; g < GS; ++g)
-            if (on[g]) acc[g] += v * G.src[g][c];
+      for (int g = 0; g < GS; ++g) {
+        if (!src[g]) continue;
+        T gv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gv[q] = src[g][cc[q]];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          T x = gv[q];
+          if (OP == EO_PRE) x = sc[q] * x;
+          if (fr1) x = sv[q] ? x - mr[g] : (T)0;
+          acc[rd][g] += vv[q] * x;
         }
       }
     }
+  }
+#pragma unroll
+  for (int rd = 0; rd < ROUNDS; ++rd)
 #pragma unroll
     for (int g = 0; g < GS; ++g)
 #pragma unroll
-      for (int o = L / 2; o > 0; o >>= 1) acc[g] += __shfl_xor_sync(0xffffffffu, acc[g], o, L);
-    if (lane != 0 || row >= E.n) continue;
+      for (int o = L / 2; o > 0; o >>= 1) acc[rd][g] += __shfl_xor_sync(0xffffffffu, acc[rd][g], o, L);
+  if (lane != 0) return;
+#pragma unroll
+  for (int rd = 0; rd < ROUNDS; ++rd) {
+    const int row = (rb * ROUNDS + rd) * per + (int)threadIdx.x / L;
+    if (row >= n) continue;
 #pragma unroll
     for (int g = 0; g < GS; ++g) {
-      if (!on[g]) continue;
-      const T s = acc[g];
       T* __restrict__ o = G.out[g];
+      if (!o) continue;
+      const T s = acc[rd][g];
       switch (OP) {
         case EO_PROLONG: o[row] = o[row] + s; break;
         case EO_PROLONGW: {
@@ -1249,7 +1281,7 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T, 
           if (d == 0) {
             const uint8_t f = flags[row];
             const int i = row / P0.g.ny, j = row - i * P0.g.ny;
-            const T bfr = (f & F_SOLV) ? G.b[g][row] - G.mr[g] : (T)0;
+            const T bfr = (f & F_SOLV) ? G.b[g][row] - mr[g] : (T)0;
             wb = (T)b_wdinv(P0, f, i, j) * bfr;
           } else {
             wb = wd[row] * G.b[g][row];
