@@ -323,10 +323,19 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
 #endif
 constexpr int kBStripRows = PCFD_BSTRIP_ROWS;
 constexpr int kBStripItems = 16;
+static_assert(kBStripRows % 2 == 0, "the FP64-operand kernels take half-height strips");
+// Strip height of a kernel whose per-cell values are of type T: FP64 values take
+// twice the registers, so their kernels walk half-height strips.
+template <class T>
+__host__ __device__ constexpr int b_rs() { return sizeof(T) == 8 ? kBStripRows / 2 : kBStripRows; }
 // Resident blocks per SM the strip kernels are compiled for (register bound
-// 65536 / (256 x this)); 1 leaves the register count to the compiler.
+// 65536 / (256 x this)).  These kernels are latency-bound, and more resident
+// blocks overlap one block's loads with another's reduction: on the 256-cavity
+// batch, 2 blocks per SM (the compiler's own 128 registers) step in 27.1 ms,
+// 4 blocks per SM (64 registers, small spills) in 26.5 ms with the coarse-level
+// kernels unchanged.
 #ifndef PCFD_BSTRIP_MINB
-#define PCFD_BSTRIP_MINB 1
+#define PCFD_BSTRIP_MINB 4
 #endif
 #define B_STRIP_KERNEL __global__ void __launch_bounds__(kBThreads, PCFD_BSTRIP_MINB)
 
@@ -335,13 +344,18 @@ constexpr int kBStripItems = 16;
 // the values unused past the grid).  body(u, c, i, j, centre, west, east,
 // south, north).  STENCIL = false: no operand (pointwise kernels); body gets
 // zeros.
-template <bool STENCIL, class T, class Op, class Load, class Body>
+// RS: the strip height of the calling kernel (kBStripRows or a divisor of it).
+// A chunk covers the same cells whatever RS is: kBStripItems strips of
+// kBStripRows rows, that is kBStripItems * kBStripRows / RS strips of RS rows.
+template <bool STENCIL, class T, int RS, class Op, class Load, class Body>
 __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load load, Body body) {
-  constexpr int RS = kBStripRows;
+  static_assert(kBStripRows % RS == 0, "strip height must divide kBStripRows");
+  constexpr int IPC = kBStripItems * (kBStripRows / RS);
   const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
   const int nx = V.g.nx, ny = V.g.ny;
-  const int it1 = min(V.items, (chunk + 1) * kBStripItems);
-  for (int it = chunk * kBStripItems + warp; it < it1; it += kBThreads / 32) {
+  const int items = V.segs * ((nx + RS - 1) / RS);
+  const int it1 = min(items, (chunk + 1) * IPC);
+  for (int it = chunk * IPC + warp; it < it1; it += kBThreads / 32) {
     const int strip = it / V.segs, seg = it - strip * V.segs;
     const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
     const bool jv = j < ny;
@@ -570,6 +584,7 @@ template <class T>
 B_STRIP_KERNEL k_b_div_rhs(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int arr,
                                                           BShared sh) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -582,9 +597,9 @@ B_STRIP_KERNEL k_b_div_rhs(const BProb<T>* __restrict__ probs,
   double* __restrict__ b = P.b;
   const double dt = P.S[S_DT];
   double acc[1] = {0.0};
-  uint8_t fv[kBStripRows];
-  double ue[kBStripRows], uw[kBStripRows], vn[kBStripRows], vs[kBStripRows];
-  b_strips<false, double>(
+  uint8_t fv[RS];
+  double ue[RS], uw[RS], vn[RS], vs[RS];
+  b_strips<false, double, RS>(
       V, e.y, [](int, int, int) { return 0.0; },
       [&](int q, int c) {
         const int i = c / g.ny, j = c - i * g.ny;
@@ -673,6 +688,7 @@ B_STRIP_KERNEL k_b_rhs_init(const BProb<T>* __restrict__ probs,
                                                            int nprob, const int2* __restrict__ map,
                                                            double tol, int maxiter, BShared sh,
                                                            LoopCtl loop) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_frozen(sh, e.x)) {
@@ -684,9 +700,9 @@ B_STRIP_KERNEL k_b_rhs_init(const BProb<T>* __restrict__ probs,
     double* __restrict__ b = P.b;
     T* __restrict__ r = P.r;
     double acc[3] = {0, 0, 0};
-    uint8_t fv[kBStripRows];
-    double bv[kBStripRows];
-    b_strips<true, double>(
+    uint8_t fv[RS];
+    double bv[RS];
+    b_strips<true, double, RS>(
         V, e.y, [&](int k, int, int) { return (double)xs[k]; },
         [&](int q, int c) {
           fv[q] = flags[c];
@@ -735,6 +751,7 @@ __device__ __forceinline__ T* b_pdir(const BProb<T>& P, int it) {
 template <class T>
 B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
                                                         const int2* __restrict__ map, BShared sh) {
+  constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
@@ -759,8 +776,8 @@ B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
     return pk * tb + z;
   };
   double acc[1] = {0.0};
-  uint8_t fv[kBStripRows];
-  b_strips<true, T>(V, e.y, pval, [&](int u, int c) { fv[u] = flags[c]; },
+  uint8_t fv[RS];
+  b_strips<true, T, RS>(V, e.y, pval, [&](int u, int c) { fv[u] = flags[c]; },
                     [&](int u, int c, int i, int j, T pc, T pw, T pe, T ps, T pnn) {
                       const T qc = b_apply5<T>(V, fv[u], i, j, pc, pw, pe, ps, pnn);
                       pn[c] = pc;
@@ -779,6 +796,7 @@ template <class T>
 B_STRIP_KERNEL k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
                                                         const int2* __restrict__ map, int maxiter,
                                                         BShared sh, LoopCtl loop) {
+  constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_solving(sh, e.x)) {
@@ -791,9 +809,9 @@ B_STRIP_KERNEL k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
     T* __restrict__ xs = P.xs;
     T* __restrict__ r = P.r;
     double acc[2] = {0, 0};
-    T pv[kBStripRows], xv[kBStripRows], rv[kBStripRows], qv[kBStripRows];
-    uint8_t fv[kBStripRows];
-    b_strips<false, T>(
+    T pv[RS], xv[RS], rv[RS], qv[RS];
+    uint8_t fv[RS];
+    b_strips<false, T, RS>(
         V, e.y, [](int, int, int) { return (T)0; },
         [&](int u, int c) {
           pv[u] = pn[c];
@@ -833,6 +851,7 @@ template <class T>
 B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, double tol,
                                                                BShared sh) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -843,9 +862,9 @@ B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
   const double* __restrict__ b = P.b;
   const uint8_t* __restrict__ flags = P.flags;
   double acc[2] = {0, 0};
-  uint8_t fv[kBStripRows];
-  double bv[kBStripRows];
-  b_strips<true, double>(
+  uint8_t fv[RS];
+  double bv[RS];
+  b_strips<true, double, RS>(
       V, e.y, [&](int k, int, int) { return zero ? 0.0 : x[k]; },
       [&](int q, int c) {
         fv[q] = flags[c];
@@ -870,6 +889,7 @@ B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
 template <class T>
 B_STRIP_KERNEL k_b_finish_apply(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, BShared sh) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -878,9 +898,9 @@ B_STRIP_KERNEL k_b_finish_apply(const BProb<T>* __restrict__ probs,
   const double m = P.S[S_MEAN_X];
   double* __restrict__ x = P.x;
   const uint8_t* __restrict__ flags = P.flags;
-  uint8_t fv[kBStripRows];
-  double xv[kBStripRows];
-  b_strips<false, double>(
+  uint8_t fv[RS];
+  double xv[RS];
+  b_strips<false, double, RS>(
       V, e.y, [](int, int, int) { return 0.0; },
       [&](int q, int c) {
         fv[q] = flags[c];
@@ -900,6 +920,7 @@ B_STRIP_KERNEL k_b_ir_residual(const BProb<T>* __restrict__ probs,
                                                               double tol, double inner_tol,
                                                               int max_passes, int first, BShared sh,
                                                               LoopCtl outer) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_frozen(sh, e.x) && (first || !P.I[I_IR_DONE])) {
@@ -912,9 +933,9 @@ B_STRIP_KERNEL k_b_ir_residual(const BProb<T>* __restrict__ probs,
     T* __restrict__ r = P.r;
     T* __restrict__ xs = P.xs;
     double acc[3] = {0, 0, 0};
-    uint8_t fv[kBStripRows];
-    double bv[kBStripRows];
-    b_strips<true, double>(
+    uint8_t fv[RS];
+    double bv[RS];
+    b_strips<true, double, RS>(
         V, e.y, [&](int k, int, int) { return x[k]; },
         [&](int q, int c) {
           fv[q] = flags[c];
@@ -982,6 +1003,7 @@ __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShare
 template <class T>
 B_STRIP_KERNEL k_b_ir_update(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, BShared sh) {
+  constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x) || P.I[I_IR_DONE]) return;
@@ -989,10 +1011,10 @@ B_STRIP_KERNEL k_b_ir_update(const BProb<T>* __restrict__ probs,
   double* __restrict__ x = P.x;
   const T* __restrict__ xs = P.xs;
   const uint8_t* __restrict__ flags = P.flags;
-  uint8_t fv[kBStripRows];
-  double xv[kBStripRows];
-  T ev[kBStripRows];
-  b_strips<false, double>(
+  uint8_t fv[RS];
+  double xv[RS];
+  T ev[RS];
+  b_strips<false, double, RS>(
       V, e.y, [](int, int, int) { return 0.0; },
       [&](int q, int c) {
         fv[q] = flags[c];
@@ -1021,6 +1043,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map, int src, int dst,
                                                        BShared sh) {
+  constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
@@ -1034,15 +1057,15 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
   T* __restrict__ xo = b_fine_buf(P, dst);
   T* __restrict__ lres0 = P.lres[0];
   double acc[2] = {0, 0};
-  uint8_t fv[kBStripRows];
-  T rv[kBStripRows];
+  uint8_t fv[RS];
+  T rv[RS];
   auto load = [&](int u, int c) {
     fv[u] = flags[c];
     rv[u] = r[c];
   };
   auto bfv = [&](int u) -> T { return (fv[u] & F_SOLV) ? rv[u] - mr : (T)0; };   // right-hand side at the cell
   if (MODE == FM_WDB) {
-    b_strips<false, T>(V, e.y, [](int, int, int) { return (T)0; }, load,
+    b_strips<false, T, RS>(V, e.y, [](int, int, int) { return (T)0; }, load,
                        [&](int u, int c, int i, int j, T, T, T, T, T) {
                          xo[c] = (T)b_wdinv(V, fv[u], i, j) * bfv(u);
                        });
@@ -1054,13 +1077,13 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
       const T bk = (fk & F_SOLV) ? rk - mr : (T)0;
       return (T)b_wdinv(V, fk, ii, jj) * bk;
     };
-    b_strips<true, T>(V, e.y, xw, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
+    b_strips<true, T, RS>(V, e.y, xw, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
       xo[c] = xc;
       lres0[c] = bfv(u) - b_apply5<T>(V, fv[u], i, j, xc, xw_, xe, xs_, xn);
     });
   } else {
     auto xv = [&](int k, int, int) -> T { return x[k]; };
-    b_strips<true, T>(V, e.y, xv, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
+    b_strips<true, T, RS>(V, e.y, xv, load, [&](int u, int c, int i, int j, T xc, T xw_, T xe, T xs_, T xn) {
       const uint8_t f = fv[u];
       if (MODE == FM_RESID) {
         lres0[c] = bfv(u) - b_apply5<T>(V, f, i, j, xc, xw_, xe, xs_, xn);
@@ -1310,8 +1333,14 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T, 
 
 // One ELL op at depth d over the map's (structure, row block x 1024 + group)
 // entries.  Members: sprobs[H.sp0 + group * GS + g], g < GS.
+// Resident blocks per SM of the coarse-level ELL kernels: the same latency
+// argument; 2 / 4 / 5 / 6 / 8 blocks per SM step the batch in 26.5 / 21.2 /
+// 19.8 / 20.1 / 20.1 ms (strip kernels at 4).
+#ifndef PCFD_BELL_MINB
+#define PCFD_BELL_MINB 5
+#endif
 template <class T, int OP, int GS>
-__global__ void __launch_bounds__(kBThreads) k_b_ellg(const BProb<T>* __restrict__ probs,
+__global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map,
                                                        const int* __restrict__ sprobs, int d, int src,
