@@ -90,7 +90,10 @@ typedef struct {
 
 typedef struct {
     int nx, ny;
-    double dx, dy, nu;
+    double dx, dy, nu;                        /* dx, dy: the uniform spacing; on a stretched
+                                                 mesh the smallest cell width / height (what
+                                                 the time-step limits answer to,
+                                                 timestepper.py:91-119)                */
     double body_fx, body_fy;                  /* config.body_force          */
     int bc_kind[4];                           /* left, right, bottom, top   */
     double bc_velocity[4];
@@ -134,6 +137,14 @@ typedef struct {
     int use_les;                              /* config.use_les: Smagorinsky closure, viscous
                                                  term in stress-divergence form   */
     double les_coeff;                         /* (Cs Delta)^2, Delta = sqrt(dx dy) */
+    const double* metrics;                    /* stretched mesh (pycfd/core/mesh.py:122-218):
+                                                 5 nx + 5 ny + 11 doubles, hx[nx], hy[ny],
+                                                 hxu[nx+1], hyv[ny+1], hx_ext[nx+2],
+                                                 hy_ext[ny+2], wx[nx+1], wy[ny+1],
+                                                 hxu*vbar[nx+1], hyv*vbar[ny+1], vbar;
+                                                 NULL on a uniform mesh (dx, dy used) */
+    double outlet_width;                      /* stretched mesh: summed widths of the
+                                                 outlet walls' faces (boundary.py:480-483) */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */
@@ -190,6 +201,13 @@ int pycfd_momentum_rhs(const double* u, const double* v, int nx, int ny, double 
 int pycfd_momentum_rhs_les(const double* u, const double* v, int nx, int ny, double dx, double dy, double nu,
                            double les_coeff, double blend, double fx, double fy, double* nu_c, double* nu_corner,
                            double* rhs_u, double* rhs_v, void* stream);
+
+/* The momentum RHS and the divergence on the solver's own mesh, uniform or
+ * stretched (replaces ProjectionSolver.momentum_rhs, pycfd/core/solver.py:500-529,
+ * and .divergence, :530-543, on the array path; laminar).  Shapes as above. */
+int pycfd_solver_momentum_rhs(pycfd_solver* s, const double* u, const double* v, double blend,
+                              double* rhs_u, double* rhs_v, void* stream);
+int pycfd_solver_divergence(pycfd_solver* s, const double* u, const double* v, double* out, void* stream);
 
 int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy,
                      double* out, void* stream);

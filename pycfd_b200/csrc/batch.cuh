@@ -670,11 +670,11 @@ __global__ void __launch_bounds__(kBThreads) k_b_combine(const BProb<T>* __restr
     B_TILE_EXT(P, tile_, nx + 3, ny + 3) {
       if (j < ny + 2) {
         const long k = (long)i * (ny + 2) + j;
-        P.u[k] = ca * P.u[k] + cb * bu[k];
+        P.u[k] = rmul(ca, P.u[k]) + rmul(cb, bu[k]);
       }
       if (i < nx + 2) {
         const long k = (long)i * (ny + 3) + j;
-        P.v[k] = ca * P.v[k] + cb * bv[k];
+        P.v[k] = rmul(ca, P.v[k]) + rmul(cb, bv[k]);
       }
     }
   }

@@ -29,6 +29,11 @@ struct BcTable {
   int n_bodies;                      // 0: one total only
   int has_outlet;
   double area;                       // cell area dx*dy
+  // stretched mesh: the packed metrics (nullptr when uniform), the grid, and the
+  // summed widths of the outlet walls' faces (pycfd/core/boundary.py:480-483)
+  const double* met;
+  int nx, ny;
+  double outlet_width;
 };
 
 struct LineRef {
@@ -138,17 +143,25 @@ __device__ void bc_mass_balance(double* u, double* v, const Geo& g, const BcTabl
     const int n_face = low ? 1 : (axis == 0 ? nx : ny) + 1;
     const int n = axis == 0 ? ny : nx;
     double s = 0.0;
-    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
-      s += axis == 0 ? u[(long)n_face * WU + k] : v[(long)k * WV + n_face];
+    if (g.met) {   // a stretched wall's faces differ in width: sum face * width
+      const Metrics M(g);
+      for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+        s += axis == 0 ? rmul(u[(long)n_face * WU + k], M.hy(k - 1)) : rmul(v[(long)k * WV + n_face], M.hx(k - 1));
+    } else {
+      for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x)
+        s += axis == 0 ? u[(long)n_face * WU + k] : v[(long)k * WV + n_face];
+    }
     s = block_sum_bcast(s);
     const double width = axis == 0 ? g.dy : g.dx;
-    const double flux_out = (low ? -1.0 : 1.0) * rmul(s, width);
+    const double flux_out = (low ? -1.0 : 1.0) * (g.met ? s : rmul(s, width));
     if (T.kind[w] == BC_OUTLET) outflux += flux_out;
     else influx -= flux_out;
   }
   double total = 0.0;
-  for (int w = 0; w < 4; ++w)
-    if (T.kind[w] == BC_OUTLET) total += rmul((double)(w < 2 ? ny : nx), w < 2 ? g.dy : g.dx);
+  if (g.met) total = T.outlet_width;
+  else
+    for (int w = 0; w < 4; ++w)
+      if (T.kind[w] == BC_OUTLET) total += rmul((double)(w < 2 ? ny : nx), w < 2 ? g.dy : g.dx);
   const bool scale_mode = outflux > 1.0e-12;
   const double scale = influx / outflux;
   const double deficit = influx - outflux;
@@ -167,6 +180,28 @@ __device__ void bc_mass_balance(double* u, double* v, const Geo& g, const BcTabl
   __syncthreads();
 }
 
+// The momentum a masked face carries per unit of the uniform cell area (uniform
+// mesh: the face value; the sum is scaled by the area after the reduction), or
+// weighted by its control volume on a stretched mesh: hxu[m-1] hy[j-1] behind
+// u face (m, j), hx[i-1] hyv[n-1] behind v face (i, n)
+// (pycfd/core/solver.py:265-274, :198-207).
+__device__ __forceinline__ double bc_momentum_u(const double* u, const BcTable& T, int idx) {
+  if (!T.met) return u[idx];
+  const int W = T.ny + 2, m = idx / W, j = idx - m * W;
+  const double* p = T.met;
+  const int nx = T.nx, ny = T.ny;
+  const double area = rmul(p[nx + ny + (m - 1)], p[nx + (j - 1)]);   // hxu[m-1] * hy[j-1]
+  return rmul(u[idx], area);
+}
+__device__ __forceinline__ double bc_momentum_v(const double* v, const BcTable& T, int idx) {
+  if (!T.met) return v[idx];
+  const int W = T.ny + 3, i = idx / W, n = idx - i * W;
+  const double* p = T.met;
+  const int nx = T.nx, ny = T.ny;
+  const double area = rmul(p[i - 1], p[2 * nx + ny + 1 + (n - 1)]);   // hx[i-1] * hyv[n-1]
+  return rmul(v[idx], area);
+}
+
 // Direct forcing (pycfd/core/solver.py:553-599): sum the masked faces for the
 // reaction force (when dt is given), then zero them.  Body b owns the list
 // entries [body_*_start[b], body_*_start[b+1]).
@@ -174,25 +209,25 @@ __device__ void bc_mask(double* u, double* v, const BcTable& T, double* S, int m
   if (mode != OP_MASK_NONE) {
     const double dt = S[S_DT];
     double su = 0.0, sv = 0.0;
-    for (int k = threadIdx.x; k < T.n_mask_u; k += blockDim.x) su += u[T.mask_u[k]];
-    for (int k = threadIdx.x; k < T.n_mask_v; k += blockDim.x) sv += v[T.mask_v[k]];
+    for (int k = threadIdx.x; k < T.n_mask_u; k += blockDim.x) su += bc_momentum_u(u, T, T.mask_u[k]);
+    for (int k = threadIdx.x; k < T.n_mask_v; k += blockDim.x) sv += bc_momentum_v(v, T, T.mask_v[k]);
     su = block_sum_bcast(su);
     sv = block_sum_bcast(sv);
     if (threadIdx.x == 0) {
-      const double fx = su * T.area / dt, fy = sv * T.area / dt;
+      const double fx = T.met ? su / dt : su * T.area / dt, fy = T.met ? sv / dt : sv * T.area / dt;
       if (mode == OP_MASK_RESET) { S[S_FX] = fx; S[S_FY] = fy; }
       else { S[S_FX] += fx; S[S_FY] += fy; }
     }
     for (int b = 0; b < T.n_bodies; ++b) {
       double bu = 0.0, bv = 0.0;
       for (int k = T.body_u_start[b] + threadIdx.x; k < T.body_u_start[b + 1]; k += blockDim.x)
-        bu += u[T.mask_u[k]];
+        bu += bc_momentum_u(u, T, T.mask_u[k]);
       for (int k = T.body_v_start[b] + threadIdx.x; k < T.body_v_start[b + 1]; k += blockDim.x)
-        bv += v[T.mask_v[k]];
+        bv += bc_momentum_v(v, T, T.mask_v[k]);
       bu = block_sum_bcast(bu);
       bv = block_sum_bcast(bv);
       if (threadIdx.x == 0) {
-        const double fx = bu * T.area / dt, fy = bv * T.area / dt;
+        const double fx = T.met ? bu / dt : bu * T.area / dt, fy = T.met ? bv / dt : bv * T.area / dt;
         if (mode == OP_MASK_RESET) { S[S_BODY_FX + b] = fx; S[S_BODY_FY + b] = fy; }
         else { S[S_BODY_FX + b] += fx; S[S_BODY_FY + b] += fy; }
       }

@@ -58,7 +58,41 @@ struct Geo {
   double pref_w, pref_e, pref_s, pref_n;
   double cx, cy;                // 1/dx^2, 1/dy^2
   int n_fluid;                  // number of solvable cells
+  const double* met;            // stretched mesh: packed metrics (Metrics below); nullptr when uniform
 };
+
+// The spacings of a stretched mesh (pycfd/core/mesh.py:122-218), packed in this
+// order by MeshMetrics.device_block: hx[nx], hy[ny] (cell widths / heights),
+// hxu[nx+1], hyv[ny+1] (centre-to-centre distance across each face, ghost
+// mirroring its neighbour), hx_ext[nx+2], hy_ext[ny+2] (widths with that ghost),
+// wx[nx+1], wy[ny+1] (upper-node weight of a corner interpolant), the Poisson
+// face denominators hxu*vbar[nx+1], hyv*vbar[ny+1] and vbar, the mean cell area
+// (pycfd/core/pressure.py:193-207).
+struct Metrics {
+  const double* p;
+  int nx, ny;
+  __device__ __forceinline__ Metrics(const Geo& g) : p(g.met), nx(g.nx), ny(g.ny) {}
+  __device__ __forceinline__ double hx(int i) const { return p[i]; }
+  __device__ __forceinline__ double hy(int j) const { return p[nx + j]; }
+  __device__ __forceinline__ double hxu(int f) const { return p[nx + ny + f]; }
+  __device__ __forceinline__ double hyv(int f) const { return p[2 * nx + ny + 1 + f]; }
+  __device__ __forceinline__ double hx_ext(int k) const { return p[2 * nx + 2 * ny + 2 + k]; }
+  __device__ __forceinline__ double hy_ext(int k) const { return p[3 * nx + 2 * ny + 4 + k]; }
+  __device__ __forceinline__ double wx(int f) const { return p[3 * nx + 3 * ny + 6 + f]; }
+  __device__ __forceinline__ double wy(int f) const { return p[4 * nx + 3 * ny + 7 + f]; }
+  __device__ __forceinline__ double axv(int f) const { return p[4 * nx + 4 * ny + 8 + f]; }
+  __device__ __forceinline__ double ayv(int f) const { return p[5 * nx + 4 * ny + 9 + f]; }
+  __device__ __forceinline__ double vbar() const { return p[5 * nx + 5 * ny + 10]; }
+  // Poisson coefficients of the faces around cell (i, j): face area over the
+  // centre distance and the mean cell area, the reference's expressions.
+  __device__ __forceinline__ double cw(int i, int j) const { return hy(j) / axv(i); }
+  __device__ __forceinline__ double ce(int i, int j) const { return hy(j) / axv(i + 1); }
+  __device__ __forceinline__ double cs(int i, int j) const { return hx(i) / ayv(j); }
+  __device__ __forceinline__ double cn(int i, int j) const { return hx(i) / ayv(j + 1); }
+  // Row scale of the Poisson system: cell area over the mean cell area.
+  __device__ __forceinline__ double row_scale(int i, int j) const { return __dmul_rn(hx(i), hy(j)) / vbar(); }
+};
+inline int metrics_count(int nx, int ny) { return 5 * nx + 5 * ny + 11; }
 
 // Reduction workspace: one row of NV partials per block plus a ticket counter.
 struct RedBuf {
@@ -183,6 +217,19 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], RedBuf rb, Fin fin)
 __device__ __forceinline__ double fine_diag(uint8_t f, int i, int j, const Geo& g) {
   if (!(f & F_SOLV)) return 1.0;
   double d = 0.0;
+  if (g.met) {   // stretched: per-face coefficients, the same order
+    const Metrics M(g);
+    const double cw = M.cw(i, j), ce = M.ce(i, j), cs = M.cs(i, j), cn = M.cn(i, j);
+    if (f & F_W) d -= cw;
+    if (g.dir_w && i == 0) d -= 2.0 * cw;
+    if (f & F_E) d -= ce;
+    if (g.dir_e && i == g.nx - 1) d -= 2.0 * ce;
+    if (f & F_S) d -= cs;
+    if (g.dir_s && j == 0) d -= 2.0 * cs;
+    if (f & F_N) d -= cn;
+    if (g.dir_n && j == g.ny - 1) d -= 2.0 * cn;
+    return d;
+  }
   if (f & F_W) d -= g.cx;
   if (g.dir_w && i == 0) d -= 2.0 * g.cx;
   if (f & F_E) d -= g.cx;
@@ -199,10 +246,18 @@ __device__ __forceinline__ double fine_diag(uint8_t f, int i, int j, const Geo& 
 __device__ __forceinline__ double fine_bc(uint8_t f, int i, int j, const Geo& g) {
   if (!(f & F_SOLV)) return 0.0;
   double b = 0.0;
-  if (g.dir_w && i == 0) b -= 2.0 * g.cx * g.pref_w;
-  if (g.dir_e && i == g.nx - 1) b -= 2.0 * g.cx * g.pref_e;
-  if (g.dir_s && j == 0) b -= 2.0 * g.cy * g.pref_s;
-  if (g.dir_n && j == g.ny - 1) b -= 2.0 * g.cy * g.pref_n;
+  if (g.met) {
+    const Metrics M(g);
+    if (g.dir_w && i == 0) b -= rmul(2.0 * M.cw(i, j), g.pref_w);
+    if (g.dir_e && i == g.nx - 1) b -= rmul(2.0 * M.ce(i, j), g.pref_e);
+    if (g.dir_s && j == 0) b -= rmul(2.0 * M.cs(i, j), g.pref_s);
+    if (g.dir_n && j == g.ny - 1) b -= rmul(2.0 * M.cn(i, j), g.pref_n);
+    return b;
+  }
+  if (g.dir_w && i == 0) b -= rmul(2.0 * g.cx, g.pref_w);
+  if (g.dir_e && i == g.nx - 1) b -= rmul(2.0 * g.cx, g.pref_e);
+  if (g.dir_s && j == 0) b -= rmul(2.0 * g.cy, g.pref_s);
+  if (g.dir_n && j == g.ny - 1) b -= rmul(2.0 * g.cy, g.pref_n);
   return b;
 }
 
@@ -221,6 +276,15 @@ __device__ __forceinline__ int nb_n(int i, int j, const Geo& g) { return i * g.n
 // flat index k = i*ny + j (so neighbour values can be formed on the fly).
 template <class T, class X>
 __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Geo& g, X x) {
+  if (g.met) {
+    const Metrics M(g);
+    T acc = (T)fine_diag(f, i, j, g) * x(c, i, j);
+    if (f & F_W) { const int a = wrap_w(i, g); acc += (T)M.cw(i, j) * x(a * g.ny + j, a, j); }
+    if (f & F_E) { const int a = wrap_e(i, g); acc += (T)M.ce(i, j) * x(a * g.ny + j, a, j); }
+    if (f & F_S) { const int b = wrap_s(j, g); acc += (T)M.cs(i, j) * x(i * g.ny + b, i, b); }
+    if (f & F_N) { const int b = wrap_n(j, g); acc += (T)M.cn(i, j) * x(i * g.ny + b, i, b); }
+    return acc;
+  }
   T acc = (T)fine_diag(f, i, j, g) * x(c, i, j);
   if (f & F_W) { const int a = wrap_w(i, g); acc += (T)g.cx * x(a * g.ny + j, a, j); }
   if (f & F_E) { const int a = wrap_e(i, g); acc += (T)g.cx * x(a * g.ny + j, a, j); }
@@ -342,6 +406,15 @@ __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body
 // order (diagonal, west, east, south, north).
 __device__ __forceinline__ double fine_apply5(uint8_t f, int i, int j, const Geo& g, double c, double w, double e,
                                               double s, double n) {
+  if (g.met) {
+    const Metrics M(g);
+    double acc = fine_diag(f, i, j, g) * c;
+    if (f & F_W) acc += M.cw(i, j) * w;
+    if (f & F_E) acc += M.ce(i, j) * e;
+    if (f & F_S) acc += M.cs(i, j) * s;
+    if (f & F_N) acc += M.cn(i, j) * n;
+    return acc;
+  }
   double acc = fine_diag(f, i, j, g) * c;
   if (f & F_W) acc += g.cx * w;
   if (f & F_E) acc += g.cx * e;

@@ -451,6 +451,7 @@ struct DtControl {
   double blend;
   double steady_tol;  // device loop: stop once max|du|/dt falls below it (0: never)
   int history;        // 1: the step is gated and appends a row to the device history
+  double ke_scale;    // the history's kinetic energy factor: dx dy (uniform), 1 (stretched: integrated per cell)
 };
 
 __device__ __forceinline__ void adaptive_dt_update(double* S, int* I, const DtControl& c) {
@@ -535,7 +536,7 @@ __global__ void k_history_append(double* __restrict__ S, int* __restrict__ I, do
     h[2] = dt;
     h[3] = dt * (umax / c.dx + vmax / c.dy);
     h[4] = S[S_STAT0 + 4];
-    h[5] = S[S_STAT0 + 5] * (c.dx * c.dy);
+    h[5] = S[S_STAT0 + 5] * c.ke_scale;
     h[6] = S[S_RESID];
     h[7] = S[S_FX];
     h[8] = S[S_FY];

@@ -169,6 +169,7 @@ struct pycfd_solver {
   double* hist = nullptr;       // device history of a device-side run loop (kHistRows x kHistCols)
   int les = 0;                  // Smagorinsky closure on
   double les_coeff = 0.0;       // (Cs Delta)^2
+  double* met = nullptr;        // stretched mesh: the packed metrics (Geo::met)
   double* les_nu_c = nullptr;   // (nx+2) x (ny+2) effective viscosity of the current stage
   double* les_nu_k = nullptr;   // (nx+1) x (ny+1) its corner average
   // CUDA-graph recording of whole steps
@@ -1198,6 +1199,12 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->omega = d->sor_omega;
   s->mg_sweeps = std::max(1, d->mg_sweeps);
   s->scheme = d->time_scheme;
+  if (d->metrics) {   // stretched mesh: the packed metrics, read by every stencil through g.met
+    if (d->use_les) return bail(fail(PCFD_E_UNSUPPORTED, "the Smagorinsky closure is provided on uniform meshes"));
+    int mrc;
+    if ((mrc = upload(s, &s->met, d->metrics, (size_t)metrics_count(nx, ny)))) return bail(mrc);
+    g.met = s->met;
+  }
   if (d->use_les) {
     if (!(d->les_coeff >= 0.0)) return bail(fail(PCFD_E_ARG, "les_coeff must be non-negative"));
     s->les = 1;
@@ -1319,6 +1326,10 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->bc.n_mask_u = (int)lu.size();
   s->bc.n_mask_v = (int)lvv.size();
   s->bc.area = d->dx * d->dy;
+  s->bc.met = s->met;
+  s->bc.nx = nx;
+  s->bc.ny = ny;
+  s->bc.outlet_width = d->outlet_width;
   s->bc.has_outlet = 0;
   for (int w = 0; w < 4; ++w) {
     s->bc.kind[w] = K[w];
@@ -1483,6 +1494,26 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   }
   if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(PCFD_E_CUDA, "setup failed"));
   *out = s;
+  return 0;
+}
+
+int pycfd_solver_momentum_rhs(pycfd_solver* s, const double* u, const double* v, double blend, double* rhs_u,
+                              double* rhs_v, void* stream) {
+  if (!s || !u || !v || !rhs_u || !rhs_v) return fail(PCFD_E_ARG, "bad arguments");
+  const Geo& g = s->g;
+  if (s->les) return fail(PCFD_E_UNSUPPORTED, "use pycfd_momentum_rhs_les for the Smagorinsky closure");
+  dim3 blk(TJ, TI), grd((g.ny + 1 + TJ - 1) / TJ, (g.nx + 1 + TI - 1) / TI);
+  if (g.met) k_rhs_str<<<grd, blk, 0, st(stream)>>>(u, v, g, blend, rhs_u, rhs_v);
+  else k_rhs<<<grd, blk, 0, st(stream)>>>(u, v, g.nx, g.ny, g.dx, g.dy, g.nu, blend, g.fx, g.fy, rhs_u, rhs_v);
+  CHECK_LAUNCH();
+  return 0;
+}
+
+int pycfd_solver_divergence(pycfd_solver* s, const double* u, const double* v, double* out, void* stream) {
+  if (!s || !u || !v || !out) return fail(PCFD_E_ARG, "bad arguments");
+  const Geo& g = s->g;
+  k_divergence_g<<<grid_for((long)g.nx * g.ny, 256), 256, 0, st(stream)>>>(u, v, g, out);
+  CHECK_LAUNCH();
   return 0;
 }
 
@@ -1723,6 +1754,7 @@ int pycfd_step_adaptive(pycfd_solver* s, const double* u0, const double* v0, dou
   c.blend = ctl->blend;
   c.steady_tol = ctl->steady_tol;
   c.history = ctl->history ? 1 : 0;
+  c.ke_scale = s->g.met ? 1.0 : s->g.dx * s->g.dy;
   if (c.history && !s->hist) TRY(dalloc(s, &s->hist, (size_t)kHistRows * kHistCols));
   // key: the five addresses plus the control values (recorded into the graph)
   const void* key[5] = {u0, v0, u, v, p};
@@ -2065,7 +2097,7 @@ int pycfd_reduce_fields(pycfd_solver* s, const double* u, const double* v, const
   o->max_du = t[2];
   o->max_dv = t[3];
   o->max_div = t[4];
-  o->kinetic_energy = t[5] * (s->g.dx * s->g.dy);
+  o->kinetic_energy = s->g.met ? t[5] : t[5] * (s->g.dx * s->g.dy);
   o->max_vorticity = t[6];
   o->finite = t[7] == 0.0;
   return 0;

@@ -90,6 +90,67 @@ __device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n,
                     blend, fy);
 }
 
+// ---- stretched mesh (pycfd/core/solver.py:336-466, the array path) ------------
+// Advection in conservative form with corner interpolants weighted by the
+// geometry (u along y with wy, v along x with wx), the donor-cell correction over
+// the same control volumes, and diffusion as a difference of two first
+// derivatives (inner gradients across the flanking cells, outer difference
+// across the face's own control volume).  Same operations, same order as the
+// reference's arrays, so the right-hand side is bit-identical to it.
+template <class U, class V>
+__device__ __forceinline__ double rhs_u_str(const U& u, const V& v, int m, int j, int ny, const Metrics& M,
+                                            double nu, double blend, double fx) {
+  const long W = ny + 2, WV = ny + 3;
+  const double u0 = u[m * W + j], ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
+  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+  const double wxa = M.wx(m - 1);
+  // corner interpolants of u (along y) and v (along x) above and below the face
+  const double uc_t = u0 + rmul(M.wy(j), un - u0);
+  const double uc_b = us + rmul(M.wy(j - 1), u0 - us);
+  const double vt0 = v[(m - 1) * WV + j + 1], vb0 = v[(m - 1) * WV + j];
+  const double vc_t = vt0 + rmul(wxa, v[m * WV + j + 1] - vt0);
+  const double vc_b = vb0 + rmul(wxa, v[m * WV + j] - vb0);
+  const double uu_r = 0.5 * (u0 + ue), uu_l = 0.5 * (uw + u0);
+  const double hxu = M.hxu(m - 1), hy = M.hy(j - 1);
+  double duudx = (rmul(uu_r, uu_r) - rmul(uu_l, uu_l)) / hxu;
+  double duvdy = (rmul(uc_t, vc_t) - rmul(uc_b, vc_b)) / hy;
+  if (blend > 0.0) {
+    duudx += rmul(blend / hxu, rmul(fabs(uu_r), u0 - ue) / 2.0 - rmul(fabs(uu_l), uw - u0) / 2.0);
+    duvdy += rmul(blend / hy, rmul(fabs(vc_t), u0 - un) / 2.0 - rmul(fabs(vc_b), us - u0) / 2.0);
+  }
+  const double gx_hi = (ue - u0) / M.hx_ext(m), gx_lo = (u0 - uw) / M.hx_ext(m - 1);
+  const double gy_hi = (un - u0) / M.hyv(j), gy_lo = (u0 - us) / M.hyv(j - 1);
+  const double d2u = (gx_hi - gx_lo) / hxu + (gy_hi - gy_lo) / hy;
+  return -(duudx + duvdy) + rmul(nu, d2u) + fx;
+}
+
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_str(const U& u, const V& v, int i, int n, int ny, const Metrics& M,
+                                            double nu, double blend, double fy) {
+  const long W = ny + 2, WV = ny + 3;
+  const double v0 = v[i * WV + n], vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
+  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+  const double wyb = M.wy(n - 1);
+  // corner interpolants at the right (i, n-1) and left (i-1, n-1) corners of the face
+  const double ur0 = u[(i + 1) * W + n - 1], ul0 = u[i * W + n - 1];
+  const double uc_r = ur0 + rmul(wyb, u[(i + 1) * W + n] - ur0);
+  const double uc_l = ul0 + rmul(wyb, u[i * W + n] - ul0);
+  const double vc_r = v0 + rmul(M.wx(i), ve - v0);
+  const double vc_l = vw + rmul(M.wx(i - 1), v0 - vw);
+  const double vv_t = 0.5 * (v0 + vn), vv_b = 0.5 * (vs + v0);
+  const double hyv = M.hyv(n - 1), hx = M.hx(i - 1);
+  double dvvdy = (rmul(vv_t, vv_t) - rmul(vv_b, vv_b)) / hyv;
+  double duvdx = (rmul(uc_r, vc_r) - rmul(uc_l, vc_l)) / hx;
+  if (blend > 0.0) {
+    dvvdy += rmul(blend / hyv, rmul(fabs(vv_t), v0 - vn) / 2.0 - rmul(fabs(vv_b), vs - v0) / 2.0);
+    duvdx += rmul(blend / hx, rmul(fabs(uc_r), v0 - ve) / 2.0 - rmul(fabs(uc_l), vw - v0) / 2.0);
+  }
+  const double hx_hi = (ve - v0) / M.hxu(i), hx_lo = (v0 - vw) / M.hxu(i - 1);
+  const double hy_hi = (vn - v0) / M.hy_ext(n), hy_lo = (v0 - vs) / M.hy_ext(n - 1);
+  const double d2v = (hx_hi - hx_lo) / hx + (hy_hi - hy_lo) / hyv;
+  return -(duvdx + dvvdy) + rmul(nu, d2v) + fy;
+}
+
 // ---- Smagorinsky large-eddy closure (pycfd/physics/turbulence.py:25-118) -------
 // Effective viscosity nu + (Cs Delta)^2 |S| on the ghosted cell grid (nx+2, ny+2)
 // and its corner average on (nx+1, ny+1), then the viscous term in
@@ -252,6 +313,18 @@ __global__ void k_rhs(const double* __restrict__ u, const double* __restrict__ v
   if (i < nx && j <= ny) rhs_v[(long)i * (ny + 1) + j] = rhs_v_at(u, v, i + 1, j + 1, ny, dx, dy, nu, blend, fy);
 }
 
+// Stateless RHS of a stretched mesh.
+__global__ void k_rhs_str(const double* __restrict__ u, const double* __restrict__ v, Geo g, double blend,
+                          double* __restrict__ rhs_u, double* __restrict__ rhs_v) {
+  pdl_begin();
+  const int nx = g.nx, ny = g.ny;
+  const Metrics M(g);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i <= nx && j < ny) rhs_u[(long)i * ny + j] = rhs_u_str(u, v, i + 1, j + 1, ny, M, g.nu, blend, g.fx);
+  if (i < nx && j <= ny) rhs_v[(long)i * (ny + 1) + j] = rhs_v_str(u, v, i + 1, j + 1, ny, M, g.nu, blend, g.fy);
+}
+
 // Predictor: us = U + dt*rhs_u on the solvable u-faces, U elsewhere (same for
 // v), where U is the stage input (pycfd/core/solver.py:619-622).  dt and the
 // upwind blend are read from device scalars so a captured step can be replayed.
@@ -266,14 +339,16 @@ __global__ void k_predictor(StageIn u, StageIn v, double* __restrict__ us, doubl
     const long k = (long)i * (ny + 2) + j;
     double val = u[k];
     if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-      val = val + rmul(dt, rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx));
+      val = val + rmul(dt, g.met ? rhs_u_str(u, v, i, j, ny, Metrics(g), g.nu, blend, g.fx)
+                                 : rhs_u_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fx));
     us[k] = val;
   }
   if (i < nx + 2 && j < ny + 3) {
     const long k = (long)i * (ny + 3) + j;
     double val = v[k];
     if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-      val = val + rmul(dt, rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy));
+      val = val + rmul(dt, g.met ? rhs_v_str(u, v, i, j, ny, Metrics(g), g.nu, blend, g.fy)
+                                 : rhs_v_at(u, v, i, j, ny, g.dx, g.dy, g.nu, blend, g.fy));
     vs[k] = val;
   }
 }
@@ -285,12 +360,33 @@ __device__ __forceinline__ double cell_div(const double* u, const double* v, int
          (v[(long)(ci + 1) * WV + cj + 2] - v[(long)(ci + 1) * WV + cj + 1]) / dy;
 }
 
+// The divergence of cell (ci, cj) divided by the cell's own width and height
+// (pycfd/core/solver.py:530-543): hx[ci], hy[cj] on a stretched mesh.
+__device__ __forceinline__ double cell_div_g(const double* u, const double* v, int ci, int cj, const Geo& g) {
+  if (g.met) {
+    const Metrics M(g);
+    return cell_div(u, v, ci, cj, g.ny, M.hx(ci), M.hy(cj));
+  }
+  return cell_div(u, v, ci, cj, g.ny, g.dx, g.dy);
+}
+
 __global__ void k_divergence(const double* __restrict__ u, const double* __restrict__ v, int nx,
                              int ny, double dx, double dy, double* __restrict__ out) {
   pdl_begin();
   for (int i = blockIdx.y * blockDim.y + threadIdx.y; i < nx; i += gridDim.y * blockDim.y)
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < ny; j += gridDim.x * blockDim.x)
       out[(long)i * ny + j] = cell_div(u, v, i, j, ny, dx, dy);
+}
+
+// Divergence on the solver's mesh (uniform or stretched), flat (nx, ny).
+__global__ void k_divergence_g(const double* __restrict__ u, const double* __restrict__ v, Geo g,
+                               double* __restrict__ out) {
+  pdl_begin();
+  const long n = (long)g.nx * g.ny;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c / g.ny), j = (int)(c - (long)i * g.ny);
+    out[c] = cell_div_g(u, v, i, j, g);
+  }
 }
 
 // Poisson right-hand side b = div/dt (+ Dirichlet term), zero on non-solvable
@@ -309,8 +405,9 @@ __global__ void k_div_rhs(const double* __restrict__ u, const double* __restrict
     const uint8_t f = flags[c];
     double val = 0.0;
     if (f & F_SOLV) {
-      const double r = rhs_in ? rhs_in[c] : cell_div(u, v, i, j, g.ny, g.dx, g.dy) / dt;
-      val = r * 1.0 + fine_bc(f, i, j, g);
+      const double r = rhs_in ? rhs_in[c] : cell_div_g(u, v, i, j, g) / dt;
+      // b = rhs * row_scale + bc (pycfd/core/pressure.py:300-308); row_scale is 1 on a uniform mesh
+      val = (g.met ? rmul(r, Metrics(g).row_scale(i, j)) : r * 1.0) + fine_bc(f, i, j, g);
       acc[0] += val;
     }
     b[c] = val;
@@ -434,12 +531,12 @@ __global__ void k_correct(double* __restrict__ u, double* __restrict__ v,
       // u faces [u_lo, u_hi) x [1, ny]: row m = r
       if (r >= g.u_lo && r < g.u_hi && j >= 1 && j <= ny) {
         const long k = (long)r * (ny + 2) + j;
-        u[k] = u[k] - dt * (p_at(x, r, j, g) - p_at(x, r - 1, j, g)) / g.dx;
+        u[k] = u[k] - dt * (p_at(x, r, j, g) - p_at(x, r - 1, j, g)) / (g.met ? Metrics(g).hxu(r - 1) : g.dx);
       }
       // v faces [1, nx] x [v_lo, v_hi): row i = r
       if (r >= 1 && r <= nx && j >= g.v_lo && j < g.v_hi) {
         const long k = (long)r * (ny + 3) + j;
-        v[k] = v[k] - dt * (p_at(x, r, j, g) - p_at(x, r, j - 1, g)) / g.dy;
+        v[k] = v[k] - dt * (p_at(x, r, j, g) - p_at(x, r, j - 1, g)) / (g.met ? Metrics(g).hyv(j - 1) : g.dy);
       }
     }
   }
@@ -450,7 +547,7 @@ __global__ void k_combine(const double* __restrict__ a, const double* __restrict
                           double cb, double* __restrict__ out, long n) {
   pdl_begin();
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
-    out[k] = ca * a[k] + cb * b[k];
+    out[k] = rmul(ca, a[k]) + rmul(cb, b[k]);
 }
 
 // Field statistics: max|u|, max|v| (physical faces), max|du|, max|dv|,
@@ -484,17 +581,22 @@ __global__ void k_field_stats(const double* __restrict__ u, const double* __rest
       if (r < nx && j < ny) {
         const int i = r;
         const bool sol = solid && solid[(long)i * ny + j];
-        if (!sol) acc[4] = fmax(acc[4], fabs(cell_div(u, v, i, j, ny, g.dx, g.dy)));
+        if (!sol) acc[4] = fmax(acc[4], fabs(cell_div_g(u, v, i, j, g)));
         const double uc = 0.5 * (u[(long)(i + 1) * W + j + 1] + u[(long)(i + 2) * W + j + 1]);
         const double vc = 0.5 * (v[(long)(i + 1) * WV + j + 1] + v[(long)(i + 1) * WV + j + 2]);
-        if (!sol) acc[5] += 0.5 * (uc * uc + vc * vc);
+        // kinetic energy density; on a stretched mesh weighted by the cell area here
+        // (the integral), on a uniform one multiplied by dx dy by the reader
+        if (!sol) acc[5] += g.met ? rmul(0.5 * (uc * uc + vc * vc), rmul(Metrics(g).hx(i), Metrics(g).hy(j)))
+                                  : 0.5 * (uc * uc + vc * vc);
         // vorticity at the four corners of the cell (pycfd/analysis/postprocess.py:21-40)
         double w4 = 0.0;
         for (int di = 0; di < 2; ++di)
           for (int dj = 0; dj < 2; ++dj) {
             const int a = i + di, bb = j + dj;
-            const double dvdx = (v[(long)(a + 1) * WV + bb + 1] - v[(long)a * WV + bb + 1]) / g.dx;
-            const double dudy = (u[(long)(a + 1) * W + bb + 1] - u[(long)(a + 1) * W + bb]) / g.dy;
+            const double dvdx = (v[(long)(a + 1) * WV + bb + 1] - v[(long)a * WV + bb + 1]) /
+                                (g.met ? Metrics(g).hxu(a) : g.dx);
+            const double dudy = (u[(long)(a + 1) * W + bb + 1] - u[(long)(a + 1) * W + bb]) /
+                                (g.met ? Metrics(g).hyv(bb) : g.dy);
             w4 += dvdx - dudy;
           }
         acc[6] = fmax(acc[6], fabs(0.25 * w4));

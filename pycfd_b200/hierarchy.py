@@ -36,15 +36,20 @@ class FineOperator:
     singular: bool
     pin: int
     bc_rhs: np.ndarray
+    row_scale: np.ndarray | float = 1.0   # cell area / mean cell area (1.0 on a uniform mesh)
 
 
-def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None) -> FineOperator:
+def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None,
+             widths=None) -> FineOperator:
     """5-point operator over the projected face set (``pycfd/core/pressure.py:110-270``).
 
     Couplings are gathered per face direction with index arithmetic; the
     diagonal accumulates the directions in the order left, right, bottom, top,
-    Dirichlet walls adding ``-2/h^2`` in place, which reproduces the reference's
-    matrix exactly.
+    Dirichlet walls adding ``-2 c`` in place, which reproduces the reference's
+    matrix exactly.  ``widths = (dx_cells, dy_cells)`` of a stretched mesh: each
+    face's coefficient is its area over the centre-to-centre distance and the
+    mean cell area, and the rows carry the cell area over the mean as their
+    scale (``pycfd/core/pressure.py:193-207``).
     """
     n = nx * ny
     fluid = np.ones((nx, ny), bool) if solid is None else ~np.asarray(solid, bool)
@@ -54,9 +59,22 @@ def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None)
     diag = np.zeros((nx, ny))
     bc = np.zeros((nx, ny))
     rows, cols, vals = [], [], []
-    cx, cy = 1.0 / (dx * dx), 1.0 / (dy * dy)
-    for wall, di, dj, c, per in (("left", -1, 0, cx, periodic_x), ("right", 1, 0, cx, periodic_x),
-                                 ("bottom", 0, -1, cy, periodic_y), ("top", 0, 1, cy, periodic_y)):
+    if widths is None:
+        cx, cy = 1.0 / (dx * dx), 1.0 / (dy * dy)
+        coef = (cx, cx, cy, cy)
+        row_scale = 1.0
+    else:
+        dxc, dyc = (np.asarray(w, dtype=float) for w in widths)
+        areas = dxc[:, None] * dyc[None, :]
+        vbar = float(areas.mean())
+        hxu = 0.5 * (np.concatenate(([dxc[0]], dxc)) + np.concatenate((dxc, [dxc[-1]])))
+        hyv = 0.5 * (np.concatenate(([dyc[0]], dyc)) + np.concatenate((dyc, [dyc[-1]])))
+        cxf = dyc[None, :] / (hxu[:, None] * vbar)     # (nx+1, ny), by x-face
+        cyf = dxc[:, None] / (hyv[None, :] * vbar)     # (nx, ny+1), by y-face
+        coef = (cxf[0:nx, :], cxf[1:nx + 1, :], cyf[:, 0:ny], cyf[:, 1:ny + 1])
+        row_scale = (areas / vbar).ravel()
+    for (wall, di, dj, per), c in zip((("left", -1, 0, periodic_x), ("right", 1, 0, periodic_x),
+                                       ("bottom", 0, -1, periodic_y), ("top", 0, 1, periodic_y)), coef):
         ni, nj = ii + di, jj + dj
         inside = (ni >= 0) & (ni < nx) & (nj >= 0) & (nj < ny)
         if per:
@@ -65,7 +83,7 @@ def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None)
         coupled = fluid & inside & fluid[ni, nj]
         rows.append(cid[coupled])
         cols.append((ni * ny + nj)[coupled])
-        vals.append(np.full(int(coupled.sum()), c))
+        vals.append(np.full(int(coupled.sum()), c) if np.isscalar(c) else c[coupled])
         diag -= c * coupled
         if wall in dirichlet:
             on_wall = fluid & ~inside
@@ -82,7 +100,7 @@ def assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None)
     A.sum_duplicates()
     flat = solvable.ravel()
     pin = int(np.argmax(flat)) if flat.any() else 0
-    return FineOperator(A, (nx, ny), flat.copy(), not dirichlet, pin, bc.ravel())
+    return FineOperator(A, (nx, ny), flat.copy(), not dirichlet, pin, bc.ravel(), row_scale)
 
 
 @dataclass
@@ -283,19 +301,20 @@ _CACHE_ORDER: list = []
 _CACHE_MAX = 8
 
 
-def hierarchy_for(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None):
+def hierarchy_for(nx, ny, dx, dy, periodic_x, periodic_y, solid=None, dirichlet=None, widths=None):
     """``(fine operator, (levels, coarsest inverse))`` of one Poisson structure.
 
     The hierarchy is a deterministic function of the assembled operator, so
-    problems that share grid, periodicity, Dirichlet walls and solid mask share
-    one build (kept for the last few structures of the process).
+    problems that share grid, spacing, periodicity, Dirichlet walls and solid
+    mask share one build (kept for the last few structures of the process).
     """
     key = (nx, ny, dx, dy, bool(periodic_x), bool(periodic_y),
            tuple(sorted((dirichlet or {}).items())),
-           None if solid is None else np.asarray(solid, bool).tobytes())
+           None if solid is None else np.asarray(solid, bool).tobytes(),
+           None if widths is None else tuple(np.asarray(w, float).tobytes() for w in widths))
     hit = _CACHE.get(key)
     if hit is None:
-        op = assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid, dirichlet)
+        op = assemble(nx, ny, dx, dy, periodic_x, periodic_y, solid, dirichlet, widths)
         hit = _CACHE[key] = (op, build_hierarchy(op))
         _CACHE_ORDER.append(key)
         while len(_CACHE_ORDER) > _CACHE_MAX:
