@@ -221,6 +221,9 @@ class _Problem:
             raise NotImplementedError("the batched path steps with time_scheme='rk3'")
         self.config = cfg
         self.mesh = StructuredMesh.from_config(cfg)
+        if not self.mesh.is_uniform:
+            raise NotImplementedError("the batched path is discretised for uniform meshes; stretched "
+                                      "problems run on ProjectionSolver")
         self.boundaries = BoundaryInfo(cfg.boundary_config, self.mesh)
         nx, ny = self.mesh.shape
         if obstacle is None:

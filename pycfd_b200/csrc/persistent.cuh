@@ -177,15 +177,17 @@ __device__ __forceinline__ double p_ld(const T* p) { return (double)__ldcg(p); }
 __device__ __forceinline__ bool p_edge(int i, int j, const Geo& g) {
   return (g.dir_w && i == 0) || (g.dir_e && i == g.nx - 1) || (g.dir_s && j == 0) || (g.dir_n && j == g.ny - 1);
 }
+// (A stretched mesh has no per-flag table: every cell forms its own coefficients.)
 __device__ __forceinline__ double p_diag(const double* dtab, uint8_t f, int i, int j, const Geo& g) {
-  return p_edge(i, j, g) ? fine_diag(f, i, j, g) : dtab[f & 31];
+  return (g.met || p_edge(i, j, g)) ? fine_diag(f, i, j, g) : dtab[f & 31];
 }
 __device__ __forceinline__ double p_wdinv(const double* wtab, uint8_t f, int i, int j, const Geo& g, double w) {
-  return p_edge(i, j, g) ? fine_wdinv(f, i, j, g, w) : wtab[f & 31];
+  return (g.met || p_edge(i, j, g)) ? fine_wdinv(f, i, j, g, w) : wtab[f & 31];
 }
 // fine_apply<double> with the tabled diagonal.
 template <class X>
 __device__ __forceinline__ double p_apply(const double* dtab, uint8_t f, int i, int j, int c, const Geo& g, X x) {
+  if (g.met) return fine_apply<double>(f, i, j, c, g, x);
   double acc = p_diag(dtab, f, i, j, g) * x(c, i, j);
   if (f & F_W) { const int a = wrap_w(i, g); acc += g.cx * x(a * g.ny + j, a, j); }
   if (f & F_E) { const int a = wrap_e(i, g); acc += g.cx * x(a * g.ny + j, a, j); }

@@ -299,10 +299,18 @@ __global__ void k_sor_half(double* __restrict__ x, const double* __restrict__ b,
     const uint8_t f = flags[c];
     const double d = fine_diag(f, i, j, g);
     double off = 0.0;
-    if (f & F_W) { const int a = wrap_w(i, g); off += g.cx * xe(a * g.ny + j, a, j); }
-    if (f & F_E) { const int a = wrap_e(i, g); off += g.cx * xe(a * g.ny + j, a, j); }
-    if (f & F_S) { const int bb = wrap_s(j, g); off += g.cy * xe(i * g.ny + bb, i, bb); }
-    if (f & F_N) { const int bb = wrap_n(j, g); off += g.cy * xe(i * g.ny + bb, i, bb); }
+    double cw = g.cx, ce = g.cx, cs = g.cy, cn = g.cy;
+    if (g.met) {   // stretched: the face coefficients of this cell
+      const Metrics M(g);
+      cw = M.cw(i, j);
+      ce = M.ce(i, j);
+      cs = M.cs(i, j);
+      cn = M.cn(i, j);
+    }
+    if (f & F_W) { const int a = wrap_w(i, g); off += cw * xe(a * g.ny + j, a, j); }
+    if (f & F_E) { const int a = wrap_e(i, g); off += ce * xe(a * g.ny + j, a, j); }
+    if (f & F_S) { const int bb = wrap_s(j, g); off += cs * xe(i * g.ny + bb, i, bb); }
+    if (f & F_N) { const int bb = wrap_n(j, g); off += cn * xe(i * g.ny + bb, i, bb); }
     const double xn = (1.0 - omega) * xe(c, i, j) + omega * (b[c] - off) / d;
     x[c] = xn;
     if (f & F_SOLV) acc[0] += xn;

@@ -21,7 +21,7 @@ from .config import (AdvectionScheme, BCKind, PressureSolver, SimulationConfig, 
                      TimeScheme, WALLS)
 from .fields import FlowField
 from .hierarchy import assemble, fused_for, hierarchy_for, tail_for
-from .mesh import StructuredMesh
+from .mesh import NonUniformMeshError, StructuredMesh
 
 #: solve status of a persistent (cooperative) solve whose grid barrier ran out of time
 PERSISTENT_TIMEOUT = -6
@@ -174,12 +174,27 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     cfg = config
     nx, ny = mesh.shape
     d = _lib.SolverDesc()
-    d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, mesh.dx, mesh.dy, config.nu
+    m = mesh.metrics
+    # dx, dy: the uniform spacing, or the smallest cell of a stretched mesh (the
+    # time-step limits answer to it, pycfd/core/timestepper.py:91-119)
+    d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, m.min_hx, m.min_hy, config.nu
     d.body_fx, d.body_fy = cfg.body_force
     if cfg.use_les:
         d.use_les = 1
         d.les_coeff = les_coefficient(cfg.smagorinsky_cs, mesh)
     keep = []
+    if not mesh.is_uniform:
+        block = m.device_block()
+        keep.append(block)
+        d.metrics = _lib.cast(block, C.c_double)
+        # summed outlet face widths, outlet walls in wall order (pycfd/core/boundary.py:480-483)
+        total = 0.0
+        for wall in WALLS:
+            if boundaries.kinds[wall] is BCKind.OUTLET:
+                total += float((mesh.dy_cells if wall in ("left", "right") else mesh.dx_cells).sum())
+        d.outlet_width = total
+    else:
+        d.metrics = _lib.cast(None, C.c_double)
     for w, wall in enumerate(WALLS):
         spec = boundaries.specs[wall]
         d.bc_kind[w] = _lib.BC_CODES[boundaries.kinds[wall].value]
@@ -282,7 +297,7 @@ def dt_control_for(config, mesh, t_end: float = float("inf"), history: bool = Fa
     (fixed ``config.dt`` when ``adaptive_dt`` is off), donor-cell blend policy.
     """
     nu = config.nu
-    dx, dy = mesh.dx, mesh.dy
+    dx, dy = mesh.metrics.min_hx, mesh.metrics.min_hy
     visc = float("inf") if nu <= 0 else 0.8 / (2.0 * nu * (1.0 / dx ** 2 + 1.0 / dy ** 2))
     c = _lib.DtControl()
     c.adaptive = int(bool(config.adaptive_dt))
@@ -354,6 +369,10 @@ class ProjectionSolver:
         self.nu = config.nu
         self.boundaries = BoundaryInfo(config.boundary_config, self.mesh)
         self.periodic_x, self.periodic_y = self.boundaries.periodic_x, self.boundaries.periodic_y
+        self._reject_stretched_periodic()
+        if config.use_les and not self.mesh.is_uniform:
+            raise NotImplementedError("the Smagorinsky closure on the GPU path is provided on uniform meshes; "
+                                      "use stretch_x = stretch_y = 1.0 with use_les=True")
         nx, ny = self.mesh.shape
         if obstacle is None:
             self.solid = np.zeros((nx, ny), dtype=bool)
@@ -372,8 +391,10 @@ class ProjectionSolver:
                     raise ValueError(f"body {k} mask must have shape {(nx, ny)}, got {b.shape}")
         self._build_slices()
         self.dirichlet_pressure = self.boundaries.dirichlet_pressure()
-        args = (nx, ny, self.mesh.dx, self.mesh.dy, self.periodic_x, self.periodic_y,
-                self.solid if self.has_obstacle else None, self.dirichlet_pressure or None)
+        m = self.mesh.metrics
+        widths = None if self.mesh.is_uniform else (self.mesh.dx_cells, self.mesh.dy_cells)
+        args = (nx, ny, m.min_hx, m.min_hy, self.periodic_x, self.periodic_y,
+                self.solid if self.has_obstacle else None, self.dirichlet_pressure or None, widths)
         self._levels, self._cinv = (None, None)
         if kind in (PressureSolver.MULTIGRID, PressureSolver.MGCG):
             self.poisson, (self._levels, self._cinv) = hierarchy_for(*args)
@@ -387,6 +408,19 @@ class ProjectionSolver:
         self._blend = 0.0
         self.last_stats = None
         self._ring = None
+
+    def _reject_stretched_periodic(self) -> None:
+        """A stretched axis cannot be periodic: its first and last cells differ, so the
+        domain does not repeat (``pycfd/core/solver.py:209-230``)."""
+        for axis, stretched, periodic, ratio in (
+                ("x", self.mesh.stretched_x, self.periodic_x, self.mesh.stretch_x),
+                ("y", self.mesh.stretched_y, self.periodic_y, self.mesh.stretch_y)):
+            if stretched and periodic:
+                raise NonUniformMeshError(
+                    f"the {axis} axis is periodic and stretched (stretch_{axis}={ratio}): the first and "
+                    "last cells differ in width, so the spacing jumps across the seam and the domain "
+                    f"does not repeat. Use stretch_{axis}=1.0 on a periodic axis, or a non-periodic "
+                    "boundary condition.")
 
     # ------------------------------------------------------------------ #
     def _build_slices(self) -> None:
@@ -512,6 +546,10 @@ class ProjectionSolver:
         nx, ny = self.mesh.shape
         ru = torch.empty((nx + 1, ny), dtype=torch.float64, device="cuda")
         rv = torch.empty((nx, ny + 1), dtype=torch.float64, device="cuda")
+        if not self.mesh.is_uniform:   # the stretched array stencils (pycfd/core/solver.py:336-466)
+            _lib.check(self._L.pycfd_solver_momentum_rhs(self._h, _lib.ptr(u), _lib.ptr(v), float(blend),
+                                                         _lib.ptr(ru), _lib.ptr(rv), _stream()))
+            return ru, rv
         fx, fy = self.config.body_force
         _lib.check(self._L.pycfd_momentum_rhs(_lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx,
                                               self.mesh.dy, self.nu, float(blend), fx, fy,
@@ -524,6 +562,10 @@ class ProjectionSolver:
         u, v = self._dev(u).contiguous(), self._dev(v).contiguous()
         nx, ny = self.mesh.shape
         out = torch.empty((nx, ny), dtype=torch.float64, device="cuda")
+        if not self.mesh.is_uniform:
+            _lib.check(self._L.pycfd_solver_divergence(self._h, _lib.ptr(u), _lib.ptr(v), _lib.ptr(out),
+                                                       _stream()))
+            return out
         _lib.check(self._L.pycfd_divergence(_lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx,
                                             self.mesh.dy, _lib.ptr(out), _stream()))
         return out
@@ -674,5 +716,6 @@ class ProjectionSolver:
         if self.config.upwind_blend is not None:
             return self.config.upwind_blend
         st = fields._stats if fields._stats is not None else self.field_stats(fields)
-        courant = max(st.max_u * dt / self.mesh.dx, st.max_v * dt / self.mesh.dy)
+        m = self.mesh.metrics   # the worst cell is the smallest one
+        courant = max(st.max_u * dt / m.min_hx, st.max_v * dt / m.min_hy)
         return float(min(1.0, 1.2 * courant))

@@ -54,7 +54,7 @@ class TimeStepper:
         nu = self.solver.nu
         if nu <= 0:
             return float("inf")
-        dx, dy = self.mesh.dx, self.mesh.dy
+        dx, dy = self.mesh.metrics.min_hx, self.mesh.metrics.min_hy   # the smallest cell
         return VISCOUS_SAFETY_FACTOR / (2.0 * nu * (1.0 / dx ** 2 + 1.0 / dy ** 2))
 
     def _stats(self, fields: FlowField):
@@ -66,13 +66,15 @@ class TimeStepper:
         if not self.config.adaptive_dt:
             return self.config.dt
         st = self._stats(fields)
-        scale = st.max_u / self.mesh.dx + st.max_v / self.mesh.dy
+        m = self.mesh.metrics
+        scale = st.max_u / m.min_hx + st.max_v / m.min_hy
         dt_conv = self.config.cfl_max / scale if scale > QUIESCENT_VELOCITY_FLOOR else float("inf")
         return float(min(dt_conv, self.viscous_dt_limit, self.config.dt))
 
     def cfl_number(self, fields: FlowField, dt: float) -> float:
         st = self._stats(fields)
-        return float(dt * (st.max_u / self.mesh.dx + st.max_v / self.mesh.dy))
+        m = self.mesh.metrics
+        return float(dt * (st.max_u / m.min_hx + st.max_v / m.min_hy))
 
     def _check_health(self, fields: FlowField, dt: float) -> None:
         st = self._stats(fields)

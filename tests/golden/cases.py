@@ -202,3 +202,28 @@ CKPT_CAVITY = dict(nx=32, ny=32, re=100.0, dt=1.0, t_end=1e9, cfl_max=0.5, adapt
 LES_CAVITY = dict(nx=40, ny=40, re=5000.0, use_les=True, smagorinsky_cs=0.17, dt=2e-3, t_end=10.0,
                   adaptive_dt=False, pressure_solver="cg", poisson_tol=1e-12,
                   boundary_config=bcs(top=("moving_wall", 1.0)), name="les_cavity")
+
+
+# Stretched meshes (pycfd/core/mesh.py:236-311, the array path of pycfd/core/solver.py)
+STRETCH_MESHES = [   # (nx, ny, lx, ly, stretch_x, stretch_y, cluster_x, cluster_y)
+    (24, 18, 1.5, 1.0, 1.07, 1.12, "low", "walls"),
+    (17, 21, 1.0, 2.0, 1.15, 0.93, "centre", "walls"),
+    (31, 16, 2.0, 1.0, 1.04, 1.0, "walls", "low"),
+]
+
+STRETCH_CAVITY = dict(nx=40, ny=32, stretch_x=1.06, stretch_y=1.08, cluster_x="walls", cluster_y="walls",
+                      re=400.0, dt=1.0, t_end=1e9, cfl_max=0.5, adaptive_dt=True, pressure_solver="mgcg",
+                      poisson_tol=1e-12, boundary_config=bcs(top=("moving_wall", 1.0)), name="stretch_cavity")
+
+STRETCH_CHANNEL = dict(nx=48, ny=24, lx=3.0, ly=1.0, stretch_x=1.03, stretch_y=1.1, cluster_x="low",
+                       cluster_y="centre", re=100.0, dt=4e-3, t_end=10.0, adaptive_dt=False,
+                       pressure_solver="mgcg", poisson_tol=1e-12,
+                       boundary_config=bcs(left=("inlet", 1.0), right=("outlet",)), name="stretch_channel")
+STRETCH_CHANNEL_CIRCLE = ((1.0, 0.5), 0.15)
+
+STRETCH_PRESSURE_OUTLET = dict(nx=36, ny=20, lx=2.0, ly=1.0, stretch_x=1.05, stretch_y=1.06, cluster_x="low",
+                               cluster_y="walls", re=50.0, dt=5e-3, t_end=10.0, adaptive_dt=False,
+                               pressure_solver="cg", poisson_tol=1e-12,
+                               boundary_config=bcs(left=("inlet", 1.0, "parabolic"),
+                                                   right=("pressure_outlet", 0.0, "uniform", 0.0)),
+                               name="stretch_po")

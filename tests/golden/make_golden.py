@@ -22,6 +22,9 @@ Cases (all seeded, all synthetic):
   ref_checkpoint.npz (+ _continued)  a reference checkpoint and the state 10 steps on
   interchange.npz  this package's checkpoint writer read back by the reference's loader
   les.npz        Smagorinsky eddy viscosity, LES momentum RHS, and 10 LES cavity steps
+  stretched.npz  stretched meshes: widths/metrics, RHS, divergence, Poisson operator, and
+                 runs of a stretched cavity, an inlet/outlet channel past a cylinder and
+                 a pressure-outlet channel
 """
 
 from __future__ import annotations
@@ -395,6 +398,67 @@ def gen_les():
     save("les.npz", **out)
 
 
+def gen_stretched():
+    """Stretched meshes on the reference's array path (pycfd/core/mesh.py:236-311,
+    pycfd/core/solver.py:336-543, pycfd/core/pressure.py:193-207): widths, faces and
+    metrics; momentum RHS and divergence on random fields (blend 0 and 0.6); the
+    assembled Poisson operator with an obstacle and a Dirichlet wall; a stretched
+    lid cavity (adaptive dt, MG-PCG) for 12 steps, an inlet/outlet channel past a
+    cylinder for 10 steps with its force history, and a pressure-outlet channel
+    (CG) for 10 steps."""
+    out = {}
+    for k, (nx, ny, lx, ly, sx, sy, cx_, cy_) in enumerate(cases.STRETCH_MESHES):
+        mesh = StructuredMesh(nx, ny, lx, ly, sx, sy, cx_, cy_)
+        m = mesh.metrics
+        out.update({f"m{k}_dx": mesh.dx_cells, f"m{k}_dy": mesh.dy_cells, f"m{k}_xf": mesh.xf,
+                    f"m{k}_yf": mesh.yf, f"m{k}_hxu": np.ravel(m.hxu), f"m{k}_hyv": np.ravel(m.hyv),
+                    f"m{k}_wx": np.ravel(m.wx_corner), f"m{k}_wy": np.ravel(m.wy_corner)})
+        c = dict(nx=nx, ny=ny, lx=lx, ly=ly, stretch_x=sx, stretch_y=sy, cluster_x=cx_, cluster_y=cy_,
+                 re=300.0 + 100 * k, body_force=(0.05 * k, -0.1), dt=1e-3, t_end=1.0, adaptive_dt=False,
+                 pressure_solver="cg", boundary_config=cases.bcs(top=("moving_wall", 1.0)), name="stretch")
+        s = ProjectionSolver(ref_config(c), mesh)
+        rng = np.random.default_rng(40 + k)
+        u = rng.standard_normal((nx + 3, ny + 2))
+        v = rng.standard_normal((nx + 2, ny + 3))
+        for b, blend in enumerate((0.0, 0.6)):
+            ru, rv = s.momentum_rhs(u, v, blend)
+            out.update({f"m{k}_b{b}_rhs_u": np.array(ru), f"m{k}_b{b}_rhs_v": np.array(rv)})
+        out.update({f"m{k}_u": u, f"m{k}_v": v, f"m{k}_div": s.divergence(u, v)})
+    # Poisson operator: obstacle, a Dirichlet (pressure outlet) wall on the right
+    mesh = StructuredMesh(*cases.STRETCH_MESHES[0])
+    solid = circle_mask(mesh, (0.7, 0.5), 0.2).mask
+    sysm = assemble_poisson_matrix(mesh, solid_mask=solid, dirichlet={"right": 0.3})
+    po = {}
+    csr_parts("A", sysm.A, po)
+    out.update({f"poisson_{k}": v for k, v in po.items()})
+    out.update({"poisson_solid": solid, "poisson_bc": sysm.bc_rhs, "poisson_row_scale": np.asarray(sysm.row_scale)})
+    # runs
+    cfg = ref_config(cases.STRETCH_CAVITY)
+    sim = Simulation(cfg)
+    sim.run(max_steps=12)
+    f = sim.fields
+    out.update({"cav_u": f.u, "cav_v": f.v, "cav_p": f.p, "cav_t": np.array(f.t)})
+    cfg = ref_config(cases.STRETCH_CHANNEL)
+    mesh = StructuredMesh.from_config(cfg)
+    solid = circle_mask(mesh, *cases.STRETCH_CHANNEL_CIRCLE).mask
+    s = ProjectionSolver(cfg, mesh, solid)
+    f = s.initialize()
+    fx, fy = [], []
+    for _ in range(10):
+        f = s.step(f, cfg.dt)
+        fx.append(s.body_force_reaction[0])
+        fy.append(s.body_force_reaction[1])
+    out.update({"ch_u": f.u, "ch_v": f.v, "ch_p": f.p, "ch_fx": np.array(fx), "ch_fy": np.array(fy),
+                "ch_solid": solid})
+    cfg = ref_config(cases.STRETCH_PRESSURE_OUTLET)
+    s = ProjectionSolver(cfg)
+    f = s.initialize()
+    for _ in range(10):
+        f = s.step(f, cfg.dt)
+    out.update({"po_u": f.u, "po_v": f.v, "po_p": f.p})
+    save("stretched.npz", **out)
+
+
 def gen_masks():
     big = StructuredMesh(2048, 1024, 2.0, 1.0)
     m = circle_mask(big, (0.5, 0.5), 0.05).mask
@@ -407,10 +471,10 @@ def gen_masks():
 if __name__ == "__main__":
     which = set(sys.argv[2:]) or {"rhs", "poisson", "multigrid", "solvers", "steps",
                                   "cavity64", "cylinder", "masks", "faces", "cylinder_long", "shapes",
-                                  "checkpoint", "interchange", "les"}
+                                  "checkpoint", "interchange", "les", "stretched"}
     for name in ("rhs", "poisson", "multigrid", "solvers", "steps", "cavity64",
                  "cylinder", "masks", "faces", "cylinder_long", "shapes", "checkpoint", "interchange",
-                 "les"):
+                 "les", "stretched"):
         if name in which:
             t0 = time.perf_counter()
             globals()["gen_" + name]()
