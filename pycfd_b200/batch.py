@@ -479,6 +479,12 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True),
     BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
                  fused_from=2),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 tail_ratio=64.0),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 tail_ratio=None),
+    BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 tail_ratio=64.0),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, ell_group=1),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, ell_group=1),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=2, tile_rows=32, ell_group=1),
