@@ -145,6 +145,10 @@ typedef struct {
                                                  NULL on a uniform mesh (dx, dy used) */
     double outlet_width;                      /* stretched mesh: summed widths of the
                                                  outlet walls' faces (boundary.py:480-483) */
+    const double* les_coeff_field;            /* stretched mesh with use_les: (Cs Delta)^2 on
+                                                 the ghosted cell grid (nx+2)*(ny+2), Delta =
+                                                 sqrt(dx_i dy_j), ghost ring repeating its
+                                                 neighbour (physics/turbulence.py:43-58) */
 } pycfd_solver_desc;
 
 /* Per-call results the Python layer reads back (one small D2H copy). */
@@ -208,6 +212,10 @@ int pycfd_momentum_rhs_les(const double* u, const double* v, int nx, int ny, dou
 int pycfd_solver_momentum_rhs(pycfd_solver* s, const double* u, const double* v, double blend,
                               double* rhs_u, double* rhs_v, void* stream);
 int pycfd_solver_divergence(pycfd_solver* s, const double* u, const double* v, double* out, void* stream);
+/* The Smagorinsky eddy viscosities (cells, corners) and the LES momentum RHS on the
+ * solver's own mesh, uniform or stretched (solver.py:467-529, turbulence.py:60-118). */
+int pycfd_solver_momentum_rhs_les(pycfd_solver* s, const double* u, const double* v, double blend,
+                                  double* nu_c, double* nu_corner, double* rhs_u, double* rhs_v, void* stream);
 
 int pycfd_divergence(const double* u, const double* v, int nx, int ny, double dx, double dy,
                      double* out, void* stream);

@@ -24,7 +24,7 @@ MAX_BODIES = 8
 EXPORTS = (
     "pycfd_last_error", "pycfd_version", "pycfd_solver_create", "pycfd_solver_destroy",
     "pycfd_momentum_rhs", "pycfd_momentum_rhs_les", "pycfd_divergence", "pycfd_solver_momentum_rhs",
-    "pycfd_solver_divergence", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
+    "pycfd_solver_divergence", "pycfd_solver_momentum_rhs_les", "pycfd_apply_velocity_bc", "pycfd_poisson_solve",
     "pycfd_mg_apply", "pycfd_project", "pycfd_initialize", "pycfd_substep", "pycfd_step",
     "pycfd_step_graph", "pycfd_step_adaptive", "pycfd_set_clock", "pycfd_get_clock",
     "pycfd_history_read",
@@ -79,7 +79,8 @@ class SolverDesc(C.Structure):
                 ("coarse_cluster_rows", C.c_int), ("sequential_launch", C.c_int),
                 ("persistent_solve", C.c_int), ("tail_level", C.c_int), ("tail_operator", _dp),
                 ("ell_thread_budget", C.c_int), ("use_les", C.c_int), ("les_coeff", C.c_double),
-                ("metrics", C.POINTER(C.c_double)), ("outlet_width", C.c_double)]
+                ("metrics", C.POINTER(C.c_double)), ("outlet_width", C.c_double),
+                ("les_coeff_field", C.POINTER(C.c_double))]
 
 
 class DtControl(C.Structure):
@@ -137,6 +138,7 @@ def load(path: str = LIB_PATH):
         "pycfd_divergence": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, vp, vp]),
         "pycfd_solver_momentum_rhs": (C.c_int, [vp, vp, vp, C.c_double, vp, vp, vp]),
         "pycfd_solver_divergence": (C.c_int, [vp, vp, vp, vp, vp]),
+        "pycfd_solver_momentum_rhs_les": (C.c_int, [vp, vp, vp, C.c_double, vp, vp, vp, vp, vp]),
         "pycfd_apply_velocity_bc": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp]),
         "pycfd_poisson_solve": (C.c_int, [vp, vp, vp, vp, vp]),
         "pycfd_mg_apply": (C.c_int, [vp, vp, vp, vp]),

@@ -71,7 +71,7 @@ struct Geo {
 struct Metrics {
   const double* p;
   int nx, ny;
-  __device__ __forceinline__ Metrics(const Geo& g) : p(g.met), nx(g.nx), ny(g.ny) {}
+  __host__ __device__ __forceinline__ Metrics(const Geo& g) : p(g.met), nx(g.nx), ny(g.ny) {}
   __device__ __forceinline__ double hx(int i) const { return p[i]; }
   __device__ __forceinline__ double hy(int j) const { return p[nx + j]; }
   __device__ __forceinline__ double hxu(int f) const { return p[nx + ny + f]; }

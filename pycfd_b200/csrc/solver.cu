@@ -170,6 +170,7 @@ struct pycfd_solver {
   int les = 0;                  // Smagorinsky closure on
   double les_coeff = 0.0;       // (Cs Delta)^2
   double* met = nullptr;        // stretched mesh: the packed metrics (Geo::met)
+  double* les_coeff_c = nullptr;  // stretched mesh with LES: (Cs Delta)^2 per ghosted cell
   double* les_nu_c = nullptr;   // (nx+2) x (ny+2) effective viscosity of the current stage
   double* les_nu_k = nullptr;   // (nx+1) x (ny+1) its corner average
   // CUDA-graph recording of whole steps
@@ -1072,8 +1073,13 @@ int substep_impl(pycfd_solver* s, StageIn uin, StageIn vin, double* us, double* 
   dim3 grd((g.ny + 3 + TJ - 1) / TJ, (g.nx + 3 + TI - 1) / TI);
   if (s->les) {
     // the stage input's effective viscosity, then the predictor in stress-divergence form
-    pdl_launch(s, k_les_nu, grid_for((long)(g.nx + 2) * (g.ny + 2), 256, kWaveBlocks), 256, 0, stream, uin, vin, g,
-               s->les_coeff, s->les_nu_c);
+    const int lg = grid_for((long)(g.nx + 2) * (g.ny + 2), 256, kWaveBlocks);
+    if (g.met)
+      pdl_launch(s, k_les_nu<Metrics>, lg, 256, 0, stream, uin, vin, g, Metrics(g), s->les_coeff,
+                 (const double*)s->les_coeff_c, s->les_nu_c);
+    else
+      pdl_launch(s, k_les_nu<UniSp>, lg, 256, 0, stream, uin, vin, g, UniSp{g.dx, g.dy}, s->les_coeff,
+                 (const double*)nullptr, s->les_nu_c);
     CHECK_LAUNCH();
     pdl_launch(s, k_les_corner, grid_for((long)(g.nx + 1) * (g.ny + 1), 256, kWaveBlocks), 256, 0, stream,
                (const double*)s->les_nu_c, g, s->les_nu_k);
@@ -1200,10 +1206,13 @@ int pycfd_solver_create(const pycfd_solver_desc* d, pycfd_solver** out) {
   s->mg_sweeps = std::max(1, d->mg_sweeps);
   s->scheme = d->time_scheme;
   if (d->metrics) {   // stretched mesh: the packed metrics, read by every stencil through g.met
-    if (d->use_les) return bail(fail(PCFD_E_UNSUPPORTED, "the Smagorinsky closure is provided on uniform meshes"));
     int mrc;
     if ((mrc = upload(s, &s->met, d->metrics, (size_t)metrics_count(nx, ny)))) return bail(mrc);
     g.met = s->met;
+    if (d->use_les) {   // the per-cell filter coefficient (Cs Delta)^2 on the ghosted cell grid
+      if (!d->les_coeff_field) return bail(fail(PCFD_E_ARG, "LES on a stretched mesh needs les_coeff_field"));
+      if ((mrc = upload(s, &s->les_coeff_c, d->les_coeff_field, (size_t)(nx + 2) * (ny + 2)))) return bail(mrc);
+    }
   }
   if (d->use_les) {
     if (!(d->les_coeff >= 0.0)) return bail(fail(PCFD_E_ARG, "les_coeff must be non-negative"));
@@ -1509,6 +1518,25 @@ int pycfd_solver_momentum_rhs(pycfd_solver* s, const double* u, const double* v,
   return 0;
 }
 
+int pycfd_solver_momentum_rhs_les(pycfd_solver* s, const double* u, const double* v, double blend, double* nu_c,
+                                  double* nu_corner, double* rhs_u, double* rhs_v, void* stream) {
+  if (!s || !u || !v || !nu_c || !nu_corner || !rhs_u || !rhs_v) return fail(PCFD_E_ARG, "bad arguments");
+  if (!s->les) return fail(PCFD_E_ARG, "the solver was created without the Smagorinsky closure");
+  const Geo& g = s->g;
+  cudaStream_t sm = st(stream);
+  const StageIn U{u, nullptr, 1.0, 0.0}, V{v, nullptr, 1.0, 0.0};
+  const int lg = grid_for((long)(g.nx + 2) * (g.ny + 2), 256, kWaveBlocks);
+  if (g.met) k_les_nu<Metrics><<<lg, 256, 0, sm>>>(U, V, g, Metrics(g), s->les_coeff, s->les_coeff_c, nu_c);
+  else k_les_nu<UniSp><<<lg, 256, 0, sm>>>(U, V, g, UniSp{g.dx, g.dy}, s->les_coeff, nullptr, nu_c);
+  CHECK_LAUNCH();
+  k_les_corner<<<grid_for((long)(g.nx + 1) * (g.ny + 1), 256, kWaveBlocks), 256, 0, sm>>>(nu_c, g, nu_corner);
+  CHECK_LAUNCH();
+  dim3 blk(TJ, TI), grd((g.ny + 1 + TJ - 1) / TJ, (g.nx + 1 + TI - 1) / TI);
+  k_rhs_les_g<<<grd, blk, 0, sm>>>(u, v, g, blend, nu_c, nu_corner, rhs_u, rhs_v);
+  CHECK_LAUNCH();
+  return 0;
+}
+
 int pycfd_solver_divergence(pycfd_solver* s, const double* u, const double* v, double* out, void* stream) {
   if (!s || !u || !v || !out) return fail(PCFD_E_ARG, "bad arguments");
   const Geo& g = s->g;
@@ -1539,7 +1567,8 @@ int pycfd_momentum_rhs_les(const double* u, const double* v, int nx, int ny, dou
   g.dy = dy;
   g.nu = nu;
   const StageIn U{u, nullptr, 1.0, 0.0}, V{v, nullptr, 1.0, 0.0};
-  k_les_nu<<<grid_for((long)(nx + 2) * (ny + 2), 256, kWaveBlocks), 256, 0, sm>>>(U, V, g, les_coeff, nu_c);
+  k_les_nu<UniSp><<<grid_for((long)(nx + 2) * (ny + 2), 256, kWaveBlocks), 256, 0, sm>>>(U, V, g, UniSp{dx, dy},
+                                                                                         les_coeff, nullptr, nu_c);
   CHECK_LAUNCH();
   k_les_corner<<<grid_for((long)(nx + 1) * (ny + 1), 256, kWaveBlocks), 256, 0, sm>>>(nu_c, g, nu_corner);
   CHECK_LAUNCH();

@@ -97,9 +97,11 @@ __device__ __forceinline__ double rhs_v_at(const U& u, const V& v, int i, int n,
 // derivatives (inner gradients across the flanking cells, outer difference
 // across the face's own control volume).  Same operations, same order as the
 // reference's arrays, so the right-hand side is bit-identical to it.
+// Advective term A_u at u face (m, j) of a stretched mesh (duudx + duvdy, the donor-cell
+// correction included).
 template <class U, class V>
-__device__ __forceinline__ double rhs_u_str(const U& u, const V& v, int m, int j, int ny, const Metrics& M,
-                                            double nu, double blend, double fx) {
+__device__ __forceinline__ double adv_u_str(const U& u, const V& v, int m, int j, int ny, const Metrics& M,
+                                            double blend) {
   const long W = ny + 2, WV = ny + 3;
   const double u0 = u[m * W + j], ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
   const double un = u[m * W + j + 1], us = u[m * W + j - 1];
@@ -118,15 +120,26 @@ __device__ __forceinline__ double rhs_u_str(const U& u, const V& v, int m, int j
     duudx += rmul(blend / hxu, rmul(fabs(uu_r), u0 - ue) / 2.0 - rmul(fabs(uu_l), uw - u0) / 2.0);
     duvdy += rmul(blend / hy, rmul(fabs(vc_t), u0 - un) / 2.0 - rmul(fabs(vc_b), us - u0) / 2.0);
   }
-  const double gx_hi = (ue - u0) / M.hx_ext(m), gx_lo = (u0 - uw) / M.hx_ext(m - 1);
-  const double gy_hi = (un - u0) / M.hyv(j), gy_lo = (u0 - us) / M.hyv(j - 1);
-  const double d2u = (gx_hi - gx_lo) / hxu + (gy_hi - gy_lo) / hy;
-  return -(duudx + duvdy) + rmul(nu, d2u) + fx;
+  return duudx + duvdy;
 }
 
 template <class U, class V>
-__device__ __forceinline__ double rhs_v_str(const U& u, const V& v, int i, int n, int ny, const Metrics& M,
-                                            double nu, double blend, double fy) {
+__device__ __forceinline__ double rhs_u_str(const U& u, const V& v, int m, int j, int ny, const Metrics& M,
+                                            double nu, double blend, double fx) {
+  const long W = ny + 2;
+  const double u0 = u[m * W + j], ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
+  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+  const double adv = adv_u_str(u, v, m, j, ny, M, blend);
+  const double gx_hi = (ue - u0) / M.hx_ext(m), gx_lo = (u0 - uw) / M.hx_ext(m - 1);
+  const double gy_hi = (un - u0) / M.hyv(j), gy_lo = (u0 - us) / M.hyv(j - 1);
+  const double d2u = (gx_hi - gx_lo) / M.hxu(m - 1) + (gy_hi - gy_lo) / M.hy(j - 1);
+  return -adv + rmul(nu, d2u) + fx;
+}
+
+// Advective term A_v at v face (i, n) of a stretched mesh (duvdx + dvvdy).
+template <class U, class V>
+__device__ __forceinline__ double adv_v_str(const U& u, const V& v, int i, int n, int ny, const Metrics& M,
+                                            double blend) {
   const long W = ny + 2, WV = ny + 3;
   const double v0 = v[i * WV + n], vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
   const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
@@ -145,10 +158,20 @@ __device__ __forceinline__ double rhs_v_str(const U& u, const V& v, int i, int n
     dvvdy += rmul(blend / hyv, rmul(fabs(vv_t), v0 - vn) / 2.0 - rmul(fabs(vv_b), vs - v0) / 2.0);
     duvdx += rmul(blend / hx, rmul(fabs(uc_r), v0 - ve) / 2.0 - rmul(fabs(uc_l), vw - v0) / 2.0);
   }
+  return duvdx + dvvdy;
+}
+
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_str(const U& u, const V& v, int i, int n, int ny, const Metrics& M,
+                                            double nu, double blend, double fy) {
+  const long WV = ny + 3;
+  const double v0 = v[i * WV + n], vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
+  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+  const double adv = adv_v_str(u, v, i, n, ny, M, blend);
   const double hx_hi = (ve - v0) / M.hxu(i), hx_lo = (v0 - vw) / M.hxu(i - 1);
   const double hy_hi = (vn - v0) / M.hy_ext(n), hy_lo = (v0 - vs) / M.hy_ext(n - 1);
-  const double d2v = (hx_hi - hx_lo) / hx + (hy_hi - hy_lo) / hyv;
-  return -(duvdx + dvvdy) + rmul(nu, d2v) + fy;
+  const double d2v = (hx_hi - hx_lo) / M.hx(i - 1) + (hy_hi - hy_lo) / M.hyv(n - 1);
+  return -adv + rmul(nu, d2v) + fy;
 }
 
 // ---- Smagorinsky large-eddy closure (pycfd/physics/turbulence.py:25-118) -------
@@ -157,34 +180,52 @@ __device__ __forceinline__ double rhs_v_str(const U& u, const V& v, int i, int n
 // stress-divergence form (pycfd/core/solver.py:467-499), uniform mesh.  The
 // expressions follow the reference's array code term by term, so the
 // viscosities and the right-hand side are bit-identical to it.
-template <class U, class V>
-__device__ __forceinline__ double les_s12_corner(const U& u, const V& v, int i, int j, int ny, double dx,
-                                                 double dy) {
+// Spacings of a uniform mesh behind the same accessors as Metrics, so one
+// template serves both: every accessor returns dx or dy.
+struct UniSp {
+  double dx, dy;
+  __device__ __forceinline__ double hx(int) const { return dx; }
+  __device__ __forceinline__ double hy(int) const { return dy; }
+  __device__ __forceinline__ double hxu(int) const { return dx; }
+  __device__ __forceinline__ double hyv(int) const { return dy; }
+  __device__ __forceinline__ double hx_ext(int) const { return dx; }
+  __device__ __forceinline__ double hy_ext(int) const { return dy; }
+};
+
+// S_12 at corner (i, j): both derivatives cross a face, so both divide by a
+// centre-to-centre distance (pycfd/physics/turbulence.py:62-65).
+template <class U, class V, class Sp>
+__device__ __forceinline__ double les_s12_corner(const U& u, const V& v, int i, int j, int ny, const Sp& sp) {
   const long W = ny + 2, WV = ny + 3;
-  const double dudy = (u[(long)(i + 1) * W + j + 1] - u[(long)(i + 1) * W + j]) / dy;
-  const double dvdx = (v[(long)(i + 1) * WV + j + 1] - v[(long)i * WV + j + 1]) / dx;
+  const double dudy = (u[(long)(i + 1) * W + j + 1] - u[(long)(i + 1) * W + j]) / sp.hyv(j);
+  const double dvdx = (v[(long)(i + 1) * WV + j + 1] - v[(long)i * WV + j + 1]) / sp.hxu(i);
   return 0.5 * (dudy + dvdx);
 }
 
 // nu_c at every ghosted cell: |S| = sqrt(2 s11^2 + 2 s22^2 + 4 s12^2), s11 and s22
-// across the cell, s12 the mean of the cell's four corner shear rates (ghost
-// cells take the nearest interior cell's mean, as the reference extends it).
-__global__ void k_les_nu(StageIn u, StageIn v, Geo g, double coeff, double* __restrict__ nu_c) {
+// across the cell (the ghost-extended widths), s12 the mean of the cell's four
+// corner shear rates (ghost cells take the nearest interior cell's mean, as the
+// reference extends it).  The coefficient (Cs Delta)^2 is one number on a uniform
+// mesh, a ghosted per-cell array on a stretched one (coeff_c, formed on the host
+// with the reference's operations, pycfd/physics/turbulence.py:43-58).
+template <class Sp>
+__global__ void k_les_nu(StageIn u, StageIn v, Geo g, Sp sp, double coeff, const double* __restrict__ coeff_c,
+                         double* __restrict__ nu_c) {
   pdl_begin();
   const int nx = g.nx, ny = g.ny;
   const long W = ny + 2, WV = ny + 3;
   const long total = (long)(nx + 2) * (ny + 2);
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     const int i = (int)(e / (ny + 2)), j = (int)(e % (ny + 2));
-    const double s11 = (u[(long)(i + 1) * W + j] - u[(long)i * W + j]) / g.dx;
-    const double s22 = (v[(long)i * WV + j + 1] - v[(long)i * WV + j]) / g.dy;
+    const double s11 = (u[(long)(i + 1) * W + j] - u[(long)i * W + j]) / sp.hx_ext(i);
+    const double s22 = (v[(long)i * WV + j + 1] - v[(long)i * WV + j]) / sp.hy_ext(j);
     const int ic = i < 1 ? 1 : (i > nx ? nx : i), jc = j < 1 ? 1 : (j > ny ? ny : j);
-    const double s12 = 0.25 * (les_s12_corner(u, v, ic - 1, jc - 1, ny, g.dx, g.dy) +
-                               les_s12_corner(u, v, ic, jc - 1, ny, g.dx, g.dy) +
-                               les_s12_corner(u, v, ic - 1, jc, ny, g.dx, g.dy) +
-                               les_s12_corner(u, v, ic, jc, ny, g.dx, g.dy));
+    const double s12 = 0.25 * (les_s12_corner(u, v, ic - 1, jc - 1, ny, sp) +
+                               les_s12_corner(u, v, ic, jc - 1, ny, sp) +
+                               les_s12_corner(u, v, ic - 1, jc, ny, sp) +
+                               les_s12_corner(u, v, ic, jc, ny, sp));
     const double smag = sqrt(2.0 * rmul(s11, s11) + 2.0 * rmul(s22, s22) + 4.0 * rmul(s12, s12));
-    nu_c[e] = g.nu + rmul(coeff, smag);
+    nu_c[e] = g.nu + rmul(coeff_c ? coeff_c[e] : coeff, smag);
   }
 }
 
@@ -263,6 +304,61 @@ __device__ __forceinline__ double rhs_v_les_at(const U& u, const V& v, int i, in
   return -(duvdx + dvvdy) + d + fy;
 }
 
+// The LES viscous term on a stretched mesh (pycfd/core/solver.py:467-499 with the
+// metric arrays) after the stretched advection.
+template <class U, class V>
+__device__ __forceinline__ double rhs_u_les_str(const U& u, const V& v, int m, int j, int ny, const Metrics& M,
+                                                double blend, double fx, const double* nu_c, const double* nu_k) {
+  const long W = ny + 2, WV = ny + 3, WK = ny + 1;
+  const double u0 = u[m * W + j], ue = u[(m + 1) * W + j], uw = u[(m - 1) * W + j];
+  const double un = u[m * W + j + 1], us = u[m * W + j - 1];
+  const double adv = adv_u_str(u, v, m, j, ny, M, blend);
+  const double hxu = M.hxu(m - 1);
+  const double dudx_r = (ue - u0) / M.hx_ext(m), dudx_l = (u0 - uw) / M.hx_ext(m - 1);
+  const double tau_t = rmul(nu_k[(long)(m - 1) * WK + j],
+                            (un - u0) / M.hyv(j) + (v[(long)m * WV + j + 1] - v[(long)(m - 1) * WV + j + 1]) / hxu);
+  const double tau_b = rmul(nu_k[(long)(m - 1) * WK + j - 1],
+                            (u0 - us) / M.hyv(j - 1) + (v[(long)m * WV + j] - v[(long)(m - 1) * WV + j]) / hxu);
+  const double d = 2.0 * (rmul(nu_c[(long)m * W + j], dudx_r) - rmul(nu_c[(long)(m - 1) * W + j], dudx_l)) / hxu +
+                   (tau_t - tau_b) / M.hy(j - 1);
+  return -adv + d + fx;
+}
+
+template <class U, class V>
+__device__ __forceinline__ double rhs_v_les_str(const U& u, const V& v, int i, int n, int ny, const Metrics& M,
+                                                double blend, double fy, const double* nu_c, const double* nu_k) {
+  const long W = ny + 2, WV = ny + 3, WK = ny + 1;
+  const double v0 = v[i * WV + n], vn = v[i * WV + n + 1], vs = v[i * WV + n - 1];
+  const double ve = v[(i + 1) * WV + n], vw = v[(i - 1) * WV + n];
+  const double adv = adv_v_str(u, v, i, n, ny, M, blend);
+  const double hyv = M.hyv(n - 1);
+  const double tau_r = rmul(nu_k[(long)i * WK + n - 1],
+                            (u[(long)(i + 1) * W + n] - u[(long)(i + 1) * W + n - 1]) / hyv + (ve - v0) / M.hxu(i));
+  const double tau_l = rmul(nu_k[(long)(i - 1) * WK + n - 1],
+                            (u[(long)i * W + n] - u[(long)i * W + n - 1]) / hyv + (v0 - vw) / M.hxu(i - 1));
+  const double dvdy_t = (vn - v0) / M.hy_ext(n), dvdy_b = (v0 - vs) / M.hy_ext(n - 1);
+  const double d = (tau_r - tau_l) / M.hx(i - 1) +
+                   2.0 * (rmul(nu_c[(long)i * W + n], dvdy_t) - rmul(nu_c[(long)i * W + n - 1], dvdy_b)) / hyv;
+  return -adv + d + fy;
+}
+
+// LES RHS of the solver's own mesh (uniform or stretched).
+__global__ void k_rhs_les_g(const double* __restrict__ u, const double* __restrict__ v, Geo g, double blend,
+                            const double* __restrict__ nu_c, const double* __restrict__ nu_k,
+                            double* __restrict__ rhs_u, double* __restrict__ rhs_v) {
+  pdl_begin();
+  const int nx = g.nx, ny = g.ny;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i <= nx && j < ny)
+    rhs_u[(long)i * ny + j] = g.met ? rhs_u_les_str(u, v, i + 1, j + 1, ny, Metrics(g), blend, g.fx, nu_c, nu_k)
+                                    : rhs_u_les_at(u, v, i + 1, j + 1, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k);
+  if (i < nx && j <= ny)
+    rhs_v[(long)i * (ny + 1) + j] =
+        g.met ? rhs_v_les_str(u, v, i + 1, j + 1, ny, Metrics(g), blend, g.fy, nu_c, nu_k)
+              : rhs_v_les_at(u, v, i + 1, j + 1, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k);
+}
+
 // Stateless LES RHS into (nx+1, ny) and (nx, ny+1) blocks.
 __global__ void k_rhs_les(const double* __restrict__ u, const double* __restrict__ v, int nx, int ny, double dx,
                           double dy, double blend, double fx, double fy, const double* __restrict__ nu_c,
@@ -290,14 +386,16 @@ __global__ void k_predictor_les(StageIn u, StageIn v, double* __restrict__ us, d
     const long k = (long)i * (ny + 2) + j;
     double val = u[k];
     if (i >= g.u_lo && i < g.u_hi && j >= 1 && j <= ny)
-      val = val + rmul(dt, rhs_u_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k));
+      val = val + rmul(dt, g.met ? rhs_u_les_str(u, v, i, j, ny, Metrics(g), blend, g.fx, nu_c, nu_k)
+                                 : rhs_u_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fx, nu_c, nu_k));
     us[k] = val;
   }
   if (i < nx + 2 && j < ny + 3) {
     const long k = (long)i * (ny + 3) + j;
     double val = v[k];
     if (i >= 1 && i <= nx && j >= g.v_lo && j < g.v_hi)
-      val = val + rmul(dt, rhs_v_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k));
+      val = val + rmul(dt, g.met ? rhs_v_les_str(u, v, i, j, ny, Metrics(g), blend, g.fy, nu_c, nu_k)
+                                 : rhs_v_les_at(u, v, i, j, ny, g.dx, g.dy, blend, g.fy, nu_c, nu_k));
     vs[k] = val;
   }
 }

@@ -136,11 +136,21 @@ class BoundaryInfo:
         return full
 
 
-def les_coefficient(cs: float, mesh) -> float:
-    """``(Cs Delta)^2`` with the filter width Delta = sqrt(dx dy) of a uniform mesh
-    (``pycfd/physics/turbulence.py:38-52``)."""
-    delta = float(np.sqrt(mesh.dx * mesh.dy))
-    return (float(cs) * delta) ** 2
+def les_coefficient(cs: float, mesh):
+    """``(Cs Delta)^2`` (``pycfd/physics/turbulence.py:38-58``): one number with the
+    filter width Delta = sqrt(dx dy) of a uniform mesh; on a stretched mesh the
+    per-cell width sqrt(dx_i dy_j) on the ghosted cell grid, the ghost ring
+    repeating its neighbour."""
+    if mesh.is_uniform:
+        delta = float(np.sqrt(mesh.dx * mesh.dy))
+        return (float(cs) * delta) ** 2
+    nx, ny = mesh.shape
+    delta = np.sqrt(mesh.dx_cells[:, None] * mesh.dy_cells[None, :])
+    coeff = np.empty((nx + 2, ny + 2))
+    coeff[1:nx + 1, 1:ny + 1] = (float(cs) * delta) ** 2
+    coeff[0, :], coeff[nx + 1, :] = coeff[1, :], coeff[nx, :]
+    coeff[:, 0], coeff[:, ny + 1] = coeff[:, 1], coeff[:, ny]
+    return coeff
 
 
 class GpuSmagorinsky:
@@ -151,7 +161,8 @@ class GpuSmagorinsky:
         self.solver = solver
         self.mesh = solver.mesh
         self.cs = float(cs)
-        self.delta = float(np.sqrt(self.mesh.dx * self.mesh.dy))
+        self.delta = (float(np.sqrt(self.mesh.dx * self.mesh.dy)) if self.mesh.is_uniform
+                      else np.sqrt(self.mesh.dx_cells[:, None] * self.mesh.dy_cells[None, :]))
         self._coeff = les_coefficient(cs, self.mesh)
         self.last_nu_t_max = 0.0
 
@@ -162,7 +173,9 @@ class GpuSmagorinsky:
         return nu_c, nu_k
 
     def __repr__(self) -> str:
-        return f"SmagorinskyModel(cs={self.cs:g}, delta={self.delta:.4g})"
+        delta = (f"{self.delta:.4g}" if np.isscalar(self.delta)
+                 else f"[{self.delta.min():.4g}, {self.delta.max():.4g}]")
+        return f"SmagorinskyModel(cs={self.cs:g}, delta={delta})"
 
 
 def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind, options,
@@ -179,10 +192,17 @@ def native_desc(config, mesh, boundaries, solid, has_obstacle, body_masks, kind,
     # time-step limits answer to it, pycfd/core/timestepper.py:91-119)
     d.nx, d.ny, d.dx, d.dy, d.nu = nx, ny, m.min_hx, m.min_hy, config.nu
     d.body_fx, d.body_fy = cfg.body_force
+    keep = []
+    d.les_coeff_field = _lib.cast(None, C.c_double)
     if cfg.use_les:
         d.use_les = 1
-        d.les_coeff = les_coefficient(cfg.smagorinsky_cs, mesh)
-    keep = []
+        coeff = les_coefficient(cfg.smagorinsky_cs, mesh)
+        if np.isscalar(coeff):
+            d.les_coeff = coeff
+        else:
+            field_ = np.ascontiguousarray(coeff, dtype=np.float64)
+            keep.append(field_)
+            d.les_coeff_field = _lib.cast(field_, C.c_double)
     if not mesh.is_uniform:
         block = m.device_block()
         keep.append(block)
@@ -370,9 +390,6 @@ class ProjectionSolver:
         self.boundaries = BoundaryInfo(config.boundary_config, self.mesh)
         self.periodic_x, self.periodic_y = self.boundaries.periodic_x, self.boundaries.periodic_y
         self._reject_stretched_periodic()
-        if config.use_les and not self.mesh.is_uniform:
-            raise NotImplementedError("the Smagorinsky closure on the GPU path is provided on uniform meshes; "
-                                      "use stretch_x = stretch_y = 1.0 with use_les=True")
         nx, ny = self.mesh.shape
         if obstacle is None:
             self.solid = np.zeros((nx, ny), dtype=bool)
@@ -529,6 +546,11 @@ class ProjectionSolver:
         f64 = dict(dtype=torch.float64, device="cuda")
         nu_c, nu_k = torch.empty((nx + 2, ny + 2), **f64), torch.empty((nx + 1, ny + 1), **f64)
         ru, rv = torch.empty((nx + 1, ny), **f64), torch.empty((nx, ny + 1), **f64)
+        if not self.mesh.is_uniform:   # the solver's own metrics and per-cell coefficient
+            _lib.check(self._L.pycfd_solver_momentum_rhs_les(
+                self._h, _lib.ptr(u), _lib.ptr(v), float(blend), _lib.ptr(nu_c), _lib.ptr(nu_k),
+                _lib.ptr(ru), _lib.ptr(rv), _stream()))
+            return nu_c, nu_k, ru, rv
         fx, fy = self.config.body_force
         _lib.check(self._L.pycfd_momentum_rhs_les(
             _lib.ptr(u), _lib.ptr(v), nx, ny, self.mesh.dx, self.mesh.dy, self.nu, self.turbulence._coeff,

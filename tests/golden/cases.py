@@ -227,3 +227,8 @@ STRETCH_PRESSURE_OUTLET = dict(nx=36, ny=20, lx=2.0, ly=1.0, stretch_x=1.05, str
                                boundary_config=bcs(left=("inlet", 1.0, "parabolic"),
                                                    right=("pressure_outlet", 0.0, "uniform", 0.0)),
                                name="stretch_po")
+
+STRETCH_LES_CAVITY = dict(nx=32, ny=28, stretch_x=1.05, stretch_y=1.07, cluster_x="walls", cluster_y="walls",
+                          re=5000.0, use_les=True, smagorinsky_cs=0.17, dt=2e-3, t_end=10.0, adaptive_dt=False,
+                          pressure_solver="cg", poisson_tol=1e-12,
+                          boundary_config=bcs(top=("moving_wall", 1.0)), name="stretch_les_cavity")

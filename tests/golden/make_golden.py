@@ -456,6 +456,27 @@ def gen_stretched():
     for _ in range(10):
         f = s.step(f, cfg.dt)
     out.update({"po_u": f.u, "po_v": f.v, "po_p": f.p})
+    # the Smagorinsky closure on a stretched mesh (pycfd/physics/turbulence.py:38-118,
+    # pycfd/core/solver.py:467-499 with the metric arrays)
+    nx, ny, lx, ly, sx, sy, cx_, cy_ = cases.STRETCH_MESHES[1]
+    c = dict(nx=nx, ny=ny, lx=lx, ly=ly, stretch_x=sx, stretch_y=sy, cluster_x=cx_, cluster_y=cy_, re=3000.0,
+             use_les=True, smagorinsky_cs=0.17, body_force=(0.1, -0.2), dt=1e-3, t_end=1.0, adaptive_dt=False,
+             pressure_solver="cg", boundary_config=cases.bcs(top=("moving_wall", 1.0)), name="stretch_les")
+    s = ProjectionSolver(ref_config(c))
+    rng = np.random.default_rng(50)
+    u = rng.standard_normal((nx + 3, ny + 2))
+    v = rng.standard_normal((nx + 2, ny + 3))
+    nu_c, nu_k = s.turbulence.eddy_viscosity(u, v, s.nu)
+    out.update({"les_u": u, "les_v": v, "les_nu_c": nu_c, "les_nu_k": nu_k})
+    for b, blend in enumerate((0.0, 0.6)):
+        ru, rv = s.momentum_rhs(u, v, blend)
+        out.update({f"les_b{b}_rhs_u": np.array(ru), f"les_b{b}_rhs_v": np.array(rv)})
+    cfg = ref_config(cases.STRETCH_LES_CAVITY)
+    s = ProjectionSolver(cfg)
+    f = s.initialize()
+    for _ in range(10):
+        f = s.step(f, cfg.dt)
+    out.update({"lescav_u": f.u, "lescav_v": f.v, "lescav_p": f.p})
     save("stretched.npz", **out)
 
 

@@ -118,8 +118,39 @@ def test_stretched_refusals():
         ProjectionSolver(_cfg(dict(nx=16, ny=16, stretch_x=1.1, re=100.0, pressure_solver="cg",
                                    boundary_config=per)))
     with pytest.raises(NotImplementedError, match="uniform meshes"):
-        ProjectionSolver(_cfg(dict(nx=16, ny=16, stretch_x=1.1, re=100.0, use_les=True, pressure_solver="cg",
-                                   boundary_config=cases.bcs(top=("moving_wall", 1.0)))))
-    with pytest.raises(NotImplementedError, match="uniform meshes"):
         BatchedSolver([_cfg(dict(nx=16, ny=16, stretch_y=1.1, re=100.0, pressure_solver="mgcg",
                                  time_scheme="rk3", boundary_config=cases.bcs(top=("moving_wall", 1.0))))])
+
+
+def test_stretched_les_viscosity_and_rhs_bit_exact(golden):
+    """Per-cell filter width sqrt(dx_i dy_j), strains over the metric spacings, the
+    stress-divergence viscous term after the stretched advection
+    (pycfd/physics/turbulence.py:38-118, pycfd/core/solver.py:467-499)."""
+    from pycfd_b200.solver import ProjectionSolver
+    g = golden("stretched.npz")
+    nx, ny, lx, ly, sx, sy, cx, cy = cases.STRETCH_MESHES[1]
+    c = dict(nx=nx, ny=ny, lx=lx, ly=ly, stretch_x=sx, stretch_y=sy, cluster_x=cx, cluster_y=cy, re=3000.0,
+             use_les=True, smagorinsky_cs=0.17, body_force=(0.1, -0.2), dt=1e-3, t_end=1.0, adaptive_dt=False,
+             pressure_solver="cg", boundary_config=cases.bcs(top=("moving_wall", 1.0)), name="stretch_les")
+    s = ProjectionSolver(_cfg(c))
+    u = torch.as_tensor(g["les_u"], device="cuda")
+    v = torch.as_tensor(g["les_v"], device="cuda")
+    nu_c, nu_k = s.turbulence.eddy_viscosity(u, v, s.nu)
+    assert np.array_equal(nu_c.cpu().numpy(), g["les_nu_c"])
+    assert np.array_equal(nu_k.cpu().numpy(), g["les_nu_k"])
+    for b, blend in enumerate((0.0, 0.6)):
+        ru, rv = s.momentum_rhs(u, v, blend)
+        assert np.array_equal(ru.cpu().numpy(), g[f"les_b{b}_rhs_u"]), blend
+        assert np.array_equal(rv.cpu().numpy(), g[f"les_b{b}_rhs_v"]), blend
+
+
+def test_stretched_les_cavity_matches_reference(golden):
+    from pycfd_b200.solver import ProjectionSolver
+    g = golden("stretched.npz")
+    cfg = _cfg(cases.STRETCH_LES_CAVITY)
+    s = ProjectionSolver(cfg)
+    f = s.initialize()
+    for _ in range(10):
+        f = s.step(f, cfg.dt)
+    for a, key in zip(f.numpy(), ("u", "v", "p")):
+        assert _rel(a, g["lescav_" + key]) < 1e-10, key
