@@ -453,6 +453,8 @@ typedef struct {
     int ell_group;      /* problems of one structure per block of a coarse-level
                            launch, sharing each matrix entry's load: 1 or 8 (0
                            reads as 8)                                          */
+    int sequential_launch;  /* 1: plain stream order between the batched kernels;
+                               0: programmatic dependent launch                 */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver

@@ -411,6 +411,7 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_stats(const BProb<T>* __restrict__ probs,
                                                         const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -447,6 +448,7 @@ __global__ void __launch_bounds__(kBThreads) k_b_stats(const BProb<T>* __restric
 // reached, freezes.
 template <class T>
 __global__ void k_b_dt(const BProb<T>* __restrict__ probs, int nprob, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nprob) return;
   const BProb<T>& P = probs[k];
@@ -470,6 +472,7 @@ __global__ void k_b_dt(const BProb<T>* __restrict__ probs, int nprob, BShared sh
 // Fixed step parameters (initial projection: dt = 1; fixed-dt runs).
 template <class T>
 __global__ void k_b_set_dt(const BProb<T>* __restrict__ probs, int nprob, double dt) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nprob) return;
   const BProb<T>& P = probs[k];
@@ -494,6 +497,7 @@ B_STRIP_KERNEL k_b_predictor(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, int src_a,
                                                             int src_b, double ca, double cb, int dst,
                                                             BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = kBStripRows;
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -555,6 +559,7 @@ B_STRIP_KERNEL k_b_predictor(const BProb<T>* __restrict__ probs,
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_boundary(const BProb<T>* __restrict__ probs, int arr,
                                                            BcProgram prog, int p_ghosts, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const BProb<T>& P = probs[blockIdx.x];
   if (b_frozen(sh, blockIdx.x)) return;
   double* u = b_arr_u(P, arr);
@@ -584,6 +589,7 @@ template <class T>
 B_STRIP_KERNEL k_b_div_rhs(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int arr,
                                                           BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -629,6 +635,7 @@ template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_correct(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int arr,
                                                           BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -660,6 +667,7 @@ template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_combine(const BProb<T>* __restrict__ probs,
                                                           const int2* __restrict__ map, int src_b,
                                                           double ca, double cb, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (b_frozen(sh, e.x)) return;
@@ -688,6 +696,7 @@ B_STRIP_KERNEL k_b_rhs_init(const BProb<T>* __restrict__ probs,
                                                            int nprob, const int2* __restrict__ map,
                                                            double tol, int maxiter, BShared sh,
                                                            LoopCtl loop) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -751,6 +760,7 @@ __device__ __forceinline__ T* b_pdir(const BProb<T>& P, int it) {
 template <class T>
 B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
                                                         const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -796,6 +806,7 @@ template <class T>
 B_STRIP_KERNEL k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
                                                         const int2* __restrict__ map, int maxiter,
                                                         BShared sh, LoopCtl loop) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -851,6 +862,7 @@ template <class T>
 B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, double tol,
                                                                BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -889,6 +901,7 @@ B_STRIP_KERNEL k_b_finish_stats(const BProb<T>* __restrict__ probs,
 template <class T>
 B_STRIP_KERNEL k_b_finish_apply(const BProb<T>* __restrict__ probs,
                                                                const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -920,6 +933,7 @@ B_STRIP_KERNEL k_b_ir_residual(const BProb<T>* __restrict__ probs,
                                                               double tol, double inner_tol,
                                                               int max_passes, int first, BShared sh,
                                                               LoopCtl outer) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -987,6 +1001,7 @@ B_STRIP_KERNEL k_b_ir_residual(const BProb<T>* __restrict__ probs,
 // Arm the inner loop: does any problem run an inner solve in this pass?
 template <class T>
 __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShared sh, LoopCtl inner) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   int any = 0;
   for (int p = threadIdx.x; p < nprob; p += blockDim.x)
     if (b_solving(sh, p)) any = 1;
@@ -1003,6 +1018,7 @@ __global__ void k_b_ir_arm(const BProb<T>* __restrict__ probs, int nprob, BShare
 template <class T>
 B_STRIP_KERNEL k_b_ir_update(const BProb<T>* __restrict__ probs,
                                                             const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<double>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -1043,6 +1059,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
                                                        const int2* __restrict__ map, int src, int dst,
                                                        BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int RS = b_rs<T>();
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
@@ -1345,6 +1362,7 @@ __global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BPro
                                                        const int2* __restrict__ map,
                                                        const int* __restrict__ sprobs, int d, int src,
                                                        int dst, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int2 e = map[blockIdx.x];
   const BHier<T>& H = hiers[e.x];
   const int rb = e.y >> 10, grp = e.y & 1023;
@@ -1384,6 +1402,7 @@ __global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BPro
 template <class T>
 __global__ void __launch_bounds__(kBThreads) k_b_coarsest(const BProb<T>* __restrict__ probs,
                                                            const int2* __restrict__ map, int d, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   extern __shared__ double sb[];
   const int2 e = map[blockIdx.x];
   if (!b_solving(sh, e.x)) return;
@@ -1463,6 +1482,7 @@ __global__ void __launch_bounds__(kTailThreads) k_b_tail(const BProb<T>* __restr
                                                           const BHier<T>* __restrict__ hiers,
                                                           const int2* __restrict__ map,
                                                           const int* __restrict__ sprobs, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   constexpr int KW = TailK<T>::KW;
   constexpr int NW = kTailThreads / 32;
   const int2 e = map[blockIdx.x];   // (structure, row tile * 64 + column tile)
@@ -1633,6 +1653,7 @@ template <class T>
 __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __restrict__ probs,
                                                                const int* __restrict__ order, int dc,
                                                                int sweeps, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   extern __shared__ double sb[];
   const int p = order[blockIdx.x];
   if (!b_solving(sh, p)) return;
@@ -1727,6 +1748,7 @@ __global__ void __launch_bounds__(kBCoarseThreads) k_b_coarse(const BProb<T>* __
 template <class T>
 __global__ void k_b_gather(const BProb<T>* __restrict__ probs, int nprob, int* __restrict__ iout,
                            double* __restrict__ dout) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nprob) return;
   const BProb<T>& P = probs[k];

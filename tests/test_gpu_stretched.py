@@ -78,7 +78,9 @@ def test_stretched_channel_past_cylinder_matches_reference(golden):
         fy.append(s.body_force_reaction[1])
     for a, key in zip(f.numpy(), ("u", "v", "p")):
         assert _rel(a, g["ch_" + key]) < 1e-10, key
-    assert _rel(fx, g["ch_fx"]) < 1e-9 and _rel(fy, g["ch_fy"]) < 1e-9
+    # the channel is symmetric: lift is round-off (1e-15), so it is held to the drag's scale
+    assert _rel(fx, g["ch_fx"]) < 1e-9
+    assert np.abs(np.asarray(fy) - g["ch_fy"]).max() <= 1e-9 * np.abs(g["ch_fx"]).max()
 
 
 def test_stretched_pressure_outlet_channel_matches_reference(golden):
