@@ -181,7 +181,7 @@ def algorithmic_bytes(kid, solver, s_bytes=8):
     raise ValueError(kid)
 
 
-def live_roofline(solver, f, dt, hbm_gbs, steps=3):
+def live_roofline(solver, f, dt, hbm_gbs, peak_src, steps=3):
     """Time the candidate kernels with CUDA events around their eager launches."""
     import ctypes as C
     from pycfd_b200 import _lib
@@ -223,7 +223,7 @@ def live_roofline(solver, f, dt, hbm_gbs, steps=3):
     return {"bound": "hbm", "kernel": KERNELS[kid], "achieved": achieved, "peak": hbm_gbs,
             "unit": "GB/s", "frac": achieved / hbm_gbs, "traffic": traffic,
             "bytes_per_launch": nbytes, "us_per_launch": per_launch_s * 1e6, "launches": cnt,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+            "peak_source": peak_src,
             "timing": "CUDA events around each eager launch of the kernel over "
                       f"{steps} replayed steps of the same workload (recorded graphs carry no events)",
             "share_of_candidates": {KERNELS[k]: v[0] for k, v in shares.items()}}
@@ -514,7 +514,8 @@ def run_batch(args, world, rank, local):
                            "mixed_batched_vs_batched_fp64": value / fp64b["value"] if fp64b else None},
                 "e2e": e2e, "clocks": ck, "roofline": roof, "gpu_launches": launches}
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = batch_cpu_baseline(cfgs, steps=1, workers=16)
+            # a bounded sample: 16 cavities of the batch, enough steps for about 10-30 s of work
+            line["cpu_baseline"] = batch_cpu_baseline(cfgs, steps=60, workers=16)
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -794,8 +795,11 @@ def run_ours(args, world, rank, local):
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except Exception:
             pass
-        hbm = peaks.get("hbm_gbs", 6650.0)
-        roof = live_roofline(solver, f, dt, hbm)
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+        if hbm is None:
+            hbm, peak_src = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+        roof = live_roofline(solver, f, dt, hbm, peak_src)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
