@@ -376,7 +376,7 @@ def run_batch(args, world, rank, local):
                             coarse_level=args.coarse_level, coarse_tail=tail != "off",
                             tail_ratio=None if tail in ("none", "off") else float(tail),
                             fused_restriction=args.fused_from > 0, fused_from=max(1, args.fused_from),
-                            ell_group=args.ell_group, sequential_launch=args.sequential)
+                            ell_group=args.ell_group, programmatic_launch=args.pdl)
     b = BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
     rec = not args.eager
@@ -864,8 +864,8 @@ def main():
                     help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
     ap.add_argument("--fused-from", type=int, default=0, choices=[0, 1, 2],
                     help="batch, --no-autotune: down sweep by fused restrictions from this level (0: off)")
-    ap.add_argument("--sequential", action="store_true",
-                    help="batch, --no-autotune: plain stream order (no programmatic dependent launch)")
+    ap.add_argument("--pdl", action="store_true",
+                    help="batch, --no-autotune: programmatic dependent launch between the kernels")
     ap.add_argument("--ell-group", type=int, default=8, choices=[1, 8],
                     help="batch, --no-autotune: problems per coarse-level block sharing the matrix loads")
     ap.add_argument("--no-profile", action="store_true",

@@ -262,7 +262,7 @@ class BatchOptions:
     fused_restriction: bool = False   #: down sweep by R (I - A W) products (one sweep, every structure tailed)
     fused_from: int = 1               #: first level so restricted (2: the fine level's restriction stays)
     ell_group: int = 8                #: problems per coarse-level block sharing the matrix loads (1 or 8)
-    sequential_launch: bool = False   #: plain stream order instead of programmatic dependent launch
+    programmatic_launch: bool = False  #: programmatic dependent launch between the kernels (off: plain order)
 
 
 class BatchedSolver:
@@ -357,7 +357,7 @@ class BatchedSolver:
         bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
                             float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows),
                             int(opts.coarse_level), int(opts.fused_from), int(opts.ell_group),
-                            int(bool(opts.sequential_launch)))
+                            int(bool(opts.programmatic_launch)))
         if max_steps is None:
             ms = None
         else:

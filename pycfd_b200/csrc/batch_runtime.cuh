@@ -383,7 +383,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 // Every batched kernel starts with pdl_begin (waits for its predecessor's grid
 // and memory), so with B->mem->pdl set a launch carries the programmatic-
 // serialization attribute and its blocks are scheduled while the predecessor
-// drains; with it clear the launches keep plain stream order.
+// drains; with it clear (the default) the launches keep plain stream order.
 #define BLAUNCH(kernel, grid, block, smem, stream, ...)                                    \
   do {                                                                                      \
     pdl_launch(B->mem, kernel, dim3(grid), dim3(block), (size_t)(smem), (stream), __VA_ARGS__); \
@@ -789,7 +789,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->fused_from = opts->fused_from == 2 ? 2 : 1;
   B->ell_group = opts->ell_group == 1 ? 1 : kBGroup;
   B->mem = new pycfd_solver();
-  B->mem->pdl = opts->sequential_launch ? 0 : 1;
+  B->mem->pdl = opts->programmatic_launch ? 1 : 0;
   B->solvers.assign(n, nullptr);
   for (int i = 0; i < n; ++i) {
     // the single-problem record: geometry, masks, boundary table, scalars, vectors
