@@ -1172,8 +1172,11 @@ __device__ __forceinline__ T b_ell_row(const Ell<T>& E, int L, int row, int lane
 // (the per-problem form).  Each problem's row sum keeps the per-problem order
 // (lane-strided entries, then the lane tree) in both.
 constexpr int kBGroup = 8;         // problems per block of the grouped form
+#ifndef PCFD_BELL_ROUNDS
+#define PCFD_BELL_ROUNDS 2
+#endif
 template <int GS>
-__host__ __device__ constexpr int b_ell_rounds() { return GS == 1 ? 8 : 2; }   // rounds of kBThreads / L rows
+__host__ __device__ constexpr int b_ell_rounds() { return GS == 1 ? 8 : PCFD_BELL_ROUNDS; }   // rounds of kBThreads / L rows
 
 // The group's vectors for one op, filled from the problem records by the first
 // GS threads; a null output marks a member that is absent or not solving.
