@@ -47,7 +47,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     # PYCFD_B200_DEFINES: extra -D options (strip heights PCFD_STRIP_ROWS and
-    # PCFD_BSTRIP_ROWS), e.g. "-DPCFD_BSTRIP_ROWS=4"
+    # PCFD_BSTRIP_ROWS, resident-block bounds PCFD_BSTRIP_MINB and PCFD_BELL_MINB,
+    # PCFD_BELL_ROUNDS), e.g. "-DPCFD_BSTRIP_ROWS=4"
     extra = os.environ.get("PYCFD_B200_DEFINES", "").split()
     if any(not d.startswith("-D") for d in extra):
         raise ValueError("PYCFD_B200_DEFINES takes -D options only")
