@@ -322,7 +322,10 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
 #define PCFD_BSTRIP_ROWS 8
 #endif
 constexpr int kBStripRows = PCFD_BSTRIP_ROWS;
-constexpr int kBStripItems = 16;
+#ifndef PCFD_BSTRIP_ITEMS
+#define PCFD_BSTRIP_ITEMS 16
+#endif
+constexpr int kBStripItems = PCFD_BSTRIP_ITEMS;   // strips of kBStripRows rows per chunk (block)
 static_assert(kBStripRows % 2 == 0, "the FP64-operand kernels take half-height strips");
 // Strip height of a kernel whose per-cell values are of type T: FP64 values take
 // twice the registers, so their kernels walk half-height strips.
