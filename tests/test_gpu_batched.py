@@ -147,6 +147,26 @@ def test_programmatic_launch_gives_the_same_bits():
                 assert np.array_equal(x, y), (prec, k)
 
 
+def test_concurrent_parts_equal_one_engine():
+    """Split over three engines on their own streams, every problem takes the steps
+    it takes in one engine, bit for bit (its arithmetic does not depend on the other
+    problems of its engine), and the results come back in the configs' order."""
+    from pycfd_b200.batch import BatchedSolver, BatchOptions, ConcurrentBatch
+    cfgs = _cavities(count=7, seed=13)
+    for prec in ("fp64", "mixed"):
+        one = BatchedSolver(cfgs, BatchOptions(precision=prec))
+        many = ConcurrentBatch(cfgs, BatchOptions(precision=prec), parts=3)
+        assert len(many.parts) == 3 and sorted(k for ks in many.index for k in ks) == list(range(len(cfgs)))
+        one.step(3)
+        many.step(3)
+        st1, st2 = one.status(), many.status()
+        assert np.array_equal(st1["steps"], st2["steps"]) and np.array_equal(st1["t"], st2["t"])
+        for k in range(len(cfgs)):
+            for x, y in zip(one.fields[k].numpy(), many.fields[k].numpy()):
+                assert np.array_equal(x, y), (prec, k)
+            assert one.field_stats(k).max_div == many.field_stats(k).max_div
+
+
 def test_mixed_batch_tracks_fp64_batch():
     """Velocity error <= 1e-6 of the FP64 batch and max|div u| <= 1e-8 after 20 steps."""
     from pycfd_b200.batch import BatchedSolver, BatchOptions
