@@ -1247,12 +1247,12 @@ __device__ __forceinline__ void b_group_fill(BGroup<T, GS>& G, int g, const BPro
 // (value, column) pairs loaded together and then every member's four gathers,
 // so a row costs one dependent load pair per four entries per lane.
 template <int L, int OP, int GS, class T>
-__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BGroup<T, GS>& G, const Ell<T>& E,
+__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const uint8_t* __restrict__ flags,
+                                            const BGroup<T, GS>& G, const Ell<T>& E,
                                             const T* __restrict__ wd, int d, int rb) {
   constexpr int per = kBThreads / L;
   constexpr int ROUNDS = b_ell_rounds<GS>();
   const int lane = (int)threadIdx.x & (L - 1);
-  const uint8_t* __restrict__ flags = P0.flags;
   const bool fr1 = OP == EO_FRESTRICT && d == 1;   // gathers the projected fine CG residual
   const T* src[GS];
   T mr[GS];
@@ -1374,32 +1374,35 @@ __global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BPro
   const int rb = e.y >> 10, grp = e.y & 1023;
   __shared__ BGroup<T, GS> G;
   __shared__ int any;
-  if (threadIdx.x == 0) any = 0;
-  __syncthreads();
-  if (threadIdx.x < GS) {
+  // The level's matrix (copied by value), its weights and the structure's leader
+  // record (geometry and flags) are loaded by every thread before the barrier, in
+  // parallel with warp 0 gathering the group's members.
+  const bool pl = OP == EO_PROLONG || OP == EO_PROLONGW;
+  const BLevel<T>& Lm = pl ? H.lv[d + 1] : H.lv[d];
+  const Ell<T> E = pl ? Lm.P : OP == EO_RESTRICT ? Lm.R : OP == EO_FRESTRICT ? Lm.M : Lm.A;
+  const int Lop = pl ? Lm.lp : OP == EO_RESTRICT ? Lm.lr : OP == EO_FRESTRICT ? Lm.lm : Lm.la;
+  const T* wd = d > 0 ? H.lv[d].wd : nullptr;
+  const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * GS]];   // the structure's geometry and flags
+  const uint8_t* flags0 = P0.flags;
+  if (threadIdx.x < 32) {   // GS <= 32: the members are lanes of warp 0
     const int k = grp * GS + (int)threadIdx.x;
     const BProb<T>* P = nullptr;
-    if (k < H.spn) {
+    if ((int)threadIdx.x < GS && k < H.spn) {
       const int pi = sprobs[H.sp0 + k];
       if (b_solving(sh, pi)) P = probs + pi;
     }
-    b_group_fill<T, OP, GS>(G, (int)threadIdx.x, P, d, src, dst);
-    if (P) any = 1;
+    if ((int)threadIdx.x < GS) b_group_fill<T, OP, GS>(G, (int)threadIdx.x, P, d, src, dst);
+    const unsigned on = __ballot_sync(0xffffffffu, P != nullptr);
+    if (threadIdx.x == 0) any = on != 0u;
   }
   __syncthreads();
   if (!any) return;
-  const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * GS]];   // the structure's geometry and flags
-  const bool pl = OP == EO_PROLONG || OP == EO_PROLONGW;
-  const BLevel<T>& Lm = pl ? H.lv[d + 1] : H.lv[d];
-  const Ell<T>& E = pl ? Lm.P : OP == EO_RESTRICT ? Lm.R : OP == EO_FRESTRICT ? Lm.M : Lm.A;
-  const int Lop = pl ? Lm.lp : OP == EO_RESTRICT ? Lm.lr : OP == EO_FRESTRICT ? Lm.lm : Lm.la;
-  const T* wd = d > 0 ? H.lv[d].wd : nullptr;
   switch (Lop) {
-    case 1: b_ellg_rows<1, OP, GS>(P0, G, E, wd, d, rb); break;
-    case 4: b_ellg_rows<4, OP, GS>(P0, G, E, wd, d, rb); break;
-    case 8: b_ellg_rows<8, OP, GS>(P0, G, E, wd, d, rb); break;
-    case 16: b_ellg_rows<16, OP, GS>(P0, G, E, wd, d, rb); break;
-    default: b_ellg_rows<32, OP, GS>(P0, G, E, wd, d, rb); break;
+    case 1: b_ellg_rows<1, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
+    case 4: b_ellg_rows<4, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
+    case 8: b_ellg_rows<8, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
+    case 16: b_ellg_rows<16, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
+    default: b_ellg_rows<32, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
   }
 }
 
