@@ -376,7 +376,8 @@ def run_batch(args, world, rank, local):
                             coarse_level=args.coarse_level, coarse_tail=tail != "off",
                             tail_ratio=None if tail in ("none", "off") else float(tail),
                             fused_restriction=args.fused_from > 0, fused_from=max(1, args.fused_from),
-                            ell_group=args.ell_group, programmatic_launch=args.pdl)
+                            ell_group=args.ell_group, programmatic_launch=args.pdl,
+                            stencil_transfer=args.stencil)
     b = ConcurrentBatch(cfgs, opts, parts=args.parts) if args.parts > 1 else BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
     rec = not args.eager
@@ -918,6 +919,8 @@ def main():
                     help="batch: batched engines stepped concurrently on their own streams (problems split by cells)")
     ap.add_argument("--pdl", action="store_true",
                     help="batch, --no-autotune: programmatic dependent launch between the kernels")
+    ap.add_argument("--stencil", action="store_true",
+                    help="batch, --no-autotune, --fused-from 1: level-0 transfers as stencils over the fine cells")
     ap.add_argument("--ell-group", type=int, default=8, choices=[1, 8],
                     help="batch, --no-autotune: problems per coarse-level block sharing the matrix loads")
     ap.add_argument("--no-profile", action="store_true",

@@ -456,6 +456,18 @@ typedef struct {
     int programmatic_launch;  /* 1: programmatic dependent launch between the batched
                                  kernels; 0: plain stream order (measured faster on
                                  the 256-cavity batch: 19.45 against 19.90 ms/step) */
+    int stencil_transfer;     /* 1: with the fused down sweep from the fine level,
+                                 the transfers between levels 0 and 1 run as stencils
+                                 over the fine cells (the fused restriction, and the
+                                 prolongation together with the last fine sweep)
+                                 instead of products with the stored P_1 and M_1.
+                                 They stand for P_1 = (I - W_0 A_0) T and
+                                 M_1 = P_1^T (I - A_0 W_0), T the aggregation of 2 x 2
+                                 fine cells: every structure's level 1 must have the
+                                 shape (ceil(nx/2), ceil(ny/2)) (else PCFD_E_UNSUPPORTED)
+                                 and its P_1 must be that smoothed aggregation (the
+                                 hierarchy this library's host side builds).  Equal to
+                                 the matrix products to rounding.  0: the products. */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver
@@ -487,8 +499,10 @@ int pycfd_batch_status(pycfd_batch* b, int* frozen, int* steps, int* iterations,
                        double* t, double* dt, void* stream);
 /* Measurement support: bracket every eager launch (record = 0) of one kernel
  * kind with CUDA events, then read the summed device time.  Ids: 1 CG
- * direction/A-product, 2 last fine V-cycle sweep, 3 first fine sweep +
- * residual, 4 coarse levels, 5 CG update, 6 predictor; 0 off. */
+ * direction/A-product, 2 last fine V-cycle sweep (with stencil transfers: and
+ * the prolongation onto the fine level), 3 first fine sweep + residual (with
+ * stencil transfers: the fused restriction into level 1), 4 coarse levels, 5 CG
+ * update, 6 predictor; 0 off. */
 int pycfd_batch_profile(pycfd_batch* b, int kernel_id);
 int pycfd_batch_profile_read(pycfd_batch* b, double* total_ms, int* launches, void* stream);
 /* Kernel launches the device executed for `steps` recorded steps since the

@@ -263,6 +263,9 @@ class BatchOptions:
     fused_from: int = 1               #: first level so restricted (2: the fine level's restriction stays)
     ell_group: int = 8                #: problems per coarse-level block sharing the matrix loads (1 or 8)
     programmatic_launch: bool = False  #: programmatic dependent launch between the kernels (off: plain order)
+    #: with the fused down sweep from the fine level: the level-0 <-> level-1 transfers
+    #: as stencils over the fine cells instead of products with the stored matrices
+    stencil_transfer: bool = False
 
 
 class BatchedSolver:
@@ -297,6 +300,7 @@ class BatchedSolver:
                          for k, cfg in enumerate(self.configs)]
         leader: dict = {}
         tailed: dict = {}
+        agg2: dict = {}
         structure = (C.c_int * n)()
         descs = (_lib.SolverDesc * n)()
         ctl = (_lib.DtControl * n)()
@@ -317,6 +321,8 @@ class BatchedSolver:
             structure[k] = leader[pb.key]
             if first:
                 tailed[pb.key] = d.tail_level > 0
+                nx0, ny0 = levels[0].shape
+                agg2[pb.key] = len(levels) >= 2 and tuple(levels[1].shape) == (-(-nx0 // 2), -(-ny0 // 2))
             te = t_end[k] if isinstance(t_end, (list, tuple, np.ndarray)) else t_end
             ctl[k] = dt_control_for(pb.config, pb.mesh, float(te))
         self.structures = len(leader)
@@ -326,6 +332,10 @@ class BatchedSolver:
         #: structure tailed, one sweep per level, per-level coarse launches)
         self._fused = bool(opts.fused_restriction and opts.mg_sweeps == 1 and opts.coarse_level == 0
                            and self._tailed == n)
+        #: the level-0 transfers run as stencils (fused sweep from the fine level, and
+        #: every structure's level 1 the 2 x 2 aggregation of its cells)
+        self._stencil = bool(opts.stencil_transfer and self._fused and opts.fused_from == 1
+                             and all(agg2.values()))
         # state in three flat pools (one host<->device copy per array kind), one view per problem
         shapes = [(pb.mesh.u_shape, pb.mesh.v_shape, pb.mesh.p_shape) for pb in self.problems]
         sizes = [[int(np.prod(sh)) for sh in trio] for trio in shapes]
@@ -357,7 +367,7 @@ class BatchedSolver:
         bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
                             float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows),
                             int(opts.coarse_level), int(opts.fused_from), int(opts.ell_group),
-                            int(bool(opts.programmatic_launch)))
+                            int(bool(opts.programmatic_launch)), int(self._stencil))
         if max_steps is None:
             ms = None
         else:
@@ -594,6 +604,10 @@ BATCH_CANDIDATES = (
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, tail_ratio=4.0),
     BatchOptions(precision="mixed", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, coarse_level=3),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True),
+    BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 stencil_transfer=True),
+    BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 stencil_transfer=True),
     BatchOptions(precision="mixed", inner_tol=3e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
                  fused_from=2),
     BatchOptions(precision="mixed", inner_tol=1e-3, mg_sweeps=1, tile_rows=32, fused_restriction=True,
@@ -609,6 +623,8 @@ BATCH_CANDIDATES = (
                  fused_from=2, ell_group=1),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True),
+    BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True,
+                 stencil_transfer=True),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, ell_group=1),
     BatchOptions(precision="fp64", inner_tol=1e-4, mg_sweeps=1, tile_rows=32, fused_restriction=True,
                  ell_group=1),

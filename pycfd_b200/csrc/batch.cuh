@@ -52,6 +52,7 @@ struct BHier {
   const T* tail;    // dense operator of the cycle at and below tail_level (row-major), or null
   int tail_level, tail_n;
   int fused;        // levels 1..tail_level carry their fused restriction M
+  int agg2;         // level 1 aggregates 2 x 2 fine cells: shape (ceil(nx/2), ceil(ny/2))
   int sp0, spn;     // this structure's problems: sprobs[sp0 .. sp0 + spn)
 };
 
@@ -69,6 +70,7 @@ struct BProb {
   int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
   int s_segs, s_items, s_chunks;         // warp strips of the solver kernels (b_strips)
   int p_chunks;                          // warp-strip chunks of the predictor (ghosted arrays)
+  int h_tr, h_tiles_j, h_tiles;          // staged tiles of the level-0 stencil transfers: rows, tiles
   int red_base;                          // first partial row of this problem
   const uint8_t* flags;
   const uint8_t* solid;
@@ -306,15 +308,17 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
 // ---- warp strips -----------------------------------------------------------------
 // The fine-level solver kernels (CG direction and operator, CG update, the
 // level-0 multigrid sweeps) walk a problem's cells in warp strips: a warp takes
-// one 32-column segment of y (lane = column, so each row of a vector is one
-// coalesced 128-byte access in FP32, 256 bytes in FP64) over kBStripRows rows of
-// x.  The stencil operand of the strip and its two halo rows go to registers
-// first, with every per-cell load of the strip, before any arithmetic; the
-// y-neighbours then come from the adjacent lanes by shuffle.  The columns just
-// west and east of the segment are the same for the whole warp: every lane forms
-// them (one broadcast load per row) and lanes 0 and `last` use them, so no load
-// sits under a lane-dependent branch and none waits for another.  Off-grid rows
-// and columns are read at a clamped (valid) index and the value dropped.
+// one segment of y (lane = column, so each row of a vector is one coalesced
+// access of 32 values) over kBStripRows rows of x.  The stencil operand of the
+// strip and its two halo rows go to registers first, with every per-cell load
+// of the strip, before any arithmetic; the y-neighbours then come from the
+// adjacent lanes by shuffle.  The columns just west and east of the segment are
+// lanes 0 and 31 themselves (a segment is the 30 columns of lanes 1..30): each
+// lane forms one operand value per row, and no load sits under a lane-dependent
+// branch.  (The alternative kept behind PCFD_BSTRIP_HALO_LANES=0, 32-column
+// segments whose lanes all form the two edge columns' values as well, issues
+// three operand loads per row instead of one.)  Off-grid rows and columns are
+// read at a clamped (valid) index and the value dropped.
 // No shared-memory staging and no block barrier until the block's reduction.
 // A block (8 warps) takes kBStripItems consecutive (strip, segment) items of one
 // problem, adjacent segments of the same rows first.
@@ -326,6 +330,14 @@ constexpr int kBStripRows = PCFD_BSTRIP_ROWS;
 #define PCFD_BSTRIP_ITEMS 16
 #endif
 constexpr int kBStripItems = PCFD_BSTRIP_ITEMS;   // strips of kBStripRows rows per chunk (block)
+// Halo lanes: 1 = a segment is 30 columns, lanes 1..30, and lanes 0 and 31 hold
+// the columns just west and east of it (each lane forms one operand value per
+// row); 0 = a segment is 32 columns and every lane also forms the two edge
+// columns' values (three operand values per row).
+#ifndef PCFD_BSTRIP_HALO_LANES
+#define PCFD_BSTRIP_HALO_LANES 1
+#endif
+constexpr int kBSegCols = PCFD_BSTRIP_HALO_LANES ? 30 : 32;   // output columns per warp segment
 static_assert(kBStripRows % 2 == 0, "the FP64-operand kernels take half-height strips");
 // Strip height of a kernel whose per-cell values are of type T: FP64 values take
 // twice the registers, so their kernels walk half-height strips.
@@ -354,35 +366,56 @@ template <bool STENCIL, class T, int RS, class Op, class Load, class Body>
 __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load load, Body body) {
   static_assert(kBStripRows % RS == 0, "strip height must divide kBStripRows");
   constexpr int IPC = kBStripItems * (kBStripRows / RS);
+  // pointwise kernels take aligned 32-column segments (no halo to hold); their
+  // items then end no later than the stencil kernels' and fit the same chunks
+  constexpr bool HALO = PCFD_BSTRIP_HALO_LANES && STENCIL;
   const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
   const int nx = V.g.nx, ny = V.g.ny;
-  const int items = V.segs * ((nx + RS - 1) / RS);
+  const int segs = HALO ? V.segs : (ny + 31) / 32;
+  const int items = segs * ((nx + RS - 1) / RS);
   const int it1 = min(items, (chunk + 1) * IPC);
   for (int it = chunk * IPC + warp; it < it1; it += kBThreads / 32) {
-    const int strip = it / V.segs, seg = it - strip * V.segs;
-    const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
-    const bool jv = j < ny;
-    const int jc = jv ? j : ny - 1;
-    const int last = min(31, ny - 1 - j0);   // the segment's last valid lane
+    const int strip = it / segs, seg = it - strip * segs;
+    const int i0 = strip * RS;
+    int j, jc;      // this lane's column and the (valid) column its loads use
+    bool jv;        // the lane's cell is one of the segment's
+    int jh = -1;    // HALO: the operand's column (wrapped), -1 off the grid
+    int last = 31;  // !HALO: the segment's last valid lane
+    if constexpr (HALO) {
+      j = seg * kBSegCols - 1 + lane;   // lanes 0 and 31: the columns beside the segment
+      jh = j;
+      if (jh < 0) jh = V.g.periodic_y ? jh + ny : -1;
+      else if (jh >= ny) jh = (V.g.periodic_y && jh == ny) ? 0 : -1;
+      jc = jh >= 0 ? jh : (j < 0 ? 0 : ny - 1);
+      jv = lane >= 1 && lane <= 30 && j < ny;
+    } else {
+      const int j0 = seg * 32;
+      j = j0 + lane;
+      jv = j < ny;
+      jc = jv ? j : ny - 1;
+      last = min(31, ny - 1 - j0);
+    }
     T ov[STENCIL ? RS + 2 : 1];
-    T ew[STENCIL ? RS : 1], ee[STENCIL ? RS : 1];
+    T ew[STENCIL && !HALO ? RS : 1], ee[STENCIL && !HALO ? RS : 1];
     if (STENCIL) {
 #pragma unroll
       for (int u = 0; u < RS + 2; ++u) {
         const int r = strip_row(i0 - 1 + u, nx, V.g.periodic_x);
         const int rc = r >= 0 ? r : 0;
         const T val = op(rc * ny + jc, rc, jc);
-        ov[u] = (jv && r >= 0) ? val : (T)0;
+        ov[u] = ((HALO ? jh >= 0 : jv) && r >= 0) ? val : (T)0;
       }
-      int jw, je;
-      strip_edges(j0, last, ny, V.g.periodic_y, &jw, &je);
-      const int jwc = jw >= 0 ? jw : 0, jec = je >= 0 ? je : 0;
+      if constexpr (!HALO) {
+        int jw, je;
+        strip_edges(seg * 32, last, ny, V.g.periodic_y, &jw, &je);
+        const int jwc = jw >= 0 ? jw : 0, jec = je >= 0 ? je : 0;
 #pragma unroll
-      for (int u = 0; u < RS; ++u) {
-        const int i = i0 + u, ic = i < nx ? i : nx - 1;
-        const T vw = op(ic * ny + jwc, ic, jwc), ve = op(ic * ny + jec, ic, jec);
-        ew[u] = (jw >= 0 && i < nx) ? vw : (T)0;
-        ee[u] = (je >= 0 && i < nx) ? ve : (T)0;
+        for (int u = 0; u < RS; ++u) {
+          const int i = i0 + u, ic = i < nx ? i : nx - 1;
+          const T vw = op(ic * ny + jwc, ic, jwc), ve = op(ic * ny + jec, ic, jec);
+          ew[u] = (jw >= 0 && i < nx) ? vw : (T)0;
+          ee[u] = (je >= 0 && i < nx) ? ve : (T)0;
+        }
       }
     }
 #pragma unroll
@@ -399,8 +432,10 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
         e = ov[u + 2];
         sv = __shfl_up_sync(0xffffffffu, c, 1);
         nv = __shfl_down_sync(0xffffffffu, c, 1);
-        if (lane == 0) sv = ew[u];
-        if (lane == last) nv = ee[u];
+        if constexpr (!HALO) {
+          if (lane == 0) sv = ew[u];
+          if (lane == last) nv = ee[u];
+        }
       }
       const int i = i0 + u;
       if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
@@ -1057,6 +1092,24 @@ __device__ __forceinline__ T* b_fine_buf(const BProb<T>& P, int sel) {
   return sel == 0 ? P.lxa[0] : sel == 1 ? P.lxb[0] : P.z;
 }
 
+// Level d's iterate in buffer sel (0: xa, 1: xb).
+template <class T>
+__device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
+  if (d == P.nlev - 1 || d == P.tail) return P.lxa[d];   // coarsest and tail results are in xa
+  return sel == 0 ? P.lxa[d] : P.lxb[d];
+}
+
+// Closes the last sweep of a cycle from its sums (t[0] = sum z over the
+// solvable cells, t[1] = r.z): the fluid mean of z and rho = r.(z - mean z).
+template <class T>
+__device__ __forceinline__ void b_last_close(const BProb<T>& P, const double* t) {
+  double* S = P.S;
+  const double m = (P.singular && P.g.n_fluid) ? t[0] / P.g.n_fluid : 0.0;
+  S[S_MEAN_Z] = m;
+  S[S_RHO_PREV] = S[S_RHO];
+  S[S_RHO] = t[1] - m * S[S_SUM_R];
+}
+
 template <class T, int MODE>
 B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                                        const BHier<T>* __restrict__ hiers,
@@ -1067,7 +1120,6 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
   const int2 e = map[blockIdx.x];
   const BProb<T>& P = probs[e.x];
   if (!b_solving(sh, e.x)) return;
-  const Geo& g = P.g;
   B_VIEW(V, P);
   // arithmetic in T (FP32 in the mixed form's inner solve), sums in FP64
   const uint8_t* __restrict__ flags = P.flags;
@@ -1119,11 +1171,250 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
   }
   if (MODE != FM_LAST) return;
   b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
-    double* S = P.S;
-    const double m = (P.singular && g.n_fluid) ? t[0] / g.n_fluid : 0.0;
-    S[S_MEAN_Z] = m;
-    S[S_RHO_PREV] = S[S_RHO];
-    S[S_RHO] = t[1] - m * S[S_SUM_R];
+    b_last_close(P, t);
+  });
+}
+
+// ---- level-0 transfers as stencils -------------------------------------------------
+// On a structure whose level 1 aggregates 2 x 2 fine cells (T: the 0/1 map of a
+// solvable cell (i, j) to aggregate (i/2, j/2)), the smoothed prolongation and
+// the fused restriction of the hierarchy are
+//   P_1 = (I - W A) T,   M_1 = P_1^T (I - A W) = T^T (I - A W)^2,
+// A the fine operator, W its damped inverse diagonal (A symmetric, W diagonal).
+// Both then run as stencils over the fine cells instead of row gathers through
+// the stored matrices: the aggregate map is index arithmetic and A the flag
+// stencil, so a fine cell costs its flags, its residual and one level-1 value.
+// Each needs values two cells away, so a block takes a tile of output cells
+// (h_tr rows of x, 28 columns of y) and stages the tile with two halo cells on
+// each side (h_tr + 4 rows x 32 columns: lane = column) in shared memory: every
+// thread issues its loads of the tile at once, then the stages run on shared
+// memory between block barriers.  The arithmetic is the matrices' definition in
+// the storage type, so the results equal the matrix products to rounding (not
+// bit for bit).
+constexpr int kBHaloTC = 28;   // output columns of a tile (input: 32, two halo columns each side)
+// Most output rows of a tile (FP32 60, FP64 28: the staged arrays stay within
+// 48 KB); a problem's tiles take ceil(nx / ceil(nx / most)) rows, rounded up to even.
+template <class T>
+__host__ __device__ constexpr int b_halo_tr_max() { return sizeof(T) == 8 ? 28 : 60; }
+#ifndef PCFD_BHALO_MINB
+#define PCFD_BHALO_MINB 4
+#endif
+#define B_HALO_KERNEL __global__ void __launch_bounds__(kBThreads, PCFD_BHALO_MINB)
+
+// Cell index of a line of n cells at offset r (at most two past either end):
+// wrapped on a periodic axis, -1 off the grid.
+__device__ __forceinline__ int b_wrap2(int r, int n, int periodic) {
+  if (r < 0) r = periodic ? r + n : -1;
+  else if (r >= n) r = periodic ? r - n : -1;
+  return (r >= 0 && r < n) ? r : -1;
+}
+
+// A tile's staged arrays: input rows x 32 columns.
+template <class T>
+struct BHaloTile {
+  static constexpr int R = b_halo_tr_max<T>() + 4;
+  uint8_t f[R][32];                          // flags (0 off the grid)
+  T dg[R][32], wd[R][32];                    // diagonal, damped inverse diagonal
+  T a[R][32], b[R][32], c[R][32];            // the stages' vectors
+};
+
+// Stage 0 of a tile with first output cell (i0, j0): thread (warp w, lane)
+// loads input rows w, w + 8, ... of column j0 - 2 + lane -- the flags and
+// get(k) (cell index k; read at a valid index, dropped off the grid), all
+// loads first -- and stores the flags, the diagonal and weighted inverse
+// diagonal (b_diag and b_wdinv) and put(row, lane, f, wd, value).
+template <class T, class Get, class Put>
+__device__ __forceinline__ void b_tile_load(const BView& V, BHaloTile<T>& S, int rows, int i0, int j0,
+                                            const uint8_t* __restrict__ flags, Get get, Put put) {
+  constexpr int K = BHaloTile<T>::R / 8;
+  const int lane = (int)(threadIdx.x & 31), w = (int)(threadIdx.x >> 5);
+  const int nx = V.g.nx, ny = V.g.ny;
+  const int col = b_wrap2(j0 - 2 + lane, ny, V.g.periodic_y), cc = col >= 0 ? col : 0;
+  uint8_t fr[K];
+  T vr[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int row = b_wrap2(i0 - 2 + w + 8 * k, nx, V.g.periodic_x), rc = row >= 0 ? row : 0;
+    const int idx = rc * ny + cc;
+    const uint8_t fk = flags[idx];
+    const T vk = get(idx, rc, cc);
+    const bool ok = row >= 0 && col >= 0 && w + 8 * k < rows;
+    fr[k] = ok ? fk : (uint8_t)0;
+    vr[k] = ok ? vk : (T)0;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int ii = w + 8 * k;
+    if (ii >= rows) break;
+    const uint8_t fu = fr[k];
+    double d = 1.0, wv = V.w0 * (1.0 / 1.0);   // b_diag, b_wdinv off the solvable cells
+    if (fu & F_SOLV) {
+      const int i = b_wrap2(i0 - 2 + ii, nx, V.g.periodic_x);
+      if (V.any_dir && (i == 0 || col == 0 || i == nx - 1 || col == ny - 1)) {
+        d = fine_diag(fu, i, col, V.g);
+        wv = V.w0 * (1.0 / d);
+      } else {
+        d = V.dtab[fu & 15];
+        wv = V.wtab[fu & 15];
+      }
+    }
+    S.f[ii][lane] = fu;
+    S.dg[ii][lane] = (T)d;
+    S.wd[ii][lane] = (T)wv;
+    put(ii, lane, fu, (T)wv, vr[k]);
+  }
+}
+
+// (A x) at staged cell (ii, jl), b_apply5's terms in its order.
+template <class T>
+__device__ __forceinline__ T b_tile_apply(const BView& V, const BHaloTile<T>& S, const T (*x)[32], int ii, int jl) {
+  const uint8_t f = S.f[ii][jl];
+  T acc = S.dg[ii][jl] * x[ii][jl];
+  if (f & F_W) acc += (T)V.g.cx * x[ii - 1][jl];
+  if (f & F_E) acc += (T)V.g.cx * x[ii + 1][jl];
+  if (f & F_S) acc += (T)V.g.cy * x[ii][jl - 1];
+  if (f & F_N) acc += (T)V.g.cy * x[ii][jl + 1];
+  return acc;
+}
+
+// b_1 = T^T (I - A W)^2 b, b the projected CG residual (the fused restriction
+// from the fine level; pycfd/core/multigrid.py:436-447 with the sweep from zero).
+// One block per tile (map entries (problem, tile)).
+template <class T>
+B_HALO_KERNEL k_b_frestrict0(const BProb<T>* __restrict__ probs, const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
+  constexpr int K = BHaloTile<T>::R / 8, AC = kBHaloTC / 2;
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_solving(sh, e.x)) return;
+  B_VIEW(V, P);
+  __shared__ BHaloTile<T> S;
+  const T* __restrict__ r = P.r;
+  T* __restrict__ b1 = P.lb[1];
+  const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
+  const int nx = V.g.nx, ny = V.g.ny, ncy = (ny + 1) >> 1;
+  const int tr = P.h_tr, rows = tr + 4;
+  const int ti = e.y / P.h_tiles_j, tj = e.y - ti * P.h_tiles_j;
+  const int i0 = ti * tr, j0 = tj * kBHaloTC;
+  const int lane = (int)(threadIdx.x & 31), w = (int)(threadIdx.x >> 5);
+  // b (0 off the solvable cells) and y = W b
+  b_tile_load<T>(V, S, rows, i0, j0, P.flags, [&](int k, int, int) { return r[k]; },
+                 [&](int ii, int jl, uint8_t f, T wd, T rv) {
+                   const T bv = (f & F_SOLV) ? rv - mr : (T)0;
+                   S.b[ii][jl] = bv;
+                   S.a[ii][jl] = wd * bv;
+                 });
+  __syncthreads();
+  const bool inner_c = lane >= 1 && lane < 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {   // z = (I - A W) b in place of b, one cell in from the tile's edge
+    const int ii = w + 8 * k;
+    if (ii >= 1 && ii < rows - 1 && inner_c) S.b[ii][lane] -= b_tile_apply<T>(V, S, S.a, ii, lane);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {   // y = W z
+    const int ii = w + 8 * k;
+    if (ii >= 1 && ii < rows - 1 && inner_c) S.a[ii][lane] = S.wd[ii][lane] * S.b[ii][lane];
+  }
+  __syncthreads();
+  // (I - A W) z on the output cells, summed over each aggregate (rows, then columns)
+  for (int ag = (int)threadIdx.x; ag < (tr / 2) * AC; ag += kBThreads) {
+    const int ar = ag / AC, ac = ag - ar * AC;
+    const int gi = i0 + 2 * ar, gj = j0 + 2 * ac;
+    if (gi >= nx || gj >= ny) continue;
+    T zq[2][2];
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj) {
+        const int ii = 2 + 2 * ar + di, jl = 2 + 2 * ac + dj;
+        const T z2 = S.b[ii][jl] - b_tile_apply<T>(V, S, S.a, ii, jl);
+        zq[di][dj] = ((S.f[ii][jl] & F_SOLV) && gi + di < nx && gj + dj < ny) ? z2 : (T)0;
+      }
+    b1[(gi >> 1) * ncy + (gj >> 1)] = (zq[0][0] + zq[1][0]) + (zq[0][1] + zq[1][1]);
+  }
+}
+
+// The last two phases of the cycle in one pass: the prolongation onto the fine
+// level with its first sweep formed again, x_0 = W b + (I - W A) T x_1, and the
+// last sweep z = x_0 + W (b - A x_0), with sum(z) and r.z (k_b_fine FM_LAST).
+template <class T>
+B_HALO_KERNEL k_b_prolong_last(const BProb<T>* __restrict__ probs, const int2* __restrict__ map, BShared sh) {
+  pdl_begin();   // programmatic dependent launch: the predecessor's results first
+  constexpr int K = BHaloTile<T>::R / 8;
+  const int2 e = map[blockIdx.x];
+  const BProb<T>& P = probs[e.x];
+  if (!b_solving(sh, e.x)) return;
+  B_VIEW(V, P);
+  __shared__ BHaloTile<T> S;
+  const T* __restrict__ r = P.r;
+  const T* __restrict__ x1 = b_lvl_x(P, 1, 1);
+  T* __restrict__ zo = P.z;
+  const T mr = (T)(P.singular ? P.S[S_MEAN_R] : 0.0);
+  const int nx = V.g.nx, ny = V.g.ny, ncy = (ny + 1) >> 1;
+  const int tr = P.h_tr, rows = tr + 4;
+  const int ti = e.y / P.h_tiles_j, tj = e.y - ti * P.h_tiles_j;
+  const int i0 = ti * tr, j0 = tj * kBHaloTC;
+  const int lane = (int)(threadIdx.x & 31), w = (int)(threadIdx.x >> 5);
+  // b (0 off the solvable cells) in b, T x_1 (the cell's aggregate value) in a;
+  // the residual itself in c for r.z
+  b_tile_load<T>(V, S, rows, i0, j0, P.flags, [&](int k, int rc, int cc) { return r[k]; },
+                 [&](int ii, int jl, uint8_t f, T, T rv) {
+                   S.b[ii][jl] = (f & F_SOLV) ? rv - mr : (T)0;
+                   S.c[ii][jl] = rv;
+                 });
+  {
+    const int col = b_wrap2(j0 - 2 + lane, ny, V.g.periodic_y), cc = col >= 0 ? col : 0;
+    T xg[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int row = b_wrap2(i0 - 2 + w + 8 * k, nx, V.g.periodic_x), rc = row >= 0 ? row : 0;
+      xg[k] = x1[(rc >> 1) * ncy + (cc >> 1)];
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int ii = w + 8 * k;
+      if (ii < rows) S.a[ii][lane] = (S.f[ii][lane] & F_SOLV) ? xg[k] : (T)0;   // this thread's own flags
+    }
+  }
+  __syncthreads();
+  const bool inner_c = lane >= 1 && lane < 31;
+  T x0[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {   // x_0 = W b + (t - W A t), one cell in from the tile's edge
+    const int ii = w + 8 * k;
+    x0[k] = (T)0;
+    if (ii >= 1 && ii < rows - 1 && inner_c) {
+      const T wd = S.wd[ii][lane];
+      const T s = S.a[ii][lane] - wd * b_tile_apply<T>(V, S, S.a, ii, lane);   // (P_1 x_1) at the cell
+      x0[k] = wd * S.b[ii][lane] + s;
+    }
+  }
+  __syncthreads();   // every read of t done: x_0 goes in its place
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int ii = w + 8 * k;
+    if (ii >= 1 && ii < rows - 1 && inner_c) S.a[ii][lane] = x0[k];
+  }
+  __syncthreads();
+  double acc[2] = {0, 0};
+  const int gj = j0 - 2 + lane;
+  if (lane >= 2 && lane < 30 && gj < ny) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {   // z = x_0 + W (b - A x_0) on the output cells
+      const int ii = w + 8 * k, gi = i0 - 2 + ii;
+      if (ii < 2 || ii >= rows - 2 || gi >= nx) continue;
+      const T xnew = S.a[ii][lane] + S.wd[ii][lane] * (S.b[ii][lane] - b_tile_apply<T>(V, S, S.a, ii, lane));
+      zo[gi * ny + gj] = xnew;
+      if (S.f[ii][lane] & F_SOLV) {
+        acc[0] += (double)xnew;
+        acc[1] += (double)S.c[ii][lane] * (double)xnew;
+      }
+    }
+  }
+  b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.h_tiles, [&](double* t) {
+    b_last_close(P, t);
   });
 }
 
@@ -1135,12 +1426,6 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
 // residual).  EO_PROLONGW: prolongation onto a level whose first-sweep iterate
 // W b was not stored -- it is formed again, with the same T roundings.
 enum BEllOp { EO_RESTRICT = 0, EO_PRE, EO_SMOOTH, EO_RESID, EO_PROLONG, EO_FRESTRICT, EO_PROLONGW };
-
-template <class T>
-__device__ __forceinline__ T* b_lvl_x(const BProb<T>& P, int d, int sel) {
-  if (d == P.nlev - 1 || d == P.tail) return P.lxa[d];   // coarsest and tail results are in xa
-  return sel == 0 ? P.lxa[d] : P.lxb[d];
-}
 
 // Row dot product of E by L lanes (L a power of two, runtime), rows past the
 // end contribute nothing; every lane of the warp calls it.

@@ -25,6 +25,8 @@ struct pycfd_batch {
   int fused = 0;                           // down sweep by fused restrictions (every structure has them)
   int fused_from = 1;                      // first level restricted by the fused product (1 or 2)
   int ell_group = kBGroup;                 // problems per block of the coarse-level launches (1 or kBGroup)
+  int stencil_req = 0;                     // level-0 transfers as stencils, as asked
+  int stencil = 0;                         // ... and in force (fused down sweep from the fine level)
   int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
@@ -34,6 +36,7 @@ struct pycfd_batch {
   int depth = 0;                           // most levels of any problem
   BMapHost fine;                           // every chunk of tiles of every problem
   BMapHost strip;                          // every chunk of warp strips of every problem (solver kernels)
+  BMapHost halo;                           // every staged tile of every problem (stencil transfers)
   BMapHost pstrip;                         // every chunk of predictor strips of every problem
   // row-block maps per depth d (problems whose level d runs per level):
   // grouped maps per depth d, entries (structure, row block x 1024 + group of ell_group problems):
@@ -77,6 +80,8 @@ int upload_hier(pycfd_batch* B, const pycfd_solver_desc* d, BHier<T>* H, std::ve
   keep->resize(Lv);
   H->nlev = Lv;
   H->w0 = d->levels[0].weight;
+  H->agg2 = Lv >= 2 && d->levels[1].shape_x == (d->nx + 1) / 2 && d->levels[1].shape_y == (d->ny + 1) / 2 &&
+            d->levels[1].n == d->levels[1].shape_x * d->levels[1].shape_y;
   for (int l = 1; l < Lv; ++l) {
     const pycfd_mg_level& in = d->levels[l];
     const pycfd_mg_level& up = d->levels[l - 1];
@@ -175,7 +180,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 
   // per-problem records
   std::vector<BProb<T>> pr(n);
-  std::vector<int2> fine, strip, pstrip;
+  std::vector<int2> fine, strip, pstrip, halo;
   B->nlev.assign(n, 0);
   B->depth = 0;
   int red_rows = 0;
@@ -200,7 +205,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.tiles = P.tiles_i * P.tiles_j;
     P.chunk_tiles = std::max(1, kBChunkCells / (B->tile_i * kBTileJ));
     P.chunks = (P.tiles + P.chunk_tiles - 1) / P.chunk_tiles;
-    P.s_segs = (s->g.ny + 31) / 32;
+    P.s_segs = (s->g.ny + kBSegCols - 1) / kBSegCols;
     P.s_items = ((s->g.nx + kBStripRows - 1) / kBStripRows) * P.s_segs;
     P.s_chunks = (P.s_items + kBStripItems - 1) / kBStripItems;
     {
@@ -208,8 +213,19 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       const int items = segs * ((s->g.nx + 3 + kBStripRows - 1) / kBStripRows);
       P.p_chunks = (items + kBStripItems - 1) / kBStripItems;
     }
+    {
+      // staged tiles of the stencil transfers: as few row bands as the most rows
+      // allow, of even height (aggregates pair rows)
+      const int most = b_halo_tr_max<T>();
+      const int bands = (s->g.nx + most - 1) / most;
+      int tr = (s->g.nx + bands - 1) / bands;
+      tr += tr & 1;
+      P.h_tr = tr;
+      P.h_tiles_j = (s->g.ny + kBHaloTC - 1) / kBHaloTC;
+      P.h_tiles = ((s->g.nx + tr - 1) / tr) * P.h_tiles_j;
+    }
     P.red_base = red_rows;
-    red_rows += std::max(P.chunks, P.s_chunks);
+    red_rows += std::max(std::max(P.chunks, P.s_chunks), P.h_tiles);
     P.flags = s->flags;
     P.solid = s->solid;
     P.bc_kind = s->bc_kind_dev;
@@ -268,10 +284,12 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
     for (int c = 0; c < P.s_chunks; ++c) strip.push_back(make_int2(i, c));
+    for (int c = 0; c < P.h_tiles; ++c) halo.push_back(make_int2(i, c));
     for (int c = 0; c < P.p_chunks; ++c) pstrip.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
   TRY(upload_map(B, &B->strip, strip));
+  TRY(upload_map(B, &B->halo, halo));
   TRY(upload_map(B, &B->pstrip, pstrip));
   // problems grouped by structure (the dense tail's block groups)
   {
@@ -297,6 +315,13 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
   B->fused = (B->coarse == 0 && B->sweeps == 1) ? 1 : 0;
   for (size_t h = 0; h < leaders.size(); ++h)
     if (!hh[h].fused || hh[h].tail_level == 0) B->fused = 0;
+  // level-0 transfers as stencils: they stand for P_1 and M_1 of the 2 x 2
+  // aggregation, so every structure must have that level 1
+  B->stencil = (B->stencil_req && B->fused && B->fused_from == 1) ? 1 : 0;
+  for (size_t h = 0; B->stencil && h < leaders.size(); ++h)
+    if (!hh[h].agg2)
+      return fail(PCFD_E_UNSUPPORTED, "stencil transfers: structure %d's level 1 is not the 2 x 2 aggregation",
+                  (int)h);
   B->mapA.assign(B->depth, BMapHost{});
   B->mapR.assign(B->depth, BMapHost{});
   B->mapP.assign(B->depth, BMapHost{});
@@ -442,6 +467,19 @@ int b_fine(pycfd_batch* B, int src, int dst, cudaStream_t st) {
   return 0;
 }
 
+// Level-0 transfers as stencils over every problem's staged tiles: the fused
+// restriction into level 1 (up = false) or the prolongation from level 1 with
+// the last fine sweep (up = true).
+template <class T>
+int b_stencil_transfer(pycfd_batch* B, bool up, cudaStream_t st) {
+  const int id = up ? 2 : 3;
+  b_prof(B, id, st);
+  if (up) BLAUNCH(k_b_prolong_last<T>, B->halo.n, kBThreads, 0, st, probs_of<T>(B), B->halo.e, B->sh);
+  else BLAUNCH(k_b_frestrict0<T>, B->halo.n, kBThreads, 0, st, probs_of<T>(B), B->halo.e, B->sh);
+  b_prof(B, id, st);
+  return 0;
+}
+
 // The dense tails of every tailed structure, one launch after the down sweep
 // (each block reads its structure's tail depth).
 template <class T>
@@ -468,6 +506,7 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
     if (fine_kept) TRY((b_fine<T, FM_PRE>(B, 0, 0, st)));
     for (int d = 1; d < D; ++d) {
       if (d < B->fused_from) TRY((b_ell<T, EO_RESTRICT>(B, B->mapR[d], d, 0, 0, st)));
+      else if (d == 1 && B->stencil) TRY(b_stencil_transfer<T>(B, false, st));
       else TRY((b_ell<T, EO_FRESTRICT>(B, B->mapR[d], d, 0, 0, st)));
     }
     TRY(b_tails<T>(B, st));
@@ -477,6 +516,7 @@ int b_vcycle(pycfd_batch* B, cudaStream_t st) {
       TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[d], d, 1, 0, st)));
       TRY((b_ell<T, EO_SMOOTH>(B, B->mapA[d], d, 0, 1, st)));
     }
+    if (B->stencil) return b_stencil_transfer<T>(B, true, st);   // prolongation and last sweep in one pass
     if (fine_kept) TRY((b_ell<T, EO_PROLONG>(B, B->mapP[0], 0, 1, 0, st)));   // x_0 stored by FM_PRE
     else TRY((b_ell<T, EO_PROLONGW>(B, B->mapP[0], 0, 1, 0, st)));
     TRY((b_fine<T, FM_LAST>(B, 0, 2, st)));
@@ -788,6 +828,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->coarse = opts->coarse_level;
   B->fused_from = opts->fused_from == 2 ? 2 : 1;
   B->ell_group = opts->ell_group == 1 ? 1 : kBGroup;
+  B->stencil_req = opts->stencil_transfer ? 1 : 0;
   B->mem = new pycfd_solver();
   B->mem->pdl = opts->programmatic_launch ? 1 : 0;
   B->solvers.assign(n, nullptr);

@@ -251,6 +251,43 @@ def test_fused_restriction_matches_two_phase_down_sweep(precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stencil_transfers_match_stored_matrices(precision):
+    """Level-0 transfers as stencils over the fine cells (the fused restriction
+    T^T (I - A W)^2 and the prolongation (I - W A) T with the last sweep) against the
+    products with the stored P_1 and M_1: cavities of odd and even size, and the
+    reference cases (periodic axes, an obstacle with an outlet, a periodic-y channel)."""
+    from pycfd_b200.batch import BatchedSolver, BatchOptions, cavity_batch_configs
+    cav = cavity_batch_configs(count=6, seed=9, sizes=(25, 32, 37, 48), re_range=(100.0, 1000.0), tol=1e-11)
+    probs = [_case(n) for n in ("periodic_mgcg", "inout_sym_obstacle_mgcg")]
+    # the periodic-y channel on a grid with three levels (its own 20 x 16 has two, so no tail)
+    chan = _case("periodic_y_sym_mgcg")[0].replace(nx=40, ny=32)
+    probs.append((chan, None, None, None, dict(steps=6)))
+    batches = [dict(configs=cav, steps=6),
+               dict(configs=[p[0] for p in probs], steps=min(p[4]["steps"] for p in probs) - 1,
+                    kw=dict(obstacles=[p[1] for p in probs], u_init=[p[2] for p in probs],
+                            v_init=[p[3] for p in probs]))]
+    bound = 1e-9 if precision == "fp64" else 1e-7
+    for bt in batches:
+        out, its = [], []
+        for stencil in (True, False):
+            b = BatchedSolver(bt["configs"], BatchOptions(precision=precision, fused_restriction=True,
+                                                           tail_ratio=None, stencil_transfer=stencil),
+                              **bt.get("kw", {}))
+            assert b._fused and b._stencil == stencil
+            b.step(bt["steps"])
+            st = b.status()
+            assert all(f == 0 for f in st["frozen"])
+            out.append([b.fields[k].numpy() for k in range(len(bt["configs"]))])
+            its.append(st["iterations"])
+            for k in range(len(bt["configs"])):
+                assert b.field_stats(k).max_div < 1e-8
+        for fa, fb in zip(*out):
+            for x, y in zip(fa[:2], fb[:2]):
+                assert rel(x, y) < bound
+        assert np.abs(its[0] - its[1]).max() <= 2, its
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_loop_cap_ends_device_loops_and_the_batch_goes_on(precision):
     """The pass cap of the device-side WHILE loops, set low from the host, ends every
     solve of a step early (reported per loop, problems unconverged, no hang); with
