@@ -301,14 +301,14 @@ __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Ge
 
 // ---- warp strips of one grid ------------------------------------------------
 // The fine-level solver kernels walk the grid in warp strips: a warp takes one
-// 32-column segment of y (lane = column: every row load is one coalesced
-// access) over kStripRows rows of x.  The stencil operand of the strip and its
-// two halo rows are formed once, into registers, before any arithmetic; the
-// y-neighbours come from the adjacent lanes by shuffle.  The columns just west
-// and east of the segment are the same for the whole warp, so every lane forms
-// them (one broadcast load per row) and lanes 0 and `last` use them: no load
-// sits under a lane-dependent branch, none waits for another, and the whole
-// strip's loads are in flight at once.  Off-grid rows and columns are read at a
+// segment of y (lane = column: every row load is one coalesced access) over
+// kStripRows rows of x.  The stencil operand of the strip and its two halo rows
+// are formed once, into registers, before any arithmetic; the y-neighbours come
+// from the adjacent lanes by shuffle.  A stencil kernel's segment is 30 columns,
+// lanes 1..30, and lanes 0 and 31 hold the columns just west and east of it, so
+// each lane forms one operand value per row, no load sits under a lane-dependent
+// branch and the whole strip's loads are in flight at once; a pointwise kernel
+// takes aligned 32-column segments.  Off-grid rows and columns are read at a
 // clamped (valid) index and the value dropped.
 // Blocks of 256 threads (8 warps) stride over the items (strip x segment).
 #ifndef PCFD_STRIP_ROWS
@@ -317,7 +317,11 @@ __device__ __forceinline__ T fine_apply(uint8_t f, int i, int j, int c, const Ge
 constexpr int kStripRows = PCFD_STRIP_ROWS;
 constexpr int kStripThreads = 256;
 
-inline int strip_items(const Geo& g) { return ((g.ny + 31) / 32) * ((g.nx + kStripRows - 1) / kStripRows); }
+constexpr int kStripSegCols = 30;   // output columns of a stencil kernel's segment (lanes 1..30)
+// items of the stencil kernels (the pointwise kernels' 32-column segments are no more)
+inline int strip_items(const Geo& g) {
+  return ((g.ny + kStripSegCols - 1) / kStripSegCols) * ((g.nx + kStripRows - 1) / kStripRows);
+}
 inline int strip_grid(const Geo& g) {
   const int b = (strip_items(g) + kStripThreads / 32 - 1) / (kStripThreads / 32);
   return b < kMaxRedBlocks ? (b < 1 ? 1 : b) : kMaxRedBlocks;
@@ -349,34 +353,35 @@ __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body
   constexpr int RS = kStripRows;
   const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
   const int nx = g.nx, ny = g.ny;
-  const int segs = (ny + 31) / 32;
+  const int segs = STENCIL ? (ny + kStripSegCols - 1) / kStripSegCols : (ny + 31) / 32;
   const int items = segs * ((nx + RS - 1) / RS);
   const int wpb = (int)(blockDim.x >> 5);
   for (int it = (int)blockIdx.x * wpb + warp; it < items; it += (int)gridDim.x * wpb) {
     const int strip = it / segs, seg = it - strip * segs;
-    const int i0 = strip * RS, j0 = seg * 32, j = j0 + lane;
-    const bool jv = j < ny;
-    const int jc = jv ? j : ny - 1;
-    const int last = min(31, ny - 1 - j0);
+    const int i0 = strip * RS;
+    int j, jc;
+    bool jv;
+    int jh = -1;   // STENCIL: the operand's column (wrapped), -1 off the grid
+    if (STENCIL) {
+      j = seg * kStripSegCols - 1 + lane;   // lanes 0 and 31: the columns beside the segment
+      jh = j;
+      if (jh < 0) jh = g.periodic_y ? jh + ny : -1;
+      else if (jh >= ny) jh = (g.periodic_y && jh == ny) ? 0 : -1;
+      jc = jh >= 0 ? jh : (j < 0 ? 0 : ny - 1);
+      jv = lane >= 1 && lane <= 30 && j < ny;
+    } else {
+      j = seg * 32 + lane;
+      jv = j < ny;
+      jc = jv ? j : ny - 1;
+    }
     double ov[STENCIL ? RS + 2 : 1];
-    double ew[STENCIL ? RS : 1], ee[STENCIL ? RS : 1];
     if (STENCIL) {
 #pragma unroll
       for (int u = 0; u < RS + 2; ++u) {
         const int r = strip_row(i0 - 1 + u, nx, g.periodic_x);
         const int rc = r >= 0 ? r : 0;
         const double val = op(rc * ny + jc, rc, jc);
-        ov[u] = (jv && r >= 0) ? val : 0.0;
-      }
-      int jw, je;
-      strip_edges(j0, last, ny, g.periodic_y, &jw, &je);
-      const int jwc = jw >= 0 ? jw : 0, jec = je >= 0 ? je : 0;
-#pragma unroll
-      for (int u = 0; u < RS; ++u) {
-        const int i = i0 + u, ic = i < nx ? i : nx - 1;
-        const double vw = op(ic * ny + jwc, ic, jwc), ve = op(ic * ny + jec, ic, jec);
-        ew[u] = (jw >= 0 && i < nx) ? vw : 0.0;
-        ee[u] = (je >= 0 && i < nx) ? ve : 0.0;
+        ov[u] = (jh >= 0 && r >= 0) ? val : 0.0;
       }
     }
 #pragma unroll
@@ -393,8 +398,6 @@ __device__ __forceinline__ void strip_cells(const Geo& g, Op op, Load load, Body
         e = ov[u + 2];
         sv = __shfl_up_sync(0xffffffffu, c, 1);
         nv = __shfl_down_sync(0xffffffffu, c, 1);
-        if (lane == 0) sv = ew[u];
-        if (lane == last) nv = ee[u];
       }
       const int i = i0 + u;
       if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
