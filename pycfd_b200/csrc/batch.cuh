@@ -1466,6 +1466,15 @@ constexpr int kBGroup = 8;         // problems per block of the grouped form
 template <int GS>
 __host__ __device__ constexpr int b_ell_rounds() { return GS == 1 ? 8 : PCFD_BELL_ROUNDS; }   // rounds of kBThreads / L rows
 
+// What the fine level's weighted inverse diagonal (b_wdinv) needs, held by a
+// coarse-level block: the structure's geometry scalars in registers and its
+// weight table in shared memory.
+struct BFineW {
+  int nx, ny, any_dir;
+  double w0;
+  const double* wtab;
+};
+
 // The group's vectors for one op, filled from the problem records by the first
 // GS threads; a null output marks a member that is absent or not solving.
 template <class T, int GS>
@@ -1532,7 +1541,7 @@ __device__ __forceinline__ void b_group_fill(BGroup<T, GS>& G, int g, const BPro
 // (value, column) pairs loaded together and then every member's four gathers,
 // so a row costs one dependent load pair per four entries per lane.
 template <int L, int OP, int GS, class T>
-__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const uint8_t* __restrict__ flags,
+__device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const BFineW& fw, const uint8_t* __restrict__ flags,
                                             const BGroup<T, GS>& G, const Ell<T>& E,
                                             const T* __restrict__ wd, int d, int rb) {
   constexpr int per = kBThreads / L;
@@ -1600,6 +1609,25 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const uint8_t* _
   for (int rd = 0; rd < ROUNDS; ++rd) {
     const int row = (rb * ROUNDS + rd) * per + (int)threadIdx.x / L;
     if (row >= n) continue;
+    // the row's W (fine level: b_wdinv of the cell, from the block's copy of the
+    // weight table) and solvable flag, formed once for the group
+    T wrow = (T)0;
+    bool srow = true;
+    if (OP == EO_PROLONGW && d == 0) {
+      const uint8_t f = flags[row];
+      srow = (f & F_SOLV) != 0;
+      double w = fw.w0 * (1.0 / 1.0);
+      if (srow) {
+        const int i = row / fw.ny, j = row - i * fw.ny;
+        if (fw.any_dir && (i == 0 || j == 0 || i == fw.nx - 1 || j == fw.ny - 1))
+          w = fw.w0 * (1.0 / fine_diag(f, i, j, P0.g));
+        else
+          w = fw.wtab[f & 15];
+      }
+      wrow = (T)w;
+    } else if (OP == EO_PROLONGW) {
+      wrow = wd[row];
+    }
 #pragma unroll
     for (int g = 0; g < GS; ++g) {
       T* __restrict__ o = G.out[g];
@@ -1610,12 +1638,10 @@ __device__ __forceinline__ void b_ellg_rows(const BProb<T>& P0, const uint8_t* _
         case EO_PROLONGW: {
           T wb;
           if (d == 0) {
-            const uint8_t f = flags[row];
-            const int i = row / P0.g.ny, j = row - i * P0.g.ny;
-            const T bfr = (f & F_SOLV) ? G.b[g][row] - mr[g] : (T)0;
-            wb = (T)b_wdinv(P0, f, i, j) * bfr;
+            const T bfr = srow ? G.b[g][row] - mr[g] : (T)0;
+            wb = wrow * bfr;
           } else {
-            wb = wd[row] * G.b[g][row];
+            wb = wrow * G.b[g][row];
           }
           o[row] = wb + s;
           break;
@@ -1669,6 +1695,9 @@ __global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BPro
   const T* wd = d > 0 ? H.lv[d].wd : nullptr;
   const BProb<T>& P0 = probs[sprobs[H.sp0 + grp * GS]];   // the structure's geometry and flags
   const uint8_t* flags0 = P0.flags;
+  __shared__ double wt0[16];
+  if (OP == EO_PROLONGW && d == 0 && threadIdx.x >= 32 && threadIdx.x < 48) wt0[threadIdx.x - 32] = P0.wtab[threadIdx.x - 32];
+  const BFineW fw{P0.g.nx, P0.g.ny, P0.any_dir, P0.w0, wt0};
   if (threadIdx.x < 32) {   // GS <= 32: the members are lanes of warp 0
     const int k = grp * GS + (int)threadIdx.x;
     const BProb<T>* P = nullptr;
@@ -1683,11 +1712,11 @@ __global__ void __launch_bounds__(kBThreads, PCFD_BELL_MINB) k_b_ellg(const BPro
   __syncthreads();
   if (!any) return;
   switch (Lop) {
-    case 1: b_ellg_rows<1, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
-    case 4: b_ellg_rows<4, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
-    case 8: b_ellg_rows<8, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
-    case 16: b_ellg_rows<16, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
-    default: b_ellg_rows<32, OP, GS>(P0, flags0, G, E, wd, d, rb); break;
+    case 1: b_ellg_rows<1, OP, GS>(P0, fw, flags0, G, E, wd, d, rb); break;
+    case 4: b_ellg_rows<4, OP, GS>(P0, fw, flags0, G, E, wd, d, rb); break;
+    case 8: b_ellg_rows<8, OP, GS>(P0, fw, flags0, G, E, wd, d, rb); break;
+    case 16: b_ellg_rows<16, OP, GS>(P0, fw, flags0, G, E, wd, d, rb); break;
+    default: b_ellg_rows<32, OP, GS>(P0, fw, flags0, G, E, wd, d, rb); break;
   }
 }
 
