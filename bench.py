@@ -378,6 +378,9 @@ def run_batch(args, world, rank, local):
                             fused_restriction=args.fused_from > 0, fused_from=max(1, args.fused_from),
                             ell_group=args.ell_group, programmatic_launch=args.pdl,
                             stencil_transfer=args.stencil)
+    if args.scalar_strips:
+        import dataclasses
+        opts = dataclasses.replace(opts, scalar_strips=True)
     b = ConcurrentBatch(cfgs, opts, parts=args.parts) if args.parts > 1 else BatchedSolver(cfgs, opts)
     setup = time.perf_counter() - t0
     rec = not args.eager
@@ -921,6 +924,9 @@ def main():
                     help="batch, --no-autotune: programmatic dependent launch between the kernels")
     ap.add_argument("--stencil", action="store_true",
                     help="batch, --no-autotune, --fused-from 1: level-0 transfers as stencils over the fine cells")
+    ap.add_argument("--scalar-strips", action="store_true",
+                    help="batch: the FP32 CG and level-0 sweep kernels on 30-column scalar strips "
+                         "(default: 128-column float4 strips)")
     ap.add_argument("--ell-group", type=int, default=8, choices=[1, 8],
                     help="batch, --no-autotune: problems per coarse-level block sharing the matrix loads")
     ap.add_argument("--no-profile", action="store_true",

@@ -468,6 +468,13 @@ typedef struct {
                                  and its P_1 must be that smoothed aggregation (the
                                  hierarchy this library's host side builds).  Equal to
                                  the matrix products to rounding.  0: the products. */
+    int scalar_strips;        /* 1: the mixed form's FP32 CG and level-0 sweep kernels
+                                 walk every problem in 30-column scalar strips; 0:
+                                 problems whose ny is a multiple of 4 walk 128-column
+                                 vector strips (four cells per lane, 16-byte loads),
+                                 the same per-cell arithmetic, the per-problem sums
+                                 added in another order.  The FP64 form always
+                                 walks scalar strips.                              */
 } pycfd_batch_opts;
 
 /* n problems: descs[i] describes problem i (time_scheme PCFD_RK3; solver

@@ -93,7 +93,8 @@ class BatchOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("maxiter", C.c_int),
                 ("inner_tol", C.c_double), ("mg_sweeps", C.c_int), ("tile_rows", C.c_int),
                 ("coarse_level", C.c_int), ("fused_from", C.c_int), ("ell_group", C.c_int),
-                ("programmatic_launch", C.c_int), ("stencil_transfer", C.c_int)]
+                ("programmatic_launch", C.c_int), ("stencil_transfer", C.c_int),
+                ("scalar_strips", C.c_int)]
 
 
 class Stats(C.Structure):

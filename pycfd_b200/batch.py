@@ -266,6 +266,9 @@ class BatchOptions:
     #: with the fused down sweep from the fine level: the level-0 <-> level-1 transfers
     #: as stencils over the fine cells instead of products with the stored matrices
     stencil_transfer: bool = False
+    #: mixed form: the FP32 CG and level-0 sweep kernels walk 30-column scalar strips
+    #: everywhere (off: 128-column float4 strips on problems whose ny is a multiple of 4)
+    scalar_strips: bool = False
 
 
 class BatchedSolver:
@@ -367,7 +370,8 @@ class BatchedSolver:
         bo = _lib.BatchOpts(1 if opts.precision == "mixed" else 0, float(tol), int(maxiter),
                             float(opts.inner_tol), int(opts.mg_sweeps), int(opts.tile_rows),
                             int(opts.coarse_level), int(opts.fused_from), int(opts.ell_group),
-                            int(bool(opts.programmatic_launch)), int(self._stencil))
+                            int(bool(opts.programmatic_launch)), int(self._stencil),
+                            int(bool(opts.scalar_strips)))
         if max_steps is None:
             ms = None
         else:

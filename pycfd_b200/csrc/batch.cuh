@@ -69,6 +69,7 @@ struct BProb {
   int tile_i, tiles_i, tiles_j, tiles;   // fine tiles: tile_i rows x 32 columns
   int chunk_tiles, chunks;               // a block of a fine launch takes a chunk of tiles
   int s_segs, s_items, s_chunks;         // warp strips of the solver kernels (b_strips)
+  int vec, v_chunks;                     // vector strips (b_vstrips) in force; their blocks
   int p_chunks;                          // warp-strip chunks of the predictor (ghosted arrays)
   int h_tr, h_tiles_j, h_tiles;          // staged tiles of the level-0 stencil transfers: rows, tiles
   int red_base;                          // first partial row of this problem
@@ -110,6 +111,10 @@ struct BShared {
 };
 
 enum BTicket { TK_CG = 0, TK_IR = 1, TK_ARM = 2, TK_COUNT = 4 };
+
+// Blocks of problem P in a launch of the FP32 solver kernels (vector or scalar strips).
+template <class T>
+__device__ __forceinline__ int b_nchunks(const BProb<T>& P) { return P.vec ? P.v_chunks : P.s_chunks; }
 
 __device__ __forceinline__ bool b_frozen(const BShared& sh, int p) { return sh.frozen[p] != 0; }
 __device__ __forceinline__ bool b_solving(const BShared& sh, int p) { return sh.solving[p] != 0; }
@@ -439,6 +444,123 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
       }
       const int i = i0 + u;
       if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, sv, nv);
+    }
+  }
+}
+
+// ---- vector strips (FP32 vectors, ny a multiple of 4) ------------------------------
+// The FP32 kernels of the mixed form's inner solve walk a problem in vector
+// strips when its rows are a multiple of 4 long: a lane holds four adjacent
+// columns of y as one 16-byte float4 (every row starts 16-byte aligned), so a
+// warp covers a 128-column segment of a row with ONE load instruction per array
+// (the flags as one 32-bit word), against one per cell in the scalar strips,
+// and the index arithmetic, clamps and per-row bookkeeping are paid once per
+// four cells.  The operand's y-neighbours are the neighbouring elements, across
+// lanes by shuffle; the two columns beside the segment come from one scalar
+// operand value per row: lane 0 forms the column west of the segment, lane 31
+// the one east of it (on a segment narrower than 128 columns, the first lane
+// past the grid forms it and passes it down by the same shuffle).  A block
+// takes kBVecRows rows of its problem, all segments.  Per cell the arithmetic
+// is the scalar strips' (the same operand, stencil and update); only the order
+// of the per-problem sums differs.
+#ifndef PCFD_BVEC_ROWS
+#define PCFD_BVEC_ROWS 16
+#endif
+constexpr int kBVecRows = PCFD_BVEC_ROWS;   // rows of one block of a vector-strip launch
+constexpr int kBVecCols = 128;              // columns of a warp segment (32 lanes x float4)
+
+__device__ __forceinline__ float4 b_ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void b_st4(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ uint32_t b_ldf4(const uint8_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
+__device__ __forceinline__ uint8_t b_fl(uint32_t w, int e) { return (uint8_t)(w >> (8 * e)); }
+__device__ __forceinline__ float b_el(const float4& a, int e) {
+  return e == 0 ? a.x : e == 1 ? a.y : e == 2 ? a.z : a.w;
+}
+
+// op4(k, i, j): the operand at cells k..k+3 of row i (k = i*ny + j, j a multiple
+// of 4; issues its loads).  op1(k, i, j): the operand at one cell (the segment's
+// edge columns).  load(u, k): the per-cell loads of body row u.  body(u, k, i,
+// j, c, w, e, s, n): the four cells k..k+3 of row i, each argument a float[4]
+// (centre, i-1, i+1, j-1, j+1).  STENCIL = false: no operand, no edges (the
+// arguments are zeros).  RS: rows per warp item, a divisor of kBVecRows.
+template <bool STENCIL, int RS, class Op4, class Op1, class Load, class Body>
+__device__ __forceinline__ void b_vstrips(const BView& V, int chunk, Op4 op4, Op1 op1, Load load, Body body) {
+  static_assert(kBVecRows % RS == 0, "rows per item must divide the block's rows");
+  const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+  const int nx = V.g.nx, ny = V.g.ny;
+  const int segs = (ny + kBVecCols - 1) / kBVecCols;
+  const int r0 = chunk * kBVecRows;
+  const int items = segs * ((min(nx - r0, kBVecRows) + RS - 1) / RS);
+  for (int it = warp; it < items; it += kBThreads / 32) {
+    const int strip = it / segs, seg = it - strip * segs;
+    const int i0 = r0 + strip * RS;
+    const int j0 = seg * kBVecCols;
+    const int nl = min(32, (ny - j0) >> 2);   // lanes over columns of the grid
+    const int j = j0 + 4 * lane;
+    const bool jv = lane < nl;
+    const int jc = jv ? j : j0;               // an aligned valid column for the loads
+    float ov[STENCIL ? RS + 2 : 1][4];
+    float eg[STENCIL ? RS : 1];
+    if constexpr (STENCIL) {
+      // the edge column this lane forms: west of the segment (lane 0), east of it
+      // (lane 31 on a full segment, else the first lane past the grid); -1 none
+      const int le = nl < 32 ? nl : 31;
+      int jh = -1;
+      if (lane == 0) jh = j0 > 0 ? j0 - 1 : (V.g.periodic_y ? ny - 1 : -1);
+      else if (lane == le) jh = j0 + 4 * nl < ny ? j0 + 4 * nl : (V.g.periodic_y ? 0 : -1);
+      const int jhc = jh >= 0 ? jh : j0;
+#pragma unroll
+      for (int u = 0; u < RS + 2; ++u) {
+        const int r = strip_row(i0 - 1 + u, nx, V.g.periodic_x);
+        const int rc = r >= 0 ? r : 0;
+        const float4 a = op4(rc * ny + jc, rc, jc);
+        const bool ok = jv && r >= 0;
+        ov[u][0] = ok ? a.x : 0.f;
+        ov[u][1] = ok ? a.y : 0.f;
+        ov[u][2] = ok ? a.z : 0.f;
+        ov[u][3] = ok ? a.w : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < RS; ++u) {
+        const int i = i0 + u, ic = i < nx ? i : nx - 1;
+        const float h = op1(ic * ny + jhc, ic, jhc);
+        eg[u] = (jh >= 0 && i < nx) ? h : 0.f;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      const int i = i0 + u, ic = i < nx ? i : nx - 1;
+      load(u, ic * ny + jc);
+    }
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f}, w[4] = {0.f, 0.f, 0.f, 0.f}, e[4] = {0.f, 0.f, 0.f, 0.f};
+      float s[4] = {0.f, 0.f, 0.f, 0.f}, n[4] = {0.f, 0.f, 0.f, 0.f};
+      if constexpr (STENCIL) {
+        // j-1 of element 0 and j+1 of element 3 from the adjacent lanes (the
+        // first lane past the grid carries the east edge in its element 0)
+        const float up = __shfl_up_sync(0xffffffffu, ov[u + 1][3], 1);
+        const float x0 = (nl < 32 && lane == nl) ? eg[u] : ov[u + 1][0];
+        const float dn = __shfl_down_sync(0xffffffffu, x0, 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          c[q] = ov[u + 1][q];
+          w[q] = ov[u][q];
+          e[q] = ov[u + 2][q];
+        }
+        s[0] = lane == 0 ? eg[u] : up;
+        s[1] = c[0];
+        s[2] = c[1];
+        s[3] = c[2];
+        n[0] = c[1];
+        n[1] = c[2];
+        n[2] = c[3];
+        n[3] = lane == 31 ? eg[u] : dn;
+      }
+      const int i = i0 + u;
+      if (jv && i < nx) body(u, i * ny + j, i, j, c, w, e, s, n);
     }
   }
 }
@@ -824,15 +946,50 @@ B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
     return pk * tb + z;
   };
   double acc[1] = {0.0};
-  uint8_t fv[RS];
-  b_strips<true, T, RS>(V, e.y, pval, [&](int u, int c) { fv[u] = flags[c]; },
-                    [&](int u, int c, int i, int j, T pc, T pw, T pe, T ps, T pnn) {
-                      const T qc = b_apply5<T>(V, fv[u], i, j, pc, pw, pe, ps, pnn);
-                      pn[c] = pc;
-                      q[c] = qc;
-                      acc[0] += (double)pc * (double)qc;
-                    });
-  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
+  bool walked = false;
+  if constexpr (sizeof(T) == 4) {
+    if (P.vec) {
+      constexpr int RSV = 2;
+      auto pval4 = [&](int k, int, int) -> float4 {   // all loads issued, then selected
+        const uint32_t fk = b_ldf4(flags + k);
+        const float4 zk = b_ld4(zraw + k);
+        const float4 pk = b_ld4(p_old + k);
+        float o[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          const float z = (b_fl(fk, s) & F_SOLV) ? b_el(zk, s) - tm : 0.f;
+          o[s] = first ? z : b_el(pk, s) * tb + z;
+        }
+        return make_float4(o[0], o[1], o[2], o[3]);
+      };
+      uint32_t fw[RSV];
+      b_vstrips<true, RSV>(V, e.y, pval4, pval, [&](int u, int k) { fw[u] = b_ldf4(flags + k); },
+                           [&](int u, int k, int i, int j, const float(&pc)[4], const float(&pw)[4],
+                               const float(&pe)[4], const float(&ps)[4], const float(&pnb)[4]) {
+                             float qc[4];
+#pragma unroll
+                             for (int s = 0; s < 4; ++s) {
+                               qc[s] = b_apply5<float>(V, b_fl(fw[u], s), i, j + s, pc[s], pw[s], pe[s], ps[s],
+                                                       pnb[s]);
+                               acc[0] += (double)pc[s] * (double)qc[s];
+                             }
+                             b_st4(pn + k, pc);
+                             b_st4(q + k, qc);
+                           });
+      walked = true;
+    }
+  }
+  if (!walked) {
+    uint8_t fv[RS];
+    b_strips<true, T, RS>(V, e.y, pval, [&](int u, int c) { fv[u] = flags[c]; },
+                      [&](int u, int c, int i, int j, T pc, T pw, T pe, T ps, T pnn) {
+                        const T qc = b_apply5<T>(V, fv[u], i, j, pc, pw, pe, ps, pnn);
+                        pn[c] = pc;
+                        q[c] = qc;
+                        acc[0] += (double)pc * (double)qc;
+                      });
+  }
+  b_reduce<1>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, b_nchunks(P), [&](double* t) {
     P.S[S_PQ] = t[0];
     P.S[S_ALPHA] = P.S[S_RHO] / t[0];
   });
@@ -858,26 +1015,62 @@ B_STRIP_KERNEL k_b_cg_xr(const BProb<T>* __restrict__ probs, int nprob,
     T* __restrict__ xs = P.xs;
     T* __restrict__ r = P.r;
     double acc[2] = {0, 0};
-    T pv[RS], xv[RS], rv[RS], qv[RS];
-    uint8_t fv[RS];
-    b_strips<false, T, RS>(
-        V, e.y, [](int, int, int) { return (T)0; },
-        [&](int u, int c) {
-          pv[u] = pn[c];
-          xv[u] = xs[c];
-          rv[u] = r[c];
-          qv[u] = q[c];
-          fv[u] = flags[c];
-        },
-        [&](int u, int c, int, int, T, T, T, T, T) {
-          const double xc = (double)xv[u] + alpha * (double)pv[u];
-          const double rc = (double)(T)((double)rv[u] - alpha * (double)qv[u]);
-          xs[c] = (T)xc;
-          r[c] = (T)rc;
-          acc[0] += rc * rc;
-          if (fv[u] & F_SOLV) acc[1] += rc;
-        });
-    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.s_chunks, [&](double* t) {
+    bool walked = false;
+    if constexpr (sizeof(T) == 4) {
+      if (P.vec) {
+        constexpr int RSV = 2;
+        float4 pw[RSV], xw[RSV], rw[RSV], qw[RSV];
+        uint32_t fw[RSV];
+        b_vstrips<false, RSV>(
+            V, e.y, [](int, int, int) { return make_float4(0.f, 0.f, 0.f, 0.f); },
+            [](int, int, int) { return 0.f; },
+            [&](int u, int k) {
+              pw[u] = b_ld4(pn + k);
+              xw[u] = b_ld4(xs + k);
+              rw[u] = b_ld4(r + k);
+              qw[u] = b_ld4(q + k);
+              fw[u] = b_ldf4(flags + k);
+            },
+            [&](int u, int k, int, int, const float(&)[4], const float(&)[4], const float(&)[4],
+                const float(&)[4], const float(&)[4]) {
+              float xo[4], ro[4];
+#pragma unroll
+              for (int s = 0; s < 4; ++s) {
+                const double xc = (double)b_el(xw[u], s) + alpha * (double)b_el(pw[u], s);
+                const double rc = (double)(float)((double)b_el(rw[u], s) - alpha * (double)b_el(qw[u], s));
+                xo[s] = (float)xc;
+                ro[s] = (float)rc;
+                acc[0] += rc * rc;
+                if (b_fl(fw[u], s) & F_SOLV) acc[1] += rc;
+              }
+              b_st4(xs + k, xo);
+              b_st4(r + k, ro);
+            });
+        walked = true;
+      }
+    }
+    if (!walked) {
+      T pv[RS], xv[RS], rv[RS], qv[RS];
+      uint8_t fv[RS];
+      b_strips<false, T, RS>(
+          V, e.y, [](int, int, int) { return (T)0; },
+          [&](int u, int c) {
+            pv[u] = pn[c];
+            xv[u] = xs[c];
+            rv[u] = r[c];
+            qv[u] = q[c];
+            fv[u] = flags[c];
+          },
+          [&](int u, int c, int, int, T, T, T, T, T) {
+            const double xc = (double)xv[u] + alpha * (double)pv[u];
+            const double rc = (double)(T)((double)rv[u] - alpha * (double)qv[u]);
+            xs[c] = (T)xc;
+            r[c] = (T)rc;
+            acc[0] += rc * rc;
+            if (fv[u] & F_SOLV) acc[1] += rc;
+          });
+    }
+    b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, b_nchunks(P), [&](double* t) {
       double* S = P.S;
       int* I = P.I;
       const int it = I[I_IT] + 1;
@@ -1129,6 +1322,88 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
   T* __restrict__ xo = b_fine_buf(P, dst);
   T* __restrict__ lres0 = P.lres[0];
   double acc[2] = {0, 0};
+  if constexpr (sizeof(T) == 4) {
+    if (P.vec) {
+      constexpr int RSV = 2;
+      uint32_t fw[RSV];
+      float4 rw[RSV];
+      auto vload = [&](int u, int k) {
+        fw[u] = b_ldf4(flags + k);
+        rw[u] = b_ld4(r + k);
+      };
+      auto vb = [&](int u, int s) -> float { return (b_fl(fw[u], s) & F_SOLV) ? b_el(rw[u], s) - mr : 0.f; };
+      if (MODE == FM_WDB) {
+        b_vstrips<false, RSV>(V, e.y, [](int, int, int) { return make_float4(0.f, 0.f, 0.f, 0.f); },
+                              [](int, int, int) { return 0.f; }, vload,
+                              [&](int u, int k, int i, int j, const float(&)[4], const float(&)[4],
+                                  const float(&)[4], const float(&)[4], const float(&)[4]) {
+                                float o[4];
+#pragma unroll
+                                for (int s = 0; s < 4; ++s) o[s] = (float)b_wdinv(V, b_fl(fw[u], s), i, j + s) * vb(u, s);
+                                b_st4(xo + k, o);
+                              });
+      } else if (MODE == FM_PRE) {
+        // first sweep from zero, x = W b, and the residual b - A W b
+        auto xw1 = [&](int k, int ii, int jj) -> float {
+          const uint8_t fk = flags[k];
+          const float rk = r[k];
+          const float bk = (fk & F_SOLV) ? rk - mr : 0.f;
+          return (float)b_wdinv(V, fk, ii, jj) * bk;
+        };
+        auto xw4 = [&](int k, int ii, int jj) -> float4 {   // all loads issued, then selected
+          const uint32_t fk = b_ldf4(flags + k);
+          const float4 rk = b_ld4(r + k);
+          float o[4];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) {
+            const uint8_t f = b_fl(fk, s);
+            const float bk = (f & F_SOLV) ? b_el(rk, s) - mr : 0.f;
+            o[s] = (float)b_wdinv(V, f, ii, jj + s) * bk;
+          }
+          return make_float4(o[0], o[1], o[2], o[3]);
+        };
+        b_vstrips<true, RSV>(V, e.y, xw4, xw1, vload,
+                             [&](int u, int k, int i, int j, const float(&xc)[4], const float(&xwe)[4],
+                                 const float(&xe)[4], const float(&xsv)[4], const float(&xn)[4]) {
+                               float o[4];
+#pragma unroll
+                               for (int s = 0; s < 4; ++s)
+                                 o[s] = vb(u, s) - b_apply5<float>(V, b_fl(fw[u], s), i, j + s, xc[s], xwe[s], xe[s],
+                                                                   xsv[s], xn[s]);
+                               b_st4(xo + k, xc);
+                               b_st4(lres0 + k, o);
+                             });
+      } else {
+        b_vstrips<true, RSV>(V, e.y, [&](int k, int, int) { return b_ld4(x + k); },
+                             [&](int k, int, int) -> float { return x[k]; }, vload,
+                             [&](int u, int k, int i, int j, const float(&xc)[4], const float(&xwe)[4],
+                                 const float(&xe)[4], const float(&xsv)[4], const float(&xn)[4]) {
+                               float o[4];
+#pragma unroll
+                               for (int s = 0; s < 4; ++s) {
+                                 const uint8_t f = b_fl(fw[u], s);
+                                 const float ax = b_apply5<float>(V, f, i, j + s, xc[s], xwe[s], xe[s], xsv[s], xn[s]);
+                                 if (MODE == FM_RESID) {
+                                   o[s] = vb(u, s) - ax;
+                                 } else {
+                                   const float xnew = xc[s] + (float)b_wdinv(V, f, i, j + s) * (vb(u, s) - ax);
+                                   o[s] = xnew;
+                                   if (MODE == FM_LAST && (f & F_SOLV)) {
+                                     acc[0] += (double)xnew;
+                                     acc[1] += (double)b_el(rw[u], s) * (double)xnew;
+                                   }
+                                 }
+                               }
+                               b_st4(MODE == FM_RESID ? lres0 + k : xo + k, o);
+                             });
+      }
+      if (MODE != FM_LAST) return;
+      b_reduce<2>(acc, sh.partials + (long)P.red_base * 8, P.counter, e.y, P.v_chunks, [&](double* t) {
+        b_last_close(P, t);
+      });
+      return;
+    }
+  }
   uint8_t fv[RS];
   T rv[RS];
   auto load = [&](int u, int c) {

@@ -27,6 +27,7 @@ struct pycfd_batch {
   int ell_group = kBGroup;                 // problems per block of the coarse-level launches (1 or kBGroup)
   int stencil_req = 0;                     // level-0 transfers as stencils, as asked
   int stencil = 0;                         // ... and in force (fused down sweep from the fine level)
+  int scalar_strips = 0;                   // FP32 solver kernels on scalar strips even where rows allow vectors
   int* order = nullptr;                    // problems by size, largest first (coarse kernel)
   std::vector<pycfd_solver*> solvers;
   pycfd_solver* mem = nullptr;             // owner of the batch's own device allocations
@@ -36,6 +37,7 @@ struct pycfd_batch {
   int depth = 0;                           // most levels of any problem
   BMapHost fine;                           // every chunk of tiles of every problem
   BMapHost strip;                          // every chunk of warp strips of every problem (solver kernels)
+  BMapHost vstrip;                         // the CG and level-0 sweep kernels: vector chunks where in force
   BMapHost halo;                           // every staged tile of every problem (stencil transfers)
   BMapHost pstrip;                         // every chunk of predictor strips of every problem
   // row-block maps per depth d (problems whose level d runs per level):
@@ -180,7 +182,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
 
   // per-problem records
   std::vector<BProb<T>> pr(n);
-  std::vector<int2> fine, strip, pstrip, halo;
+  std::vector<int2> fine, strip, vstrip, pstrip, halo;
   B->nlev.assign(n, 0);
   B->depth = 0;
   int red_rows = 0;
@@ -208,6 +210,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     P.s_segs = (s->g.ny + kBSegCols - 1) / kBSegCols;
     P.s_items = ((s->g.nx + kBStripRows - 1) / kBStripRows) * P.s_segs;
     P.s_chunks = (P.s_items + kBStripItems - 1) / kBStripItems;
+    P.v_chunks = (s->g.nx + kBVecRows - 1) / kBVecRows;
     {
       const int segs = (s->g.ny + 3 + kBPredCols - 1) / kBPredCols;
       const int items = segs * ((s->g.nx + 3 + kBStripRows - 1) / kBStripRows);
@@ -225,7 +228,7 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
       P.h_tiles = ((s->g.nx + tr - 1) / tr) * P.h_tiles_j;
     }
     P.red_base = red_rows;
-    red_rows += std::max(std::max(P.chunks, P.s_chunks), P.h_tiles);
+    red_rows += std::max(std::max(P.chunks, std::max(P.s_chunks, P.v_chunks)), P.h_tiles);
     P.flags = s->flags;
     P.solid = s->solid;
     P.bc_kind = s->bc_kind_dev;
@@ -260,6 +263,14 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     TRY(dalloc(B->mem, &P.lxa[0], nc0));
     TRY(dalloc(B->mem, &P.lxb[0], nc0));
     TRY(dalloc(B->mem, &P.lres[0], nc0));
+    {
+      // vector strips: FP32 vectors, rows a multiple of 4 long, every vector the
+      // kernels read or write as float4 16-byte aligned (flags 4-byte aligned)
+      auto a16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+      const bool al = a16(P.xs) && a16(P.r) && a16(P.z) && a16(P.pa) && a16(P.pb) && a16(P.q) &&
+                      a16(P.lxa[0]) && a16(P.lxb[0]) && a16(P.lres[0]) && ((uintptr_t)P.flags & 3u) == 0;
+      P.vec = (sizeof(T) == 4 && !B->scalar_strips && s->g.ny % 4 == 0 && al) ? 1 : 0;
+    }
     const std::vector<Level>& K = keep[hid[i]];
     for (int l = 1; l < P.nlev; ++l) {
       TRY(dalloc(B->mem, &P.lb[l], K[l].n));
@@ -284,11 +295,13 @@ int batch_build(pycfd_batch* B, const pycfd_solver_desc* descs, const int* struc
     for (int l = 0; l < kBMaxLevels; ++l) P.lv[l] = hh[hid[i]].lv[l];
     for (int c = 0; c < P.chunks; ++c) fine.push_back(make_int2(i, c));
     for (int c = 0; c < P.s_chunks; ++c) strip.push_back(make_int2(i, c));
+    for (int c = 0, nc = P.vec ? P.v_chunks : P.s_chunks; c < nc; ++c) vstrip.push_back(make_int2(i, c));
     for (int c = 0; c < P.h_tiles; ++c) halo.push_back(make_int2(i, c));
     for (int c = 0; c < P.p_chunks; ++c) pstrip.push_back(make_int2(i, c));
   }
   TRY(upload_map(B, &B->fine, fine));
   TRY(upload_map(B, &B->strip, strip));
+  TRY(upload_map(B, &B->vstrip, vstrip));
   TRY(upload_map(B, &B->halo, halo));
   TRY(upload_map(B, &B->pstrip, pstrip));
   // problems grouped by structure (the dense tail's block groups)
@@ -461,7 +474,7 @@ template <class T, int MODE>
 int b_fine(pycfd_batch* B, int src, int dst, cudaStream_t st) {
   const int id = MODE == FM_LAST ? 2 : MODE == FM_PRE ? 3 : 0;
   b_prof(B, id, st);
-  BLAUNCH((k_b_fine<T, MODE>), B->strip.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->strip.e, src,
+  BLAUNCH((k_b_fine<T, MODE>), B->vstrip.n, kBThreads, 0, st, probs_of<T>(B), hiers_of<T>(B), B->vstrip.e, src,
           dst, B->sh);
   b_prof(B, id, st);
   return 0;
@@ -640,10 +653,10 @@ int b_solve_fp64(pycfd_batch* B, cudaStream_t st) {
   auto pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
     b_prof(B, 1, s2);
-    BLAUNCH(k_b_cg_pq<T>, B->strip.n, kBThreads, 0, s2, P, B->strip.e, B->sh);
+    BLAUNCH(k_b_cg_pq<T>, B->vstrip.n, kBThreads, 0, s2, P, B->vstrip.e, B->sh);
     b_prof(B, 1, s2);
     b_prof(B, 5, s2);
-    BLAUNCH(k_b_cg_xr<T>, B->strip.n, kBThreads, 0, s2, P, B->n, B->strip.e, B->maxiter, B->sh, ctl);
+    BLAUNCH(k_b_cg_xr<T>, B->vstrip.n, kBThreads, 0, s2, P, B->n, B->vstrip.e, B->maxiter, B->sh, ctl);
     b_prof(B, 5, s2);
     return 0;
   };
@@ -677,10 +690,10 @@ int b_solve_mixed(pycfd_batch* B, cudaStream_t st) {
   auto inner_pass = [&](cudaStream_t s2) -> int {
     TRY(b_vcycle<T>(B, s2));
     b_prof(B, 1, s2);
-    BLAUNCH(k_b_cg_pq<T>, B->strip.n, kBThreads, 0, s2, P, B->strip.e, B->sh);
+    BLAUNCH(k_b_cg_pq<T>, B->vstrip.n, kBThreads, 0, s2, P, B->vstrip.e, B->sh);
     b_prof(B, 1, s2);
     b_prof(B, 5, s2);
-    BLAUNCH(k_b_cg_xr<T>, B->strip.n, kBThreads, 0, s2, P, B->n, B->strip.e, kInnerMaxIterB, B->sh, inner);
+    BLAUNCH(k_b_cg_xr<T>, B->vstrip.n, kBThreads, 0, s2, P, B->n, B->vstrip.e, kInnerMaxIterB, B->sh, inner);
     b_prof(B, 5, s2);
     return 0;
   };
@@ -829,6 +842,7 @@ int pycfd_batch_create(const pycfd_solver_desc* descs, const int* structure, con
   B->fused_from = opts->fused_from == 2 ? 2 : 1;
   B->ell_group = opts->ell_group == 1 ? 1 : kBGroup;
   B->stencil_req = opts->stencil_transfer ? 1 : 0;
+  B->scalar_strips = opts->scalar_strips ? 1 : 0;
   B->mem = new pycfd_solver();
   B->mem->pdl = opts->programmatic_launch ? 1 : 0;
   B->solvers.assign(n, nullptr);

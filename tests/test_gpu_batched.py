@@ -308,3 +308,35 @@ def test_loop_cap_ends_device_loops_and_the_batch_goes_on(precision):
     assert b.capped() == 0
     st = b.status()
     assert (st["status"] == 0).all() and (st["steps"] == 5).all()
+
+
+def test_vector_strips_match_scalar_strips():
+    """The mixed form's FP32 CG and level-0 sweep kernels on 128-column float4 strips
+    against the 30-column scalar strips: rows a multiple of 4 long and not (those
+    stay scalar in one launch with the vector ones), a second segment one lane wide
+    (132 columns), both periodic axes, an obstacle beside an outlet and a periodic-y
+    channel (edge columns wrapped across the seam)."""
+    from pycfd_b200.batch import BatchedSolver, BatchOptions, cavity_batch_configs
+    cav = cavity_batch_configs(count=6, seed=11, sizes=(25, 32, 37, 48, 132), re_range=(100.0, 1000.0),
+                               tol=1e-11)
+    probs = [_case(n) for n in REF_CASES]
+    batches = [dict(configs=cav, steps=5),
+               dict(configs=[p[0] for p in probs], steps=min(p[4]["steps"] for p in probs) - 1,
+                    kw=dict(obstacles=[p[1] for p in probs], u_init=[p[2] for p in probs],
+                            v_init=[p[3] for p in probs]))]
+    for bt in batches:
+        out, its = [], []
+        for scalar in (True, False):
+            b = BatchedSolver(bt["configs"], BatchOptions(precision="mixed", scalar_strips=scalar),
+                              **bt.get("kw", {}))
+            b.step(bt["steps"])
+            st = b.status()
+            assert all(f == 0 for f in st["frozen"])
+            out.append([b.fields[k].numpy() for k in range(len(bt["configs"]))])
+            its.append(st["iterations"])
+            for k in range(len(bt["configs"])):
+                assert b.field_stats(k).max_div < 1e-8
+        for fa, fb in zip(*out):
+            for x, y in zip(fa[:2], fb[:2]):
+                assert rel(x, y) < 1e-7
+        assert np.abs(its[0] - its[1]).max() <= 2, its
