@@ -451,6 +451,23 @@ def run_batch(args, world, rank, local):
                              "gb_s": (v[2] / (v[0] / 1e3) / 1e9) if v[0] > 0 and v[2] else None}
                             for k, v in prof.items()},
                 "traffic_source": "profiles/roofline_traffic.json (one ncu capture of this kernel)"}
+        if args.parts > 1:
+            # the same kernel kinds at full size: the whole batch in one engine, so every
+            # launch covers every cavity (the timed step's parts launch a quarter each)
+            b1 = BatchedSolver(cfgs, opts)
+            b1.step(1, record=False)
+            one = {}
+            for kid in prof:
+                kms1, kn1, kits1 = b1.profile(kid, 1)
+                kb1 = batch_kernel_bytes(kid, cells, kits1, s_bytes)
+                gbs = kb1 / (kms1 / 1e3) / 1e9 if kms1 > 0 and kb1 else None
+                one[KERNEL_NAMES[kid].split(" ")[0] + ("" if kid not in (2, 3) else f"[{kid}]")] = {
+                    "us_per_launch": 1e3 * kms1 / max(kn1, 1), "launches": kn1, "gb_s": gbs,
+                    "frac": gbs / hbm if gbs else None}
+            del b1
+            roof["one_engine"] = {"note": "each kind timed by CUDA events around its eager launches "
+                                          "over one step of the whole batch in one engine",
+                                  "kernels": one}
     # end to end: (u, v) of every cavity from pinned host memory, one step, (u, v, p) back
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
     e2e = None

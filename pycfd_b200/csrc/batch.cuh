@@ -274,17 +274,30 @@ struct BView {
   const double* dtab;
   const double* wtab;
   int segs, items;   // warp strips: 32-column segments per row, strips x segments
+  // FP32 copies for the vector strips, indexed by the flag's low five bits (a
+  // cell without F_SOLV reads 1 and w0): the values (float)b_diag and
+  // (float)b_wdinv give away from Dirichlet edges
+  const float* df;
+  const float* wf;
+  float cxf, cyf;
 };
 
 // Declares `V` for problem record P; every thread of the block must reach it.
 #define B_VIEW(V, P)                                                                           \
   __shared__ double V##_dt[16], V##_wt[16];                                                    \
+  __shared__ float V##_df[32], V##_wf[32];                                                     \
   if (threadIdx.x < 16) {                                                                      \
     V##_dt[threadIdx.x] = (P).dtab[threadIdx.x];                                               \
     V##_wt[threadIdx.x] = (P).wtab[threadIdx.x];                                               \
   }                                                                                            \
+  if (threadIdx.x < 32) {                                                                      \
+    const bool sv_ = (threadIdx.x & F_SOLV) != 0;                                              \
+    V##_df[threadIdx.x] = sv_ ? (float)(P).dtab[threadIdx.x & 15] : 1.0f;                      \
+    V##_wf[threadIdx.x] = sv_ ? (float)(P).wtab[threadIdx.x & 15] : (float)((P).w0 * (1.0 / 1.0)); \
+  }                                                                                            \
   __syncthreads();                                                                             \
-  const BView V{(P).g, (P).any_dir, (P).w0, V##_dt, V##_wt, (P).s_segs, (P).s_items}
+  const BView V{(P).g, (P).any_dir, (P).w0, V##_dt, V##_wt, (P).s_segs, (P).s_items,          \
+                V##_df, V##_wf, (float)(P).g.cx, (float)(P).g.cy}
 
 __device__ __forceinline__ double b_diag(const BView& V, uint8_t f, int i, int j) {
   if (!(f & F_SOLV)) return 1.0;
@@ -297,6 +310,18 @@ __device__ __forceinline__ double b_wdinv(const BView& V, uint8_t f, int i, int 
     return V.w0 * (1.0 / fine_diag(f, i, j, V.g));
   return V.wtab[f & 15];
 }
+// (float)b_diag and (float)b_wdinv from the block's FP32 tables (one 32-bit
+// shared load, no conversion, away from Dirichlet edges).
+__device__ __forceinline__ float b_diag_f(const BView& V, uint8_t f, int i, int j) {
+  if (V.any_dir && (f & F_SOLV) && (i == 0 || j == 0 || i == V.g.nx - 1 || j == V.g.ny - 1))
+    return (float)fine_diag(f, i, j, V.g);
+  return V.df[f & 31];
+}
+__device__ __forceinline__ float b_wdinv_f(const BView& V, uint8_t f, int i, int j) {
+  if (V.any_dir && (f & F_SOLV) && (i == 0 || j == 0 || i == V.g.nx - 1 || j == V.g.ny - 1))
+    return (float)(V.w0 * (1.0 / fine_diag(f, i, j, V.g)));
+  return V.wf[f & 31];
+}
 
 // (A x) at a cell from its value and its four neighbours' values, fine_apply's
 // terms in its order (diagonal, west, east, south, north), in arithmetic type A.
@@ -307,6 +332,16 @@ __device__ __forceinline__ A b_apply5(const BView& V, uint8_t f, int i, int j, T
   if (f & F_E) acc += (A)V.g.cx * (A)e;
   if (f & F_S) acc += (A)V.g.cy * (A)s;
   if (f & F_N) acc += (A)V.g.cy * (A)n;
+  return acc;
+}
+// b_apply5<float> from the FP32 tables: the same value.
+__device__ __forceinline__ float b_apply5f(const BView& V, uint8_t f, int i, int j, float c, float w, float e,
+                                           float s, float n) {
+  float acc = b_diag_f(V, f, i, j) * c;
+  if (f & F_W) acc += V.cxf * w;
+  if (f & F_E) acc += V.cxf * e;
+  if (f & F_S) acc += V.cyf * s;
+  if (f & F_N) acc += V.cyf * n;
   return acc;
 }
 
@@ -464,7 +499,7 @@ __device__ __forceinline__ void b_strips(const BView& V, int chunk, Op op, Load 
 // is the scalar strips' (the same operand, stencil and update); only the order
 // of the per-problem sums differs.
 #ifndef PCFD_BVEC_ROWS
-#define PCFD_BVEC_ROWS 16
+#define PCFD_BVEC_ROWS 32
 #endif
 constexpr int kBVecRows = PCFD_BVEC_ROWS;   // rows of one block of a vector-strip launch
 constexpr int kBVecCols = 128;              // columns of a warp segment (32 lanes x float4)
@@ -969,7 +1004,7 @@ B_STRIP_KERNEL k_b_cg_pq(const BProb<T>* __restrict__ probs,
                              float qc[4];
 #pragma unroll
                              for (int s = 0; s < 4; ++s) {
-                               qc[s] = b_apply5<float>(V, b_fl(fw[u], s), i, j + s, pc[s], pw[s], pe[s], ps[s],
+                               qc[s] = b_apply5f(V, b_fl(fw[u], s), i, j + s, pc[s], pw[s], pe[s], ps[s],
                                                        pnb[s]);
                                acc[0] += (double)pc[s] * (double)qc[s];
                              }
@@ -1339,7 +1374,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                   const float(&)[4], const float(&)[4], const float(&)[4]) {
                                 float o[4];
 #pragma unroll
-                                for (int s = 0; s < 4; ++s) o[s] = (float)b_wdinv(V, b_fl(fw[u], s), i, j + s) * vb(u, s);
+                                for (int s = 0; s < 4; ++s) o[s] = b_wdinv_f(V, b_fl(fw[u], s), i, j + s) * vb(u, s);
                                 b_st4(xo + k, o);
                               });
       } else if (MODE == FM_PRE) {
@@ -1348,7 +1383,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
           const uint8_t fk = flags[k];
           const float rk = r[k];
           const float bk = (fk & F_SOLV) ? rk - mr : 0.f;
-          return (float)b_wdinv(V, fk, ii, jj) * bk;
+          return b_wdinv_f(V, fk, ii, jj) * bk;
         };
         auto xw4 = [&](int k, int ii, int jj) -> float4 {   // all loads issued, then selected
           const uint32_t fk = b_ldf4(flags + k);
@@ -1358,7 +1393,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
           for (int s = 0; s < 4; ++s) {
             const uint8_t f = b_fl(fk, s);
             const float bk = (f & F_SOLV) ? b_el(rk, s) - mr : 0.f;
-            o[s] = (float)b_wdinv(V, f, ii, jj + s) * bk;
+            o[s] = b_wdinv_f(V, f, ii, jj + s) * bk;
           }
           return make_float4(o[0], o[1], o[2], o[3]);
         };
@@ -1368,7 +1403,7 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
                                float o[4];
 #pragma unroll
                                for (int s = 0; s < 4; ++s)
-                                 o[s] = vb(u, s) - b_apply5<float>(V, b_fl(fw[u], s), i, j + s, xc[s], xwe[s], xe[s],
+                                 o[s] = vb(u, s) - b_apply5f(V, b_fl(fw[u], s), i, j + s, xc[s], xwe[s], xe[s],
                                                                    xsv[s], xn[s]);
                                b_st4(xo + k, xc);
                                b_st4(lres0 + k, o);
@@ -1382,11 +1417,11 @@ B_STRIP_KERNEL k_b_fine(const BProb<T>* __restrict__ probs,
 #pragma unroll
                                for (int s = 0; s < 4; ++s) {
                                  const uint8_t f = b_fl(fw[u], s);
-                                 const float ax = b_apply5<float>(V, f, i, j + s, xc[s], xwe[s], xe[s], xsv[s], xn[s]);
+                                 const float ax = b_apply5f(V, f, i, j + s, xc[s], xwe[s], xe[s], xsv[s], xn[s]);
                                  if (MODE == FM_RESID) {
                                    o[s] = vb(u, s) - ax;
                                  } else {
-                                   const float xnew = xc[s] + (float)b_wdinv(V, f, i, j + s) * (vb(u, s) - ax);
+                                   const float xnew = xc[s] + b_wdinv_f(V, f, i, j + s) * (vb(u, s) - ax);
                                    o[s] = xnew;
                                    if (MODE == FM_LAST && (f & F_SOLV)) {
                                      acc[0] += (double)xnew;

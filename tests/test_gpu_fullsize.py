@@ -63,3 +63,39 @@ def test_cylinder_2048x1024_against_oracle():
     assert np.all(gu[gpu.u_upd][gpu.u_face_solid] == 0.0)
     # the solve tolerance sets the divergence: match the oracle's own level
     assert gpu.max_divergence(f) < 2.0 * ref.max_divergence(u, v) + 1e-12
+
+
+def test_taylor_green_512_full_run_fp64_and_mixed():
+    """The vortex over its full 500 steps (dt = 0.4 * 2 pi / 512, t = 2.45): the FP64 path
+    and the mixed form each against the analytic decay u, v ~ exp(-2 nu t),
+    p ~ exp(-4 nu t) (discretisation error, about 6e-8 on velocity), the mixed form
+    within 1e-6 of FP64 on velocity, max|div u| <= 1e-8 for both."""
+    from pycfd_b200.solver import GpuOptions, ProjectionSolver
+    cfg = cases.to_config(cases.tgv_cfg(512), SimulationConfig, BCSpec, BCKind)
+    u0, v0 = cases.tg_init(512, 512, cfg.lx, cfg.ly)
+    steps = 500
+    out = {}
+    for prec in ("fp64", "mixed"):
+        s = ProjectionSolver(cfg, options=GpuOptions(precision=prec))
+        f = s.initialize(u0, v0)
+        for _ in range(steps):
+            f = s.advance(f, cfg.dt)
+        t = f.t
+        assert t == pytest.approx(steps * cfg.dt, rel=1e-12)
+        Xu, Yu = s.mesh.u_grid()
+        Xv, Yv = s.mesh.v_grid()
+        ue = np.sin(Xu) * np.cos(Yu) * np.exp(-2 * cfg.nu * t)
+        ve = -np.cos(Xv) * np.sin(Yv) * np.exp(-2 * cfg.nu * t)
+        pe = 0.25 * (np.cos(2 * s.mesh.xc)[:, None] + np.cos(2 * s.mesh.yc)[None, :]) * np.exp(-4 * cfg.nu * t)
+        pe -= pe.mean()
+        u = f.u_phys.cpu().numpy()
+        v = f.v_phys.cpu().numpy()
+        p = f.p[1:-1, 1:-1].cpu().numpy()
+        p = p - p.mean()
+        assert rel(u, ue) < 1e-6 and rel(v, ve) < 1e-6, prec
+        assert rel(p, pe) < 1e-3, prec
+        assert s.max_divergence(f) <= 1e-8, prec
+        out[prec] = (u, v)
+    scale = max(np.abs(out["fp64"][0]).max(), np.abs(out["fp64"][1]).max())
+    dv = max(np.abs(out["mixed"][0] - out["fp64"][0]).max(), np.abs(out["mixed"][1] - out["fp64"][1]).max())
+    assert dv / scale <= 1e-6
