@@ -92,6 +92,43 @@ def test_library_exports_every_header_symbol():
     assert L.pycfd_version() == 1
 
 
+# ctypes mirrors of the header's structs (pycfd_b200/_lib.py) and the C names they bind
+_STRUCTS = {"Shape": "pycfd_shape", "AdjArgs": "pycfd_adj_args", "MgLevel": "pycfd_mg_level",
+            "SolverDesc": "pycfd_solver_desc", "DtControl": "pycfd_dt_control",
+            "BatchOpts": "pycfd_batch_opts", "Stats": "pycfd_stats", "FieldStats": "pycfd_field_stats"}
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Every struct the Python binding passes through the C ABI has the header's size and
+    field offsets: a C program compiled against include/pycfd_b200.h prints sizeof and
+    offsetof for each field the ctypes mirror names, in the mirror's order."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pycfd_b200.h"', "int main(void) {"]
+    expect = []
+    for py, cname in _STRUCTS.items():
+        cls = getattr(_lib, py)
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expect.append((py, "sizeof", ctypes.sizeof(cls)))
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+            expect.append((py, fname, getattr(cls, fname).offset))
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                           text=True).stdout.split()]
+    assert len(got) == len(expect)
+    for (py, what, want), have in zip(expect, got):
+        assert have == want, (py, what, have, want)
+
+
 def test_config_validation_and_roundtrip():
     with pytest.raises(ValueError, match="at least 4x4"):
         SimulationConfig(nx=2, ny=8)
