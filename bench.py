@@ -10,8 +10,9 @@ max over ranks).  The working set (~0.5 GB) exceeds L2.  Beside it the line
 carries the batched engine in FP64 and the plain FP64 path (one single-problem
 solver per cavity, recorded steps on 16 streams), their ratios, the per-kernel
 roofline of one eager step (each part's launches, and the same kernels at full size
-in one engine), the end-to-end figure through host buffers and the CPU baseline.  Under torchrun the 256*N cavities of one seeded draw are split
-over the ranks by cell count (no exchange on the data path).
+in one engine), the end-to-end figure through host buffers and the CPU baseline.
+Under torchrun the 256*N cavities of one seeded draw are split over the ranks by
+cell count (no exchange on the data path).
 
 ``--workload tgv512``: one SSP-RK3 step of the 512x512 Taylor-Green vortex on the
 single-problem path (L2 flushed between steps).  Other workloads: adjoint,
