@@ -373,8 +373,8 @@ __global__ void k_resnorm(double* __restrict__ x, const double* __restrict__ b,
 // FP32 solve A e = r from e = 0 (r32 = r).  The inner solve stops at
 // max(inner_tol ||r||, kIrLastFraction tol ||b||): a pass that only has to take
 // the residual the rest of the way to the outer target stops there instead of
-// reducing it by the full inner_tol (the outer test on the true residual stays
-// the judge).
+// reducing it by the full inner_tol (the outer test on the true residual still
+// decides convergence).
 constexpr double kIrLastFraction = 0.5;
 __global__ void k_ir_residual(double* __restrict__ b, double* __restrict__ x,
                               float* __restrict__ r32, float* __restrict__ e32,

@@ -3,7 +3,7 @@
 The outer loop stops on the true FP64 residual ||b - A p|| < tol ||b||, so the
 form reaches the same tolerance as the FP64 path; velocity, pressure and
 divergence differences against the reference's own step are checked here at
-1e-10 relative (the same bar as the FP64 path), and the north_star's looser
+1e-10 relative (the same bar as the FP64 path), and the mixed form's own looser
 bars (velocity error <= 1e-6 against the FP64 result, max|div u| <= 1e-8) on a
 Taylor-Green vortex.
 """
